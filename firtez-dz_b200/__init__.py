@@ -1,0 +1,202 @@
+"""firtez-dz B200: GPU Stokes synthesis of FIRTEZ-dz behind a C-ABI.
+
+Host-side mirror of the reference's interface for the hot path, over ctypes:
+
+  * ``lines_parse(text)``            -- NREAD_LINES_DATABASE (src/lines_database.f90:380)
+  * ``regions_from_lines_section``   -- the LINES: section of the control file
+                                        (src/input_file.f90:290-366) + WAVE_INIT
+  * ``Synthesis(...).forward(model)``-- FORWARD3D/FORWARD1D (src/forward.f90:43, :857)
+                                        batched over columns on one GPU
+
+Arrays use the reference layouts: ``model`` is MODEL(NZ,13,ncol) REAL*4,
+i.e. a C-ordered numpy array of shape (ncol, 13, nz); ``syn`` is
+RSYN1D(NFREQ,ncol) REAL*8, i.e. shape (ncol, 4, numw).
+
+The library is ``libfzb200.so`` next to this file (built by ``make`` in this
+directory).  There is no CPU path: without the library or without a CUDA
+device every compute call raises.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libfzb200.so")
+
+MAXBLEND = 8
+
+# Model parameter indices (src/atm_param.f90:38-75), 0-based
+TEM, PG, RHO, PEL, MW, BX, BY, BZ, VX, VY, VZ, TAU5, ZZ = range(13)
+
+FZ_OK, FZ_CHEM_NOCONV, FZ_NAN = 0, 1, 2
+
+LINE_DTYPE = np.dtype([
+    ("num", "<i4"), ("zn", "<i4"), ("ion", "<i4"), ("flag", "<i4"), ("otr", "<i4", 2),
+    ("abo_ierr", "<i4"), ("pad", "<i4"),
+    ("l0", "<f8"), ("loggf", "<f8"), ("eplow", "<f8"), ("alpha", "<f8"), ("sigma", "<f8"),
+    ("sl", "<f8"), ("ll", "<f8"), ("jl", "<f8"), ("su", "<f8"), ("lu", "<f8"), ("ju", "<f8"),
+    ("elowlim", "<f8"), ("eupplim", "<f8"),
+], align=True)
+
+REGION_DTYPE = np.dtype([
+    ("nblend", "<i4"), ("line", "<i4", MAXBLEND), ("wdif", "<f8", MAXBLEND),
+    ("numwave", "<i4"), ("pad", "<i4"), ("wave_ini", "<f8"), ("dlambda", "<f8"),
+], align=True)
+
+
+class FzError(RuntimeError):
+    pass
+
+
+_lib = None
+
+
+def build():
+    """Compile libfzb200.so for sm_100a (nvcc cross-compiles without a GPU)."""
+    import subprocess
+    subprocess.check_call(["make", "-s", "-C", HERE])
+
+
+def lib():
+    """The loaded CUDA library (raises if it is missing)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise FzError("libfzb200.so not built (run make in %s)" % HERE)
+        L = ctypes.CDLL(LIB_PATH)
+        P = ctypes.c_void_p
+        L.fz_version.restype = ctypes.c_int
+        L.fz_strerror.restype = ctypes.c_char_p
+        L.fz_strerror.argtypes = [ctypes.c_int]
+        L.fz_lines_parse.argtypes = [ctypes.c_char_p, P, ctypes.c_int]
+        L.fz_create.argtypes = [ctypes.POINTER(P), P, ctypes.c_int, P, ctypes.c_int, ctypes.c_int, P, ctypes.c_int]
+        L.fz_destroy.argtypes = [P]
+        L.fz_numw.argtypes = [P]
+        L.fz_get_gain.argtypes = [P, P]
+        L.fz_forward.argtypes = [P, ctypes.c_int, P, ctypes.c_int, P, P, P]
+        L.fz_forward_device.argtypes = [P, ctypes.c_int, P, ctypes.c_int, P, P, P, P]
+        L.fz_profile_enable.argtypes = [P, ctypes.c_int]
+        L.fz_profile_read.argtypes = [P, P, P, ctypes.c_int]
+        L.fz_measure_fp32_peak.argtypes = [ctypes.c_int, P]
+        _lib = L
+    return _lib
+
+
+def _check(rc):
+    if rc < 0:
+        raise FzError(lib().fz_strerror(rc).decode())
+    return rc
+
+
+def _p(a):
+    return a.ctypes.data_as(ctypes.c_void_p)
+
+
+def lines_parse(text):
+    """Parse lines_database.dat text into a LINE_DTYPE array."""
+    out = np.zeros(512, dtype=LINE_DTYPE)
+    n = _check(lib().fz_lines_parse(text.encode(), _p(out), len(out)))
+    return out[:n].copy()
+
+
+def regions_from_lines_section(section, lines):
+    """Regions from LINES: rows like ``4,5 500 -700.0 5.0``.
+
+    First field: database ids of the main line and its blends (comma
+    separated); then NUMWAVE, WAVE_INI [mA] and DELTA_LAMBDA [mA].  BLENDSDIFF
+    is 1e3*(lambda_blend - lambda_main) [mA] (src/input_file.f90:346-354)."""
+    ids = {int(n): i for i, n in enumerate(lines["num"])}
+    rows = [r.split() for r in section.strip().splitlines() if r.strip() and not r.strip().startswith("#")]
+    reg = np.zeros(len(rows), dtype=REGION_DTYPE)
+    for k, f in enumerate(rows):
+        nums = [int(x) for x in f[0].split(",") if x]
+        if len(nums) > MAXBLEND:
+            raise ValueError("too many blends")
+        reg["nblend"][k] = len(nums)
+        for b, n in enumerate(nums):
+            if n not in ids:
+                raise ValueError("line %d is not in the database" % n)
+            reg["line"][k, b] = ids[n]
+            if b > 0:
+                reg["wdif"][k, b] = 1.0e3 * (lines["l0"][ids[n]] - lines["l0"][ids[nums[0]]])
+        reg["numwave"][k] = int(f[1])
+        reg["wave_ini"][k] = float(f[2])
+        reg["dlambda"][k] = float(f[3])
+    return reg
+
+
+class Synthesis:
+    """A GPU synthesis context for one line set and height count."""
+
+    def __init__(self, lines, regions, nz, gain=None, device=0):
+        self.lines = np.ascontiguousarray(lines, dtype=LINE_DTYPE)
+        self.regions = np.ascontiguousarray(regions, dtype=REGION_DTYPE)
+        self.nz = int(nz)
+        self.numw = int(self.regions["numwave"].sum())
+        h = ctypes.c_void_p()
+        g = None if gain is None else np.ascontiguousarray(gain, dtype=np.float32).reshape(self.numw, 4)
+        _check(lib().fz_create(ctypes.byref(h), _p(self.lines), len(self.lines), _p(self.regions),
+                               len(self.regions), self.nz, None if g is None else _p(g), int(device)))
+        self._h = h
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().fz_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def gain(self):
+        """GAIN1D(4,NUMW) as a (numw, 4) float32 array."""
+        g = np.zeros((self.numw, 4), dtype=np.float32)
+        _check(lib().fz_get_gain(self._h, _p(g)))
+        return g
+
+    def forward(self, model, hydrostatic=False):
+        """Synthesise host-resident columns.  model: (ncol, 13, nz) float32.
+
+        Returns (syn (ncol, 4, numw) float64, model_out, status (ncol,))."""
+        m = np.ascontiguousarray(model, dtype=np.float32)
+        if m.ndim == 2:
+            m = m[None]
+        ncol, npar, nz = m.shape
+        if npar != 13 or nz != self.nz:
+            raise ValueError("model must be (ncol, 13, %d)" % self.nz)
+        syn = np.zeros((ncol, 4, self.numw))
+        mo = np.empty_like(m)
+        st = np.zeros(ncol, dtype=np.int32)
+        _check(lib().fz_forward(self._h, ncol, _p(m), int(bool(hydrostatic)), _p(syn), _p(mo), _p(st)))
+        return syn, mo, st
+
+    def profile(self, on=True):
+        _check(lib().fz_profile_enable(self._h, int(bool(on))))
+
+    def profile_read(self):
+        """{kernel: (total ms, launches)} since the last read."""
+        ms = np.zeros(2)
+        n = np.zeros(2, dtype=np.int32)
+        _check(lib().fz_profile_read(self._h, _p(ms), _p(n), 2))
+        return {"k_chem": (ms[0], int(n[0])), "k_synth": (ms[1], int(n[1]))}
+
+    def forward_device(self, model_ptr, ncol, syn_ptr, model_out_ptr, status_ptr=0, stream=0, hydrostatic=False):
+        """Enqueue a synthesis on device pointers (e.g. torch ``data_ptr()``)."""
+        _check(lib().fz_forward_device(self._h, int(ncol), ctypes.c_void_p(model_ptr), int(bool(hydrostatic)),
+                                       ctypes.c_void_p(syn_ptr), ctypes.c_void_p(model_out_ptr),
+                                       ctypes.c_void_p(status_ptr) if status_ptr else None,
+                                       ctypes.c_void_p(stream) if stream else None))
+
+
+def measure_fp32_peak(device=0):
+    """Measured FP32 FMA peak of the device in TFLOP/s."""
+    t = np.zeros(1)
+    _check(lib().fz_measure_fp32_peak(int(device), _p(t)))
+    return float(t[0])
+
+
+from . import atmos  # noqa: E402,F401

@@ -1,0 +1,124 @@
+/*
+ * firtez-dz B200 -- C-ABI of the GPU Stokes synthesis / pixel-wise
+ * Levenberg-Marquardt path of FIRTEZ-dz.
+ *
+ * Plain C types only; every array is a host or device pointer plus sizes.
+ * Layouts are the reference's (Fortran column-major):
+ *
+ *   model   MODEL(NZ,13,ncol) REAL*4, parameter order of src/atm_param.f90:38-75:
+ *           1 T[K] 2 Pg[dyn cm^-2] 3 rho[g cm^-3] 4 Pe 5 mu 6 Bx[G] 7 By 8 Bz
+ *           9 vx 10 vy 11 vz[cm/s] 12 log tau5 13 z[km]   (index 1 = bottom)
+ *   syn     RSYN1D(NFREQ,ncol) REAL*8, NFREQ = 4*NUMW, Stokes-major blocks
+ *           I(1:NUMW),Q,U,V already multiplied by GAIN (src/forward.f90:793-853)
+ *   gain    GAIN1D(4,NUMW) REAL*4 (src/normalization.f90:696-754)
+ *
+ * Return codes: 0 = OK, < 0 = API error (fz_strerror).  Per-column status
+ * words replace the reference's STOP statements.
+ */
+#ifndef FZ_B200_H
+#define FZ_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define FZ_MAXBLEND 8
+#define FZ_MAXLINES 64
+
+/* API errors */
+#define FZ_ERR_ARG (-1)
+#define FZ_ERR_CUDA (-2)
+#define FZ_ERR_NOMEM (-3)
+#define FZ_ERR_PARSE (-4)
+#define FZ_ERR_LIMIT (-5)
+#define FZ_ERR_STATE (-6)
+
+/* per-column status bits */
+#define FZ_OK 0
+#define FZ_CHEM_NOCONV 1 /* GET_RHO: >= 100 iterations or nH < 0 (chemical_equilibrium.f90:242) */
+#define FZ_NAN 2         /* non-finite opacity / Stokes (rtesolver.f90:337-352, voigt.f:88-95) */
+
+/* One row of lines_database.dat after NREAD_LINES_DATABASE
+ * (replaces the module arrays LINE_NUM, LINE_ZN, LINE_ION, LINE_L0, LOGGF,
+ * EPLOW, ALPHA, SIGMA, SL..JU of src/forward_param.f90:17-21). */
+typedef struct {
+  int32_t num, zn, ion, flag;
+  int32_t otr[2];
+  int32_t abo_ierr, pad;
+  double l0, loggf, eplow, alpha, sigma;
+  double sl, ll, jl, su, lu, ju;
+  double elowlim, eupplim;
+} fz_line;
+
+/* One spectral region of the LINES: section: IND_LINE/BLENDSID (0-based
+ * indices into the line table), BLENDSDIFF [mA], NUMWAVE, WAVE_INI and
+ * DELTA_LAMBDA [mA] (src/input_file.f90:290-366, src/pre_post_duties.f90:592-621). */
+typedef struct {
+  int32_t nblend;
+  int32_t line[FZ_MAXBLEND];
+  double wdif[FZ_MAXBLEND];
+  int32_t numwave, pad;
+  double wave_ini, dlambda;
+} fz_region;
+
+typedef struct fz_ctx fz_ctx;
+
+/* Library version (major*100+minor). */
+int fz_version(void);
+const char* fz_strerror(int code);
+
+/* Parse the text of lines_database.dat: 13- or 8-column rows terminated by
+ * END, ABO collision parameters interpolated where the row leaves them 0.
+ * Replaces NREAD_LINES_DATABASE (src/lines_database.f90:380-530).
+ * Returns the number of rows or a negative error. */
+int fz_lines_parse(const char* text, fz_line* out, int maxn);
+
+/* Create a context on CUDA device `device` for a fixed line set and height
+ * count: uploads the line table, the Zeeman patterns (ZEEMAN_COMP,
+ * src/magsplit.f90:38-187, hoisted out of the z loop) and the wavelength grid
+ * (WAVE_INIT).  gain may be NULL: the HSRA continuum normalisation GET_NORM
+ * (src/normalization.f90:696-754) is then computed on the GPU.
+ * Replaces the set-up done by START_STEP (src/pre_post_duties.f90:59-93). */
+int fz_create(fz_ctx** ctx, const fz_line* lines, int nlines, const fz_region* regions, int nregions,
+              int nz, const float* gain, int device);
+int fz_destroy(fz_ctx* ctx);
+
+/* Number of wavelengths NUMW of the context. */
+int fz_numw(const fz_ctx* ctx);
+/* Copy GAIN1D(4,NUMW) to host memory. */
+int fz_get_gain(fz_ctx* ctx, float* gain);
+
+/* Forward synthesis of ncol columns, host buffers: the batched equivalent of
+ * the worker side of FORWARD3D + FORWARD1D (src/forward.f90:106-291,
+ * :857-1029) without response functions.  model is read; model_out (may be
+ * NULL, may equal model) receives the updated rho, Pe, mu, log tau5 and, with
+ * hydrostatic != 0, Pg (RK4_INTEGRATION_LOG, src/hydrostatic_tools.f90:150-222).
+ * syn is RSYN1D(NFREQ,ncol), status is (ncol) or NULL. */
+int fz_forward(fz_ctx* ctx, int ncol, const float* model, int hydrostatic, double* syn, float* model_out,
+               int* status);
+
+/* Same, with device pointers, enqueued on `stream` (a cudaStream_t, NULL =
+ * default stream).  model_out is required (it may alias model).  Scratch
+ * memory is owned by the context and grows on demand. */
+int fz_forward_device(fz_ctx* ctx, int ncol, const float* d_model, int hydrostatic, double* d_syn,
+                      float* d_model_out, int* d_status, void* stream);
+
+/* Per-kernel timing: when enabled, every launch of the context is bracketed
+ * by CUDA events on its stream; fz_profile_read returns the accumulated
+ * milliseconds and launch counts of the kernels (names in order:
+ * "k_chem", "k_synth") and resets them.  Replaces the reference's
+ * SYSTEM_CLOCK "Forward 3D:" timer (src/forward.f90:99-100, :295-297). */
+int fz_profile_enable(fz_ctx* ctx, int on);
+int fz_profile_read(fz_ctx* ctx, double* ms, int* launches, int n);
+
+/* Peak FP32 FMA throughput of device `device` in TFLOP/s (2 FLOP per FMA),
+ * measured by a register-resident FMA-chain kernel; the denominator of the
+ * FP32-pipe roofline of the synthesis kernel. */
+int fz_measure_fp32_peak(int device, double* tflops);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* FZ_B200_H */

@@ -1,0 +1,762 @@
+#!/usr/bin/env python3
+"""Generate the physical data tables shared by the CUDA library and the oracle.
+
+TEST INFRASTRUCTURE / BUILD RECIPE.  This script reads the FIRTEZ-dz Fortran
+sources (default location ``/root/reference/src``) and writes
+
+  * ``firtez-dz_b200/csrc/fz_tables.h``   -- data tables in this project's own
+    layout (per-element atomic constants, partition-function pieces, ABO
+    collision tables, the HSRA reference atmosphere);
+  * ``tests/golden/partition_function.npz`` -- golden values of the partition
+    functions obtained by *literally* evaluating the reference's Fortran
+    assignments (with Fortran kind/rounding semantics) on a temperature grid.
+
+The data are the reference's physical tables (they must be identical for
+parity).  Sources:
+
+  atomic constants      src/atom_database.f90:55-105   (ATOM_INIT)
+  partition functions   src/atom_database.f90:121-1035 (PARTITION_FUNCTION)
+  ABO cross sections    src/damping.f90:24-821         (CS_SP ... AL_DF)
+  HSRA model            src/normalization.f90:135-393  (SET_HSRA_MODEL)
+
+Fortran semantics reproduced here: a real literal without a ``D`` exponent is
+default REAL (float32); an operation whose operands are both default REAL (or
+integer) is rounded to float32; mixed operations promote to float64.
+
+Partition-function representation (own design, evaluated uniformly on the GPU):
+for every element and ionisation stage a list of *value pieces* applied in
+order (a later piece whose condition holds replaces the earlier one), and a
+list of *derivative pieces* with the same override semantics.
+
+  value piece  : U = form(Horner(c, var))  if cond(T)
+                 form 0 = poly, 1 = base + exp(poly), 2 = max(clamp, poly)
+  deriv piece  : dU = mult * Horner(dc, var) * [(Uref - base)] / Uref^upow
+                 where Uref is value piece #ref of the same stage.
+"""
+import argparse
+import math
+import os
+import re
+import sys
+
+import numpy as np
+
+REF_DEFAULT = "/root/reference/src"
+
+# ----------------------------------------------------------------------------
+# Fortran-typed scalar
+# ----------------------------------------------------------------------------
+_ORD = {"i": 0, "s": 1, "d": 2}
+
+
+def _cast(v, k):
+    if k == "s":
+        return float(np.float32(v))
+    if k == "i":
+        return int(v)
+    return float(v)
+
+
+class F:
+    """A Fortran scalar with kind 'i' (integer), 's' (REAL*4) or 'd' (REAL*8)."""
+
+    __slots__ = ("v", "k")
+
+    def __init__(self, v, k):
+        self.v = _cast(v, k)
+        self.k = k
+
+    def _bin(self, o, op):
+        if not isinstance(o, F):
+            return NotImplemented
+        k = self.k if _ORD[self.k] >= _ORD[o.k] else o.k
+        a, b = _cast(self.v, k), _cast(o.v, k)
+        if k == "s":
+            a32, b32 = np.float32(a), np.float32(b)
+            with np.errstate(all="ignore"):
+                r = {"+": a32 + b32, "-": a32 - b32, "*": a32 * b32, "/": a32 / b32}[op]
+            return F(float(r), "s")
+        if k == "i":
+            if op == "/":
+                q = abs(a) // abs(b)
+                return F(q if (a >= 0) == (b >= 0) else -q, "i")
+            return F({"+": a + b, "-": a - b, "*": a * b}[op], "i")
+        return F({"+": a + b, "-": a - b, "*": a * b, "/": a / b}[op], "d")
+
+    def __add__(self, o): return self._bin(o, "+")
+    def __sub__(self, o): return self._bin(o, "-")
+    def __mul__(self, o): return self._bin(o, "*")
+    def __truediv__(self, o): return self._bin(o, "/")
+    def __neg__(self): return F(-self.v, self.k)
+    def __pos__(self): return self
+
+    def _cmp(self, o):
+        k = self.k if _ORD[self.k] >= _ORD[o.k] else o.k
+        return _cast(self.v, k), _cast(o.v, k)
+
+    def __gt__(self, o): a, b = self._cmp(o); return a > b
+    def __lt__(self, o): a, b = self._cmp(o); return a < b
+    def __ge__(self, o): a, b = self._cmp(o); return a >= b
+    def __le__(self, o): a, b = self._cmp(o); return a <= b
+    def __ne__(self, o): a, b = self._cmp(o); return a != b
+    def __eq__(self, o): a, b = self._cmp(o); return a == b
+    __hash__ = None
+
+
+def lit(s):
+    """Typed value of a Fortran numeric literal."""
+    s = s.upper()
+    if "D" in s:
+        return F(float(s.replace("D", "E")), "d")
+    if "." in s or "E" in s:
+        return F(float(s), "s")
+    return F(int(s), "i")
+
+
+def f_exp(a):
+    if a.k == "d":
+        return F(math.exp(a.v), "d")
+    return F(float(np.exp(np.float32(a.v))), "s")
+
+
+def f_max(a, b):
+    k = a.k if _ORD[a.k] >= _ORD[b.k] else b.k
+    return F(max(_cast(a.v, k), _cast(b.v, k)), k)
+
+
+# ----------------------------------------------------------------------------
+# Fortran source helpers
+# ----------------------------------------------------------------------------
+def read_logical_lines(path, start, end):
+    """Lines start..end (1-based, inclusive), comments stripped, '&' joined."""
+    with open(path) as fh:
+        raw = fh.readlines()[start - 1:end]
+    out, acc = [], ""
+    for ln in raw:
+        ln = ln.split("!")[0].rstrip()
+        if not ln.strip():
+            continue
+        if ln.rstrip().endswith("&"):
+            acc += ln.rstrip()[:-1] + " "
+            continue
+        acc += ln
+        out.append(acc.strip())
+        acc = ""
+    return out
+
+
+_NUM = re.compile(r"(?<![A-Za-z_0-9])(\d+\.\d*(?:[EeDd][+-]?\d+)?|\.\d+(?:[EeDd][+-]?\d+)?|\d+[EeDd][+-]?\d+|\d+)")
+
+
+def to_python(expr):
+    """Translate a Fortran expression into a Python expression over F values."""
+    e = expr.upper()
+    e = (e.replace(".GT.", ">").replace(".LT.", "<").replace(".GE.", ">=")
+         .replace(".LE.", "<=").replace(".NE.", "!=").replace(".EQ.", "=="))
+    e = re.sub(r"\bAMAX1\s*\(", "MAX(", e)
+    e = _NUM.sub(lambda m: 'L("%s")' % m.group(1), e)
+    return e
+
+
+def parse_array_literal(text):
+    """Numbers of a Fortran array constructor '(/ ... /)' with kinds."""
+    i0 = text.index("(/") + 2
+    body = text[i0:text.index("/)", i0)]
+    vals = []
+    for tok in body.split(","):
+        tok = tok.strip()
+        if tok:
+            vals.append(lit(tok))
+    return vals
+
+
+def grab_assignment(lines, name):
+    """The logical line assigning NAME(:)=(/ ... /)."""
+    for ln in lines:
+        if re.match(r"^%s\s*\(:\)\s*=" % re.escape(name), ln, re.I):
+            return ln
+    raise KeyError(name)
+
+
+# ----------------------------------------------------------------------------
+# Partition functions: parse CASE blocks into statements
+# ----------------------------------------------------------------------------
+def parse_partition_cases(path):
+    lines = read_logical_lines(path, 121, 1035)
+    cases = {}
+    cur = None
+    cond_stack = []
+    for ln in lines:
+        u = ln.upper()
+        m = re.match(r"^CASE\s*\((\d+)\)", u)
+        if m:
+            cur = int(m.group(1))
+            cases[cur] = []
+            cond_stack = []
+            continue
+        if cur is None:
+            continue
+        if u.startswith("END SELECT"):
+            cur = None
+            continue
+        m = re.match(r"^IF\s*\((.*)\)\s*THEN$", u)
+        if m:
+            cond_stack.append(m.group(1))
+            continue
+        if u in ("ENDIF", "END IF"):
+            cond_stack.pop()
+            continue
+        m = re.match(r"^IF\s*\((.*?)\)\s*([A-Z]+\s*=.*)$", u)
+        cond = list(cond_stack)
+        stmt = u
+        if m:
+            # single-line IF: the condition is the balanced parenthesis group
+            depth, i = 0, u.index("(")
+            for j in range(i, len(u)):
+                depth += u[j] == "("
+                depth -= u[j] == ")"
+                if depth == 0:
+                    break
+            cond = cond + [u[i + 1:j]]
+            stmt = u[j + 1:].strip()
+        lhs, rhs = stmt.split("=", 1)
+        cases[cur].append((cond, lhs.strip(), rhs.strip()))
+    return cases
+
+
+STAGES = ["UI", "UII", "UIII"]
+DSTAGES = ["DUI", "DUII", "DUIII"]
+
+
+def literal_partition(stmts, T):
+    """Literal evaluation of one CASE block at temperature T (float64)."""
+    Tf = F(T, "d")
+    env = {
+        "L": lit, "EXP": f_exp, "MAX": f_max,
+        "T": Tf, "X": F(math.log(5040.0 / T), "d"), "Y": F(1.0e-3 * T, "d"),
+        "DX": F(-1.0 / T, "d"),
+    }
+    for n in STAGES + DSTAGES:
+        env[n] = F(0.0, "d")
+    for cond, lhs, rhs in stmts:
+        ok = all(eval(to_python(c), {}, env) for c in cond)
+        if ok:
+            env[lhs] = F(eval(to_python(rhs), {}, env).v, "d")  # targets are REAL(8)
+    return [env[n].v for n in STAGES + DSTAGES]
+
+
+# ---------------- symbolic extraction into pieces ----------------------------
+class P:
+    """Polynomial in one variable (T, Y or X) with float64 coefficients."""
+
+    def __init__(self, var, c):
+        self.var, self.c = var, list(c)
+
+    @staticmethod
+    def lift(o, var):
+        if isinstance(o, P):
+            return o
+        return P(var, [float(o.v)])
+
+    def _var(self, o):
+        if isinstance(o, P) and o.var != self.var and len(o.c) > 1 and len(self.c) > 1:
+            raise ValueError("mixed variables")
+        return self.var if len(self.c) > 1 or not isinstance(o, P) else o.var
+
+    def __add__(self, o):
+        if isinstance(o, (Term, E, M)):
+            return NotImplemented
+        v = self._var(o); o = P.lift(o, v)
+        n = max(len(self.c), len(o.c))
+        a = self.c + [0.0] * (n - len(self.c)); b = o.c + [0.0] * (n - len(o.c))
+        return P(v, [x + y for x, y in zip(a, b)])
+
+    __radd__ = __add__
+
+    def __neg__(self):
+        return P(self.var, [-x for x in self.c])
+
+    def __sub__(self, o):
+        if isinstance(o, (Term, E, M)):
+            return NotImplemented
+        return self + (-(o) if isinstance(o, P) else F(-o.v, o.k))
+
+    def __rsub__(self, o):
+        return (-self) + o
+
+    def __mul__(self, o):
+        if isinstance(o, (Term, DXs, Us)):
+            return NotImplemented
+        if isinstance(o, F):
+            return P(self.var, [x * float(o.v) for x in self.c])
+        v = self._var(o)
+        r = [0.0] * (len(self.c) + len(o.c) - 1)
+        for i, x in enumerate(self.c):
+            for j, y in enumerate(o.c):
+                r[i + j] += x * y
+        return P(v, r)
+
+    __rmul__ = __mul__
+
+    def __truediv__(self, o):
+        if isinstance(o, F):
+            return P(self.var, [x / float(o.v) for x in self.c])
+        return Term.of(self) / o
+
+
+class E:
+    def __init__(self, base, p):
+        self.base, self.p = base, p
+
+    def __radd__(self, o):
+        return E(self.base + float(o.v), self.p)
+
+    __add__ = __radd__
+
+
+class M:
+    def __init__(self, clamp, p):
+        self.clamp, self.p = clamp, p
+
+
+class DXs:
+    pass
+
+
+class Us:
+    """Current value of a stage's partition function (reference by piece)."""
+
+    def __init__(self, stage, ref, base=None):
+        self.stage, self.ref, self.base = stage, ref, base
+
+    def __sub__(self, o):
+        return Us(self.stage, self.ref, float(o.v))
+
+    def __rtruediv__(self, o):
+        return Term.of(o) / self
+
+
+class Term:
+    """mult * poly * DX^dx * (U-base)^ub / U^up"""
+
+    def __init__(self, poly, mult=1.0, dx=0, ub=None, up=0, ref=None):
+        self.poly, self.mult, self.dx, self.ub, self.up, self.ref = poly, mult, dx, ub, up, ref
+
+    @staticmethod
+    def of(o):
+        if isinstance(o, Term):
+            return o
+        if isinstance(o, P):
+            return Term(o)
+        if isinstance(o, F):
+            return Term(P("T", [float(o.v)]))
+        if isinstance(o, DXs):
+            return Term(P("T", [1.0]), dx=1)
+        raise TypeError(o)
+
+    def copy(self):
+        return Term(self.poly, self.mult, self.dx, self.ub, self.up, self.ref)
+
+    def __mul__(self, o):
+        t = self.copy()
+        if isinstance(o, F):
+            t.mult *= float(o.v)
+        elif isinstance(o, P):
+            t.poly = t.poly * o
+        elif isinstance(o, DXs):
+            t.dx += 1
+        elif isinstance(o, Us):
+            assert o.base is not None and t.ub is None
+            t.ub, t.ref = o.base, o.ref
+        elif isinstance(o, Term):
+            assert o.dx == 0 and o.ub is None and o.up == 0
+            t.mult *= o.mult
+            t.poly = t.poly * o.poly
+        else:
+            raise TypeError(o)
+        return t
+
+    __rmul__ = __mul__
+
+    def __truediv__(self, o):
+        t = self.copy()
+        if isinstance(o, Us):
+            assert o.base is None
+            t.up += 1
+            assert t.ref in (None, o.ref)
+            t.ref = o.ref
+        elif isinstance(o, F):
+            t.mult /= float(o.v)
+        else:
+            raise TypeError(o)
+        return t
+
+    def __neg__(self):
+        t = self.copy(); t.mult = -t.mult; return t
+
+
+def _p_mul_dx(self, o):
+    if isinstance(o, DXs):
+        return Term(self, dx=1)
+    if isinstance(o, Term):
+        return o * self
+    if isinstance(o, Us):
+        raise TypeError
+    return P.__mul__(self, o)
+
+
+def _dx_mul(self, o):
+    return Term.of(self) * o
+
+
+DXs.__mul__ = _dx_mul
+DXs.__rmul__ = _dx_mul
+DXs.__neg__ = lambda self: Term(P("T", [-1.0]), dx=1)
+
+
+def sym_eval(rhs, env):
+    class _P(P):
+        pass
+    e = to_python(rhs)
+    return eval(e, {}, env)
+
+
+def _sym_lit(s):
+    return lit(s)
+
+
+def _sym_exp(a):
+    return E(0.0, a)
+
+
+def _sym_max(a, b):
+    if isinstance(a, F) and isinstance(b, P):
+        return M(float(a.v), b)
+    raise ValueError("unexpected MAX form")
+
+
+def extract_pieces(stmts):
+    """Value/derivative pieces per stage from one CASE block."""
+    vpieces = {s: [] for s in STAGES}
+    dpieces = {s: [] for s in STAGES}
+    cur_ref = {s: None for s in STAGES}
+    cur_d = {s: None for s in STAGES}       # current derivative Term (symbolic)
+
+    def cond_of(cond):
+        # supported: [] ; ['T .GT. x'] ; ['T .LT. x'] ; ['T .LE. x'] ; ['UI .NE. c']
+        if not cond:
+            return ("always", 0.0)
+        assert len(cond) == 1, cond
+        c = cond[0].replace(" ", "")
+        m = re.match(r"^T\.(GT|LT|LE|GE)\.(.+)$", c)
+        if m:
+            return ({"GT": "gt", "LT": "lt", "LE": "le", "GE": "ge"}[m.group(1)], float(lit(m.group(2)).v))
+        m = re.match(r"^(UI|UII|UIII)\.NE\.(.+)$", c)
+        if m:
+            return ("neclamp", float(lit(m.group(2)).v))
+        raise ValueError(cond)
+
+    for cond, lhs, rhs in stmts:
+        cnd = cond_of(cond)
+        env = {"L": _sym_lit, "EXP": _sym_exp, "MAX": _sym_max,
+               "T": P("T", [0.0, 1.0]), "Y": P("Y", [0.0, 1.0]), "X": P("X", [0.0, 1.0]),
+               "DX": DXs()}
+        for s in STAGES:
+            env[s] = Us(s, cur_ref[s])
+        for s, ds in zip(STAGES, DSTAGES):
+            env[ds] = cur_d[s]
+        if lhs in STAGES:
+            if re.fullmatch(r"U(I|II|III)", rhs.strip()):
+                src = rhs.strip()
+                # alias: copy the source stage's pieces (value and derivative)
+                vpieces[lhs] = [dict(p) for p in vpieces[src]]
+                dpieces[lhs] = [dict(p) for p in dpieces[src]]
+                cur_ref[lhs] = cur_ref[src]
+                continue
+            val = sym_eval(rhs, env)
+            if isinstance(val, F):
+                piece = dict(form=0, var="T", c=[float(val.v)], clamp=0.0)
+            elif isinstance(val, P):
+                piece = dict(form=0, var=val.var, c=val.c, clamp=0.0)
+            elif isinstance(val, E):
+                piece = dict(form=1, var=val.p.var, c=val.p.c, base=val.base, clamp=0.0)
+            elif isinstance(val, M):
+                piece = dict(form=2, var=val.p.var, c=val.p.c, clamp=val.clamp)
+            else:
+                raise ValueError((lhs, rhs, val))
+            piece.setdefault("base", 0.0)
+            piece["cond"], piece["th"] = cnd
+            vpieces[lhs].append(piece)
+            cur_ref[lhs] = len(vpieces[lhs]) - 1
+        elif lhs in DSTAGES:
+            s = STAGES[DSTAGES.index(lhs)]
+            if re.fullmatch(r"DU(I|II|III)", rhs.strip()):
+                src = STAGES[DSTAGES.index(rhs.strip())]
+                dpieces[s] = [dict(p) for p in dpieces[src]]
+                cur_d[s] = cur_d[src]
+                continue
+            val = sym_eval(rhs, env)
+            t = Term.of(val) if not isinstance(val, Term) else val
+            cur_d[s] = t
+            if t.ref is None:
+                t.ref = cur_ref[s]
+            ref = t.ref if t.ref is not None else cur_ref[s]
+            # the value in force when this statement runs: skip back over
+            # value pieces whose condition excludes this statement's condition
+            while ref is not None and ref > 0 and _exclusive(vpieces[s][ref], cnd):
+                ref -= 1
+            piece = dict(var=t.poly.var, c=t.poly.c, mult=t.mult, dx=t.dx,
+                         ub=(t.ub is not None), base=(t.ub or 0.0), up=t.up, ref=ref)
+            piece["cond"], piece["th"] = cnd
+            # a statement DU = DU*(...)/U refines the previous piece in place
+            if rhs.replace(" ", "").startswith(lhs) or ("(" + lhs) in rhs.replace(" ", "") and lhs + "/" in rhs.replace(" ", ""):
+                if dpieces[s] and dpieces[s][-1]["cond"] == piece["cond"] and dpieces[s][-1]["th"] == piece["th"]:
+                    dpieces[s][-1] = piece
+                    continue
+            dpieces[s].append(piece)
+        else:
+            raise ValueError(lhs)
+    return vpieces, dpieces
+
+
+def _exclusive(vp, cnd):
+    a, ta = vp["cond"], vp["th"]
+    b, tb = cnd
+    if ta != tb:
+        return False
+    return {("gt", "le"), ("le", "gt"), ("lt", "ge"), ("ge", "lt")}.__contains__((a, b))
+
+
+COND_CODE = {"always": 0, "gt": 1, "lt": 2, "le": 3, "ge": 4, "neclamp": 5}
+VAR_CODE = {"T": 0, "Y": 1, "X": 2}
+
+
+def eval_pieces(vp, dp, T):
+    """Python model of the table evaluator (mirrors the C/CUDA code)."""
+    vals = {"T": T, "Y": 1.0e-3 * T, "X": math.log(5040.0 / T)}
+
+    def horner(c, x):
+        r = c[-1]
+        for a in reversed(c[:-1]):
+            r = a + x * r
+        return r
+
+    def vpiece(p):
+        h = horner(p["c"], vals[p["var"]])
+        if p["form"] == 1:
+            return p["base"] + math.exp(h)
+        if p["form"] == 2:
+            return max(p["clamp"], h)
+        return h
+
+    def holds(cond, th, U=None):
+        return {"always": True, "gt": T > th, "lt": T < th, "le": T <= th, "ge": T >= th,
+                "neclamp": (U is not None and U != th)}[cond]
+
+    U, dU = [], []
+    for s in STAGES:
+        u, active = 0.0, -1
+        for i, p in enumerate(vp[s]):
+            if holds(p["cond"], p["th"]):
+                active = i
+        u = vpiece(vp[s][active]) if active >= 0 else 0.0
+        d = 0.0
+        for p in dp[s]:
+            uref = vpiece(vp[s][p["ref"]]) if p["ref"] is not None and vp[s] else u
+            if holds(p["cond"], p["th"], uref):
+                h = horner(p["c"], vals[p["var"]]) * p["mult"]
+                if p["dx"]:
+                    h *= (-1.0 / T) ** p["dx"]
+                if p["ub"]:
+                    h *= (uref - p["base"])
+                d = h / uref ** p["up"]
+        U.append(u); dU.append(d)
+    return U + dU
+
+
+# ----------------------------------------------------------------------------
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--ref", default=REF_DEFAULT)
+    ap.add_argument("--out-header", default=None)
+    ap.add_argument("--out-golden", default=None)
+    a = ap.parse_args()
+    repo = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    out_h = a.out_header or os.path.join(repo, "firtez-dz_b200", "csrc", "fz_tables.h")
+    out_g = a.out_golden or os.path.join(repo, "tests", "golden", "partition_function.npz")
+    src = a.ref
+
+    # --- atomic constants ----------------------------------------------------
+    ad = os.path.join(src, "atom_database.f90")
+    init = read_logical_lines(ad, 47, 119)
+    XI = parse_array_literal(grab_assignment(init, "XI"))
+    XII = parse_array_literal(grab_assignment(init, "XII"))
+    ABUND = parse_array_literal(grab_assignment(init, "ABUND"))
+    MATOM = parse_array_literal(grab_assignment(init, "MATOM"))
+    for arr in (XI, XII, ABUND, MATOM):
+        assert len(arr) == 92
+
+    # --- partition functions -------------------------------------------------
+    cases = parse_partition_cases(ad)
+    assert sorted(cases) == list(range(1, 93)), sorted(cases)
+    vps, dps = {}, {}
+    for z in range(1, 93):
+        vps[z], dps[z] = extract_pieces(cases[z])
+
+    # golden: literal evaluation on a T grid (dense + threshold neighbourhoods)
+    grid = list(np.geomspace(1500.0, 60000.0, 700))
+    ths = set()
+    for z in range(1, 93):
+        for s in STAGES:
+            for p in vps[z][s] + dps[z][s]:
+                if p["cond"] in ("gt", "lt", "le", "ge"):
+                    ths.add(p["th"])
+    for th in sorted(ths):
+        grid += [th * (1 - 1e-9), th, th * (1 + 1e-9)]
+    grid = np.array(sorted(set(float(t) for t in grid)))
+    gold = np.zeros((92, len(grid), 6))
+    model = np.zeros_like(gold)
+    for z in range(1, 93):
+        for it, T in enumerate(grid):
+            gold[z - 1, it] = literal_partition(cases[z], float(T))
+            model[z - 1, it] = eval_pieces(vps[z], dps[z], float(T))
+    rel = np.abs(model - gold) / np.maximum(np.abs(gold), 1e-300)
+    worst_u = rel[:, :, :3].max()
+    worst_d = np.where(np.abs(gold[:, :, 3:]) > 0, rel[:, :, 3:], np.abs(model[:, :, 3:])).max()
+    print("piece model vs literal: max rel U = %.3e, max rel dU = %.3e" % (worst_u, worst_d))
+    if worst_u > 1e-14 or worst_d > 1e-9:
+        bad = np.argwhere(rel > 1e-9)
+        for zb, tb, kb in bad[:20]:
+            print("  mismatch Z=%d T=%.6g k=%d gold=%r model=%r" % (zb + 1, grid[tb], kb, gold[zb, tb, kb], model[zb, tb, kb]))
+        sys.exit("partition-function extraction does not reproduce the reference")
+
+    # --- ABO tables ----------------------------------------------------------
+    dm = os.path.join(src, "damping.f90")
+    dlines = read_logical_lines(dm, 20, 822)
+    abo = {}
+    for nm, shp in (("CS_SP", (46, 43)), ("AL_SP", (46, 43)), ("CS_PD", (43, 33)),
+                    ("AL_PD", (43, 33)), ("CS_DF", (33, 28)), ("AL_DF", (33, 28))):
+        ln = next(l for l in dlines if re.search(r"::\s*%s\s*\(" % nm, l))
+        vals = parse_array_literal(ln[ln.index("SOURCE"):])
+        assert len(vals) == shp[0] * shp[1], (nm, len(vals))
+        assert "order=(/2,1/)" in ln.replace(" ", "").lower()
+        # ORDER=(2,1): the source fills the second index fastest -> row major
+        abo[nm] = np.array([float(v.v) for v in vals]).reshape(shp)
+
+    # --- HSRA ----------------------------------------------------------------
+    nm = os.path.join(src, "normalization.f90")
+    hl = read_logical_lines(nm, 135, 393)
+    hsra = {}
+    for key in ("HSRA_TEM", "HSRA_PG", "HSRA_RHO", "HSRA_Z"):
+        vals = parse_array_literal(grab_assignment(hl, key))
+        assert len(vals) == 387, (key, len(vals))
+        hsra[key] = [float(np.float32(v.v)) for v in vals]   # REAL(SP) arrays
+
+    write_header(out_h, XI, XII, ABUND, MATOM, vps, dps, abo, hsra)
+    os.makedirs(os.path.dirname(out_g), exist_ok=True)
+    # the committed golden file keeps a coarser grid (every threshold kept)
+    keep = np.zeros(len(grid), dtype=bool)
+    keep[::8] = True
+    for th in ths:
+        keep |= np.abs(grid / th - 1.0) < 2e-9
+    np.savez_compressed(out_g, T=grid[keep], U=gold[:, keep])
+    print("wrote", out_h, "and", out_g)
+
+
+def _fmt(x):
+    return repr(float(x)) if math.isfinite(x) else "0.0"
+
+
+def write_header(path, XI, XII, ABUND, MATOM, vps, dps, abo, hsra):
+    MAXV = max(len(vps[z][s]) for z in vps for s in STAGES)
+    MAXD = max(len(dps[z][s]) for z in dps for s in STAGES)
+    MAXC = max(len(p["c"]) for z in vps for s in STAGES for p in vps[z][s] + dps[z][s])
+    L = []
+    w = L.append
+    w("// Generated by oracle/gen_tables.py from the FIRTEZ-dz sources. Do not edit.")
+    w("// Data: src/atom_database.f90 (ATOM_INIT, PARTITION_FUNCTION),")
+    w("//       src/damping.f90 (ABO tables), src/normalization.f90 (HSRA).")
+    w("// Values are float64 images of the Fortran constants (REAL*4 literals")
+    w("// are rounded to float32 first, as the Fortran compiler does).")
+    w("#pragma once")
+    w("#define FZ_NELEM 92")
+    w("#define FZ_PF_MAXV %d" % MAXV)
+    w("#define FZ_PF_MAXD %d" % MAXD)
+    w("#define FZ_PF_MAXC %d" % MAXC)
+    w("#ifndef FZ_TABLE_QUAL")
+    w("#define FZ_TABLE_QUAL static const")
+    w("#endif")
+
+    def arr(name, vals):
+        w("FZ_TABLE_QUAL double %s[%d] = {" % (name, len(vals)))
+        for i in range(0, len(vals), 6):
+            w("  " + ", ".join(_fmt(v) for v in vals[i:i + 6]) + ",")
+        w("};")
+
+    arr("fz_tab_xi", [v.v for v in XI])
+    arr("fz_tab_xii", [v.v for v in XII])
+    arr("fz_tab_abund", [v.v for v in ABUND])
+    arr("fz_tab_matom", [v.v for v in MATOM])
+    # partition-function value pieces: [elem][stage][piece]
+    w("typedef struct { int cond; int form; int var; int nc; double th; double base; double clamp; double c[FZ_PF_MAXC]; } fz_pf_vpiece;")
+    w("typedef struct { int cond; int var; int nc; int dx; int ub; int up; int ref; int pad; double th; double base; double mult; double c[FZ_PF_MAXC]; } fz_pf_dpiece;")
+    w("FZ_TABLE_QUAL int fz_tab_pf_nv[FZ_NELEM][3] = {")
+    for z in range(1, 93):
+        w("  {%s}," % ", ".join(str(len(vps[z][s])) for s in STAGES))
+    w("};")
+    w("FZ_TABLE_QUAL int fz_tab_pf_nd[FZ_NELEM][3] = {")
+    for z in range(1, 93):
+        w("  {%s}," % ", ".join(str(len(dps[z][s])) for s in STAGES))
+    w("};")
+    w("FZ_TABLE_QUAL fz_pf_vpiece fz_tab_pf_v[FZ_NELEM][3][FZ_PF_MAXV] = {")
+    for z in range(1, 93):
+        w("  { // Z=%d" % z)
+        for s in STAGES:
+            items = []
+            for p in vps[z][s]:
+                c = p["c"] + [0.0] * (MAXC - len(p["c"]))
+                items.append("{%d,%d,%d,%d,%s,%s,%s,{%s}}" % (
+                    COND_CODE[p["cond"]], p["form"], VAR_CODE[p["var"]], len(p["c"]),
+                    _fmt(p["th"]), _fmt(p["base"]), _fmt(p["clamp"]), ",".join(_fmt(x) for x in c)))
+            w("    {%s}," % ", ".join(items) if items else "    {{0,0,0,1,0.0,0.0,0.0,{0.0}}},")
+        w("  },")
+    w("};")
+    w("FZ_TABLE_QUAL fz_pf_dpiece fz_tab_pf_d[FZ_NELEM][3][FZ_PF_MAXD] = {")
+    for z in range(1, 93):
+        w("  { // Z=%d" % z)
+        for s in STAGES:
+            items = []
+            for p in dps[z][s]:
+                c = p["c"] + [0.0] * (MAXC - len(p["c"]))
+                items.append("{%d,%d,%d,%d,%d,%d,%d,0,%s,%s,%s,{%s}}" % (
+                    COND_CODE[p["cond"]], VAR_CODE[p["var"]], len(p["c"]), p["dx"], int(p["ub"]),
+                    p["up"], p["ref"] if p["ref"] is not None else -1,
+                    _fmt(p["th"]), _fmt(p["base"]), _fmt(p["mult"]), ",".join(_fmt(x) for x in c)))
+            w("    {%s}," % ", ".join(items) if items else "    {{0,0,1,0,0,0,-1,0,0.0,0.0,0.0,{0.0}}},")
+        w("  },")
+    w("};")
+    for nm, a in abo.items():
+        n0, n1 = a.shape
+        w("FZ_TABLE_QUAL double fz_tab_abo_%s[%d][%d] = {" % (nm.lower(), n0, n1))
+        for i in range(n0):
+            w("  {" + ", ".join(_fmt(v) for v in a[i]) + "},")
+        w("};")
+    w("#define FZ_HSRA_LEN 387")
+    for key, vals in hsra.items():
+        w("FZ_TABLE_QUAL float fz_tab_%s[FZ_HSRA_LEN] = {" % key.lower())
+        for i in range(0, len(vals), 6):
+            w("  " + ", ".join(repr(float(v)) + "f" for v in vals[i:i + 6]) + ",")
+        w("};")
+    with open(path, "w") as fh:
+        fh.write("\n".join(L) + "\n")
+    # plain number lists for host-side initialisers
+    d = os.path.dirname(path)
+    for nm, vals in (("fz_abund.inc", ABUND), ("fz_matom.inc", MATOM)):
+        with open(os.path.join(d, nm), "w") as fh:
+            fh.write("// Generated by oracle/gen_tables.py (src/atom_database.f90 ATOM_INIT).\n")
+            for i in range(0, len(vals), 6):
+                fh.write("  " + ", ".join(_fmt(v.v) for v in vals[i:i + 6]) + ",\n")
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,35 @@
+#!/usr/bin/env python3
+"""Copy the reference's data fixtures into tests/golden/ and extract the
+alternative abundance set they were generated with.
+
+TEST INFRASTRUCTURE.  Reads the reference tree (default /root/reference):
+
+  default/test_atmos.bin, default/rf_test_atmos.bin  -- v3 model files (1x1x256)
+  default/lines_database.dat                         -- line database
+  src/atom_database.f90:89-97                         -- the commented-out
+      "Abundances Vigeesh" set; the fixtures' rho, Pe, mu were computed with it.
+"""
+import os
+import re
+import shutil
+import sys
+
+import numpy as np
+
+ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+here = os.path.dirname(os.path.abspath(__file__))
+for f in ("test_atmos.bin", "rf_test_atmos.bin", "lines_database.dat"):
+    shutil.copyfile(os.path.join(ref, "default", f), os.path.join(here, f))
+src = open(os.path.join(ref, "src", "atom_database.f90")).read().splitlines()
+i0 = next(i for i, l in enumerate(src) if "Abundances Vigeesh" in l)
+txt = ""
+for l in src[i0 + 1:]:
+    l = l.lstrip()
+    if not l.startswith("!"):
+        break
+    txt += l.lstrip("!").strip().rstrip("&")
+body = txt[txt.index("(/") + 2:txt.index("/)")]
+ab = np.array([float(np.float32(float(x))) for x in body.replace("&", "").split(",") if x.strip()])
+assert len(ab) == 92, len(ab)
+np.save(os.path.join(here, "abund_fixture.npy"), ab)
+print("fixtures written to", here)

@@ -1,0 +1,130 @@
+"""ctypes wrapper of the FP64 CPU oracle (oracle/liborc.so).
+
+TEST INFRASTRUCTURE: imported only by tests/, __graft_entry__.smoke() and the
+cpu_baseline leg of bench.py, as the checker.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+LIB_PATH = os.path.join(ROOT, "oracle", "liborc.so")
+
+MAXBLEND = 8
+
+LINE_DTYPE = np.dtype([
+    ("num", "<i4"), ("zn", "<i4"), ("ion", "<i4"), ("flag", "<i4"), ("otr", "<i4", 2),
+    ("abo_ierr", "<i4"), ("pad", "<i4"),
+    ("l0", "<f8"), ("loggf", "<f8"), ("eplow", "<f8"), ("alpha", "<f8"), ("sigma", "<f8"),
+    ("sl", "<f8"), ("ll", "<f8"), ("jl", "<f8"), ("su", "<f8"), ("lu", "<f8"), ("ju", "<f8"),
+    ("elowlim", "<f8"), ("eupplim", "<f8"),
+], align=True)
+
+REGION_DTYPE = np.dtype([
+    ("nblend", "<i4"), ("line", "<i4", MAXBLEND), ("wdif", "<f8", MAXBLEND),
+    ("numwave", "<i4"), ("pad", "<i4"), ("wave_ini", "<f8"), ("dlambda", "<f8"),
+], align=True)
+
+_lib = None
+
+
+def build():
+    import subprocess
+    subprocess.check_call(["make", "-s", "-C", os.path.join(ROOT, "oracle")])
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            build()
+        L = ctypes.CDLL(LIB_PATH)
+        P = ctypes.c_void_p
+        L.orc_partition.argtypes = [ctypes.c_int, ctypes.c_double, P]
+        L.orc_get_rho.argtypes = [ctypes.c_double, ctypes.c_double, P, P]
+        L.orc_opac_continuum.argtypes = [ctypes.c_float, ctypes.c_double, ctypes.c_double, ctypes.c_double]
+        L.orc_opac_continuum.restype = ctypes.c_double
+        L.orc_parse_lines.argtypes = [ctypes.c_char_p, P, ctypes.c_int]
+        L.orc_zeeman.argtypes = [P, P, P, P, ctypes.c_int]
+        L.orc_voigt.argtypes = [ctypes.c_int, ctypes.c_double, P, P, P]
+        L.orc_gain.argtypes = [P, ctypes.c_int, P, ctypes.c_int, P]
+        L.orc_forward.argtypes = [P, ctypes.c_int, P, ctypes.c_int, P, ctypes.c_int, ctypes.c_int, P,
+                                  ctypes.c_int, P, P, ctypes.c_int]
+        L.orc_set_abundances.argtypes = [P]
+        _lib = L
+    return _lib
+
+
+def _p(a):
+    return a.ctypes.data_as(ctypes.c_void_p)
+
+
+def set_abundances(ab=None):
+    if ab is None:
+        lib().orc_set_abundances(None)
+    else:
+        ab = np.ascontiguousarray(ab, dtype=np.float64)
+        lib().orc_set_abundances(_p(ab))
+
+
+def partition(zn, T):
+    out = np.zeros(6)
+    lib().orc_partition(int(zn), float(T), _p(out))
+    return out
+
+
+def get_rho(T, pg, nelec=0.0):
+    ne = np.array([nelec], dtype=np.float64)
+    out = np.zeros(5)
+    st = lib().orc_get_rho(float(T), float(pg), _p(ne), _p(out))
+    return dict(nhyd=out[0], pelec=out[1], dens=out[2], molecw=out[3], iters=int(out[4]), nelec=ne[0], status=st)
+
+
+def parse_lines(text):
+    out = np.zeros(512, dtype=LINE_DTYPE)
+    n = lib().orc_parse_lines(text.encode(), _p(out), len(out))
+    if n < 0:
+        raise ValueError("line database parse failed (%d)" % n)
+    return out[:n].copy()
+
+
+def zeeman(line):
+    ln = np.ascontiguousarray(np.array(line, dtype=LINE_DTYPE).reshape(1))
+    sh, st, ty = np.zeros(64), np.zeros(64), np.zeros(64, dtype=np.int32)
+    n = lib().orc_zeeman(_p(ln), _p(sh), _p(st), _p(ty), 64)
+    return sh[:n], st[:n], ty[:n]
+
+
+def voigt(a, v):
+    v = np.ascontiguousarray(v, dtype=np.float64)
+    h, f = np.zeros_like(v), np.zeros_like(v)
+    lib().orc_voigt(len(v), float(a), _p(v), _p(h), _p(f))
+    return h, f
+
+
+def gain(lines, regions):
+    lines = np.ascontiguousarray(lines, dtype=LINE_DTYPE)
+    regions = np.ascontiguousarray(regions, dtype=REGION_DTYPE)
+    numw = int(regions["numwave"].sum())
+    g = np.zeros((numw, 4), dtype=np.float32)
+    st = lib().orc_gain(_p(lines), len(lines), _p(regions), len(regions), _p(g))
+    return g, st
+
+
+def forward(lines, regions, gain_, model, hydrostatic=False, nthreads=0):
+    """model: (ncol, 13, nz) float32 (C order == Fortran MODEL(NZ,13,ncol)).
+
+    Returns (stokes (ncol, 4, numw) float64, model_out, status)."""
+    lines = np.ascontiguousarray(lines, dtype=LINE_DTYPE)
+    regions = np.ascontiguousarray(regions, dtype=REGION_DTYPE)
+    g = np.ascontiguousarray(gain_, dtype=np.float32)
+    m = np.array(model, dtype=np.float32, order="C", copy=True)
+    ncol, npar, nz = m.shape
+    assert npar == 13
+    numw = int(regions["numwave"].sum())
+    stokes = np.zeros((ncol, 4, numw))
+    status = np.zeros(ncol, dtype=np.int32)
+    lib().orc_forward(_p(lines), len(lines), _p(regions), len(regions), _p(g), nz, ncol, _p(m),
+                      int(bool(hydrostatic)), _p(stokes), _p(status), int(nthreads))
+    return stokes, m, status

@@ -1,0 +1,85 @@
+"""GPU synthesis parity against the FP64 CPU oracle, through the C-ABI.
+
+Tolerances (FP32 kernels vs FP64 restatement): Stokes I/Ic within 1e-5
+relative, Q/U/V within 1e-6 Ic absolute.  Chemistry and hydrostatic
+integration run in FP64 on the GPU; the updated model (rho, Pe, mu, Pg) must
+agree to float32 rounding (plus the GET_RHO convergence tolerance).
+"""
+import numpy as np
+import pytest
+
+import fixtures
+
+pytestmark = pytest.mark.gpu
+
+TOL_I = 1e-5
+TOL_QUV = 1e-6
+
+
+def stokes_errors(g, o):
+    """max relative error of I, max absolute error of Q/U/V (per column Ic units)."""
+    ei = np.max(np.abs(g[:, 0] - o[:, 0]) / np.abs(o[:, 0]))
+    eq = np.max(np.abs(g[:, 1:] - o[:, 1:]))
+    return ei, eq
+
+
+@pytest.fixture(scope="module")
+def workload(fz, orc):
+    lines = fz.lines_parse(fz.atmos.line_database_text())
+    reg = fz.regions_from_lines_section(fz.atmos.lines_section(2), lines)
+    return lines, reg
+
+
+def test_gain_matches_oracle(fz, orc, workload):
+    lines, reg = workload
+    ctx = fz.Synthesis(lines, reg, nz=96)
+    g_gpu = ctx.gain
+    g_orc, st = orc.gain(lines, reg)
+    assert st == 0
+    assert np.max(np.abs(g_gpu / g_orc - 1)) < 2e-7
+    assert np.all(g_gpu[:, 3] == -g_gpu[:, 0])
+
+
+@pytest.mark.parametrize("hydrostatic", [False, True])
+def test_synthesis_matches_oracle(fz, orc, workload, hydrostatic):
+    lines, reg = workload
+    nz, ncol = 96, 64
+    m = fz.atmos.make_columns(ncol, nz, seed=11)
+    g, _ = orc.gain(lines, reg)
+    ctx = fz.Synthesis(lines, reg, nz=nz, gain=g)
+    syn, mo, st = ctx.forward(m, hydrostatic=hydrostatic)
+    ref, mref, sref = orc.forward(lines, reg, g, m, hydrostatic=hydrostatic)
+    assert np.all(st == 0) and np.all(sref == 0)
+    ei, eq = stokes_errors(syn, ref)
+    print("max rel err I %.3e, max abs err QUV %.3e" % (ei, eq))
+    assert ei < TOL_I
+    assert eq < TOL_QUV
+    # updated model: rho, mu (and Pg in hydrostatic mode) to float rounding
+    for p in (2, 4) + ((1,) if hydrostatic else ()):
+        assert np.max(np.abs(mo[:, p] / mref[:, p] - 1)) < 2e-6, p
+    assert np.max(np.abs(mo[:, 11] - mref[:, 11])) < 1e-5     # log tau5
+
+
+def test_zero_field_gives_zero_polarisation(fz, orc, workload):
+    lines, reg = workload
+    m = fz.atmos.make_columns(8, 64, seed=5)
+    m[:, 5:8] = 0.0
+    ctx = fz.Synthesis(lines, reg, nz=64)
+    syn, _, st = ctx.forward(m)
+    assert np.all(st == 0)
+    assert np.all(syn[:, 1:] == 0.0)
+
+
+def test_reference_fixture_with_blend(fz, orc):
+    """test_syn1/test_rf set-up: lines 4,5 blended, 500 points from -700 mA."""
+    lines = fz.lines_parse(fixtures.fixture_lines_text())
+    reg = fz.regions_from_lines_section("4,5 500 -700.0 5.0", lines)
+    m = np.concatenate([fixtures.fixture_model("test_atmos.bin"), fixtures.fixture_model("rf_test_atmos.bin")])
+    g, _ = orc.gain(lines, reg)
+    ctx = fz.Synthesis(lines, reg, nz=m.shape[2], gain=g)
+    syn, mo, st = ctx.forward(m)
+    ref, mref, sref = orc.forward(lines, reg, g, m)
+    ei, eq = stokes_errors(syn, ref)
+    print("fixture: max rel err I %.3e, max abs err QUV %.3e" % (ei, eq))
+    assert np.all(syn[0, 1:] == 0.0)          # B = 0 column
+    assert ei < TOL_I and eq < TOL_QUV

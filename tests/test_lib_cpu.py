@@ -1,0 +1,65 @@
+"""The C-ABI library on the CPU side: it loads without a GPU, exports every
+symbol of include/fz_b200.h, and its line-database reader (host code) equals
+the oracle's restatement of NREAD_LINES_DATABASE on the reference database."""
+import os
+import re
+
+import numpy as np
+
+import fixtures
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def declared_symbols():
+    names = set()
+    for fn in os.listdir(os.path.join(ROOT, "include")):
+        if fn.endswith(".h"):
+            txt = open(os.path.join(ROOT, "include", fn)).read()
+            txt = re.sub(r"/\*.*?\*/", "", txt, flags=re.S)
+            names |= set(re.findall(r"\b(fz_\w+)\s*\(", txt))
+    return sorted(names)
+
+
+def test_library_exports_every_declared_symbol(fz):
+    L = fz.lib()
+    names = declared_symbols()
+    assert "fz_forward" in names and "fz_create" in names
+    missing = [n for n in names if not hasattr(L, n)]
+    assert not missing, missing
+
+
+def test_line_parser_matches_oracle(fz, orc):
+    text = fixtures.fixture_lines_text()
+    a = fz.lines_parse(text)
+    b = orc.parse_lines(text)
+    assert len(a) == len(b) == 37
+    for f in fz.LINE_DTYPE.names:
+        if f == "pad":
+            continue
+        assert np.array_equal(a[f], b[f]), f
+    fe = a[a["num"] == 4][0]
+    assert fe["flag"] == 0 and fe["abo_ierr"] == 0 and fe["sigma"] > 0 and fe["alpha"] > 0
+    assert fe["l0"] == 6301.500977            # REAL*4 read, rounded to 1e-6
+
+
+def test_line_parser_workload_database(fz, orc):
+    text = fz.atmos.line_database_text()
+    a, b = fz.lines_parse(text), orc.parse_lines(text)
+    for f in ("l0", "loggf", "eplow", "alpha", "sigma", "sl", "ll", "jl", "su", "lu", "ju"):
+        assert np.array_equal(a[f], b[f]), f
+
+
+def test_parser_rejects_malformed(fz):
+    import pytest
+    with pytest.raises(fz.FzError):
+        fz.lines_parse("1 026 1 6301.5 5.0P2.0\nEND\n")
+    with pytest.raises(fz.FzError):
+        fz.lines_parse("1  026  1   6301.5010  5.0P2.0  5.0D2.0  -0.720  3.654  0.000  0000.000 ps 0 0\n")
+
+
+def test_regions_from_lines_section(fz):
+    lines = fz.lines_parse(fixtures.fixture_lines_text())
+    reg = fz.regions_from_lines_section("4,5 500 -700.0 5.0", lines)
+    assert reg["nblend"][0] == 2 and reg["numwave"][0] == 500
+    assert abs(reg["wdif"][0, 1] - 1e3 * (6302.493652 - 6301.500977)) < 1e-6
