@@ -268,10 +268,12 @@ def main():
     hbm, how = peaks()
     kname = max(prof, key=lambda k: prof[k][0])
     kms = prof[kname][0] / max(prof[kname][1], 1)
-    if kname == "k_chem":
-        alg = a.ncol * (6 + 5) * a.nz * 4        # T,Pg,B,v in; Pg,rho,Pe,mu,tau5 out
+    if kname == "k_chain":
+        alg = a.ncol * (2 + 4) * a.nz * 4        # T,Pg in; Pg,rho,Pe,mu out
+    elif kname == "k_opac":
+        alg = a.ncol * (5 * 4) * a.nz            # T,Bx,By,Bz,vz in (nH, ne and the slab are intermediates)
     else:
-        alg = a.ncol * 4 * numw * 8              # RSYN1D out (slab in is an intermediate)
+        alg = a.ncol * 4 * numw * 8              # RSYN1D out (the slab is an intermediate)
     achieved = alg / (kms * 1e-3) / 1e9
     traffic = None
     tf = os.path.join(ROOT, "profiles", "traffic.json")

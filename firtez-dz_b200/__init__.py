@@ -30,6 +30,7 @@ MAXBLEND = 8
 TEM, PG, RHO, PEL, MW, BX, BY, BZ, VX, VY, VZ, TAU5, ZZ = range(13)
 
 FZ_OK, FZ_CHEM_NOCONV, FZ_NAN = 0, 1, 2
+KERNELS = ("k_chain", "k_opac", "k_synth")
 
 LINE_DTYPE = np.dtype([
     ("num", "<i4"), ("zn", "<i4"), ("ion", "<i4"), ("flag", "<i4"), ("otr", "<i4", 2),
@@ -179,10 +180,10 @@ class Synthesis:
 
     def profile_read(self):
         """{kernel: (total ms, launches)} since the last read."""
-        ms = np.zeros(2)
-        n = np.zeros(2, dtype=np.int32)
-        _check(lib().fz_profile_read(self._h, _p(ms), _p(n), 2))
-        return {"k_chem": (ms[0], int(n[0])), "k_synth": (ms[1], int(n[1]))}
+        ms = np.zeros(3)
+        n = np.zeros(3, dtype=np.int32)
+        _check(lib().fz_profile_read(self._h, _p(ms), _p(n), 3))
+        return {k: (ms[i], int(n[i])) for i, k in enumerate(KERNELS)}
 
     def forward_device(self, model_ptr, ncol, syn_ptr, model_out_ptr, status_ptr=0, stream=0, hydrostatic=False):
         """Enqueue a synthesis on device pointers (e.g. torch ``data_ptr()``)."""

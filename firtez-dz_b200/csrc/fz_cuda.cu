@@ -1,15 +1,19 @@
 // firtez-dz B200: kernels and C-ABI of the Stokes synthesis path.
 //
 // Data flow of one fz_forward call (all on one stream):
-//   k_chem   one warp per column, FP64: (optional) hydrostatic RK4 from the top,
-//            chemical equilibrium per height, continuum/line opacity, damping,
-//            Doppler widths and field geometry -> a per-column "opacity slab"
-//            (nz rows of SW floats) in scratch memory, plus the updated model
-//            (rho, Pe, mu, log tau5, Pg) like FORWARD1D writes it back.
+//   k_chain  one warp per column, FP64, lanes over the 92 elements: the
+//            sequential part of FORWARD1D -- the GET_RHO warm-start chain along
+//            z and, in hydrostatic mode, the RK4 integration of ln Pg from the
+//            top.  Writes (nH, ne) per height to scratch and rho, Pe, mu, Pg
+//            into the output model.
+//   k_opac   one thread per (column, height), FP64: continuum/line opacity,
+//            damping, Doppler width, velocity shift and field geometry ->
+//            the per-column "opacity slab" (nz rows of SW floats) in scratch.
 //   k_synth  one CTA per column, one thread per wavelength, FP32: stages the
 //            slab in shared memory, walks the heights bottom -> top evaluating
 //            the Zeeman-split Voigt/Faraday profiles, the 4x4 evolution
-//            operator and the formal-solution recurrence, writes RSYN1D.
+//            operator and the formal-solution recurrence, writes RSYN1D; one
+//            thread integrates log tau5.
 #include <cuda_runtime.h>
 
 #include <cmath>
@@ -37,12 +41,11 @@ constexpr int MAXNZ = 1024;
 struct DevParams {
   int nz, numw, nreg, nlu, sw;
   int reg_p0[MAXREG], reg_nw[MAXREG], reg_nb[MAXREG], reg_lb[MAXREG];
-  double reg_l0[MAXREG];   // central wavelength of the region's main line [A]
-  LineP lu[MAXLU];         // used lines in region order
+  ContP cont[MAXREG + 1];   // continuum constants of each region's main line, then 5000 A
+  LineP lu[MAXLU];          // used lines in region order
   int lu_nc[MAXLU], lu_c0[MAXLU];
   float comp_shift[MAXCOMP], comp_str[MAXCOMP];
   int comp_type[MAXCOMP];
-  double matom_h, matom_he, abund_he;
 };
 
 // Per-wavelength constants.
@@ -53,124 +56,65 @@ struct LamP {
   int reg;
 };
 
-// slab row layout
+// slab row layout: T, boundary flag, KC5 (REAL), rho (REAL), kc*dz per
+// region, 6 field-geometry factors, 4 floats per used line
 __host__ __device__ inline int slab_w(int nreg, int nlu) {
-  const int w = 2 + nreg + 6 + 4 * nlu;
+  const int w = 4 + nreg + 6 + 4 * nlu;
   return (w + 3) & ~3;
 }
-__host__ __device__ inline int slab_geo(int nreg) { return 2 + nreg; }
-__host__ __device__ inline int slab_line(int nreg) { return 2 + nreg + 6; }
+__host__ __device__ inline int slab_geo(int nreg) { return 4 + nreg; }
+__host__ __device__ inline int slab_line(int nreg) { return 4 + nreg + 6; }
 
-// ------------------------------------------------------------------ k_chem
 __device__ __forceinline__ float mget(const float* m, int nz, int p, int k) { return m[p * nz + k]; }
 
-// Per-height quantities of the slab (lanes split the work).
-__device__ void fill_row(const DevParams& P, const Consts& K, float* row, int lane, float T, double nhyd,
-                         double nelec, double dz, float bx, float by, float bz, float vz, float* kc5_out) {
-  if (lane == 0) {
-    double kc5 = opac_continuum(T, 5000.0, nelec, nhyd);
-    kc5 = kc5 / nhyd * (1.0 / MAMU);
-    row[0] = T;
-    row[1] = (kc5 < KC5THRESHOLD) ? 0.0f : 1.0f;
-    *kc5_out = (float)kc5;
-  } else if (lane <= P.nreg) {
-    const int r = lane - 1;
-    const double kc = opac_continuum(T, P.reg_l0[r], nelec, nhyd);
-    row[2 + r] = (float)(kc * dz);
-  } else if (lane >= 9 && lane < 9 + P.nlu) {   // regions use lanes 1..8, lines 9..24
-    const int b = lane - 9;
-    const LineP& L = P.lu[b];
-    const double klin = opac_line(L, T, nelec, nhyd, K);
-    const double damp = get_damping(L, nhyd, T, K, P.matom_h, P.matom_he, P.abund_he);
-    const double vdop = sqrt(2.0 * KBOL * (double)T / (L.matom * MAMU));
-    const double dldop = 1e3 * (vdop * L.l0 / LIGHT);
-    const double dlv = -1e3 * L.l0 * (double)vz / LIGHT;
-    float* q = row + slab_line(P.nreg) + 4 * b;
-    q[0] = (float)(klin * dz);
-    q[1] = (float)damp;
-    q[2] = (float)(1.0 / dldop);
-    q[3] = (float)(dlv - L.wdif);
-  } else if (lane == 31) {
-    // field geometry, src/absorption_matrix.f90:919-991
-    const double x = bx, y = by, z = bz;
-    const double x2 = pow(x, 2.0), y2 = pow(y, 2.0), z2 = pow(z, 2.0);
-    const double b2 = x2 + y2 + z2, b = sqrt(b2);
-    double cosg = 0, cgf = 1, sgf = 1, c2p = 0, s2p = 0;
-    if (b > 0) {
-      cosg = z / b;
-      cgf = 1 + z2 / b2;
-      sgf = 1 - z2 / b2;
-    }
-    if (x != 0 || y != 0) {
-      c2p = (x2 - y2) / (x2 + y2);
-      s2p = 2. * x * y / (x2 + y2);
-    }
-    float* g = row + slab_geo(P.nreg);
-    g[0] = (float)(0.25 * cgf);
-    g[1] = (float)(0.5 * sgf);
-    g[2] = (float)(sgf * c2p);
-    g[3] = (float)(sgf * s2p);
-    g[4] = (float)(0.5 * cosg);
-    g[5] = (float)b;
-  }
+template <typename T>
+__device__ __forceinline__ void copy_to_shared(T* dst, const T* src) {
+  const int* s = reinterpret_cast<const int*>(src);
+  int* d = reinterpret_cast<int*>(dst);
+  for (int i = threadIdx.x; i < (int)(sizeof(T) / 4); i += blockDim.x) d[i] = s[i];
 }
 
-__device__ __forceinline__ double layer_dz(const float* m, int nz, int k) {
-  // DELTAZ of EVOL_OPERATOR, src/rtesolver.f90:439-443 (z in km)
-  return (k == nz - 1) ? 1e5 * fabs((double)mget(m, nz, 12, k) - (double)mget(m, nz, 12, k - 1))
-                       : 1e5 * fabs((double)mget(m, nz, 12, k + 1) - (double)mget(m, nz, 12, k));
-}
-
+// ----------------------------------------------------------------- k_chain
+// One warp per column walks the heights sequentially: the GET_RHO warm-start
+// chain (NELEC of one call seeds the next, src/forward.f90:914) and, in
+// hydrostatic mode, the RK4 integration of ln Pg from the top
+// (RK4_INTEGRATION_LOG, src/hydrostatic_tools.f90:150-222, RK4_LOG :350-396).
+// Writes per height (nH, ne) as FORWARD1D uses them, and rho, Pe, mu (and
+// Pg) into the output model.
 template <bool HE>
-__global__ void __launch_bounds__(128) k_chem(const DevParams* __restrict__ Pg, const Consts* __restrict__ Kg,
-                                              int ncol, const float* model, float* mout,
-                                              float* __restrict__ slab, int* __restrict__ status) {
-  extern __shared__ float sm_chem[];
+__global__ void __launch_bounds__(128) k_chain(const Consts* __restrict__ Kg, int ncol, int nz, const float* model,
+                                               float* mout, double2* __restrict__ chem, int* __restrict__ status) {
   __shared__ Consts K;
-  __shared__ DevParams P;
-  {
-    const int* src = reinterpret_cast<const int*>(Kg);
-    int* dst = reinterpret_cast<int*>(&K);
-    for (int i = threadIdx.x; i < (int)(sizeof(Consts) / 4); i += blockDim.x) dst[i] = src[i];
-    const int* s2 = reinterpret_cast<const int*>(Pg);
-    int* d2 = reinterpret_cast<int*>(&P);
-    for (int i = threadIdx.x; i < (int)(sizeof(DevParams) / 4); i += blockDim.x) d2[i] = s2[i];
-  }
+  copy_to_shared(&K, Kg);
   __syncthreads();
   const int lane = threadIdx.x & 31;
-  const int wib = threadIdx.x >> 5;
-  const int col = blockIdx.x * (blockDim.x >> 5) + wib;
+  const int col = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
   if (col >= ncol) return;
-  const int nz = P.nz, sw = P.sw;
-  float* kc5s = sm_chem + wib * 2 * nz;   // per warp: kc5 (REAL) and rho
-  float* rhos = kc5s + nz;
   const float* m = model + (size_t)col * 13 * nz;
   float* mo = mout + (size_t)col * 13 * nz;
-  float* sl = slab + (size_t)col * nz * sw;
+  double2* ch = chem + (size_t)col * nz;
   if (mo != m)
     for (int i = lane; i < 13 * nz; i += 32) mo[i] = m[i];
   __syncwarp();
+  double ab[3];
+#pragma unroll
+  for (int j = 0; j < 3; ++j) ab[j] = (lane + 32 * j < FZ_NELEM) ? K.ab10[lane + 32 * j] : 0.0;
   int st = 0;
   if (!HE) {
     double nelec = 0.0;
     WarpSaha w;
     for (int k = 0; k < nz; ++k) {
-      const float T = mget(m, nz, 0, k);
-      saha_prepare(w, (double)T, K, lane);
-      const RhoOut r = get_rho_warp(w, (double)mget(m, nz, 1, k), nelec, K, lane);
+      saha_prepare(w, (double)mget(m, nz, 0, k), K, lane);
+      const RhoOut r = get_rho_warp(w, ab, (double)mget(m, nz, 1, k), nelec, K, lane);
       st |= r.status;
       if (lane == 0) {
-        const float rho = (float)r.dens;
-        mo[2 * nz + k] = rho;
+        mo[2 * nz + k] = (float)r.dens;
         mo[3 * nz + k] = (float)r.pelec;
         mo[4 * nz + k] = (float)r.molecw;
-        rhos[k] = rho;
+        ch[k] = make_double2(r.nhyd, nelec);
       }
-      fill_row(P, K, sl + (size_t)k * sw, lane, T, r.nhyd, nelec, layer_dz(m, nz, k), mget(m, nz, 5, k),
-               mget(m, nz, 6, k), mget(m, nz, 7, k), mget(m, nz, 10, k), &kc5s[k]);
     }
   } else {
-    // RK4_INTEGRATION_LOG, src/hydrostatic_tools.f90:150-222, RK4_LOG :350-396
     const int top = nz - 1;
     double nelec = (double)mget(m, nz, 3, top) / KBOL / (double)mget(m, nz, 0, top);
     double t0 = (double)mget(m, nz, 12, top) * 1000.0 * 100.0;
@@ -178,21 +122,18 @@ __global__ void __launch_bounds__(128) k_chem(const DevParams* __restrict__ Pg, 
     WarpSaha s0, sm, s1;
     saha_prepare(s0, (double)mget(m, nz, 0, top), K, lane);
     auto emit = [&](int k, double pg8, const RhoOut& r) {
-      const float T = mget(m, nz, 0, k);
-      const float pel = (float)r.pelec;
       if (lane == 0) {
+        const float pel = (float)r.pelec;
         mo[1 * nz + k] = (float)exp(pg8);
         mo[2 * nz + k] = (float)r.dens;
         mo[3 * nz + k] = pel;
         mo[4 * nz + k] = (float)r.molecw;
-        rhos[k] = (float)r.dens;
+        // FORWARD1D uses NELEC = PEL/KBOL/TEM from the REAL*4 model (src/forward.f90:900)
+        ch[k] = make_double2(r.nhyd, (double)pel / KBOL / (double)mget(m, nz, 0, k));
       }
-      const double vnelec = (double)pel / KBOL / (double)T;   // src/forward.f90:900
-      fill_row(P, K, sl + (size_t)k * sw, lane, T, r.nhyd, vnelec, layer_dz(m, nz, k), mget(m, nz, 5, k),
-               mget(m, nz, 6, k), mget(m, nz, 7, k), mget(m, nz, 10, k), &kc5s[k]);
     };
     {
-      const RhoOut r = get_rho_warp(s0, exp(u0), nelec, K, lane);
+      const RhoOut r = get_rho_warp(s0, ab, exp(u0), nelec, K, lane);
       st |= r.status;
       emit(top, u0, r);
     }
@@ -200,27 +141,27 @@ __global__ void __launch_bounds__(128) k_chem(const DevParams* __restrict__ Pg, 
       const double dz = ((double)mget(m, nz, 12, k) - (double)mget(m, nz, 12, k + 1)) * 1000.0 * 100.0;
       const double t1 = t0 + dz;
       const double tm0 = (double)mget(m, nz, 0, k + 1), tm1 = (double)mget(m, nz, 0, k);
-      RhoOut q = get_rho_warp(s0, exp(u0), nelec, K, lane);
+      RhoOut q = get_rho_warp(s0, ab, exp(u0), nelec, K, lane);
       st |= q.status;
       const double k1 = (-q.molecw * MAMU * GRAV / (KBOL * tm0)) * dz;
       const double it1 = t0 + dz / 2.0;
       const double iy1 = u0 + k1 / 2.0;
       const double tem = tm0 / dz * (t0 + dz - it1) + tm1 / dz * (it1 - t0);
       saha_prepare(sm, tem, K, lane);
-      q = get_rho_warp(sm, exp(iy1), nelec, K, lane);
+      q = get_rho_warp(sm, ab, exp(iy1), nelec, K, lane);
       st |= q.status;
       const double k2 = (-q.molecw * MAMU * GRAV / (KBOL * tem)) * dz;
       const double iy2 = u0 + k2 / 2.0;
-      q = get_rho_warp(sm, exp(iy2), nelec, K, lane);
+      q = get_rho_warp(sm, ab, exp(iy2), nelec, K, lane);
       st |= q.status;
       const double k3 = (-q.molecw * MAMU * GRAV / (KBOL * tem)) * dz;
       const double iy3 = u0 + k3;
       saha_prepare(s1, tm1, K, lane);
-      q = get_rho_warp(s1, exp(iy3), nelec, K, lane);
+      q = get_rho_warp(s1, ab, exp(iy3), nelec, K, lane);
       st |= q.status;
       const double k4 = (-q.molecw * MAMU * GRAV / (KBOL * tm1)) * dz;
       const double u1 = u0 + 1.0 / 6.0 * (k1 + 2.0 * k2 + 2.0 * k3 + k4);
-      q = get_rho_warp(s1, exp(u1), nelec, K, lane);
+      q = get_rho_warp(s1, ab, exp(u1), nelec, K, lane);
       st |= q.status;
       emit(k, u1, q);
       u0 = u1;
@@ -228,18 +169,77 @@ __global__ void __launch_bounds__(128) k_chem(const DevParams* __restrict__ Pg, 
       s0 = s1;
     }
   }
-  __syncwarp();
-  // log tau5 from the top, src/forward.f90:1000-1006 (REAL*4 accumulation)
-  if (lane == 0) {
-    float tau = 1e-9f;
-    mo[11 * nz + nz - 1] = log10f(tau);
-    for (int k = nz - 2; k >= 0; --k) {
-      const float a = (kc5s[k] * rhos[k] + kc5s[k + 1] * rhos[k + 1]) / 2.0f;
-      const double b = ((double)mget(m, nz, 12, k + 1) - (double)mget(m, nz, 12, k)) * 1000.0 * 100.0;
-      tau = (float)((double)tau + (double)a * b);
-      mo[11 * nz + k] = log10f(tau);
+  if (lane == 0 && status) status[col] = st;
+}
+
+// ------------------------------------------------------------------ k_opac
+// One thread per (column, height): every per-height quantity of the slab.
+// KC5 and the boundary flag (src/forward.f90:926-931), KC of each region at
+// its main line (:940), KLIN and the damping of every line (:949-951), the
+// Doppler width, velocity shift and field geometry of GET_ABS_MAT
+// (src/absorption_matrix.f90:914-991, :1018).
+__global__ void __launch_bounds__(256) k_opac(const DevParams* __restrict__ Pg, const Consts* __restrict__ Kg,
+                                              int ncol, const float* __restrict__ mout,
+                                              const double2* __restrict__ chem, float* __restrict__ slab) {
+  __shared__ DevParams P;
+  __shared__ Consts K;
+  copy_to_shared(&P, Pg);
+  copy_to_shared(&K, Kg);
+  __syncthreads();
+  const int nz = P.nz, sw = P.sw;
+  const size_t total = (size_t)ncol * nz;
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (size_t)gridDim.x * blockDim.x) {
+    const int col = (int)(i / nz), k = (int)(i % nz);
+    const float* m = mout + (size_t)col * 13 * nz;
+    const double2 c = chem[i];
+    const double nhyd = c.x, nelec = c.y;
+    const float Tf = mget(m, nz, 0, k);
+    const double T = (double)Tf;
+    const double dz = (k == nz - 1) ? 1e5 * fabs((double)mget(m, nz, 12, k) - (double)mget(m, nz, 12, k - 1))
+                                    : 1e5 * fabs((double)mget(m, nz, 12, k + 1) - (double)mget(m, nz, 12, k));
+    float* row = slab + i * sw;
+    const double kc5 = opac_continuum(T, nelec, nhyd, P.cont[P.nreg]) / nhyd * (1.0 / MAMU);
+    row[0] = Tf;
+    row[1] = (kc5 < KC5THRESHOLD) ? 0.0f : 1.0f;
+    row[2] = (float)kc5;
+    row[3] = mget(m, nz, 2, k);
+    for (int r = 0; r < P.nreg; ++r) row[4 + r] = (float)(opac_continuum(T, nelec, nhyd, P.cont[r]) * dz);
+    // field geometry, src/absorption_matrix.f90:919-991
+    {
+      const double x = mget(m, nz, 5, k), y = mget(m, nz, 6, k), z = mget(m, nz, 7, k);
+      const double x2 = x * x, y2 = y * y, z2 = z * z;
+      const double b2 = x2 + y2 + z2, b = sqrt(b2);
+      double cosg = 0, cgf = 1, sgf = 1, c2p = 0, s2p = 0;
+      if (b > 0) {
+        cosg = z / b;
+        cgf = 1 + z2 / b2;
+        sgf = 1 - z2 / b2;
+      }
+      if (x != 0 || y != 0) {
+        c2p = (x2 - y2) / (x2 + y2);
+        s2p = 2. * x * y / (x2 + y2);
+      }
+      float* g = row + slab_geo(P.nreg);
+      g[0] = (float)(0.25 * cgf);
+      g[1] = (float)(0.5 * sgf);
+      g[2] = (float)(sgf * c2p);
+      g[3] = (float)(sgf * s2p);
+      g[4] = (float)(0.5 * cosg);
+      g[5] = (float)b;
     }
-    if (status) status[col] = st;
+    const double vz = (double)mget(m, nz, 10, k);
+    for (int b = 0; b < P.nlu; ++b) {
+      const LineP& L = P.lu[b];
+      const double klin = opac_line(L, T, nelec, nhyd, K);
+      const double damp = get_damping(L, nhyd, T);
+      const double dldop = 1e3 * (sqrt(L.vdk * T) * L.l0 / LIGHT);
+      const double dlv = -1e3 * L.l0 * vz / LIGHT;
+      float* q = row + slab_line(P.nreg) + 4 * b;
+      q[0] = (float)(klin * dz);
+      q[1] = (float)damp;
+      q[2] = (float)(1.0 / dldop);
+      q[3] = (float)(dlv - L.wdif);
+    }
   }
 }
 
@@ -247,15 +247,11 @@ __global__ void __launch_bounds__(128) k_chem(const DevParams* __restrict__ Pg, 
 __global__ void __launch_bounds__(MAXNUMW) k_synth(const DevParams* __restrict__ Pg, const LamP* __restrict__ lam,
                                                    const float* __restrict__ gain, int ncol,
                                                    const float* __restrict__ slab, double* __restrict__ syn,
-                                                   int* __restrict__ status) {
+                                                   float* mout, int* __restrict__ status) {
   extern __shared__ float4 sm_synth4[];
   float* sm = reinterpret_cast<float*>(sm_synth4);
   __shared__ DevParams P;
-  {
-    const int* s2 = reinterpret_cast<const int*>(Pg);
-    int* d2 = reinterpret_cast<int*>(&P);
-    for (int i = threadIdx.x; i < (int)(sizeof(DevParams) / 4); i += blockDim.x) d2[i] = s2[i];
-  }
+  copy_to_shared(&P, Pg);
   const int col = blockIdx.x;
   const int nz = Pg->nz, sw = Pg->sw;
   // stage the column's slab (nz*sw floats, 16-byte rows) in shared memory
@@ -267,6 +263,18 @@ __global__ void __launch_bounds__(MAXNUMW) k_synth(const DevParams* __restrict__
   __syncthreads();
   const int l = threadIdx.x;
   if (l >= P.numw) return;
+  if (l == 0) {
+    // log tau5 from the top, src/forward.f90:1000-1006 (REAL*4 accumulation)
+    float* mo = mout + (size_t)col * 13 * nz;
+    float tau = 1e-9f;
+    mo[11 * nz + nz - 1] = log10f(tau);
+    for (int k = nz - 2; k >= 0; --k) {
+      const float a = (sm[k * sw + 2] * sm[k * sw + 3] + sm[(k + 1) * sw + 2] * sm[(k + 1) * sw + 3]) / 2.0f;
+      const double b = ((double)mo[12 * nz + k + 1] - (double)mo[12 * nz + k]) * 1000.0 * 100.0;
+      tau = (float)((double)tau + (double)a * b);
+      mo[11 * nz + k] = log10f(tau);
+    }
+  }
   const LamP lp = lam[l];
   const int r = lp.reg;
   const int nb = P.reg_nb[r], lb = P.reg_lb[r];
@@ -284,7 +292,7 @@ __global__ void __launch_bounds__(MAXNUMW) k_synth(const DevParams* __restrict__
     }
     const float g1 = row[goff], g2 = row[goff + 1], g3 = row[goff + 2], g4 = row[goff + 3], g5 = row[goff + 4],
                 B = row[goff + 5];
-    float tI = row[2 + r], tQ = 0.f, tU = 0.f, tV = 0.f, rQ = 0.f, rU = 0.f, rV = 0.f;
+    float tI = row[4 + r], tQ = 0.f, tU = 0.f, tV = 0.f, rQ = 0.f, rU = 0.f, rV = 0.f;
     for (int b = 0; b < nb; ++b) {
       const float* q = row + loff + 4 * (lb + b);
       const float kldz = q[0], a = q[1], idd = q[2];
@@ -362,15 +370,17 @@ __global__ void k_gain(const DevParams* __restrict__ Pg, const Consts* __restric
   const int N = FZ_HSRA_LEN;
   if (threadIdx.x < 32) {
     const int lane = threadIdx.x;
+    double ab[3];
+    for (int j = 0; j < 3; ++j) ab[j] = (lane + 32 * j < FZ_NELEM) ? K.ab10[lane + 32 * j] : 0.0;
     double nelec = 0.0;
     WarpSaha w;
     int st = 0;
     for (int k = 0; k < N; ++k) {
-      const float T = fz_tab_hsra_tem[k];
-      saha_prepare(w, (double)T, K, lane);
-      const RhoOut r = get_rho_warp(w, (double)fz_tab_hsra_pg[k], nelec, K, lane);
+      const double T = (double)fz_tab_hsra_tem[k];
+      saha_prepare(w, T, K, lane);
+      const RhoOut r = get_rho_warp(w, ab, (double)fz_tab_hsra_pg[k], nelec, K, lane);
       st |= r.status;
-      if (lane < P.nreg) sm_gain[k * P.nreg + lane] = opac_continuum(T, P.reg_l0[lane], nelec, r.nhyd);
+      if (lane < P.nreg) sm_gain[k * P.nreg + lane] = opac_continuum(T, nelec, r.nhyd, P.cont[lane]);
     }
     if (lane == 0 && status) *status = st;
   }
@@ -424,26 +434,158 @@ __global__ void k_fp32_peak(float* out, int iters, float s) {
 }
 
 // ------------------------------------------------------------------ context
+const double kAbund[FZ_NELEM] = {
+#include "fz_abund.inc"
+};
+const double kMatom[FZ_NELEM] = {
+#include "fz_matom.inc"
+};
+const double kXI[FZ_NELEM] = {
+#include "fz_xi.inc"
+};
+const double kXII[FZ_NELEM] = {
+#include "fz_xii.inc"
+};
+
 void host_consts(Consts& K) {
   K.csaha1 = std::pow(HPLA, 3.0) / std::pow(2.0 * DPI * MELE * KBOL, 3.0 / 2.0);
   K.csaha2 = EVOLT / KBOL;
   K.rbohr = std::pow(HPLA, 2.0) / (4.0 * std::pow(DPI, 2.0) * MELE * std::pow(QELE, 2.0));
   K.deno_sa = 0.0;
   K.deno_sam = 0.0;
-  static const double ab[FZ_NELEM] = {
-#include "fz_abund.inc"
-  };
   for (int i = 0; i < FZ_NELEM; ++i) {
-    K.ab10[i] = std::pow(10.0, ab[i] - 12.0);
+    K.ab10[i] = std::pow(10.0, kAbund[i] - 12.0);
     K.deno_sa = K.deno_sa + K.ab10[i];
   }
-  static const double mat[FZ_NELEM] = {
-#include "fz_matom.inc"
-  };
-  for (int i = 0; i < FZ_NELEM; ++i) K.deno_sam = K.deno_sam + MAMU * mat[i] * K.ab10[i];
+  for (int i = 0; i < FZ_NELEM; ++i) K.deno_sam = K.deno_sam + MAMU * kMatom[i] * K.ab10[i];
+}
+
+// Wavelength-only factors of OPAC_CONTINUUM at lambda0 [A], src/cont_opacity.f90:48-357.
+ContP host_cont(double l0) {
+  static const double A1[6] = {0, 2483.346, -3449.889, 2200.04, -696.271, 88.283};
+  static const double B1[6] = {0, 285.827, -1158.382, 2427.719, -1841.4, 444.517};
+  static const double C1[6] = {0, -2054.291, 8746.523, -13651.105, 8624.97, -1863.864};
+  static const double D1[6] = {0, 2827.776, -11485.632, 16755.524, -10051.53, 2095.288};
+  static const double E1[6] = {0, -1341.537, 5303.609, -7510.494, 4400.067, -901.788};
+  static const double F1[6] = {0, 208.952, -812.939, 1132.738, -655.02, 132.985};
+  static const double A2[4] = {518.1021, 473.2636, -482.2089, 115.5291};
+  static const double B2[4] = {-734.8666, 1443.4137, -737.1616, 169.6374};
+  static const double C2[4] = {1021.1775, -1977.3395, 1096.8827, -245.649};
+  static const double D2[4] = {-479.0721, 922.3575, -521.1341, 114.243};
+  static const double E2[4] = {93.1373, -178.9275, 101.7963, -21.9972};
+  static const double F2[4] = {-6.4285, 12.36, -7.0571, 1.5097};
+  ContP c;
+  std::memset(&c, 0, sizeof(c));
+  const double lm = l0 / 1e4;
+  const double p2 = std::pow(lm, 2.0), p3 = std::pow(lm, 3.0), p4 = std::pow(lm, 4.0);
+  if (lm < 0.3645) {
+    c.nff = 4;
+    for (int i = 0; i < 4; ++i) c.ffc[i] = A2[i] * p2 + B2[i] + C2[i] / lm + D2[i] / p2 + E2[i] / p3 + F2[i] / p4;
+  } else {
+    c.nff = 6;
+    for (int i = 0; i < 6; ++i) c.ffc[i] = A1[i] * p2 + B1[i] + C1[i] / lm + D1[i] / p2 + E1[i] / p3 + F1[i] / p4;
+  }
+  const double LAMBDAP = 1.6419, CTE = 0.75e-18, ALPHA = (HPLA * LIGHT / KBOL) * 1e4;
+  static const double CC[6] = {152.519, 49.534, -118.858, 92.536, -34.194, 4.982};
+  if (lm < LAMBDAP) {
+    const double com = 1.0 / lm - 1.0 / LAMBDAP;
+    double sg = CC[0] + CC[1] * std::pow(com, 0.5) + CC[2] * com + CC[3] * std::pow(com, 1.5) +
+                CC[4] * std::pow(com, 2.0) + CC[5] * std::pow(com, 2.5);
+    c.sbf = CTE * sg * std::pow(lm, 3.0) * std::pow(com, 1.5);
+    c.bfa1 = ALPHA / LAMBDAP;
+    c.bfa2 = ALPHA / lm;
+  }
+  const double IOPOT = (double)13.595f, E8 = (double)1e-8f;   // REAL*4 literals, :255-264
+  const double HC1 = E8 * IOPOT * EVOLT / (HPLA * LIGHT);
+  const double HC2 = std::pow(E8, 3.0) * 64.0 * std::pow(DPI, 4.0) * MELE * std::pow(QELE, 10.0) /
+                     (3.0 * std::sqrt(3.0) * std::pow(LIGHT, 4.0) * std::pow(HPLA, 6.0));
+  const double HC3 = HPLA * LIGHT / (KBOL * E8);
+  const double HC4 = IOPOT * EVOLT / KBOL;
+  c.n0 = 1 + (int)std::floor(std::sqrt(HC1 * l0));
+  c.hpre = HC2 * std::pow(l0, 3.0);
+  c.c3l = HC3 / l0;
+  c.c4 = HC4;
+  c.ray = (5.799e-13 + (1.422e-6 + 2.784 / std::pow(l0, 2.0)) / std::pow(l0, 2.0)) / std::pow(l0, 4.0);
+  c.ct = (8.0 * DPI / 3.0) * (std::pow(QELE / LIGHT, 4.0)) / std::pow(MELE, 2.0);
+  return c;
+}
+
+// REFRAX, src/atom_database.f90:1039-1074
+double host_refrax(double w) {
+  const double T = 15.0, P = 760.0, H = 0.0;
+  const double s = 1.0 / std::pow(w, 2.0);
+  const double r = 6.4328e-5 + 2.94981e-2 / (146.0 - s) + 2.554e-4 / (41.0 - s);
+  const double y = 1.0 / (273.15 + T);
+  const double alpha = 3.67e-3 + 3.3e-4 * std::exp((0.19 - w) / 0.12);
+  const double wvsp = std::pow(
+      10.0, -55.1132754 +
+                y * (1.19551822e5 +
+                     y * (-9.70108858e7 + y * (4.12856913e10 + y * (-9.87931835e12 + y * (1.25868645e15 - 6.66885272e16 * y))))));
+  const double wvp = 1.0e-2 * H * wvsp;
+  return 1.0 + 1.31579e-3 * r * P / (1.0 + alpha * (T - 1.0) / (1.0 + 15.0 * alpha)) - 5.49e-8 * wvp / (1.0 + alpha * T);
+}
+
+// Per-line constants of OPAC_LINE (src/line_opacity.f90:34-108) and
+// GET_DAMPING (src/damping.f90:842-1012; ABO or Unsold van der Waals).
+LineP host_line(const fz_line& L, double wdif, const Consts& K) {
+  LineP q;
+  std::memset(&q, 0, sizeof(q));
+  const int z = L.zn - 1;
+  const double m = kMatom[z];
+  q.l0 = L.l0;
+  q.wdif = wdif;
+  q.zn = L.zn;
+  q.ion = L.ion;
+  q.term1 = std::sqrt(DPI) * std::pow(QELE, 2.0) / (MELE * LIGHT) * std::pow(10.0, L.loggf) * L.l0 * 1e-8;
+  q.m2k = m * MAMU / (2.0 * KBOL);
+  q.chik = L.eplow * EVOLT / KBOL;
+  q.hclk = HPLA * LIGHT / (1.0e-8 * L.l0 * KBOL);
+  q.nab = std::pow(10.0, kAbund[z] - 12.0);
+  q.xi_k = K.csaha2 * kXI[z];
+  q.xii_k = K.csaha2 * kXII[z];
+  q.vdk = 2.0 * KBOL / (MAMU * m);
+  const double lambda = L.l0 * 1e-8;
+  q.grad = 0.2223 / std::pow(lambda, 2.0);
+  q.dfac = lambda / (4.0 * DPI);
+  const double mu_h = MAMU * (m * kMatom[0]) / (m + kMatom[0]);
+  const double mu_he = MAMU * (m * kMatom[1]) / (m + kMatom[1]);
+  const double he = std::pow(10.0, kAbund[1] - 12.0);
+  if (L.sigma > 0 && L.alpha > 0) {
+    const double e1 = 2.0 - L.alpha / 2.0, e2 = (1.0 - L.alpha) / 2.0;
+    const double gf =
+        1.0 + (-0.5748646 + (0.9512363 + (-0.6998588 + (0.4245549 - 0.1010678 * e1) * e1) * e1) * e1) * e1;
+    double beta = std::pow(4.0 / DPI, L.alpha / 2.0) * gf * std::pow(1e6, L.alpha) * (L.sigma * std::pow(K.rbohr, 2.0)) *
+                  std::pow(8.0 * KBOL / DPI, e2);
+    beta = 2.0 * beta;
+    q.gc = beta * (std::pow(mu_h, -e2) + (double)0.3181818f * he * std::pow(mu_he, -e2));
+    q.ge = e2;
+  } else {
+    double rindex = (double)1.0004f;
+    if (lambda * 1e8 >= 1800.0) rindex = host_refrax(lambda * 1e4);
+    const double lvac = rindex * lambda;
+    const double epupp = L.eplow + (HPLA * LIGHT / lvac) / EVOLT;
+    const double ionf = (double)(float)(L.ion - 1);
+    double ed1, ed2, chyd;
+    if (L.ion == 1) {
+      ed1 = std::max(kXI[z] - epupp - kXI[z] * ionf, 1.0);
+      ed2 = std::max(kXI[z] - L.eplow - kXI[z] * ionf, 3.0);
+      chyd = 1.0;
+    } else {
+      ed1 = std::max(kXII[z] - epupp - kXI[z] * ionf, 1.0);
+      ed2 = std::max(kXII[z] - L.eplow - kXI[z] * ionf, 3.0);
+      chyd = (double)1.741f;
+    }
+    chyd = chyd * 17.0 * std::pow(8.0 * KBOL / DPI, 0.3);
+    chyd = chyd * std::pow(std::pow(10.0, -30.5325) * (1.0 / std::pow(ed1, 2.0) - 1.0 / std::pow(ed2, 2.0)), 0.4);
+    q.gc = chyd * (std::pow(mu_h, -0.3) + he * std::pow(mu_he, -0.3));
+    q.ge = 0.3;
+  }
+  return q;
 }
 
 }  // namespace
+
+constexpr int NKERN = 3;   // k_chain, k_opac, k_synth
 
 struct fz_ctx {
   int device = 0;
@@ -456,15 +598,17 @@ struct fz_ctx {
   Consts* d_consts = nullptr;
   LamP* d_lam = nullptr;
   float* d_gain = nullptr;
-  // scratch (grown on demand)
+  // scratch (grown on demand): per (column, height) nH, ne and the opacity slab
   float* d_slab = nullptr;
-  size_t slab_cols = 0;
+  double2* d_chem = nullptr;
+  size_t scratch_cols = 0;
   // staging for the host-buffer API
   float* d_model = nullptr;
   double* d_syn = nullptr;
   int* d_status = nullptr;
   size_t io_cols = 0;
   cudaStream_t stream = nullptr;
+  int nsm = 148;
   // per-kernel profiling (pending event pairs are resolved on read)
   bool prof = false;
   struct Pending {
@@ -472,8 +616,8 @@ struct fz_ctx {
     cudaEvent_t a, b;
   };
   std::vector<Pending> pending;
-  double prof_ms[2] = {0, 0};
-  int prof_n[2] = {0, 0};
+  double prof_ms[NKERN] = {0, 0, 0};
+  int prof_n[NKERN] = {0, 0, 0};
 };
 
 namespace {
@@ -491,13 +635,16 @@ int cuda_fail(cudaError_t e) {
     if (_rc) return _rc;                      \
   } while (0)
 
-int ensure_slab(fz_ctx* c, int ncol) {
-  if ((size_t)ncol <= c->slab_cols) return 0;
-  if (c->d_slab) cudaFree(c->d_slab);
+int ensure_scratch(fz_ctx* c, int ncol) {
+  if ((size_t)ncol <= c->scratch_cols) return 0;
+  cudaFree(c->d_slab);
+  cudaFree(c->d_chem);
   c->d_slab = nullptr;
-  c->slab_cols = 0;
+  c->d_chem = nullptr;
+  c->scratch_cols = 0;
   FZ_CK(cudaMalloc(&c->d_slab, (size_t)ncol * c->nz * c->sw * sizeof(float)));
-  c->slab_cols = ncol;
+  FZ_CK(cudaMalloc(&c->d_chem, (size_t)ncol * c->nz * sizeof(double2)));
+  c->scratch_cols = ncol;
   return 0;
 }
 
@@ -521,25 +668,31 @@ struct ProfScope {
 
 int launch_forward(fz_ctx* c, int ncol, const float* d_model, int hydrostatic, double* d_syn, float* d_mout,
                    int* d_status, cudaStream_t s) {
-  int rc = ensure_slab(c, ncol);
+  int rc = ensure_scratch(c, ncol);
   if (rc) return rc;
   if (d_status) FZ_CK(cudaMemsetAsync(d_status, 0, ncol * sizeof(int), s));
   const int wpb = 4;
-  const size_t smc = (size_t)wpb * 2 * c->nz * sizeof(float);
   const dim3 gc((ncol + wpb - 1) / wpb);
   {
     ProfScope ps(c, 0, s);
     if (hydrostatic)
-      k_chem<true><<<gc, wpb * 32, smc, s>>>(c->d_params, c->d_consts, ncol, d_model, d_mout, c->d_slab, d_status);
+      k_chain<true><<<gc, wpb * 32, 0, s>>>(c->d_consts, ncol, c->nz, d_model, d_mout, c->d_chem, d_status);
     else
-      k_chem<false><<<gc, wpb * 32, smc, s>>>(c->d_params, c->d_consts, ncol, d_model, d_mout, c->d_slab, d_status);
+      k_chain<false><<<gc, wpb * 32, 0, s>>>(c->d_consts, ncol, c->nz, d_model, d_mout, c->d_chem, d_status);
+  }
+  FZ_CK(cudaGetLastError());
+  {
+    ProfScope ps(c, 1, s);
+    const size_t total = (size_t)ncol * c->nz;
+    const int blocks = (int)std::min<size_t>((total + 255) / 256, (size_t)c->nsm * 16);
+    k_opac<<<blocks, 256, 0, s>>>(c->d_params, c->d_consts, ncol, d_mout, c->d_chem, c->d_slab);
   }
   FZ_CK(cudaGetLastError());
   const int threads = (c->numw + 31) & ~31;
   const size_t sms = (size_t)c->nz * c->sw * sizeof(float);
   {
-    ProfScope ps(c, 1, s);
-    k_synth<<<ncol, threads, sms, s>>>(c->d_params, c->d_lam, c->d_gain, ncol, c->d_slab, d_syn, d_status);
+    ProfScope ps(c, 2, s);
+    k_synth<<<ncol, threads, sms, s>>>(c->d_params, c->d_lam, c->d_gain, ncol, c->d_slab, d_syn, d_mout, d_status);
   }
   FZ_CK(cudaGetLastError());
   return 0;
@@ -583,6 +736,8 @@ int fz_create(fz_ctx** out, const fz_line* lines, int nlines, const fz_region* r
   c->regs.assign(regs, regs + nreg);
   DevParams& P = c->hp;
   std::memset(&P, 0, sizeof(P));
+  Consts K;
+  host_consts(K);
   int numw = 0, nlu = 0, ncomp = 0;
   std::vector<LamP> lam;
   std::vector<double> lam_l;
@@ -597,22 +752,14 @@ int fz_create(fz_ctx** out, const fz_line* lines, int nlines, const fz_region* r
     P.reg_nb[r] = R.nblend;
     P.reg_lb[r] = nlu;
     const fz_line& main = lines[R.line[0]];
-    P.reg_l0[r] = main.l0;
+    P.cont[r] = host_cont(main.l0);
     for (int b = 0; b < R.nblend; ++b) {
       if (R.line[b] < 0 || R.line[b] >= nlines || nlu >= MAXLU) {
         delete c;
         return nlu >= MAXLU ? FZ_ERR_LIMIT : FZ_ERR_ARG;
       }
       const fz_line& L = lines[R.line[b]];
-      LineP& q = P.lu[nlu];
-      q.l0 = L.l0;
-      q.loggf = L.loggf;
-      q.eplow = L.eplow;
-      q.alpha = L.alpha;
-      q.sigma = L.sigma;
-      q.zn = L.zn;
-      q.ion = L.ion;
-      q.wdif = b == 0 ? 0.0 : R.wdif[b];
+      P.lu[nlu] = host_line(L, b == 0 ? 0.0 : R.wdif[b], K);
       std::vector<double> sh, stg;
       std::vector<int> ty;
       const int n = fzh_zeeman(L, sh, stg, ty);
@@ -647,6 +794,7 @@ int fz_create(fz_ctx** out, const fz_line* lines, int nlines, const fz_region* r
     delete c;
     return FZ_ERR_LIMIT;
   }
+  P.cont[nreg] = host_cont(5000.0);   // KC5 (src/forward.f90:926)
   c->numw = numw;
   c->nlu = nlu;
   c->sw = slab_w(nreg, nlu);
@@ -655,29 +803,13 @@ int fz_create(fz_ctx** out, const fz_line* lines, int nlines, const fz_region* r
   P.nreg = nreg;
   P.nlu = nlu;
   P.sw = c->sw;
-  Consts K;
-  host_consts(K);
-  {
-    static const double mat[FZ_NELEM] = {
-#include "fz_matom.inc"
-    };
-    static const double ab[FZ_NELEM] = {
-#include "fz_abund.inc"
-    };
-    for (int b = 0; b < nlu; ++b) {
-      P.lu[b].matom = mat[P.lu[b].zn - 1];
-      P.lu[b].abund = ab[P.lu[b].zn - 1];
-    }
-    P.matom_h = mat[0];
-    P.matom_he = mat[1];
-    P.abund_he = ab[1];
-  }
   int rc = 0;
   auto fail = [&](int code) {
     fz_destroy(c);
     return code;
   };
   if ((rc = cuda_fail(cudaSetDevice(device)))) return fail(rc);
+  cudaDeviceGetAttribute(&c->nsm, cudaDevAttrMultiProcessorCount, device);
   if ((rc = cuda_fail(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking)))) return fail(rc);
   if ((rc = cuda_fail(cudaMalloc(&c->d_params, sizeof(DevParams))))) return fail(rc);
   if ((rc = cuda_fail(cudaMalloc(&c->d_consts, sizeof(Consts))))) return fail(rc);
@@ -763,6 +895,7 @@ int fz_destroy(fz_ctx* c) {
   cudaFree(c->d_lam);
   cudaFree(c->d_gain);
   cudaFree(c->d_slab);
+  cudaFree(c->d_chem);
   cudaFree(c->d_model);
   cudaFree(c->d_syn);
   cudaFree(c->d_status);
@@ -793,13 +926,13 @@ int fz_profile_read(fz_ctx* c, double* ms, int* launches, int n) {
     cudaEventDestroy(p.b);
   }
   c->pending.clear();
-  for (int i = 0; i < n && i < 2; ++i) {
+  for (int i = 0; i < n && i < NKERN; ++i) {
     if (ms) ms[i] = c->prof_ms[i];
     if (launches) launches[i] = c->prof_n[i];
     c->prof_ms[i] = 0;
     c->prof_n[i] = 0;
   }
-  return 2;
+  return NKERN;
 }
 
 int fz_get_gain(fz_ctx* c, float* gain) {

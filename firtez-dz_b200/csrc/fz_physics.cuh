@@ -115,8 +115,14 @@ struct RhoOut {
 
 // GET_RHO, src/chemical_equilibrium.f90:165-278.  All lanes of the warp call
 // it with the same arguments; nelec (the warm-start chain) is updated in
-// every lane identically.
-__device__ RhoOut get_rho_warp(const WarpSaha& w, double PG, double& nelec, const Consts& K, int lane) {
+// every lane identically.  The electron sum of SHORT_ION_CALC_TEMPRHO
+// (:1659-1701), NELEC_EST = N_H+ - N_H- + sum_{Z>1} (N_II + N_III), is
+// evaluated per element as ab*(1+y)/(1+y+xy) (hydrogen: ab*(1-xy)/(1+y+xy))
+// with x = ne*alpha_I, y = ne*alpha_II: algebraically the reference's three
+// quotients, one division instead of five.  ab[j] = 10**(ABUND-12) of the
+// lane's elements (0 past element 92).
+__device__ RhoOut get_rho_warp(const WarpSaha& w, const double ab[3], double PG, double& nelec, const Consts& K,
+                               int lane) {
   RhoOut r;
   const double T = w.T;
   double nhyd = 0.0;
@@ -127,35 +133,21 @@ __device__ RhoOut get_rho_warp(const WarpSaha& w, double PG, double& nelec, cons
   double err = 1.0;
   int iter = 1;
   double nnew = nelec, nold = nelec;
+  const double kt = KBOL * T, dkt = K.deno_sa * KBOL * T;
   while (err > 1.0e-4 && iter <= 100 && nhyd >= 0.0) {
     nold = nnew;
-    const double nume = PG - nnew * KBOL * T;
-    nhyd = nume / (K.deno_sa * KBOL * T);
+    nhyd = (PG - nnew * kt) / dkt;
     const double ne = nnew;
-    double h = 0.0, s2 = 0.0, s3 = 0.0;
+    double s = 0.0;
 #pragma unroll
     for (int j = 0; j < 3; ++j) {
-      const int e = lane + 32 * j;
-      if (e < FZ_NELEM) {
-        const double vnt = nhyd * K.ab10[e];
-        const double na1 = ne * w.a1[j], na2 = ne * w.a2[j];
-        const double r2 = 1.0 / na2;
-        const double vnii = vnt / (na1 + 1.0 + r2);
-        const double vniii = vnt / (1.0 + na2 * (na1 + 1.0));
-        if (e == 0) {
-          const double vni = vnt / (1.0 + (1.0 / na1) * (1.0 + r2));
-          h = vniii - vni;
-        } else {
-          s2 += vnii;
-          s3 += vniii;
-        }
-      }
+      const double x = ne * w.a1[j], y = ne * w.a2[j];
+      const double xy = x * y;
+      const double num = (j == 0 && lane == 0) ? (1.0 - xy) : (1.0 + y);
+      s += ab[j] * num / (1.0 + y + xy);
     }
-    h = warp_sum(h);
-    s2 = warp_sum(s2);
-    s3 = warp_sum(s3);
-    double est = h;
-    est = est + s2 + s3;
+    s = warp_sum(s);
+    const double est = nhyd * s;
     nnew = (fmax(est, 0.0) + nold) / 2.0;
     err = fabs((nnew - nold) / nnew);
     iter = iter + 1;
@@ -175,177 +167,87 @@ __device__ RhoOut get_rho_warp(const WarpSaha& w, double PG, double& nelec, cons
 }
 
 // ----------------------------------------------------- continuum opacity
-__device__ double hminus_ff(double T, double ne, double l0) {
-  const double A1[6] = {0, 2483.346, -3449.889, 2200.04, -696.271, 88.283};
-  const double B1[6] = {0, 285.827, -1158.382, 2427.719, -1841.4, 444.517};
-  const double C1[6] = {0, -2054.291, 8746.523, -13651.105, 8624.97, -1863.864};
-  const double D1[6] = {0, 2827.776, -11485.632, 16755.524, -10051.53, 2095.288};
-  const double E1[6] = {0, -1341.537, 5303.609, -7510.494, 4400.067, -901.788};
-  const double F1[6] = {0, 208.952, -812.939, 1132.738, -655.02, 132.985};
-  const double A2[4] = {518.1021, 473.2636, -482.2089, 115.5291};
-  const double B2[4] = {-734.8666, 1443.4137, -737.1616, 169.6374};
-  const double C2[4] = {1021.1775, -1977.3395, 1096.8827, -245.649};
-  const double D2[4] = {-479.0721, 922.3575, -521.1341, 114.243};
-  const double E2[4] = {93.1373, -178.9275, 101.7963, -21.9972};
-  const double F2[4] = {-6.4285, 12.36, -7.0571, 1.5097};
-  const double lm = l0 / 1e4;
+// OPAC_CONTINUUM, src/cont_opacity.f90:305-357, with every factor that
+// depends only on the wavelength precomputed on the host (ContP):
+//   H- free-free  (:48-120):  1e-29 k ne T sum_i c_i theta^(1+i/2)
+//   H- bound-free (:124-181): T^-2.5 e^(a1/T) (1 - e^(-a2/T)) sigma ne k T
+//   Thomson (:187-217), Rayleigh (:221-239), neutral H bf/ff (:243-301).
+struct ContP {
+  int nff, n0, pad0, pad1;
+  double ffc[6];
+  double sbf, bfa1, bfa2;        // sigma_bf (0 if lambda >= 1.6419 um), ALPHA/LAMBDAP, ALPHA/lambda_um
+  double hpre, c3l, c4, ray;     // C2 lambda^3, C3/lambda, C4, Rayleigh
+  double ct;                     // Thomson constant
+};
+
+__device__ __forceinline__ double opac_continuum(double T, double ne, double nh, const ContP& c) {
   const double th = 5040.0 / T;
-  const double lm2 = pow(lm, 2.0), lm3 = pow(lm, 3.0), lm4 = pow(lm, 4.0);
-  double part1;
-  if (lm < 0.3645) {
-    double c[4];
-    for (int i = 0; i < 4; ++i) c[i] = A2[i] * lm2 + B2[i] + C2[i] / lm + D2[i] / lm2 + E2[i] / lm3 + F2[i] / lm4;
-    part1 = c[0] * th + c[1] * pow(th, 1.5) + c[2] * pow(th, 2.0) + c[3] * pow(th, 2.5);
-  } else {
-    double c[6];
-    for (int i = 0; i < 6; ++i) c[i] = A1[i] * lm2 + B1[i] + C1[i] / lm + D1[i] / lm2 + E1[i] / lm3 + F1[i] / lm4;
-    part1 = c[0] * th + c[1] * pow(th, 1.5) + c[2] * pow(th, 2.0) + c[3] * pow(th, 2.5) + c[4] * pow(th, 3.0) +
-            c[5] * pow(th, 3.5);
+  const double sq = sqrt(th);
+  const double th2 = th * th;
+  double part1 = c.ffc[0] * th + c.ffc[1] * th * sq + c.ffc[2] * th2 + c.ffc[3] * th2 * sq;
+  if (c.nff == 6) part1 += c.ffc[4] * th2 * th + c.ffc[5] * th2 * th * sq;
+  const double hmff = 1e-29 * part1 * KBOL * ne * T;
+  double hmbf = 0.0;
+  if (c.sbf != 0.0) {
+    const double part = (1.0 / (T * T * sqrt(T))) * exp(c.bfa1 / T) * (1.0 - exp(-c.bfa2 / T));
+    hmbf = part * c.sbf * ne * KBOL * T;
   }
-  return 1e-29 * part1 * KBOL * ne * T;
-}
-
-__device__ double hminus_bf(double T, double ne, double l0) {
-  const double LAMBDAP = 1.6419, CTE = 0.75e-18;
-  const double ALPHA = (HPLA * LIGHT / KBOL) * 1e4;
-  const double CC[6] = {152.519, 49.534, -118.858, 92.536, -34.194, 4.982};
-  const double lm = l0 / 1e4;
-  if (!(lm < LAMBDAP)) return 0.0;
-  const double com = 1.0 / lm - 1.0 / LAMBDAP;
-  double sigma = CC[0] + CC[1] * pow(com, 0.5) + CC[2] * com + CC[3] * pow(com, 1.5) + CC[4] * pow(com, 2.0) +
-                 CC[5] * pow(com, 2.5);
-  sigma = CTE * sigma * pow(lm, 3.0) * pow(com, 1.5);
-  const double part = pow(T, -2.5) * exp(ALPHA / (T * LAMBDAP)) * (1.0 - exp(-ALPHA / (T * lm)));
-  return part * sigma * ne * KBOL * T;
-}
-
-__device__ double opac_continuum(float Tsp, double l0, double ne, double nh) {
-  const double T = (double)Tsp;
-  // THOMSON, :187-217
-  const double CT = (8.0 * DPI / 3.0) * (pow(QELE / LIGHT, 4.0)) / pow(MELE, 2.0);
-  const double thom = CT * (ne / nh);
-  // RAYLEIGH_H, :221-239
-  const double ray = (5.799e-13 + (1.422e-6 + 2.784 / pow(l0, 2.0)) / pow(l0, 2.0)) / pow(l0, 4.0);
-  // HYDROGEN, :243-301 (REAL*4 literals 13.595 and 1E-8)
-  const double IOPOT = (double)13.595f;
-  const double E8 = (double)1e-8f;
-  const double C1 = E8 * IOPOT * EVOLT / (HPLA * LIGHT);
-  const double C2 = pow(E8, 3.0) * 64.0 * pow(DPI, 4.0) * MELE * pow(QELE, 10.0) /
-                    (3.0 * sqrt(3.0) * pow(LIGHT, 4.0) * pow(HPLA, 6.0));
-  const double C3 = HPLA * LIGHT / (KBOL * E8);
-  const double C4 = IOPOT * EVOLT / KBOL;
-  const int n0 = 1 + (int)floor(sqrt(C1 * l0));
+  const double thom = c.ct * (ne / nh);
   double sum;
-  if (n0 <= 8) {
-    sum = exp(C4 / (T * pow((double)n0, 2.0))) * pow((double)n0, -3.0);
-    for (int i = n0 + 1; i <= 8; ++i) sum = sum + exp(C4 / (T * pow((double)i, 2.0))) * pow((double)i, -3.0);
-    sum = sum + (0.117 + exp(C4 / (T * pow(9.0, 2.0)))) * (T / (2.0 * C4));
+  if (c.n0 <= 8) {
+    sum = 0.0;
+    for (int i = c.n0; i <= 8; ++i) {
+      const double di = (double)i;
+      sum += exp(c.c4 / (T * di * di)) / (di * di * di);
+    }
+    sum += (0.117 + exp(c.c4 / (T * 81.0))) * (T / (2.0 * c.c4));
   } else {
-    sum = (0.117 + exp(C4 / (T * pow((double)n0, 2.0)))) * (T / (2.0 * C4));
+    const double dn = (double)c.n0;
+    sum = (0.117 + exp(c.c4 / (T * dn * dn))) * (T / (2.0 * c.c4));
   }
-  const double hyd = C2 * sum * (1.0 - exp(-C3 / (T * l0))) * exp(-C4 / T) * pow(l0, 3.0);
-  const double factor = hminus_ff(T, ne, l0) + hminus_bf(T, ne, l0) + thom + ray + hyd;
-  return nh * factor;
+  const double hyd = c.hpre * sum * (1.0 - exp(-c.c3l / T)) * exp(-c.c4 / T);
+  return nh * (hmff + hmbf + thom + c.ray + hyd);
 }
 
 // ------------------------------------------------------ line opacity, damping
-struct LineP {   // one spectral line, FP64 constants
-  double l0, loggf, eplow, alpha, sigma, matom, abund, wdif;
+// Per-line constants precomputed on the host.
+struct LineP {
+  double l0, wdif;
+  double term1;      // TERM1 of OPAC_LINE, src/line_opacity.f90:95
+  double m2k;        // matom m_u / (2 k): TERM2 = sqrt(m2k / T)
+  double chik;       // EPLOW e / k:        TERM4 = exp(-chik / T)
+  double hclk;       // h c / (lambda k):   TERM5 = 1 - exp(-hclk / T)
+  double nab;        // 10**(ABUND-12)
+  double xi_k, xii_k;    // CSAHA2 * XI, XII of the element
+  double vdk;        // 2 k / (m_u matom): v_D = sqrt(vdk T)
+  double grad;       // radiative damping 0.2223 / lambda^2
+  double gc, ge;     // collisional: gamma_col = gc nH T^ge
+  double dfac;       // lambda / (4 pi)
   int zn, ion;
 };
 
-// ION_CALC_TEMPX (value), src/chemical_equilibrium.f90:1511-1597
-__device__ double ion_calc_tempx(int zn, int ion, double T, double ne, double n, const Consts& K, double* upi) {
+// OPAC_LINE (LTE) with ION_CALC_TEMPX, src/line_opacity.f90:34-108,
+// src/chemical_equilibrium.f90:1511-1597.
+__device__ __forceinline__ double opac_line(const LineP& L, double T, double ne, double nh, const Consts& K) {
   const double var[3] = {T, 1.0e-3 * T, log(5040.0 / T)};
   double U[3];
-  partition_u(zn, T, var, U);
-  const double lamelec = K.csaha1 * pow(T, -3.0 / 2.0);
-  const double e1 = exp(clamp650(K.csaha2 * fz_tab_xi[zn - 1] / T));
-  const double e2 = exp(clamp650(K.csaha2 * fz_tab_xii[zn - 1] / T));
-  const double al1 = (U[0] / (2.0 * U[1])) * lamelec * e1;
-  const double al2 = (U[1] / (2.0 * U[2])) * lamelec * e2;
-  const double deno = pow(ne, 2.0) * al1 * al2 + ne * al2 + 1.0;
-  double nume = 1.0;
-  if (ion == 1) nume = pow(ne, 2.0) * al1 * al2;
-  if (ion == 2) nume = ne * al2;
-  *upi = U[ion - 1];
-  return n * nume / deno;
+  partition_u(L.zn, T, var, U);
+  const double lamelec = K.csaha1 / (T * sqrt(T));
+  const double al1 = (U[0] / (2.0 * U[1])) * lamelec * exp(clamp650(L.xi_k / T));
+  const double al2 = (U[1] / (2.0 * U[2])) * lamelec * exp(clamp650(L.xii_k / T));
+  const double deno = ne * ne * al1 * al2 + ne * al2 + 1.0;
+  const double nume = L.ion == 1 ? ne * ne * al1 * al2 : (L.ion == 2 ? ne * al2 : 1.0);
+  const double npi = nh * L.nab * nume / deno;
+  const double t2 = sqrt(L.m2k / T);
+  const double t4 = exp(-L.chik / T);
+  const double t5 = 1.0 - exp(-L.hclk / T);
+  return L.term1 * t2 * (npi / U[L.ion - 1]) * t4 * t5;
 }
 
-// OPAC_LINE, src/line_opacity.f90:34-108 (LTE)
-__device__ double opac_line(const LineP& L, float Tsp, double ne, double nh, const Consts& K) {
-  const double T = (double)Tsp;
-  const double n = nh * pow(10.0, L.abund - 12.0);
-  double upi;
-  const double npi = ion_calc_tempx(L.zn, L.ion, T, ne, n, K, &upi);
-  const double t1 = sqrt(DPI) * pow(QELE, 2.0) / (MELE * LIGHT) * pow(10.0, L.loggf) * L.l0 * 1e-8;
-  const double t2 = sqrt(L.matom * MAMU / (2.0 * KBOL * T));
-  const double t3 = 1.0 * npi / upi;
-  const double t4 = exp(-L.eplow * EVOLT / (KBOL * T));
-  const double t5 = 1.0 - (1.0 / 1.0) * exp(-HPLA * LIGHT / (1.0e-8 * L.l0 * KBOL * T));
-  return t1 * t2 * t3 * t4 * t5;
-}
-
-// REFRAX, src/atom_database.f90:1039-1074
-__device__ double refrax(double w) {
-  const double T = 15.0, P = 760.0, H = 0.0;
-  const double s = 1.0 / pow(w, 2.0);
-  const double r = 6.4328e-5 + 2.94981e-2 / (146.0 - s) + 2.554e-4 / (41.0 - s);
-  const double y = 1.0 / (273.15 + T);
-  const double alpha = 3.67e-3 + 3.3e-4 * exp((0.19 - w) / 0.12);
-  const double wvsp =
-      pow(10.0, -55.1132754 +
-                    y * (1.19551822e5 +
-                         y * (-9.70108858e7 + y * (4.12856913e10 + y * (-9.87931835e12 + y * (1.25868645e15 - 6.66885272e16 * y))))));
-  const double wvp = 1.0e-2 * H * wvsp;
-  return 1.0 + 1.31579e-3 * r * P / (1.0 + alpha * (T - 1.0) / (1.0 + 15.0 * alpha)) - 5.49e-8 * wvp / (1.0 + alpha * T);
-}
-
-// GET_DAMPING, src/damping.f90:842-1012 (value)
-__device__ double get_damping(const LineP& L, double nhyd, float Tsp, const Consts& K, double matom_h,
-                              double matom_he, double abund_he) {
-  const double lambda = L.l0 * 1e-8;
-  const double T8 = (double)Tsp;
-  const double RAT = (double)0.3181818f;
-  const double m = L.matom;
-  const double vdop = sqrt(2.0 * KBOL * T8 / (MAMU * m));
-  const double grad = 0.2223 / pow(lambda, 2.0);
-  const double mu_h = MAMU * (m * matom_h) / (m + matom_h);
-  const double mu_he = MAMU * (m * matom_he) / (m + matom_he);
-  const double nhe = nhyd * pow(10.0, abund_he - 12.0);
-  double gcol;
-  if (L.sigma > 0 && L.alpha > 0) {
-    const double e1 = 2.0 - L.alpha / 2.0;
-    const double e2 = (1.0 - L.alpha) / 2.0;
-    const double gammaf =
-        1.0 + (-0.5748646 + (0.9512363 + (-0.6998588 + (0.4245549 - 0.1010678 * e1) * e1) * e1) * e1) * e1;
-    double beta = pow(4.0 / DPI, L.alpha / 2.0) * gammaf * pow(1e6, L.alpha) * (L.sigma * pow(K.rbohr, 2.0)) *
-                  pow(8.0 * KBOL / DPI, e2);
-    beta = 2.0 * beta;
-    gcol = beta * pow(T8, e2) * (nhyd * pow(mu_h, -e2) + RAT * nhe * pow(mu_he, -e2));
-  } else {
-    double rindex = (double)1.0004f;
-    if (lambda * 1e8 >= 1800.0) rindex = refrax(lambda * 1e4);
-    const double lvac = rindex * lambda;
-    const double epupp = L.eplow + (HPLA * LIGHT / lvac) / EVOLT;
-    const double xi = fz_tab_xi[L.zn - 1], xii = fz_tab_xii[L.zn - 1];
-    const double ionf = (double)(float)(L.ion - 1);
-    double ed1, ed2, chyd;
-    if (L.ion == 1) {
-      ed1 = fmax(xi - epupp - xi * ionf, 1.0);
-      ed2 = fmax(xi - L.eplow - xi * ionf, 3.0);
-      chyd = 1.0;
-    } else {
-      ed1 = fmax(xii - epupp - xi * ionf, 1.0);
-      ed2 = fmax(xii - L.eplow - xi * ionf, 3.0);
-      chyd = (double)1.741f;
-    }
-    chyd = chyd * 17.0 * pow(8.0 * KBOL / DPI, 0.3);
-    chyd = chyd * pow(pow(10.0, -30.5325) * (1.0 / pow(ed1, 2.0) - 1.0 / pow(ed2, 2.0)), 0.4);
-    const double chydp = chyd * (nhyd * pow(mu_h, -0.3) + nhe * pow(mu_he, -0.3));
-    gcol = chydp * pow(T8, 0.3);
-  }
-  return (grad + gcol) * lambda / (4.0 * DPI * vdop);
+// GET_DAMPING, src/damping.f90:842-1012: a = (gamma_rad + gamma_col) lambda / (4 pi v_D)
+__device__ __forceinline__ double get_damping(const LineP& L, double nh, double T) {
+  const double gcol = L.gc * nh * pow(T, L.ge);
+  return (L.grad + gcol) * L.dfac / sqrt(L.vdk * T);
 }
 
 // ------------------------------------------------------------ FP32 Voigt

@@ -108,7 +108,7 @@ int fz_forward_device(fz_ctx* ctx, int ncol, const float* d_model, int hydrostat
 /* Per-kernel timing: when enabled, every launch of the context is bracketed
  * by CUDA events on its stream; fz_profile_read returns the accumulated
  * milliseconds and launch counts of the kernels (names in order:
- * "k_chem", "k_synth") and resets them.  Replaces the reference's
+ * "k_chain", "k_opac", "k_synth") and resets them; returns the kernel count.  Replaces the reference's
  * SYSTEM_CLOCK "Forward 3D:" timer (src/forward.f90:99-100, :295-297). */
 int fz_profile_enable(fz_ctx* ctx, int on);
 int fz_profile_read(fz_ctx* ctx, double* ms, int* launches, int n);

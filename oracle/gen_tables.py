@@ -751,7 +751,7 @@ def write_header(path, XI, XII, ABUND, MATOM, vps, dps, abo, hsra):
         fh.write("\n".join(L) + "\n")
     # plain number lists for host-side initialisers
     d = os.path.dirname(path)
-    for nm, vals in (("fz_abund.inc", ABUND), ("fz_matom.inc", MATOM)):
+    for nm, vals in (("fz_abund.inc", ABUND), ("fz_matom.inc", MATOM), ("fz_xi.inc", XI), ("fz_xii.inc", XII)):
         with open(os.path.join(d, nm), "w") as fh:
             fh.write("// Generated by oracle/gen_tables.py (src/atom_database.f90 ATOM_INIT).\n")
             for i in range(0, len(vals), 6):
