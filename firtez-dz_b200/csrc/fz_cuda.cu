@@ -44,6 +44,7 @@ struct DevParams {
   ContP cont[MAXREG + 1];   // continuum constants of each region's main line, then 5000 A
   LineP lu[MAXLU];          // used lines in region order
   int lu_nc[MAXLU], lu_c0[MAXLU];
+  int lu_nt[MAXLU][3];      // components per type: sigma_red, pi, sigma_blue
   float comp_shift[MAXCOMP], comp_str[MAXCOMP];
   int comp_type[MAXCOMP];
 };
@@ -82,8 +83,9 @@ __device__ __forceinline__ void copy_to_shared(T* dst, const T* src) {
 // Writes per height (nH, ne) as FORWARD1D uses them, and rho, Pe, mu (and
 // Pg) into the output model.
 template <bool HE>
-__global__ void __launch_bounds__(128) k_chain(const Consts* __restrict__ Kg, int ncol, int nz, const float* model,
-                                               float* mout, double2* __restrict__ chem, int* __restrict__ status) {
+__global__ void __launch_bounds__(128) k_chain(const Consts* __restrict__ Kg, const PFTable* __restrict__ tb, int ncol,
+                                               int nz, const float* model, float* mout, double2* __restrict__ chem,
+                                               int* __restrict__ status) {
   __shared__ Consts K;
   copy_to_shared(&K, Kg);
   __syncthreads();
@@ -104,7 +106,7 @@ __global__ void __launch_bounds__(128) k_chain(const Consts* __restrict__ Kg, in
     double nelec = 0.0;
     WarpSaha w;
     for (int k = 0; k < nz; ++k) {
-      saha_prepare(w, (double)mget(m, nz, 0, k), K, lane);
+      saha_prepare(w, (double)mget(m, nz, 0, k), K, tb, lane);
       const RhoOut r = get_rho_warp(w, ab, (double)mget(m, nz, 1, k), nelec, K, lane);
       st |= r.status;
       if (lane == 0) {
@@ -120,7 +122,7 @@ __global__ void __launch_bounds__(128) k_chain(const Consts* __restrict__ Kg, in
     double t0 = (double)mget(m, nz, 12, top) * 1000.0 * 100.0;
     double u0 = log((double)mget(m, nz, 1, top));
     WarpSaha s0, sm, s1;
-    saha_prepare(s0, (double)mget(m, nz, 0, top), K, lane);
+    saha_prepare(s0, (double)mget(m, nz, 0, top), K, tb, lane);
     auto emit = [&](int k, double pg8, const RhoOut& r) {
       if (lane == 0) {
         const float pel = (float)r.pelec;
@@ -147,7 +149,7 @@ __global__ void __launch_bounds__(128) k_chain(const Consts* __restrict__ Kg, in
       const double it1 = t0 + dz / 2.0;
       const double iy1 = u0 + k1 / 2.0;
       const double tem = tm0 / dz * (t0 + dz - it1) + tm1 / dz * (it1 - t0);
-      saha_prepare(sm, tem, K, lane);
+      saha_prepare(sm, tem, K, tb, lane);
       q = get_rho_warp(sm, ab, exp(iy1), nelec, K, lane);
       st |= q.status;
       const double k2 = (-q.molecw * MAMU * GRAV / (KBOL * tem)) * dz;
@@ -156,7 +158,7 @@ __global__ void __launch_bounds__(128) k_chain(const Consts* __restrict__ Kg, in
       st |= q.status;
       const double k3 = (-q.molecw * MAMU * GRAV / (KBOL * tem)) * dz;
       const double iy3 = u0 + k3;
-      saha_prepare(s1, tm1, K, lane);
+      saha_prepare(s1, tm1, K, tb, lane);
       q = get_rho_warp(s1, ab, exp(iy3), nelec, K, lane);
       st |= q.status;
       const double k4 = (-q.molecw * MAMU * GRAV / (KBOL * tm1)) * dz;
@@ -298,23 +300,26 @@ __global__ void __launch_bounds__(MAXNUMW) k_synth(const DevParams* __restrict__
       const float kldz = q[0], a = q[1], idd = q[2];
       const float x0 = lp.wave + q[3];
       float h0 = 0.f, h1 = 0.f, h2 = 0.f, f0 = 0.f, f1 = 0.f, f2 = 0.f;
-      const int c0 = P.lu_c0[lb + b], nc = P.lu_nc[lb + b];
-      for (int c = c0; c < c0 + nc; ++c) {
-        const float u = (x0 + P.comp_shift[c] * B) * idd;
+      // components are stored sigma_red (dM=-1), pi, sigma_blue (dM=+1)
+      int c = P.lu_c0[lb + b];
+      const int e0 = c + P.lu_nt[lb + b][0], e1 = e0 + P.lu_nt[lb + b][1], e2 = e1 + P.lu_nt[lb + b][2];
+      for (; c < e0; ++c) {
         float h, f;
-        voigt_f32(a, u, h, f);
-        const float s = P.comp_str[c];
-        const int ty = P.comp_type[c];
-        if (ty < 0) {
-          h0 = fmaf(s, h, h0);
-          f0 = fmaf(s, f, f0);
-        } else if (ty == 0) {
-          h1 = fmaf(s, h, h1);
-          f1 = fmaf(s, f, f1);
-        } else {
-          h2 = fmaf(s, h, h2);
-          f2 = fmaf(s, f, f2);
-        }
+        voigt_f32(a, fmaf(P.comp_shift[c], B, x0) * idd, h, f);
+        h0 = fmaf(P.comp_str[c], h, h0);
+        f0 = fmaf(P.comp_str[c], f, f0);
+      }
+      for (; c < e1; ++c) {
+        float h, f;
+        voigt_f32(a, fmaf(P.comp_shift[c], B, x0) * idd, h, f);
+        h1 = fmaf(P.comp_str[c], h, h1);
+        f1 = fmaf(P.comp_str[c], f, f1);
+      }
+      for (; c < e2; ++c) {
+        float h, f;
+        voigt_f32(a, fmaf(P.comp_shift[c], B, x0) * idd, h, f);
+        h2 = fmaf(P.comp_str[c], h, h2);
+        f2 = fmaf(P.comp_str[c], f, f2);
       }
       const float hs = h0 + h2, fs = f0 + f2;
       const float hl = 0.5f * h1 - 0.25f * hs, fl = 0.5f * f1 - 0.25f * fs;
@@ -362,7 +367,7 @@ __global__ void __launch_bounds__(MAXNUMW) k_synth(const DevParams* __restrict__
 // thread integrates its wavelengths through the continuum-only atmosphere
 // with the reference's REAL*4 rounding of the intermediate intensities.
 __global__ void k_gain(const DevParams* __restrict__ Pg, const Consts* __restrict__ Kg,
-                       const double* __restrict__ lam_l /* (numw) full wavelength [A] */, float* gain,
+                       const PFTable* __restrict__ tb, const double* __restrict__ lam_l /* (numw) [A] */, float* gain,
                        int* status) {
   extern __shared__ double sm_gain[];   // (387 x nreg) continuum opacities
   const DevParams& P = *Pg;
@@ -377,7 +382,7 @@ __global__ void k_gain(const DevParams* __restrict__ Pg, const Consts* __restric
     int st = 0;
     for (int k = 0; k < N; ++k) {
       const double T = (double)fz_tab_hsra_tem[k];
-      saha_prepare(w, T, K, lane);
+      saha_prepare(w, T, K, tb, lane);
       const RhoOut r = get_rho_warp(w, ab, (double)fz_tab_hsra_pg[k], nelec, K, lane);
       st |= r.status;
       if (lane < P.nreg) sm_gain[k * P.nreg + lane] = opac_continuum(T, nelec, r.nhyd, P.cont[lane]);
@@ -596,6 +601,7 @@ struct fz_ctx {
   DevParams hp{};
   DevParams* d_params = nullptr;
   Consts* d_consts = nullptr;
+  PFTable* d_pf = nullptr;
   LamP* d_lam = nullptr;
   float* d_gain = nullptr;
   // scratch (grown on demand): per (column, height) nH, ne and the opacity slab
@@ -676,9 +682,9 @@ int launch_forward(fz_ctx* c, int ncol, const float* d_model, int hydrostatic, d
   {
     ProfScope ps(c, 0, s);
     if (hydrostatic)
-      k_chain<true><<<gc, wpb * 32, 0, s>>>(c->d_consts, ncol, c->nz, d_model, d_mout, c->d_chem, d_status);
+      k_chain<true><<<gc, wpb * 32, 0, s>>>(c->d_consts, c->d_pf, ncol, c->nz, d_model, d_mout, c->d_chem, d_status);
     else
-      k_chain<false><<<gc, wpb * 32, 0, s>>>(c->d_consts, ncol, c->nz, d_model, d_mout, c->d_chem, d_status);
+      k_chain<false><<<gc, wpb * 32, 0, s>>>(c->d_consts, c->d_pf, ncol, c->nz, d_model, d_mout, c->d_chem, d_status);
   }
   FZ_CK(cudaGetLastError());
   {
@@ -769,10 +775,17 @@ int fz_create(fz_ctx** out, const fz_line* lines, int nlines, const fz_region* r
       }
       P.lu_c0[nlu] = ncomp;
       P.lu_nc[nlu] = n;
-      for (int i = 0; i < n; ++i) {
-        P.comp_shift[ncomp + i] = (float)sh[i];
-        P.comp_str[ncomp + i] = (float)stg[i];
-        P.comp_type[ncomp + i] = ty[i];
+      int at = ncomp;
+      for (int t = -1; t <= 1; ++t) {   // group by type (ZEEMAN_COMP order kept within a type)
+        P.lu_nt[nlu][t + 1] = 0;
+        for (int i = 0; i < n; ++i)
+          if (ty[i] == t) {
+            P.comp_shift[at] = (float)sh[i];
+            P.comp_str[at] = (float)stg[i];
+            P.comp_type[at] = t;
+            ++at;
+            ++P.lu_nt[nlu][t + 1];
+          }
       }
       ncomp += n;
       ++nlu;
@@ -813,6 +826,12 @@ int fz_create(fz_ctx** out, const fz_line* lines, int nlines, const fz_region* r
   if ((rc = cuda_fail(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking)))) return fail(rc);
   if ((rc = cuda_fail(cudaMalloc(&c->d_params, sizeof(DevParams))))) return fail(rc);
   if ((rc = cuda_fail(cudaMalloc(&c->d_consts, sizeof(Consts))))) return fail(rc);
+  if ((rc = cuda_fail(cudaMalloc(&c->d_pf, sizeof(PFTable))))) return fail(rc);
+  {
+    std::vector<char> buf(sizeof(PFTable));
+    fzh_pf_table(reinterpret_cast<PFTable*>(buf.data()));
+    if ((rc = cuda_fail(cudaMemcpy(c->d_pf, buf.data(), sizeof(PFTable), cudaMemcpyHostToDevice)))) return fail(rc);
+  }
   if ((rc = cuda_fail(cudaMalloc(&c->d_lam, numw * sizeof(LamP))))) return fail(rc);
   if ((rc = cuda_fail(cudaMalloc(&c->d_gain, 4 * numw * sizeof(float))))) return fail(rc);
   if ((rc = cuda_fail(cudaMemcpy(c->d_params, &P, sizeof(P), cudaMemcpyHostToDevice)))) return fail(rc);
@@ -833,8 +852,8 @@ int fz_create(fz_ctx** out, const fz_line* lines, int nlines, const fz_region* r
       return fail(rc);
     }
     cudaMemcpy(d_l, lam_l.data(), numw * sizeof(double), cudaMemcpyHostToDevice);
-    k_gain<<<1, 256, FZ_HSRA_LEN * nreg * sizeof(double), c->stream>>>(c->d_params, c->d_consts, d_l, c->d_gain,
-                                                                        d_st);
+    k_gain<<<1, 256, FZ_HSRA_LEN * nreg * sizeof(double), c->stream>>>(c->d_params, c->d_consts, c->d_pf, d_l,
+                                                                        c->d_gain, d_st);
     rc = cuda_fail(cudaGetLastError());
     if (!rc) rc = cuda_fail(cudaStreamSynchronize(c->stream));
     int st = 0;
@@ -892,6 +911,7 @@ int fz_destroy(fz_ctx* c) {
   if (c->stream) cudaStreamSynchronize(c->stream);
   cudaFree(c->d_params);
   cudaFree(c->d_consts);
+  cudaFree(c->d_pf);
   cudaFree(c->d_lam);
   cudaFree(c->d_gain);
   cudaFree(c->d_slab);

@@ -10,6 +10,7 @@
 
 #include "fz_host.h"
 #include "fz_tables.h"
+#include "fz_pftable.h"
 
 namespace {
 
@@ -222,4 +223,23 @@ int fzh_zeeman(const fz_line& ln, std::vector<double>& shift, std::vector<double
   for (size_t i = 0; i < type.size(); ++i) sum[type[i] + 1] += strength[i];
   for (size_t i = 0; i < type.size(); ++i) strength[i] /= sum[type[i] + 1];
   return (int)type.size();
+}
+
+void fzh_pf_table(PFTable* t) {
+  std::memset(t, 0, sizeof(*t));
+  for (int e = 0; e < FZ_NELEM; ++e)
+    for (int s = 0; s < 3; ++s) {
+      t->nv[e][s] = fz_tab_pf_nv[e][s];
+      for (int i = 0; i < fz_tab_pf_nv[e][s]; ++i) {
+        const fz_pf_vpiece& v = fz_tab_pf_v[e][s][i];
+        PFPiece& p = t->p[e][s][i];
+        for (int k = 0; k < v.nc && k < 6; ++k) p.c[k] = v.c[k];
+        p.th = v.th;
+        p.base = v.base;
+        p.clamp = v.clamp;
+        p.cond = v.cond;
+        p.form = v.form;
+        p.var = v.var;
+      }
+    }
 }

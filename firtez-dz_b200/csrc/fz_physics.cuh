@@ -14,6 +14,7 @@
 
 #define FZ_TABLE_QUAL static __device__ const
 #include "fz_tables.h"
+#include "fz_pftable.h"
 
 namespace fzd {
 
@@ -48,6 +49,46 @@ __device__ __forceinline__ bool pf_cond(int cond, double th, double T, double u)
          (cond == 4 && T >= th) || (cond == 5 && u != th);
 }
 
+__device__ __forceinline__ double horner6(const double* c, double x) {
+  double r = c[5];
+  r = __dadd_rn(c[4], __dmul_rn(x, r));
+  r = __dadd_rn(c[3], __dmul_rn(x, r));
+  r = __dadd_rn(c[2], __dmul_rn(x, r));
+  r = __dadd_rn(c[1], __dmul_rn(x, r));
+  r = __dadd_rn(c[0], __dmul_rn(x, r));
+  return r;
+}
+
+// U of one (element, stage) without divergent branches: the active piece
+// (the last whose condition holds) is selected by predication, then one
+// Horner evaluation and one exponential (used only by exp forms).
+__device__ __forceinline__ double pf_stage(const PFTable* __restrict__ tb, int e, int s, double T,
+                                           const double var[3]) {
+  const int nv = tb->nv[e][s];
+  int act = 0;
+#pragma unroll
+  for (int i = 1; i < FZ_PF_MAXV; ++i) {
+    const int cond = __ldg(&tb->p[e][s][i].cond);
+    const double th = __ldg(&tb->p[e][s][i].th);
+    const bool ok = (cond == 1 && T > th) || (cond == 2 && T < th) || (cond == 3 && T <= th) || (cond == 4 && T >= th);
+    act = (i < nv && ok) ? i : act;
+  }
+  const PFPiece* p = &tb->p[e][s][act];
+  double c[6];
+#pragma unroll
+  for (int i = 0; i < 6; ++i) c[i] = __ldg(&p->c[i]);
+  const int form = __ldg(&p->form), v = __ldg(&p->var);
+  const double x = v == 0 ? var[0] : (v == 1 ? var[1] : var[2]);
+  const double h = horner6(c, x);
+  const double ex = exp(h);
+  double u = h;
+  u = form == 1 ? __ldg(&p->base) + ex : u;
+  u = form == 2 ? fmax(__ldg(&p->clamp), h) : u;
+  return nv > 0 ? u : 0.0;
+}
+
+// U_I, U_II, U_III of element zn (1-based), src/atom_database.f90:121-1035
+// (generated piece table; branchy, used outside the warp chemistry).
 __device__ __forceinline__ double pf_vpiece(const fz_pf_vpiece& p, const double var[3]) {
   const double h = horner_exact(p.c, p.nc, var[p.var]);
   if (p.form == 1) return p.base + exp(h);
@@ -55,7 +96,6 @@ __device__ __forceinline__ double pf_vpiece(const fz_pf_vpiece& p, const double 
   return h;
 }
 
-// U_I, U_II, U_III of element zn (1-based), src/atom_database.f90:121-1035.
 __device__ __forceinline__ void partition_u(int zn, double T, const double var[3], double U[3]) {
   const int e = zn - 1;
 #pragma unroll
@@ -66,6 +106,16 @@ __device__ __forceinline__ void partition_u(int zn, double T, const double var[3
       if (pf_cond(fz_tab_pf_v[e][s][i].cond, fz_tab_pf_v[e][s][i].th, T, 0.0)) act = i;
     U[s] = act >= 0 ? pf_vpiece(fz_tab_pf_v[e][s][act], var) : 0.0;
   }
+}
+
+// 1/y to ~1 ulp: hardware approximation refined by two Newton steps.
+__device__ __forceinline__ double rcp_d(double y) {
+  double r;
+  asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(r) : "d"(y));
+  double e = fma(-y, r, 1.0);
+  r = fma(r, e, r);
+  e = fma(-y, r, 1.0);
+  return fma(r, e, r);
 }
 
 // --------------------------------------------------------- warp chemistry
@@ -82,23 +132,24 @@ __device__ __forceinline__ double clamp650(double e) {
   return e;
 }
 
-__device__ void saha_prepare(WarpSaha& w, double T, const Consts& K, int lane) {
+__device__ __noinline__ void saha_prepare(WarpSaha& w, double T, const Consts& K, const PFTable* __restrict__ tb,
+                                         int lane) {
+  // SHORT_PRE_ION_CALC_TEMPRHO, src/chemical_equilibrium.f90:1601-1652
   w.T = T;
   const double lamelec = K.csaha1 * pow(T, -3.0 / 2.0);
   const double var[3] = {T, 1.0e-3 * T, log(5040.0 / T)};
+  const double it = 1.0 / T;
 #pragma unroll
   for (int j = 0; j < 3; ++j) {
-    const int e = lane + 32 * j;
-    w.a1[j] = 0.0;
-    w.a2[j] = 0.0;
-    if (e < FZ_NELEM) {
-      double U[3];
-      partition_u(e + 1, T, var, U);
-      const double e1 = exp(clamp650(K.csaha2 * fz_tab_xi[e] / T));
-      const double e2 = exp(clamp650(K.csaha2 * fz_tab_xii[e] / T));
-      w.a1[j] = (U[0] / (2.0 * U[1])) * lamelec * e1;
-      w.a2[j] = (U[1] / (2.0 * U[2])) * lamelec * e2;
-    }
+    const int e = min(lane + 32 * j, FZ_NELEM - 1);
+    const double u0 = pf_stage(tb, e, 0, T, var);
+    const double u1 = pf_stage(tb, e, 1, T, var);
+    const double u2 = pf_stage(tb, e, 2, T, var);
+    const double e1 = exp(clamp650(K.csaha2 * fz_tab_xi[e] * it));
+    const double e2 = exp(clamp650(K.csaha2 * fz_tab_xii[e] * it));
+    const bool on = lane + 32 * j < FZ_NELEM;
+    w.a1[j] = on ? (u0 / (2.0 * u1)) * lamelec * e1 : 0.0;
+    w.a2[j] = on ? (u1 / (2.0 * u2)) * lamelec * e2 : 0.0;
   }
 }
 
@@ -121,8 +172,8 @@ struct RhoOut {
 // with x = ne*alpha_I, y = ne*alpha_II: algebraically the reference's three
 // quotients, one division instead of five.  ab[j] = 10**(ABUND-12) of the
 // lane's elements (0 past element 92).
-__device__ RhoOut get_rho_warp(const WarpSaha& w, const double ab[3], double PG, double& nelec, const Consts& K,
-                               int lane) {
+__device__ __noinline__ RhoOut get_rho_warp(const WarpSaha& w, const double ab[3], double PG, double& nelec,
+                                            const Consts& K, int lane) {
   RhoOut r;
   const double T = w.T;
   double nhyd = 0.0;
@@ -144,7 +195,7 @@ __device__ RhoOut get_rho_warp(const WarpSaha& w, const double ab[3], double PG,
       const double x = ne * w.a1[j], y = ne * w.a2[j];
       const double xy = x * y;
       const double num = (j == 0 && lane == 0) ? (1.0 - xy) : (1.0 + y);
-      s += ab[j] * num / (1.0 + y + xy);
+      s = fma(ab[j] * num, rcp_d(1.0 + y + xy), s);
     }
     s = warp_sum(s);
     const double est = nhyd * s;
@@ -253,7 +304,11 @@ __device__ __forceinline__ double get_damping(const LineP& L, double nh, double 
 // ------------------------------------------------------------ FP32 Voigt
 // Hui, Armstrong & Wray (1978) 7-pole rational approximation of the complex
 // probability function, as src/voigt.f:17-98: H = Re w, F = sign(v) Im w
-// with w evaluated at z = a - i|v|.  Division by range reduction (Smith).
+// with w = P(z)/Q(z) at z = a - i|v|.  P (degree 6) and Q (monic, degree 7)
+// have real coefficients, so each is reduced modulo the real quadratic
+// (z^2 - 2 Re z z + |z|^2) that z solves (Knuth, TAOCP vol. 2, 4.6.4):
+// 2 FMA per degree instead of a complex multiply-add.  The quotient is
+// formed with range reduction (Smith), written without branches.
 __device__ __forceinline__ void voigt_f32(float a, float u, float& H, float& F) {
   const float A0 = 122.607931777104326f, A1 = 214.382388694706425f, A2 = 181.928533092181549f,
               A3 = 93.155580458138441f, A4 = 30.180142196210589f, A5 = 5.912626209773153f,
@@ -261,37 +316,28 @@ __device__ __forceinline__ void voigt_f32(float a, float u, float& H, float& F) 
               B2 = 457.334478783897737f, B3 = 348.703917719495792f, B4 = 170.354001821091472f,
               B5 = 53.992906912940207f, B6 = 10.479857114260399f;
   const float v = fabsf(u);
-  const float zr = a, zi = -v;
-  // numerator
-  float nr = fmaf(A6, zr, A5), ni = A6 * zi;
-  float tr, ti;
-#define FZ_CSTEP(C)                        \
-  tr = fmaf(nr, zr, -ni * zi) + (C);       \
-  ti = fmaf(nr, zi, ni * zr);              \
-  nr = tr;                                 \
-  ni = ti;
-  FZ_CSTEP(A4) FZ_CSTEP(A3) FZ_CSTEP(A2) FZ_CSTEP(A1) FZ_CSTEP(A0)
-  float dr = zr + B6, di = zi;
-#define FZ_DSTEP(C)                        \
-  tr = fmaf(dr, zr, -di * zi) + (C);       \
-  ti = fmaf(dr, zi, di * zr);              \
-  dr = tr;                                 \
-  di = ti;
-  FZ_DSTEP(B5) FZ_DSTEP(B4) FZ_DSTEP(B3) FZ_DSTEP(B2) FZ_DSTEP(B1) FZ_DSTEP(B0)
-#undef FZ_CSTEP
-#undef FZ_DSTEP
-  float wr, wi;
-  if (fabsf(dr) >= fabsf(di)) {
-    const float r = __fdividef(di, dr);
-    const float den = __frcp_rn(fmaf(di, r, dr));
-    wr = fmaf(ni, r, nr) * den;
-    wi = fmaf(-nr, r, ni) * den;
-  } else {
-    const float r = __fdividef(dr, di);
-    const float den = __frcp_rn(fmaf(dr, r, di));
-    wr = fmaf(nr, r, ni) * den;
-    wi = fmaf(ni, r, -nr) * den;
-  }
+  const float x = a, y = -v;
+  const float r = 2.0f * x, s = fmaf(x, x, v * v);
+  float p1 = A6, p0 = A5, t;
+#define FZ_KSTEP(C, hi, lo) \
+  t = hi;                   \
+  hi = fmaf(r, t, lo);      \
+  lo = fmaf(-s, t, (C));
+  FZ_KSTEP(A4, p1, p0) FZ_KSTEP(A3, p1, p0) FZ_KSTEP(A2, p1, p0) FZ_KSTEP(A1, p1, p0) FZ_KSTEP(A0, p1, p0)
+  float q1 = 1.0f, q0 = B6;
+  FZ_KSTEP(B5, q1, q0) FZ_KSTEP(B4, q1, q0) FZ_KSTEP(B3, q1, q0) FZ_KSTEP(B2, q1, q0) FZ_KSTEP(B1, q1, q0)
+  FZ_KSTEP(B0, q1, q0)
+#undef FZ_KSTEP
+  // P = p1 z + p0, Q = q1 z + q0
+  const float nr = fmaf(p1, x, p0), ni = p1 * y;
+  const float dr = fmaf(q1, x, q0), di = q1 * y;
+  const bool big = fabsf(dr) >= fabsf(di);
+  const float A = big ? dr : di, Bq = big ? di : dr;
+  const float X = big ? nr : ni, Y = big ? ni : nr;
+  const float rr = __fdividef(Bq, A);
+  const float den = __frcp_rn(fmaf(Bq, rr, A));
+  const float wr = fmaf(Y, rr, X) * den;
+  const float wi = (big ? 1.0f : -1.0f) * fmaf(-X, rr, Y) * den;
   H = wr;
   F = (u < 0.0f) ? -wi : wi;
 }
