@@ -100,7 +100,7 @@ __global__ void __launch_bounds__(128) k_chain(const Consts* __restrict__ Kg, co
   __syncwarp();
   double ab[3];
 #pragma unroll
-  for (int j = 0; j < 3; ++j) ab[j] = (lane + 32 * j < FZ_NELEM) ? K.ab10[lane + 32 * j] : 0.0;
+  for (int j = 0; j < 3; ++j) ab[j] = K.lane_elem[32 * j + lane] >= 0 ? K.ab10[K.lane_elem[32 * j + lane]] : 0.0;
   int st = 0;
   if (!HE) {
     double nelec = 0.0;
@@ -376,7 +376,7 @@ __global__ void k_gain(const DevParams* __restrict__ Pg, const Consts* __restric
   if (threadIdx.x < 32) {
     const int lane = threadIdx.x;
     double ab[3];
-    for (int j = 0; j < 3; ++j) ab[j] = (lane + 32 * j < FZ_NELEM) ? K.ab10[lane + 32 * j] : 0.0;
+    for (int j = 0; j < 3; ++j) ab[j] = K.lane_elem[32 * j + lane] >= 0 ? K.ab10[K.lane_elem[32 * j + lane]] : 0.0;
     double nelec = 0.0;
     WarpSaha w;
     int st = 0;
@@ -463,6 +463,19 @@ void host_consts(Consts& K) {
     K.deno_sa = K.deno_sa + K.ab10[i];
   }
   for (int i = 0; i < FZ_NELEM; ++i) K.deno_sam = K.deno_sam + MAMU * kMatom[i] * K.ab10[i];
+  // lane/slot assignment of the elements: exponential-form elements first
+  std::vector<int> order;
+  PFTable* t = new PFTable;
+  fzh_pf_table(t);
+  for (int pass = 0; pass < 2; ++pass)
+    for (int e = 0; e < FZ_NELEM; ++e) {
+      bool ex = false;
+      for (int s = 0; s < 3; ++s)
+        for (int i = 0; i < t->nv[e][s]; ++i) ex = ex || t->p[e][s][i].form == 1;
+      if (ex == (pass == 0)) order.push_back(e);
+    }
+  delete t;
+  for (int i = 0; i < 96; ++i) K.lane_elem[i] = i < (int)order.size() ? order[i] : -1;
 }
 
 // Wavelength-only factors of OPAC_CONTINUUM at lambda0 [A], src/cont_opacity.f90:48-357.

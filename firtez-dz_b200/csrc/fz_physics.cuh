@@ -22,6 +22,10 @@ namespace fzd {
 struct Consts {
   double csaha1, csaha2, rbohr, deno_sa, deno_sam;
   double ab10[FZ_NELEM];   // 10**(ABUND-12)
+  // element handled by lane l in slot j of the warp chemistry: lane_elem[32*j+l]
+  // (-1 = idle).  Slot 0 holds every element whose partition function has an
+  // exponential piece, so slots 1 and 2 never evaluate one.
+  int lane_elem[96];
 };
 
 constexpr double DPI = 3.141592653589793238462643;
@@ -62,6 +66,7 @@ __device__ __forceinline__ double horner6(const double* c, double x) {
 // U of one (element, stage) without divergent branches: the active piece
 // (the last whose condition holds) is selected by predication, then one
 // Horner evaluation and one exponential (used only by exp forms).
+template <bool EXPF>
 __device__ __forceinline__ double pf_stage(const PFTable* __restrict__ tb, int e, int s, double T,
                                            const double var[3]) {
   const int nv = tb->nv[e][s];
@@ -80,9 +85,8 @@ __device__ __forceinline__ double pf_stage(const PFTable* __restrict__ tb, int e
   const int form = __ldg(&p->form), v = __ldg(&p->var);
   const double x = v == 0 ? var[0] : (v == 1 ? var[1] : var[2]);
   const double h = horner6(c, x);
-  const double ex = exp(h);
   double u = h;
-  u = form == 1 ? __ldg(&p->base) + ex : u;
+  if (EXPF) u = form == 1 ? __ldg(&p->base) + exp(h) : u;
   u = form == 2 ? fmax(__ldg(&p->clamp), h) : u;
   return nv > 0 ? u : 0.0;
 }
@@ -138,18 +142,25 @@ __device__ __noinline__ void saha_prepare(WarpSaha& w, double T, const Consts& K
   w.T = T;
   const double lamelec = K.csaha1 * pow(T, -3.0 / 2.0);
   const double var[3] = {T, 1.0e-3 * T, log(5040.0 / T)};
-  const double it = 1.0 / T;
+  const double it = rcp_d(T);
 #pragma unroll
   for (int j = 0; j < 3; ++j) {
-    const int e = min(lane + 32 * j, FZ_NELEM - 1);
-    const double u0 = pf_stage(tb, e, 0, T, var);
-    const double u1 = pf_stage(tb, e, 1, T, var);
-    const double u2 = pf_stage(tb, e, 2, T, var);
+    const int el = K.lane_elem[32 * j + lane];
+    const int e = el < 0 ? 0 : el;
+    double u0, u1, u2;
+    if (j == 0) {
+      u0 = pf_stage<true>(tb, e, 0, T, var);
+      u1 = pf_stage<true>(tb, e, 1, T, var);
+      u2 = pf_stage<true>(tb, e, 2, T, var);
+    } else {
+      u0 = pf_stage<false>(tb, e, 0, T, var);
+      u1 = pf_stage<false>(tb, e, 1, T, var);
+      u2 = pf_stage<false>(tb, e, 2, T, var);
+    }
     const double e1 = exp(clamp650(K.csaha2 * fz_tab_xi[e] * it));
     const double e2 = exp(clamp650(K.csaha2 * fz_tab_xii[e] * it));
-    const bool on = lane + 32 * j < FZ_NELEM;
-    w.a1[j] = on ? (u0 / (2.0 * u1)) * lamelec * e1 : 0.0;
-    w.a2[j] = on ? (u1 / (2.0 * u2)) * lamelec * e2 : 0.0;
+    w.a1[j] = el >= 0 ? (u0 * (0.5 * rcp_d(u1))) * lamelec * e1 : 0.0;
+    w.a2[j] = el >= 0 ? (u1 * (0.5 * rcp_d(u2))) * lamelec * e2 : 0.0;
   }
 }
 
@@ -181,35 +192,35 @@ __device__ __noinline__ RhoOut get_rho_warp(const WarpSaha& w, const double ab[3
   if (nelec < 1.0) nelec = PG / (101.0 * KBOL * T);
   const double pelec = nelec * KBOL * T;
   if (pelec > PG) nelec = (PG * 0.5) / (KBOL * T);
-  double err = 1.0;
   int iter = 1;
   double nnew = nelec, nold = nelec;
-  const double kt = KBOL * T, dkt = K.deno_sa * KBOL * T;
-  while (err > 1.0e-4 && iter <= 100 && nhyd >= 0.0) {
+  const double kt = KBOL * T, idkt = rcp_d(K.deno_sa * KBOL * T);
+  bool go = true;
+  while (go) {
     nold = nnew;
-    nhyd = (PG - nnew * kt) / dkt;
+    nhyd = (PG - nnew * kt) * idkt;
     const double ne = nnew;
     double s = 0.0;
 #pragma unroll
     for (int j = 0; j < 3; ++j) {
       const double x = ne * w.a1[j], y = ne * w.a2[j];
       const double xy = x * y;
-      const double num = (j == 0 && lane == 0) ? (1.0 - xy) : (1.0 + y);
+      const double num = (K.lane_elem[32 * j + lane] == 0) ? (1.0 - xy) : (1.0 + y);   // hydrogen: N_H+ - N_H-
       s = fma(ab[j] * num, rcp_d(1.0 + y + xy), s);
     }
     s = warp_sum(s);
     const double est = nhyd * s;
-    nnew = (fmax(est, 0.0) + nold) / 2.0;
-    err = fabs((nnew - nold) / nnew);
+    nnew = (fmax(est, 0.0) + nold) * 0.5;
     iter = iter + 1;
+    // ERROR = |(NEW-OLD)/NEW| > 1e-4, ITER <= 100, NHYD >= 0
+    go = fabs(nnew - nold) > 1.0e-4 * fabs(nnew) && iter <= 100 && nhyd >= 0.0;
   }
   r.status = 0;
   if (iter >= 100 || nhyd < 0.0) r.status = 1;
   nelec = nnew;
-  const double nume = PG - nelec * KBOL * T;
-  nhyd = nume / (K.deno_sa * KBOL * T);
+  nhyd = (PG - nelec * KBOL * T) * idkt;
   r.dens = nhyd * K.deno_sam + nelec * MELE;
-  r.molecw = ((r.dens * KBOL * T) / MAMU) * (1.0 / PG);
+  r.molecw = ((r.dens * KBOL * T) * (1.0 / MAMU)) * rcp_d(PG);
   if (nhyd != nhyd || nnew != nnew) r.status = 2;
   if (nelec < 0.0 || nhyd <= 0.0) r.status = 1;
   r.nhyd = nhyd;
