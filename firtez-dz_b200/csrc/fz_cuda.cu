@@ -83,7 +83,7 @@ __device__ __forceinline__ void copy_to_shared(T* dst, const T* src) {
 // Writes per height (nH, ne) as FORWARD1D uses them, and rho, Pe, mu (and
 // Pg) into the output model.
 template <bool HE>
-__global__ void __launch_bounds__(128) k_chain(const Consts* __restrict__ Kg, const PFTable* __restrict__ tb, int ncol,
+__global__ void __launch_bounds__(128, 8) k_chain(const Consts* __restrict__ Kg, const PFTable* __restrict__ tb, int ncol,
                                                int nz, const float* model, float* mout, double2* __restrict__ chem,
                                                int* __restrict__ status) {
   __shared__ Consts K;
@@ -121,54 +121,57 @@ __global__ void __launch_bounds__(128) k_chain(const Consts* __restrict__ Kg, co
     double nelec = (double)mget(m, nz, 3, top) / KBOL / (double)mget(m, nz, 0, top);
     double t0 = (double)mget(m, nz, 12, top) * 1000.0 * 100.0;
     double u0 = log((double)mget(m, nz, 1, top));
-    WarpSaha s0, sm, s1;
-    saha_prepare(s0, (double)mget(m, nz, 0, top), K, tb, lane);
-    auto emit = [&](int k, double pg8, const RhoOut& r) {
+    // One Saha buffer serves the whole integration: within a step the RK4
+    // stages need T(k+1) (stage 1), the linear midpoint (stages 2, 3) and
+    // T(k) (stage 4 and the final GET_RHO), and T(k) is the next step's T(k+1).
+    WarpSaha w;
+    saha_prepare(w, (double)mget(m, nz, 0, top), K, tb, lane);
+    {
+      const RhoOut r = get_rho_warp(w, ab, exp(u0), nelec, K, lane);
+      st |= r.status;
       if (lane == 0) {
         const float pel = (float)r.pelec;
-        mo[1 * nz + k] = (float)exp(pg8);
-        mo[2 * nz + k] = (float)r.dens;
-        mo[3 * nz + k] = pel;
-        mo[4 * nz + k] = (float)r.molecw;
-        // FORWARD1D uses NELEC = PEL/KBOL/TEM from the REAL*4 model (src/forward.f90:900)
-        ch[k] = make_double2(r.nhyd, (double)pel / KBOL / (double)mget(m, nz, 0, k));
+        mo[1 * nz + top] = (float)exp(u0);
+        mo[2 * nz + top] = (float)r.dens;
+        mo[3 * nz + top] = pel;
+        mo[4 * nz + top] = (float)r.molecw;
+        ch[top] = make_double2(r.nhyd, (double)pel / KBOL / (double)mget(m, nz, 0, top));
       }
-    };
-    {
-      const RhoOut r = get_rho_warp(s0, ab, exp(u0), nelec, K, lane);
-      st |= r.status;
-      emit(top, u0, r);
     }
     for (int k = nz - 2; k >= 0; --k) {
       const double dz = ((double)mget(m, nz, 12, k) - (double)mget(m, nz, 12, k + 1)) * 1000.0 * 100.0;
       const double t1 = t0 + dz;
       const double tm0 = (double)mget(m, nz, 0, k + 1), tm1 = (double)mget(m, nz, 0, k);
-      RhoOut q = get_rho_warp(s0, ab, exp(u0), nelec, K, lane);
-      st |= q.status;
-      const double k1 = (-q.molecw * MAMU * GRAV / (KBOL * tm0)) * dz;
       const double it1 = t0 + dz / 2.0;
-      const double iy1 = u0 + k1 / 2.0;
-      const double tem = tm0 / dz * (t0 + dz - it1) + tm1 / dz * (it1 - t0);
-      saha_prepare(sm, tem, K, tb, lane);
-      q = get_rho_warp(sm, ab, exp(iy1), nelec, K, lane);
-      st |= q.status;
-      const double k2 = (-q.molecw * MAMU * GRAV / (KBOL * tem)) * dz;
-      const double iy2 = u0 + k2 / 2.0;
-      q = get_rho_warp(sm, ab, exp(iy2), nelec, K, lane);
-      st |= q.status;
-      const double k3 = (-q.molecw * MAMU * GRAV / (KBOL * tem)) * dz;
-      const double iy3 = u0 + k3;
-      saha_prepare(s1, tm1, K, tb, lane);
-      q = get_rho_warp(s1, ab, exp(iy3), nelec, K, lane);
-      st |= q.status;
-      const double k4 = (-q.molecw * MAMU * GRAV / (KBOL * tm1)) * dz;
-      const double u1 = u0 + 1.0 / 6.0 * (k1 + 2.0 * k2 + 2.0 * k3 + k4);
-      q = get_rho_warp(s1, ab, exp(u1), nelec, K, lane);
-      st |= q.status;
-      emit(k, u1, q);
+      const double tmid = tm0 / dz * (t0 + dz - it1) + tm1 / dz * (it1 - t0);
+      double kk[4] = {0.0, 0.0, 0.0, 0.0};
+      double u1 = 0.0;
+#pragma unroll 1
+      for (int stg = 0; stg < 5; ++stg) {
+        if (stg == 1 || stg == 3) saha_prepare(w, stg == 1 ? tmid : tm1, K, tb, lane);
+        const double tem = stg == 0 ? tm0 : (stg < 3 ? tmid : tm1);
+        const double y = stg == 0 ? u0 : (stg == 1 ? u0 + kk[0] / 2.0 : (stg == 2 ? u0 + kk[1] / 2.0 : (stg == 3 ? u0 + kk[2] : u1)));
+        const RhoOut q = get_rho_warp(w, ab, exp(y), nelec, K, lane);
+        st |= q.status;
+        if (stg < 4) {
+          const double d = (-q.molecw * MAMU * GRAV / (KBOL * tem)) * dz;
+          kk[0] = stg == 0 ? d : kk[0];
+          kk[1] = stg == 1 ? d : kk[1];
+          kk[2] = stg == 2 ? d : kk[2];
+          kk[3] = stg == 3 ? d : kk[3];
+          if (stg == 3) u1 = u0 + 1.0 / 6.0 * (kk[0] + 2.0 * kk[1] + 2.0 * kk[2] + kk[3]);
+        } else if (lane == 0) {
+          const float pel = (float)q.pelec;
+          mo[1 * nz + k] = (float)exp(u1);
+          mo[2 * nz + k] = (float)q.dens;
+          mo[3 * nz + k] = pel;
+          mo[4 * nz + k] = (float)q.molecw;
+          // FORWARD1D uses NELEC = PEL/KBOL/TEM from the REAL*4 model (src/forward.f90:900)
+          ch[k] = make_double2(q.nhyd, (double)pel / KBOL / tm1);
+        }
+      }
       u0 = u1;
       t0 = t1;
-      s0 = s1;
     }
   }
   if (lane == 0 && status) status[col] = st;

@@ -136,7 +136,7 @@ __device__ __forceinline__ double clamp650(double e) {
   return e;
 }
 
-__device__ __noinline__ void saha_prepare(WarpSaha& w, double T, const Consts& K, const PFTable* __restrict__ tb,
+__device__ __forceinline__ void saha_prepare(WarpSaha& w, double T, const Consts& K, const PFTable* __restrict__ tb,
                                          int lane) {
   // SHORT_PRE_ION_CALC_TEMPRHO, src/chemical_equilibrium.f90:1601-1652
   w.T = T;
@@ -183,7 +183,7 @@ struct RhoOut {
 // with x = ne*alpha_I, y = ne*alpha_II: algebraically the reference's three
 // quotients, one division instead of five.  ab[j] = 10**(ABUND-12) of the
 // lane's elements (0 past element 92).
-__device__ __noinline__ RhoOut get_rho_warp(const WarpSaha& w, const double ab[3], double PG, double& nelec,
+__device__ __forceinline__ RhoOut get_rho_warp(const WarpSaha& w, const double ab[3], double PG, double& nelec,
                                             const Consts& K, int lane) {
   RhoOut r;
   const double T = w.T;
