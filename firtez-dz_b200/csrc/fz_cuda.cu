@@ -83,7 +83,7 @@ __device__ __forceinline__ void copy_to_shared(T* dst, const T* src) {
 // Writes per height (nH, ne) as FORWARD1D uses them, and rho, Pe, mu (and
 // Pg) into the output model.
 template <bool HE>
-__global__ void __launch_bounds__(128, 8) k_chain(const Consts* __restrict__ Kg, const PFTable* __restrict__ tb, int ncol,
+__global__ void __launch_bounds__(128) k_chain(const Consts* __restrict__ Kg, const PFTable* __restrict__ tb, int ncol,
                                                int nz, const float* model, float* mout, double2* __restrict__ chem,
                                                int* __restrict__ status) {
   __shared__ Consts K;
