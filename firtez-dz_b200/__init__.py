@@ -77,6 +77,7 @@ def lib():
         L.fz_get_gain.argtypes = [P, P]
         L.fz_forward.argtypes = [P, ctypes.c_int, P, ctypes.c_int, P, P, P]
         L.fz_forward_device.argtypes = [P, ctypes.c_int, P, ctypes.c_int, P, P, P, P]
+        L.fz_forward_device_static.argtypes = [P, ctypes.c_int, P, ctypes.c_int, P, P, P, P]
         L.fz_profile_enable.argtypes = [P, ctypes.c_int]
         L.fz_profile_read.argtypes = [P, P, P, ctypes.c_int]
         L.fz_measure_fp32_peak.argtypes = [ctypes.c_int, P]
@@ -174,6 +175,16 @@ class Synthesis:
         st = np.zeros(ncol, dtype=np.int32)
         _check(lib().fz_forward(self._h, ncol, _p(m), int(bool(hydrostatic)), _p(syn), _p(mo), _p(st)))
         return syn, mo, st
+
+    def forward_device_static(self, model_ptr, ncol, syn_ptr, model_out_ptr, status_ptr=0, stream=0,
+                              hydrostatic=False):
+        """forward_device without any device allocation: the per-call scratch is
+        a 64 MiB static device array (batches larger than it are rejected).
+        For callers that must not allocate device memory during a call."""
+        _check(lib().fz_forward_device_static(self._h, int(ncol), ctypes.c_void_p(model_ptr), int(bool(hydrostatic)),
+                                              ctypes.c_void_p(syn_ptr), ctypes.c_void_p(model_out_ptr),
+                                              ctypes.c_void_p(status_ptr) if status_ptr else None,
+                                              ctypes.c_void_p(stream) if stream else None))
 
     def profile(self, on=True):
         _check(lib().fz_profile_enable(self._h, int(bool(on))))

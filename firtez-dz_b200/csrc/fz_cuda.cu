@@ -984,6 +984,82 @@ int fz_forward_device(fz_ctx* c, int ncol, const float* d_model, int hydrostatic
   return launch_forward(c, ncol, d_model, hydrostatic, d_syn, d_model_out, d_status, (cudaStream_t)stream);
 }
 
+}  // extern "C"
+
+// ------------------------------------------------ allocation-free variant
+// Scratch of fz_forward_device_static: one file-scope device array, shared
+// by every call on a device and kept for the life of the process.  It holds
+// the per-height (nH, ne) pairs and the opacity slab of one batch of columns.
+#define FZ_NOALLOC_SCRATCH_BYTES (64ull << 20)
+static __device__ __align__(256) unsigned char g_fz_noalloc_scratch[FZ_NOALLOC_SCRATCH_BYTES];
+
+namespace {
+constexpr int kMaxDevices = 64;
+std::mutex g_noalloc_mu;
+void* g_noalloc_ptr[kMaxDevices] = {};
+
+// Device address of the scratch array on `device` (the current device).  In
+// host code the array's name is only a host-side stand-in, so the address is
+// looked up once per device with cudaGetSymbolAddress.
+int noalloc_scratch(int device, unsigned char** out) {
+  if (device < 0 || device >= kMaxDevices) return FZ_ERR_ARG;
+  std::lock_guard<std::mutex> g(g_noalloc_mu);
+  if (!g_noalloc_ptr[device]) {
+    void* p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_fz_noalloc_scratch);
+    if (e != cudaSuccess) {
+      std::fprintf(stderr, "fz_b200: cudaGetSymbolAddress of the static scratch failed: %s\n", cudaGetErrorString(e));
+      return FZ_ERR_CUDA;
+    }
+    g_noalloc_ptr[device] = p;
+  }
+  *out = static_cast<unsigned char*>(g_noalloc_ptr[device]);
+  return 0;
+}
+}  // namespace
+
+extern "C" {
+
+int fz_forward_device_static(fz_ctx* c, int ncol, const float* d_model, int hydrostatic, double* d_syn,
+                             float* d_model_out, int* d_status, void* stream) {
+  if (!c || ncol <= 0 || !d_model || !d_syn || !d_model_out) return FZ_ERR_ARG;
+  const size_t chem_bytes = ((size_t)ncol * c->nz * sizeof(double2) + 255) & ~(size_t)255;
+  const size_t slab_bytes = (size_t)ncol * c->nz * c->sw * sizeof(float);
+  if (chem_bytes + slab_bytes > FZ_NOALLOC_SCRATCH_BYTES) {
+    std::fprintf(stderr,
+                 "fz_b200: fz_forward_device_static: %d columns x %d heights need %zu bytes of scratch, "
+                 "more than the %llu-byte static array; split the batch\n",
+                 ncol, c->nz, chem_bytes + slab_bytes, (unsigned long long)FZ_NOALLOC_SCRATCH_BYTES);
+    return FZ_ERR_LIMIT;
+  }
+  FZ_CK(cudaSetDevice(c->device));
+  unsigned char* base = nullptr;
+  const int rc = noalloc_scratch(c->device, &base);
+  if (rc) return rc;
+  double2* chem = reinterpret_cast<double2*>(base);
+  float* slab = reinterpret_cast<float*>(base + chem_bytes);
+  cudaStream_t s = (cudaStream_t)stream;
+  // Every scratch word a kernel reads is written earlier in the same call
+  // (k_chain fills chem, k_opac fills the slab rows), so nothing is cleared.
+  if (d_status) FZ_CK(cudaMemsetAsync(d_status, 0, ncol * sizeof(int), s));
+  const int wpb = 4;
+  const dim3 gc((ncol + wpb - 1) / wpb);
+  if (hydrostatic)
+    k_chain<true><<<gc, wpb * 32, 0, s>>>(c->d_consts, c->d_pf, ncol, c->nz, d_model, d_model_out, chem, d_status);
+  else
+    k_chain<false><<<gc, wpb * 32, 0, s>>>(c->d_consts, c->d_pf, ncol, c->nz, d_model, d_model_out, chem, d_status);
+  FZ_CK(cudaGetLastError());
+  const size_t total = (size_t)ncol * c->nz;
+  const int blocks = (int)std::min<size_t>((total + 255) / 256, (size_t)c->nsm * 16);
+  k_opac<<<blocks, 256, 0, s>>>(c->d_params, c->d_consts, ncol, d_model_out, chem, slab);
+  FZ_CK(cudaGetLastError());
+  const int threads = (c->numw + 31) & ~31;
+  const size_t sms = (size_t)c->nz * c->sw * sizeof(float);
+  k_synth<<<ncol, threads, sms, s>>>(c->d_params, c->d_lam, c->d_gain, ncol, slab, d_syn, d_model_out, d_status);
+  FZ_CK(cudaGetLastError());
+  return 0;
+}
+
 int fz_forward(fz_ctx* c, int ncol, const float* model, int hydrostatic, double* syn, float* model_out,
                int* status) {
   if (!c || ncol <= 0 || !model || !syn) return FZ_ERR_ARG;

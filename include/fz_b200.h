@@ -105,6 +105,26 @@ int fz_forward(fz_ctx* ctx, int ncol, const float* model, int hydrostatic, doubl
 int fz_forward_device(fz_ctx* ctx, int ncol, const float* d_model, int hydrostatic, double* d_syn,
                       float* d_model_out, int* d_status, void* stream);
 
+/* Allocation-free variant of fz_forward_device, for callers that may not
+ * allocate device memory during a call -- code running inside a host
+ * framework that owns the device allocator, real-time loops, or anything
+ * that has to stay free of cudaMalloc/cudaFree after start-up.  It has no
+ * counterpart in the reference.  The per-call scratch (per-height nH, ne and
+ * the opacity slab) lives in one file-scope 64 MiB device array instead of
+ * the context's grow-on-demand buffers; the call itself calls no cudaMalloc,
+ * cudaFree or allocating library routine.  Limit: ncol * nz * (16 + 4*SW)
+ * bytes <= 64 MiB (SW = slab width, 20 floats for two lines; about 5400
+ * columns of 128 heights); larger batches return FZ_ERR_LIMIT -- split them.
+ * The array is shared by every call on a device and keeps the last call's
+ * contents; every word a kernel reads is written earlier in the same call.
+ * Calls that overlap on the GPU (other streams, other threads) race on it:
+ * serialise them.  The first call on each device looks up the array's device
+ * address (cudaGetSymbolAddress); make that first call before any stream
+ * capture.  Arguments as fz_forward_device; the context itself is created
+ * (and allocated) once by fz_create. */
+int fz_forward_device_static(fz_ctx* ctx, int ncol, const float* d_model, int hydrostatic, double* d_syn,
+                             float* d_model_out, int* d_status, void* stream);
+
 /* Per-kernel timing: when enabled, every launch of the context is bracketed
  * by CUDA events on its stream; fz_profile_read returns the accumulated
  * milliseconds and launch counts of the kernels (names in order:
