@@ -18,6 +18,7 @@
 #include <algorithm>
 #include <cmath>
 #include <complex>
+#include <limits>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -913,6 +914,8 @@ int forward1d(const Setup& s, const float* gain, Col& c, int hydrostatic, double
   return st;
 }
 
+#include "fz_oracle_rf.inc"
+
 // ---------------------------------------------------- line database parse
 // NCOLUMNS, src/lines_database.f90:145-190 (no commas in the database)
 std::vector<std::string> split_ws(const std::string& ln) {
@@ -1207,6 +1210,31 @@ int orc_forward(const orc_line* lines, int nlines, const orc_region* regs, int n
   }
   (void)nthreads;
   return 0;
+}
+
+int orc_forward_rf(const orc_line* lines, int nlines, const orc_region* regs, int nreg, const float* gain, int nz,
+                   int ncol, float* model, int hydrostatic, const int* nodes, double* stokes, float* jac, int* status,
+                   int nthreads) {
+  int np = 0;
+  for (int p = 1; p <= 8; ++p) {
+    if (nodes[p - 1] <= 0) continue;
+    if (p == 3 || p == 8) return -1;   // constant-density pair and P0 are not restated
+    if (nodes[p - 1] > nz) return -2;   // GET_INT_COEFS stops when NJ > NZ
+    np += nodes[p - 1];
+  }
+  Setup s = make_setup(lines, nlines, regs, nreg);
+  const int numw = s.numw;
+#ifdef _OPENMP
+  if (nthreads <= 0) nthreads = omp_get_max_threads();
+#pragma omp parallel for schedule(dynamic, 1) num_threads(nthreads)
+#endif
+  for (int i = 0; i < ncol; ++i) {
+    Col c{model + (size_t)i * nz * 13, nz};
+    status[i] = forward1d_rf(s, gain, c, hydrostatic, nodes, stokes + (size_t)i * 4 * numw,
+                             jac + (size_t)i * 4 * numw * np);
+  }
+  (void)nthreads;
+  return np;
 }
 
 }  // extern "C"

@@ -89,6 +89,17 @@ int orc_forward(const orc_line* lines, int nlines, const orc_region* regs, int n
                 const float* gain, int nz, int ncol, float* model, int hydrostatic,
                 double* stokes, int* status, int nthreads);
 
+/* FORWARD1D with response functions (MRESPFUNCT): Stokes as orc_forward plus
+ * the node Jacobian EQVDSYN (src/forward.f90:552-681) of every reference
+ * parameter p (1 T, 2 Pg, 4 Bx, 5 By, 6 Bz, 7 v_z) with nodes[p-1] > 0 nodes
+ * (nodes[p-1] == NZ gives the response function at every height).  jac is
+ * (4*NUMW, NP, ncol) REAL*4 with NP = sum of nodes.  Returns NP, or -1 for an
+ * unsupported parameter (3, 8) and -2 for nodes > NZ. */
+int orc_forward_rf(const orc_line* lines, int nlines, const orc_region* regs, int nreg,
+                   const float* gain, int nz, int ncol, float* model, int hydrostatic,
+                   const int* nodes /* [8] */, double* stokes, float* jac, int* status,
+                   int nthreads);
+
 #ifdef __cplusplus
 }
 #endif

@@ -52,6 +52,8 @@ def lib():
         L.orc_forward.argtypes = [P, ctypes.c_int, P, ctypes.c_int, P, ctypes.c_int, ctypes.c_int, P,
                                   ctypes.c_int, P, P, ctypes.c_int]
         L.orc_set_abundances.argtypes = [P]
+        L.orc_forward_rf.argtypes = [P, ctypes.c_int, P, ctypes.c_int, P, ctypes.c_int, ctypes.c_int, P,
+                                     ctypes.c_int, P, P, P, P, ctypes.c_int]
         _lib = L
     return _lib
 
@@ -128,3 +130,33 @@ def forward(lines, regions, gain_, model, hydrostatic=False, nthreads=0):
     lib().orc_forward(_p(lines), len(lines), _p(regions), len(regions), _p(g), nz, ncol, _p(m),
                       int(bool(hydrostatic)), _p(stokes), _p(status), int(nthreads))
     return stokes, m, status
+
+
+# reference parameter index (1-based) -> name, as in src/atm_param.f90 order
+RF_PARAMS = {1: "T", 2: "Pg", 4: "Bx", 5: "By", 6: "Bz", 7: "vz"}
+
+
+def forward_rf(lines, regions, gain_, model, nodes, hydrostatic=False, nthreads=0):
+    """FORWARD1D with response functions.
+
+    nodes: dict {reference parameter index: node count} (1 T, 2 Pg, 4 Bx,
+    5 By, 6 Bz, 7 vz).  Returns (stokes (ncol,4,numw), jac (ncol, NP, 4*numw)
+    float32 = EQVDSYN transposed per column, model_out, status)."""
+    lines = np.ascontiguousarray(lines, dtype=LINE_DTYPE)
+    regions = np.ascontiguousarray(regions, dtype=REGION_DTYPE)
+    g = np.ascontiguousarray(gain_, dtype=np.float32)
+    m = np.array(model, dtype=np.float32, order="C", copy=True)
+    ncol, npar, nz = m.shape
+    numw = int(regions["numwave"].sum())
+    nv = np.zeros(8, dtype=np.int32)
+    for p, n in nodes.items():
+        nv[p - 1] = n
+    np_ = int(nv.sum())
+    stokes = np.zeros((ncol, 4, numw))
+    jac = np.zeros((ncol, np_, 4 * numw), dtype=np.float32)
+    status = np.zeros(ncol, dtype=np.int32)
+    r = lib().orc_forward_rf(_p(lines), len(lines), _p(regions), len(regions), _p(g), nz, ncol, _p(m),
+                             int(bool(hydrostatic)), _p(nv), _p(stokes), _p(jac), _p(status), int(nthreads))
+    if r < 0:
+        raise ValueError("orc_forward_rf rejected the node set (%d)" % r)
+    return stokes, jac, m, status
