@@ -7,6 +7,9 @@ Host-side mirror of the reference's interface for the hot path, over ctypes:
                                         (src/input_file.f90:290-366) + WAVE_INIT
   * ``Synthesis(...).forward(model)``-- FORWARD3D/FORWARD1D (src/forward.f90:43, :857)
                                         batched over columns on one GPU
+  * ``Synthesis.rf_nodes(nodes)`` and ``forward_rf(model)`` -- FORWARD1D with
+                                        response functions: the node Jacobian
+                                        EQVDSYN (src/forward.f90:511-681)
 
 Arrays use the reference layouts: ``model`` is MODEL(NZ,13,ncol) REAL*4,
 i.e. a C-ordered numpy array of shape (ncol, 13, nz); ``syn`` is
@@ -30,7 +33,11 @@ MAXBLEND = 8
 TEM, PG, RHO, PEL, MW, BX, BY, BZ, VX, VY, VZ, TAU5, ZZ = range(13)
 
 FZ_OK, FZ_CHEM_NOCONV, FZ_NAN = 0, 1, 2
-KERNELS = ("k_chain", "k_opac", "k_synth")
+KERNELS = ("k_chain", "k_opac", "k_synth", "k_opac_rf", "k_synth_rf")
+
+# free-parameter indices of the reference (atm_param.f90 order, 1-based) that
+# carry response functions
+RF_PARAMS = {1: "T", 2: "Pg", 4: "Bx", 5: "By", 6: "Bz", 7: "vz"}
 
 LINE_DTYPE = np.dtype([
     ("num", "<i4"), ("zn", "<i4"), ("ion", "<i4"), ("flag", "<i4"), ("otr", "<i4", 2),
@@ -81,6 +88,9 @@ def lib():
         L.fz_profile_enable.argtypes = [P, ctypes.c_int]
         L.fz_profile_read.argtypes = [P, P, P, ctypes.c_int]
         L.fz_measure_fp32_peak.argtypes = [ctypes.c_int, P]
+        L.fz_rf_nodes.argtypes = [P, P]
+        L.fz_forward_rf.argtypes = [P, ctypes.c_int, P, ctypes.c_int, P, P, P, P]
+        L.fz_forward_rf_device.argtypes = [P, ctypes.c_int, P, ctypes.c_int, P, P, P, P, P]
         _lib = L
     return _lib
 
@@ -191,10 +201,54 @@ class Synthesis:
 
     def profile_read(self):
         """{kernel: (total ms, launches)} since the last read."""
-        ms = np.zeros(3)
-        n = np.zeros(3, dtype=np.int32)
-        _check(lib().fz_profile_read(self._h, _p(ms), _p(n), 3))
+        nk = len(KERNELS)
+        ms = np.zeros(nk)
+        n = np.zeros(nk, dtype=np.int32)
+        _check(lib().fz_profile_read(self._h, _p(ms), _p(n), nk))
         return {k: (ms[i], int(n[i])) for i, k in enumerate(KERNELS)}
+
+    def rf_nodes(self, nodes):
+        """Select the free parameters of the response functions.
+
+        nodes: {reference parameter (1 T, 2 Pg, 4 Bx, 5 By, 6 Bz, 7 vz): node
+        count}; a count equal to nz gives the response at every height.
+        Returns NP, the number of Jacobian columns."""
+        v = np.zeros(8, dtype=np.int32)
+        for p, n in nodes.items():
+            if not 1 <= int(p) <= 8:
+                raise ValueError("parameter index %r out of range" % p)
+            v[int(p) - 1] = int(n)
+        self.np = _check(lib().fz_rf_nodes(self._h, _p(v)))
+        return self.np
+
+    def forward_rf(self, model, hydrostatic=False):
+        """Synthesis plus the node Jacobian of host-resident columns.
+
+        Returns (syn (ncol, 4, numw) float64, jac (ncol, NP, 4*numw) float32 --
+        EQVDSYN(NFREQ, NP) per column --, model_out, status)."""
+        m = np.ascontiguousarray(model, dtype=np.float32)
+        if m.ndim == 2:
+            m = m[None]
+        ncol, npar, nz = m.shape
+        if npar != 13 or nz != self.nz:
+            raise ValueError("model must be (ncol, 13, %d)" % self.nz)
+        if not getattr(self, "np", 0):
+            raise FzError("call rf_nodes() first")
+        syn = np.zeros((ncol, 4, self.numw))
+        jac = np.zeros((ncol, self.np, 4 * self.numw), dtype=np.float32)
+        mo = np.empty_like(m)
+        st = np.zeros(ncol, dtype=np.int32)
+        _check(lib().fz_forward_rf(self._h, ncol, _p(m), int(bool(hydrostatic)), _p(syn), _p(jac), _p(mo), _p(st)))
+        return syn, jac, mo, st
+
+    def forward_rf_device(self, model_ptr, ncol, syn_ptr, jac_ptr, model_out_ptr, status_ptr=0, stream=0,
+                          hydrostatic=False):
+        """Enqueue synthesis + node Jacobian on device pointers."""
+        _check(lib().fz_forward_rf_device(self._h, int(ncol), ctypes.c_void_p(model_ptr), int(bool(hydrostatic)),
+                                          ctypes.c_void_p(syn_ptr), ctypes.c_void_p(jac_ptr),
+                                          ctypes.c_void_p(model_out_ptr),
+                                          ctypes.c_void_p(status_ptr) if status_ptr else None,
+                                          ctypes.c_void_p(stream) if stream else None))
 
     def forward_device(self, model_ptr, ncol, syn_ptr, model_out_ptr, status_ptr=0, stream=0, hydrostatic=False):
         """Enqueue a synthesis on device pointers (e.g. torch ``data_ptr()``)."""

@@ -26,6 +26,7 @@
 #include "../../include/fz_b200.h"
 #include "fz_host.h"
 #include "fz_physics.cuh"
+#include "fz_rf.cuh"
 
 using namespace fzd;
 
@@ -45,6 +46,7 @@ struct DevParams {
   LineP lu[MAXLU];          // used lines in region order
   int lu_nc[MAXLU], lu_c0[MAXLU];
   int lu_nt[MAXLU][3];      // components per type: sigma_red, pi, sigma_blue
+  float lu_duv[MAXLU];      // -1e3 lambda0 / c: d u / d v_z = lu_duv / Doppler width [mA]
   float comp_shift[MAXCOMP], comp_str[MAXCOMP];
   int comp_type[MAXCOMP];
 };
@@ -334,17 +336,17 @@ __global__ void __launch_bounds__(MAXNUMW) k_synth(const DevParams* __restrict__
       rU = fmaf(kldz, g4 * fl, rU);
       rV = fmaf(kldz, g5 * (f0 - f2), rV);
     }
-    float O[16];
+    float O[16], om0 = 0.0f;
     if (!(isfinite(tI) && isfinite(tQ) && isfinite(tU) && isfinite(tV) && isfinite(rQ) && isfinite(rU) &&
           isfinite(rV))) {
       bad = 1;   // the reference replaces a non-finite matrix by the identity
 #pragma unroll
       for (int i = 0; i < 16; ++i) O[i] = (i % 5 == 0) ? 1.f : 0.f;
     } else {
-      evol_f32(tI, tQ, tU, tV, rQ, rU, rV, O);
+      evol_f32(tI, tQ, tU, tV, rQ, rU, rV, O, om0);
     }
     // I_k = (1 - O) S + O I_{k-1}, src/rtesolver.f90:163-187
-    const float n0 = fmaf(1.0f - O[0], S, fmaf(O[0], I0, fmaf(O[1], I1, fmaf(O[2], I2, O[3] * I3))));
+    const float n0 = fmaf(om0, S, fmaf(O[0], I0, fmaf(O[1], I1, fmaf(O[2], I2, O[3] * I3))));
     const float n1 = fmaf(-O[4], S, fmaf(O[4], I0, fmaf(O[5], I1, fmaf(O[6], I2, O[7] * I3))));
     const float n2 = fmaf(-O[8], S, fmaf(O[8], I0, fmaf(O[9], I1, fmaf(O[10], I2, O[11] * I3))));
     const float n3 = fmaf(-O[12], S, fmaf(O[12], I0, fmaf(O[13], I1, fmaf(O[14], I2, O[15] * I3))));
@@ -361,6 +363,460 @@ __global__ void __launch_bounds__(MAXNUMW) k_synth(const DevParams* __restrict__
   o[2 * nw + l] = (double)I2 * (double)gain[4 * l + 2];
   o[3 * nw + l] = (double)I3 * (double)gain[4 * l + 3];
   if (!(isfinite(I0) && isfinite(I1) && isfinite(I2) && isfinite(I3))) bad = 1;
+  if (status && __any_sync(__activemask(), bad) && (l & 31) == 0) atomicOr(&status[col], FZ_NAN);
+}
+
+// ------------------------------------------------------ response functions
+// RF slab row = the synthesis row followed by the derivative inputs:
+//   dkc_t*dz, dkc_p*dz per region; per used line dkl_t*dz, dkl_p*dz,
+//   ddam_t, ddam_p; per field component i (x, y, z) the derivatives of the
+//   five geometry factors (0.25 cgf, 0.5 sgf, sgf c2p, sgf s2p, 0.5 cosg);
+//   dB/dB_i (3); hydrostatic factor c_K (below) and Pg_K.
+__host__ __device__ inline int rf_base(int nreg, int nlu) { return 4 + nreg + 6 + 4 * nlu; }
+__host__ __device__ inline int rf_dkc(int nreg, int nlu) { return rf_base(nreg, nlu); }
+__host__ __device__ inline int rf_dline(int nreg, int nlu) { return rf_base(nreg, nlu) + 2 * nreg; }
+__host__ __device__ inline int rf_dgeo(int nreg, int nlu) { return rf_dline(nreg, nlu) + 4 * nlu; }
+__host__ __device__ inline int rf_db(int nreg, int nlu) { return rf_dgeo(nreg, nlu) + 15; }
+__host__ __device__ inline int rf_he(int nreg, int nlu) { return rf_db(nreg, nlu) + 3; }
+__host__ __device__ inline int rf_w(int nreg, int nlu) { return (rf_he(nreg, nlu) + 2 + 3) & ~3; }
+
+// Node layout of the Jacobian: parameter slots T|Pg, Pg|T, Bx, By, Bz, v_z
+// (reference parameters 1, 2, 4, 5, 6, 7); slot p owns nodes [n0[p], n0[p]+nj[p]).
+constexpr int NSLOT = 6;
+constexpr int MAXNP = 64;
+struct RFConf {
+  int np;
+  int nj[NSLOT], n0[NSLOT];
+};
+
+// One warp per (column, height), FP64: the synthesis slab row of k_opac plus
+// the derivative inputs.  Chemistry derivatives at the (T, Pg, NELEC) that
+// FORWARD1D passes to GET_DNHYDDTEMP (src/forward.f90:917-918); the
+// hydrostatic factor of GET_HYD_DERIVATIVES (:1050-1057) is stored as
+// c_K = DPGDTK_HE(I) / Pg(I) = -(Pg_K mu_K)_REAL*4 CTE / T_K^2 / Pg_K.
+__global__ void __launch_bounds__(128) k_opac_rf(const DevParams* __restrict__ Pg, const Consts* __restrict__ Kg,
+                                                 int ncol, const float* __restrict__ mout,
+                                                 const double2* __restrict__ chem, float* __restrict__ slab) {
+  __shared__ DevParams P;
+  __shared__ Consts K;
+  copy_to_shared(&P, Pg);
+  copy_to_shared(&K, Kg);
+  __syncthreads();
+  const int nz = P.nz, nreg = P.nreg, nlu = P.nlu;
+  const int sw = rf_w(nreg, nlu);
+  const int lane = threadIdx.x & 31;
+  const int wpb = blockDim.x >> 5;
+  const size_t total = (size_t)ncol * nz;
+  for (size_t i = (size_t)blockIdx.x * wpb + (threadIdx.x >> 5); i < total; i += (size_t)gridDim.x * wpb) {
+    const int col = (int)(i / nz), k = (int)(i % nz);
+    const float* m = mout + (size_t)col * 13 * nz;
+    const double2 c = chem[i];
+    const double nhyd = c.x, nelec = c.y;
+    const float Tf = mget(m, nz, 0, k);
+    const double T = (double)Tf;
+    const double dz = (k == nz - 1) ? 1e5 * fabs((double)mget(m, nz, 12, k) - (double)mget(m, nz, 12, k - 1))
+                                    : 1e5 * fabs((double)mget(m, nz, 12, k + 1) - (double)mget(m, nz, 12, k));
+    const ChemDer cd = chem_der_warp(T, (double)mget(m, nz, 1, k), nelec, K, lane);
+    float* row = slab + i * sw;
+    if (lane == 0) {
+      const double kc5 = opac_continuum(T, nelec, nhyd, P.cont[P.nreg]) / nhyd * (1.0 / MAMU);
+      row[0] = Tf;
+      row[1] = (kc5 < KC5THRESHOLD) ? 0.0f : 1.0f;
+      row[2] = (float)kc5;
+      row[3] = mget(m, nz, 2, k);
+      const double x = mget(m, nz, 5, k), y = mget(m, nz, 6, k), z = mget(m, nz, 7, k);
+      const double x2 = x * x, y2 = y * y, z2 = z * z;
+      const double b2 = x2 + y2 + z2, b = sqrt(b2);
+      const double xm = x2 - y2, xp = x2 + y2;
+      double cosg = 0, cgf = 1, sgf = 1, c2p = 0, s2p = 0;
+      double dcgf[3] = {0, 0, 0}, dc2p[3] = {0, 0, 0}, ds2p[3] = {0, 0, 0}, dcg[3] = {0, 0, 0}, db[3] = {0, 0, 0};
+      if (b > 0) {
+        cosg = z / b;
+        cgf = 1 + z2 / b2;
+        sgf = 1 - z2 / b2;
+        // src/absorption_matrix.f90:1852-1873 (0/0 for Bx = By = 0 < B, as there)
+        dcgf[0] = -2.0 * x * z2 / b2 / b2;
+        dcgf[1] = -2.0 * y * z2 / b2 / b2;
+        dcgf[2] = (2.0 * z * (b2 - z2)) / b2 / b2;
+        dc2p[0] = 4.0 * x * y2 / xp / xp;
+        dc2p[1] = -4.0 * y * x2 / xp / xp;
+        ds2p[0] = -2.0 * y * xm / xp / xp;
+        ds2p[1] = 2.0 * x * xm / xp / xp;
+        dcg[0] = -(z * x) / b / b2;
+        dcg[1] = -(z * y) / b / b2;
+        dcg[2] = (1.0 - cosg * cosg) / b;
+        db[0] = x / b;
+        db[1] = y / b;
+        db[2] = z / b;
+      }
+      if (x != 0 || y != 0) {
+        c2p = xm / xp;
+        s2p = 2. * x * y / xp;
+      }
+      float* g = row + slab_geo(nreg);
+      g[0] = (float)(0.25 * cgf);
+      g[1] = (float)(0.5 * sgf);
+      g[2] = (float)(sgf * c2p);
+      g[3] = (float)(sgf * s2p);
+      g[4] = (float)(0.5 * cosg);
+      g[5] = (float)b;
+      float* dg = row + rf_dgeo(nreg, nlu);
+      for (int q = 0; q < 3; ++q) {
+        const double dsgf = -dcgf[q];
+        dg[5 * q + 0] = (float)(0.25 * dcgf[q]);
+        dg[5 * q + 1] = (float)(0.5 * dsgf);
+        dg[5 * q + 2] = (float)(dsgf * c2p + sgf * dc2p[q]);
+        dg[5 * q + 3] = (float)(dsgf * s2p + sgf * ds2p[q]);
+        dg[5 * q + 4] = (float)(0.5 * dcg[q]);
+        row[rf_db(nreg, nlu) + q] = (float)db[q];
+      }
+      double ck = 0.0;
+      const float pgk = mget(m, nz, 1, k);
+      if (k > 0) {
+        const double cte =
+            MAMU / KBOL * GRAV * ((double)mget(m, nz, 12, k) - (double)mget(m, nz, 12, k - 1)) * 1.0e3 * 1.0e2;
+        const float pm = pgk * mget(m, nz, 4, k);
+        ck = -((double)pm * cte / T / T) / (double)pgk;
+      }
+      row[rf_he(nreg, nlu)] = (float)ck;
+      row[rf_he(nreg, nlu) + 1] = pgk;
+    } else if (lane <= nreg) {
+      const int r = lane - 1;
+      row[4 + r] = (float)(opac_continuum(T, nelec, nhyd, P.cont[r]) * dz);
+      double dt, dp;
+      cont_der(T, nelec, nhyd, P.cont[r], cd, dt, dp);
+      row[rf_dkc(nreg, nlu) + 2 * r] = (float)(dt * dz);
+      row[rf_dkc(nreg, nlu) + 2 * r + 1] = (float)(dp * dz);
+    } else if (lane >= 16 && lane < 16 + nlu) {
+      const int b = lane - 16;
+      const LineP& L = P.lu[b];
+      const double klin = opac_line(L, T, nelec, nhyd, K);
+      const double damp = get_damping(L, nhyd, T);
+      const double dldop = 1e3 * (sqrt(L.vdk * T) * L.l0 / LIGHT);
+      const double dlv = -1e3 * L.l0 * (double)mget(m, nz, 10, k) / LIGHT;
+      float* q = row + slab_line(nreg) + 4 * b;
+      q[0] = (float)(klin * dz);
+      q[1] = (float)damp;
+      q[2] = (float)(1.0 / dldop);
+      q[3] = (float)(dlv - L.wdif);
+      double dkt, dkp, ddt, ddp;
+      line_der(L, T, nelec, nhyd, cd, K, dkt, dkp);
+      damp_der(L, nhyd, T, cd, ddt, ddp);
+      float* d = row + rf_dline(nreg, nlu) + 4 * b;
+      d[0] = (float)(dkt * dz);
+      d[1] = (float)(dkp * dz);
+      d[2] = (float)ddt;
+      d[3] = (float)ddp;
+    }
+  }
+}
+
+// Linear maps from the per-type (sigma_red, pi, sigma_blue) sums of one line
+// to the seven matrix elements (eta_I,Q,U,V, rho_Q,U,V), the grouping of the
+// component accumulation of src/absorption_matrix.f90:1948-2278.
+struct Geo {
+  float g1, g2, g3, g4, g5;
+};
+__device__ __forceinline__ void lmap(const Geo& g, const float h[3], const float f[3], float o[7]) {
+  const float hs = h[0] + h[2], fs = f[0] + f[2];
+  const float hl = 0.5f * h[1] - 0.25f * hs, fl = 0.5f * f[1] - 0.25f * fs;
+  o[0] = g.g1 * hs + g.g2 * h[1];
+  o[1] = g.g3 * hl;
+  o[2] = g.g4 * hl;
+  o[3] = g.g5 * (h[0] - h[2]);
+  o[4] = g.g3 * fl;
+  o[5] = g.g4 * fl;
+  o[6] = g.g5 * (f[0] - f[2]);
+}
+
+// One CTA per column, one thread per wavelength, FP32: the synthesis of
+// k_synth plus, per height, the derivatives of the seven optical depths for
+// the six parameters (WDEV, src/absorption_matrix.f90:1717-2642), the local
+// response functions of OLD_ANALYTICAL_SOLVER (src/rtesolver.f90:194-260)
+// and their forward accumulation into the node Jacobian:
+//   D_j <- O_K D_j + coef(K, j) RF_p(K)
+// which equals OLD_DSYN_PROPAGATION (src/forward.f90:511-548) followed by
+// the hat-function contraction of CALCULATE_EQUIVALENT_DSYN (:552-681).
+// Hydrostatic mode adds the global T term of :218-232 through the
+// recurrence H_K = O_K H_{K-1} + RF_Pg(K) Pg_K (skipped where O_K(1,1) <=
+// 1e-5), RF_T(K) += c_K O_K H_{K-1}, and evaluates the B and v_z terms with
+// the layer's outgoing Stokes vector, as the reference does (STKIN is
+// reassigned at :230).  Layers that take the boundary condition have no
+// response and reset the accumulators (their operator is taken as 0).
+// Shared memory: the slab, the coefficient table (nz x np) and the node
+// accumulators (np x 4 x blockDim).
+template <bool HE>
+__global__ void __launch_bounds__(256) k_synth_rf(const DevParams* __restrict__ Pg, const RFConf* __restrict__ Rg,
+                                                  const LamP* __restrict__ lam, const float* __restrict__ gain,
+                                                  int ncol, const float* __restrict__ slab,
+                                                  const float* __restrict__ coefg, double* __restrict__ syn,
+                                                  float* __restrict__ jac, float* mout, int* __restrict__ status) {
+  extern __shared__ float4 sm_rf4[];
+  __shared__ DevParams P;
+  __shared__ RFConf C;
+  __shared__ unsigned inf_mask[2];
+  copy_to_shared(&P, Pg);
+  copy_to_shared(&C, Rg);
+  const int col = blockIdx.x;
+  const int nz = Pg->nz, nreg = Pg->nreg, nlu = Pg->nlu, np = Rg->np;
+  const int sw = rf_w(nreg, nlu);
+  const int nthr = blockDim.x;
+  float* sm = reinterpret_cast<float*>(sm_rf4);
+  float* coef = sm + nz * sw;
+  float* Dacc = coef + nz * np;
+  {
+    const float4* src = reinterpret_cast<const float4*>(slab + (size_t)col * nz * sw);
+    const int n4 = nz * sw / 4;
+    for (int i = threadIdx.x; i < n4; i += nthr) sm_rf4[i] = __ldg(src + i);
+    for (int i = threadIdx.x; i < nz * np; i += nthr) coef[i] = __ldg(coefg + i);
+    for (int i = threadIdx.x; i < np * 4 * nthr; i += nthr) Dacc[i] = 0.0f;
+    if (threadIdx.x < 2) inf_mask[threadIdx.x] = 0u;
+  }
+  __syncthreads();
+  const int l = threadIdx.x;
+  const bool active = l < P.numw;
+  if (l == 0) {
+    // log tau5, src/forward.f90:1000-1006 (as k_synth)
+    float* mo = mout + (size_t)col * 13 * nz;
+    float tau = 1e-9f;
+    mo[11 * nz + nz - 1] = log10f(tau);
+    for (int k = nz - 2; k >= 0; --k) {
+      const float a = (sm[k * sw + 2] * sm[k * sw + 3] + sm[(k + 1) * sw + 2] * sm[(k + 1) * sw + 3]) / 2.0f;
+      const double b = ((double)mo[12 * nz + k + 1] - (double)mo[12 * nz + k]) * 1000.0 * 100.0;
+      tau = (float)((double)tau + (double)a * b);
+      mo[11 * nz + k] = log10f(tau);
+    }
+  }
+  const LamP lp = lam[active ? l : 0];
+  const int r = lp.reg;
+  const int nb = P.reg_nb[r], lb = P.reg_lb[r];
+  const int goff = slab_geo(nreg), loff = slab_line(nreg);
+  const int dkoff = rf_dkc(nreg, nlu) + 2 * r, dloff = rf_dline(nreg, nlu), dgoff = rf_dgeo(nreg, nlu);
+  const int dboff = rf_db(nreg, nlu), heoff = rf_he(nreg, nlu);
+  float I0 = 0.f, I1 = 0.f, I2 = 0.f, I3 = 0.f;
+  float H[4] = {0.f, 0.f, 0.f, 0.f};
+  int bad = 0;
+  for (int k = 0; active && k < nz; ++k) {
+    const float* row = sm + k * sw;
+    const float T = row[0];
+    const float q = lp.c2 / T;
+    const float em1 = expm1f(q);
+    const float S = lp.c1 / em1;
+    if (k == 0 || row[1] != 0.0f) {   // SET_BOUNDARY
+      I0 = S;
+      I1 = I2 = I3 = 0.f;
+      for (int j = 0; j < np; ++j)
+#pragma unroll
+        for (int c = 0; c < 4; ++c) Dacc[(j * 4 + c) * nthr + l] = 0.0f;
+      continue;
+    }
+    const Geo g{row[goff], row[goff + 1], row[goff + 2], row[goff + 3], row[goff + 4]};
+    const float B = row[goff + 5];
+    const float halfT = 0.5f / T;
+    float tI = row[4 + r], tQ = 0.f, tU = 0.f, tV = 0.f, rQ = 0.f, rU = 0.f, rV = 0.f;
+    float dtau[NSLOT][7];
+#pragma unroll
+    for (int p = 0; p < NSLOT; ++p)
+#pragma unroll
+      for (int x = 0; x < 7; ++x) dtau[p][x] = 0.0f;
+    dtau[0][0] = row[dkoff];
+    dtau[1][0] = row[dkoff + 1];
+    for (int b = 0; b < nb; ++b) {
+      const float* qq = row + loff + 4 * (lb + b);
+      const float kldz = qq[0], a = qq[1], idd = qq[2];
+      const float x0 = lp.wave + qq[3];
+      // per-type sums: value (h, f) and the derivative sums of WDEV
+      float hh[3] = {0, 0, 0}, ff[3] = {0, 0, 0}, av[3] = {0, 0, 0}, ca[3] = {0, 0, 0};
+      float avu[3] = {0, 0, 0}, cau[3] = {0, 0, 0}, avs[3] = {0, 0, 0}, cas[3] = {0, 0, 0};
+      int c = P.lu_c0[lb + b];
+#pragma unroll
+      for (int t = 0; t < 3; ++t) {
+        const int e = c + P.lu_nt[lb + b][t];
+        for (; c < e; ++c) {
+          const float shf = P.comp_shift[c], st = P.comp_str[c];
+          const float u = fmaf(shf, B, x0) * idd;
+          float h, f;
+          voigt_f32(a, u, h, f);
+          const float dhv = 2.0f * fmaf(a, f, -u * h);                       // 2(-u H + a F)
+          const float dha = 2.0f * (fmaf(a, h, u * f) - 0.56418958354775628f);  // 2(-1/sqrt(pi) + a H + u F)
+          hh[t] = fmaf(st, h, hh[t]);
+          ff[t] = fmaf(st, f, ff[t]);
+          const float sv = st * dhv, sa = st * dha;
+          av[t] += sv;
+          ca[t] += sa;
+          avu[t] = fmaf(sv, u, avu[t]);
+          cau[t] = fmaf(sa, u, cau[t]);
+          avs[t] = fmaf(sv, shf, avs[t]);
+          cas[t] = fmaf(sa, shf, cas[t]);
+        }
+      }
+      {
+        // value part: same expressions as k_synth
+        const float hs = hh[0] + hh[2], fs = ff[0] + ff[2];
+        const float hl = 0.5f * hh[1] - 0.25f * hs, fl = 0.5f * ff[1] - 0.25f * fs;
+        tI = fmaf(kldz, g.g1 * hs + g.g2 * hh[1], tI);
+        tQ = fmaf(kldz, g.g3 * hl, tQ);
+        tU = fmaf(kldz, g.g4 * hl, tU);
+        tV = fmaf(kldz, g.g5 * (hh[0] - hh[2]), tV);
+        rQ = fmaf(kldz, g.g3 * fl, rQ);
+        rU = fmaf(kldz, g.g4 * fl, rU);
+        rV = fmaf(kldz, g.g5 * (ff[0] - ff[2]), rV);
+      }
+      const float* dl = row + dloff + 4 * (lb + b);
+      const float dkt = dl[0], dkp = dl[1], ddt = dl[2], ddp = dl[3];
+      float base[7], tmp[7];
+      lmap(g, hh, ff, base);
+      // T at constant Pg: dKLIN, du/dT = -u/(2T), da/dT
+      {
+        float xe[3], xr[3];
+#pragma unroll
+        for (int t = 0; t < 3; ++t) {
+          xe[t] = fmaf(ca[t], ddt, -avu[t] * halfT);
+          xr[t] = fmaf(av[t], ddt, cau[t] * halfT);
+        }
+        lmap(g, xe, xr, tmp);
+#pragma unroll
+        for (int x = 0; x < 7; ++x) dtau[0][x] += fmaf(dkt, base[x], kldz * tmp[x]);
+      }
+      // Pg at constant T: dKLIN and da/dPg (the reference's KLIN*acc*DDAMDPG_TEMP)
+      lmap(g, ca, av, tmp);
+#pragma unroll
+      for (int x = 0; x < 7; ++x) dtau[1][x] += fmaf(dkp, base[x], kldz * ddp * tmp[x]);
+      // v_z: du/dv = lu_duv / Doppler width
+      {
+        float nca[3] = {-ca[0], -ca[1], -ca[2]};
+        lmap(g, av, nca, tmp);
+        const float kv = kldz * P.lu_duv[lb + b] * idd;
+#pragma unroll
+        for (int x = 0; x < 7; ++x) dtau[5][x] += kv * tmp[x];
+      }
+      // B_i: geometry factors and the shift term du/dB = shift / Doppler width
+      {
+        float ncs[3] = {-cas[0], -cas[1], -cas[2]};
+        float sh7[7];
+        lmap(g, avs, ncs, sh7);
+#pragma unroll
+        for (int i = 0; i < 3; ++i) {
+          const float* dg = row + dgoff + 5 * i;
+          const Geo gd{dg[0], dg[1], dg[2], dg[3], dg[4]};
+          lmap(gd, hh, ff, tmp);
+          const float kb = idd * row[dboff + i];
+#pragma unroll
+          for (int x = 0; x < 7; ++x) dtau[2 + i][x] += kldz * fmaf(kb, sh7[x], tmp[x]);
+        }
+      }
+    }
+    float O[16], om0 = 0.0f;
+    EvolSt es;
+    const bool fin = isfinite(tI) && isfinite(tQ) && isfinite(tU) && isfinite(tV) && isfinite(rQ) &&
+                     isfinite(rU) && isfinite(rV);
+    if (!fin) {
+      bad = 1;
+#pragma unroll
+      for (int i = 0; i < 16; ++i) O[i] = (i % 5 == 0) ? 1.f : 0.f;
+    } else {
+      evol_state(tI, tQ, tU, tV, rQ, rU, rV, O, om0, es);
+    }
+    const float n0 = fmaf(om0, S, fmaf(O[0], I0, fmaf(O[1], I1, fmaf(O[2], I2, O[3] * I3))));
+    const float n1 = fmaf(-O[4], S, fmaf(O[4], I0, fmaf(O[5], I1, fmaf(O[6], I2, O[7] * I3))));
+    const float n2 = fmaf(-O[8], S, fmaf(O[8], I0, fmaf(O[9], I1, fmaf(O[10], I2, O[11] * I3))));
+    const float n3 = fmaf(-O[12], S, fmaf(O[12], I0, fmaf(O[13], I1, fmaf(O[14], I2, O[15] * I3))));
+    float rf[NSLOT][4];
+    if (fin) {
+      EvolW wi;
+      const float win[4] = {I0 - S, I1, I2, I3};
+      evol_w(es, O, win, wi);
+      evol_dir(es, wi, dtau[0], rf[0]);
+      evol_dir(es, wi, dtau[1], rf[1]);
+      if (HE) {
+        EvolW wo;
+        const float wout[4] = {n0 - S, n1, n2, n3};
+        evol_w(es, O, wout, wo);
+#pragma unroll
+        for (int p = 2; p < NSLOT; ++p) evol_dir(es, wo, dtau[p], rf[p]);
+      } else {
+#pragma unroll
+        for (int p = 2; p < NSLOT; ++p) evol_dir(es, wi, dtau[p], rf[p]);
+      }
+    } else {
+#pragma unroll
+      for (int p = 0; p < NSLOT; ++p)
+#pragma unroll
+        for (int c = 0; c < 4; ++c) rf[p][c] = 0.0f;
+    }
+    // source-function term of the T response: (1 - O) e0 dS/dT, with
+    // dS/dT = c1 (c2/T^2) e^q / (e^q - 1)^2 (src/rtesolver.f90:1039-1066)
+    {
+      const float dS = lp.c1 * (q / T) * ((em1 + 1.0f) / (em1 * em1));
+      rf[0][0] = fmaf(om0, dS, rf[0][0]);
+      rf[0][1] = fmaf(-O[4], dS, rf[0][1]);
+      rf[0][2] = fmaf(-O[8], dS, rf[0][2]);
+      rf[0][3] = fmaf(-O[12], dS, rf[0][3]);
+    }
+    if (HE) {
+      const float ck = row[heoff], pgk = row[heoff + 1];
+      const bool prop = O[0] > 1.0e-5f;
+      float OH[4];
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+        OH[i] = prop ? O[4 * i] * H[0] + O[4 * i + 1] * H[1] + O[4 * i + 2] * H[2] + O[4 * i + 3] * H[3] : H[i];
+#pragma unroll
+      for (int i = 0; i < 4; ++i) {
+        rf[0][i] = fmaf(ck, OH[i], rf[0][i]);
+        H[i] = prop ? fmaf(rf[1][i], pgk, OH[i]) : H[i];
+      }
+    }
+    // node accumulation
+    const float* ck = coef + k * np;
+#pragma unroll
+    for (int p = 0; p < NSLOT; ++p) {
+      const int j0 = C.n0[p], j1 = j0 + C.nj[p];
+      for (int j = j0; j < j1; ++j) {
+        float* d = Dacc + (j * 4) * nthr + l;
+        const float d0 = d[0], d1 = d[nthr], d2 = d[2 * nthr], d3 = d[3 * nthr];
+        const float cj = ck[j];
+        d[0] = fmaf(cj, rf[p][0], fmaf(O[0], d0, fmaf(O[1], d1, fmaf(O[2], d2, O[3] * d3))));
+        d[nthr] = fmaf(cj, rf[p][1], fmaf(O[4], d0, fmaf(O[5], d1, fmaf(O[6], d2, O[7] * d3))));
+        d[2 * nthr] = fmaf(cj, rf[p][2], fmaf(O[8], d0, fmaf(O[9], d1, fmaf(O[10], d2, O[11] * d3))));
+        d[3 * nthr] = fmaf(cj, rf[p][3], fmaf(O[12], d0, fmaf(O[13], d1, fmaf(O[14], d2, O[15] * d3))));
+      }
+    }
+    I0 = n0;
+    I1 = n1;
+    I2 = n2;
+    I3 = n3;
+  }
+  const int nw = P.numw;
+  const int nfreq = 4 * nw;
+  unsigned mask[2] = {0u, 0u};
+  if (active) {
+    double* o = syn + (size_t)col * 4 * nw;
+    o[0 * nw + l] = (double)I0 * (double)gain[4 * l + 0];
+    o[1 * nw + l] = (double)I1 * (double)gain[4 * l + 1];
+    o[2 * nw + l] = (double)I2 * (double)gain[4 * l + 2];
+    o[3 * nw + l] = (double)I3 * (double)gain[4 * l + 3];
+    if (!(isfinite(I0) && isfinite(I1) && isfinite(I2) && isfinite(I3))) bad = 1;
+    // EQVDSYN = REAL(sum) * GAIN (src/forward.f90:614-621)
+    float* jo = jac + (size_t)col * np * nfreq;
+    for (int j = 0; j < np; ++j)
+#pragma unroll
+      for (int c = 0; c < 4; ++c) {
+        const float v = Dacc[(j * 4 + c) * nthr + l] * gain[4 * l + c];
+        jo[(size_t)j * nfreq + c * nw + l] = v;
+        if (isinf(v)) mask[j >> 5] |= 1u << (j & 31);
+      }
+  }
+  // columns whose |.| sum overflows REAL*4 are zeroed (:673-679)
+  if (mask[0]) atomicOr(&inf_mask[0], mask[0]);
+  if (mask[1]) atomicOr(&inf_mask[1], mask[1]);
+  __syncthreads();
+  if ((inf_mask[0] | inf_mask[1]) && active) {
+    float* jo = jac + (size_t)col * np * nfreq;
+    for (int j = 0; j < np; ++j)
+      if (inf_mask[j >> 5] & (1u << (j & 31)))
+#pragma unroll
+        for (int c = 0; c < 4; ++c) jo[(size_t)j * nfreq + c * nw + l] = 0.0f;
+  }
   if (status && __any_sync(__activemask(), bad) && (l & 31) == 0) atomicOr(&status[col], FZ_NAN);
 }
 
@@ -606,7 +1062,7 @@ LineP host_line(const fz_line& L, double wdif, const Consts& K) {
 
 }  // namespace
 
-constexpr int NKERN = 3;   // k_chain, k_opac, k_synth
+constexpr int NKERN = 5;   // k_chain, k_opac, k_synth, k_opac_rf, k_synth_rf
 
 struct fz_ctx {
   int device = 0;
@@ -638,8 +1094,16 @@ struct fz_ctx {
     cudaEvent_t a, b;
   };
   std::vector<Pending> pending;
-  double prof_ms[NKERN] = {0, 0, 0};
-  int prof_n[NKERN] = {0, 0, 0};
+  double prof_ms[NKERN] = {0, 0, 0, 0, 0};
+  int prof_n[NKERN] = {0, 0, 0, 0, 0};
+  // response functions: node layout, hat coefficients (nz x np), RF slab
+  RFConf rf{};
+  RFConf* d_rf = nullptr;
+  float* d_coef = nullptr;
+  float* d_rfslab = nullptr;
+  size_t rf_cols = 0;
+  float* d_jac = nullptr;   // staging of the host-buffer API
+  size_t jac_cols = 0;
 };
 
 namespace {
@@ -720,6 +1184,88 @@ int launch_forward(fz_ctx* c, int ncol, const float* d_model, int hydrostatic, d
   return 0;
 }
 
+size_t rf_smem(const fz_ctx* c) {
+  const int threads = (c->numw + 31) & ~31;
+  return ((size_t)c->nz * rf_w(c->nreg, c->nlu) + (size_t)c->nz * c->rf.np + (size_t)c->rf.np * 4 * threads) *
+         sizeof(float);
+}
+
+int launch_forward_rf(fz_ctx* c, int ncol, const float* d_model, int hydrostatic, double* d_syn, float* d_jac,
+                      float* d_mout, int* d_status, cudaStream_t s) {
+  if (c->rf.np <= 0 || !c->d_coef) return FZ_ERR_STATE;
+  int rc = ensure_scratch(c, ncol);
+  if (rc) return rc;
+  const int swr = rf_w(c->nreg, c->nlu);
+  if ((size_t)ncol > c->rf_cols) {
+    cudaFree(c->d_rfslab);
+    c->d_rfslab = nullptr;
+    c->rf_cols = 0;
+    FZ_CK(cudaMalloc(&c->d_rfslab, (size_t)ncol * c->nz * swr * sizeof(float)));
+    c->rf_cols = ncol;
+  }
+  if (d_status) FZ_CK(cudaMemsetAsync(d_status, 0, ncol * sizeof(int), s));
+  const int wpb = 4;
+  const dim3 gc((ncol + wpb - 1) / wpb);
+  {
+    ProfScope ps(c, 0, s);
+    if (hydrostatic)
+      k_chain<true><<<gc, wpb * 32, 0, s>>>(c->d_consts, c->d_pf, ncol, c->nz, d_model, d_mout, c->d_chem, d_status);
+    else
+      k_chain<false><<<gc, wpb * 32, 0, s>>>(c->d_consts, c->d_pf, ncol, c->nz, d_model, d_mout, c->d_chem, d_status);
+  }
+  FZ_CK(cudaGetLastError());
+  {
+    ProfScope ps(c, 3, s);
+    const size_t warps = (size_t)ncol * c->nz;
+    const int blocks = (int)std::min<size_t>((warps + 3) / 4, (size_t)c->nsm * 32);
+    k_opac_rf<<<blocks, 128, 0, s>>>(c->d_params, c->d_consts, ncol, d_mout, c->d_chem, c->d_rfslab);
+  }
+  FZ_CK(cudaGetLastError());
+  const int threads = (c->numw + 31) & ~31;
+  const size_t sms = rf_smem(c);
+  {
+    ProfScope ps(c, 4, s);
+    if (hydrostatic)
+      k_synth_rf<true><<<ncol, threads, sms, s>>>(c->d_params, c->d_rf, c->d_lam, c->d_gain, ncol, c->d_rfslab,
+                                                  c->d_coef, d_syn, d_jac, d_mout, d_status);
+    else
+      k_synth_rf<false><<<ncol, threads, sms, s>>>(c->d_params, c->d_rf, c->d_lam, c->d_gain, ncol, c->d_rfslab,
+                                                   c->d_coef, d_syn, d_jac, d_mout, d_status);
+  }
+  FZ_CK(cudaGetLastError());
+  return 0;
+}
+
+// GET_INT_COEFS with GET_POSITIONS (src/get_dmodel.f90:452-466, 563-644):
+// hat functions on equally spaced node positions, coef(height, node).
+bool int_coefs(int nz, int nj, std::vector<double>& coef) {
+  coef.assign((size_t)nz * nj, 0.0);
+  if (nj == 1) {
+    for (int i = 0; i < nz; ++i) coef[i] = 1.0;
+  } else if (nj < nz) {
+    std::vector<double> pos(nj);
+    const double step = (double)(nz - 1) / (double)(nj - 1);
+    for (int i = 1; i <= nj; ++i) pos[i - 1] = ((double)i - 1.0) * step + 1.0;
+    for (int j = 1; j <= nj; ++j) {
+      const double ji = pos[std::max(j - 1, 1) - 1], jf = pos[std::min(j + 1, nj) - 1], jm = pos[j - 1];
+      for (int i = 1; i <= nz; ++i) {
+        const double di = (double)i;
+        if (di < ji || di > jf) continue;
+        double v;
+        if (di == jm) v = 1.0;
+        else if (di < jm) v = 1.0 / (jm - ji) * (di - ji);
+        else v = 1.0 / (jf - jm) * (jf - di);
+        coef[(size_t)(j - 1) * nz + (i - 1)] = v;
+      }
+    }
+  } else if (nj == nz) {
+    for (int i = 0; i < nz; ++i) coef[(size_t)i * nz + i] = 1.0;
+  } else {
+    return false;
+  }
+  return true;
+}
+
 }  // namespace
 
 extern "C" {
@@ -782,6 +1328,7 @@ int fz_create(fz_ctx** out, const fz_line* lines, int nlines, const fz_region* r
       }
       const fz_line& L = lines[R.line[b]];
       P.lu[nlu] = host_line(L, b == 0 ? 0.0 : R.wdif[b], K);
+      P.lu_duv[nlu] = (float)(-1e3 * L.l0 / LIGHT);
       std::vector<double> sh, stg;
       std::vector<int> ty;
       const int n = fzh_zeeman(L, sh, stg, ty);
@@ -935,6 +1482,10 @@ int fz_destroy(fz_ctx* c) {
   cudaFree(c->d_model);
   cudaFree(c->d_syn);
   cudaFree(c->d_status);
+  cudaFree(c->d_rf);
+  cudaFree(c->d_coef);
+  cudaFree(c->d_rfslab);
+  cudaFree(c->d_jac);
   for (auto& p : c->pending) {
     cudaEventDestroy(p.a);
     cudaEventDestroy(p.b);
@@ -982,6 +1533,99 @@ int fz_forward_device(fz_ctx* c, int ncol, const float* d_model, int hydrostatic
   if (!c || ncol <= 0 || !d_model || !d_syn || !d_model_out) return FZ_ERR_ARG;
   FZ_CK(cudaSetDevice(c->device));
   return launch_forward(c, ncol, d_model, hydrostatic, d_syn, d_model_out, d_status, (cudaStream_t)stream);
+}
+
+int fz_rf_nodes(fz_ctx* c, const int* nodes) {
+  if (!c || !nodes) return FZ_ERR_ARG;
+  // reference parameter (1-based) of each slot; rho (3) and P0 (8) are not supported
+  static const int kRef[NSLOT] = {1, 2, 4, 5, 6, 7};
+  if (nodes[2] != 0 || nodes[7] != 0) return FZ_ERR_ARG;
+  RFConf rf{};
+  int np = 0;
+  for (int p = 0; p < NSLOT; ++p) {
+    const int nj = nodes[kRef[p] - 1];
+    if (nj < 0 || nj > c->nz) return FZ_ERR_ARG;
+    rf.n0[p] = np;
+    rf.nj[p] = nj;
+    np += nj;
+  }
+  if (np <= 0) return FZ_ERR_ARG;
+  if (np > MAXNP) return FZ_ERR_LIMIT;
+  rf.np = np;
+  std::vector<float> tab((size_t)c->nz * np, 0.0f);
+  std::vector<double> cf;
+  for (int p = 0; p < NSLOT; ++p) {
+    if (rf.nj[p] == 0) continue;
+    int_coefs(c->nz, rf.nj[p], cf);
+    for (int j = 0; j < rf.nj[p]; ++j)
+      for (int k = 0; k < c->nz; ++k) tab[(size_t)k * np + rf.n0[p] + j] = (float)cf[(size_t)j * c->nz + k];
+  }
+  c->rf.np = 0;
+  FZ_CK(cudaSetDevice(c->device));
+  FZ_CK(cudaStreamSynchronize(c->stream));
+  cudaFree(c->d_coef);
+  c->d_coef = nullptr;
+  if (!c->d_rf) FZ_CK(cudaMalloc(&c->d_rf, sizeof(RFConf)));
+  FZ_CK(cudaMalloc(&c->d_coef, tab.size() * sizeof(float)));
+  FZ_CK(cudaMemcpy(c->d_coef, tab.data(), tab.size() * sizeof(float), cudaMemcpyHostToDevice));
+  FZ_CK(cudaMemcpy(c->d_rf, &rf, sizeof(RFConf), cudaMemcpyHostToDevice));
+  c->rf = rf;
+  const size_t sms = rf_smem(c);
+  int maxsm = 0;
+  FZ_CK(cudaDeviceGetAttribute(&maxsm, cudaDevAttrMaxSharedMemoryPerBlockOptin, c->device));
+  if (sms > (size_t)maxsm) {
+    c->rf.np = 0;
+    return FZ_ERR_LIMIT;
+  }
+  FZ_CK(cudaFuncSetAttribute(k_synth_rf<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sms));
+  FZ_CK(cudaFuncSetAttribute(k_synth_rf<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sms));
+  return np;
+}
+
+int fz_forward_rf_device(fz_ctx* c, int ncol, const float* d_model, int hydrostatic, double* d_syn, float* d_jac,
+                         float* d_model_out, int* d_status, void* stream) {
+  if (!c || ncol <= 0 || !d_model || !d_syn || !d_jac || !d_model_out) return FZ_ERR_ARG;
+  FZ_CK(cudaSetDevice(c->device));
+  return launch_forward_rf(c, ncol, d_model, hydrostatic, d_syn, d_jac, d_model_out, d_status, (cudaStream_t)stream);
+}
+
+int fz_forward_rf(fz_ctx* c, int ncol, const float* model, int hydrostatic, double* syn, float* jac, float* model_out,
+                  int* status) {
+  if (!c || ncol <= 0 || !model || !syn || !jac) return FZ_ERR_ARG;
+  if (c->rf.np <= 0) return FZ_ERR_STATE;
+  FZ_CK(cudaSetDevice(c->device));
+  if ((size_t)ncol > c->io_cols) {
+    cudaFree(c->d_model);
+    cudaFree(c->d_syn);
+    cudaFree(c->d_status);
+    c->d_model = nullptr;
+    c->d_syn = nullptr;
+    c->d_status = nullptr;
+    c->io_cols = 0;
+    FZ_CK(cudaMalloc(&c->d_model, (size_t)ncol * 13 * c->nz * sizeof(float)));
+    FZ_CK(cudaMalloc(&c->d_syn, (size_t)ncol * 4 * c->numw * sizeof(double)));
+    FZ_CK(cudaMalloc(&c->d_status, (size_t)ncol * sizeof(int)));
+    c->io_cols = ncol;
+  }
+  const size_t jb = (size_t)ncol * c->rf.np * 4 * c->numw * sizeof(float);
+  if ((size_t)ncol * c->rf.np > c->jac_cols) {
+    cudaFree(c->d_jac);
+    c->d_jac = nullptr;
+    c->jac_cols = 0;
+    FZ_CK(cudaMalloc(&c->d_jac, jb));
+    c->jac_cols = (size_t)ncol * c->rf.np;
+  }
+  cudaStream_t s = c->stream;
+  const size_t mb = (size_t)ncol * 13 * c->nz * sizeof(float);
+  FZ_CK(cudaMemcpyAsync(c->d_model, model, mb, cudaMemcpyHostToDevice, s));
+  int rc = launch_forward_rf(c, ncol, c->d_model, hydrostatic, c->d_syn, c->d_jac, c->d_model, c->d_status, s);
+  if (rc) return rc;
+  FZ_CK(cudaMemcpyAsync(syn, c->d_syn, (size_t)ncol * 4 * c->numw * sizeof(double), cudaMemcpyDeviceToHost, s));
+  FZ_CK(cudaMemcpyAsync(jac, c->d_jac, jb, cudaMemcpyDeviceToHost, s));
+  if (model_out) FZ_CK(cudaMemcpyAsync(model_out, c->d_model, mb, cudaMemcpyDeviceToHost, s));
+  if (status) FZ_CK(cudaMemcpyAsync(status, c->d_status, ncol * sizeof(int), cudaMemcpyDeviceToHost, s));
+  FZ_CK(cudaStreamSynchronize(s));
+  return 0;
 }
 
 }  // extern "C"

@@ -354,12 +354,12 @@ __device__ __forceinline__ void voigt_f32(float a, float u, float& H, float& F) 
 }
 
 // Evolution operator O of one layer from its optical-depth increments
-// t = eta*dz (src/rtesolver.f90:269-473).  The reference's clamp of cosh and
+// t = eta*dz (src/rtesolver.f90:269-473), and om0 = 1 - O(1,1).  The reference's clamp of cosh and
 // sinh at 2^53 (-> 1e15, :464-465) is reproduced; below it the operator is
 // evaluated with cancellation-free forms (cosh x -+ cos y via sinh^2(x/2),
 // sin^2(y/2); lambda_1,2 from the larger root).
 __device__ __forceinline__ void evol_f32(float tI, float tQ, float tU, float tV, float rQ, float rU, float rV,
-                                         float O[16]) {
+                                         float O[16], float& om0) {
   const float eta2 = tQ * tQ + tU * tU + tV * tV;
   const float rho2 = rQ * rQ + rU * rU + rV * rV;
   const float er = tQ * rQ + tU * rU + tV * rV;
@@ -395,6 +395,7 @@ __device__ __forceinline__ void evol_f32(float tI, float tQ, float tU, float tV,
   const float E = expf(-tI);
   float P, Qm, sh, s2v;
   const float XCLAMP = 37.42994775f;   // cosh, sinh >= 2^53 in float64
+  float amb = 0.0f;                    // sinh^2(x/2) - sin^2(y/2) = P - 1
   s2v = sinf(y);
   if (x >= XCLAMP) {
     const float c2 = cosf(y);
@@ -404,12 +405,16 @@ __device__ __forceinline__ void evol_f32(float tI, float tQ, float tU, float tV,
   } else {
     const float shx = sinhf(0.5f * x), siy = sinf(0.5f * y);
     const float a = shx * shx, b = siy * siy;
-    P = 1.0f + a - b;
+    amb = a - b;
+    P = 1.0f + amb;
     Qm = a + b;
     sh = sinhf(x);
   }
   const float eP = E * P, eQ = E * Qm, eS = E * s2v, eH = E * sh;
   O[0] = eP + eQ * m4_11;
+  // 1 - O(1,1) without cancellation in optically thin layers:
+  // (1 - e^-tI) - e^-tI (P - 1 + Qm M4(1,1))
+  om0 = (x >= XCLAMP) ? 1.0f - O[0] : -expm1f(-tI) - E * (amb + Qm * m4_11);
   O[5] = eP + eQ * m4_22;
   O[10] = eP + eQ * m4_33;
   O[15] = eP + eQ * m4_44;

@@ -125,10 +125,35 @@ int fz_forward_device(fz_ctx* ctx, int ncol, const float* d_model, int hydrostat
 int fz_forward_device_static(fz_ctx* ctx, int ncol, const float* d_model, int hydrostatic, double* d_syn,
                              float* d_model_out, int* d_status, void* stream);
 
+/* Response functions.  fz_rf_nodes selects the free parameters and their
+ * node counts, nodes[p-1] for the reference parameter p of atm_param.f90
+ * (1 T, 2 Pg, 4 Bx, 5 By, 6 Bz, 7 v_z; 3 rho and 8 P0 must be 0); the hat
+ * interpolation of GET_INT_COEFS (src/get_dmodel.f90:563-644) maps nodes to
+ * heights, so nodes[p-1] == nz gives the response at every height.  Returns
+ * NP = sum of the node counts (<= 64) or a negative error.  Replaces the node
+ * set-up of UPDATE_COEFS (src/get_dmodel.f90:648-721). */
+int fz_rf_nodes(fz_ctx* ctx, const int* nodes /* [8] */);
+
+/* Forward synthesis with response functions: as fz_forward plus the node
+ * Jacobian EQVDSYN(NFREQ, NP) of every column, REAL*4, Stokes-major rows
+ * (I,Q,U,V blocks of NUMW) x GAIN, parameters in reference order with their
+ * nodes -- FORWARD1D with MRESPFUNCT followed by OLD_DSYN_PROPAGATION and
+ * CALCULATE_EQUIVALENT_DSYN (src/forward.f90:511-681, :857-1029).  jac is
+ * (NFREQ, NP, ncol).  With hydrostatic != 0 the T response carries the
+ * reference's global term through the pressure stratification and the B and
+ * v_z responses use the layer's outgoing Stokes vector, as the reference's
+ * OLD_ANALYTICAL_SOLVER does (src/rtesolver.f90:218-260).  FZ_ERR_STATE if
+ * fz_rf_nodes was not called. */
+int fz_forward_rf(fz_ctx* ctx, int ncol, const float* model, int hydrostatic, double* syn, float* jac,
+                  float* model_out, int* status);
+int fz_forward_rf_device(fz_ctx* ctx, int ncol, const float* d_model, int hydrostatic, double* d_syn,
+                         float* d_jac, float* d_model_out, int* d_status, void* stream);
+
 /* Per-kernel timing: when enabled, every launch of the context is bracketed
  * by CUDA events on its stream; fz_profile_read returns the accumulated
  * milliseconds and launch counts of the kernels (names in order:
- * "k_chain", "k_opac", "k_synth") and resets them; returns the kernel count.  Replaces the reference's
+ * "k_chain", "k_opac", "k_synth", "k_opac_rf", "k_synth_rf") and resets
+ * them; returns the kernel count.  Replaces the reference's
  * SYSTEM_CLOCK "Forward 3D:" timer (src/forward.f90:99-100, :295-297). */
 int fz_profile_enable(fz_ctx* ctx, int on);
 int fz_profile_read(fz_ctx* ctx, double* ms, int* launches, int n);
