@@ -57,6 +57,16 @@ class FzError(RuntimeError):
     pass
 
 
+class LMOpts(ctypes.Structure):
+    """fz_lm_opts: stop rules and weights of the batched inversion."""
+    _fields_ = [("maxsteps", ctypes.c_int), ("maxit", ctypes.c_int), ("dchi2", ctypes.c_double),
+                ("svdtol", ctypes.c_double), ("isigma", ctypes.c_double), ("wstk", ctypes.c_float * 4),
+                ("slots", ctypes.c_int), ("pad", ctypes.c_int)]
+
+    def __init__(self, maxsteps=5, maxit=40, dchi2=0.0, svdtol=1e-4, isigma=4e-3, wstk=(1, 1, 1, 1), slots=0):
+        super().__init__(maxsteps, maxit, dchi2, svdtol, isigma, (ctypes.c_float * 4)(*wstk), slots, 0)
+
+
 _lib = None
 
 
@@ -91,6 +101,9 @@ def lib():
         L.fz_rf_nodes.argtypes = [P, P]
         L.fz_forward_rf.argtypes = [P, ctypes.c_int, P, ctypes.c_int, P, P, P, P]
         L.fz_forward_rf_device.argtypes = [P, ctypes.c_int, P, ctypes.c_int, P, P, P, P, P]
+        L.fz_invert.argtypes = [P, ctypes.c_int, P, P, ctypes.c_int, P, P, P, P, P, P]
+        L.fz_invert_device.argtypes = [P, ctypes.c_int, P, P, ctypes.c_int, P, P, P, P, P, P, P]
+        L.fz_lm_perturbation.argtypes = [P, ctypes.c_int, ctypes.c_int, ctypes.c_int, P, P, P, ctypes.c_double, P]
         _lib = L
     return _lib
 
@@ -240,6 +253,48 @@ class Synthesis:
         st = np.zeros(ncol, dtype=np.int32)
         _check(lib().fz_forward_rf(self._h, ncol, _p(m), int(bool(hydrostatic)), _p(syn), _p(jac), _p(mo), _p(st)))
         return syn, jac, mo, st
+
+    def invert(self, obs, init, hydrostatic=True, opts=None, want_syn=False):
+        """Batched LM inversion of host-resident pixels with the node layout of
+        rf_nodes().  obs: (npix, 4, numw) float64 GAIN-normalised Stokes;
+        init: (npix, 13, nz) float32 initial models.  Returns (best models,
+        chi2, iterations, status[, best synthesis])."""
+        o = np.ascontiguousarray(obs, dtype=np.float64)
+        m = np.ascontiguousarray(init, dtype=np.float32)
+        npix = o.shape[0]
+        if o.shape[1:] != (4, self.numw) or m.shape != (npix, 13, self.nz):
+            raise ValueError("obs must be (npix, 4, numw) and init (npix, 13, nz)")
+        opts = opts or LMOpts()
+        mo = np.empty_like(m)
+        chi = np.zeros(npix)
+        it = np.zeros(npix, dtype=np.int32)
+        st = np.zeros(npix, dtype=np.int32)
+        syn = np.zeros_like(o) if want_syn else None
+        _check(lib().fz_invert(self._h, npix, _p(o), _p(m), int(bool(hydrostatic)), ctypes.byref(opts), _p(mo),
+                               _p(chi), _p(it), None if syn is None else _p(syn), _p(st)))
+        return (mo, chi, it, st, syn) if want_syn else (mo, chi, it, st)
+
+    def invert_device(self, npix, obs_ptr, init_ptr, model_out_ptr, chi2_ptr, iters_ptr, status_ptr=0, syn_ptr=0,
+                      hydrostatic=True, opts=None, stream=0):
+        """Batched LM inversion on device pointers."""
+        opts = opts or LMOpts()
+        _check(lib().fz_invert_device(self._h, int(npix), ctypes.c_void_p(obs_ptr), ctypes.c_void_p(init_ptr),
+                                      int(bool(hydrostatic)), ctypes.byref(opts), ctypes.c_void_p(model_out_ptr),
+                                      ctypes.c_void_p(chi2_ptr), ctypes.c_void_p(iters_ptr),
+                                      ctypes.c_void_p(syn_ptr) if syn_ptr else None,
+                                      ctypes.c_void_p(status_ptr) if status_ptr else None,
+                                      ctypes.c_void_p(stream) if stream else None))
+
+    def lm_perturbation(self, jac, diff, lam, svdtol=1e-4):
+        """Batched GET_PERTURBATION: jac (npix, np, nfreq) normalised Jacobian,
+        diff (npix, nfreq), lam (npix,).  Returns delta (npix, np)."""
+        j = np.ascontiguousarray(jac, dtype=np.float32)
+        d = np.ascontiguousarray(diff, dtype=np.float64)
+        lm = np.ascontiguousarray(lam, dtype=np.float64)
+        npix, npar, nf = j.shape
+        out = np.zeros((npix, npar))
+        _check(lib().fz_lm_perturbation(self._h, npix, npar, nf, _p(j), _p(d), _p(lm), float(svdtol), _p(out)))
+        return out
 
     def forward_rf_device(self, model_ptr, ncol, syn_ptr, jac_ptr, model_out_ptr, status_ptr=0, stream=0,
                           hydrostatic=False):

@@ -14,6 +14,7 @@
 //            the Zeeman-split Voigt/Faraday profiles, the 4x4 evolution
 //            operator and the formal-solution recurrence, writes RSYN1D; one
 //            thread integrates log tau5.
+#include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
 #include <cmath>
@@ -820,6 +821,12 @@ __global__ void __launch_bounds__(256) k_synth_rf(const DevParams* __restrict__ 
   if (status && __any_sync(__activemask(), bad) && (l & 31) == 0) atomicOr(&status[col], FZ_NAN);
 }
 
+}  // namespace
+
+#include "fz_lm.cuh"
+
+namespace {
+
 // ------------------------------------------------------------------ k_gain
 // HSRA continuum normalisation, src/normalization.f90:696-754: one block;
 // warp 0 runs the chemistry of the 387 layers (nelec chain), then every
@@ -1104,6 +1111,13 @@ struct fz_ctx {
   size_t rf_cols = 0;
   float* d_jac = nullptr;   // staging of the host-buffer API
   size_t jac_cols = 0;
+  double* d_coef64 = nullptr;   // (nz, np) hat table in FP64 for the LM update
+  // LM slot pool (grown on demand)
+  LMSlots lm{};
+  size_t lm_cap = 0;
+  int lm_np = 0;
+  LMQueue* d_q = nullptr;
+  int* h_done = nullptr;   // pinned
 };
 
 namespace {
@@ -1233,6 +1247,100 @@ int launch_forward_rf(fz_ctx* c, int ncol, const float* d_model, int hydrostatic
                                                    c->d_coef, d_syn, d_jac, d_mout, d_status);
   }
   FZ_CK(cudaGetLastError());
+  return 0;
+}
+
+void lm_free(fz_ctx* c) {
+  LMSlots& L = c->lm;
+  cudaFree(L.pix);
+  cudaFree(L.skip);
+  cudaFree(L.iter);
+  cudaFree(L.st);
+  cudaFree(L.mcur);
+  cudaFree(L.mbest);
+  cudaFree(L.syn);
+  cudaFree(L.synb);
+  cudaFree(L.jac);
+  cudaFree(L.jacb);
+  cudaFree(L.obs);
+  cudaFree(L.diff);
+  cudaFree(L.H);
+  cudaFree(L.g);
+  cudaFree(L.delta);
+  cudaFree(L.status);
+  L = LMSlots{};
+  c->lm_cap = 0;
+}
+
+// slot pool for S slots of the current node layout
+int lm_alloc(fz_ctx* c, int S) {
+  const int np = c->rf.np, nf = 4 * c->numw, nm = 13 * c->nz;
+  if ((size_t)S <= c->lm_cap && c->lm.S == S && c->lm_np == np) return 0;
+  lm_free(c);
+  c->lm_np = np;
+  LMSlots& L = c->lm;
+  L.S = S;
+  FZ_CK(cudaMalloc(&L.pix, S * sizeof(int)));
+  FZ_CK(cudaMalloc(&L.skip, S * sizeof(int)));
+  FZ_CK(cudaMalloc(&L.iter, S * sizeof(int)));
+  FZ_CK(cudaMalloc(&L.st, 5 * (size_t)S * sizeof(double)));
+  FZ_CK(cudaMalloc(&L.mcur, (size_t)S * nm * sizeof(float)));
+  FZ_CK(cudaMalloc(&L.mbest, (size_t)S * nm * sizeof(float)));
+  FZ_CK(cudaMalloc(&L.syn, (size_t)S * nf * sizeof(double)));
+  FZ_CK(cudaMalloc(&L.synb, (size_t)S * nf * sizeof(double)));
+  FZ_CK(cudaMalloc(&L.jac, (size_t)S * np * nf * sizeof(float)));
+  FZ_CK(cudaMalloc(&L.jacb, (size_t)S * np * nf * sizeof(float)));
+  FZ_CK(cudaMalloc(&L.obs, (size_t)S * nf * sizeof(double)));
+  FZ_CK(cudaMalloc(&L.diff, (size_t)S * nf * sizeof(double)));
+  FZ_CK(cudaMalloc(&L.H, (size_t)S * np * np * sizeof(double)));
+  FZ_CK(cudaMalloc(&L.g, (size_t)S * np * sizeof(double)));
+  FZ_CK(cudaMalloc(&L.delta, (size_t)S * np * sizeof(double)));
+  FZ_CK(cudaMalloc(&L.status, (size_t)S * sizeof(int)));
+  c->lm_cap = S;
+  return 0;
+}
+
+// ISIGMAP of SET_WEIGHTS (src/get_dmodel.f90:2024-2047) with the WSTK
+// normalisation of src/input_file.f90:1298-1303, all Stokes inverted.
+std::vector<double> lm_weights(int numw, const float wstk[4], double isigma) {
+  float ss = 0.0f;
+  for (int i = 0; i < 4; ++i) ss += wstk[i] * wstk[i];
+  const float minw = std::sqrt(ss) / std::sqrt(4.0f);
+  std::vector<double> w(4 * (size_t)numw);
+  for (int i = 0; i < 4; ++i) {
+    const float wi = wstk[i] / minw;
+    for (int l = 0; l < numw; ++l) w[(size_t)i * numw + l] = (double)(wi * wi) / (isigma * isigma);
+  }
+  return w;
+}
+
+int lm_conf(fz_ctx* c, int npix, const fz_lm_opts* o, LMConf& C) {
+  if (c->rf.np <= 0) return FZ_ERR_STATE;
+  if (c->rf.np > LM_MAXNP) return FZ_ERR_LIMIT;
+  static const int kRef[NSLOT] = {1, 2, 4, 5, 6, 7};
+  static const int kRow[9] = {0, 0, 1, 2, 5, 6, 7, 10, 1};   // model row of reference parameter 1..8
+  std::memset(&C, 0, sizeof(C));
+  C.np = c->rf.np;
+  C.nfreq = 4 * c->numw;
+  C.nz = c->nz;
+  C.npix = npix;
+  C.maxsteps = o && o->maxsteps > 0 ? o->maxsteps : 5;
+  C.maxit = o && o->maxit > 0 ? o->maxit : 40;
+  C.dchi2 = o ? o->dchi2 : 0.0;
+  C.svdtol = o && o->svdtol > 0 ? o->svdtol : 1.0e-4;
+  C.inu = (double)C.nfreq;
+  const double norms[8] = {6000.0, 1.0e5, 1.0e-5, 1.0e3, 1.0e3, 1.0e3, 1.0e6, 6.0e2};
+  // nodes in reference parameter order (the slot order of the Jacobian)
+  for (int p = 0; p < NSLOT; ++p) {
+    const int rp = kRef[p];
+    C.nodes_ref[rp - 1] = c->rf.nj[p];
+    for (int j = 0; j < c->rf.nj[p]; ++j) {
+      const int n = c->rf.n0[p] + j;
+      C.row_of[n] = kRow[rp];
+      C.par_of[n] = rp;
+      C.norm[n] = norms[rp - 1];
+    }
+  }
   return 0;
 }
 
@@ -1486,6 +1594,10 @@ int fz_destroy(fz_ctx* c) {
   cudaFree(c->d_coef);
   cudaFree(c->d_rfslab);
   cudaFree(c->d_jac);
+  cudaFree(c->d_coef64);
+  lm_free(c);
+  cudaFree(c->d_q);
+  if (c->h_done) cudaFreeHost(c->h_done);
   for (auto& p : c->pending) {
     cudaEventDestroy(p.a);
     cudaEventDestroy(p.b);
@@ -1568,6 +1680,19 @@ int fz_rf_nodes(fz_ctx* c, const int* nodes) {
   if (!c->d_rf) FZ_CK(cudaMalloc(&c->d_rf, sizeof(RFConf)));
   FZ_CK(cudaMalloc(&c->d_coef, tab.size() * sizeof(float)));
   FZ_CK(cudaMemcpy(c->d_coef, tab.data(), tab.size() * sizeof(float), cudaMemcpyHostToDevice));
+  {
+    std::vector<double> t64((size_t)c->nz * np, 0.0);
+    for (int p = 0; p < NSLOT; ++p) {
+      if (rf.nj[p] == 0) continue;
+      int_coefs(c->nz, rf.nj[p], cf);
+      for (int j = 0; j < rf.nj[p]; ++j)
+        for (int k = 0; k < c->nz; ++k) t64[(size_t)k * np + rf.n0[p] + j] = cf[(size_t)j * c->nz + k];
+    }
+    cudaFree(c->d_coef64);
+    c->d_coef64 = nullptr;
+    FZ_CK(cudaMalloc(&c->d_coef64, t64.size() * sizeof(double)));
+    FZ_CK(cudaMemcpy(c->d_coef64, t64.data(), t64.size() * sizeof(double), cudaMemcpyHostToDevice));
+  }
   FZ_CK(cudaMemcpy(c->d_rf, &rf, sizeof(RFConf), cudaMemcpyHostToDevice));
   c->rf = rf;
   const size_t sms = rf_smem(c);
@@ -1587,6 +1712,148 @@ int fz_forward_rf_device(fz_ctx* c, int ncol, const float* d_model, int hydrosta
   if (!c || ncol <= 0 || !d_model || !d_syn || !d_jac || !d_model_out) return FZ_ERR_ARG;
   FZ_CK(cudaSetDevice(c->device));
   return launch_forward_rf(c, ncol, d_model, hydrostatic, d_syn, d_jac, d_model_out, d_status, (cudaStream_t)stream);
+}
+
+int fz_invert_device(fz_ctx* c, int npix, const double* d_obs, const float* d_init, int hydrostatic,
+                     const fz_lm_opts* opts, float* d_model_out, double* d_chi2, int* d_iters, double* d_syn_out,
+                     int* d_status, void* stream) {
+  if (!c || npix <= 0 || !d_obs || !d_init || !d_model_out || !d_chi2 || !d_iters) return FZ_ERR_ARG;
+  FZ_CK(cudaSetDevice(c->device));
+  LMConf C;
+  int rc = lm_conf(c, npix, opts, C);
+  if (rc) return rc;
+  int S = (opts && opts->slots > 0) ? opts->slots : 8192;
+  if (S > npix) S = npix;
+  if ((rc = lm_alloc(c, S))) return rc;
+  cudaStream_t s = (cudaStream_t)stream;
+  if (!c->d_q) FZ_CK(cudaMalloc(&c->d_q, sizeof(LMQueue)));
+  if (!c->h_done) FZ_CK(cudaMallocHost(&c->h_done, sizeof(int)));
+  static const float kW1[4] = {1.f, 1.f, 1.f, 1.f};
+  const std::vector<double> w =
+      lm_weights(c->numw, opts ? opts->wstk : kW1, (opts && opts->isigma > 0) ? opts->isigma : 4.0e-3);
+  double* d_w = nullptr;
+  FZ_CK(cudaMalloc(&d_w, w.size() * sizeof(double)));
+  struct Free {
+    double* p;
+    ~Free() { cudaFree(p); }
+  } fw{d_w};
+  FZ_CK(cudaMemcpyAsync(d_w, w.data(), w.size() * sizeof(double), cudaMemcpyHostToDevice, s));
+  FZ_CK(cudaMemsetAsync(c->d_q, 0, sizeof(LMQueue), s));
+  if (d_status) FZ_CK(cudaMemsetAsync(d_status, 0, npix * sizeof(int), s));
+  const LMSlots L = c->lm;
+  k_lm_fill<<<S, 128, 0, s>>>(C, L, c->d_q, d_obs, d_init);
+  FZ_CK(cudaGetLastError());
+  const size_t usm = (size_t)(C.nz + 3 * C.np) * sizeof(double) + (size_t)C.nz * sizeof(float);
+  // every pixel needs at most maxit iterations; slots are refilled at once
+  const long long cap = (long long)C.maxit * ((npix + S - 1) / S + 1) + 8;
+  for (long long it = 0; it < cap; ++it) {
+    if ((rc = launch_forward_rf(c, S, L.mcur, hydrostatic, L.syn, L.jac, L.mcur, L.status, s))) return rc;
+    k_lm_accept<<<S, 256, 0, s>>>(C, L, c->d_q, d_w, d_obs, d_init, d_model_out, d_chi2, d_iters, d_syn_out,
+                                  d_status);
+    k_lm_normal<<<(S + 3) / 4, 128, 0, s>>>(C, L, d_w);
+    k_lm_solve<<<(S + 3) / 4, 128, 0, s>>>(C, L);
+    k_lm_update<<<S, 128, usm, s>>>(C, L, c->d_coef64);
+    FZ_CK(cudaGetLastError());
+    FZ_CK(cudaMemcpyAsync(c->h_done, &c->d_q->done, sizeof(int), cudaMemcpyDeviceToHost, s));
+    FZ_CK(cudaStreamSynchronize(s));
+    if (*c->h_done >= npix) return 0;
+  }
+  return FZ_ERR_STATE;
+}
+
+int fz_invert(fz_ctx* c, int npix, const double* obs, const float* init, int hydrostatic, const fz_lm_opts* opts,
+              float* model_out, double* chi2, int* iters, double* syn_out, int* status) {
+  if (!c || npix <= 0 || !obs || !init || !model_out || !chi2 || !iters) return FZ_ERR_ARG;
+  FZ_CK(cudaSetDevice(c->device));
+  const size_t nf = 4 * (size_t)c->numw, nm = 13 * (size_t)c->nz;
+  double *d_obs = nullptr, *d_chi = nullptr, *d_syn = nullptr;
+  float *d_init = nullptr, *d_out = nullptr;
+  int *d_it = nullptr, *d_st = nullptr;
+  int rc = 0;
+  cudaStream_t s = c->stream;
+  do {
+    if ((rc = cuda_fail(cudaMalloc(&d_obs, npix * nf * sizeof(double))))) break;
+    if ((rc = cuda_fail(cudaMalloc(&d_init, npix * nm * sizeof(float))))) break;
+    if ((rc = cuda_fail(cudaMalloc(&d_out, npix * nm * sizeof(float))))) break;
+    if ((rc = cuda_fail(cudaMalloc(&d_chi, npix * sizeof(double))))) break;
+    if ((rc = cuda_fail(cudaMalloc(&d_it, npix * sizeof(int))))) break;
+    if ((rc = cuda_fail(cudaMalloc(&d_st, npix * sizeof(int))))) break;
+    if (syn_out && (rc = cuda_fail(cudaMalloc(&d_syn, npix * nf * sizeof(double))))) break;
+    if ((rc = cuda_fail(cudaMemcpyAsync(d_obs, obs, npix * nf * sizeof(double), cudaMemcpyHostToDevice, s)))) break;
+    if ((rc = cuda_fail(cudaMemcpyAsync(d_init, init, npix * nm * sizeof(float), cudaMemcpyHostToDevice, s)))) break;
+    if ((rc = fz_invert_device(c, npix, d_obs, d_init, hydrostatic, opts, d_out, d_chi, d_it, d_syn, d_st, s))) break;
+    if ((rc = cuda_fail(cudaMemcpyAsync(model_out, d_out, npix * nm * sizeof(float), cudaMemcpyDeviceToHost, s)))) break;
+    if ((rc = cuda_fail(cudaMemcpyAsync(chi2, d_chi, npix * sizeof(double), cudaMemcpyDeviceToHost, s)))) break;
+    if ((rc = cuda_fail(cudaMemcpyAsync(iters, d_it, npix * sizeof(int), cudaMemcpyDeviceToHost, s)))) break;
+    if (status && (rc = cuda_fail(cudaMemcpyAsync(status, d_st, npix * sizeof(int), cudaMemcpyDeviceToHost, s))))
+      break;
+    if (syn_out &&
+        (rc = cuda_fail(cudaMemcpyAsync(syn_out, d_syn, npix * nf * sizeof(double), cudaMemcpyDeviceToHost, s))))
+      break;
+    rc = cuda_fail(cudaStreamSynchronize(s));
+  } while (false);
+  cudaFree(d_obs);
+  cudaFree(d_init);
+  cudaFree(d_out);
+  cudaFree(d_chi);
+  cudaFree(d_it);
+  cudaFree(d_st);
+  cudaFree(d_syn);
+  return rc;
+}
+
+int fz_lm_perturbation(fz_ctx* c, int npix, int np, int nfreq, const float* jac, const double* diff,
+                       const double* lambda, double svdtol, double* delta) {
+  if (!c || npix <= 0 || np <= 0 || np > LM_MAXNP || nfreq <= 0 || (nfreq & 3) || !jac || !diff || !lambda || !delta)
+    return FZ_ERR_ARG;
+  FZ_CK(cudaSetDevice(c->device));
+  LMConf C;
+  std::memset(&C, 0, sizeof(C));
+  C.np = np;
+  C.nfreq = nfreq;
+  C.inu = 1.0;
+  C.svdtol = svdtol > 0 ? svdtol : 1.0e-4;
+  for (int j = 0; j < np; ++j) C.norm[j] = 1.0;
+  LMSlots L{};
+  L.S = npix;
+  std::vector<int> zeros(npix, 0);
+  std::vector<double> st(5 * (size_t)npix, 0.0);
+  for (int i = 0; i < npix; ++i) st[5 * (size_t)i + 2] = lambda[i];
+  std::vector<double> ones(nfreq, 1.0);
+  double* d_w = nullptr;
+  int rc = 0;
+  do {
+    if ((rc = cuda_fail(cudaMalloc(&L.pix, npix * sizeof(int))))) break;
+    if ((rc = cuda_fail(cudaMalloc(&L.skip, npix * sizeof(int))))) break;
+    if ((rc = cuda_fail(cudaMalloc(&L.st, st.size() * sizeof(double))))) break;
+    if ((rc = cuda_fail(cudaMalloc(&L.jacb, (size_t)npix * np * nfreq * sizeof(float))))) break;
+    if ((rc = cuda_fail(cudaMalloc(&L.diff, (size_t)npix * nfreq * sizeof(double))))) break;
+    if ((rc = cuda_fail(cudaMalloc(&L.H, (size_t)npix * np * np * sizeof(double))))) break;
+    if ((rc = cuda_fail(cudaMalloc(&L.g, (size_t)npix * np * sizeof(double))))) break;
+    if ((rc = cuda_fail(cudaMalloc(&L.delta, (size_t)npix * np * sizeof(double))))) break;
+    if ((rc = cuda_fail(cudaMalloc(&d_w, nfreq * sizeof(double))))) break;
+    cudaMemcpy(L.pix, zeros.data(), npix * sizeof(int), cudaMemcpyHostToDevice);
+    cudaMemcpy(L.skip, zeros.data(), npix * sizeof(int), cudaMemcpyHostToDevice);
+    cudaMemcpy(L.st, st.data(), st.size() * sizeof(double), cudaMemcpyHostToDevice);
+    cudaMemcpy(L.jacb, jac, (size_t)npix * np * nfreq * sizeof(float), cudaMemcpyHostToDevice);
+    cudaMemcpy(L.diff, diff, (size_t)npix * nfreq * sizeof(double), cudaMemcpyHostToDevice);
+    cudaMemcpy(d_w, ones.data(), nfreq * sizeof(double), cudaMemcpyHostToDevice);
+    k_lm_normal<<<(npix + 3) / 4, 128, 0, c->stream>>>(C, L, d_w);
+    k_lm_solve<<<(npix + 3) / 4, 128, 0, c->stream>>>(C, L);
+    if ((rc = cuda_fail(cudaGetLastError()))) break;
+    if ((rc = cuda_fail(cudaStreamSynchronize(c->stream)))) break;
+    rc = cuda_fail(cudaMemcpy(delta, L.delta, (size_t)npix * np * sizeof(double), cudaMemcpyDeviceToHost));
+  } while (false);
+  cudaFree(L.pix);
+  cudaFree(L.skip);
+  cudaFree(L.st);
+  cudaFree(L.jacb);
+  cudaFree(L.diff);
+  cudaFree(L.H);
+  cudaFree(L.g);
+  cudaFree(L.delta);
+  cudaFree(d_w);
+  return rc;
 }
 
 int fz_forward_rf(fz_ctx* c, int ncol, const float* model, int hydrostatic, double* syn, float* jac, float* model_out,

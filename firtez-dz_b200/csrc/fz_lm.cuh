@@ -1,0 +1,484 @@
+// Batched pixel-wise Levenberg-Marquardt (sm_100a), included by fz_cuda.cu.
+//
+// One inversion = a pool of S slots, each holding one pixel: its observed
+// Stokes vector, current and best model, synthesis and node Jacobian, and the
+// LM state of the reference (INV_SLA(1:9), src/invert3d.f90:275-286).  Every
+// iteration runs, on all slots:
+//   forward synthesis + node Jacobian of the current models (k_chain,
+//   k_opac_rf, k_synth_rf);
+//   k_lm_accept   chi2, accept/revert, lambda update (NEW_CALCULATE_CHI2,
+//                 UPDATE_LAMBDA, src/get_dmodel.f90:917-1032), the weighted
+//                 residual, the per-pixel stop rule; a finished pixel writes
+//                 its best model out and its slot takes the next pixel of
+//                 the work queue (a device counter);
+//   k_lm_normal   H = Jn^T Jn on the tensor cores (mma.sync bf16, the FP32
+//                 Jacobian split in hi + lo bf16 parts, hi*hi + hi*lo + lo*hi
+//                 accumulated in FP32) and g = Jn^T r in FP64, Jn the
+//                 normalised Jacobian of NORMALIZE_JACOB (:725-770);
+//   k_lm_solve    one warp per pixel, FP64: (H + lambda diag H)^+ g by a
+//                 one-sided Jacobi SVD with the reference's relative cut
+//                 (GET_PERTURBATION/GET_INVERSE, src/lm.f90:61-204);
+//   k_lm_update   REARANGE_DA_MODEL / SORT_DELTA_TO_ATMOSPHERE
+//                 (:1715-2016): node clipping, SIR-like expansion, limits,
+//                 the log tau5 taper of T.
+#pragma once
+
+namespace {
+
+constexpr int LM_MAXNP = 16;    // tensor-core tile of the normal equations
+constexpr int LM_PAD = -1;      // empty slot
+constexpr int LM_SKIP = 1;      // slot refilled this iteration: no step yet
+
+struct LMConf {
+  int np, nfreq, nz, npix;
+  int maxsteps, maxit;
+  double dchi2, svdtol, inu;
+  int nodes_ref[8];            // node count per reference parameter
+  int row_of[LM_MAXNP];        // model row of each node's parameter
+  int par_of[LM_MAXNP];        // reference parameter (1-based) of each node
+  double norm[LM_MAXNP];       // PARAM_NORMS of each node's parameter
+};
+
+// Slot pool (device pointers), one allocation per field.
+struct LMSlots {
+  int S;
+  int* pix;          // pixel index, LM_PAD if empty
+  int* skip;         // LM_SKIP if the slot was refilled in this iteration
+  int* iter;
+  double* st;        // 5 per slot: chicur, chibest, lambda, steps, precyc
+  float* mcur;       // (S, 13, nz)
+  float* mbest;
+  double* syn;       // (S, nfreq) forward output of mcur
+  double* synb;      // best synthesis
+  float* jac;        // (S, np, nfreq) forward output
+  float* jacb;       // best Jacobian
+  double* obs;       // (S, nfreq)
+  double* diff;      // weighted residual (S, nfreq)
+  double* H;         // (S, np, np)
+  double* g;         // (S, np)
+  double* delta;     // (S, np)
+  int* status;       // forward status (S)
+};
+
+struct LMQueue {
+  int next;          // next pixel to load
+  int done;          // finished pixels
+};
+
+// PARAM_NORMS (src/get_dmodel.f90:31), LOWLIM/UPPLIM (:1885-1901)
+__constant__ double c_lm_norm[8] = {6000.0, 1.0e5, 1.0e-5, 1.0e3, 1.0e3, 1.0e3, 1.0e6, 6.0e2};
+__constant__ double c_lm_low[8] = {2500.0, 1.0e-2, 1.0e-10, -5.0e4, -5.0e4, -5.0e4, -1.0e7, 1.0e-8};
+__constant__ double c_lm_upp[8] = {1.8e4, 1.0e12, 1.0e10, 5.0e4, 5.0e4, 5.0e4, 1.0e7, 1.0e12};
+
+__device__ __forceinline__ double block_sum_d(double v, double* red) {
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  const int w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  __syncthreads();
+  if ((threadIdx.x & 31) == 0) red[w] = v;
+  __syncthreads();
+  double s = 0.0;
+  for (int i = 0; i < nw; ++i) s += red[i];
+  return s;
+}
+
+// Load pixel p (or mark the slot empty) -- INITIALIZE_CYCLE's per-pixel state.
+__device__ void lm_load_slot(const LMConf& C, const LMSlots& Sl, int s, int p, const double* __restrict__ obs_all,
+                             const float* __restrict__ init_all) {
+  const int nm = 13 * C.nz;
+  if (p < C.npix) {
+    for (int i = threadIdx.x; i < nm; i += blockDim.x) Sl.mcur[(size_t)s * nm + i] = init_all[(size_t)p * nm + i];
+    for (int i = threadIdx.x; i < C.nfreq; i += blockDim.x)
+      Sl.obs[(size_t)s * C.nfreq + i] = obs_all[(size_t)p * C.nfreq + i];
+    if (threadIdx.x == 0) {
+      Sl.pix[s] = p;
+      Sl.iter[s] = 0;
+      double* st = Sl.st + 5 * (size_t)s;
+      st[0] = 1.0e29;
+      st[1] = 1.0e29;
+      st[2] = 10.0;
+      st[3] = 0.0;
+      st[4] = 0.0;
+    }
+  } else if (threadIdx.x == 0) {
+    Sl.pix[s] = LM_PAD;
+  }
+}
+
+// One CTA per slot: initial fill from the queue.
+__global__ void k_lm_fill(LMConf C, LMSlots Sl, LMQueue* q, const double* __restrict__ obs_all,
+                          const float* __restrict__ init_all) {
+  __shared__ int p;
+  if (threadIdx.x == 0) p = atomicAdd(&q->next, 1);
+  __syncthreads();
+  lm_load_slot(C, Sl, blockIdx.x, p, obs_all, init_all);
+  if (threadIdx.x == 0) Sl.skip[blockIdx.x] = 0;
+}
+
+// One CTA per slot: chi2, accept/revert, lambda, residual, stop rule, refill.
+__global__ void __launch_bounds__(256) k_lm_accept(LMConf C, LMSlots Sl, LMQueue* q, const double* __restrict__ w,
+                                                   const double* __restrict__ obs_all,
+                                                   const float* __restrict__ init_all, float* __restrict__ out_model,
+                                                   double* __restrict__ out_chi, int* __restrict__ out_iter,
+                                                   double* __restrict__ out_syn, int* __restrict__ out_status) {
+  __shared__ double red[8];
+  __shared__ int acc, fin, np_next;
+  const int s = blockIdx.x;
+  if (threadIdx.x == 0) Sl.skip[s] = 0;
+  const int p = Sl.pix[s];
+  if (p < 0) return;
+  const int nf = C.nfreq, nm = 13 * C.nz;
+  const double* obs = Sl.obs + (size_t)s * nf;
+  const double* syn = Sl.syn + (size_t)s * nf;
+  double e = 0.0;
+  for (int i = threadIdx.x; i < nf; i += blockDim.x) {
+    const double d = obs[i] - syn[i];
+    e += d * d * w[i];
+  }
+  const double chi = block_sum_d(e, red) / C.inu;
+  double* st = Sl.st + 5 * (size_t)s;
+  if (threadIdx.x == 0) {
+    const double chibest = st[1];
+    const int ok = Sl.status[s] == 0 && chi == chi;
+    acc = ok && chi < chibest;
+    // UPDATE_LAMBDA (src/get_dmodel.f90:917-956), FACTOR = 0.01
+    double lam = st[2], steps = st[3], precyc = st[4], chipre = chibest;
+    const double cc = ok ? chi : 1.0e300;
+    const double gain = chipre - cc;
+    if (gain > 0) {
+      steps = (gain > 0.01 * chipre) ? fmax(0.0, steps - 1.0) : steps + 1.0;
+      chipre = cc;
+      lam = lam / sqrt(10.0);
+    } else {
+      if (fabs(precyc - 1.0) < 1.0e-2) {
+        precyc = 0.0;
+        lam = lam * 3.0;
+      } else {
+        lam = lam * 10.0;
+      }
+      steps = steps + 1.0;
+    }
+    lam = fmax(1.0e-2, lam);
+    const int it = Sl.iter[s] + 1;
+    Sl.iter[s] = it;
+    // stop rule: steps > MAXSTEPS (GET_DMODEL3DS, src/get_dmodel.f90:1476),
+    // the iteration cap, and an accepted step that improved chi2 by less than
+    // dchi2 (relative)
+    const bool small = acc && chibest < 1.0e29 && (chibest - cc) < C.dchi2 * chibest;
+    fin = steps > (double)C.maxsteps || it >= C.maxit || small;
+    st[0] = chi;
+    st[1] = chipre;
+    st[2] = lam;
+    st[3] = steps;
+    st[4] = precyc;
+  }
+  __syncthreads();
+  if (acc) {
+    const float* mc = Sl.mcur + (size_t)s * nm;
+    float* mb = Sl.mbest + (size_t)s * nm;
+    for (int i = threadIdx.x; i < nm; i += blockDim.x) mb[i] = mc[i];
+    double* sb = Sl.synb + (size_t)s * nf;
+    for (int i = threadIdx.x; i < nf; i += blockDim.x) sb[i] = syn[i];
+    const float4* jc = reinterpret_cast<const float4*>(Sl.jac + (size_t)s * C.np * nf);
+    float4* jb = reinterpret_cast<float4*>(Sl.jacb + (size_t)s * C.np * nf);
+    for (int i = threadIdx.x; i < C.np * nf / 4; i += blockDim.x) jb[i] = jc[i];
+  } else {
+    const float* mb = Sl.mbest + (size_t)s * nm;
+    float* mc = Sl.mcur + (size_t)s * nm;
+    for (int i = threadIdx.x; i < nm; i += blockDim.x) mc[i] = mb[i];
+  }
+  __syncthreads();
+  if (fin) {
+    // the pixel's result is its best model (END_CYCLE, src/invert3d.f90:306-312)
+    const float* mb = Sl.mbest + (size_t)s * nm;
+    for (int i = threadIdx.x; i < nm; i += blockDim.x) out_model[(size_t)p * nm + i] = mb[i];
+    if (out_syn)
+      for (int i = threadIdx.x; i < nf; i += blockDim.x) out_syn[(size_t)p * nf + i] = Sl.synb[(size_t)s * nf + i];
+    if (threadIdx.x == 0) {
+      out_chi[p] = st[1];
+      out_iter[p] = Sl.iter[s];
+      if (out_status) out_status[p] = st[1] < 1.0e29 ? 0 : FZ_NAN;
+      atomicAdd(&q->done, 1);
+      np_next = atomicAdd(&q->next, 1);
+      Sl.skip[s] = LM_SKIP;
+    }
+    __syncthreads();
+    lm_load_slot(C, Sl, s, np_next, obs_all, init_all);
+    return;
+  }
+  // weighted residual of the best synthesis (:1027)
+  const double* sb = Sl.synb + (size_t)s * nf;
+  double* df = Sl.diff + (size_t)s * nf;
+  const double rin = 1.0 / sqrt(C.inu);
+  for (int i = threadIdx.x; i < nf; i += blockDim.x) df[i] = (obs[i] - sb[i]) * sqrt(w[i]) * rin;
+}
+
+// bf16 split of a float: hi = RN(x), lo = RN(x - hi)
+__device__ __forceinline__ void bf16_split(float x, unsigned short& hi, unsigned short& lo) {
+  const __nv_bfloat16 h = __float2bfloat16_rn(x);
+  const __nv_bfloat16 l = __float2bfloat16_rn(x - __bfloat162float(h));
+  hi = __bfloat16_as_ushort(h);
+  lo = __bfloat16_as_ushort(l);
+}
+
+__device__ __forceinline__ unsigned pack2(unsigned short a, unsigned short b) {
+  return (unsigned)a | ((unsigned)b << 16);
+}
+
+__device__ __forceinline__ void mma_bf16(float c[4], const unsigned a[4], const unsigned b[2]) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+      "{%0,%1,%2,%3};\n"
+      : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
+      : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b[0]), "r"(b[1]));
+}
+
+// One warp per slot: H = Jn^T Jn (np <= 16) on the tensor cores and
+// g = Jn^T r in FP64.  Jn(r, c) = J(r, c) sqrt(w_r / INU) PARAM_NORM(c).
+// Per k-step of 16 frequencies a thread holds rows {grp, grp+8} x
+// frequencies {2t, 2t+1, 2t+8, 2t+9} of Jn^T: exactly its A fragment, and
+// (column grp of tile 0, column grp+8 of tile 1) its B fragments.
+__global__ void __launch_bounds__(128) k_lm_normal(LMConf C, LMSlots Sl, const double* __restrict__ w) {
+  const int lane = threadIdx.x & 31;
+  const int s = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  if (s >= Sl.S) return;
+  if (Sl.pix[s] < 0 || Sl.skip[s]) return;
+  const int nf = C.nfreq, np = C.np;
+  const float* J = Sl.jacb + (size_t)s * np * nf;
+  const int grp = lane >> 2, t = lane & 3;
+  const int m0 = grp, m1 = grp + 8;
+  const float n0 = m0 < np ? (float)C.norm[m0] : 0.0f, n1 = m1 < np ? (float)C.norm[m1] : 0.0f;
+  const float* r0 = J + (size_t)(m0 < np ? m0 : 0) * nf;
+  const float* r1 = J + (size_t)(m1 < np ? m1 : 0) * nf;
+  const float rin = (float)(1.0 / sqrt(C.inu));
+  float c0[4] = {0, 0, 0, 0}, c1[4] = {0, 0, 0, 0};
+  for (int k0 = 0; k0 < nf; k0 += 16) {
+    float v[2][4];   // [row m0/m1][freq 2t, 2t+1, 2t+8, 2t+9]
+    const int ks[4] = {k0 + 2 * t, k0 + 2 * t + 1, k0 + 2 * t + 8, k0 + 2 * t + 9};
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      const bool in = ks[i] < nf;
+      const float sw = in ? sqrtf((float)w[ks[i]]) * rin : 0.0f;
+      v[0][i] = (in && m0 < np) ? r0[ks[i]] * sw * n0 : 0.0f;
+      v[1][i] = (in && m1 < np) ? r1[ks[i]] * sw * n1 : 0.0f;
+    }
+    unsigned short hi[2][4], lo[2][4];
+#pragma unroll
+    for (int r = 0; r < 2; ++r)
+#pragma unroll
+      for (int i = 0; i < 4; ++i) bf16_split(v[r][i], hi[r][i], lo[r][i]);
+    // A (row-major 16x16): a0 = (m0, 2t..2t+1), a1 = (m1, 2t..), a2 = (m0, 2t+8..), a3 = (m1, 2t+8..)
+    const unsigned ah[4] = {pack2(hi[0][0], hi[0][1]), pack2(hi[1][0], hi[1][1]), pack2(hi[0][2], hi[0][3]),
+                            pack2(hi[1][2], hi[1][3])};
+    const unsigned al[4] = {pack2(lo[0][0], lo[0][1]), pack2(lo[1][0], lo[1][1]), pack2(lo[0][2], lo[0][3]),
+                            pack2(lo[1][2], lo[1][3])};
+    // B (col-major 16x8), column grp of tile 0 = row m0 of Jn^T, of tile 1 = row m1
+    const unsigned b0h[2] = {pack2(hi[0][0], hi[0][1]), pack2(hi[0][2], hi[0][3])};
+    const unsigned b0l[2] = {pack2(lo[0][0], lo[0][1]), pack2(lo[0][2], lo[0][3])};
+    const unsigned b1h[2] = {pack2(hi[1][0], hi[1][1]), pack2(hi[1][2], hi[1][3])};
+    const unsigned b1l[2] = {pack2(lo[1][0], lo[1][1]), pack2(lo[1][2], lo[1][3])};
+    mma_bf16(c0, ah, b0h);
+    mma_bf16(c0, ah, b0l);
+    mma_bf16(c0, al, b0h);
+    mma_bf16(c1, ah, b1h);
+    mma_bf16(c1, ah, b1l);
+    mma_bf16(c1, al, b1h);
+  }
+  // C fragment: c[0..1] = (row grp, cols 2t, 2t+1), c[2..3] = (row grp+8, cols 2t, 2t+1)
+  double* H = Sl.H + (size_t)s * np * np;
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    const int row = grp + (i >= 2 ? 8 : 0);
+    const int colA = 2 * t + (i & 1), colB = 8 + 2 * t + (i & 1);
+    if (row < np && colA < np) H[row * np + colA] = (double)c0[i];
+    if (row < np && colB < np) H[row * np + colB] = (double)c1[i];
+  }
+  // g = Jn^T r (FP64)
+  const double* df = Sl.diff + (size_t)s * nf;
+  for (int c = 0; c < np; ++c) {
+    const float* rc = J + (size_t)c * nf;
+    double acc = 0.0;
+    for (int k = lane; k < nf; k += 32) acc += (double)rc[k] * sqrt(w[k]) * df[k];
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    if (lane == 0) Sl.g[(size_t)s * np + c] = acc * C.norm[c] / sqrt(C.inu);
+  }
+}
+
+// One warp per slot, FP64: delta = (H + lambda diag H)^+ g by one-sided
+// Jacobi (Hestenes) on the columns of the symmetric matrix, singular values
+// below svdtol * max dropped (GET_INVERSE, src/lm.f90:61-133); NaN entries
+// of delta are zeroed (NEW_SOLVE_PERTURBATION, src/get_dmodel.f90:806-820).
+__global__ void __launch_bounds__(128) k_lm_solve(LMConf C, LMSlots Sl) {
+  __shared__ double smA[4][LM_MAXNP][LM_MAXNP + 1], smV[4][LM_MAXNP][LM_MAXNP + 1];
+  const int lane = threadIdx.x & 31, wi = threadIdx.x >> 5;
+  const int s = blockIdx.x * (blockDim.x >> 5) + wi;
+  if (s >= Sl.S) return;
+  if (Sl.pix[s] < 0 || Sl.skip[s]) return;
+  const int np = C.np;
+  const double lam = Sl.st[5 * (size_t)s + 2];
+  const double* H = Sl.H + (size_t)s * np * np;
+  double(*A)[LM_MAXNP + 1] = smA[wi];
+  double(*V)[LM_MAXNP + 1] = smV[wi];
+  // lane i owns row i
+  if (lane < np)
+    for (int j = 0; j < np; ++j) {
+      double h = H[lane * np + j];
+      if (j == lane) h = h + h * lam;   // GET_TERM1 (src/lm.f90:43-57)
+      A[lane][j] = h;
+      V[lane][j] = (lane == j) ? 1.0 : 0.0;
+    }
+  __syncwarp();
+  for (int sweep = 0; sweep < 40; ++sweep) {
+    int rot = 0;
+    for (int p = 0; p < np - 1; ++p)
+      for (int q = p + 1; q < np; ++q) {
+        double a = 0.0, b = 0.0, c = 0.0;
+        if (lane < np) {
+          const double xp = A[lane][p], xq = A[lane][q];
+          a = xp * xp;
+          b = xq * xq;
+          c = xp * xq;
+        }
+        for (int o = 16; o > 0; o >>= 1) {
+          a += __shfl_xor_sync(0xffffffffu, a, o);
+          b += __shfl_xor_sync(0xffffffffu, b, o);
+          c += __shfl_xor_sync(0xffffffffu, c, o);
+        }
+        if (fabs(c) > 1e-15 * sqrt(a * b) && c != 0.0) {
+          ++rot;
+          const double zeta = (b - a) / (2.0 * c);
+          const double tt = (zeta >= 0.0 ? 1.0 : -1.0) / (fabs(zeta) + sqrt(1.0 + zeta * zeta));
+          const double cs = 1.0 / sqrt(1.0 + tt * tt), sn = cs * tt;
+          if (lane < np) {
+            const double xp = A[lane][p], xq = A[lane][q];
+            A[lane][p] = cs * xp - sn * xq;
+            A[lane][q] = sn * xp + cs * xq;
+            const double vp = V[lane][p], vq = V[lane][q];
+            V[lane][p] = cs * vp - sn * vq;
+            V[lane][q] = sn * vp + cs * vq;
+          }
+        }
+        __syncwarp();
+      }
+    if (rot == 0) break;
+  }
+  // sigma_j = |A_j|, u_j = A_j / sigma_j; t_j = u_j.g / sigma_j above the cut
+  double sig = 0.0, smax = 0.0;
+  double tj = 0.0;
+  const double* g = Sl.g + (size_t)s * np;
+  for (int j = 0; j < np; ++j) {
+    double a = 0.0, u = 0.0;
+    if (lane < np) {
+      a = A[lane][j] * A[lane][j];
+      u = A[lane][j] * g[lane];
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+      a += __shfl_xor_sync(0xffffffffu, a, o);
+      u += __shfl_xor_sync(0xffffffffu, u, o);
+    }
+    const double sj = sqrt(a);
+    smax = fmax(smax, sj);
+    if (lane == j) {
+      sig = sj;
+      tj = u;   // sigma_j * (u_j . g)
+    }
+  }
+  const double thr = smax * C.svdtol;
+  const double coef = (lane < np && sig >= thr && sig > 0.0) ? tj / (sig * sig) : 0.0;
+  // delta_i = sum_j V_ij coef_j
+  double d = 0.0;
+  for (int j = 0; j < np; ++j) {
+    const double cj = __shfl_sync(0xffffffffu, coef, j);
+    if (lane < np) d += V[lane][j] * cj;
+  }
+  if (lane < np) Sl.delta[(size_t)s * np + lane] = (d == d) ? d : 0.0;
+}
+
+// One CTA per slot: REARANGE_DA_MODEL with SORT_DELTA_TO_ATMOSPHERE
+// (NODE_EXPANSION = 1) for every free parameter, then the T taper in log
+// tau5 (src/get_dmodel.f90:1975-1989).  coef is the (nz, np) hat table in
+// FP64.  MPERT = 0.15 (IFREE_VAR_SPACE, :420).
+__global__ void __launch_bounds__(128) k_lm_update(LMConf C, LMSlots Sl, const double* __restrict__ coef) {
+  extern __shared__ double sm_upd[];
+  const int s = blockIdx.x;
+  if (Sl.pix[s] < 0 || Sl.skip[s]) return;
+  const int nz = C.nz, np = C.np;
+  double* nzp = sm_upd;             // nz
+  double* avg = nzp + nz;           // np
+  double* itd = avg + np;           // np
+  double* csum = itd + np;          // np
+  float* pert = reinterpret_cast<float*>(csum + np);   // nz
+  float* m = Sl.mcur + (size_t)s * 13 * nz;
+  const double* delta = Sl.delta + (size_t)s * np;
+  const double MPERT = 0.15;
+  int j0 = 0;
+  for (int rp = 1; rp <= 8; ++rp) {
+    const int nj = C.nodes_ref[rp - 1];
+    if (nj <= 0) continue;
+    const int row = C.row_of[j0];
+    float* ip = m + row * nz;
+    const double fac = c_lm_norm[rp - 1], absl = c_lm_norm[rp - 1] * MPERT;
+    const double inf = c_lm_low[rp - 1], sup = c_lm_upp[rp - 1];
+    // CONTRACT_VECTOR of the current profile, clip of the node deltas
+    if (threadIdx.x < nj) {
+      const int j = j0 + threadIdx.x;
+      double a = 0.0, cs = 0.0;
+      for (int k = 0; k < nz; ++k) {
+        const double c = coef[k * np + j];
+        a += (double)ip[k] * c;
+        cs += c;
+      }
+      a /= cs;
+      double pr = fmax(absl, fabs(MPERT * a));
+      if (a == 0.0) pr = absl;
+      double t = delta[j] * fac;
+      if (fabs(t) > pr) t = t / fabs(t) * pr;
+      avg[threadIdx.x] = a;
+      itd[threadIdx.x] = t;
+      csum[threadIdx.x] = cs;
+    }
+    __syncthreads();
+    // NZPERT = EXPAND(avg + itd) - IPAR
+    for (int k = threadIdx.x; k < nz; k += blockDim.x) {
+      double v = 0.0;
+      for (int j = 0; j < nj; ++j) v += (avg[j] + itd[j]) * coef[k * np + j0 + j];
+      nzp[k] = v - (double)ip[k];
+    }
+    __syncthreads();
+    // ITDELTA = CONTRACT(REAL(NZPERT))
+    if (threadIdx.x < nj) {
+      const int j = j0 + threadIdx.x;
+      double a = 0.0;
+      for (int k = 0; k < nz; ++k) a += (double)(float)nzp[k] * coef[k * np + j];
+      itd[threadIdx.x] = a / csum[threadIdx.x];
+    }
+    __syncthreads();
+    // NZPERT = EXPAND(ITDELTA), limits
+    for (int k = threadIdx.x; k < nz; k += blockDim.x) {
+      double v = 0.0;
+      for (int j = 0; j < nj; ++j) v += itd[j] * coef[k * np + j0 + j];
+      const float op = ip[k] + (float)v;
+      if (op < inf) v = inf - (double)ip[k];
+      if (op > sup) v = sup - (double)ip[k];
+      pert[k] = (float)v;
+    }
+    __syncthreads();
+    if (rp == 1 && threadIdx.x == 0) {
+      const float* tau = m + 11 * nz;
+      const float tll = -11.5f, tul = 0.5f;
+      for (int k = nz - 1; k >= 0; --k) {
+        if (tau[k] < tll) {
+          const float x = fabsf(tau[k] - tll) / 0.5f;
+          pert[k] = expf(-(x * x)) * pert[k];
+        } else if (tau[k] > tul && k + 1 < nz) {
+          pert[k] = pert[k + 1];
+        }
+      }
+    }
+    __syncthreads();
+    for (int k = threadIdx.x; k < nz; k += blockDim.x) ip[k] = pert[k] + ip[k];
+    __syncthreads();
+    j0 += nj;
+  }
+}
+
+}  // namespace

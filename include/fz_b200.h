@@ -149,6 +149,45 @@ int fz_forward_rf(fz_ctx* ctx, int ncol, const float* model, int hydrostatic, do
 int fz_forward_rf_device(fz_ctx* ctx, int ncol, const float* d_model, int hydrostatic, double* d_syn,
                          float* d_jac, float* d_model_out, int* d_status, void* stream);
 
+/* Options of the batched inversion (the reference's control-file values in
+ * brackets): maxsteps, the per-pixel limit on the STEPS counter of
+ * UPDATE_LAMBDA (MAXITER, 5); maxit, a hard cap on iterations per pixel;
+ * dchi2, an accepted step whose relative chi2 gain is below it ends the
+ * pixel (0 = off); svdtol, the relative SVD cut (RSVDTOL, 1e-4); isigma, the
+ * noise (NOISE, 4e-3); wstk, the Stokes weights (1,1,1,1); slots, the number
+ * of pixels in flight (0 = 8192). */
+typedef struct {
+  int maxsteps, maxit;
+  double dchi2, svdtol, isigma;
+  float wstk[4];
+  int slots, pad;
+} fz_lm_opts;
+
+/* Batched pixel-wise Levenberg-Marquardt inversion of npix pixels with the
+ * node layout of fz_rf_nodes (NP <= 16): the cycle loop of INVERT3D
+ * (src/invert3d.f90:57-178) with GET_DMODEL3DS/GET_PERT_1D per pixel
+ * (src/get_dmodel.f90:1201-1577), each pixel iterating until its own stop
+ * rule, finished pixels replaced from a device work queue.  obs is
+ * OBS3D(NFREQ, npix) (Stokes-major, GAIN-normalised, as RSYN1D); init is the
+ * initial model MODEL(NZ,13,npix).  Outputs: the best model, its chi2
+ * (NEW_CALCULATE_CHI2 normalisation), the iterations used, optionally the
+ * best synthesis (syn_out, may be NULL) and a status per pixel. */
+int fz_invert(fz_ctx* ctx, int npix, const double* obs, const float* init, int hydrostatic,
+              const fz_lm_opts* opts, float* model_out, double* chi2, int* iters, double* syn_out,
+              int* status);
+int fz_invert_device(fz_ctx* ctx, int npix, const double* d_obs, const float* d_init, int hydrostatic,
+                     const fz_lm_opts* opts, float* d_model_out, double* d_chi2, int* d_iters,
+                     double* d_syn_out, int* d_status, void* stream);
+
+/* Batched GET_PERTURBATION (src/lm.f90:137-204, SOLVER_METHOD = 1) on host
+ * buffers: for each pixel H = J^T J (tensor cores, split-bf16 x3, FP32
+ * accumulation), g = J^T diff, (H + lambda diag H)^+ g by an FP64 Jacobi SVD
+ * with singular values below svdtol * max dropped.  jac is the normalised
+ * JACOB as REAL*4, (nfreq, np, npix); diff (nfreq, npix); lambda (npix);
+ * delta (np, npix).  np <= 16, nfreq a multiple of 4. */
+int fz_lm_perturbation(fz_ctx* ctx, int npix, int np, int nfreq, const float* jac, const double* diff,
+                       const double* lambda, double svdtol, double* delta);
+
 /* Per-kernel timing: when enabled, every launch of the context is bracketed
  * by CUDA events on its stream; fz_profile_read returns the accumulated
  * milliseconds and launch counts of the kernels (names in order:

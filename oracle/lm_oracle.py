@@ -1,0 +1,253 @@
+"""TEST INFRASTRUCTURE -- not part of the product.
+
+FP64 restatement of FIRTEZ-dz's pixel-wise Levenberg-Marquardt step, used by
+tests/ and by the CPU baseline of bench.py as the checker.  The SVD is LAPACK
+DGESVD through scipy, the routine the reference itself calls
+(src/lm.f90:93-103; LAPACK 3.7/3.9 in the reference's manual).
+
+Followed routines (src/get_dmodel.f90 unless noted):
+  GET_PERT_1D :1201-1244, NEW_CALCULATE_CHI2 :960-1032, UPDATE_LAMBDA
+  :917-956, NORMALIZE_JACOB :725-770 (PARAM_NORMS :31), NEW_SOLVE_PERTURBATION
+  :780-829, GET_PERTURBATION/GET_INVERSE src/lm.f90:61-204, LIMIT_PERTURBATION
+  :884-907, REARANGE_DA_MODEL :1843-2016, SORT_DELTA_TO_ATMOSPHERE :1715-1836,
+  EXPAND/CONTRACT_VECTOR :839-880, GET_INT_COEFS :563-644, SET_WEIGHTS
+  :2024-2047 with the WSTK normalisation of src/input_file.f90:1298-1303,
+  INITIALIZE_CYCLE src/invert3d.f90:228-300 (initial state), IFREE_VAR_SPACE
+  :411-442 (MPERT = 0.15, RSVDTOL = 1e-4).
+
+Vertical regularisation (GET_IT_PENALTIES) is off, as in the configurations
+the library targets; SOLVER_METHOD = 1 (SVD) and NODE_EXPANSION = 1 (SIR-like,
+the reference default, src/input_file.f90:452-453).
+"""
+import numpy as np
+from scipy.linalg import lapack
+
+PARAM_NORMS = np.array([6000.0, 1.0e5, 1.0e-5, 1.0e3, 1.0e3, 1.0e3, 1.0e6, 6.0e2])
+LOWLIM = np.array([2500.0, 1.0e-2, 1.0e-10, -5.0e4, -5.0e4, -5.0e4, -1.0e7, 1.0e-8])
+UPPLIM = np.array([1.8e4, 1.0e12, 1.0e10, 5.0e4, 5.0e4, 5.0e4, 1.0e7, 1.0e12])
+# model row of each reference parameter (src/get_dmodel.f90:1861-1868), 0-based
+ATMPOS = {1: 0, 2: 1, 3: 2, 4: 5, 5: 6, 6: 7, 7: 10, 8: 1}
+MPERT = 0.15
+RSVDTOL = 1.0e-4
+TAU_ROW = 11
+
+
+def int_coefs(nz, nj):
+    """GET_INT_COEFS with GET_POSITIONS: (nz, nj) hat coefficients."""
+    c = np.zeros((nz, nj))
+    if nj == 1:
+        c[:, 0] = 1.0
+    elif nj < nz:
+        step = (nz - 1) / (nj - 1)
+        pos = (np.arange(1, nj + 1) - 1.0) * step + 1.0
+        for j in range(1, nj + 1):
+            ji, jf, jm = pos[max(j - 1, 1) - 1], pos[min(j + 1, nj) - 1], pos[j - 1]
+            for i in range(1, nz + 1):
+                if i < ji or i > jf:
+                    continue
+                if i == jm:
+                    c[i - 1, j - 1] = 1.0
+                elif i < jm:
+                    c[i - 1, j - 1] = 1.0 / (jm - ji) * (i - ji)
+                else:
+                    c[i - 1, j - 1] = 1.0 / (jf - jm) * (jf - i)
+    elif nj == nz:
+        c[:, :] = np.eye(nz)
+    else:
+        raise ValueError("NJ cannot be larger than NZ")
+    return c
+
+
+def weights(numw, wstk=(1.0, 1.0, 1.0, 1.0), isigma=4.0e-3):
+    """ISIGMAP(NFREQ) for all four Stokes parameters inverted."""
+    w = np.array(wstk, dtype=np.float32)
+    minw = np.float32(np.sqrt(np.sum(w.astype(np.float32) ** 2)) / np.sqrt(np.float32(4.0)))
+    w = (w / minw).astype(np.float32)
+    return np.repeat(w.astype(np.float64) ** 2 / isigma ** 2, numw)
+
+
+def update_lambda(chicur, chipre, lam, steps, precyc, factor=0.01):
+    """UPDATE_LAMBDA; returns (chipre, lam, steps, precyc)."""
+    lmin = 1.0e-2
+    if chipre - chicur > 0:
+        if chipre - chicur > factor * chipre:
+            steps = max(0.0, steps - 1.0)
+        else:
+            steps = steps + 1.0
+        chipre = chicur
+        lam = lam / np.sqrt(10.0)
+    else:
+        if abs(precyc - 1.0) < 1.0e-2:
+            precyc = 0.0
+            lam = lam * 3.0
+        else:
+            lam = lam * 10.0
+        steps = steps + 1.0
+    return chipre, max(lmin, lam), steps, precyc
+
+
+def pinv_dgesvd(m, svdtol=RSVDTOL):
+    """GET_INVERSE (src/lm.f90:61-133): DGESVD pseudo-inverse, singular
+    values below svdtol * max dropped."""
+    u, s, vt, info = lapack.dgesvd(np.asfortranarray(m), full_matrices=True)
+    if info != 0:
+        raise RuntimeError("dgesvd info %d" % info)
+    thr = np.max(np.abs(s)) * svdtol
+    si = np.where(np.abs(s) < thr, 0.0, 1.0 / np.where(s == 0, 1.0, s))
+    return vt.T @ (np.diag(si) @ u.T)
+
+
+def get_perturbation(jac_n, diff, lam, svdtol=RSVDTOL):
+    """GET_PERTURBATION (src/lm.f90:137-204) with SOLVER_METHOD = 1: jac_n is
+    the normalised JACOB (NFREQ, NP), diff the weighted residual."""
+    hss = jac_n.T @ jac_n
+    term2 = jac_n.T @ diff
+    term1 = hss.copy()
+    term1[np.diag_indices_from(term1)] += np.diag(hss) * lam
+    delta = pinv_dgesvd(term1, svdtol) @ term2
+    return np.where(np.isnan(delta), 0.0, delta)
+
+
+def contract(ivec_sp, coefs):
+    """CONTRACT_VECTOR: node averages of a REAL*4 height profile."""
+    o = (ivec_sp.astype(np.float32).astype(np.float64)[:, None] * coefs).sum(axis=0)
+    return o / coefs.sum(axis=0)
+
+
+def expand(ivec, coefs):
+    """EXPAND_VECTOR."""
+    return coefs @ ivec
+
+
+def sort_delta(delta, factor, ipar, inf, sup, coefs, absolute):
+    """SORT_DELTA_TO_ATMOSPHERE with NODE_EXPANSION = 1: returns the REAL*4
+    height perturbation of one parameter (and the clipped node deltas)."""
+    itd = delta * factor
+    avg = contract(ipar, coefs)
+    pert = np.maximum(absolute, np.abs(MPERT * avg)) if absolute > 0 else np.abs(MPERT * avg)
+    pert = np.where(avg == 0, absolute, pert)
+    itd = np.where(np.abs(itd) > pert, itd / np.abs(np.where(itd == 0, 1.0, itd)) * pert, itd)
+    nzpert = expand(avg + itd, coefs)
+    nzpert = nzpert - ipar.astype(np.float64)
+    itd = contract(nzpert.astype(np.float32), coefs)
+    nzpert = expand(itd, coefs)
+    opar = (ipar + nzpert.astype(np.float32)).astype(np.float32)
+    nzpert = np.where(opar < inf, inf - ipar.astype(np.float64), nzpert)
+    nzpert = np.where(opar > sup, sup - ipar.astype(np.float64), nzpert)
+    return nzpert.astype(np.float32), itd
+
+
+def rearange(model, delta, nodes):
+    """REARANGE_DA_MODEL (non-errors limits): applies the node perturbation
+    delta to model (13, NZ) REAL*4 in place.  nodes: {param: NJ}."""
+    nz = model.shape[1]
+    j0 = 0
+    for p in range(1, 9):
+        nj = nodes.get(p, 0)
+        if nj <= 0:
+            continue
+        row = ATMPOS[p]
+        coefs = int_coefs(nz, nj)
+        bumod = model[row].copy()
+        pert, _ = sort_delta(delta[j0:j0 + nj], PARAM_NORMS[p - 1], model[row], LOWLIM[p - 1], UPPLIM[p - 1],
+                             coefs, PARAM_NORMS[p - 1] * MPERT)
+        if p == 1:
+            tll, tul = np.float32(-11.5), np.float32(0.5)
+            tau = model[TAU_ROW]
+            for k in range(nz - 1, -1, -1):
+                if tau[k] < tll:
+                    pert[k] = np.float32(np.exp(np.float32(-(np.float32(abs(tau[k] - tll)) / np.float32(0.5)) ** 2))) * pert[k]
+                elif tau[k] > tul and k + 1 < nz:
+                    pert[k] = pert[k + 1]
+        model[row] = (pert + bumod).astype(np.float32)
+        j0 += nj
+
+
+def normalize_jacob(jac, w, inu, nodes):
+    """NORMALIZE_JACOB: JACOB (NFREQ, NP) REAL*8 of the REAL*4 EQVDSYN."""
+    j = jac.astype(np.float64) * (np.sqrt(w) / np.sqrt(inu))[:, None]
+    c = 0
+    for p in range(1, 9):
+        nj = nodes.get(p, 0)
+        if nj > 0:
+            j[:, c:c + nj] *= PARAM_NORMS[p - 1]
+            c += nj
+    return j
+
+
+class PixelState:
+    """INV_SLA(1:9) of one pixel plus its best/current model, synthesis and
+    Jacobian (INITIALIZE_CYCLE, src/invert3d.f90:275-286)."""
+
+    def __init__(self, model):
+        self.steps, self.chicur, self.chibest, self.precyc, self.lam = 0.0, 1.0e29, 1.0e29, 0.0, 10.0
+        self.cur = np.array(model, dtype=np.float32)
+        self.best = self.cur.copy()
+        self.best_syn = None
+        self.best_jac = None
+
+
+def lm_accept(st, obs, syn, jac, w, ok=True):
+    """NEW_CALCULATE_CHI2 + UPDATE_LAMBDA for one pixel; returns (chi, accepted,
+    previous best chi)."""
+    inu = float(obs.size)
+    chi = float(np.sum((obs - syn) ** 2 * w) / inu) if ok else 1.0e300
+    prev = st.chibest
+    st.chicur = chi
+    acc = chi < st.chibest
+    if acc:
+        st.best = st.cur.copy()
+        st.best_jac = jac.copy()
+        st.best_syn = syn.copy()
+    else:
+        st.cur = st.best.copy()
+    st.chibest, st.lam, st.steps, st.precyc = update_lambda(chi, st.chibest, st.lam, st.steps, st.precyc, 0.01)
+    return chi, acc, prev
+
+
+def lm_perturb(st, obs, w, nodes):
+    """The rest of GET_PERT_1D: normalised Jacobian, GET_PERTURBATION and
+    REARANGE_DA_MODEL; st.cur becomes the next trial model."""
+    inu = float(obs.size)
+    diff = (obs - st.best_syn) * np.sqrt(w) / np.sqrt(inu)
+    jn = normalize_jacob(st.best_jac, w, inu, nodes)
+    delta = get_perturbation(jn, diff, st.lam)
+    rearange(st.cur, delta, nodes)
+    return delta
+
+
+def lm_step(st, obs, syn, jac, w, nodes):
+    """GET_PERT_1D for one pixel (syn/jac: forward synthesis and EQVDSYN of
+    st.cur, obs/syn RSYN1D(NFREQ), jac (NFREQ, NP) REAL*4)."""
+    lm_accept(st, obs, syn, jac, w)
+    return lm_perturb(st, obs, w, nodes)
+
+
+def invert(forward_rf, obs, init, nodes, w, maxsteps=5, maxit=40, dchi2=0.0):
+    """Pixel-wise inversion with the stop rules of the batched GPU inversion
+    (steps > maxsteps, maxit iterations, or an accepted step gaining less than
+    dchi2 relative).  forward_rf(models (n,13,nz)) -> (syn (n,nfreq),
+    jac (n,nfreq,np), models_out, status); obs (npix, nfreq).
+    Returns (best models, chi2, iterations)."""
+    npix = obs.shape[0]
+    states = [PixelState(init[i]) for i in range(npix)]
+    iters = np.zeros(npix, dtype=np.int32)
+    active = list(range(npix))
+    while active:
+        models = np.stack([states[i].cur for i in active])
+        syn, jac, mo, status = forward_rf(models)
+        still = []
+        for a, i in enumerate(active):
+            st = states[i]
+            st.cur = mo[a].copy()
+            _, acc, prev = lm_accept(st, obs[i], syn[a], jac[a], w, ok=status[a] == 0)
+            iters[i] += 1
+            small = acc and prev < 1.0e29 and (prev - st.chibest) < dchi2 * prev
+            if st.steps > maxsteps or iters[i] >= maxit or small:
+                continue
+            lm_perturb(st, obs[i], w, nodes)
+            still.append(i)
+        active = still
+    best = np.stack([st.best for st in states])
+    chi = np.array([st.chibest for st in states])
+    return best, chi, iters

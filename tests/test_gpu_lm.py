@@ -1,0 +1,76 @@
+"""GPU Levenberg-Marquardt against the FP64 oracle.
+
+* GET_PERTURBATION: the tensor-core normal equations (split-bf16 x3, FP32
+  accumulation, ~1e-5 relative) and the FP64 Jacobi SVD against the oracle's
+  FP64 products and LAPACK DGESVD, on Jacobians whose singular values keep a
+  gap around the 1e-4 cut (a cut decision flips when a singular value sits
+  at the threshold, in any precision):  |delta_gpu - delta| <= 1e-3 |delta|.
+* The batched inversion against the oracle's pixel-wise inversion of the
+  same observations and initial guess: the GPU's FP32 response functions and
+  tensor-core Hessian make the iterations drift apart, so the comparison is
+  on the outcome -- the chi2 each reaches (median ratio within [0.5, 2]),
+  both reducing chi2 at least 5x.
+"""
+import os
+import sys
+
+import numpy as np
+import pytest
+
+sys.path.insert(0, os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "oracle"))
+import lm_oracle as lmo  # noqa: E402
+import lmcase  # noqa: E402
+
+pytestmark = pytest.mark.gpu
+
+
+def _ctx(fz, orc, nz):
+    lines = fz.lines_parse(fz.atmos.line_database_text())
+    reg = fz.regions_from_lines_section(fz.atmos.lines_section(2), lines)
+    g, _ = orc.gain(lines, reg)
+    return lines, reg, g, fz.Synthesis(lines, reg, nz=nz, gain=g)
+
+
+def test_lm_perturbation_matches_oracle(fz, orc):
+    _, _, _, ctx = _ctx(fz, orc, 32)
+    rng = np.random.default_rng(5)
+    npix, npar, nf = 24, 13, 896
+    jac = np.zeros((npix, npar, nf), dtype=np.float32)
+    diff = rng.standard_normal((npix, nf))
+    lam = 10.0 ** rng.uniform(-2, 1, npix)
+    for i in range(npix):
+        u, _ = np.linalg.qr(rng.standard_normal((nf, npar)))
+        v, _ = np.linalg.qr(rng.standard_normal((npar, npar)))
+        # singular values of J: kept directions down to 3e-2 (H: 1e-3),
+        # dropped ones at 3e-3 (H: 1e-5): a 10x gap around the cut in H
+        s = np.concatenate([np.logspace(0, -1.5, npar - 3), np.full(3, 3e-3)]) * 50.0
+        jac[i] = ((u * s) @ v.T).T.astype(np.float32)
+    d = ctx.lm_perturbation(jac, diff, lam)
+    for i in range(npix):
+        ref = lmo.get_perturbation(jac[i].T.astype(np.float64), diff[i], lam[i])
+        assert np.linalg.norm(d[i] - ref) <= 1e-3 * np.linalg.norm(ref), i
+
+
+def test_batched_inversion_matches_oracle_outcome(fz, orc):
+    nz, npix = 48, 8
+    lines, reg, g, ctx = _ctx(fz, orc, nz)
+    true = fz.atmos.make_columns(npix, nz, seed=12)
+    obs, true_he, _ = orc.forward(lines, reg, g, true, hydrostatic=True)
+    init = lmcase.initial_guess(true_he, seed=1)
+    w = lmo.weights(ctx.numw, isigma=1e-3)
+    f = lmcase.oracle_forward_rf(orc, lines, reg, g, he=True)
+    syn0, _, _, _ = f(init)
+    chi0 = np.sum((obs.reshape(npix, -1) - syn0) ** 2 * w, axis=1) / syn0.shape[1]
+    _, ochi, oit = lmo.invert(f, obs.reshape(npix, -1), init, lmcase.NODES, w, maxsteps=5, maxit=25)
+    ctx.rf_nodes(lmcase.NODES)
+    opts = fz.LMOpts(maxsteps=5, maxit=25, isigma=1e-3, slots=5)   # fewer slots than pixels: refills
+    best, chi, it, st = ctx.invert(obs, init, hydrostatic=True, opts=opts)
+    assert np.all(st == 0) and np.all(np.isfinite(best))
+    assert np.all(it <= 25) and np.all(it >= 1)
+    assert np.all(chi < 0.2 * chi0), (chi0, chi)
+    ratio = np.median(chi / ochi)
+    assert 0.5 <= ratio <= 2.0, (chi, ochi)
+    # the reported chi2 is the chi2 of the returned model
+    syn, _, _ = orc.forward(lines, reg, g, best, hydrostatic=True)
+    chk = np.sum((obs.reshape(npix, -1) - syn.reshape(npix, -1)) ** 2 * w, axis=1) / syn0.shape[1]
+    assert np.allclose(chk, chi, rtol=1e-3), (chk, chi)

@@ -1,0 +1,71 @@
+"""Pins of the FP64 Levenberg-Marquardt oracle (oracle/lm_oracle.py).
+
+The reference has no golden inversion outputs; the oracle's pieces are pinned
+against their definitions (DGESVD pseudo-inverse against numpy's, the
+UPDATE_LAMBDA branches, the hat basis), and a short oracle inversion of
+synthetic observations must recover the atmosphere it was generated from.
+"""
+import os
+import sys
+
+import numpy as np
+import pytest
+
+sys.path.insert(0, os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "oracle"))
+import lm_oracle as lmo  # noqa: E402
+import lmcase  # noqa: E402
+
+
+def test_pinv_matches_numpy_with_cut():
+    rng = np.random.default_rng(3)
+    for cond in (1e2, 1e6):
+        q, _ = np.linalg.qr(rng.standard_normal((13, 13)))
+        s = np.logspace(0, -np.log10(cond), 13)
+        m = (q * s) @ q.T
+        a = lmo.pinv_dgesvd(m, 1e-4)
+        b = np.linalg.pinv(m, rcond=1e-4, hermitian=True)
+        assert np.allclose(a, b, rtol=1e-9, atol=1e-9 * np.abs(b).max())
+
+
+def test_update_lambda_branches():
+    # big improvement: steps decrease (not below 0), lambda / sqrt(10)
+    assert lmo.update_lambda(1.0, 2.0, 10.0, 0.0, 0.0) == (1.0, 10.0 / np.sqrt(10.0), 0.0, 0.0)
+    # small improvement (< 1 %): steps increase
+    c, lam, st, pc = lmo.update_lambda(0.999, 1.0, 1.0, 2.0, 0.0)
+    assert (c, st) == (0.999, 3.0) and np.isclose(lam, 1.0 / np.sqrt(10.0))
+    # no improvement: lambda x 10; after a PRECYC = 1 cycle: x 3 and PRECYC reset
+    assert lmo.update_lambda(2.0, 1.0, 1.0, 0.0, 0.0) == (1.0, 10.0, 1.0, 0.0)
+    assert lmo.update_lambda(2.0, 1.0, 1.0, 0.0, 1.0) == (1.0, 3.0, 1.0, 0.0)
+    # floor 1e-2
+    assert lmo.update_lambda(0.5, 1.0, 0.01, 0.0, 0.0)[1] == 0.01
+
+
+def test_hat_basis_partition_of_unity():
+    for nz, nj in ((48, 5), (128, 2), (128, 13), (64, 64)):
+        c = lmo.int_coefs(nz, nj)
+        assert np.allclose(c.sum(axis=1), 1.0)
+        assert c.shape == (nz, nj)
+
+
+def test_oracle_inversion_recovers_the_atmosphere(fz, orc):
+    lines = orc.parse_lines(fz.atmos.line_database_text())
+    reg = fz.regions_from_lines_section(fz.atmos.lines_section(2), lines)
+    g, _ = orc.gain(lines, reg)
+    nz = 48
+    true = fz.atmos.make_columns(3, nz, seed=12)
+    obs, true_he, _ = orc.forward(lines, reg, g, true, hydrostatic=True)
+    obs = obs.reshape(3, -1)
+    init = lmcase.initial_guess(true_he, seed=1)
+    w = lmo.weights(obs.shape[1] // 4, isigma=1e-3)
+    f = lmcase.oracle_forward_rf(orc, lines, reg, g, he=True)
+    syn0, _, _, _ = f(init)
+    chi0 = np.sum((obs - syn0) ** 2 * w, axis=1) / obs.shape[1]
+    best, chi, it = lmo.invert(f, obs, init, lmcase.NODES, w, maxsteps=5, maxit=25)
+    # The reference's step keeps every node direction whose singular value is
+    # above 1e-4 of the largest (RSVDTOL) and re-projects the model on the
+    # node basis at every step (NODE_EXPANSION = 1); with T dominating H
+    # through the hydrostatic coupling it stops well before the noise level,
+    # by the STEPS > MAXSTEPS rule.
+    assert np.all(chi < 0.2 * chi0), (chi0, chi)
+    assert np.all(it < 25)
+    assert np.all(np.isfinite(best))
