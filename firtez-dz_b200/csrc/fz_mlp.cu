@@ -1,0 +1,519 @@
+// Warm-start network of the inversion: an MLP from the observed Stokes vector
+// to the node values of the model, trained and run with hand-written BF16
+// kernels (sm_100a): tensor-core GEMMs (mma.sync m16n8k16 bf16, FP32
+// accumulation) with fused bias / GELU / GELU' epilogues, an MSE loss kernel
+// and Adam on FP32 master weights.  It has no counterpart in the reference,
+// whose initial guess is the model in the control file (or the Stokes-moment
+// assists of SET_TAU, src/invert3d.f90:492-727).
+//
+// Layouts: activations row-major [batch][features] in bf16; weights W[out][in]
+// row-major (bf16 copy for the GEMMs, FP32 master for Adam); biases FP32.
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <vector>
+
+#include "../../include/fz_b200.h"
+
+namespace {
+
+constexpr int BM = 128, BN = 128, BK = 32, SK = BK + 8;   // smem row stride (bf16) avoids bank conflicts
+constexpr int MLP_MAXL = 8;
+
+enum GemmMode { NT = 0, NN = 1, TN = 2 };
+enum Epi { EPI_FWD_GELU = 0, EPI_FWD_LIN = 1, EPI_BWD_GELU = 2, EPI_F32 = 3 };
+
+__device__ __forceinline__ float gelu(float z) { return 0.5f * z * (1.0f + erff(z * 0.70710678118654752f)); }
+__device__ __forceinline__ float gelu_d(float z) {
+  const float cdf = 0.5f * (1.0f + erff(z * 0.70710678118654752f));
+  const float pdf = 0.39894228040143268f * expf(-0.5f * z * z);
+  return cdf + z * pdf;
+}
+
+__device__ __forceinline__ void mma16816(float c[4], const unsigned a[4], const unsigned b[2]) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+      "{%0,%1,%2,%3};\n"
+      : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
+      : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b[0]), "r"(b[1]));
+}
+
+// Element (m, k) of the logical A (M x K) and (n, k) of the logical B^T
+// (N x K) for each mode:
+//   NT: A[m][k] = a[m*lda + k],  B[n][k] = b[n*ldb + k]   (Y = X W^T)
+//   NN: A[m][k] = a[m*lda + k],  B[n][k] = b[k*ldb + n]   (dX = dZ W)
+//   TN: A[m][k] = a[k*lda + m],  B[n][k] = b[k*ldb + n]   (dW = dZ^T X)
+template <int MODE>
+__device__ __forceinline__ __nv_bfloat16 ldA(const __nv_bfloat16* a, int lda, int m, int k, int M, int K) {
+  if (m >= M || k >= K) return __float2bfloat16(0.0f);
+  return MODE == TN ? a[(size_t)k * lda + m] : a[(size_t)m * lda + k];
+}
+template <int MODE>
+__device__ __forceinline__ __nv_bfloat16 ldB(const __nv_bfloat16* b, int ldb, int n, int k, int N, int K) {
+  if (n >= N || k >= K) return __float2bfloat16(0.0f);
+  return MODE == NT ? b[(size_t)n * ldb + k] : b[(size_t)k * ldb + n];
+}
+
+// C (M x N) = A B^T with the logical operands above; 256 threads, 128x128
+// tile, 8 warps as 2 (m) x 4 (n), each warp 64 x 32 = 4 x 4 mma tiles.
+// Epilogues:
+//   EPI_FWD_GELU: z = C + bias[n] -> zout (fp32, pre-activation), out = bf16(gelu(z))
+//   EPI_FWD_LIN : z = C + bias[n] -> fout (fp32)
+//   EPI_BWD_GELU: out = bf16(C * gelu'(zin[m][n]))
+//   EPI_F32     : fout = C (fp32)
+template <int MODE, int EPI>
+__global__ void __launch_bounds__(256) k_gemm(int M, int N, int K, const __nv_bfloat16* __restrict__ A, int lda,
+                                              const __nv_bfloat16* __restrict__ B, int ldb,
+                                              const float* __restrict__ bias, const float* __restrict__ zin,
+                                              float* __restrict__ zout, float* __restrict__ fout,
+                                              __nv_bfloat16* __restrict__ out, int ldc) {
+  __shared__ __align__(16) __nv_bfloat16 As[BM][SK];
+  __shared__ __align__(16) __nv_bfloat16 Bs[BN][SK];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int wm = warp >> 2, wn = warp & 3;   // warp tile origin: (wm*64, wn*32)
+  const int m0 = blockIdx.y * BM, n0 = blockIdx.x * BN;
+  const int grp = lane >> 2, t4 = lane & 3;
+  float acc[4][4][4];
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j)
+#pragma unroll
+      for (int e = 0; e < 4; ++e) acc[i][j][e] = 0.0f;
+  for (int k0 = 0; k0 < K; k0 += BK) {
+    // stage: 128 x 32 elements of A and of B^T, 16 per thread
+    for (int i = tid; i < BM * BK; i += 256) {
+      // walk the contiguous global direction with consecutive threads
+      int r, c;
+      if (MODE == TN) { c = i / BM; r = i % BM; } else { r = i / BK; c = i % BK; }
+      As[r][c] = ldA<MODE>(A, lda, m0 + r, k0 + c, M, K);
+    }
+    for (int i = tid; i < BN * BK; i += 256) {
+      int r, c;
+      if (MODE == NT) { r = i / BK; c = i % BK; } else { c = i / BN; r = i % BN; }
+      Bs[r][c] = ldB<MODE>(B, ldb, n0 + r, k0 + c, N, K);
+    }
+    __syncthreads();
+#pragma unroll
+    for (int kk = 0; kk < BK; kk += 16) {
+      unsigned af[4][4], bf[4][2];
+#pragma unroll
+      for (int i = 0; i < 4; ++i) {
+        const int r = wm * 64 + i * 16 + grp;
+        af[i][0] = *reinterpret_cast<const unsigned*>(&As[r][kk + 2 * t4]);
+        af[i][1] = *reinterpret_cast<const unsigned*>(&As[r + 8][kk + 2 * t4]);
+        af[i][2] = *reinterpret_cast<const unsigned*>(&As[r][kk + 2 * t4 + 8]);
+        af[i][3] = *reinterpret_cast<const unsigned*>(&As[r + 8][kk + 2 * t4 + 8]);
+      }
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        const int n = wn * 32 + j * 8 + grp;
+        bf[j][0] = *reinterpret_cast<const unsigned*>(&Bs[n][kk + 2 * t4]);
+        bf[j][1] = *reinterpret_cast<const unsigned*>(&Bs[n][kk + 2 * t4 + 8]);
+      }
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) mma16816(acc[i][j], af[i], bf[j]);
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j)
+#pragma unroll
+      for (int e = 0; e < 4; ++e) {
+        const int m = m0 + wm * 64 + i * 16 + grp + (e >= 2 ? 8 : 0);
+        const int n = n0 + wn * 32 + j * 8 + 2 * t4 + (e & 1);
+        if (m >= M || n >= N) continue;
+        const float c = acc[i][j][e];
+        const size_t o = (size_t)m * ldc + n;
+        if (EPI == EPI_FWD_GELU) {
+          const float z = c + bias[n];
+          zout[o] = z;
+          out[o] = __float2bfloat16_rn(gelu(z));
+        } else if (EPI == EPI_FWD_LIN) {
+          fout[o] = c + bias[n];
+        } else if (EPI == EPI_BWD_GELU) {
+          out[o] = __float2bfloat16_rn(c * gelu_d(zin[o]));
+        } else {
+          fout[o] = c;
+        }
+      }
+}
+
+// MSE loss 1/(n*nout) sum (y - t)^2 and dL/dy in bf16
+__global__ void k_mse(int n, int nout, const float* __restrict__ y, const float* __restrict__ t,
+                      __nv_bfloat16* __restrict__ dy, float* __restrict__ loss) {
+  __shared__ float red[8];
+  const size_t total = (size_t)n * nout;
+  float s = 0.0f;
+  const float sc = 2.0f / (float)total;
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (size_t)gridDim.x * blockDim.x) {
+    const float d = y[i] - t[i];
+    s += d * d;
+    dy[i] = __float2bfloat16_rn(sc * d);
+  }
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    float b = 0.0f;
+    for (int i = 0; i < (int)(blockDim.x >> 5); ++i) b += red[i];
+    atomicAdd(loss, b / (float)total);
+  }
+}
+
+// bias gradient: column sums of dZ (bf16, n x m)
+__global__ void k_colsum(int n, int m, const __nv_bfloat16* __restrict__ dz, float* __restrict__ db) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= m) return;
+  float s = 0.0f;
+  for (int i = 0; i < n; ++i) s += __bfloat162float(dz[(size_t)i * m + j]);
+  db[j] = s;
+}
+
+__global__ void k_to_bf16(size_t n, const float* __restrict__ x, __nv_bfloat16* __restrict__ y) {
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+    y[i] = __float2bfloat16_rn(x[i]);
+}
+
+// Adam (Kingma & Ba 2015) on FP32 masters, refreshing the bf16 copy
+__global__ void k_adam(size_t n, float* __restrict__ w, const float* __restrict__ g, float* __restrict__ m1,
+                       float* __restrict__ m2, __nv_bfloat16* __restrict__ wb, float lr, float b1, float b2,
+                       float c1, float c2, float eps) {
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    const float gi = g[i];
+    const float a = b1 * m1[i] + (1.0f - b1) * gi;
+    const float b = b2 * m2[i] + (1.0f - b2) * gi * gi;
+    m1[i] = a;
+    m2[i] = b;
+    const float wi = w[i] - lr * (a * c1) / (sqrtf(b * c2) + eps);
+    w[i] = wi;
+    if (wb) wb[i] = __float2bfloat16_rn(wi);
+  }
+}
+
+// deterministic initial weights: uniform(-1,1)*sqrt(6/(fan_in+fan_out)) from a
+// counter-based hash (splitmix64)
+__global__ void k_init(size_t n, float* __restrict__ w, unsigned long long seed, float scale) {
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    unsigned long long z = seed + 0x9E3779B97F4A7C15ull * (i + 1);
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    z ^= z >> 31;
+    const float u = (float)((z >> 40) * (1.0 / 16777216.0)) * 2.0f - 1.0f;
+    w[i] = u * scale;
+  }
+}
+
+}  // namespace
+
+struct fz_mlp {
+  int device = 0;
+  int nl = 0;                 // layers
+  int dim[MLP_MAXL + 1] = {};
+  // per layer: FP32 master W (out x in) and b, bf16 W, grads, Adam moments
+  float *W[MLP_MAXL] = {}, *b[MLP_MAXL] = {}, *gW[MLP_MAXL] = {}, *gb[MLP_MAXL] = {};
+  float *mW[MLP_MAXL] = {}, *vW[MLP_MAXL] = {}, *mb[MLP_MAXL] = {}, *vb[MLP_MAXL] = {};
+  __nv_bfloat16* Wb[MLP_MAXL] = {};
+  // activations for a batch capacity
+  int cap = 0;
+  __nv_bfloat16* act[MLP_MAXL + 1] = {};   // act[0] = input (bf16), act[l] = gelu(z_l)
+  float* z[MLP_MAXL] = {};                 // pre-activations
+  float* yout = nullptr;                    // last layer output (fp32)
+  __nv_bfloat16* dz[MLP_MAXL] = {};        // dL/dz per layer
+  float* loss = nullptr;
+  long long step = 0;
+  cudaStream_t stream = nullptr;
+};
+
+namespace {
+
+int mlp_fail(cudaError_t e) {
+  if (e != cudaSuccess) {
+    std::fprintf(stderr, "fz_b200 mlp: CUDA error %s\n", cudaGetErrorString(e));
+    return FZ_ERR_CUDA;
+  }
+  return 0;
+}
+#define MLP_CK(x)                 \
+  do {                            \
+    int _rc = mlp_fail(x);        \
+    if (_rc) return _rc;          \
+  } while (0)
+
+int grid1(size_t n) { return (int)std::min<size_t>((n + 255) / 256, 148 * 16); }
+
+int mlp_reserve(fz_mlp* p, int n) {
+  if (n <= p->cap) return 0;
+  for (int l = 0; l <= p->nl; ++l) cudaFree(p->act[l]), p->act[l] = nullptr;
+  for (int l = 0; l < p->nl; ++l) {
+    cudaFree(p->z[l]), p->z[l] = nullptr;
+    cudaFree(p->dz[l]), p->dz[l] = nullptr;
+  }
+  cudaFree(p->yout);
+  p->yout = nullptr;
+  p->cap = 0;
+  for (int l = 0; l <= p->nl; ++l) MLP_CK(cudaMalloc(&p->act[l], (size_t)n * p->dim[l] * sizeof(__nv_bfloat16)));
+  for (int l = 0; l < p->nl; ++l) {
+    MLP_CK(cudaMalloc(&p->z[l], (size_t)n * p->dim[l + 1] * sizeof(float)));
+    MLP_CK(cudaMalloc(&p->dz[l], (size_t)n * p->dim[l + 1] * sizeof(__nv_bfloat16)));
+  }
+  MLP_CK(cudaMalloc(&p->yout, (size_t)n * p->dim[p->nl] * sizeof(float)));
+  p->cap = n;
+  return 0;
+}
+
+template <int MODE, int EPI>
+void gemm(cudaStream_t s, int M, int N, int K, const __nv_bfloat16* A, int lda, const __nv_bfloat16* B, int ldb,
+          const float* bias, const float* zin, float* zout, float* fout, __nv_bfloat16* out, int ldc) {
+  const dim3 grid((N + BN - 1) / BN, (M + BM - 1) / BM);
+  k_gemm<MODE, EPI><<<grid, 256, 0, s>>>(M, N, K, A, lda, B, ldb, bias, zin, zout, fout, out, ldc);
+}
+
+// forward of n rows already in act[0]; output in yout
+void mlp_fwd(fz_mlp* p, int n) {
+  for (int l = 0; l < p->nl; ++l) {
+    const int in = p->dim[l], out = p->dim[l + 1];
+    if (l + 1 < p->nl)
+      gemm<NT, EPI_FWD_GELU>(p->stream, n, out, in, p->act[l], in, p->Wb[l], in, p->b[l], nullptr, p->z[l], nullptr,
+                             p->act[l + 1], out);
+    else
+      gemm<NT, EPI_FWD_LIN>(p->stream, n, out, in, p->act[l], in, p->Wb[l], in, p->b[l], nullptr, nullptr, p->yout,
+                            nullptr, out);
+  }
+}
+
+// backward from dz[nl-1]; fills gW, gb
+void mlp_bwd(fz_mlp* p, int n) {
+  for (int l = p->nl - 1; l >= 0; --l) {
+    const int in = p->dim[l], out = p->dim[l + 1];
+    // dW (out x in) = dZ^T (out x n) X (n x in)
+    gemm<TN, EPI_F32>(p->stream, out, in, n, p->dz[l], out, p->act[l], in, nullptr, nullptr, nullptr, p->gW[l],
+                      nullptr, in);
+    k_colsum<<<(out + 255) / 256, 256, 0, p->stream>>>(n, out, p->dz[l], p->gb[l]);
+    if (l > 0)   // dZ_{l-1} = (dZ_l W_l) * gelu'(z_{l-1})
+      gemm<NN, EPI_BWD_GELU>(p->stream, n, in, out, p->dz[l], out, p->Wb[l], in, nullptr, p->z[l - 1], nullptr,
+                             nullptr, p->dz[l - 1], in);
+  }
+}
+
+}  // namespace
+
+extern "C" {
+
+int fz_mlp_create(fz_mlp** out, int nlayers, const int* dims, unsigned long long seed, int device) {
+  if (!out || nlayers < 1 || nlayers > MLP_MAXL || !dims) return FZ_ERR_ARG;
+  for (int l = 0; l <= nlayers; ++l)
+    if (dims[l] <= 0 || (l < nlayers && dims[l] % 8)) return FZ_ERR_ARG;   // input widths: 16-byte rows
+  fz_mlp* p = new (std::nothrow) fz_mlp;
+  if (!p) return FZ_ERR_NOMEM;
+  p->device = device;
+  p->nl = nlayers;
+  for (int l = 0; l <= nlayers; ++l) p->dim[l] = dims[l];
+  int rc = 0;
+  auto fail = [&](int code) {
+    fz_mlp_destroy(p);
+    return code;
+  };
+  if ((rc = mlp_fail(cudaSetDevice(device)))) return fail(rc);
+  if ((rc = mlp_fail(cudaStreamCreateWithFlags(&p->stream, cudaStreamNonBlocking)))) return fail(rc);
+  for (int l = 0; l < nlayers; ++l) {
+    const size_t nw = (size_t)dims[l] * dims[l + 1];
+    float** f32[] = {&p->W[l], &p->gW[l], &p->mW[l], &p->vW[l]};
+    for (float** q : f32)
+      if ((rc = mlp_fail(cudaMalloc(q, nw * sizeof(float))))) return fail(rc);
+    float** f32b[] = {&p->b[l], &p->gb[l], &p->mb[l], &p->vb[l]};
+    for (float** q : f32b)
+      if ((rc = mlp_fail(cudaMalloc(q, dims[l + 1] * sizeof(float))))) return fail(rc);
+    if ((rc = mlp_fail(cudaMalloc(&p->Wb[l], nw * sizeof(__nv_bfloat16))))) return fail(rc);
+    const float sc = std::sqrt(6.0f / (float)(dims[l] + dims[l + 1]));
+    k_init<<<grid1(nw), 256, 0, p->stream>>>(nw, p->W[l], seed + 1000003ull * l, sc);
+    k_to_bf16<<<grid1(nw), 256, 0, p->stream>>>(nw, p->W[l], p->Wb[l]);
+    cudaMemsetAsync(p->b[l], 0, dims[l + 1] * sizeof(float), p->stream);
+    cudaMemsetAsync(p->mW[l], 0, nw * sizeof(float), p->stream);
+    cudaMemsetAsync(p->vW[l], 0, nw * sizeof(float), p->stream);
+    cudaMemsetAsync(p->mb[l], 0, dims[l + 1] * sizeof(float), p->stream);
+    cudaMemsetAsync(p->vb[l], 0, dims[l + 1] * sizeof(float), p->stream);
+  }
+  if ((rc = mlp_fail(cudaMalloc(&p->loss, sizeof(float))))) return fail(rc);
+  if ((rc = mlp_fail(cudaStreamSynchronize(p->stream)))) return fail(rc);
+  *out = p;
+  return 0;
+}
+
+int fz_mlp_destroy(fz_mlp* p) {
+  if (!p) return 0;
+  cudaSetDevice(p->device);
+  if (p->stream) cudaStreamSynchronize(p->stream);
+  for (int l = 0; l < MLP_MAXL; ++l) {
+    cudaFree(p->W[l]);
+    cudaFree(p->b[l]);
+    cudaFree(p->gW[l]);
+    cudaFree(p->gb[l]);
+    cudaFree(p->mW[l]);
+    cudaFree(p->vW[l]);
+    cudaFree(p->mb[l]);
+    cudaFree(p->vb[l]);
+    cudaFree(p->Wb[l]);
+    cudaFree(p->z[l]);
+    cudaFree(p->dz[l]);
+  }
+  for (int l = 0; l <= MLP_MAXL; ++l) cudaFree(p->act[l]);
+  cudaFree(p->yout);
+  cudaFree(p->loss);
+  if (p->stream) cudaStreamDestroy(p->stream);
+  delete p;
+  return 0;
+}
+
+// Parameters as FP32 in layer order: W0 (out x in), b0, W1, b1, ...
+long long fz_mlp_nparams(const fz_mlp* p) {
+  if (!p) return FZ_ERR_ARG;
+  long long n = 0;
+  for (int l = 0; l < p->nl; ++l) n += (long long)p->dim[l] * p->dim[l + 1] + p->dim[l + 1];
+  return n;
+}
+
+int fz_mlp_get_params(fz_mlp* p, float* host, int grads) {
+  if (!p || !host) return FZ_ERR_ARG;
+  MLP_CK(cudaSetDevice(p->device));
+  MLP_CK(cudaStreamSynchronize(p->stream));
+  size_t o = 0;
+  for (int l = 0; l < p->nl; ++l) {
+    const size_t nw = (size_t)p->dim[l] * p->dim[l + 1];
+    MLP_CK(cudaMemcpy(host + o, grads ? p->gW[l] : p->W[l], nw * sizeof(float), cudaMemcpyDeviceToHost));
+    o += nw;
+    MLP_CK(cudaMemcpy(host + o, grads ? p->gb[l] : p->b[l], p->dim[l + 1] * sizeof(float), cudaMemcpyDeviceToHost));
+    o += p->dim[l + 1];
+  }
+  return 0;
+}
+
+int fz_mlp_set_params(fz_mlp* p, const float* host) {
+  if (!p || !host) return FZ_ERR_ARG;
+  MLP_CK(cudaSetDevice(p->device));
+  size_t o = 0;
+  for (int l = 0; l < p->nl; ++l) {
+    const size_t nw = (size_t)p->dim[l] * p->dim[l + 1];
+    MLP_CK(cudaMemcpy(p->W[l], host + o, nw * sizeof(float), cudaMemcpyHostToDevice));
+    o += nw;
+    MLP_CK(cudaMemcpy(p->b[l], host + o, p->dim[l + 1] * sizeof(float), cudaMemcpyHostToDevice));
+    o += p->dim[l + 1];
+    k_to_bf16<<<grid1(nw), 256, 0, p->stream>>>(nw, p->W[l], p->Wb[l]);
+  }
+  MLP_CK(cudaGetLastError());
+  MLP_CK(cudaStreamSynchronize(p->stream));
+  return 0;
+}
+
+// Forward on device rows x (n x dim0, fp32) -> y (n x dimL, fp32), in chunks.
+int fz_mlp_forward_device(fz_mlp* p, int n, const float* d_x, float* d_y, void* stream) {
+  if (!p || n <= 0 || !d_x || !d_y) return FZ_ERR_ARG;
+  MLP_CK(cudaSetDevice(p->device));
+  const int chunk = 16384;
+  int rc = mlp_reserve(p, std::min(n, chunk));
+  if (rc) return rc;
+  cudaStream_t s = p->stream;
+  cudaEvent_t ev;
+  MLP_CK(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+  if (stream) {   // order after the caller's stream
+    cudaEventRecord(ev, (cudaStream_t)stream);
+    cudaStreamWaitEvent(s, ev, 0);
+  }
+  const int d0 = p->dim[0], dl = p->dim[p->nl];
+  for (int i = 0; i < n; i += chunk) {
+    const int m = std::min(chunk, n - i);
+    k_to_bf16<<<grid1((size_t)m * d0), 256, 0, s>>>((size_t)m * d0, d_x + (size_t)i * d0, p->act[0]);
+    mlp_fwd(p, m);
+    cudaMemcpyAsync(d_y + (size_t)i * dl, p->yout, (size_t)m * dl * sizeof(float), cudaMemcpyDeviceToDevice, s);
+  }
+  cudaEventRecord(ev, s);
+  if (stream) cudaStreamWaitEvent((cudaStream_t)stream, ev, 0);
+  const int r2 = mlp_fail(cudaGetLastError());
+  if (!stream) cudaStreamSynchronize(s);
+  cudaEventDestroy(ev);
+  return r2;
+}
+
+// Loss and gradients of one batch (no update); loss to *loss (host).
+int fz_mlp_grad_device(fz_mlp* p, int n, const float* d_x, const float* d_t, float* loss) {
+  if (!p || n <= 0 || !d_x || !d_t) return FZ_ERR_ARG;
+  MLP_CK(cudaSetDevice(p->device));
+  int rc = mlp_reserve(p, n);
+  if (rc) return rc;
+  cudaStream_t s = p->stream;
+  const int d0 = p->dim[0], dl = p->dim[p->nl];
+  k_to_bf16<<<grid1((size_t)n * d0), 256, 0, s>>>((size_t)n * d0, d_x, p->act[0]);
+  mlp_fwd(p, n);
+  MLP_CK(cudaMemsetAsync(p->loss, 0, sizeof(float), s));
+  k_mse<<<grid1((size_t)n * dl), 256, 0, s>>>(n, dl, p->yout, d_t, p->dz[p->nl - 1], p->loss);
+  mlp_bwd(p, n);
+  MLP_CK(cudaGetLastError());
+  if (loss) MLP_CK(cudaMemcpyAsync(loss, p->loss, sizeof(float), cudaMemcpyDeviceToHost, s));
+  MLP_CK(cudaStreamSynchronize(s));
+  return 0;
+}
+
+// Mini-batch Adam training over n device rows for `epochs` passes (rows
+// visited in a fixed permutation per epoch from `seed`); mean loss of the
+// last epoch to *loss.
+int fz_mlp_train_device(fz_mlp* p, int n, const float* d_x, const float* d_t, int batch, int epochs, float lr,
+                        unsigned long long seed, float* loss) {
+  if (!p || n <= 0 || !d_x || !d_t || batch <= 0 || epochs <= 0) return FZ_ERR_ARG;
+  MLP_CK(cudaSetDevice(p->device));
+  int rc = mlp_reserve(p, batch);
+  if (rc) return rc;
+  cudaStream_t s = p->stream;
+  const int d0 = p->dim[0], dl = p->dim[p->nl];
+  const int nb = n / batch;
+  if (nb <= 0) return FZ_ERR_ARG;
+  // batch order: a fixed random permutation of the batch indices per epoch
+  std::vector<int> order(nb);
+  unsigned long long st = seed | 1ull;
+  float last = 0.0f;
+  for (int e = 0; e < epochs && !rc; ++e) {
+    for (int i = 0; i < nb; ++i) order[i] = i;
+    for (int i = nb - 1; i > 0; --i) {
+      st ^= st << 13;
+      st ^= st >> 7;
+      st ^= st << 17;
+      const int j = (int)(st % (unsigned long long)(i + 1));
+      std::swap(order[i], order[j]);
+    }
+    cudaMemsetAsync(p->loss, 0, sizeof(float), s);
+    for (int bi = 0; bi < nb; ++bi) {
+      const size_t r0 = (size_t)order[bi] * batch;
+      k_to_bf16<<<grid1((size_t)batch * d0), 256, 0, s>>>((size_t)batch * d0, d_x + r0 * d0, p->act[0]);
+      mlp_fwd(p, batch);
+      k_mse<<<grid1((size_t)batch * dl), 256, 0, s>>>(batch, dl, p->yout, d_t + r0 * dl, p->dz[p->nl - 1], p->loss);
+      mlp_bwd(p, batch);
+      ++p->step;
+      const float b1 = 0.9f, b2 = 0.999f;
+      const float c1 = 1.0f / (1.0f - std::pow(b1, (float)p->step));
+      const float c2 = 1.0f / (1.0f - std::pow(b2, (float)p->step));
+      for (int l = 0; l < p->nl; ++l) {
+        const size_t nw = (size_t)p->dim[l] * p->dim[l + 1];
+        k_adam<<<grid1(nw), 256, 0, s>>>(nw, p->W[l], p->gW[l], p->mW[l], p->vW[l], p->Wb[l], lr, b1, b2, c1, c2,
+                                         1e-8f);
+        k_adam<<<grid1(p->dim[l + 1]), 256, 0, s>>>(p->dim[l + 1], p->b[l], p->gb[l], p->mb[l], p->vb[l], nullptr,
+                                                    lr, b1, b2, c1, c2, 1e-8f);
+      }
+    }
+    float h = 0.0f;
+    rc = mlp_fail(cudaMemcpyAsync(&h, p->loss, sizeof(float), cudaMemcpyDeviceToHost, s));
+    if (!rc) rc = mlp_fail(cudaStreamSynchronize(s));
+    last = h / (float)nb;
+  }
+  if (!rc) rc = mlp_fail(cudaGetLastError());
+  if (loss) *loss = last;
+  return rc;
+}
+
+}  // extern "C"

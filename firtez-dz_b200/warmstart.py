@@ -1,0 +1,215 @@
+"""Learned initial guess of the inversion.
+
+No counterpart in the reference: its LM starts from the model given in the
+control file (or from the Stokes-moment assists of SET_TAU,
+src/invert3d.f90:492-727).  Here an MLP maps the observed Stokes vector
+(4 x NUMW, GAIN-normalised) to the node values of the free parameters -- the
+CONTRACT_VECTOR averages (src/get_dmodel.f90:861-880) of T, Bx, By, Bz and
+v_z over the hat basis of GET_INT_COEFS -- and the predicted nodes, expanded
+on the height grid (EXPAND_VECTOR), replace those rows of a default model.
+
+The network is trained on (model, profile) pairs that the library's own GPU
+forward solver synthesises from seeded atmospheres, with the library's BF16
+kernels (fz_mlp_*).  Device buffers are torch tensors (memory and streams
+only); every FLOP of training and inference runs in libfzb200.so.
+"""
+import ctypes
+
+import numpy as np
+
+from . import FzError, _check, _p, atmos, lib
+
+# (reference parameter, model row) of the free parameters the network predicts
+PARAM_ROWS = ((1, 0), (2, 1), (4, 5), (5, 6), (6, 7), (7, 10))
+
+
+def _bind():
+    L = lib()
+    if getattr(L, "_mlp_bound", False):
+        return L
+    P = ctypes.c_void_p
+    L.fz_mlp_create.argtypes = [ctypes.POINTER(P), ctypes.c_int, P, ctypes.c_ulonglong, ctypes.c_int]
+    L.fz_mlp_destroy.argtypes = [P]
+    L.fz_mlp_nparams.argtypes = [P]
+    L.fz_mlp_nparams.restype = ctypes.c_longlong
+    L.fz_mlp_get_params.argtypes = [P, P, ctypes.c_int]
+    L.fz_mlp_set_params.argtypes = [P, P]
+    L.fz_mlp_forward_device.argtypes = [P, ctypes.c_int, P, P, P]
+    L.fz_mlp_grad_device.argtypes = [P, ctypes.c_int, P, P, P]
+    L.fz_mlp_train_device.argtypes = [P, ctypes.c_int, P, P, ctypes.c_int, ctypes.c_int, ctypes.c_float,
+                                      ctypes.c_ulonglong, P]
+    L._mlp_bound = True
+    return L
+
+
+class MLP:
+    """Fully connected network dims[0] -> ... -> dims[-1], GELU in between."""
+
+    def __init__(self, dims=(896, 1024, 1024, 512, 13), seed=0, device=0):
+        L = _bind()
+        self.dims = tuple(int(d) for d in dims)
+        d = np.array(self.dims, dtype=np.int32)
+        h = ctypes.c_void_p()
+        _check(L.fz_mlp_create(ctypes.byref(h), len(self.dims) - 1, _p(d), int(seed), int(device)))
+        self._h = h
+
+    def close(self):
+        if getattr(self, "_h", None):
+            _bind().fz_mlp_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def nparams(self):
+        return int(_bind().fz_mlp_nparams(self._h))
+
+    def get_params(self, grads=False):
+        out = np.zeros(self.nparams, dtype=np.float32)
+        _check(_bind().fz_mlp_get_params(self._h, _p(out), int(bool(grads))))
+        return out
+
+    def set_params(self, params):
+        p = np.ascontiguousarray(params, dtype=np.float32)
+        if p.size != self.nparams:
+            raise ValueError("expected %d parameters" % self.nparams)
+        _check(_bind().fz_mlp_set_params(self._h, _p(p)))
+
+    def forward_device(self, n, x_ptr, y_ptr, stream=0):
+        _check(_bind().fz_mlp_forward_device(self._h, int(n), ctypes.c_void_p(x_ptr), ctypes.c_void_p(y_ptr),
+                                             ctypes.c_void_p(stream) if stream else None))
+
+    def grad_device(self, n, x_ptr, t_ptr):
+        loss = ctypes.c_float()
+        _check(_bind().fz_mlp_grad_device(self._h, int(n), ctypes.c_void_p(x_ptr), ctypes.c_void_p(t_ptr),
+                                          ctypes.byref(loss)))
+        return loss.value
+
+    def train_device(self, n, x_ptr, t_ptr, batch=1024, epochs=1, lr=1e-3, seed=0):
+        loss = ctypes.c_float()
+        _check(_bind().fz_mlp_train_device(self._h, int(n), ctypes.c_void_p(x_ptr), ctypes.c_void_p(t_ptr),
+                                           int(batch), int(epochs), float(lr), int(seed), ctypes.byref(loss)))
+        return loss.value
+
+
+def hat_coefs(nz, nj):
+    """GET_INT_COEFS (src/get_dmodel.f90:563-644): (nz, nj) hat functions."""
+    c = np.zeros((nz, nj))
+    if nj == 1:
+        c[:, 0] = 1.0
+        return c
+    if nj == nz:
+        return np.eye(nz)
+    step = (nz - 1) / (nj - 1)
+    pos = np.arange(nj) * step + 1.0
+    i = np.arange(1, nz + 1, dtype=np.float64)
+    for j in range(nj):
+        ji, jf, jm = pos[max(j - 1, 0)], pos[min(j + 1, nj - 1)], pos[j]
+        up = (i >= ji) & (i < jm)
+        dn = (i > jm) & (i <= jf)
+        c[up, j] = (i[up] - ji) / (jm - ji)
+        c[dn, j] = (jf - i[dn]) / (jf - jm)
+        c[i == jm, j] = 1.0
+    return c
+
+
+def default_models(npix, nz, b=100.0, seed=0):
+    """The plain initial guess: the mean temperature stratification, its
+    hydrostatic pressure, a field of (b, b, b) G and v_z = 0."""
+    z = atmos.z_grid(nz)
+    T = atmos.mean_temperature(z)[None, :]
+    m = np.zeros((npix, 13, nz), dtype=np.float32)
+    m[:, 0] = T
+    m[:, 1] = atmos.hydrostatic_pg(T, z)
+    m[:, 5:8] = b
+    m[:, 12] = z[None, :]
+    return m
+
+
+class WarmStart:
+    """Stokes vector -> node values -> initial model, for the node layout
+    {reference parameter: NJ} of the inversion (T, Bx, By, Bz, v_z)."""
+
+    def __init__(self, nz, nodes, numw, hidden=(1024, 1024, 512), seed=0, device=0):
+        self.nz, self.numw = int(nz), int(numw)
+        self.nodes = {int(p): int(n) for p, n in nodes.items() if n > 0}
+        self.params = [(p, r) for p, r in PARAM_ROWS if p in self.nodes]
+        self.nout = sum(self.nodes[p] for p, _ in self.params)
+        self.coefs = {p: hat_coefs(self.nz, self.nodes[p]) for p, _ in self.params}
+        self.mlp = MLP((4 * self.numw,) + tuple(hidden) + (self.nout,), seed=seed, device=device)
+        self.xmu = self.xsd = self.tmu = self.tsd = None
+
+    def targets(self, models):
+        """Node values (CONTRACT_VECTOR) of models (n, 13, nz) -> (n, nout)."""
+        cols = []
+        for p, row in self.params:
+            c = self.coefs[p]
+            cols.append((models[:, row].astype(np.float64) @ c) / c.sum(axis=0))
+        return np.concatenate(cols, axis=1)
+
+    def expand(self, nodes_v, base):
+        """EXPAND_VECTOR of predicted nodes (n, nout) into copies of base."""
+        m = np.array(base, dtype=np.float32, copy=True)
+        j = 0
+        for p, row in self.params:
+            nj = self.nodes[p]
+            m[:, row] = (nodes_v[:, j:j + nj] @ self.coefs[p].T).astype(np.float32)
+            j += nj
+        return m
+
+    def make_training_set(self, synth, ncol, seed, noise=1e-3, chunk=65536):
+        """Seeded atmospheres synthesised on the GPU (hydrostatic) plus
+        Gaussian noise: returns device tensors (x (ncol, 4 numw), t (ncol, nout))
+        normalised with the set's own mean and spread."""
+        import torch
+        x = torch.empty((ncol, 4 * self.numw), dtype=torch.float32, device="cuda")
+        t = np.empty((ncol, self.nout))
+        gen = torch.Generator(device="cuda")
+        gen.manual_seed(int(seed) + 7)
+        stream = torch.cuda.current_stream().cuda_stream
+        for i in range(0, ncol, chunk):
+            n = min(chunk, ncol - i)
+            m = torch.from_numpy(atmos.make_columns(n, self.nz, seed=int(seed) * 1000003 + i)).cuda()
+            syn = torch.empty((n, 4, self.numw), dtype=torch.float64, device="cuda")
+            mo = torch.empty_like(m)
+            synth.forward_device(m.data_ptr(), n, syn.data_ptr(), mo.data_ptr(), 0, stream=stream, hydrostatic=True)
+            x[i:i + n] = (syn.reshape(n, -1) + noise * torch.randn(syn.reshape(n, -1).shape, device="cuda",
+                                                                     dtype=torch.float64, generator=gen)).float()
+            t[i:i + n] = self.targets(mo.cpu().numpy())
+        self.xmu = x.mean(dim=0, keepdim=True)
+        self.xsd = x.std(dim=0, keepdim=True) + 1e-6
+        x.sub_(self.xmu).div_(self.xsd)
+        self.tmu = t.mean(axis=0, keepdims=True)
+        self.tsd = t.std(axis=0, keepdims=True) + 1e-12
+        tt = torch.from_numpy(((t - self.tmu) / self.tsd).astype(np.float32)).cuda()
+        return x, tt
+
+    def fit(self, x, t, epochs=8, batch=1024, lr=1e-3, seed=0):
+        """Adam on the device training set; returns the last epoch's mean loss."""
+        import torch
+        torch.cuda.synchronize()
+        n = (x.shape[0] // batch) * batch
+        return self.mlp.train_device(n, x.data_ptr(), t.data_ptr(), batch=batch, epochs=epochs, lr=lr, seed=seed)
+
+    def predict_nodes(self, obs):
+        """obs (npix, 4, numw) -> node values (npix, nout) in physical units."""
+        import torch
+        if self.xmu is None:
+            raise FzError("the network has no normalisation: train it first")
+        x = torch.from_numpy(np.ascontiguousarray(obs, dtype=np.float32).reshape(obs.shape[0], -1)).cuda()
+        x = ((x - self.xmu) / self.xsd).contiguous()
+        y = torch.empty((x.shape[0], self.nout), dtype=torch.float32, device="cuda")
+        torch.cuda.synchronize()
+        self.mlp.forward_device(x.shape[0], x.data_ptr(), y.data_ptr())
+        return y.cpu().numpy().astype(np.float64) * self.tsd + self.tmu
+
+    def initial_models(self, obs, base=None):
+        """Warm-start models for observations obs (npix, 4, numw)."""
+        nodes_v = self.predict_nodes(obs)
+        if base is None:
+            base = default_models(obs.shape[0], self.nz)
+        return self.expand(nodes_v, base)

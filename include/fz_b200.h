@@ -188,6 +188,26 @@ int fz_invert_device(fz_ctx* ctx, int npix, const double* d_obs, const float* d_
 int fz_lm_perturbation(fz_ctx* ctx, int npix, int np, int nfreq, const float* jac, const double* diff,
                        const double* lambda, double svdtol, double* delta);
 
+/* Warm-start network (no counterpart in the reference): an MLP of nlayers
+ * fully connected layers dims[0] -> dims[1] -> ... -> dims[nlayers] with GELU
+ * between layers, trained and evaluated with hand-written BF16 tensor-core
+ * kernels (FP32 accumulation, FP32 master weights, Adam).  dims[0..nlayers-1]
+ * must be multiples of 8.  Weights start from a seeded uniform
+ * Glorot initialisation.  Parameters are exchanged as FP32 in layer order
+ * (W0[out][in], b0, W1, b1, ...); fz_mlp_get_params with grads != 0 returns
+ * the gradients of the last fz_mlp_grad_device call instead.  Rows are
+ * row-major FP32 on the device; the loss is the mean squared error. */
+typedef struct fz_mlp fz_mlp;
+int fz_mlp_create(fz_mlp** mlp, int nlayers, const int* dims, unsigned long long seed, int device);
+int fz_mlp_destroy(fz_mlp* mlp);
+long long fz_mlp_nparams(const fz_mlp* mlp);
+int fz_mlp_get_params(fz_mlp* mlp, float* host, int grads);
+int fz_mlp_set_params(fz_mlp* mlp, const float* host);
+int fz_mlp_forward_device(fz_mlp* mlp, int n, const float* d_x, float* d_y, void* stream);
+int fz_mlp_grad_device(fz_mlp* mlp, int n, const float* d_x, const float* d_t, float* loss);
+int fz_mlp_train_device(fz_mlp* mlp, int n, const float* d_x, const float* d_t, int batch, int epochs, float lr,
+                        unsigned long long seed, float* loss);
+
 /* Per-kernel timing: when enabled, every launch of the context is bracketed
  * by CUDA events on its stream; fz_profile_read returns the accumulated
  * milliseconds and launch counts of the kernels (names in order:

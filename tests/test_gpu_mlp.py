@@ -1,0 +1,96 @@
+"""The warm-start network on the GPU.
+
+* Forward and gradients of the BF16 kernels against the FP64 oracle
+  (oracle/mlp_oracle.py) evaluated on the same bf16-rounded operands; the GPU
+  also keeps the activations and dL/dz in bf16 between layers, so each
+  layer's gradient is compared in relative L2 norm:
+      |g_gpu - g_oracle| <= 3e-2 |g_oracle|,  outputs within 1e-2.
+* Training reduces the loss.
+* The gain over the method without it: LM started from the network's
+  prediction reaches a lower median chi2 in fewer iterations than LM from
+  the default guess, on held-out seeded pixels.
+"""
+import os
+import sys
+
+import numpy as np
+import pytest
+
+sys.path.insert(0, os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "oracle"))
+import mlp_oracle as mo  # noqa: E402
+import lmcase  # noqa: E402
+
+pytestmark = pytest.mark.gpu
+
+DIMS = (896, 1024, 1024, 512, 13)
+
+
+def _layers(flat, dims):
+    out, o = [], 0
+    for i in range(len(dims) - 1):
+        n = dims[i] * dims[i + 1] + dims[i + 1]
+        out.append(flat[o:o + n])
+        o += n
+    return out
+
+
+def test_forward_and_gradients_match_oracle(fz):
+    import torch
+    from firtez_dz_b200 import warmstart as ws
+    net = ws.MLP(DIMS, seed=3)
+    assert net.nparams == 2499597
+    rng = np.random.default_rng(4)
+    n = 256
+    x = rng.standard_normal((n, DIMS[0])).astype(np.float32)
+    t = rng.standard_normal((n, DIMS[-1])).astype(np.float32)
+    dx, dt = torch.from_numpy(x).cuda(), torch.from_numpy(t).cuda()
+    y = torch.empty((n, DIMS[-1]), dtype=torch.float32, device="cuda")
+    net.forward_device(n, dx.data_ptr(), y.data_ptr())
+    p = net.get_params()
+    yo, _ = mo.forward(p, DIMS, x)
+    yg = y.cpu().numpy()
+    assert np.linalg.norm(yg - yo) <= 1e-2 * np.linalg.norm(yo)
+    loss = net.grad_device(n, dx.data_ptr(), dt.data_ptr())
+    g = net.get_params(grads=True)
+    lo, go = mo.loss_and_grad(p, DIMS, x, t)
+    assert abs(loss - lo) <= 1e-2 * lo
+    for a, b in zip(_layers(g, DIMS), _layers(go, DIMS)):
+        assert np.linalg.norm(a - b) <= 3e-2 * np.linalg.norm(b)
+
+
+def test_training_reduces_loss(fz):
+    import torch
+    from firtez_dz_b200 import warmstart as ws
+    rng = np.random.default_rng(1)
+    n, d = 16384, 64
+    x = rng.standard_normal((n, d)).astype(np.float32)
+    a = rng.standard_normal((d, 5)) / np.sqrt(d)
+    t = np.tanh(x @ a).astype(np.float32)
+    net = ws.MLP((d, 256, 256, 5), seed=2)
+    dx, dt = torch.from_numpy(x).cuda(), torch.from_numpy(t).cuda()
+    first = net.train_device(n, dx.data_ptr(), dt.data_ptr(), batch=256, epochs=1, lr=1e-3, seed=1)
+    last = net.train_device(n, dx.data_ptr(), dt.data_ptr(), batch=256, epochs=8, lr=1e-3, seed=2)
+    assert last < 0.2 * first, (first, last)
+
+
+def test_warm_start_beats_default_guess(fz):
+    from firtez_dz_b200 import warmstart as ws
+    nz = 64
+    lines = fz.lines_parse(fz.atmos.line_database_text())
+    reg = fz.regions_from_lines_section(fz.atmos.lines_section(2), lines)
+    ctx = fz.Synthesis(lines, reg, nz=nz)
+    warm = ws.WarmStart(nz, lmcase.NODES, ctx.numw, seed=5)
+    x, t = warm.make_training_set(ctx, 131072, seed=11, noise=1e-3)
+    loss = warm.fit(x, t, epochs=6, batch=1024, lr=1e-3)
+    assert loss < 0.5   # normalised targets: well below the variance 1
+    npix = 96
+    true = fz.atmos.make_columns(npix, nz, seed=424242)
+    obs, true_he, _ = ctx.forward(true, hydrostatic=True)
+    obs = obs + np.random.default_rng(9).normal(0.0, 1e-3, obs.shape)
+    ctx.rf_nodes(lmcase.NODES)
+    opts = fz.LMOpts(maxsteps=5, maxit=40, isigma=1e-3, dchi2=1e-3)
+    _, chi_p, it_p, st_p = ctx.invert(obs, ws.default_models(npix, nz), hydrostatic=True, opts=opts)
+    _, chi_w, it_w, st_w = ctx.invert(obs, warm.initial_models(obs), hydrostatic=True, opts=opts)
+    assert np.all(st_p == 0) and np.all(st_w == 0)
+    assert np.median(chi_w) < np.median(chi_p), (np.median(chi_w), np.median(chi_p))
+    assert it_w.mean() <= it_p.mean() + 1.0
