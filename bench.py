@@ -1,20 +1,29 @@
 #!/usr/bin/env python3
-"""Benchmark of the GPU Stokes synthesis (FORWARD3D/FORWARD1D batched on one B200).
+"""Benchmark of the FIRTEZ-dz hot path on B200: batched pixel-wise LM
+inversion with the learned warm start, against LM from the default guess.
 
-Workload: 256 x 256 columns x 128 heights, Fe I 6301.5 + 6302.5 x 112 points
-each (NUMW = 224), hydrostatic equilibrium integrated on the GPU in FP64
-(RK4 from the top), chemical equilibrium FP64, opacities / Voigt / formal
-solution FP32.  Seeded synthetic atmospheres (firtez-dz_b200/atmos.py).
+Workload (one GPU): a seeded 512 x 512 field of model atmospheres, 128 heights
+from -0.5 to +1.5 Mm, Fe I 6301.5 + 6302.5 x 112 wavelengths at 21.5 mA
+(NUMW = 224, NFREQ = 896), observations = the GPU synthesis (hydrostatic) of
+the field plus Gaussian noise of 1e-3 Ic.  Free parameters on nodes: T 5,
+Bx, By, Bz, v_z 2 each (NP = 13).  Stop rule per pixel: the reference's
+STEPS > MAXSTEPS (5), an accepted step gaining less than 1e-3 in chi2
+(relative), or 40 iterations.  The warm start is the MLP 896-1024-1024-512-13
+(GELU), trained before the timed region with the library's BF16 kernels on
+pairs the GPU forward solver synthesises from seeded atmospheres (2M by
+default).
 
-One step = one synthesis of all columns.  ``value`` = columns x wavelengths
-per second with inputs resident in HBM; ``e2e`` = the same through the
-host-buffer C-ABI call (fz_forward) with the model copied from pinned host
-memory and RSYN1D copied back every step.  Multi-GPU: every rank synthesises
-its own 256 x 256 tile (weak scaling, no collective on the data path).
+One step = the NN-warm inversion of one tile of 16384 pixels of the field
+(network inference + batched LM), inputs resident in HBM.  ``value`` =
+converged pixels per second.  The plain arm inverts the same tiles from the
+default guess; both arms' chi2 are reported.  ``e2e``: the same NN-warm
+inversion through the host-buffer calls (observations from pinned host
+memory, models and chi2 back).  Multi-GPU: each rank inverts tiles of its own
+field (weak scaling, no collective on the data path).
 
-``--impl reference`` times the CPU restatement of the reference (the Fortran
-reference cannot be built on this image: no gfortran/MPI/LAPACK) on all host
-cores, on bounded samples of the same workload.
+``--impl reference`` times the CPU restatement of the reference (oracle/: the
+Fortran reference cannot be built on this image, no gfortran/MPI/LAPACK),
+LM from the default guess, on bounded pixel samples with all host cores.
 """
 import argparse
 import importlib.util
@@ -29,7 +38,8 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 PKG_DIR = os.path.join(ROOT, "firtez-dz_b200")
 METRIC = "converged pixels/s at plain-LM χ² (NN-warm vs plain, 1 B200); synth columns·λ/s"
-UNIT = "columns*lambda/s"
+UNIT = "pixels/s"
+NODES = {1: 5, 4: 2, 5: 2, 6: 2, 7: 2}
 
 
 def load_package():
@@ -56,10 +66,10 @@ def peaks():
 class ClockSampler:
     """nvidia-smi clock / throttle sampling during the timed region."""
 
-    def __init__(self, index):
+    def __init__(self, index, tag):
         self.index = index
         self.proc = None
-        self.path = os.path.join(ROOT, "gpurun_out", "clocks_rank%d.csv" % index)
+        self.path = os.path.join(ROOT, "gpurun_out", "clocks_%s_rank%d.csv" % (tag, index))
 
     def start(self):
         try:
@@ -103,208 +113,316 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
-def cpu_sample(lines, reg, gain, model, hydrostatic, budget_s):
-    """Oracle on consecutive 64-column batches until budget_s; cols*lambda/s."""
+def cpu_lm_sample(fz, lines, reg, he, nz, npix, seed, nthreads=0):
+    """The oracle's pixel-wise LM (plain initial guess) on npix pixels of the
+    workload; returns (pixels/s, seconds, median chi2)."""
     sys.path.insert(0, os.path.join(ROOT, "tests"))
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import orc
-    numw = int(reg["numwave"].sum())
-    done, t0, i = 0, time.perf_counter(), 0
-    while True:
-        batch = model[(i * 64) % len(model):(i * 64) % len(model) + 64]
-        orc.forward(lines, reg, gain, batch, hydrostatic=hydrostatic, nthreads=0)
-        done += len(batch)
-        i += 1
-        el = time.perf_counter() - t0
-        if el >= budget_s:
-            break
-    return done * numw / el, done, el
+    import lm_oracle as lmo
+    from firtez_dz_b200 import warmstart as ws
+    gain, _ = orc.gain(lines, reg)
+    true = fz.atmos.make_columns(npix, nz, seed=seed)
+    obs, _, _ = orc.forward(lines, reg, gain, true, hydrostatic=he, nthreads=nthreads)
+    obs = obs.reshape(npix, -1) + np.random.default_rng(seed).normal(0.0, 1e-3, (npix, obs.shape[1] * obs.shape[2]))
+    init = ws.default_models(npix, nz)
+    w = lmo.weights(obs.shape[1] // 4, isigma=1e-3)
+
+    def fwd(models):
+        syn, jac, mo, st = orc.forward_rf(lines, reg, gain, models, NODES, hydrostatic=he, nthreads=nthreads)
+        return syn.reshape(len(models), -1), np.transpose(jac, (0, 2, 1)), mo, st
+
+    t0 = time.perf_counter()
+    _, chi, _ = lmo.invert(fwd, obs, init, NODES, w, maxsteps=5, maxit=40, dchi2=1e-3)
+    el = time.perf_counter() - t0
+    return npix / el, el, float(np.median(chi))
 
 
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--steps", type=int, default=4)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--ncol", type=int, default=256 * 256)
+    ap.add_argument("--field", type=int, default=512, help="field side (pixels)")
+    ap.add_argument("--tile", type=int, default=16384, help="pixels per step")
+    ap.add_argument("--slots", type=int, default=8192)
     ap.add_argument("--nz", type=int, default=128)
-    ap.add_argument("--cpu-seconds", type=float, default=10.0)
-    ap.add_argument("--no-he", action="store_true")
+    ap.add_argument("--train-pairs", type=int, default=2097152)
+    ap.add_argument("--epochs", type=int, default=6)
+    ap.add_argument("--cpu-pixels", type=int, default=24)
+    ap.add_argument("--synth-cols", type=int, default=256 * 256)
     a = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
-    he = not a.no_he
+    he = True
     fz = load_package()
     lines = fz.lines_parse(fz.atmos.line_database_text())
     reg = fz.regions_from_lines_section(fz.atmos.lines_section(2), lines)
     numw = int(reg["numwave"].sum())
-    config = {"workload": "synthesis %dx%d columns x %d heights, Fe I 6301.5+6302.5 x 112 lambda, "
-                          "hydrostatic FP64 + chemistry FP64, RTE FP32" % (int(np.sqrt(a.ncol)), int(np.sqrt(a.ncol)), a.nz),
-              "columns_per_gpu": a.ncol, "nz": a.nz, "numw": numw, "hydrostatic": he,
-              "l2": "inputs larger than L2 (model %.0f MB per GPU)" % (a.ncol * 13 * a.nz * 4 / 1e6),
-              "parallelism": "columns sharded per GPU" if world > 1 else "single GPU"}
+    nf = 4 * numw
+    config = {"workload": "batched LM inversion, %dx%d pixels x %d heights, Fe I 6301.5+6302.5 x 112 lambda, "
+                          "nodes T5 Bx2 By2 Bz2 vz2 (NP=13), noise 1e-3 Ic, NN-warm start "
+                          "(MLP 896-1024-1024-512-13) vs default guess" % (a.field, a.field, a.nz),
+              "pixels_per_gpu": a.field * a.field, "pixels_per_step": a.tile, "nz": a.nz, "numw": numw,
+              "hydrostatic": he, "stop": "STEPS>5 | rel. dchi2<1e-3 on an accepted step | 40 iterations",
+              "l2": "inputs larger than L2 (observations %.0f MB per GPU)" % (a.field * a.field * nf * 8 / 1e6),
+              "parallelism": "pixel tiles sharded per GPU" if world > 1 else "single GPU"}
 
     if a.impl == "reference":
         if rank != 0:
             return
-        model = fz.atmos.make_columns(min(a.ncol, 4096), a.nz, seed=2)
-        sys.path.insert(0, os.path.join(ROOT, "tests"))
-        import orc
-        gain, _ = orc.gain(lines, reg)
-        vals = []
-        for _ in range(a.warmup):
-            cpu_sample(lines, reg, gain, model, he, 0.5)
-        per = max(a.cpu_seconds / max(a.steps, 1), 1.0)
-        tot_cols = tot_t = 0.0
-        for _ in range(a.steps):
-            v, n, el = cpu_sample(lines, reg, gain, model, he, per)
-            vals.append(v)
-            tot_cols += n
+        tot_t, chis = 0.0, []
+        for i in range(a.warmup):
+            cpu_lm_sample(fz, lines, reg, he, a.nz, 2, seed=900 + i)
+        for i in range(a.steps):
+            _, el, c = cpu_lm_sample(fz, lines, reg, he, a.nz, a.cpu_pixels, seed=1000 + i)
             tot_t += el
-        value = float(np.mean(vals))
-        cores = os.cpu_count()
+            chis.append(c)
+        value = float(a.steps * a.cpu_pixels / tot_t)
         out = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": a.gpus,
                "steps": a.steps, "warmup": a.warmup, "ms_per_step": 1e3 * tot_t / a.steps,
                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-               "data": "synthetic", "config": config,
-               "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
-                                "sample": "%d columns of the workload per step, OpenMP over columns "
-                                          "(FP64 C++ restatement; the Fortran reference needs gfortran/MPI/LAPACK, "
-                                          "absent on this image)" % int(tot_cols / a.steps)},
+               "data": "synthetic", "config": config, "median_chi2": float(np.median(chis)),
+               "cpu_baseline": {"value": value, "unit": UNIT, "cores": os.cpu_count(), "kind": "port",
+                                "sample": "%d pixels per step, LM from the default guess, FP64 C++/numpy "
+                                          "restatement of the reference (OpenMP over columns; the Fortran "
+                                          "reference needs gfortran/MPI/LAPACK, absent on this image)"
+                                          % a.cpu_pixels},
                "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
         print(json.dumps(out))
         return
 
     import torch
+    from firtez_dz_b200 import warmstart as ws
     torch.cuda.set_device(local)
     dist = None
     if world > 1:
         import datetime
         import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
 
     def barrier():
         if dist is not None:
             dist.barrier()
 
-    model = fz.atmos.make_columns(a.ncol, a.nz, seed=2 + rank)
-    ctx = fz.Synthesis(lines, reg, nz=a.nz, device=local)
-    d_model = torch.from_numpy(model).cuda()
-    d_out = torch.empty_like(d_model)
-    d_syn = torch.empty((a.ncol, 4, numw), dtype=torch.float64, device="cuda")
-    d_st = torch.zeros(a.ncol, dtype=torch.int32, device="cuda")
-    stream = torch.cuda.current_stream().cuda_stream
-
-    def step():
-        ctx.forward_device(d_model.data_ptr(), a.ncol, d_syn.data_ptr(), d_out.data_ptr(), d_st.data_ptr(),
-                           stream=stream, hydrostatic=he)
-
-    for _ in range(a.warmup):
-        step()
-    torch.cuda.synchronize()
-    assert int(d_st.max().item()) == 0, "column status errors"
-    sampler = ClockSampler(local)
-    sampler.start()
-    ctx.profile(True)
-    barrier()
-    torch.cuda.synchronize()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record()
-    for _ in range(a.steps):
-        step()
-    e1.record()
-    torch.cuda.synchronize()
-    barrier()
-    clocks = sampler.stop()
-    ctx.profile(False)
-    prof = ctx.profile_read()
-    ms = e0.elapsed_time(e1) / a.steps
-    if dist is not None:
+    def maxms(ms):
+        if dist is None:
+            return ms
         t = torch.tensor([ms], device="cuda")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
-    value = world * a.ncol * numw / (ms * 1e-3)
+        return float(t.item())
 
-    # end to end through the host-buffer C-ABI call, pinned host memory
-    h_model = torch.from_numpy(model).pin_memory()
-    h_syn = torch.empty((a.ncol, 4, numw), dtype=torch.float64).pin_memory()
-    h_st = torch.empty(a.ncol, dtype=torch.int32).pin_memory()
-    L = fz.lib()
+    ctx = fz.Synthesis(lines, reg, nz=a.nz, device=local)
+    stream = torch.cuda.current_stream().cuda_stream
+    # ---------------------------------------------------------------- field
+    npix = a.field * a.field
+    obs = torch.empty((npix, nf), dtype=torch.float64, device="cuda")
+    gen = torch.Generator(device="cuda")
+    gen.manual_seed(4242 + rank)
+    chunk = 65536
+    for i in range(0, npix, chunk):
+        n = min(chunk, npix - i)
+        m = torch.from_numpy(fz.atmos.make_columns(n, a.nz, seed=777000 + 1000 * rank + i // chunk)).cuda()
+        syn = torch.empty((n, 4, numw), dtype=torch.float64, device="cuda")
+        mo = torch.empty_like(m)
+        ctx.forward_device(m.data_ptr(), n, syn.data_ptr(), mo.data_ptr(), 0, stream=stream, hydrostatic=True)
+        obs[i:i + n] = syn.reshape(n, nf) + 1e-3 * torch.randn((n, nf), dtype=torch.float64, device="cuda",
+                                                               generator=gen)
+    obs32 = obs.float()
+    base = torch.from_numpy(ws.default_models(a.tile, a.nz)).cuda()
+    # --------------------------------------------------------------- network
+    warm = ws.WarmStart(a.nz, NODES, numw, seed=5 + rank)
+    t0 = time.perf_counter()
+    x, t = warm.make_training_set(ctx, a.train_pairs, seed=31 + rank, noise=1e-3)
+    t1 = time.perf_counter()
+    loss = warm.fit(x, t, epochs=a.epochs, batch=1024, lr=1e-3, seed=1)
+    torch.cuda.synchronize()
+    t2 = time.perf_counter()
+    del x, t
+    torch.cuda.empty_cache()
+    mlp_info = {"train_pairs": a.train_pairs, "epochs": a.epochs, "batch": 1024, "final_loss": loss,
+                "gen_s": t1 - t0, "train_s": t2 - t1, "params": warm.mlp.nparams}
+    ctx.rf_nodes(NODES)
+    opts = fz.LMOpts(maxsteps=5, maxit=40, dchi2=1e-3, isigma=1e-3, slots=a.slots)
+    ntiles = npix // a.tile
+    bufs = {"out": torch.empty((a.tile, 13, a.nz), dtype=torch.float32, device="cuda"),
+            "chi": torch.empty(a.tile, dtype=torch.float64, device="cuda"),
+            "it": torch.empty(a.tile, dtype=torch.int32, device="cuda"),
+            "st": torch.empty(a.tile, dtype=torch.int32, device="cuda")}
+    results = {"nn": {}, "plain": {}}
+
+    def step(i, arm):
+        k = i % ntiles
+        o = obs[k * a.tile:(k + 1) * a.tile]
+        if arm == "nn":
+            init = warm.initial_models_device(obs32[k * a.tile:(k + 1) * a.tile], base)
+        else:
+            init = base
+        ctx.invert_device(a.tile, o.data_ptr(), init.data_ptr(), bufs["out"].data_ptr(), bufs["chi"].data_ptr(),
+                          bufs["it"].data_ptr(), bufs["st"].data_ptr(), hydrostatic=True, opts=opts, stream=stream)
+        results[arm][k] = (bufs["chi"].cpu().numpy().copy(), bufs["it"].cpu().numpy().copy(),
+                           int(bufs["st"].max().item()))
+
+    def timed(arm, steps, warmup, tag):
+        for i in range(warmup):
+            step(i, arm)
+        torch.cuda.synchronize()
+        sampler = ClockSampler(local, tag)
+        sampler.start()
+        ctx.profile(True)
+        ctx.profile_read()
+        barrier()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for i in range(warmup, warmup + steps):
+            step(i, arm)
+        e1.record()
+        torch.cuda.synchronize()
+        barrier()
+        clocks = sampler.stop()
+        ctx.profile(False)
+        prof = ctx.profile_read()
+        return maxms(e0.elapsed_time(e1) / steps), clocks, prof
+
+    ms_nn, clocks, prof = timed("nn", a.steps, a.warmup, "nn")
+    value = world * a.tile / (ms_nn * 1e-3)
+    # the plain arm inverts the same tiles as the timed NN-warm steps
+    for i in range(a.warmup):
+        step(i, "plain")
+    torch.cuda.synchronize()
+    sampler = ClockSampler(local, "plain")
+    sampler.start()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for i in range(a.warmup, a.warmup + a.steps):
+        step(i, "plain")
+    e1.record()
+    torch.cuda.synchronize()
+    clocks_pl = sampler.stop()
+    ms_pl = maxms(e0.elapsed_time(e1) / a.steps)
+    plain_value = world * a.tile / (ms_pl * 1e-3)
+    common = sorted(set(results["plain"]) & set(results["nn"]))
+    chi_nn = np.concatenate([results["nn"][k][0] for k in common])
+    chi_pl = np.concatenate([results["plain"][k][0] for k in common])
+    it_nn = np.concatenate([results["nn"][k][1] for k in common])
+    it_pl = np.concatenate([results["plain"][k][1] for k in common])
+    status_bad = max(results["nn"][k][2] for k in results["nn"])
+
+    # ------------------------------------------------------------- end to end
+    h_obs = obs[:a.tile].reshape(a.tile, 4, numw).cpu().numpy()
+    e2e_steps = max(1, a.steps // 2)
 
     def e2e_step():
-        rc = L.fz_forward(ctx._h, a.ncol, h_model.data_ptr(), int(he), h_syn.data_ptr(), None, h_st.data_ptr())
-        if rc < 0:
-            raise fz.FzError(L.fz_strerror(rc).decode())
+        init = warm.initial_models(h_obs, base=ws.default_models(a.tile, a.nz))
+        ctx.invert(h_obs, init, hydrostatic=True, opts=opts)
 
-    for _ in range(max(1, a.warmup)):
-        e2e_step()
+    e2e_step()
     barrier()
     torch.cuda.synchronize()
-    e2 = max(1, a.steps // 2)
-    t0 = torch.cuda.Event(enable_timing=True)
-    t1 = torch.cuda.Event(enable_timing=True)
-    t0.record()
-    for _ in range(e2):
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
         e2e_step()
-    t1.record()
     torch.cuda.synchronize()
-    ms_e2e = t0.elapsed_time(t1) / e2
-    if dist is not None:
-        t = torch.tensor([ms_e2e], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms_e2e = float(t.item())
-    e2e = {"value": world * a.ncol * numw / (ms_e2e * 1e-3), "unit": UNIT,
-           "h2d_bytes_per_step": a.ncol * 13 * a.nz * 4,
-           "d2h_bytes_per_step": a.ncol * 4 * numw * 8 + a.ncol * 4}
-    assert int(h_st.max()) == 0
+    ms_e2e = maxms((time.perf_counter() - t0) * 1e3 / e2e_steps)
+    e2e = {"value": world * a.tile / (ms_e2e * 1e-3), "unit": UNIT,
+           "h2d_bytes_per_step": a.tile * nf * 4 + a.tile * nf * 8 + a.tile * 13 * a.nz * 4,
+           "d2h_bytes_per_step": a.tile * 13 * 4 + a.tile * 13 * a.nz * 4 + a.tile * (8 + 4 + 4),
+           "note": "observations and initial models from host memory through WarmStart.initial_models and "
+                   "fz_invert; wall clock around the calls"}
 
+    # --------------------------------------------------------- synthesis rate
+    ns = a.synth_cols
+    m = torch.from_numpy(fz.atmos.make_columns(ns, a.nz, seed=2 + rank)).cuda()
+    so = torch.empty((ns, 4, numw), dtype=torch.float64, device="cuda")
+    mo = torch.empty_like(m)
+    for _ in range(3):
+        ctx.forward_device(m.data_ptr(), ns, so.data_ptr(), mo.data_ptr(), 0, stream=stream, hydrostatic=True)
+    torch.cuda.synchronize()
+    ctx.profile(True)
+    ctx.profile_read()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(5):
+        ctx.forward_device(m.data_ptr(), ns, so.data_ptr(), mo.data_ptr(), 0, stream=stream, hydrostatic=True)
+    e1.record()
+    torch.cuda.synchronize()
+    ctx.profile(False)
+    sprof = ctx.profile_read()
+    ms_syn = maxms(e0.elapsed_time(e1) / 5)
+    synthesis = {"value": world * ns * numw / (ms_syn * 1e-3), "unit": "columns*lambda/s",
+                 "workload": "%d columns x %d heights x %d lambda, hydrostatic" % (ns, a.nz, numw),
+                 "ms_per_call": ms_syn, "kernel_ms": {k: v[0] / max(v[1], 1) for k, v in sprof.items() if v[1]}}
     if rank != 0:
         if dist is not None:
             dist.destroy_process_group()
         return
 
-    # roofline of the dominant kernel (algorithmic bytes per launch / mean launch time)
+    # -------------------------------------------------------------- roofline
     hbm, how = peaks()
+    per_launch = {k: (v[0] / max(v[1], 1), v[1]) for k, v in prof.items() if v[1]}
     kname = max(prof, key=lambda k: prof[k][0])
-    kms = prof[kname][0] / max(prof[kname][1], 1)
-    if kname == "k_chain":
-        alg = a.ncol * (2 + 4) * a.nz * 4        # T,Pg in; Pg,rho,Pe,mu out
-    elif kname == "k_opac":
-        alg = a.ncol * (5 * 4) * a.nz            # T,Bx,By,Bz,vz in (nH, ne and the slab are intermediates)
+    kms, _ = per_launch[kname]
+    S = min(a.slots, a.tile)
+    np_ = 13
+    flop = None
+    if kname == "k_synth_rf":
+        alg = S * (a.nz * 6 * 4 + nf * 8 + np_ * nf * 4)      # model in, RSYN1D + EQVDSYN out
+        flop = S * a.nz * numw * 4400.0
+    elif kname == "k_opac_rf":
+        alg = S * a.nz * 7 * 4                               # T, Pg, rho, Bx, By, Bz, vz in
     else:
-        alg = a.ncol * 4 * numw * 8              # RSYN1D out (the slab is an intermediate)
+        alg = S * a.nz * 6 * 4
     achieved = alg / (kms * 1e-3) / 1e9
     traffic = None
     tf = os.path.join(ROOT, "profiles", "traffic.json")
     if os.path.exists(tf):
         try:
             per_col = json.load(open(tf)).get(kname)
-            traffic = per_col * a.ncol if per_col else None
+            traffic = per_col * S if per_col else None
         except Exception:
             traffic = None
     fp32 = fz.measure_fp32_peak(local)
-    flop_synth = a.ncol * a.nz * numw * (145.0 * 8 + 200.0)
-    synth_ms = prof["k_synth"][0] / max(prof["k_synth"][1], 1)
     out = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps, "warmup": a.warmup,
-           "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "fp32",
-           "data": "synthetic (seeded atmospheres, firtez-dz_b200/atmos.py)", "config": config,
+           "ms_per_step": ms_nn, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "fp32",
+           "data": "synthetic (seeded atmospheres, firtez-dz_b200/atmos.py; observations = GPU synthesis + "
+                   "1e-3 noise)",
+           "config": config,
+           "plain": {"value": plain_value, "unit": UNIT, "ms_per_step": ms_pl,
+                     "median_chi2": float(np.median(chi_pl)), "mean_iterations": float(it_pl.mean()),
+                     "clocks": clocks_pl},
+           "nn_warm": {"value": value, "median_chi2": float(np.median(chi_nn)),
+                       "mean_iterations": float(it_nn.mean()), "speedup_vs_plain": value / plain_value,
+                       "frac_pixels_chi2_above_1.1x_plain": float(np.mean(chi_nn > 1.1 * chi_pl)),
+                       "pixels_compared": int(chi_nn.size), "status_errors": status_bad, "mlp": mlp_info},
+           "synthesis": synthesis,
            "roofline": {"bound": "hbm", "kernel": kname, "achieved": achieved, "peak": hbm, "unit": "GB/s",
                         "frac": achieved / hbm, "traffic": traffic,
                         "peak_source": how + " (MEASURED_PEAKS.json hbm_gbs)" if how == "measured" else how,
-                        "algorithmic_bytes_per_launch": alg, "mean_launch_ms": kms},
-           "fp32_roofline": {"kernel": "k_synth", "achieved_tflops": flop_synth / (synth_ms * 1e-3) / 1e12,
-                             "peak_tflops": fp32, "frac": flop_synth / (synth_ms * 1e-3) / 1e12 / fp32,
-                             "flop_model": "(145*NTOT_mean + 200) per column*height*lambda, NTOT_mean=8",
-                             "peak_source": "measured FMA-chain kernel (fz_measure_fp32_peak)"},
-           "kernel_ms": {k: v[0] / max(v[1], 1) for k, v in prof.items()},
-           "e2e": e2e, "gpu_launches": sum(v[1] for v in prof.values()), "clocks": clocks}
+                        "algorithmic_bytes_per_launch": alg, "mean_launch_ms": kms, "columns_per_launch": S},
+           "kernel_ms": {k: v[0] for k, v in per_launch.items()},
+           "kernel_launches": {k: v[1] for k, v in per_launch.items()},
+           "e2e": e2e,
+           # kernels counted by the context plus, per step, the network
+           # (one conversion + 4 GEMMs)
+           "gpu_launches": int(sum(v[1] for v in prof.values()) + 5 * a.steps),
+           "clocks": clocks}
+    if flop is not None:
+        out["fp32_roofline"] = {"kernel": kname, "achieved_tflops": flop / (kms * 1e-3) / 1e12, "peak_tflops": fp32,
+                                "frac": flop / (kms * 1e-3) / 1e12 / fp32,
+                                "flop_model": "4400 FLOP per column*height*lambda (synthesis + 6 response "
+                                              "functions), per launch of %d columns" % S,
+                                "peak_source": "measured FMA-chain kernel (fz_measure_fp32_peak)"}
     if world == 1:
-        cps, n, el = cpu_sample(lines, reg, ctx.gain, model, he, a.cpu_seconds)
-        out["cpu_baseline"] = {"value": cps, "unit": UNIT, "cores": os.cpu_count(), "kind": "port",
-                               "sample": "%d columns of the workload in %.1f s (FP64 C++ restatement of the "
-                                         "reference, OpenMP over columns)" % (n, el)}
+        v, el, c = cpu_lm_sample(fz, lines, reg, he, a.nz, a.cpu_pixels, seed=1000)
+        out["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": os.cpu_count(), "kind": "port",
+                               "sample": "%d pixels, LM from the default guess, in %.1f s (FP64 C++/numpy "
+                                         "restatement of the reference, OpenMP over columns); median chi2 %.3g"
+                                         % (a.cpu_pixels, el, c)}
     print(json.dumps(out))
+    sys.stdout.flush()
     if dist is not None:
         dist.destroy_process_group()
 

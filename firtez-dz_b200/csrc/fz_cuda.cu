@@ -1069,7 +1069,7 @@ LineP host_line(const fz_line& L, double wdif, const Consts& K) {
 
 }  // namespace
 
-constexpr int NKERN = 5;   // k_chain, k_opac, k_synth, k_opac_rf, k_synth_rf
+constexpr int NKERN = 10;   // k_chain, k_opac, k_synth, k_opac_rf, k_synth_rf, k_lm_fill, k_lm_accept, k_lm_normal, k_lm_solve, k_lm_update
 
 struct fz_ctx {
   int device = 0;
@@ -1101,8 +1101,8 @@ struct fz_ctx {
     cudaEvent_t a, b;
   };
   std::vector<Pending> pending;
-  double prof_ms[NKERN] = {0, 0, 0, 0, 0};
-  int prof_n[NKERN] = {0, 0, 0, 0, 0};
+  double prof_ms[NKERN] = {};
+  int prof_n[NKERN] = {};
   // response functions: node layout, hat coefficients (nz x np), RF slab
   RFConf rf{};
   RFConf* d_rf = nullptr;
@@ -1741,18 +1741,33 @@ int fz_invert_device(fz_ctx* c, int npix, const double* d_obs, const float* d_in
   FZ_CK(cudaMemsetAsync(c->d_q, 0, sizeof(LMQueue), s));
   if (d_status) FZ_CK(cudaMemsetAsync(d_status, 0, npix * sizeof(int), s));
   const LMSlots L = c->lm;
-  k_lm_fill<<<S, 128, 0, s>>>(C, L, c->d_q, d_obs, d_init);
+  {
+    ProfScope ps(c, 5, s);
+    k_lm_fill<<<S, 128, 0, s>>>(C, L, c->d_q, d_obs, d_init);
+  }
   FZ_CK(cudaGetLastError());
   const size_t usm = (size_t)(C.nz + 3 * C.np) * sizeof(double) + (size_t)C.nz * sizeof(float);
   // every pixel needs at most maxit iterations; slots are refilled at once
   const long long cap = (long long)C.maxit * ((npix + S - 1) / S + 1) + 8;
   for (long long it = 0; it < cap; ++it) {
     if ((rc = launch_forward_rf(c, S, L.mcur, hydrostatic, L.syn, L.jac, L.mcur, L.status, s))) return rc;
-    k_lm_accept<<<S, 256, 0, s>>>(C, L, c->d_q, d_w, d_obs, d_init, d_model_out, d_chi2, d_iters, d_syn_out,
-                                  d_status);
-    k_lm_normal<<<(S + 3) / 4, 128, 0, s>>>(C, L, d_w);
-    k_lm_solve<<<(S + 3) / 4, 128, 0, s>>>(C, L);
-    k_lm_update<<<S, 128, usm, s>>>(C, L, c->d_coef64);
+    {
+      ProfScope ps(c, 6, s);
+      k_lm_accept<<<S, 256, 0, s>>>(C, L, c->d_q, d_w, d_obs, d_init, d_model_out, d_chi2, d_iters, d_syn_out,
+                                    d_status);
+    }
+    {
+      ProfScope ps(c, 7, s);
+      k_lm_normal<<<(S + 3) / 4, 128, 0, s>>>(C, L, d_w);
+    }
+    {
+      ProfScope ps(c, 8, s);
+      k_lm_solve<<<(S + 3) / 4, 128, 0, s>>>(C, L);
+    }
+    {
+      ProfScope ps(c, 9, s);
+      k_lm_update<<<S, 128, usm, s>>>(C, L, c->d_coef64);
+    }
     FZ_CK(cudaGetLastError());
     FZ_CK(cudaMemcpyAsync(c->h_done, &c->d_q->done, sizeof(int), cudaMemcpyDeviceToHost, s));
     FZ_CK(cudaStreamSynchronize(s));

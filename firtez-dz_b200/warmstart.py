@@ -207,6 +207,30 @@ class WarmStart:
         self.mlp.forward_device(x.shape[0], x.data_ptr(), y.data_ptr())
         return y.cpu().numpy().astype(np.float64) * self.tsd + self.tmu
 
+    def initial_models_device(self, x_obs, base):
+        """Warm-start models on the device: x_obs (npix, 4*numw) float32 raw
+        Stokes (device tensor), base (npix, 13, nz) float32 device tensor whose
+        free-parameter rows are replaced.  Returns a new device tensor."""
+        import torch
+        n = x_obs.shape[0]
+        x = ((x_obs - self.xmu) / self.xsd).contiguous()
+        y = torch.empty((n, self.nout), dtype=torch.float32, device="cuda")
+        torch.cuda.synchronize()
+        self.mlp.forward_device(n, x.data_ptr(), y.data_ptr())
+        if not hasattr(self, "_dev"):
+            self._dev = (torch.from_numpy(self.tsd.astype(np.float32)).cuda(),
+                         torch.from_numpy(self.tmu.astype(np.float32)).cuda(),
+                         {p: torch.from_numpy(self.coefs[p].T.astype(np.float32)).cuda() for p, _ in self.params})
+        tsd, tmu, ct = self._dev
+        nodes_v = y * tsd + tmu
+        m = base.clone()
+        j = 0
+        for p, row in self.params:
+            nj = self.nodes[p]
+            m[:, row] = nodes_v[:, j:j + nj] @ ct[p]
+            j += nj
+        return m
+
     def initial_models(self, obs, base=None):
         """Warm-start models for observations obs (npix, 4, numw)."""
         nodes_v = self.predict_nodes(obs)
