@@ -34,7 +34,7 @@ TEM, PG, RHO, PEL, MW, BX, BY, BZ, VX, VY, VZ, TAU5, ZZ = range(13)
 
 FZ_OK, FZ_CHEM_NOCONV, FZ_NAN = 0, 1, 2
 KERNELS = ("k_chain", "k_opac", "k_synth", "k_opac_rf", "k_synth_rf", "k_lm_fill", "k_lm_accept", "k_lm_normal",
-           "k_lm_solve", "k_lm_update")
+           "k_lm_solve", "k_lm_update", "k_chemder")
 
 # free-parameter indices of the reference (atm_param.f90 order, 1-based) that
 # carry response functions
@@ -103,7 +103,7 @@ def lib():
         L.fz_forward_rf.argtypes = [P, ctypes.c_int, P, ctypes.c_int, P, P, P, P]
         L.fz_forward_rf_device.argtypes = [P, ctypes.c_int, P, ctypes.c_int, P, P, P, P, P]
         L.fz_invert.argtypes = [P, ctypes.c_int, P, P, ctypes.c_int, P, P, P, P, P, P]
-        L.fz_invert_device.argtypes = [P, ctypes.c_int, P, P, ctypes.c_int, P, P, P, P, P, P, P]
+        L.fz_invert_device.argtypes = [P, ctypes.c_int, P, P, P, ctypes.c_int, P, P, P, P, P, P, P]
         L.fz_lm_perturbation.argtypes = [P, ctypes.c_int, ctypes.c_int, ctypes.c_int, P, P, P, ctypes.c_double, P]
         _lib = L
     return _lib
@@ -276,10 +276,12 @@ class Synthesis:
         return (mo, chi, it, st, syn) if want_syn else (mo, chi, it, st)
 
     def invert_device(self, npix, obs_ptr, init_ptr, model_out_ptr, chi2_ptr, iters_ptr, status_ptr=0, syn_ptr=0,
-                      hydrostatic=True, opts=None, stream=0):
-        """Batched LM inversion on device pointers."""
+                      hydrostatic=True, opts=None, stream=0, target_ptr=0):
+        """Batched LM inversion on device pointers (target_ptr: optional
+        per-pixel chi2 goal, float64)."""
         opts = opts or LMOpts()
         _check(lib().fz_invert_device(self._h, int(npix), ctypes.c_void_p(obs_ptr), ctypes.c_void_p(init_ptr),
+                                      ctypes.c_void_p(target_ptr) if target_ptr else None,
                                       int(bool(hydrostatic)), ctypes.byref(opts), ctypes.c_void_p(model_out_ptr),
                                       ctypes.c_void_p(chi2_ptr), ctypes.c_void_p(iters_ptr),
                                       ctypes.c_void_p(syn_ptr) if syn_ptr else None,

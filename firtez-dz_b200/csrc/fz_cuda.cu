@@ -390,14 +390,35 @@ struct RFConf {
   int nj[NSLOT], n0[NSLOT];
 };
 
-// One warp per (column, height), FP64: the synthesis slab row of k_opac plus
-// the derivative inputs.  Chemistry derivatives at the (T, Pg, NELEC) that
-// FORWARD1D passes to GET_DNHYDDTEMP (src/forward.f90:917-918); the
-// hydrostatic factor of GET_HYD_DERIVATIVES (:1050-1057) is stored as
-// c_K = DPGDTK_HE(I) / Pg(I) = -(Pg_K mu_K)_REAL*4 CTE / T_K^2 / Pg_K.
-__global__ void __launch_bounds__(128) k_opac_rf(const DevParams* __restrict__ Pg, const Consts* __restrict__ Kg,
+// One warp per (column, height), FP64, lanes over the elements: the
+// chemistry derivatives of GET_DNHYDDTEMP at the (T, Pg, NELEC) that
+// FORWARD1D passes to it (src/forward.f90:917-918).
+__global__ void __launch_bounds__(128) k_chemder(const DevParams* __restrict__ Pg, const Consts* __restrict__ Kg,
                                                  int ncol, const float* __restrict__ mout,
-                                                 const double2* __restrict__ chem, float* __restrict__ slab) {
+                                                 const double2* __restrict__ chem, double4* __restrict__ chemd) {
+  __shared__ Consts K;
+  copy_to_shared(&K, Kg);
+  __syncthreads();
+  const int nz = Pg->nz;
+  const int lane = threadIdx.x & 31;
+  const int wpb = blockDim.x >> 5;
+  const size_t total = (size_t)ncol * nz;
+  for (size_t i = (size_t)blockIdx.x * wpb + (threadIdx.x >> 5); i < total; i += (size_t)gridDim.x * wpb) {
+    const int col = (int)(i / nz), k = (int)(i % nz);
+    const float* m = mout + (size_t)col * 13 * nz;
+    const ChemDer cd = chem_der_warp((double)mget(m, nz, 0, k), (double)mget(m, nz, 1, k), chem[i].y, K, lane);
+    if (lane == 0) chemd[i] = make_double4(cd.dne_p, cd.dnh_p, cd.dne_t, cd.dnh_t);
+  }
+}
+
+// One thread per (column, height), FP64: the synthesis slab row of k_opac
+// plus the derivative inputs of the response functions.  The hydrostatic
+// factor of GET_HYD_DERIVATIVES (:1050-1057) is stored as
+// c_K = DPGDTK_HE(I) / Pg(I) = -(Pg_K mu_K)_REAL*4 CTE / T_K^2 / Pg_K.
+__global__ void __launch_bounds__(256) k_opac_rf(const DevParams* __restrict__ Pg, const Consts* __restrict__ Kg,
+                                                 int ncol, const float* __restrict__ mout,
+                                                 const double2* __restrict__ chem, const double4* __restrict__ chemd,
+                                                 float* __restrict__ slab) {
   __shared__ DevParams P;
   __shared__ Consts K;
   copy_to_shared(&P, Pg);
@@ -405,21 +426,24 @@ __global__ void __launch_bounds__(128) k_opac_rf(const DevParams* __restrict__ P
   __syncthreads();
   const int nz = P.nz, nreg = P.nreg, nlu = P.nlu;
   const int sw = rf_w(nreg, nlu);
-  const int lane = threadIdx.x & 31;
-  const int wpb = blockDim.x >> 5;
   const size_t total = (size_t)ncol * nz;
-  for (size_t i = (size_t)blockIdx.x * wpb + (threadIdx.x >> 5); i < total; i += (size_t)gridDim.x * wpb) {
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (size_t)gridDim.x * blockDim.x) {
     const int col = (int)(i / nz), k = (int)(i % nz);
     const float* m = mout + (size_t)col * 13 * nz;
     const double2 c = chem[i];
     const double nhyd = c.x, nelec = c.y;
+    const double4 d4 = chemd[i];
+    ChemDer cd;
+    cd.dne_p = d4.x;
+    cd.dnh_p = d4.y;
+    cd.dne_t = d4.z;
+    cd.dnh_t = d4.w;
     const float Tf = mget(m, nz, 0, k);
     const double T = (double)Tf;
     const double dz = (k == nz - 1) ? 1e5 * fabs((double)mget(m, nz, 12, k) - (double)mget(m, nz, 12, k - 1))
                                     : 1e5 * fabs((double)mget(m, nz, 12, k + 1) - (double)mget(m, nz, 12, k));
-    const ChemDer cd = chem_der_warp(T, (double)mget(m, nz, 1, k), nelec, K, lane);
     float* row = slab + i * sw;
-    if (lane == 0) {
+    {
       const double kc5 = opac_continuum(T, nelec, nhyd, P.cont[P.nreg]) / nhyd * (1.0 / MAMU);
       row[0] = Tf;
       row[1] = (kc5 < KC5THRESHOLD) ? 0.0f : 1.0f;
@@ -481,15 +505,15 @@ __global__ void __launch_bounds__(128) k_opac_rf(const DevParams* __restrict__ P
       }
       row[rf_he(nreg, nlu)] = (float)ck;
       row[rf_he(nreg, nlu) + 1] = pgk;
-    } else if (lane <= nreg) {
-      const int r = lane - 1;
+    }
+    for (int r = 0; r < nreg; ++r) {
       row[4 + r] = (float)(opac_continuum(T, nelec, nhyd, P.cont[r]) * dz);
       double dt, dp;
       cont_der(T, nelec, nhyd, P.cont[r], cd, dt, dp);
       row[rf_dkc(nreg, nlu) + 2 * r] = (float)(dt * dz);
       row[rf_dkc(nreg, nlu) + 2 * r + 1] = (float)(dp * dz);
-    } else if (lane >= 16 && lane < 16 + nlu) {
-      const int b = lane - 16;
+    }
+    for (int b = 0; b < nlu; ++b) {
       const LineP& L = P.lu[b];
       const double klin = opac_line(L, T, nelec, nhyd, K);
       const double damp = get_damping(L, nhyd, T);
@@ -547,7 +571,7 @@ __device__ __forceinline__ void lmap(const Geo& g, const float h[3], const float
 // Shared memory: the slab, the coefficient table (nz x np) and the node
 // accumulators (np x 4 x blockDim).
 template <bool HE>
-__global__ void __launch_bounds__(256) k_synth_rf(const DevParams* __restrict__ Pg, const RFConf* __restrict__ Rg,
+__global__ void __launch_bounds__(256, 2) k_synth_rf(const DevParams* __restrict__ Pg, const RFConf* __restrict__ Rg,
                                                   const LamP* __restrict__ lam, const float* __restrict__ gain,
                                                   int ncol, const float* __restrict__ slab,
                                                   const float* __restrict__ coefg, double* __restrict__ syn,
@@ -724,20 +748,23 @@ __global__ void __launch_bounds__(256) k_synth_rf(const DevParams* __restrict__ 
     const float n3 = fmaf(-O[12], S, fmaf(O[12], I0, fmaf(O[13], I1, fmaf(O[14], I2, O[15] * I3))));
     float rf[NSLOT][4];
     if (fin) {
+      // runtime loops over the parameters: one copy of the directional
+      // derivative per Stokes vector it acts on keeps the code in the
+      // instruction cache
       EvolW wi;
       const float win[4] = {I0 - S, I1, I2, I3};
       evol_w(es, O, win, wi);
-      evol_dir(es, wi, dtau[0], rf[0]);
-      evol_dir(es, wi, dtau[1], rf[1]);
       if (HE) {
+#pragma unroll 1
+        for (int p = 0; p < 2; ++p) evol_dir(es, wi, dtau[p], rf[p]);
         EvolW wo;
         const float wout[4] = {n0 - S, n1, n2, n3};
         evol_w(es, O, wout, wo);
-#pragma unroll
+#pragma unroll 1
         for (int p = 2; p < NSLOT; ++p) evol_dir(es, wo, dtau[p], rf[p]);
       } else {
-#pragma unroll
-        for (int p = 2; p < NSLOT; ++p) evol_dir(es, wi, dtau[p], rf[p]);
+#pragma unroll 1
+        for (int p = 0; p < NSLOT; ++p) evol_dir(es, wi, dtau[p], rf[p]);
       }
     } else {
 #pragma unroll
@@ -1069,7 +1096,7 @@ LineP host_line(const fz_line& L, double wdif, const Consts& K) {
 
 }  // namespace
 
-constexpr int NKERN = 10;   // k_chain, k_opac, k_synth, k_opac_rf, k_synth_rf, k_lm_fill, k_lm_accept, k_lm_normal, k_lm_solve, k_lm_update
+constexpr int NKERN = 11;   // k_chain, k_opac, k_synth, k_opac_rf, k_synth_rf, k_lm_fill, k_lm_accept, k_lm_normal, k_lm_solve, k_lm_update, k_chemder
 
 struct fz_ctx {
   int device = 0;
@@ -1108,6 +1135,7 @@ struct fz_ctx {
   RFConf* d_rf = nullptr;
   float* d_coef = nullptr;
   float* d_rfslab = nullptr;
+  double4* d_chemd = nullptr;   // chemistry derivatives per (column, height)
   size_t rf_cols = 0;
   float* d_jac = nullptr;   // staging of the host-buffer API
   size_t jac_cols = 0;
@@ -1212,9 +1240,12 @@ int launch_forward_rf(fz_ctx* c, int ncol, const float* d_model, int hydrostatic
   const int swr = rf_w(c->nreg, c->nlu);
   if ((size_t)ncol > c->rf_cols) {
     cudaFree(c->d_rfslab);
+    cudaFree(c->d_chemd);
     c->d_rfslab = nullptr;
+    c->d_chemd = nullptr;
     c->rf_cols = 0;
     FZ_CK(cudaMalloc(&c->d_rfslab, (size_t)ncol * c->nz * swr * sizeof(float)));
+    FZ_CK(cudaMalloc(&c->d_chemd, (size_t)ncol * c->nz * sizeof(double4)));
     c->rf_cols = ncol;
   }
   if (d_status) FZ_CK(cudaMemsetAsync(d_status, 0, ncol * sizeof(int), s));
@@ -1228,11 +1259,17 @@ int launch_forward_rf(fz_ctx* c, int ncol, const float* d_model, int hydrostatic
       k_chain<false><<<gc, wpb * 32, 0, s>>>(c->d_consts, c->d_pf, ncol, c->nz, d_model, d_mout, c->d_chem, d_status);
   }
   FZ_CK(cudaGetLastError());
+  const size_t cells = (size_t)ncol * c->nz;
+  {
+    ProfScope ps(c, 10, s);
+    const int blocks = (int)std::min<size_t>((cells + 3) / 4, (size_t)c->nsm * 32);
+    k_chemder<<<blocks, 128, 0, s>>>(c->d_params, c->d_consts, ncol, d_mout, c->d_chem, c->d_chemd);
+  }
+  FZ_CK(cudaGetLastError());
   {
     ProfScope ps(c, 3, s);
-    const size_t warps = (size_t)ncol * c->nz;
-    const int blocks = (int)std::min<size_t>((warps + 3) / 4, (size_t)c->nsm * 32);
-    k_opac_rf<<<blocks, 128, 0, s>>>(c->d_params, c->d_consts, ncol, d_mout, c->d_chem, c->d_rfslab);
+    const int b2 = (int)std::min<size_t>((cells + 255) / 256, (size_t)c->nsm * 16);
+    k_opac_rf<<<b2, 256, 0, s>>>(c->d_params, c->d_consts, ncol, d_mout, c->d_chem, c->d_chemd, c->d_rfslab);
   }
   FZ_CK(cudaGetLastError());
   const int threads = (c->numw + 31) & ~31;
@@ -1593,6 +1630,7 @@ int fz_destroy(fz_ctx* c) {
   cudaFree(c->d_rf);
   cudaFree(c->d_coef);
   cudaFree(c->d_rfslab);
+  cudaFree(c->d_chemd);
   cudaFree(c->d_jac);
   cudaFree(c->d_coef64);
   lm_free(c);
@@ -1704,6 +1742,10 @@ int fz_rf_nodes(fz_ctx* c, const int* nodes) {
   }
   FZ_CK(cudaFuncSetAttribute(k_synth_rf<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sms));
   FZ_CK(cudaFuncSetAttribute(k_synth_rf<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sms));
+  // all of the SM's unified L1/shared storage as shared memory: two CTAs of
+  // ~90 KB each can then be resident
+  FZ_CK(cudaFuncSetAttribute(k_synth_rf<true>, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
+  FZ_CK(cudaFuncSetAttribute(k_synth_rf<false>, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
   return np;
 }
 
@@ -1714,9 +1756,9 @@ int fz_forward_rf_device(fz_ctx* c, int ncol, const float* d_model, int hydrosta
   return launch_forward_rf(c, ncol, d_model, hydrostatic, d_syn, d_jac, d_model_out, d_status, (cudaStream_t)stream);
 }
 
-int fz_invert_device(fz_ctx* c, int npix, const double* d_obs, const float* d_init, int hydrostatic,
-                     const fz_lm_opts* opts, float* d_model_out, double* d_chi2, int* d_iters, double* d_syn_out,
-                     int* d_status, void* stream) {
+int fz_invert_device(fz_ctx* c, int npix, const double* d_obs, const float* d_init, const double* d_target_chi2,
+                     int hydrostatic, const fz_lm_opts* opts, float* d_model_out, double* d_chi2, int* d_iters,
+                     double* d_syn_out, int* d_status, void* stream) {
   if (!c || npix <= 0 || !d_obs || !d_init || !d_model_out || !d_chi2 || !d_iters) return FZ_ERR_ARG;
   FZ_CK(cudaSetDevice(c->device));
   LMConf C;
@@ -1753,8 +1795,8 @@ int fz_invert_device(fz_ctx* c, int npix, const double* d_obs, const float* d_in
     if ((rc = launch_forward_rf(c, S, L.mcur, hydrostatic, L.syn, L.jac, L.mcur, L.status, s))) return rc;
     {
       ProfScope ps(c, 6, s);
-      k_lm_accept<<<S, 256, 0, s>>>(C, L, c->d_q, d_w, d_obs, d_init, d_model_out, d_chi2, d_iters, d_syn_out,
-                                    d_status);
+      k_lm_accept<<<S, 256, 0, s>>>(C, L, c->d_q, d_w, d_obs, d_init, d_target_chi2, d_model_out, d_chi2, d_iters,
+                                    d_syn_out, d_status);
     }
     {
       ProfScope ps(c, 7, s);
@@ -1796,7 +1838,9 @@ int fz_invert(fz_ctx* c, int npix, const double* obs, const float* init, int hyd
     if (syn_out && (rc = cuda_fail(cudaMalloc(&d_syn, npix * nf * sizeof(double))))) break;
     if ((rc = cuda_fail(cudaMemcpyAsync(d_obs, obs, npix * nf * sizeof(double), cudaMemcpyHostToDevice, s)))) break;
     if ((rc = cuda_fail(cudaMemcpyAsync(d_init, init, npix * nm * sizeof(float), cudaMemcpyHostToDevice, s)))) break;
-    if ((rc = fz_invert_device(c, npix, d_obs, d_init, hydrostatic, opts, d_out, d_chi, d_it, d_syn, d_st, s))) break;
+    if ((rc = fz_invert_device(c, npix, d_obs, d_init, nullptr, hydrostatic, opts, d_out, d_chi, d_it, d_syn, d_st,
+                               s)))
+      break;
     if ((rc = cuda_fail(cudaMemcpyAsync(model_out, d_out, npix * nm * sizeof(float), cudaMemcpyDeviceToHost, s)))) break;
     if ((rc = cuda_fail(cudaMemcpyAsync(chi2, d_chi, npix * sizeof(double), cudaMemcpyDeviceToHost, s)))) break;
     if ((rc = cuda_fail(cudaMemcpyAsync(iters, d_it, npix * sizeof(int), cudaMemcpyDeviceToHost, s)))) break;

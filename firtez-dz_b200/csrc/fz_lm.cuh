@@ -8,7 +8,8 @@
 //   k_opac_rf, k_synth_rf);
 //   k_lm_accept   chi2, accept/revert, lambda update (NEW_CALCULATE_CHI2,
 //                 UPDATE_LAMBDA, src/get_dmodel.f90:917-1032), the weighted
-//                 residual, the per-pixel stop rule; a finished pixel writes
+//                 residual, the per-pixel stop rule (optionally a per-pixel
+//                 chi2 goal); a finished pixel writes
 //                 its best model out and its slot takes the next pixel of
 //                 the work queue (a device counter);
 //   k_lm_normal   H = Jn^T Jn on the tensor cores (mma.sync bf16, the FP32
@@ -117,7 +118,8 @@ __global__ void k_lm_fill(LMConf C, LMSlots Sl, LMQueue* q, const double* __rest
 // One CTA per slot: chi2, accept/revert, lambda, residual, stop rule, refill.
 __global__ void __launch_bounds__(256) k_lm_accept(LMConf C, LMSlots Sl, LMQueue* q, const double* __restrict__ w,
                                                    const double* __restrict__ obs_all,
-                                                   const float* __restrict__ init_all, float* __restrict__ out_model,
+                                                   const float* __restrict__ init_all,
+                                                   const double* __restrict__ target, float* __restrict__ out_model,
                                                    double* __restrict__ out_chi, int* __restrict__ out_iter,
                                                    double* __restrict__ out_syn, int* __restrict__ out_status) {
   __shared__ double red[8];
@@ -164,7 +166,9 @@ __global__ void __launch_bounds__(256) k_lm_accept(LMConf C, LMSlots Sl, LMQueue
     // the iteration cap, and an accepted step that improved chi2 by less than
     // dchi2 (relative)
     const bool small = acc && chibest < 1.0e29 && (chibest - cc) < C.dchi2 * chibest;
-    fin = steps > (double)C.maxsteps || it >= C.maxit || small;
+    // optional per-pixel goal: stop once the best chi2 reaches it
+    const bool goal = target != nullptr && chipre <= target[p];
+    fin = steps > (double)C.maxsteps || it >= C.maxit || small || goal;
     st[0] = chi;
     st[1] = chipre;
     st[2] = lam;

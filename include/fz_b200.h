@@ -175,9 +175,13 @@ typedef struct {
 int fz_invert(fz_ctx* ctx, int npix, const double* obs, const float* init, int hydrostatic,
               const fz_lm_opts* opts, float* model_out, double* chi2, int* iters, double* syn_out,
               int* status);
-int fz_invert_device(fz_ctx* ctx, int npix, const double* d_obs, const float* d_init, int hydrostatic,
-                     const fz_lm_opts* opts, float* d_model_out, double* d_chi2, int* d_iters,
-                     double* d_syn_out, int* d_status, void* stream);
+/* Device-pointer variant; d_target_chi2 (npix, may be NULL) adds a per-pixel
+ * goal: a pixel also stops once its best chi2 is at or below its goal (e.g.
+ * the chi2 another start reached on the same pixel). */
+int fz_invert_device(fz_ctx* ctx, int npix, const double* d_obs, const float* d_init,
+                     const double* d_target_chi2, int hydrostatic, const fz_lm_opts* opts,
+                     float* d_model_out, double* d_chi2, int* d_iters, double* d_syn_out, int* d_status,
+                     void* stream);
 
 /* Batched GET_PERTURBATION (src/lm.f90:137-204, SOLVER_METHOD = 1) on host
  * buffers: for each pixel H = J^T J (tensor cores, split-bf16 x3, FP32
@@ -212,7 +216,7 @@ int fz_mlp_train_device(fz_mlp* mlp, int n, const float* d_x, const float* d_t, 
  * by CUDA events on its stream; fz_profile_read returns the accumulated
  * milliseconds and launch counts of the kernels (names in order:
  * "k_chain", "k_opac", "k_synth", "k_opac_rf", "k_synth_rf", "k_lm_fill",
- * "k_lm_accept", "k_lm_normal", "k_lm_solve", "k_lm_update") and resets
+ * "k_lm_accept", "k_lm_normal", "k_lm_solve", "k_lm_update", "k_chemder") and resets
  * them; returns the kernel count.  Replaces the reference's
  * SYSTEM_CLOCK "Forward 3D:" timer (src/forward.f90:99-100, :295-297). */
 int fz_profile_enable(fz_ctx* ctx, int on);
