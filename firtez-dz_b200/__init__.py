@@ -97,7 +97,7 @@ def lib():
         L.fz_forward_device.argtypes = [P, ctypes.c_int, P, ctypes.c_int, P, P, P, P]
         L.fz_forward_device_static.argtypes = [P, ctypes.c_int, P, ctypes.c_int, P, P, P, P]
         L.fz_profile_enable.argtypes = [P, ctypes.c_int]
-        L.fz_profile_read.argtypes = [P, P, P, ctypes.c_int]
+        L.fz_profile_read.argtypes = [P, P, P, P, ctypes.c_int]
         L.fz_measure_fp32_peak.argtypes = [ctypes.c_int, P]
         L.fz_rf_nodes.argtypes = [P, P]
         L.fz_forward_rf.argtypes = [P, ctypes.c_int, P, ctypes.c_int, P, P, P, P]
@@ -213,12 +213,16 @@ class Synthesis:
     def profile(self, on=True):
         _check(lib().fz_profile_enable(self._h, int(bool(on))))
 
-    def profile_read(self):
-        """{kernel: (total ms, launches)} since the last read."""
+    def profile_read(self, items=False):
+        """{kernel: (total ms, launches[, columns or slots processed])} since
+        the last read."""
         nk = len(KERNELS)
         ms = np.zeros(nk)
         n = np.zeros(nk, dtype=np.int32)
-        _check(lib().fz_profile_read(self._h, _p(ms), _p(n), nk))
+        it = np.zeros(nk, dtype=np.int64)
+        _check(lib().fz_profile_read(self._h, _p(ms), _p(n), _p(it), nk))
+        if items:
+            return {k: (ms[i], int(n[i]), int(it[i])) for i, k in enumerate(KERNELS)}
         return {k: (ms[i], int(n[i])) for i, k in enumerate(KERNELS)}
 
     def rf_nodes(self, nodes):

@@ -1130,6 +1130,7 @@ struct fz_ctx {
   std::vector<Pending> pending;
   double prof_ms[NKERN] = {};
   int prof_n[NKERN] = {};
+  long long prof_items[NKERN] = {};
   // response functions: node layout, hat coefficients (nz x np), RF slab
   RFConf rf{};
   RFConf* d_rf = nullptr;
@@ -1141,7 +1142,8 @@ struct fz_ctx {
   size_t jac_cols = 0;
   double* d_coef64 = nullptr;   // (nz, np) hat table in FP64 for the LM update
   // LM slot pool (grown on demand)
-  LMSlots lm{};
+  LMSlots lm{}, lm2{};   // two pools: the tail of an inversion is compacted into the other one
+  int* d_dest = nullptr;
   size_t lm_cap = 0;
   int lm_np = 0;
   LMQueue* d_q = nullptr;
@@ -1176,13 +1178,15 @@ int ensure_scratch(fz_ctx* c, int ncol) {
   return 0;
 }
 
+// brackets one launch with events; `items` = columns (or slots) it processes
 struct ProfScope {
   fz_ctx* c;
   int kernel;
   cudaStream_t s;
   cudaEvent_t a = nullptr, b = nullptr;
-  ProfScope(fz_ctx* c_, int k, cudaStream_t s_) : c(c_), kernel(k), s(s_) {
+  ProfScope(fz_ctx* c_, int k, cudaStream_t s_, long long items = 0) : c(c_), kernel(k), s(s_) {
     if (!c->prof) return;
+    c->prof_items[k] += items;
     cudaEventCreate(&a);
     cudaEventCreate(&b);
     cudaEventRecord(a, s);
@@ -1202,7 +1206,7 @@ int launch_forward(fz_ctx* c, int ncol, const float* d_model, int hydrostatic, d
   const int wpb = 4;
   const dim3 gc((ncol + wpb - 1) / wpb);
   {
-    ProfScope ps(c, 0, s);
+    ProfScope ps(c, 0, s, ncol);
     if (hydrostatic)
       k_chain<true><<<gc, wpb * 32, 0, s>>>(c->d_consts, c->d_pf, ncol, c->nz, d_model, d_mout, c->d_chem, d_status);
     else
@@ -1210,7 +1214,7 @@ int launch_forward(fz_ctx* c, int ncol, const float* d_model, int hydrostatic, d
   }
   FZ_CK(cudaGetLastError());
   {
-    ProfScope ps(c, 1, s);
+    ProfScope ps(c, 1, s, ncol);
     const size_t total = (size_t)ncol * c->nz;
     const int blocks = (int)std::min<size_t>((total + 255) / 256, (size_t)c->nsm * 16);
     k_opac<<<blocks, 256, 0, s>>>(c->d_params, c->d_consts, ncol, d_mout, c->d_chem, c->d_slab);
@@ -1219,7 +1223,7 @@ int launch_forward(fz_ctx* c, int ncol, const float* d_model, int hydrostatic, d
   const int threads = (c->numw + 31) & ~31;
   const size_t sms = (size_t)c->nz * c->sw * sizeof(float);
   {
-    ProfScope ps(c, 2, s);
+    ProfScope ps(c, 2, s, ncol);
     k_synth<<<ncol, threads, sms, s>>>(c->d_params, c->d_lam, c->d_gain, ncol, c->d_slab, d_syn, d_mout, d_status);
   }
   FZ_CK(cudaGetLastError());
@@ -1252,7 +1256,7 @@ int launch_forward_rf(fz_ctx* c, int ncol, const float* d_model, int hydrostatic
   const int wpb = 4;
   const dim3 gc((ncol + wpb - 1) / wpb);
   {
-    ProfScope ps(c, 0, s);
+    ProfScope ps(c, 0, s, ncol);
     if (hydrostatic)
       k_chain<true><<<gc, wpb * 32, 0, s>>>(c->d_consts, c->d_pf, ncol, c->nz, d_model, d_mout, c->d_chem, d_status);
     else
@@ -1261,13 +1265,13 @@ int launch_forward_rf(fz_ctx* c, int ncol, const float* d_model, int hydrostatic
   FZ_CK(cudaGetLastError());
   const size_t cells = (size_t)ncol * c->nz;
   {
-    ProfScope ps(c, 10, s);
+    ProfScope ps(c, 10, s, ncol);
     const int blocks = (int)std::min<size_t>((cells + 3) / 4, (size_t)c->nsm * 32);
     k_chemder<<<blocks, 128, 0, s>>>(c->d_params, c->d_consts, ncol, d_mout, c->d_chem, c->d_chemd);
   }
   FZ_CK(cudaGetLastError());
   {
-    ProfScope ps(c, 3, s);
+    ProfScope ps(c, 3, s, ncol);
     const int b2 = (int)std::min<size_t>((cells + 255) / 256, (size_t)c->nsm * 16);
     k_opac_rf<<<b2, 256, 0, s>>>(c->d_params, c->d_consts, ncol, d_mout, c->d_chem, c->d_chemd, c->d_rfslab);
   }
@@ -1275,7 +1279,7 @@ int launch_forward_rf(fz_ctx* c, int ncol, const float* d_model, int hydrostatic
   const int threads = (c->numw + 31) & ~31;
   const size_t sms = rf_smem(c);
   {
-    ProfScope ps(c, 4, s);
+    ProfScope ps(c, 4, s, ncol);
     if (hydrostatic)
       k_synth_rf<true><<<ncol, threads, sms, s>>>(c->d_params, c->d_rf, c->d_lam, c->d_gain, ncol, c->d_rfslab,
                                                   c->d_coef, d_syn, d_jac, d_mout, d_status);
@@ -1287,8 +1291,7 @@ int launch_forward_rf(fz_ctx* c, int ncol, const float* d_model, int hydrostatic
   return 0;
 }
 
-void lm_free(fz_ctx* c) {
-  LMSlots& L = c->lm;
+void lm_free_pool(LMSlots& L) {
   cudaFree(L.pix);
   cudaFree(L.skip);
   cudaFree(L.iter);
@@ -1306,16 +1309,17 @@ void lm_free(fz_ctx* c) {
   cudaFree(L.delta);
   cudaFree(L.status);
   L = LMSlots{};
+}
+
+void lm_free(fz_ctx* c) {
+  lm_free_pool(c->lm);
+  lm_free_pool(c->lm2);
+  cudaFree(c->d_dest);
+  c->d_dest = nullptr;
   c->lm_cap = 0;
 }
 
-// slot pool for S slots of the current node layout
-int lm_alloc(fz_ctx* c, int S) {
-  const int np = c->rf.np, nf = 4 * c->numw, nm = 13 * c->nz;
-  if ((size_t)S <= c->lm_cap && c->lm.S == S && c->lm_np == np) return 0;
-  lm_free(c);
-  c->lm_np = np;
-  LMSlots& L = c->lm;
+int lm_alloc_pool(LMSlots& L, int S, int np, int nf, int nm) {
   L.S = S;
   FZ_CK(cudaMalloc(&L.pix, S * sizeof(int)));
   FZ_CK(cudaMalloc(&L.skip, S * sizeof(int)));
@@ -1333,6 +1337,22 @@ int lm_alloc(fz_ctx* c, int S) {
   FZ_CK(cudaMalloc(&L.g, (size_t)S * np * sizeof(double)));
   FZ_CK(cudaMalloc(&L.delta, (size_t)S * np * sizeof(double)));
   FZ_CK(cudaMalloc(&L.status, (size_t)S * sizeof(int)));
+  return 0;
+}
+
+// slot pools for S slots of the current node layout
+int lm_alloc(fz_ctx* c, int S) {
+  const int np = c->rf.np, nf = 4 * c->numw, nm = 13 * c->nz;
+  if ((size_t)S <= c->lm_cap && c->lm.S == S && c->lm_np == np) return 0;
+  lm_free(c);
+  c->lm_np = np;
+  int rc = lm_alloc_pool(c->lm, S, np, nf, nm);
+  if (!rc) rc = lm_alloc_pool(c->lm2, S, np, nf, nm);
+  if (!rc) rc = cuda_fail(cudaMalloc(&c->d_dest, S * sizeof(int)));
+  if (rc) {
+    lm_free(c);
+    return rc;
+  }
   c->lm_cap = S;
   return 0;
 }
@@ -1651,7 +1671,7 @@ int fz_profile_enable(fz_ctx* c, int on) {
   return 0;
 }
 
-int fz_profile_read(fz_ctx* c, double* ms, int* launches, int n) {
+int fz_profile_read(fz_ctx* c, double* ms, int* launches, long long* items, int n) {
   if (!c) return FZ_ERR_ARG;
   for (auto& p : c->pending) {
     float t = 0.f;
@@ -1666,8 +1686,10 @@ int fz_profile_read(fz_ctx* c, double* ms, int* launches, int n) {
   for (int i = 0; i < n && i < NKERN; ++i) {
     if (ms) ms[i] = c->prof_ms[i];
     if (launches) launches[i] = c->prof_n[i];
+    if (items) items[i] = c->prof_items[i];
     c->prof_ms[i] = 0;
     c->prof_n[i] = 0;
+    c->prof_items[i] = 0;
   }
   return NKERN;
 }
@@ -1782,38 +1804,50 @@ int fz_invert_device(fz_ctx* c, int npix, const double* d_obs, const float* d_in
   FZ_CK(cudaMemcpyAsync(d_w, w.data(), w.size() * sizeof(double), cudaMemcpyHostToDevice, s));
   FZ_CK(cudaMemsetAsync(c->d_q, 0, sizeof(LMQueue), s));
   if (d_status) FZ_CK(cudaMemsetAsync(d_status, 0, npix * sizeof(int), s));
-  const LMSlots L = c->lm;
+  LMSlots L = c->lm, L2 = c->lm2;   // L is the pool in use; it shrinks to the occupied slots in the tail
   {
-    ProfScope ps(c, 5, s);
+    ProfScope ps(c, 5, s, S);
     k_lm_fill<<<S, 128, 0, s>>>(C, L, c->d_q, d_obs, d_init);
   }
   FZ_CK(cudaGetLastError());
   const size_t usm = (size_t)(C.nz + 3 * C.np) * sizeof(double) + (size_t)C.nz * sizeof(float);
+  LMQueue hq{};
   // every pixel needs at most maxit iterations; slots are refilled at once
   const long long cap = (long long)C.maxit * ((npix + S - 1) / S + 1) + 8;
   for (long long it = 0; it < cap; ++it) {
-    if ((rc = launch_forward_rf(c, S, L.mcur, hydrostatic, L.syn, L.jac, L.mcur, L.status, s))) return rc;
+    const int n = L.S;
+    if ((rc = launch_forward_rf(c, n, L.mcur, hydrostatic, L.syn, L.jac, L.mcur, L.status, s))) return rc;
     {
-      ProfScope ps(c, 6, s);
-      k_lm_accept<<<S, 256, 0, s>>>(C, L, c->d_q, d_w, d_obs, d_init, d_target_chi2, d_model_out, d_chi2, d_iters,
+      ProfScope ps(c, 6, s, n);
+      k_lm_accept<<<n, 256, 0, s>>>(C, L, c->d_q, d_w, d_obs, d_init, d_target_chi2, d_model_out, d_chi2, d_iters,
                                     d_syn_out, d_status);
     }
     {
-      ProfScope ps(c, 7, s);
-      k_lm_normal<<<(S + 3) / 4, 128, 0, s>>>(C, L, d_w);
+      ProfScope ps(c, 7, s, n);
+      k_lm_normal<<<(n + 3) / 4, 128, 0, s>>>(C, L, d_w);
     }
     {
-      ProfScope ps(c, 8, s);
-      k_lm_solve<<<(S + 3) / 4, 128, 0, s>>>(C, L);
+      ProfScope ps(c, 8, s, n);
+      k_lm_solve<<<(n + 3) / 4, 128, 0, s>>>(C, L);
     }
     {
-      ProfScope ps(c, 9, s);
-      k_lm_update<<<S, 128, usm, s>>>(C, L, c->d_coef64);
+      ProfScope ps(c, 9, s, n);
+      k_lm_update<<<n, 128, usm, s>>>(C, L, c->d_coef64);
     }
+    k_lm_scan<<<1, 1024, 0, s>>>(n, L.pix, c->d_dest, c->d_q);
     FZ_CK(cudaGetLastError());
-    FZ_CK(cudaMemcpyAsync(c->h_done, &c->d_q->done, sizeof(int), cudaMemcpyDeviceToHost, s));
+    FZ_CK(cudaMemcpyAsync(&hq, c->d_q, sizeof(LMQueue), cudaMemcpyDeviceToHost, s));
     FZ_CK(cudaStreamSynchronize(s));
-    if (*c->h_done >= npix) return 0;
+    if (hq.done >= npix) return 0;
+    // the queue is drained: move the occupied slots to the front of the
+    // other pool once a quarter of the pool has emptied, and iterate on them only
+    if (hq.next >= npix && hq.active > 0 && hq.active <= (3 * n) / 4) {
+      k_lm_compact<<<n, 256, 0, s>>>(C, L, L2, c->d_dest);
+      FZ_CK(cudaGetLastError());
+      std::swap(L, L2);
+      L.S = hq.active;
+      L2.S = S;
+    }
   }
   return FZ_ERR_STATE;
 }

@@ -243,3 +243,28 @@ void fzh_pf_table(PFTable* t) {
       }
     }
 }
+
+int fzh_pfd_table(PFDTable* t) {
+  std::memset(t, 0, sizeof(*t));
+  for (int e = 0; e < FZ_NELEM; ++e)
+    for (int s = 0; s < 3; ++s) {
+      if (fz_tab_pf_nd[e][s] > 3) return -1;
+      t->nd[e][s] = fz_tab_pf_nd[e][s];
+      for (int i = 0; i < fz_tab_pf_nd[e][s]; ++i) {
+        const fz_pf_dpiece& v = fz_tab_pf_d[e][s][i];
+        if (v.nc > 6 || v.dx > 1 || v.up > 1 || v.ref > 2) return -1;
+        PFDPiece& p = t->d[e][s][i];
+        for (int k = 0; k < v.nc; ++k) p.c[k] = v.c[k];
+        p.th = v.th;
+        p.base = v.base;
+        p.mult = v.mult;
+        p.cond = v.cond;
+        p.var = v.var;
+        p.dx = v.dx;
+        p.ub = v.ub;
+        p.up = v.up;
+        p.ref = v.ref;
+      }
+    }
+  return 0;
+}

@@ -64,6 +64,8 @@ struct LMSlots {
 struct LMQueue {
   int next;          // next pixel to load
   int done;          // finished pixels
+  int active;        // occupied slots (k_lm_scan)
+  int pad;
 };
 
 // PARAM_NORMS (src/get_dmodel.f90:31), LOWLIM/UPPLIM (:1885-1901)
@@ -483,6 +485,53 @@ __global__ void __launch_bounds__(128) k_lm_update(LMConf C, LMSlots Sl, const d
     __syncthreads();
     j0 += nj;
   }
+}
+
+// One block of 1024 threads: destination of every occupied slot when the
+// pool is compacted (exclusive scan of the occupancy flags), and their count.
+__global__ void __launch_bounds__(1024) k_lm_scan(int S, const int* __restrict__ pix, int* __restrict__ dest,
+                                                  LMQueue* q) {
+  __shared__ int part[1024];
+  const int per = (S + blockDim.x - 1) / blockDim.x;
+  const int b = threadIdx.x * per, e = min(S, b + per);
+  int n = 0;
+  for (int i = b; i < e; ++i) n += pix[i] >= 0;
+  part[threadIdx.x] = n;
+  __syncthreads();
+  for (int o = 1; o < (int)blockDim.x; o <<= 1) {   // inclusive Hillis-Steele scan
+    const int v = threadIdx.x >= o ? part[threadIdx.x - o] : 0;
+    __syncthreads();
+    part[threadIdx.x] += v;
+    __syncthreads();
+  }
+  int d = part[threadIdx.x] - n;
+  for (int i = b; i < e; ++i) dest[i] = pix[i] >= 0 ? d++ : -1;
+  if (threadIdx.x == blockDim.x - 1) q->active = part[threadIdx.x];
+}
+
+// One CTA per source slot: copy an occupied slot to its compacted position
+// in the other pool (the state the next iteration reads).
+__global__ void __launch_bounds__(256) k_lm_compact(LMConf C, LMSlots A, LMSlots B, const int* __restrict__ dest) {
+  const int s = blockIdx.x, d = dest[s];
+  if (d < 0) return;
+  const int nf = C.nfreq, nm = 13 * C.nz;
+  if (threadIdx.x == 0) {
+    B.pix[d] = A.pix[s];
+    B.iter[d] = A.iter[s];
+    B.skip[d] = A.skip[s];
+  }
+  if (threadIdx.x < 5) B.st[5 * (size_t)d + threadIdx.x] = A.st[5 * (size_t)s + threadIdx.x];
+  for (int i = threadIdx.x; i < nm; i += blockDim.x) {
+    B.mcur[(size_t)d * nm + i] = A.mcur[(size_t)s * nm + i];
+    B.mbest[(size_t)d * nm + i] = A.mbest[(size_t)s * nm + i];
+  }
+  for (int i = threadIdx.x; i < nf; i += blockDim.x) {
+    B.synb[(size_t)d * nf + i] = A.synb[(size_t)s * nf + i];
+    B.obs[(size_t)d * nf + i] = A.obs[(size_t)s * nf + i];
+  }
+  const float4* ja = reinterpret_cast<const float4*>(A.jacb + (size_t)s * C.np * nf);
+  float4* jb = reinterpret_cast<float4*>(B.jacb + (size_t)d * C.np * nf);
+  for (int i = threadIdx.x; i < C.np * nf / 4; i += blockDim.x) jb[i] = ja[i];
 }
 
 }  // namespace

@@ -214,13 +214,14 @@ int fz_mlp_train_device(fz_mlp* mlp, int n, const float* d_x, const float* d_t, 
 
 /* Per-kernel timing: when enabled, every launch of the context is bracketed
  * by CUDA events on its stream; fz_profile_read returns the accumulated
- * milliseconds and launch counts of the kernels (names in order:
+ * milliseconds, launch counts and processed columns (or LM slots; items
+ * may be NULL) of the kernels (names in order:
  * "k_chain", "k_opac", "k_synth", "k_opac_rf", "k_synth_rf", "k_lm_fill",
  * "k_lm_accept", "k_lm_normal", "k_lm_solve", "k_lm_update", "k_chemder") and resets
  * them; returns the kernel count.  Replaces the reference's
  * SYSTEM_CLOCK "Forward 3D:" timer (src/forward.f90:99-100, :295-297). */
 int fz_profile_enable(fz_ctx* ctx, int on);
-int fz_profile_read(fz_ctx* ctx, double* ms, int* launches, int n);
+int fz_profile_read(fz_ctx* ctx, double* ms, int* launches, long long* items, int n);
 
 /* Peak FP32 FMA throughput of device `device` in TFLOP/s (2 FLOP per FMA),
  * measured by a register-resident FMA-chain kernel; the denominator of the
