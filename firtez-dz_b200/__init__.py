@@ -102,7 +102,7 @@ def lib():
         L.fz_rf_nodes.argtypes = [P, P]
         L.fz_forward_rf.argtypes = [P, ctypes.c_int, P, ctypes.c_int, P, P, P, P]
         L.fz_forward_rf_device.argtypes = [P, ctypes.c_int, P, ctypes.c_int, P, P, P, P, P]
-        L.fz_invert.argtypes = [P, ctypes.c_int, P, P, ctypes.c_int, P, P, P, P, P, P]
+        L.fz_invert.argtypes = [P, ctypes.c_int, P, P, P, ctypes.c_int, P, P, P, P, P, P]
         L.fz_invert_device.argtypes = [P, ctypes.c_int, P, P, P, ctypes.c_int, P, P, P, P, P, P, P]
         L.fz_lm_perturbation.argtypes = [P, ctypes.c_int, ctypes.c_int, ctypes.c_int, P, P, P, ctypes.c_double, P]
         _lib = L
@@ -259,23 +259,30 @@ class Synthesis:
         _check(lib().fz_forward_rf(self._h, ncol, _p(m), int(bool(hydrostatic)), _p(syn), _p(jac), _p(mo), _p(st)))
         return syn, jac, mo, st
 
-    def invert(self, obs, init, hydrostatic=True, opts=None, want_syn=False):
+    def invert(self, obs, init, hydrostatic=True, opts=None, want_syn=False, target=None):
         """Batched LM inversion of host-resident pixels with the node layout of
         rf_nodes().  obs: (npix, 4, numw) float64 GAIN-normalised Stokes;
-        init: (npix, 13, nz) float32 initial models.  Returns (best models,
-        chi2, iterations, status[, best synthesis])."""
+        init: (npix, 13, nz) float32 initial models; target: optional
+        per-pixel chi2 goal (npix,).  Returns (best models, chi2, iterations,
+        status[, best synthesis])."""
         o = np.ascontiguousarray(obs, dtype=np.float64)
         m = np.ascontiguousarray(init, dtype=np.float32)
         npix = o.shape[0]
         if o.shape[1:] != (4, self.numw) or m.shape != (npix, 13, self.nz):
             raise ValueError("obs must be (npix, 4, numw) and init (npix, 13, nz)")
+        tg = None
+        if target is not None:
+            tg = np.ascontiguousarray(target, dtype=np.float64)
+            if tg.shape != (npix,):
+                raise ValueError("target must be (npix,)")
         opts = opts or LMOpts()
         mo = np.empty_like(m)
         chi = np.zeros(npix)
         it = np.zeros(npix, dtype=np.int32)
         st = np.zeros(npix, dtype=np.int32)
         syn = np.zeros_like(o) if want_syn else None
-        _check(lib().fz_invert(self._h, npix, _p(o), _p(m), int(bool(hydrostatic)), ctypes.byref(opts), _p(mo),
+        _check(lib().fz_invert(self._h, npix, _p(o), _p(m), None if tg is None else _p(tg), int(bool(hydrostatic)),
+                               ctypes.byref(opts), _p(mo),
                                _p(chi), _p(it), None if syn is None else _p(syn), _p(st)))
         return (mo, chi, it, st, syn) if want_syn else (mo, chi, it, st)
 

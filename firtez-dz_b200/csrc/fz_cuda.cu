@@ -394,6 +394,7 @@ struct RFConf {
 // chemistry derivatives of GET_DNHYDDTEMP at the (T, Pg, NELEC) that
 // FORWARD1D passes to it (src/forward.f90:917-918).
 __global__ void __launch_bounds__(128) k_chemder(const DevParams* __restrict__ Pg, const Consts* __restrict__ Kg,
+                                                 const PFTable* __restrict__ tb, const PFDTable* __restrict__ td,
                                                  int ncol, const float* __restrict__ mout,
                                                  const double2* __restrict__ chem, double4* __restrict__ chemd) {
   __shared__ Consts K;
@@ -406,7 +407,7 @@ __global__ void __launch_bounds__(128) k_chemder(const DevParams* __restrict__ P
   for (size_t i = (size_t)blockIdx.x * wpb + (threadIdx.x >> 5); i < total; i += (size_t)gridDim.x * wpb) {
     const int col = (int)(i / nz), k = (int)(i % nz);
     const float* m = mout + (size_t)col * 13 * nz;
-    const ChemDer cd = chem_der_warp((double)mget(m, nz, 0, k), (double)mget(m, nz, 1, k), chem[i].y, K, lane);
+    const ChemDer cd = chem_der_warp((double)mget(m, nz, 0, k), (double)mget(m, nz, 1, k), chem[i].y, K, tb, td, lane);
     if (lane == 0) chemd[i] = make_double4(cd.dne_p, cd.dnh_p, cd.dne_t, cd.dnh_t);
   }
 }
@@ -1108,6 +1109,7 @@ struct fz_ctx {
   DevParams* d_params = nullptr;
   Consts* d_consts = nullptr;
   PFTable* d_pf = nullptr;
+  PFDTable* d_pfd = nullptr;
   LamP* d_lam = nullptr;
   float* d_gain = nullptr;
   // scratch (grown on demand): per (column, height) nH, ne and the opacity slab
@@ -1267,7 +1269,7 @@ int launch_forward_rf(fz_ctx* c, int ncol, const float* d_model, int hydrostatic
   {
     ProfScope ps(c, 10, s, ncol);
     const int blocks = (int)std::min<size_t>((cells + 3) / 4, (size_t)c->nsm * 32);
-    k_chemder<<<blocks, 128, 0, s>>>(c->d_params, c->d_consts, ncol, d_mout, c->d_chem, c->d_chemd);
+    k_chemder<<<blocks, 128, 0, s>>>(c->d_params, c->d_consts, c->d_pf, c->d_pfd, ncol, d_mout, c->d_chem, c->d_chemd);
   }
   FZ_CK(cudaGetLastError());
   {
@@ -1560,6 +1562,12 @@ int fz_create(fz_ctx** out, const fz_line* lines, int nlines, const fz_region* r
     fzh_pf_table(reinterpret_cast<PFTable*>(buf.data()));
     if ((rc = cuda_fail(cudaMemcpy(c->d_pf, buf.data(), sizeof(PFTable), cudaMemcpyHostToDevice)))) return fail(rc);
   }
+  if ((rc = cuda_fail(cudaMalloc(&c->d_pfd, sizeof(PFDTable))))) return fail(rc);
+  {
+    std::vector<char> buf(sizeof(PFDTable));
+    if (fzh_pfd_table(reinterpret_cast<PFDTable*>(buf.data())) != 0) return fail(FZ_ERR_STATE);
+    if ((rc = cuda_fail(cudaMemcpy(c->d_pfd, buf.data(), sizeof(PFDTable), cudaMemcpyHostToDevice)))) return fail(rc);
+  }
   if ((rc = cuda_fail(cudaMalloc(&c->d_lam, numw * sizeof(LamP))))) return fail(rc);
   if ((rc = cuda_fail(cudaMalloc(&c->d_gain, 4 * numw * sizeof(float))))) return fail(rc);
   if ((rc = cuda_fail(cudaMemcpy(c->d_params, &P, sizeof(P), cudaMemcpyHostToDevice)))) return fail(rc);
@@ -1640,6 +1648,7 @@ int fz_destroy(fz_ctx* c) {
   cudaFree(c->d_params);
   cudaFree(c->d_consts);
   cudaFree(c->d_pf);
+  cudaFree(c->d_pfd);
   cudaFree(c->d_lam);
   cudaFree(c->d_gain);
   cudaFree(c->d_slab);
@@ -1852,12 +1861,12 @@ int fz_invert_device(fz_ctx* c, int npix, const double* d_obs, const float* d_in
   return FZ_ERR_STATE;
 }
 
-int fz_invert(fz_ctx* c, int npix, const double* obs, const float* init, int hydrostatic, const fz_lm_opts* opts,
-              float* model_out, double* chi2, int* iters, double* syn_out, int* status) {
+int fz_invert(fz_ctx* c, int npix, const double* obs, const float* init, const double* target_chi2, int hydrostatic,
+              const fz_lm_opts* opts, float* model_out, double* chi2, int* iters, double* syn_out, int* status) {
   if (!c || npix <= 0 || !obs || !init || !model_out || !chi2 || !iters) return FZ_ERR_ARG;
   FZ_CK(cudaSetDevice(c->device));
   const size_t nf = 4 * (size_t)c->numw, nm = 13 * (size_t)c->nz;
-  double *d_obs = nullptr, *d_chi = nullptr, *d_syn = nullptr;
+  double *d_obs = nullptr, *d_chi = nullptr, *d_syn = nullptr, *d_tgt = nullptr;
   float *d_init = nullptr, *d_out = nullptr;
   int *d_it = nullptr, *d_st = nullptr;
   int rc = 0;
@@ -1872,8 +1881,12 @@ int fz_invert(fz_ctx* c, int npix, const double* obs, const float* init, int hyd
     if (syn_out && (rc = cuda_fail(cudaMalloc(&d_syn, npix * nf * sizeof(double))))) break;
     if ((rc = cuda_fail(cudaMemcpyAsync(d_obs, obs, npix * nf * sizeof(double), cudaMemcpyHostToDevice, s)))) break;
     if ((rc = cuda_fail(cudaMemcpyAsync(d_init, init, npix * nm * sizeof(float), cudaMemcpyHostToDevice, s)))) break;
-    if ((rc = fz_invert_device(c, npix, d_obs, d_init, nullptr, hydrostatic, opts, d_out, d_chi, d_it, d_syn, d_st,
-                               s)))
+    if (target_chi2) {
+      if ((rc = cuda_fail(cudaMalloc(&d_tgt, npix * sizeof(double))))) break;
+      if ((rc = cuda_fail(cudaMemcpyAsync(d_tgt, target_chi2, npix * sizeof(double), cudaMemcpyHostToDevice, s))))
+        break;
+    }
+    if ((rc = fz_invert_device(c, npix, d_obs, d_init, d_tgt, hydrostatic, opts, d_out, d_chi, d_it, d_syn, d_st, s)))
       break;
     if ((rc = cuda_fail(cudaMemcpyAsync(model_out, d_out, npix * nm * sizeof(float), cudaMemcpyDeviceToHost, s)))) break;
     if ((rc = cuda_fail(cudaMemcpyAsync(chi2, d_chi, npix * sizeof(double), cudaMemcpyDeviceToHost, s)))) break;
@@ -1892,6 +1905,7 @@ int fz_invert(fz_ctx* c, int npix, const double* obs, const float* init, int hyd
   cudaFree(d_it);
   cudaFree(d_st);
   cudaFree(d_syn);
+  cudaFree(d_tgt);
   return rc;
 }
 

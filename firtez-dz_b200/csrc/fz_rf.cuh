@@ -67,47 +67,139 @@ struct ChemDer {
   double dne_t, dnh_t;   // DNELECDTEMP_PG, DNHYDDTEMP_PG
 };
 
+__device__ __forceinline__ double sel3(const double v[3], int i) { return i == 0 ? v[0] : (i == 1 ? v[1] : v[2]); }
+
+// U and dlnU/dT of one (element, stage) from the padded device tables, with
+// lanes on different elements: every value piece is evaluated once (the
+// derivative pieces' conditions and factors refer to them), the active value
+// and derivative pieces are selected by predication, and only the active
+// derivative piece is evaluated.  Same pieces, same Horner order and the same
+// rounded -1/T as partition_udu, so the results agree bit for bit.
+__device__ __forceinline__ void pf_stage_udu(const PFTable* __restrict__ tb, const PFDTable* __restrict__ td, int e,
+                                             int s, double T, double it, const double var[3], double& U,
+                                             double& dU) {
+  const int nv = __ldg(&tb->nv[e][s]);
+  double vals[FZ_PF_MAXV];
+  int act = 0;
+#pragma unroll
+  for (int i = 0; i < FZ_PF_MAXV; ++i) {
+    const PFPiece* p = &tb->p[e][s][i];
+    double u = 0.0;
+    if (i < nv) {
+      double c[6];
+#pragma unroll
+      for (int k = 0; k < 6; ++k) c[k] = __ldg(&p->c[k]);
+      const int form = __ldg(&p->form), v = __ldg(&p->var);
+      const double h = horner6(c, v == 0 ? var[0] : (v == 1 ? var[1] : var[2]));
+      u = h;
+      if (form == 1) u = __ldg(&p->base) + exp(h);
+      if (form == 2) u = fmax(__ldg(&p->clamp), h);
+      if (i > 0) {
+        const int cond = __ldg(&p->cond);
+        const double th = __ldg(&p->th);
+        const bool ok = (cond == 1 && T > th) || (cond == 2 && T < th) || (cond == 3 && T <= th) ||
+                        (cond == 4 && T >= th);
+        act = ok ? i : act;
+      }
+    }
+    vals[i] = u;
+  }
+  U = nv > 0 ? sel3(vals, act) : 0.0;
+  const int nd = __ldg(&td->nd[e][s]);
+  int dact = -1;
+  double uref = U;
+#pragma unroll
+  for (int i = 0; i < 3; ++i) {
+    const PFDPiece* p = &td->d[e][s][i];
+    const int cond = __ldg(&p->cond), ref = __ldg(&p->ref);
+    const double th = __ldg(&p->th);
+    const double ur = ref < 0 ? U : sel3(vals, ref);
+    const bool ok = i < nd && (cond == 0 || (cond == 1 && T > th) || (cond == 2 && T < th) ||
+                               (cond == 3 && T <= th) || (cond == 4 && T >= th) || (cond == 5 && ur != th));
+    dact = ok ? i : dact;
+    uref = ok ? ur : uref;
+  }
+  double d = 0.0;
+  if (dact >= 0) {
+    const PFDPiece* p = &td->d[e][s][dact];
+    double c[6];
+#pragma unroll
+    for (int k = 0; k < 6; ++k) c[k] = __ldg(&p->c[k]);
+    const int v = __ldg(&p->var);
+    double h = horner6(c, v == 0 ? var[0] : (v == 1 ? var[1] : var[2])) * __ldg(&p->mult);
+    if (__ldg(&p->dx)) h *= -it;
+    if (__ldg(&p->ub)) h *= (uref - __ldg(&p->base));
+    if (__ldg(&p->up)) h /= uref;
+    d = h;
+  }
+  dU = d;
+}
+
 // GET_NE_TEMP_SNE_ALT (:892-957) and GET_DNE_PG (:2062-2155) by one warp,
 // lanes over the elements.  In GET_DNE_PG every element's term of the sum is
 // affine in the trial derivative DNE (ION_CALC_TEMPPGAS, :1791-1872), so the
 // sum is A + B*DNE with A, B reduced once; the reference's damped fixed
 // point (tolerance 1e-6, <= 101 passes) then runs on these two scalars with
-// its own update and stopping rules.
-__device__ __forceinline__ ChemDer chem_der_warp(double T, double P, double NE, const Consts& K, int lane) {
-  const double nh = (P - NE * KBOL * T) / (KBOL * T * K.deno_sa);
+// its own update and stopping rules.  The per-element algebra of
+// ION_CALC_NETEMP_NEW (:1376-1442) and ION_CALC_TEMPPGAS is written on the
+// reciprocals 1/(NE a_I), 1/(NE a_II), 1/x_1..3 and 1/DENOI (eight divisions
+// instead of some forty); the T-only factors are taken once per warp.
+__device__ __forceinline__ ChemDer chem_der_warp(double T, double P, double NE, const Consts& K,
+                                                 const PFTable* __restrict__ tb, const PFDTable* __restrict__ td,
+                                                 int lane) {
+  const double it = 1.0 / T;
+  const double ideno = 1.0 / K.deno_sa;
+  const double nh = (P - NE * KBOL * T) * (it / KBOL) * ideno;
+  const double var[3] = {T, 1.0e-3 * T, log(5040.0 / T)};
+  const double lamelec = K.csaha1 * pow(T, -3.0 / 2.0);
+  const double dlam = -1.5 * it;
+  const double it2 = it * it;
+  const double ine = 1.0 / NE;
+  const double ne2 = NE * NE, ine2 = ine * ine;
+  const double pk = P * it2 / KBOL;
   double sn = 0.0, sd = 0.0, sa = 0.0, sb = 0.0;
 #pragma unroll 1
   for (int j = 0; j < 3; ++j) {
     const int e = K.lane_elem[32 * j + lane];
     if (e < 0) continue;
-    const Alpha al = alpha_of(e, T, K);
-    const double a1 = al.a1, a2 = al.a2, da1 = al.da1, da2 = al.da2;
+    double U[3], dU[3];
+#pragma unroll
+    for (int s = 0; s < 3; ++s) pf_stage_udu(tb, td, e, s, T, it, var, U[s], dU[s]);
+    const double xi = __ldg(&fz_tab_xi[e]), xii = __ldg(&fz_tab_xii[e]);
+    const double e1 = exp(clamp650(K.csaha2 * xi * it));
+    const double e2 = exp(clamp650(K.csaha2 * xii * it));
+    const double a1 = (U[0] / (2.0 * U[1])) * lamelec * e1;
+    const double a2 = (U[1] / (2.0 * U[2])) * lamelec * e2;
+    const double da1 = a1 * (dU[0] - dU[1] + dlam - K.csaha2 * xi * it2);
+    const double da2 = a2 * (dU[1] - dU[2] + dlam - K.csaha2 * xii * it2);
     const double ab = K.ab10[e];
     const double n = nh * ab;
-    const double x1 = 1.0 + (1.0 / (NE * a1)) * (1.0 + (1.0 / (NE * a2)));
-    const double x2 = NE * a1 + 1.0 + (1.0 / (NE * a2));
-    const double x3 = 1.0 + NE * a2 * (NE * a1 + 1.0);
-    const double ni = n / x1, nii = n / x2, niii = n / x3;
-    const double denoi = ((a1 * NE + 1.0) * a2) * NE + 1.0;
+    const double p1 = NE * a1, p2 = NE * a2;
+    const double ip1 = 1.0 / p1, ip2 = 1.0 / p2;
+    const double ia1 = NE * ip1, ia2 = NE * ip2;
+    const double f1 = 1.0 / (1.0 + ip1 * (1.0 + ip2));   // ni / n
+    const double f2 = 1.0 / (p1 + 1.0 + ip2);            // nii / n
+    const double f3 = 1.0 / (1.0 + p2 * (p1 + 1.0));     // niii / n
+    const double ni = n * f1, nii = n * f2, niii = n * f3;
+    const double idn = 1.0 / ((p1 + 1.0) * p2 + 1.0);
     const double g = 2.0 * a1 * a2 * NE + a2;
-    const double r = ab / K.deno_sa;
-    // ION_CALC_NETEMP_NEW (:1376-1442)
-    const double dn_i = ni / n * r / KBOL / T, dn_ii = nii / n * r / KBOL / T, dn_iii = niii / n * r / KBOL / T;
-    const double dd_i = -(ni / n * r) + n * (2.0 * a1 * a2 * NE) / denoi - ni * g / denoi;
-    const double dd_ii = -(nii / n * r) + n * a2 / denoi - nii * g / denoi;
-    const double dd_iii = -(niii / n * r) - niii * g / denoi;
+    const double r = ab * ideno;
+    const double rk = r * it / KBOL;
+    // ION_CALC_NETEMP_NEW
+    const double dn_i = f1 * rk, dn_ii = f2 * rk, dn_iii = f3 * rk;
+    const double dd_i = -(f1 * r) + (n * (2.0 * a1 * a2 * NE) - ni * g) * idn;
+    const double dd_ii = -(f2 * r) + (n * a2 - nii * g) * idn;
+    const double dd_iii = -(f3 * r) - niii * g * idn;
     // ION_CALC_TEMPPGAS at DNE = 0 (A) and its DNE-coefficient (B)
-    const double dn0 = -(r * (P / (KBOL * T * T)));
-    const double ne2 = NE * NE;
-    const double i1 = 1.0 / (x1 * x1), i2 = 1.0 / (x2 * x2), i3 = 1.0 / (x3 * x3);
-    const double dni0 = dn0 * ni / n - n * i1 * (1.0 / (ne2 * a1)) *
-                                           ((-1.0 / a1) * (NE * da1) * (1.0 + 1.0 / (NE * a2)) -
-                                            (1.0 / (NE * a2 * a2)) * (NE * da2));
-    const double dni1 = -r * ni / n - n * i1 * (1.0 / (ne2 * a1)) * (-(1.0 + 1.0 / (NE * a2)) - 1.0 / (NE * a2));
-    const double dnii0 = dn0 * nii / n - n * i2 * (NE * da1 - (NE * da2) / (ne2 * a2 * a2));
-    const double dnii1 = -r * nii / n - n * i2 * (a1 - 1.0 / (ne2 * a2));
-    const double dniii0 = dn0 * niii / n - n * i3 * (ne2 * da2 * a1 + ne2 * a2 * da1 + NE * da2);
-    const double dniii1 = -r * niii / n - n * i3 * (2.0 * NE * a1 * a2 + a2);
+    const double dn0 = -(r * pk);
+    const double i1 = f1 * f1, i2 = f2 * f2, i3 = f3 * f3;
+    const double q1 = n * i1 * (ine2 * ia1);
+    const double dni0 = dn0 * f1 - q1 * ((-ia1) * (NE * da1) * (1.0 + ip2) - (ip2 * ia2) * (NE * da2));
+    const double dni1 = -r * f1 - q1 * (-(1.0 + ip2) - ip2);
+    const double dnii0 = dn0 * f2 - n * i2 * (NE * da1 - (NE * da2) * (ine2 * ia2 * ia2));
+    const double dnii1 = -r * f2 - n * i2 * (a1 - ine2 * ia2);
+    const double dniii0 = dn0 * f3 - n * i3 * (ne2 * da2 * a1 + ne2 * a2 * da1 + NE * da2);
+    const double dniii1 = -r * f3 - n * i3 * (2.0 * NE * a1 * a2 + a2);
     if (e == 0) {   // hydrogen: N_H+ - N_H- (:1841-1846)
       sn += -dn_i + dn_iii;
       sd += -dd_i + dd_iii;
@@ -126,7 +218,7 @@ __device__ __forceinline__ ChemDer chem_der_warp(double T, double P, double NE, 
   sb = warp_sum(sb);
   ChemDer c;
   c.dne_p = sn / (1.0 - sd);
-  c.dnh_p = 1.0 / K.deno_sa * (1.0 / KBOL / T - c.dne_p);
+  c.dnh_p = ideno * (it / KBOL - c.dne_p);
   double dold = 0.0, dnew = 0.0, derr = 1.0e20;
   int iter = 0;
   while (derr > 1e-6 && iter <= 100) {
@@ -137,7 +229,7 @@ __device__ __forceinline__ ChemDer chem_der_warp(double T, double P, double NE, 
     iter = iter + 1;
   }
   c.dne_t = sa + sb * dnew;
-  c.dnh_t = (-1.0 / K.deno_sa) * (P / (KBOL * T * T) + c.dne_t);
+  c.dnh_t = (-ideno) * (pk + c.dne_t);
   return c;
 }
 

@@ -232,8 +232,15 @@ class WarmStart:
         return m
 
     def initial_models(self, obs, base=None):
-        """Warm-start models for observations obs (npix, 4, numw)."""
-        nodes_v = self.predict_nodes(obs)
+        """Warm-start models for host observations obs (npix, 4, numw): the
+        network and the node expansion run on the device; returns host
+        models (npix, 13, nz) float32 (base: host models whose other rows
+        are kept, default_models() if None)."""
+        import torch
+        n = obs.shape[0]
+        x = torch.from_numpy(np.ascontiguousarray(obs, dtype=np.float32).reshape(n, -1)).cuda()
         if base is None:
-            base = default_models(obs.shape[0], self.nz)
-        return self.expand(nodes_v, base)
+            b = torch.from_numpy(default_models(1, self.nz)).cuda().expand(n, -1, -1)
+        else:
+            b = torch.from_numpy(np.ascontiguousarray(base, dtype=np.float32)).cuda()
+        return self.initial_models_device(x, b).cpu().numpy()

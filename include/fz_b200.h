@@ -172,12 +172,12 @@ typedef struct {
  * initial model MODEL(NZ,13,npix).  Outputs: the best model, its chi2
  * (NEW_CALCULATE_CHI2 normalisation), the iterations used, optionally the
  * best synthesis (syn_out, may be NULL) and a status per pixel. */
-int fz_invert(fz_ctx* ctx, int npix, const double* obs, const float* init, int hydrostatic,
-              const fz_lm_opts* opts, float* model_out, double* chi2, int* iters, double* syn_out,
-              int* status);
-/* Device-pointer variant; d_target_chi2 (npix, may be NULL) adds a per-pixel
- * goal: a pixel also stops once its best chi2 is at or below its goal (e.g.
- * the chi2 another start reached on the same pixel). */
+int fz_invert(fz_ctx* ctx, int npix, const double* obs, const float* init, const double* target_chi2,
+              int hydrostatic, const fz_lm_opts* opts, float* model_out, double* chi2, int* iters,
+              double* syn_out, int* status);
+/* Device-pointer variant.  In both, target_chi2 (npix, may be NULL) adds a
+ * per-pixel goal: a pixel also stops once its best chi2 is at or below its
+ * goal (e.g. the chi2 another start reached on the same pixel). */
 int fz_invert_device(fz_ctx* ctx, int npix, const double* d_obs, const float* d_init,
                      const double* d_target_chi2, int hydrostatic, const fz_lm_opts* opts,
                      float* d_model_out, double* d_chi2, int* d_iters, double* d_syn_out, int* d_status,
