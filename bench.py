@@ -226,6 +226,8 @@ def main():
     gen = torch.Generator(device="cuda")
     gen.manual_seed(4242 + rank)
     chunk = 65536
+    warm = ws.WarmStart(a.nz, NODES, numw, seed=5 + rank)
+    true_models = torch.empty((npix, 13, a.nz), dtype=torch.float32, device="cuda")
     for i in range(0, npix, chunk):
         n = min(chunk, npix - i)
         m = torch.from_numpy(fz.atmos.make_columns(n, a.nz, seed=777000 + 1000 * rank + i // chunk)).cuda()
@@ -234,10 +236,10 @@ def main():
         ctx.forward_device(m.data_ptr(), n, syn.data_ptr(), mo.data_ptr(), 0, stream=stream, hydrostatic=True)
         obs[i:i + n] = syn.reshape(n, nf) + 1e-3 * torch.randn((n, nf), dtype=torch.float64, device="cuda",
                                                                generator=gen)
+        true_models[i:i + n] = mo
     obs32 = obs.float()
     base = torch.from_numpy(ws.default_models(a.tile, a.nz)).cuda()
     # --------------------------------------------------------------- network
-    warm = ws.WarmStart(a.nz, NODES, numw, seed=5 + rank)
     t0 = time.perf_counter()
     x, t = warm.make_training_set(ctx, a.train_pairs, seed=31 + rank, noise=1e-3)
     t1 = time.perf_counter()
@@ -257,13 +259,17 @@ def main():
             "st": torch.empty(a.tile, dtype=torch.int32, device="cuda")}
     results = {"nn": {}, "plain": {}, "free": {}}
     targets = {}
+    # one output model buffer per (arm, tile), allocated before any timing:
+    # the inverted models are compared with the true atmospheres afterwards
+    outs = {(arm, k): torch.empty((a.tile, 13, a.nz), dtype=torch.float32, device="cuda")
+            for arm in results for k in range(ntiles)}
 
     def step(i, arm):
         k = i % ntiles
         o = obs[k * a.tile:(k + 1) * a.tile]
         init = base if arm == "plain" else warm.initial_models_device(obs32[k * a.tile:(k + 1) * a.tile], base)
         tgt = targets[k].data_ptr() if arm == "nn" else 0
-        ctx.invert_device(a.tile, o.data_ptr(), init.data_ptr(), bufs["out"].data_ptr(), bufs["chi"].data_ptr(),
+        ctx.invert_device(a.tile, o.data_ptr(), init.data_ptr(), outs[(arm, k)].data_ptr(), bufs["chi"].data_ptr(),
                           bufs["it"].data_ptr(), bufs["st"].data_ptr(), hydrostatic=True, opts=opts, stream=stream,
                           target_ptr=tgt)
         if arm == "plain":
@@ -332,6 +338,34 @@ def main():
     chi_nn, chi_pl, chi_fr = cat("nn", 0), cat("plain", 0), cat("free", 0)
     it_nn, it_pl, it_fr = cat("nn", 1), cat("plain", 1), cat("free", 1)
     status_bad = max(results[arm][k][2] for arm in results for k in results[arm])
+
+    # ------------------------------------------------------ parameter errors
+    # errors of the inverted atmospheres against the true ones at the heights
+    # where the lines form (log tau5 of the true atmosphere in [-3, 0]);
+    # B_perp = |(Bx, By)| (the 180-degree azimuth ambiguity leaves Q, U
+    # unchanged under (Bx, By) -> -(Bx, By))
+    def height_errors(est, tru):
+        tau = tru[:, 11]
+        msk = (tau >= -3.0) & (tau <= 0.0)
+        e = {}
+        for name, d in (("T_K", est[:, 0] - tru[:, 0]), ("Bz_G", est[:, 7] - tru[:, 7]),
+                        ("vz_km_s", (est[:, 10] - tru[:, 10]) * 1e-5),
+                        ("Bperp_G", torch.hypot(est[:, 5], est[:, 6]) - torch.hypot(tru[:, 5], tru[:, 6]))):
+            v = d[msk].double()
+            e[name] = {"rms": float(torch.sqrt(torch.mean(v * v))), "median_abs": float(torch.median(v.abs()))}
+        return e
+
+    def tiles(src):
+        return torch.cat([src(k) for k in common])
+
+    tru_c = tiles(lambda k: true_models[k * a.tile:(k + 1) * a.tile])
+    errors = {arm: height_errors(tiles(lambda k: outs[(arm, k)]), tru_c) for arm in ("plain", "nn", "free")}
+    errors["nn_prior"] = height_errors(
+        tiles(lambda k: warm.initial_models_device(obs32[k * a.tile:(k + 1) * a.tile], base)), tru_c)
+    errors["default_guess"] = height_errors(base[:1].expand(tru_c.shape[0], -1, -1), tru_c)
+    errors["heights_compared_per_pixel"] = float(((tru_c[:, 11] >= -3.0) & (tru_c[:, 11] <= 0.0)).sum()
+                                                 / tru_c.shape[0])
+    del outs
 
     # ------------------------------------------------------------- end to end
     h_obs = obs[:a.tile].reshape(a.tile, 4, numw).cpu().numpy()
@@ -435,6 +469,9 @@ def main():
                             "median_chi2": float(np.median(chi_fr)), "mean_iterations": float(it_fr.mean()),
                             "speedup_vs_plain": free_value / plain_value,
                             "frac_pixels_chi2_above_1.1x_plain": float(np.mean(chi_fr > 1.1 * chi_pl))},
+           "parameter_errors": dict(errors, definition="errors of T, Bz, v_z and |B_perp| of the inverted "
+                                           "atmospheres against the true ones at the heights where the true "
+                                           "log tau5 is in [-3, 0], over the compared pixels"),
            "synthesis": synthesis,
            "roofline": {"bound": "hbm", "kernel": kname, "achieved": achieved, "peak": hbm, "unit": "GB/s",
                         "frac": achieved / hbm, "traffic": traffic,

@@ -34,7 +34,7 @@ TEM, PG, RHO, PEL, MW, BX, BY, BZ, VX, VY, VZ, TAU5, ZZ = range(13)
 
 FZ_OK, FZ_CHEM_NOCONV, FZ_NAN = 0, 1, 2
 KERNELS = ("k_chain", "k_opac", "k_synth", "k_opac_rf", "k_synth_rf", "k_lm_fill", "k_lm_accept", "k_lm_normal",
-           "k_lm_solve", "k_lm_update", "k_chemder")
+           "k_lm_solve", "k_lm_update", "k_chemder", "k_rf_prop")
 
 # free-parameter indices of the reference (atm_param.f90 order, 1-based) that
 # carry response functions
@@ -66,6 +66,16 @@ class LMOpts(ctypes.Structure):
 
     def __init__(self, maxsteps=5, maxit=40, dchi2=0.0, svdtol=1e-4, isigma=4e-3, wstk=(1, 1, 1, 1), slots=0):
         super().__init__(maxsteps, maxit, dchi2, svdtol, isigma, (ctypes.c_float * 4)(*wstk), slots, 0)
+
+
+class Tune(ctypes.Structure):
+    """fz_tune: launch shapes chosen by the autotuner (and their timings)."""
+    _fields_ = [("chain_warps", ctypes.c_int), ("chemder_blocks_per_sm", ctypes.c_int),
+                ("opac_rf_threads", ctypes.c_int), ("lm_slots", ctypes.c_int), ("chain_ms", ctypes.c_float),
+                ("chemder_ms", ctypes.c_float), ("opac_rf_ms", ctypes.c_float), ("lm_pixels_per_s", ctypes.c_float)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
 
 
 _lib = None
@@ -102,6 +112,12 @@ def lib():
         L.fz_rf_nodes.argtypes = [P, P]
         L.fz_forward_rf.argtypes = [P, ctypes.c_int, P, ctypes.c_int, P, P, P, P]
         L.fz_forward_rf_device.argtypes = [P, ctypes.c_int, P, ctypes.c_int, P, P, P, P, P]
+        L.fz_forward_rf_full.argtypes = [P, ctypes.c_int, P, ctypes.c_int, P, P, P, P]
+        L.fz_autotune_forward.argtypes = [P, ctypes.c_int, P, ctypes.c_int, P]
+        L.fz_autotune_lm.argtypes = [P, ctypes.c_int, P, P, P, ctypes.c_int, P, P, ctypes.c_int, P]
+        L.fz_tune_get.argtypes = [P, P]
+        L.fz_tune_set.argtypes = [P, P]
+        L.fz_forward_rf_full_device.argtypes = [P, ctypes.c_int, P, ctypes.c_int, P, P, P, P, P]
         L.fz_invert.argtypes = [P, ctypes.c_int, P, P, P, ctypes.c_int, P, P, P, P, P, P]
         L.fz_invert_device.argtypes = [P, ctypes.c_int, P, P, P, ctypes.c_int, P, P, P, P, P, P, P]
         L.fz_lm_perturbation.argtypes = [P, ctypes.c_int, ctypes.c_int, ctypes.c_int, P, P, P, ctypes.c_double, P]
@@ -258,6 +274,69 @@ class Synthesis:
         st = np.zeros(ncol, dtype=np.int32)
         _check(lib().fz_forward_rf(self._h, ncol, _p(m), int(bool(hydrostatic)), _p(syn), _p(jac), _p(mo), _p(st)))
         return syn, jac, mo, st
+
+    def forward_rf_full(self, model, hydrostatic=False):
+        """Synthesis plus the response functions at every height of
+        host-resident columns.
+
+        Returns (syn (ncol, 4, numw) float64, rf (ncol, 6, nz, 4*numw) float32
+        -- parameters T, Pg, Bx, By, Bz, v_z; the EQVDSYN layout with one node
+        per height --, model_out, status)."""
+        m = np.ascontiguousarray(model, dtype=np.float32)
+        if m.ndim == 2:
+            m = m[None]
+        ncol, npar, nz = m.shape
+        if npar != 13 or nz != self.nz:
+            raise ValueError("model must be (ncol, 13, %d)" % self.nz)
+        syn = np.zeros((ncol, 4, self.numw))
+        rf = np.zeros((ncol, 6, self.nz, 4 * self.numw), dtype=np.float32)
+        mo = np.empty_like(m)
+        st = np.zeros(ncol, dtype=np.int32)
+        _check(lib().fz_forward_rf_full(self._h, ncol, _p(m), int(bool(hydrostatic)), _p(syn), _p(rf), _p(mo),
+                                        _p(st)))
+        return syn, rf, mo, st
+
+    def forward_rf_full_device(self, model_ptr, ncol, syn_ptr, rf_ptr, model_out_ptr, status_ptr=0, stream=0,
+                               hydrostatic=False):
+        """Enqueue synthesis + response functions at every height on device
+        pointers (rf: ncol * 6 * nz * 4 * numw float32)."""
+        _check(lib().fz_forward_rf_full_device(self._h, int(ncol), ctypes.c_void_p(model_ptr),
+                                               int(bool(hydrostatic)), ctypes.c_void_p(syn_ptr),
+                                               ctypes.c_void_p(rf_ptr), ctypes.c_void_p(model_out_ptr),
+                                               ctypes.c_void_p(status_ptr) if status_ptr else None,
+                                               ctypes.c_void_p(stream) if stream else None))
+
+    def autotune_forward(self, model_ptr, ncol, hydrostatic=True):
+        """Time the launch-shape candidates of the RF path's chemistry and
+        opacity kernels on ncol device columns and keep the fastest; returns
+        the chosen shapes (dict)."""
+        t = Tune()
+        _check(lib().fz_autotune_forward(self._h, int(ncol), ctypes.c_void_p(model_ptr), int(bool(hydrostatic)),
+                                         ctypes.byref(t)))
+        return t.as_dict()
+
+    def autotune_lm(self, npix, obs_ptr, init_ptr, candidates=(2048, 4096, 8192, 16384), hydrostatic=True,
+                    opts=None, target_ptr=0):
+        """Invert the same npix device pixels once per candidate slot count
+        and keep the fastest as the default; returns the chosen shapes."""
+        t = Tune()
+        c = np.ascontiguousarray(candidates, dtype=np.int32)
+        opts = opts or LMOpts()
+        _check(lib().fz_autotune_lm(self._h, int(npix), ctypes.c_void_p(obs_ptr), ctypes.c_void_p(init_ptr),
+                                    ctypes.c_void_p(target_ptr) if target_ptr else None, int(bool(hydrostatic)),
+                                    ctypes.byref(opts), _p(c), int(c.size), ctypes.byref(t)))
+        return t.as_dict()
+
+    def tune(self, **shapes):
+        """Current launch shapes; keyword arguments set them first."""
+        t = Tune()
+        _check(lib().fz_tune_get(self._h, ctypes.byref(t)))
+        if shapes:
+            for k, v in shapes.items():
+                setattr(t, k, int(v))
+            _check(lib().fz_tune_set(self._h, ctypes.byref(t)))
+        d = t.as_dict()
+        return {k: d[k] for k in ("chain_warps", "chemder_blocks_per_sm", "opac_rf_threads", "lm_slots")}
 
     def invert(self, obs, init, hydrostatic=True, opts=None, want_syn=False, target=None):
         """Batched LM inversion of host-resident pixels with the node layout of

@@ -571,20 +571,27 @@ __device__ __forceinline__ void lmap(const Geo& g, const float h[3], const float
 // response and reset the accumulators (their operator is taken as 0).
 // Shared memory: the slab, the coefficient table (nz x np) and the node
 // accumulators (np x 4 x blockDim).
-template <bool HE>
+//
+// FULL: the response functions at every height instead of the node
+// Jacobian (NJ = NZ for every parameter): the local RFs of each layer go to
+// jac in the (NFREQ, 6 NZ) layout and the layer's operator to oscr
+// ((nz, 16, NUMW) per column, zero where the boundary condition is taken);
+// k_rf_prop then applies the products of the operators above each layer.
+template <bool HE, bool FULL>
 __global__ void __launch_bounds__(256, 2) k_synth_rf(const DevParams* __restrict__ Pg, const RFConf* __restrict__ Rg,
                                                   const LamP* __restrict__ lam, const float* __restrict__ gain,
                                                   int ncol, const float* __restrict__ slab,
                                                   const float* __restrict__ coefg, double* __restrict__ syn,
-                                                  float* __restrict__ jac, float* mout, int* __restrict__ status) {
+                                                  float* __restrict__ jac, float* __restrict__ oscr, float* mout,
+                                                  int* __restrict__ status) {
   extern __shared__ float4 sm_rf4[];
   __shared__ DevParams P;
   __shared__ RFConf C;
   __shared__ unsigned inf_mask[2];
   copy_to_shared(&P, Pg);
-  copy_to_shared(&C, Rg);
+  if (!FULL) copy_to_shared(&C, Rg);
   const int col = blockIdx.x;
-  const int nz = Pg->nz, nreg = Pg->nreg, nlu = Pg->nlu, np = Rg->np;
+  const int nz = Pg->nz, nreg = Pg->nreg, nlu = Pg->nlu, np = FULL ? 0 : Rg->np;
   const int sw = rf_w(nreg, nlu);
   const int nthr = blockDim.x;
   float* sm = reinterpret_cast<float*>(sm_rf4);
@@ -594,10 +601,15 @@ __global__ void __launch_bounds__(256, 2) k_synth_rf(const DevParams* __restrict
     const float4* src = reinterpret_cast<const float4*>(slab + (size_t)col * nz * sw);
     const int n4 = nz * sw / 4;
     for (int i = threadIdx.x; i < n4; i += nthr) sm_rf4[i] = __ldg(src + i);
-    for (int i = threadIdx.x; i < nz * np; i += nthr) coef[i] = __ldg(coefg + i);
-    for (int i = threadIdx.x; i < np * 4 * nthr; i += nthr) Dacc[i] = 0.0f;
+    if (!FULL) {
+      for (int i = threadIdx.x; i < nz * np; i += nthr) coef[i] = __ldg(coefg + i);
+      for (int i = threadIdx.x; i < np * 4 * nthr; i += nthr) Dacc[i] = 0.0f;
+    }
     if (threadIdx.x < 2) inf_mask[threadIdx.x] = 0u;
   }
+  const size_t fstride = (size_t)4 * Pg->numw;   // NFREQ
+  float* jcol = jac + (size_t)col * (FULL ? NSLOT * nz : 0) * fstride;
+  float* ocol = FULL ? oscr + (size_t)col * nz * 16 * Pg->numw : nullptr;
   __syncthreads();
   const int l = threadIdx.x;
   const bool active = l < P.numw;
@@ -631,9 +643,19 @@ __global__ void __launch_bounds__(256, 2) k_synth_rf(const DevParams* __restrict
     if (k == 0 || row[1] != 0.0f) {   // SET_BOUNDARY
       I0 = S;
       I1 = I2 = I3 = 0.f;
-      for (int j = 0; j < np; ++j)
+      if (FULL) {
+        const int nw = P.numw;
 #pragma unroll
-        for (int c = 0; c < 4; ++c) Dacc[(j * 4 + c) * nthr + l] = 0.0f;
+        for (int p = 0; p < NSLOT; ++p)
+#pragma unroll
+          for (int c = 0; c < 4; ++c) jcol[((size_t)p * nz + k) * fstride + c * nw + l] = 0.0f;
+#pragma unroll
+        for (int i = 0; i < 16; ++i) ocol[((size_t)k * 16 + i) * nw + l] = 0.0f;
+      } else {
+        for (int j = 0; j < np; ++j)
+#pragma unroll
+          for (int c = 0; c < 4; ++c) Dacc[(j * 4 + c) * nthr + l] = 0.0f;
+      }
       continue;
     }
     const Geo g{row[goff], row[goff + 1], row[goff + 2], row[goff + 3], row[goff + 4]};
@@ -795,6 +817,20 @@ __global__ void __launch_bounds__(256, 2) k_synth_rf(const DevParams* __restrict
         H[i] = prop ? fmaf(rf[1][i], pgk, OH[i]) : H[i];
       }
     }
+    if (FULL) {
+      const int nw = P.numw;
+#pragma unroll
+      for (int p = 0; p < NSLOT; ++p)
+#pragma unroll
+        for (int c = 0; c < 4; ++c) jcol[((size_t)p * nz + k) * fstride + c * nw + l] = rf[p][c];
+#pragma unroll
+      for (int i = 0; i < 16; ++i) ocol[((size_t)k * 16 + i) * nw + l] = O[i];
+      I0 = n0;
+      I1 = n1;
+      I2 = n2;
+      I3 = n3;
+      continue;
+    }
     // node accumulation
     const float* ck = coef + k * np;
 #pragma unroll
@@ -825,6 +861,12 @@ __global__ void __launch_bounds__(256, 2) k_synth_rf(const DevParams* __restrict
     o[2 * nw + l] = (double)I2 * (double)gain[4 * l + 2];
     o[3 * nw + l] = (double)I3 * (double)gain[4 * l + 3];
     if (!(isfinite(I0) && isfinite(I1) && isfinite(I2) && isfinite(I3))) bad = 1;
+  }
+  if (FULL) {
+    if (status && __any_sync(__activemask(), bad) && (l & 31) == 0) atomicOr(&status[col], FZ_NAN);
+    return;
+  }
+  if (active) {
     // EQVDSYN = REAL(sum) * GAIN (src/forward.f90:614-621)
     float* jo = jac + (size_t)col * np * nfreq;
     for (int j = 0; j < np; ++j)
@@ -847,6 +889,69 @@ __global__ void __launch_bounds__(256, 2) k_synth_rf(const DevParams* __restrict
         for (int c = 0; c < 4; ++c) jo[(size_t)j * nfreq + c * nw + l] = 0.0f;
   }
   if (status && __any_sync(__activemask(), bad) && (l & 31) == 0) atomicOr(&status[col], FZ_NAN);
+}
+
+// Response functions at emergence from the local ones (FULL mode of
+// k_synth_rf): RF(K) = O_NZ ... O_{K+1} RF_loc(K), OLD_DSYN_PROPAGATION
+// (src/forward.f90:511-548), times GAIN as CALCULATE_EQUIVALENT_DSYN with
+// NJ = NZ (:604-621).  One CTA per column, one thread per wavelength walking
+// down from the top with the 4x4 product of the operators above in
+// registers; in place on rf.  A (parameter, height) column with an infinite
+// entry is zeroed, the SUM(ABS(.)) > HUGE test of :672-679.
+__global__ void __launch_bounds__(256) k_rf_prop(int nz, int nw, const float* __restrict__ gain,
+                                                 const float* __restrict__ oscr, float* __restrict__ rf) {
+  extern __shared__ int flg[];
+  const int col = blockIdx.x, l = threadIdx.x;
+  for (int i = l; i < nz; i += blockDim.x) flg[i] = 0;
+  __syncthreads();
+  const bool active = l < nw;
+  const size_t nfreq = 4 * (size_t)nw;
+  float* base = rf + (size_t)col * NSLOT * nz * nfreq + l;
+  if (active) {
+    float g[4];
+#pragma unroll
+    for (int c = 0; c < 4; ++c) g[c] = gain[4 * l + c];
+    const float* ob = oscr + (size_t)col * nz * 16 * nw + l;
+    float A[16];
+#pragma unroll
+    for (int i = 0; i < 16; ++i) A[i] = (i % 5 == 0) ? 1.0f : 0.0f;
+    for (int k = nz - 1; k >= 0; --k) {
+      int f = 0;
+#pragma unroll
+      for (int p = 0; p < NSLOT; ++p) {
+        float* q = base + ((size_t)p * nz + k) * nfreq;
+        const float r0 = q[0], r1 = q[nw], r2 = q[2 * nw], r3 = q[3 * nw];
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+          const float v = fmaf(A[4 * i], r0, fmaf(A[4 * i + 1], r1, fmaf(A[4 * i + 2], r2, A[4 * i + 3] * r3))) * g[i];
+          q[(size_t)i * nw] = v;
+          if (isinf(v)) f |= 1 << p;
+        }
+      }
+      if (f) atomicOr(&flg[k], f);
+      float O[16];
+#pragma unroll
+      for (int i = 0; i < 16; ++i) O[i] = ob[((size_t)k * 16 + i) * nw];
+      float B[16];
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+          B[4 * i + j] = fmaf(A[4 * i], O[j], fmaf(A[4 * i + 1], O[4 + j], fmaf(A[4 * i + 2], O[8 + j], A[4 * i + 3] * O[12 + j])));
+#pragma unroll
+      for (int i = 0; i < 16; ++i) A[i] = B[i];
+    }
+  }
+  __syncthreads();
+  if (active)
+    for (int k = 0; k < nz; ++k) {
+      const int f = flg[k];
+      if (!f) continue;
+      for (int p = 0; p < NSLOT; ++p)
+        if (f & (1 << p))
+#pragma unroll
+          for (int c = 0; c < 4; ++c) base[((size_t)p * nz + k) * nfreq + (size_t)c * nw] = 0.0f;
+    }
 }
 
 }  // namespace
@@ -1097,7 +1202,7 @@ LineP host_line(const fz_line& L, double wdif, const Consts& K) {
 
 }  // namespace
 
-constexpr int NKERN = 11;   // k_chain, k_opac, k_synth, k_opac_rf, k_synth_rf, k_lm_fill, k_lm_accept, k_lm_normal, k_lm_solve, k_lm_update, k_chemder
+constexpr int NKERN = 12;   // k_chain, k_opac, k_synth, k_opac_rf, k_synth_rf, k_lm_fill, k_lm_accept, k_lm_normal, k_lm_solve, k_lm_update, k_chemder, k_rf_prop
 
 struct fz_ctx {
   int device = 0;
@@ -1110,6 +1215,14 @@ struct fz_ctx {
   Consts* d_consts = nullptr;
   PFTable* d_pf = nullptr;
   PFDTable* d_pfd = nullptr;
+  struct {
+    int chain_warps = 4;       // k_chain warps (columns) per block
+    int chemder_bpsm = 32;     // k_chemder resident-block cap per SM (0 = one block per 4 cells)
+    int opacrf_threads = 256;  // k_opac_rf block size
+    int lm_slots = 8192;       // pixels in flight when fz_lm_opts.slots == 0
+  } tune;
+  float* d_oscr = nullptr;   // operators of the full-height RF path (ncol, nz, 16, numw)
+  size_t oscr_len = 0;
   LamP* d_lam = nullptr;
   float* d_gain = nullptr;
   // scratch (grown on demand): per (column, height) nH, ne and the opacity slab
@@ -1149,7 +1262,8 @@ struct fz_ctx {
   size_t lm_cap = 0;
   int lm_np = 0;
   LMQueue* d_q = nullptr;
-  int* h_done = nullptr;   // pinned
+  int* h_done = nullptr;
+  LMQueue* h_q = nullptr;   // pinned copy of the work-queue state   // pinned
 };
 
 namespace {
@@ -1238,9 +1352,7 @@ size_t rf_smem(const fz_ctx* c) {
          sizeof(float);
 }
 
-int launch_forward_rf(fz_ctx* c, int ncol, const float* d_model, int hydrostatic, double* d_syn, float* d_jac,
-                      float* d_mout, int* d_status, cudaStream_t s) {
-  if (c->rf.np <= 0 || !c->d_coef) return FZ_ERR_STATE;
+int ensure_rf_scratch(fz_ctx* c, int ncol) {
   int rc = ensure_scratch(c, ncol);
   if (rc) return rc;
   const int swr = rf_w(c->nreg, c->nlu);
@@ -1254,40 +1366,102 @@ int launch_forward_rf(fz_ctx* c, int ncol, const float* d_model, int hydrostatic
     FZ_CK(cudaMalloc(&c->d_chemd, (size_t)ncol * c->nz * sizeof(double4)));
     c->rf_cols = ncol;
   }
-  if (d_status) FZ_CK(cudaMemsetAsync(d_status, 0, ncol * sizeof(int), s));
-  const int wpb = 4;
+  return 0;
+}
+
+// The chemistry and opacity-derivative launches of the RF path with an
+// explicit launch shape (the autotuner's candidates; c->tune otherwise).
+void launch_chain(fz_ctx* c, int ncol, const float* d_model, float* d_mout, int* d_status, int hydrostatic, int wpb,
+                  cudaStream_t s) {
   const dim3 gc((ncol + wpb - 1) / wpb);
+  if (hydrostatic)
+    k_chain<true><<<gc, wpb * 32, 0, s>>>(c->d_consts, c->d_pf, ncol, c->nz, d_model, d_mout, c->d_chem, d_status);
+  else
+    k_chain<false><<<gc, wpb * 32, 0, s>>>(c->d_consts, c->d_pf, ncol, c->nz, d_model, d_mout, c->d_chem, d_status);
+}
+
+void launch_chemder(fz_ctx* c, int ncol, const float* d_mout, int bpsm, cudaStream_t s) {
+  const size_t cells = (size_t)ncol * c->nz;
+  size_t blocks = (cells + 3) / 4;
+  if (bpsm > 0) blocks = std::min<size_t>(blocks, (size_t)c->nsm * bpsm);
+  k_chemder<<<(int)blocks, 128, 0, s>>>(c->d_params, c->d_consts, c->d_pf, c->d_pfd, ncol, d_mout, c->d_chem,
+                                        c->d_chemd);
+}
+
+void launch_opac_rf(fz_ctx* c, int ncol, const float* d_mout, int threads, cudaStream_t s) {
+  const size_t cells = (size_t)ncol * c->nz;
+  const int b2 = (int)std::min<size_t>((cells + threads - 1) / threads, (size_t)c->nsm * (4096 / threads));
+  k_opac_rf<<<b2, threads, 0, s>>>(c->d_params, c->d_consts, ncol, d_mout, c->d_chem, c->d_chemd, c->d_rfslab);
+}
+
+// full = false: node Jacobian (NFREQ, NP) per column with the layout of
+// fz_rf_nodes; full = true: response functions at every height
+// (NFREQ, 6 NZ) per column.
+int launch_forward_rf(fz_ctx* c, int ncol, const float* d_model, int hydrostatic, double* d_syn, float* d_jac,
+                      float* d_mout, int* d_status, cudaStream_t s, bool full = false) {
+  if (!full && (c->rf.np <= 0 || !c->d_coef)) return FZ_ERR_STATE;
+  int rc = ensure_rf_scratch(c, ncol);
+  if (rc) return rc;
+  const int swr = rf_w(c->nreg, c->nlu);
+  if (d_status) FZ_CK(cudaMemsetAsync(d_status, 0, ncol * sizeof(int), s));
   {
     ProfScope ps(c, 0, s, ncol);
-    if (hydrostatic)
-      k_chain<true><<<gc, wpb * 32, 0, s>>>(c->d_consts, c->d_pf, ncol, c->nz, d_model, d_mout, c->d_chem, d_status);
-    else
-      k_chain<false><<<gc, wpb * 32, 0, s>>>(c->d_consts, c->d_pf, ncol, c->nz, d_model, d_mout, c->d_chem, d_status);
+    launch_chain(c, ncol, d_model, d_mout, d_status, hydrostatic, c->tune.chain_warps, s);
   }
   FZ_CK(cudaGetLastError());
-  const size_t cells = (size_t)ncol * c->nz;
   {
     ProfScope ps(c, 10, s, ncol);
-    const int blocks = (int)std::min<size_t>((cells + 3) / 4, (size_t)c->nsm * 32);
-    k_chemder<<<blocks, 128, 0, s>>>(c->d_params, c->d_consts, c->d_pf, c->d_pfd, ncol, d_mout, c->d_chem, c->d_chemd);
+    launch_chemder(c, ncol, d_mout, c->tune.chemder_bpsm, s);
   }
   FZ_CK(cudaGetLastError());
   {
     ProfScope ps(c, 3, s, ncol);
-    const int b2 = (int)std::min<size_t>((cells + 255) / 256, (size_t)c->nsm * 16);
-    k_opac_rf<<<b2, 256, 0, s>>>(c->d_params, c->d_consts, ncol, d_mout, c->d_chem, c->d_chemd, c->d_rfslab);
+    launch_opac_rf(c, ncol, d_mout, c->tune.opacrf_threads, s);
   }
   FZ_CK(cudaGetLastError());
   const int threads = (c->numw + 31) & ~31;
+  if (full) {
+    const size_t need = (size_t)ncol * c->nz * 16 * c->numw;
+    if (need > c->oscr_len) {
+      cudaFree(c->d_oscr);
+      c->d_oscr = nullptr;
+      c->oscr_len = 0;
+      FZ_CK(cudaMalloc(&c->d_oscr, need * sizeof(float)));
+      c->oscr_len = need;
+    }
+    const size_t sms = (size_t)c->nz * swr * sizeof(float);
+    FZ_CK(cudaFuncSetAttribute(k_synth_rf<true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sms));
+    FZ_CK(cudaFuncSetAttribute(k_synth_rf<false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sms));
+    {
+      ProfScope ps(c, 4, s, ncol);
+      if (hydrostatic)
+        k_synth_rf<true, true><<<ncol, threads, sms, s>>>(c->d_params, c->d_rf, c->d_lam, c->d_gain, ncol,
+                                                          c->d_rfslab, nullptr, d_syn, d_jac, c->d_oscr, d_mout,
+                                                          d_status);
+      else
+        k_synth_rf<false, true><<<ncol, threads, sms, s>>>(c->d_params, c->d_rf, c->d_lam, c->d_gain, ncol,
+                                                           c->d_rfslab, nullptr, d_syn, d_jac, c->d_oscr, d_mout,
+                                                           d_status);
+    }
+    FZ_CK(cudaGetLastError());
+    {
+      ProfScope ps(c, 11, s, ncol);
+      k_rf_prop<<<ncol, threads, c->nz * sizeof(int), s>>>(c->nz, c->numw, c->d_gain, c->d_oscr, d_jac);
+    }
+    FZ_CK(cudaGetLastError());
+    return 0;
+  }
   const size_t sms = rf_smem(c);
   {
     ProfScope ps(c, 4, s, ncol);
     if (hydrostatic)
-      k_synth_rf<true><<<ncol, threads, sms, s>>>(c->d_params, c->d_rf, c->d_lam, c->d_gain, ncol, c->d_rfslab,
-                                                  c->d_coef, d_syn, d_jac, d_mout, d_status);
+      k_synth_rf<true, false><<<ncol, threads, sms, s>>>(c->d_params, c->d_rf, c->d_lam, c->d_gain, ncol,
+                                                         c->d_rfslab, c->d_coef, d_syn, d_jac, nullptr, d_mout,
+                                                         d_status);
     else
-      k_synth_rf<false><<<ncol, threads, sms, s>>>(c->d_params, c->d_rf, c->d_lam, c->d_gain, ncol, c->d_rfslab,
-                                                   c->d_coef, d_syn, d_jac, d_mout, d_status);
+      k_synth_rf<false, false><<<ncol, threads, sms, s>>>(c->d_params, c->d_rf, c->d_lam, c->d_gain, ncol,
+                                                          c->d_rfslab, c->d_coef, d_syn, d_jac, nullptr, d_mout,
+                                                          d_status);
   }
   FZ_CK(cudaGetLastError());
   return 0;
@@ -1649,6 +1823,7 @@ int fz_destroy(fz_ctx* c) {
   cudaFree(c->d_consts);
   cudaFree(c->d_pf);
   cudaFree(c->d_pfd);
+  cudaFree(c->d_oscr);
   cudaFree(c->d_lam);
   cudaFree(c->d_gain);
   cudaFree(c->d_slab);
@@ -1665,6 +1840,7 @@ int fz_destroy(fz_ctx* c) {
   lm_free(c);
   cudaFree(c->d_q);
   if (c->h_done) cudaFreeHost(c->h_done);
+  if (c->h_q) cudaFreeHost(c->h_q);
   for (auto& p : c->pending) {
     cudaEventDestroy(p.a);
     cudaEventDestroy(p.b);
@@ -1771,12 +1947,12 @@ int fz_rf_nodes(fz_ctx* c, const int* nodes) {
     c->rf.np = 0;
     return FZ_ERR_LIMIT;
   }
-  FZ_CK(cudaFuncSetAttribute(k_synth_rf<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sms));
-  FZ_CK(cudaFuncSetAttribute(k_synth_rf<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sms));
+  FZ_CK(cudaFuncSetAttribute(k_synth_rf<true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sms));
+  FZ_CK(cudaFuncSetAttribute(k_synth_rf<false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sms));
   // all of the SM's unified L1/shared storage as shared memory: two CTAs of
   // ~90 KB each can then be resident
-  FZ_CK(cudaFuncSetAttribute(k_synth_rf<true>, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
-  FZ_CK(cudaFuncSetAttribute(k_synth_rf<false>, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
+  FZ_CK(cudaFuncSetAttribute(k_synth_rf<true, false>, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
+  FZ_CK(cudaFuncSetAttribute(k_synth_rf<false, false>, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
   return np;
 }
 
@@ -1795,7 +1971,7 @@ int fz_invert_device(fz_ctx* c, int npix, const double* d_obs, const float* d_in
   LMConf C;
   int rc = lm_conf(c, npix, opts, C);
   if (rc) return rc;
-  int S = (opts && opts->slots > 0) ? opts->slots : 8192;
+  int S = (opts && opts->slots > 0) ? opts->slots : c->tune.lm_slots;
   if (S > npix) S = npix;
   if ((rc = lm_alloc(c, S))) return rc;
   cudaStream_t s = (cudaStream_t)stream;
@@ -1823,9 +1999,14 @@ int fz_invert_device(fz_ctx* c, int npix, const double* d_obs, const float* d_in
   LMQueue hq{};
   // every pixel needs at most maxit iterations; slots are refilled at once
   const long long cap = (long long)C.maxit * ((npix + S - 1) / S + 1) + 8;
-  for (long long it = 0; it < cap; ++it) {
-    const int n = L.S;
-    if ((rc = launch_forward_rf(c, n, L.mcur, hydrostatic, L.syn, L.jac, L.mcur, L.status, s))) return rc;
+  if (!c->h_q) FZ_CK(cudaMallocHost(&c->h_q, sizeof(LMQueue)));
+  if ((rc = ensure_rf_scratch(c, S))) return rc;
+  // one LM iteration over the n slots of pool L: forward + node Jacobian,
+  // accept/refill, normal equations, solve, update, and the queue state to
+  // the host
+  auto iteration = [&](int n) -> int {
+    int r = launch_forward_rf(c, n, L.mcur, hydrostatic, L.syn, L.jac, L.mcur, L.status, s);
+    if (r) return r;
     {
       ProfScope ps(c, 6, s, n);
       k_lm_accept<<<n, 256, 0, s>>>(C, L, c->d_q, d_w, d_obs, d_init, d_target_chi2, d_model_out, d_chi2, d_iters,
@@ -1845,8 +2026,47 @@ int fz_invert_device(fz_ctx* c, int npix, const double* d_obs, const float* d_in
     }
     k_lm_scan<<<1, 1024, 0, s>>>(n, L.pix, c->d_dest, c->d_q);
     FZ_CK(cudaGetLastError());
-    FZ_CK(cudaMemcpyAsync(&hq, c->d_q, sizeof(LMQueue), cudaMemcpyDeviceToHost, s));
+    FZ_CK(cudaMemcpyAsync(c->h_q, c->d_q, sizeof(LMQueue), cudaMemcpyDeviceToHost, s));
+    return 0;
+  };
+  // Without profiling, the iteration is captured once per pool state (slot
+  // count and pool) as a CUDA graph and replayed until a compaction changes
+  // it; with profiling, its kernels are launched one by one between events.
+  struct Graph {
+    cudaGraph_t g = nullptr;
+    cudaGraphExec_t e = nullptr;
+    void reset() {
+      if (e) cudaGraphExecDestroy(e);
+      if (g) cudaGraphDestroy(g);
+      e = nullptr;
+      g = nullptr;
+    }
+    ~Graph() { reset(); }
+  } graph;
+  int graph_n = -1;
+  const float* graph_pool = nullptr;
+  for (long long it = 0; it < cap; ++it) {
+    const int n = L.S;
+    if (c->prof) {
+      if ((rc = iteration(n))) return rc;
+    } else {
+      if (!graph.e || graph_n != n || graph_pool != L.mcur) {
+        graph.reset();
+        FZ_CK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+        rc = iteration(n);
+        cudaGraph_t g = nullptr;
+        const cudaError_t ce = cudaStreamEndCapture(s, &g);
+        graph.g = g;
+        if (rc) return rc;
+        FZ_CK(ce);
+        FZ_CK(cudaGraphInstantiate(&graph.e, graph.g, 0));
+        graph_n = n;
+        graph_pool = L.mcur;
+      }
+      FZ_CK(cudaGraphLaunch(graph.e, s));
+    }
     FZ_CK(cudaStreamSynchronize(s));
+    hq = *c->h_q;
     if (hq.done >= npix) return 0;
     // the queue is drained: move the occupied slots to the front of the
     // other pool once a quarter of the pool has emptied, and iterate on them only
@@ -1963,10 +2183,11 @@ int fz_lm_perturbation(fz_ctx* c, int npix, int np, int nfreq, const float* jac,
   return rc;
 }
 
-int fz_forward_rf(fz_ctx* c, int ncol, const float* model, int hydrostatic, double* syn, float* jac, float* model_out,
-                  int* status) {
+static int forward_rf_host(fz_ctx* c, int ncol, const float* model, int hydrostatic, double* syn, float* jac,
+                           float* model_out, int* status, bool full) {
   if (!c || ncol <= 0 || !model || !syn || !jac) return FZ_ERR_ARG;
-  if (c->rf.np <= 0) return FZ_ERR_STATE;
+  if (!full && c->rf.np <= 0) return FZ_ERR_STATE;
+  const int npj = full ? NSLOT * c->nz : c->rf.np;
   FZ_CK(cudaSetDevice(c->device));
   if ((size_t)ncol > c->io_cols) {
     cudaFree(c->d_model);
@@ -1981,24 +2202,196 @@ int fz_forward_rf(fz_ctx* c, int ncol, const float* model, int hydrostatic, doub
     FZ_CK(cudaMalloc(&c->d_status, (size_t)ncol * sizeof(int)));
     c->io_cols = ncol;
   }
-  const size_t jb = (size_t)ncol * c->rf.np * 4 * c->numw * sizeof(float);
-  if ((size_t)ncol * c->rf.np > c->jac_cols) {
+  const size_t jb = (size_t)ncol * npj * 4 * c->numw * sizeof(float);
+  if ((size_t)ncol * npj > c->jac_cols) {
     cudaFree(c->d_jac);
     c->d_jac = nullptr;
     c->jac_cols = 0;
     FZ_CK(cudaMalloc(&c->d_jac, jb));
-    c->jac_cols = (size_t)ncol * c->rf.np;
+    c->jac_cols = (size_t)ncol * npj;
   }
   cudaStream_t s = c->stream;
   const size_t mb = (size_t)ncol * 13 * c->nz * sizeof(float);
   FZ_CK(cudaMemcpyAsync(c->d_model, model, mb, cudaMemcpyHostToDevice, s));
-  int rc = launch_forward_rf(c, ncol, c->d_model, hydrostatic, c->d_syn, c->d_jac, c->d_model, c->d_status, s);
+  int rc = launch_forward_rf(c, ncol, c->d_model, hydrostatic, c->d_syn, c->d_jac, c->d_model, c->d_status, s, full);
   if (rc) return rc;
   FZ_CK(cudaMemcpyAsync(syn, c->d_syn, (size_t)ncol * 4 * c->numw * sizeof(double), cudaMemcpyDeviceToHost, s));
   FZ_CK(cudaMemcpyAsync(jac, c->d_jac, jb, cudaMemcpyDeviceToHost, s));
   if (model_out) FZ_CK(cudaMemcpyAsync(model_out, c->d_model, mb, cudaMemcpyDeviceToHost, s));
   if (status) FZ_CK(cudaMemcpyAsync(status, c->d_status, ncol * sizeof(int), cudaMemcpyDeviceToHost, s));
   FZ_CK(cudaStreamSynchronize(s));
+  return 0;
+}
+
+int fz_forward_rf(fz_ctx* c, int ncol, const float* model, int hydrostatic, double* syn, float* jac, float* model_out,
+                  int* status) {
+  return forward_rf_host(c, ncol, model, hydrostatic, syn, jac, model_out, status, false);
+}
+
+int fz_forward_rf_full(fz_ctx* c, int ncol, const float* model, int hydrostatic, double* syn, float* rf,
+                       float* model_out, int* status) {
+  return forward_rf_host(c, ncol, model, hydrostatic, syn, rf, model_out, status, true);
+}
+
+int fz_forward_rf_full_device(fz_ctx* c, int ncol, const float* d_model, int hydrostatic, double* d_syn, float* d_rf,
+                              float* d_model_out, int* d_status, void* stream) {
+  if (!c || ncol <= 0 || !d_model || !d_syn || !d_rf || !d_model_out) return FZ_ERR_ARG;
+  FZ_CK(cudaSetDevice(c->device));
+  return launch_forward_rf(c, ncol, d_model, hydrostatic, d_syn, d_rf, d_model_out, d_status, (cudaStream_t)stream,
+                           true);
+}
+
+// ------------------------------------------------------------- autotuner
+// Launch shapes of the RF path measured on the caller's columns: every
+// candidate of a kernel runs once untimed and three times between CUDA events
+// on the context's stream, with the inputs the previous kernel of the chain
+// left (the kernels are deterministic, so repeated launches do the same
+// work); the fastest is kept in the context.
+int fz_autotune_forward(fz_ctx* c, int ncol, const float* d_model, int hydrostatic, fz_tune* out) {
+  if (!c || ncol <= 0 || !d_model) return FZ_ERR_ARG;
+  FZ_CK(cudaSetDevice(c->device));
+  int rc = ensure_rf_scratch(c, ncol);
+  if (rc) return rc;
+  cudaStream_t s = c->stream;
+  float* d_mout = nullptr;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  struct Cleanup {
+    float*& m;
+    cudaEvent_t &a, &b;
+    ~Cleanup() {
+      cudaFree(m);
+      if (a) cudaEventDestroy(a);
+      if (b) cudaEventDestroy(b);
+    }
+  } cl{d_mout, e0, e1};
+  FZ_CK(cudaMalloc(&d_mout, (size_t)ncol * 13 * c->nz * sizeof(float)));
+  FZ_CK(cudaEventCreate(&e0));
+  FZ_CK(cudaEventCreate(&e1));
+  auto timed = [&](auto&& launch, float& ms) -> int {
+    launch();
+    FZ_CK(cudaEventRecord(e0, s));
+    for (int r = 0; r < 3; ++r) launch();
+    FZ_CK(cudaEventRecord(e1, s));
+    FZ_CK(cudaEventSynchronize(e1));
+    FZ_CK(cudaGetLastError());
+    FZ_CK(cudaEventElapsedTime(&ms, e0, e1));
+    ms /= 3.0f;
+    return 0;
+  };
+  float best = 0.0f, ms = 0.0f, tchain = 0.0f, tchem = 0.0f, topac = 0.0f;
+  int bw = c->tune.chain_warps;
+  static const int kWarps[] = {1, 2, 4};
+  for (int i = 0; i < 3; ++i) {
+    const int w = kWarps[i];
+    if ((rc = timed([&] { launch_chain(c, ncol, d_model, d_mout, nullptr, hydrostatic, w, s); }, ms))) return rc;
+    if (i == 0 || ms < best) best = ms, bw = w;
+  }
+  tchain = best;
+  launch_chain(c, ncol, d_model, d_mout, nullptr, hydrostatic, bw, s);
+  int bb = c->tune.chemder_bpsm;
+  static const int kBpsm[] = {8, 16, 32, 64, 0};
+  for (int i = 0; i < 5; ++i) {
+    const int b = kBpsm[i];
+    if ((rc = timed([&] { launch_chemder(c, ncol, d_mout, b, s); }, ms))) return rc;
+    if (i == 0 || ms < best) best = ms, bb = b;
+  }
+  tchem = best;
+  int bt = c->tune.opacrf_threads;
+  static const int kThreads[] = {64, 128, 256};
+  for (int i = 0; i < 3; ++i) {
+    const int t = kThreads[i];
+    if ((rc = timed([&] { launch_opac_rf(c, ncol, d_mout, t, s); }, ms))) return rc;
+    if (i == 0 || ms < best) best = ms, bt = t;
+  }
+  topac = best;
+  c->tune.chain_warps = bw;
+  c->tune.chemder_bpsm = bb;
+  c->tune.opacrf_threads = bt;
+  if (out) {
+    out->chain_warps = bw;
+    out->chemder_blocks_per_sm = bb;
+    out->opac_rf_threads = bt;
+    out->lm_slots = c->tune.lm_slots;
+    out->chain_ms = tchain;
+    out->chemder_ms = tchem;
+    out->opac_rf_ms = topac;
+  }
+  return 0;
+}
+
+// Pixels in flight of the batched inversion: each candidate inverts the same
+// npix pixels (device buffers as fz_invert_device) and the highest
+// pixels/s is kept as the default of fz_lm_opts.slots == 0.
+int fz_autotune_lm(fz_ctx* c, int npix, const double* d_obs, const float* d_init, const double* d_target_chi2,
+                   int hydrostatic, const fz_lm_opts* opts, const int* candidates, int ncand, fz_tune* out) {
+  if (!c || npix <= 0 || !d_obs || !d_init || !candidates || ncand <= 0) return FZ_ERR_ARG;
+  FZ_CK(cudaSetDevice(c->device));
+  cudaStream_t s = c->stream;
+  float* d_mo = nullptr;
+  double* d_chi = nullptr;
+  int* d_it = nullptr;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  int rc = 0;
+  float bestrate = -1.0f;
+  int bests = c->tune.lm_slots;
+  do {
+    if ((rc = cuda_fail(cudaMalloc(&d_mo, (size_t)npix * 13 * c->nz * sizeof(float))))) break;
+    if ((rc = cuda_fail(cudaMalloc(&d_chi, (size_t)npix * sizeof(double))))) break;
+    if ((rc = cuda_fail(cudaMalloc(&d_it, (size_t)npix * sizeof(int))))) break;
+    if ((rc = cuda_fail(cudaEventCreate(&e0)))) break;
+    if ((rc = cuda_fail(cudaEventCreate(&e1)))) break;
+    fz_lm_opts o{};
+    if (opts) o = *opts;
+    for (int i = 0; i < ncand && !rc; ++i) {
+      if (candidates[i] <= 0) {
+        rc = FZ_ERR_ARG;
+        break;
+      }
+      o.slots = std::min(candidates[i], npix);
+      if ((rc = cuda_fail(cudaEventRecord(e0, s)))) break;
+      if ((rc = fz_invert_device(c, npix, d_obs, d_init, d_target_chi2, hydrostatic, &o, d_mo, d_chi, d_it, nullptr,
+                                 nullptr, s)))
+        break;
+      if ((rc = cuda_fail(cudaEventRecord(e1, s)))) break;
+      if ((rc = cuda_fail(cudaEventSynchronize(e1)))) break;
+      float ms = 0.0f;
+      if ((rc = cuda_fail(cudaEventElapsedTime(&ms, e0, e1)))) break;
+      const float rate = (float)npix / (ms * 1e-3f);
+      if (rate > bestrate) bestrate = rate, bests = o.slots;
+    }
+  } while (false);
+  cudaFree(d_mo);
+  cudaFree(d_chi);
+  cudaFree(d_it);
+  if (e0) cudaEventDestroy(e0);
+  if (e1) cudaEventDestroy(e1);
+  if (rc) return rc;
+  c->tune.lm_slots = bests;
+  if (out) {
+    out->lm_slots = bests;
+    out->lm_pixels_per_s = bestrate;
+  }
+  return 0;
+}
+
+int fz_tune_get(fz_ctx* c, fz_tune* t) {
+  if (!c || !t) return FZ_ERR_ARG;
+  t->chain_warps = c->tune.chain_warps;
+  t->chemder_blocks_per_sm = c->tune.chemder_bpsm;
+  t->opac_rf_threads = c->tune.opacrf_threads;
+  t->lm_slots = c->tune.lm_slots;
+  return 0;
+}
+
+int fz_tune_set(fz_ctx* c, const fz_tune* t) {
+  if (!c || !t) return FZ_ERR_ARG;
+  if (t->chain_warps < 1 || t->chain_warps > 4 || t->chemder_blocks_per_sm < 0 || t->lm_slots < 1 ||
+      (t->opac_rf_threads != 64 && t->opac_rf_threads != 128 && t->opac_rf_threads != 256))
+    return FZ_ERR_ARG;
+  c->tune.chain_warps = t->chain_warps;
+  c->tune.chemder_bpsm = t->chemder_blocks_per_sm;
+  c->tune.opacrf_threads = t->opac_rf_threads;
+  c->tune.lm_slots = t->lm_slots;
   return 0;
 }
 

@@ -148,9 +148,23 @@ __global__ void __launch_bounds__(256) k_gemm(int M, int N, int K, const __nv_bf
 }
 
 // MSE loss 1/(n*nout) sum (y - t)^2 and dL/dy in bf16
+// Training-step state on the device, so that one captured step replays for
+// every batch: the position in the epoch's batch order and the Adam step.
+struct TrainState {
+  int bi;
+  int step;
+};
+
+// Row offset of the current batch (order: the epoch's batch permutation).
+__device__ __forceinline__ size_t batch_row(const int* order, const TrainState* st, int n) {
+  return order ? (size_t)order[st->bi] * n : 0;
+}
+
 __global__ void k_mse(int n, int nout, const float* __restrict__ y, const float* __restrict__ t,
-                      __nv_bfloat16* __restrict__ dy, float* __restrict__ loss) {
+                      __nv_bfloat16* __restrict__ dy, float* __restrict__ loss, const int* __restrict__ order,
+                      const TrainState* __restrict__ st) {
   __shared__ float red[8];
+  t += batch_row(order, st, n) * nout;
   const size_t total = (size_t)n * nout;
   float s = 0.0f;
   const float sc = 2.0f / (float)total;
@@ -183,10 +197,27 @@ __global__ void k_to_bf16(size_t n, const float* __restrict__ x, __nv_bfloat16* 
     y[i] = __float2bfloat16_rn(x[i]);
 }
 
-// Adam (Kingma & Ba 2015) on FP32 masters, refreshing the bf16 copy
+// the current batch's rows (n x d) of x as bf16
+__global__ void k_batch_bf16(int n, int d, const float* __restrict__ x, const int* __restrict__ order,
+                             const TrainState* __restrict__ st, __nv_bfloat16* __restrict__ y) {
+  x += batch_row(order, st, n) * d;
+  const size_t total = (size_t)n * d;
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (size_t)gridDim.x * blockDim.x)
+    y[i] = __float2bfloat16_rn(x[i]);
+}
+
+__global__ void k_train_advance(TrainState* st) {
+  st->bi += 1;
+  st->step += 1;
+}
+
+// Adam (Kingma & Ba 2015) on FP32 masters, refreshing the bf16 copy; the
+// bias corrections 1/(1 - b^t) of step t = st->step + 1
 __global__ void k_adam(size_t n, float* __restrict__ w, const float* __restrict__ g, float* __restrict__ m1,
                        float* __restrict__ m2, __nv_bfloat16* __restrict__ wb, float lr, float b1, float b2,
-                       float c1, float c2, float eps) {
+                       const TrainState* __restrict__ st, float eps) {
+  const float t = (float)(st->step + 1);
+  const float c1 = 1.0f / (1.0f - powf(b1, t)), c2 = 1.0f / (1.0f - powf(b2, t));
   for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
     const float gi = g[i];
     const float a = b1 * m1[i] + (1.0f - b1) * gi;
@@ -231,6 +262,9 @@ struct fz_mlp {
   float* loss = nullptr;
   long long step = 0;
   cudaStream_t stream = nullptr;
+  TrainState* tstate = nullptr;   // device
+  int* order = nullptr;           // device batch order of one epoch
+  int order_cap = 0;
 };
 
 namespace {
@@ -368,6 +402,8 @@ int fz_mlp_destroy(fz_mlp* p) {
   for (int l = 0; l <= MLP_MAXL; ++l) cudaFree(p->act[l]);
   cudaFree(p->yout);
   cudaFree(p->loss);
+  cudaFree(p->tstate);
+  cudaFree(p->order);
   if (p->stream) cudaStreamDestroy(p->stream);
   delete p;
   return 0;
@@ -453,7 +489,7 @@ int fz_mlp_grad_device(fz_mlp* p, int n, const float* d_x, const float* d_t, flo
   k_to_bf16<<<grid1((size_t)n * d0), 256, 0, s>>>((size_t)n * d0, d_x, p->act[0]);
   mlp_fwd(p, n);
   MLP_CK(cudaMemsetAsync(p->loss, 0, sizeof(float), s));
-  k_mse<<<grid1((size_t)n * dl), 256, 0, s>>>(n, dl, p->yout, d_t, p->dz[p->nl - 1], p->loss);
+  k_mse<<<grid1((size_t)n * dl), 256, 0, s>>>(n, dl, p->yout, d_t, p->dz[p->nl - 1], p->loss, nullptr, nullptr);
   mlp_bwd(p, n);
   MLP_CK(cudaGetLastError());
   if (loss) MLP_CK(cudaMemcpyAsync(loss, p->loss, sizeof(float), cudaMemcpyDeviceToHost, s));
@@ -474,6 +510,38 @@ int fz_mlp_train_device(fz_mlp* p, int n, const float* d_x, const float* d_t, in
   const int d0 = p->dim[0], dl = p->dim[p->nl];
   const int nb = n / batch;
   if (nb <= 0) return FZ_ERR_ARG;
+  if (!p->tstate && (rc = mlp_fail(cudaMalloc(&p->tstate, sizeof(TrainState))))) return rc;
+  if (nb > p->order_cap) {
+    cudaFree(p->order);
+    p->order = nullptr;
+    p->order_cap = 0;
+    if ((rc = mlp_fail(cudaMalloc(&p->order, nb * sizeof(int))))) return rc;
+    p->order_cap = nb;
+  }
+  // One training step (batch gather, forward, loss, backward, Adam, state
+  // advance) captured once as a CUDA graph and replayed for every batch: the
+  // batch offset and the Adam step come from the device state.
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  if ((rc = mlp_fail(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal)))) return rc;
+  {
+    k_batch_bf16<<<grid1((size_t)batch * d0), 256, 0, s>>>(batch, d0, d_x, p->order, p->tstate, p->act[0]);
+    mlp_fwd(p, batch);
+    k_mse<<<grid1((size_t)batch * dl), 256, 0, s>>>(batch, dl, p->yout, d_t, p->dz[p->nl - 1], p->loss, p->order,
+                                                   p->tstate);
+    mlp_bwd(p, batch);
+    const float b1 = 0.9f, b2 = 0.999f;
+    for (int l = 0; l < p->nl; ++l) {
+      const size_t nw = (size_t)p->dim[l] * p->dim[l + 1];
+      k_adam<<<grid1(nw), 256, 0, s>>>(nw, p->W[l], p->gW[l], p->mW[l], p->vW[l], p->Wb[l], lr, b1, b2, p->tstate,
+                                       1e-8f);
+      k_adam<<<grid1(p->dim[l + 1]), 256, 0, s>>>(p->dim[l + 1], p->b[l], p->gb[l], p->mb[l], p->vb[l], nullptr, lr,
+                                                  b1, b2, p->tstate, 1e-8f);
+    }
+    k_train_advance<<<1, 1, 0, s>>>(p->tstate);
+  }
+  rc = mlp_fail(cudaStreamEndCapture(s, &graph));
+  if (!rc) rc = mlp_fail(cudaGraphInstantiate(&exec, graph, 0));
   // batch order: a fixed random permutation of the batch indices per epoch
   std::vector<int> order(nb);
   unsigned long long st = seed | 1ull;
@@ -487,30 +555,19 @@ int fz_mlp_train_device(fz_mlp* p, int n, const float* d_x, const float* d_t, in
       const int j = (int)(st % (unsigned long long)(i + 1));
       std::swap(order[i], order[j]);
     }
-    cudaMemsetAsync(p->loss, 0, sizeof(float), s);
-    for (int bi = 0; bi < nb; ++bi) {
-      const size_t r0 = (size_t)order[bi] * batch;
-      k_to_bf16<<<grid1((size_t)batch * d0), 256, 0, s>>>((size_t)batch * d0, d_x + r0 * d0, p->act[0]);
-      mlp_fwd(p, batch);
-      k_mse<<<grid1((size_t)batch * dl), 256, 0, s>>>(batch, dl, p->yout, d_t + r0 * dl, p->dz[p->nl - 1], p->loss);
-      mlp_bwd(p, batch);
-      ++p->step;
-      const float b1 = 0.9f, b2 = 0.999f;
-      const float c1 = 1.0f / (1.0f - std::pow(b1, (float)p->step));
-      const float c2 = 1.0f / (1.0f - std::pow(b2, (float)p->step));
-      for (int l = 0; l < p->nl; ++l) {
-        const size_t nw = (size_t)p->dim[l] * p->dim[l + 1];
-        k_adam<<<grid1(nw), 256, 0, s>>>(nw, p->W[l], p->gW[l], p->mW[l], p->vW[l], p->Wb[l], lr, b1, b2, c1, c2,
-                                         1e-8f);
-        k_adam<<<grid1(p->dim[l + 1]), 256, 0, s>>>(p->dim[l + 1], p->b[l], p->gb[l], p->mb[l], p->vb[l], nullptr,
-                                                    lr, b1, b2, c1, c2, 1e-8f);
-      }
-    }
+    const TrainState ts{0, (int)p->step};
+    rc = mlp_fail(cudaMemcpyAsync(p->order, order.data(), nb * sizeof(int), cudaMemcpyHostToDevice, s));
+    if (!rc) rc = mlp_fail(cudaMemcpyAsync(p->tstate, &ts, sizeof(ts), cudaMemcpyHostToDevice, s));
+    if (!rc) rc = mlp_fail(cudaMemsetAsync(p->loss, 0, sizeof(float), s));
+    for (int bi = 0; bi < nb && !rc; ++bi) rc = mlp_fail(cudaGraphLaunch(exec, s));
+    p->step += nb;
     float h = 0.0f;
-    rc = mlp_fail(cudaMemcpyAsync(&h, p->loss, sizeof(float), cudaMemcpyDeviceToHost, s));
+    if (!rc) rc = mlp_fail(cudaMemcpyAsync(&h, p->loss, sizeof(float), cudaMemcpyDeviceToHost, s));
     if (!rc) rc = mlp_fail(cudaStreamSynchronize(s));
     last = h / (float)nb;
   }
+  if (exec) cudaGraphExecDestroy(exec);
+  if (graph) cudaGraphDestroy(graph);
   if (!rc) rc = mlp_fail(cudaGetLastError());
   if (loss) *loss = last;
   return rc;

@@ -149,6 +149,42 @@ int fz_forward_rf(fz_ctx* ctx, int ncol, const float* model, int hydrostatic, do
 int fz_forward_rf_device(fz_ctx* ctx, int ncol, const float* d_model, int hydrostatic, double* d_syn,
                          float* d_jac, float* d_model_out, int* d_status, void* stream);
 
+/* Forward synthesis with the response functions at every height, the
+ * WRITE RESPONSE FUNCTION output (src/pre_post_duties.f90:331-353): the
+ * EQVDSYN of CALCULATE_EQUIVALENT_DSYN with NJ = NZ for each of T, Pg, Bx,
+ * By, Bz, v_z (src/forward.f90:552-681), i.e. rf is (NFREQ, 6 NZ, ncol)
+ * REAL*4, parameter blocks of NZ heights in that order, x GAIN; the same
+ * hydrostatic conventions as fz_forward_rf.  Needs no fz_rf_nodes call.
+ * 2.75 MB of rf per column at NZ = 128, NUMW = 224 (plus a device scratch of
+ * the per-layer operators, 64 B per height and wavelength): callers stream
+ * large fields in batches. */
+int fz_forward_rf_full(fz_ctx* ctx, int ncol, const float* model, int hydrostatic, double* syn, float* rf,
+                       float* model_out, int* status);
+int fz_forward_rf_full_device(fz_ctx* ctx, int ncol, const float* d_model, int hydrostatic, double* d_syn,
+                              float* d_rf, float* d_model_out, int* d_status, void* stream);
+
+/* Launch-shape autotuner (no counterpart in the reference).  The shapes
+ * live in the context and apply to every later call on it:
+ *   chain_warps            columns (warps) per block of the chemistry chain
+ *                          kernel, 1..4
+ *   chemder_blocks_per_sm  grid cap of the chemistry-derivative kernel per
+ *                          SM (0 = one block per 4 heights)
+ *   opac_rf_threads        block size of the opacity-derivative kernel
+ *                          (64, 128 or 256)
+ *   lm_slots               pixels in flight of the inversion when
+ *                          fz_lm_opts.slots is 0
+ * fz_autotune_forward times the candidates of the first three on ncol
+ * device columns; fz_autotune_lm inverts the same npix pixels once per
+ * candidate slot count and keeps the highest pixels/s.  The *_ms and
+ * lm_pixels_per_s fields report the winners' timings. */
+typedef struct {
+  int chain_warps, chemder_blocks_per_sm, opac_rf_threads, lm_slots;
+  float chain_ms, chemder_ms, opac_rf_ms, lm_pixels_per_s;
+} fz_tune;
+int fz_autotune_forward(fz_ctx* ctx, int ncol, const float* d_model, int hydrostatic, fz_tune* out);
+int fz_tune_get(fz_ctx* ctx, fz_tune* out);
+int fz_tune_set(fz_ctx* ctx, const fz_tune* t);
+
 /* Options of the batched inversion (the reference's control-file values in
  * brackets): maxsteps, the per-pixel limit on the STEPS counter of
  * UPDATE_LAMBDA (MAXITER, 5); maxit, a hard cap on iterations per pixel;
@@ -182,6 +218,9 @@ int fz_invert_device(fz_ctx* ctx, int npix, const double* d_obs, const float* d_
                      const double* d_target_chi2, int hydrostatic, const fz_lm_opts* opts,
                      float* d_model_out, double* d_chi2, int* d_iters, double* d_syn_out, int* d_status,
                      void* stream);
+
+int fz_autotune_lm(fz_ctx* ctx, int npix, const double* d_obs, const float* d_init, const double* d_target_chi2,
+                   int hydrostatic, const fz_lm_opts* opts, const int* candidates, int ncand, fz_tune* out);
 
 /* Batched GET_PERTURBATION (src/lm.f90:137-204, SOLVER_METHOD = 1) on host
  * buffers: for each pixel H = J^T J (tensor cores, split-bf16 x3, FP32
@@ -217,7 +256,7 @@ int fz_mlp_train_device(fz_mlp* mlp, int n, const float* d_x, const float* d_t, 
  * milliseconds, launch counts and processed columns (or LM slots; items
  * may be NULL) of the kernels (names in order:
  * "k_chain", "k_opac", "k_synth", "k_opac_rf", "k_synth_rf", "k_lm_fill",
- * "k_lm_accept", "k_lm_normal", "k_lm_solve", "k_lm_update", "k_chemder") and resets
+ * "k_lm_accept", "k_lm_normal", "k_lm_solve", "k_lm_update", "k_chemder", "k_rf_prop") and resets
  * them; returns the kernel count.  Replaces the reference's
  * SYSTEM_CLOCK "Forward 3D:" timer (src/forward.f90:99-100, :295-297). */
 int fz_profile_enable(fz_ctx* ctx, int on);

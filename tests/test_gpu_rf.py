@@ -78,3 +78,53 @@ def test_rf_nodes_validation(fz, orc):
         ctx.rf_nodes({1: 33})           # more nodes than heights
     with pytest.raises(fz.FzError):
         ctx.forward_rf(m)               # no node layout yet
+
+
+@pytest.mark.parametrize("he", [True, False])
+def test_full_height_rf_matches_oracle(fz, orc, he):
+    """fz_forward_rf_full: the WRITE RESPONSE FUNCTION output (one node per
+    height for T, Pg, Bx, By, Bz, v_z) against the oracle's EQVDSYN with
+    NJ = NZ; heights compared against the strongest height of the same
+    (column, parameter)."""
+    nz = 32
+    lines, reg, g, m = _setup(fz, orc, nz=nz, ncol=4, seed=11)
+    if not he:
+        _, m, _ = orc.forward(lines, reg, g, m, hydrostatic=True)
+    ctx = fz.Synthesis(lines, reg, nz=nz, gain=g)
+    syn, rf, mo, st = ctx.forward_rf_full(m, hydrostatic=he)
+    nodes = {1: nz, 2: nz, 4: nz, 5: nz, 6: nz, 7: nz}
+    osyn, ojac, _, ost = orc.forward_rf(lines, reg, g, m, nodes, hydrostatic=he)
+    assert np.all(st == 0) and np.all(ost == 0)
+    assert rf.shape == (m.shape[0], 6, nz, 4 * syn.shape[2])
+    assert np.max(np.abs(syn[:, 0] - osyn[:, 0]) / np.abs(osyn[:, 0])) < 1e-5
+    assert np.max(np.abs(syn[:, 1:] - osyn[:, 1:])) < 1e-6
+    o = ojac.reshape(rf.shape)
+    err = np.abs(rf.astype(np.float64) - o).max(axis=3)           # (ncol, 6, nz)
+    pmax = np.abs(o).max(axis=(2, 3))                               # (ncol, 6)
+    assert np.all(pmax > 0)
+    rel = err / pmax[:, :, None]
+    assert rel.max() <= RF_TOL, rel.max()
+
+
+@pytest.mark.parametrize("he", [True, False])
+def test_full_height_rf_contracts_to_node_jacobian(fz, orc, he):
+    """At the benchmark's height grid: the hat-function contraction of the
+    response functions at every height equals the node Jacobian of the node
+    path (CALCULATE_EQUIVALENT_DSYN is linear in DSYN1D), to FP32 rounding."""
+    from firtez_dz_b200 import warmstart as ws
+    nz = 128
+    lines, reg, g, m = _setup(fz, orc, nz=nz, ncol=16, seed=5)
+    ctx = fz.Synthesis(lines, reg, nz=nz, gain=g)
+    nodes = {1: 5, 2: 3, 4: 2, 5: 2, 6: 2, 7: 2}
+    ctx.rf_nodes(nodes)
+    _, jac, _, st1 = ctx.forward_rf(m, hydrostatic=he)
+    _, rf, _, st2 = ctx.forward_rf_full(m, hydrostatic=he)
+    assert np.all(st1 == 0) and np.all(st2 == 0)
+    cols = []
+    for slot, p in enumerate((1, 2, 4, 5, 6, 7)):
+        c = ws.hat_coefs(nz, nodes[p])                               # (nz, nj)
+        cols.append(np.einsum("kj,nkf->njf", c, rf[:, slot].astype(np.float64)))
+    jc = np.concatenate(cols, axis=1)
+    scale = np.abs(jac).max(axis=2, keepdims=True)
+    assert np.all(scale > 0)
+    assert np.max(np.abs(jc - jac) / scale) <= 1e-4
