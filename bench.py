@@ -156,6 +156,8 @@ def main():
     ap.add_argument("--epochs", type=int, default=6)
     ap.add_argument("--cpu-pixels", type=int, default=24)
     ap.add_argument("--synth-cols", type=int, default=256 * 256)
+    ap.add_argument("--rf-chunk", type=int, default=4096, help="columns per full-height RF call")
+    ap.add_argument("--no-tune", action="store_true", help="keep the default launch shapes")
     a = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -252,6 +254,19 @@ def main():
                 "gen_s": t1 - t0, "train_s": t2 - t1, "params": warm.mlp.nparams}
     ctx.rf_nodes(NODES)
     opts = fz.LMOpts(maxsteps=5, maxit=40, dchi2=1e-3, isigma=1e-3, slots=a.slots)
+    tuned = None
+    if not a.no_tune:
+        # the autotuner: launch shapes of the RF chemistry kernels on default-guess
+        # columns, then the slot count by inverting the first tile (plain LM)
+        # once per candidate; the arms below use the tuned slot count
+        t0 = time.perf_counter()
+        tf = ctx.autotune_forward(base.data_ptr(), min(8192, a.tile), hydrostatic=True)
+        cands = tuple(c for c in (a.tile // 4, a.tile // 2, a.tile) if c >= 256)
+        tl = ctx.autotune_lm(a.tile, obs[:a.tile].data_ptr(), base.data_ptr(), candidates=cands, opts=opts)
+        tuned = {"shapes": ctx.tune(), "slot_candidates": list(cands),
+                 "forward_ms": {k: tf[k] for k in ("chain_ms", "chemder_ms", "opac_rf_ms")},
+                 "lm_pixels_per_s_at_best": tl["lm_pixels_per_s"], "tuning_s": time.perf_counter() - t0}
+        opts = fz.LMOpts(maxsteps=5, maxit=40, dchi2=1e-3, isigma=1e-3, slots=0)
     ntiles = npix // a.tile
     bufs = {"out": torch.empty((a.tile, 13, a.nz), dtype=torch.float32, device="cuda"),
             "chi": torch.empty(a.tile, dtype=torch.float64, device="cuda"),
@@ -414,6 +429,41 @@ def main():
     synthesis = {"value": world * ns * numw / (ms_syn * 1e-3), "unit": "columns*lambda/s",
                  "workload": "%d columns x %d heights x %d lambda, hydrostatic" % (ns, a.nz, numw),
                  "ms_per_call": ms_syn, "kernel_ms": {k: v[0] / max(v[1], 1) for k, v in sprof.items() if v[1]}}
+    # ------------------------------- response functions at every height (C2)
+    # 256x256 columns (the synthesis sub-metric's) through fz_forward_rf_full
+    # in batches of rf_chunk columns; each batch's output (rf_chunk x 6 x NZ x
+    # NFREQ float32, 11.3 GB at 4096) is overwritten by the next
+    rc_ = min(a.rf_chunk, ns)
+    rfo = torch.empty((rc_, 6, a.nz, nf), dtype=torch.float32, device="cuda")
+    sor = torch.empty((rc_, 4, numw), dtype=torch.float64, device="cuda")
+    mor = torch.empty((rc_, 13, a.nz), dtype=torch.float32, device="cuda")
+    nb_rf = ns // rc_
+
+    def rf_batch(i):
+        ctx.forward_rf_full_device(m[i * rc_:(i + 1) * rc_].data_ptr(), rc_, sor.data_ptr(), rfo.data_ptr(),
+                                   mor.data_ptr(), 0, stream=stream, hydrostatic=True)
+
+    rf_batch(0)
+    torch.cuda.synchronize()
+    ctx.profile(True)
+    ctx.profile_read()
+    e0.record()
+    for i in range(nb_rf):
+        rf_batch(i)
+    e1.record()
+    torch.cuda.synchronize()
+    ctx.profile(False)
+    rprof = ctx.profile_read()
+    ms_rf = maxms(e0.elapsed_time(e1))
+    rf_full = {"value": world * nb_rf * rc_ * numw / (ms_rf * 1e-3), "unit": "columns*lambda/s",
+               "workload": "%d columns x %d heights x %d lambda, hydrostatic, RFs to T, Pg, Bx, By, Bz, v_z at "
+                           "every height (fz_forward_rf_full, %d columns per call)" % (nb_rf * rc_, a.nz, numw, rc_),
+               "ms_total": ms_rf, "rf_bytes_per_column": 6 * a.nz * nf * 4,
+               "kernel_ms": {k: v[0] / max(v[1], 1) for k, v in rprof.items() if v[1]},
+               "error_vs_oracle": "tests/test_gpu_rf.py: every (column, parameter, height) within 2e-3 of the "
+                                  "parameter's largest response; Stokes I 1e-5 relative, Q/U/V 1e-6 I_c"}
+    del rfo, sor, mor
+    torch.cuda.empty_cache()
     if rank != 0:
         if dist is not None:
             dist.destroy_process_group()
@@ -449,7 +499,7 @@ def main():
            "ms_per_step": ms_nn, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "fp32",
            "data": "synthetic (seeded atmospheres, firtez-dz_b200/atmos.py; observations = GPU synthesis + "
                    "1e-3 noise)",
-           "config": config,
+           "config": dict(config, autotuned=tuned if tuned else "off (--no-tune): slots %d" % a.slots),
            "plain": {"value": plain_value, "unit": UNIT, "ms_per_step": ms_pl,
                      "median_chi2": float(np.median(chi_pl)), "mean_iterations": float(it_pl.mean()),
                      "clocks": clocks_pl},
@@ -473,6 +523,7 @@ def main():
                                            "atmospheres against the true ones at the heights where the true "
                                            "log tau5 is in [-3, 0], over the compared pixels"),
            "synthesis": synthesis,
+           "rf_full": rf_full,
            "roofline": {"bound": "hbm", "kernel": kname, "achieved": achieved, "peak": hbm, "unit": "GB/s",
                         "frac": achieved / hbm, "traffic": traffic,
                         "peak_source": how + " (MEASURED_PEAKS.json hbm_gbs)" if how == "measured" else how,

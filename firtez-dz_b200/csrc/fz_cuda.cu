@@ -396,16 +396,18 @@ struct RFConf {
 __global__ void __launch_bounds__(128) k_chemder(const DevParams* __restrict__ Pg, const Consts* __restrict__ Kg,
                                                  const PFTable* __restrict__ tb, const PFDTable* __restrict__ td,
                                                  int ncol, const float* __restrict__ mout,
-                                                 const double2* __restrict__ chem, double4* __restrict__ chemd) {
+                                                 const double2* __restrict__ chem, double4* __restrict__ chemd,
+                                                 const int* __restrict__ list, const int* __restrict__ nlist) {
   __shared__ Consts K;
   copy_to_shared(&K, Kg);
   __syncthreads();
   const int nz = Pg->nz;
   const int lane = threadIdx.x & 31;
   const int wpb = blockDim.x >> 5;
-  const size_t total = (size_t)ncol * nz;
-  for (size_t i = (size_t)blockIdx.x * wpb + (threadIdx.x >> 5); i < total; i += (size_t)gridDim.x * wpb) {
-    const int col = (int)(i / nz), k = (int)(i % nz);
+  const size_t total = (size_t)(list ? *nlist : ncol) * nz;
+  for (size_t j = (size_t)blockIdx.x * wpb + (threadIdx.x >> 5); j < total; j += (size_t)gridDim.x * wpb) {
+    const int k = (int)(j % nz), col = list ? list[j / nz] : (int)(j / nz);
+    const size_t i = (size_t)col * nz + k;
     const float* m = mout + (size_t)col * 13 * nz;
     const ChemDer cd = chem_der_warp((double)mget(m, nz, 0, k), (double)mget(m, nz, 1, k), chem[i].y, K, tb, td, lane);
     if (lane == 0) chemd[i] = make_double4(cd.dne_p, cd.dnh_p, cd.dne_t, cd.dnh_t);
@@ -419,7 +421,8 @@ __global__ void __launch_bounds__(128) k_chemder(const DevParams* __restrict__ P
 __global__ void __launch_bounds__(256) k_opac_rf(const DevParams* __restrict__ Pg, const Consts* __restrict__ Kg,
                                                  int ncol, const float* __restrict__ mout,
                                                  const double2* __restrict__ chem, const double4* __restrict__ chemd,
-                                                 float* __restrict__ slab) {
+                                                 float* __restrict__ slab, const int* __restrict__ list,
+                                                 const int* __restrict__ nlist) {
   __shared__ DevParams P;
   __shared__ Consts K;
   copy_to_shared(&P, Pg);
@@ -427,9 +430,10 @@ __global__ void __launch_bounds__(256) k_opac_rf(const DevParams* __restrict__ P
   __syncthreads();
   const int nz = P.nz, nreg = P.nreg, nlu = P.nlu;
   const int sw = rf_w(nreg, nlu);
-  const size_t total = (size_t)ncol * nz;
-  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (size_t)gridDim.x * blockDim.x) {
-    const int col = (int)(i / nz), k = (int)(i % nz);
+  const size_t total = (size_t)(list ? *nlist : ncol) * nz;
+  for (size_t j = (size_t)blockIdx.x * blockDim.x + threadIdx.x; j < total; j += (size_t)gridDim.x * blockDim.x) {
+    const int k = (int)(j % nz), col = list ? list[j / nz] : (int)(j / nz);
+    const size_t i = (size_t)col * nz + k;
     const float* m = mout + (size_t)col * 13 * nz;
     const double2 c = chem[i];
     const double nhyd = c.x, nelec = c.y;
@@ -583,14 +587,16 @@ __global__ void __launch_bounds__(256, 2) k_synth_rf(const DevParams* __restrict
                                                   int ncol, const float* __restrict__ slab,
                                                   const float* __restrict__ coefg, double* __restrict__ syn,
                                                   float* __restrict__ jac, float* __restrict__ oscr, float* mout,
-                                                  int* __restrict__ status) {
+                                                  int* __restrict__ status, const int* __restrict__ list,
+                                                  const int* __restrict__ nlist) {
+  if (list && (int)blockIdx.x >= *nlist) return;
   extern __shared__ float4 sm_rf4[];
   __shared__ DevParams P;
   __shared__ RFConf C;
   __shared__ unsigned inf_mask[2];
   copy_to_shared(&P, Pg);
   if (!FULL) copy_to_shared(&C, Rg);
-  const int col = blockIdx.x;
+  const int col = list ? list[blockIdx.x] : (int)blockIdx.x;
   const int nz = Pg->nz, nreg = Pg->nreg, nlu = Pg->nlu, np = FULL ? 0 : Rg->np;
   const int sw = rf_w(nreg, nlu);
   const int nthr = blockDim.x;
@@ -771,22 +777,22 @@ __global__ void __launch_bounds__(256, 2) k_synth_rf(const DevParams* __restrict
     const float n3 = fmaf(-O[12], S, fmaf(O[12], I0, fmaf(O[13], I1, fmaf(O[14], I2, O[15] * I3))));
     float rf[NSLOT][4];
     if (fin) {
-      // runtime loops over the parameters: one copy of the directional
-      // derivative per Stokes vector it acts on keeps the code in the
-      // instruction cache
+      // unrolled over the parameters: the optical-depth derivatives and the
+      // response vectors stay in registers (a runtime parameter index would
+      // put both arrays in local memory; measured 8-13 % slower)
       EvolW wi;
       const float win[4] = {I0 - S, I1, I2, I3};
       evol_w(es, O, win, wi);
       if (HE) {
-#pragma unroll 1
+#pragma unroll
         for (int p = 0; p < 2; ++p) evol_dir(es, wi, dtau[p], rf[p]);
         EvolW wo;
         const float wout[4] = {n0 - S, n1, n2, n3};
         evol_w(es, O, wout, wo);
-#pragma unroll 1
+#pragma unroll
         for (int p = 2; p < NSLOT; ++p) evol_dir(es, wo, dtau[p], rf[p]);
       } else {
-#pragma unroll 1
+#pragma unroll
         for (int p = 0; p < NSLOT; ++p) evol_dir(es, wi, dtau[p], rf[p]);
       }
     } else {
@@ -1319,7 +1325,7 @@ int launch_forward(fz_ctx* c, int ncol, const float* d_model, int hydrostatic, d
   int rc = ensure_scratch(c, ncol);
   if (rc) return rc;
   if (d_status) FZ_CK(cudaMemsetAsync(d_status, 0, ncol * sizeof(int), s));
-  const int wpb = 4;
+  const int wpb = c->tune.chain_warps;
   const dim3 gc((ncol + wpb - 1) / wpb);
   {
     ProfScope ps(c, 0, s, ncol);
@@ -1380,18 +1386,55 @@ void launch_chain(fz_ctx* c, int ncol, const float* d_model, float* d_mout, int*
     k_chain<false><<<gc, wpb * 32, 0, s>>>(c->d_consts, c->d_pf, ncol, c->nz, d_model, d_mout, c->d_chem, d_status);
 }
 
-void launch_chemder(fz_ctx* c, int ncol, const float* d_mout, int bpsm, cudaStream_t s) {
+// list / nlist (device): only the columns list[0 .. *nlist) of the first ncol
+// (ncol bounds the grid); null: columns 0 .. ncol.
+void launch_chemder(fz_ctx* c, int ncol, const float* d_mout, int bpsm, cudaStream_t s, const int* list = nullptr,
+                    const int* nlist = nullptr) {
   const size_t cells = (size_t)ncol * c->nz;
   size_t blocks = (cells + 3) / 4;
   if (bpsm > 0) blocks = std::min<size_t>(blocks, (size_t)c->nsm * bpsm);
   k_chemder<<<(int)blocks, 128, 0, s>>>(c->d_params, c->d_consts, c->d_pf, c->d_pfd, ncol, d_mout, c->d_chem,
-                                        c->d_chemd);
+                                        c->d_chemd, list, nlist);
 }
 
-void launch_opac_rf(fz_ctx* c, int ncol, const float* d_mout, int threads, cudaStream_t s) {
+void launch_opac_rf(fz_ctx* c, int ncol, const float* d_mout, int threads, cudaStream_t s, const int* list = nullptr,
+                    const int* nlist = nullptr) {
   const size_t cells = (size_t)ncol * c->nz;
   const int b2 = (int)std::min<size_t>((cells + threads - 1) / threads, (size_t)c->nsm * (4096 / threads));
-  k_opac_rf<<<b2, threads, 0, s>>>(c->d_params, c->d_consts, ncol, d_mout, c->d_chem, c->d_chemd, c->d_rfslab);
+  k_opac_rf<<<b2, threads, 0, s>>>(c->d_params, c->d_consts, ncol, d_mout, c->d_chem, c->d_chemd, c->d_rfslab, list,
+                                   nlist);
+}
+
+// The response-function stage of the node path (chemistry derivatives,
+// opacity derivatives, RF synthesis + node Jacobian) on columns whose
+// chemistry k_chain has already left in the context's scratch.
+int launch_rf_stage(fz_ctx* c, int ncol, int hydrostatic, double* d_syn, float* d_jac, float* d_mout, int* d_status,
+                    cudaStream_t s, const int* list = nullptr, const int* nlist = nullptr) {
+  {
+    ProfScope ps(c, 10, s, list ? 0 : ncol);
+    launch_chemder(c, ncol, d_mout, c->tune.chemder_bpsm, s, list, nlist);
+  }
+  FZ_CK(cudaGetLastError());
+  {
+    ProfScope ps(c, 3, s, list ? 0 : ncol);
+    launch_opac_rf(c, ncol, d_mout, c->tune.opacrf_threads, s, list, nlist);
+  }
+  FZ_CK(cudaGetLastError());
+  const int threads = (c->numw + 31) & ~31;
+  const size_t sms = rf_smem(c);
+  {
+    ProfScope ps(c, 4, s, list ? 0 : ncol);
+    if (hydrostatic)
+      k_synth_rf<true, false><<<ncol, threads, sms, s>>>(c->d_params, c->d_rf, c->d_lam, c->d_gain, ncol,
+                                                         c->d_rfslab, c->d_coef, d_syn, d_jac, nullptr, d_mout,
+                                                         d_status, list, nlist);
+    else
+      k_synth_rf<false, false><<<ncol, threads, sms, s>>>(c->d_params, c->d_rf, c->d_lam, c->d_gain, ncol,
+                                                          c->d_rfslab, c->d_coef, d_syn, d_jac, nullptr, d_mout,
+                                                          d_status, list, nlist);
+  }
+  FZ_CK(cudaGetLastError());
+  return 0;
 }
 
 // full = false: node Jacobian (NFREQ, NP) per column with the layout of
@@ -1409,6 +1452,7 @@ int launch_forward_rf(fz_ctx* c, int ncol, const float* d_model, int hydrostatic
     launch_chain(c, ncol, d_model, d_mout, d_status, hydrostatic, c->tune.chain_warps, s);
   }
   FZ_CK(cudaGetLastError());
+  if (!full) return launch_rf_stage(c, ncol, hydrostatic, d_syn, d_jac, d_mout, d_status, s);
   {
     ProfScope ps(c, 10, s, ncol);
     launch_chemder(c, ncol, d_mout, c->tune.chemder_bpsm, s);
@@ -1420,7 +1464,7 @@ int launch_forward_rf(fz_ctx* c, int ncol, const float* d_model, int hydrostatic
   }
   FZ_CK(cudaGetLastError());
   const int threads = (c->numw + 31) & ~31;
-  if (full) {
+  {
     const size_t need = (size_t)ncol * c->nz * 16 * c->numw;
     if (need > c->oscr_len) {
       cudaFree(c->d_oscr);
@@ -1437,11 +1481,11 @@ int launch_forward_rf(fz_ctx* c, int ncol, const float* d_model, int hydrostatic
       if (hydrostatic)
         k_synth_rf<true, true><<<ncol, threads, sms, s>>>(c->d_params, c->d_rf, c->d_lam, c->d_gain, ncol,
                                                           c->d_rfslab, nullptr, d_syn, d_jac, c->d_oscr, d_mout,
-                                                          d_status);
+                                                          d_status, nullptr, nullptr);
       else
         k_synth_rf<false, true><<<ncol, threads, sms, s>>>(c->d_params, c->d_rf, c->d_lam, c->d_gain, ncol,
                                                            c->d_rfslab, nullptr, d_syn, d_jac, c->d_oscr, d_mout,
-                                                           d_status);
+                                                           d_status, nullptr, nullptr);
     }
     FZ_CK(cudaGetLastError());
     {
@@ -1451,20 +1495,6 @@ int launch_forward_rf(fz_ctx* c, int ncol, const float* d_model, int hydrostatic
     FZ_CK(cudaGetLastError());
     return 0;
   }
-  const size_t sms = rf_smem(c);
-  {
-    ProfScope ps(c, 4, s, ncol);
-    if (hydrostatic)
-      k_synth_rf<true, false><<<ncol, threads, sms, s>>>(c->d_params, c->d_rf, c->d_lam, c->d_gain, ncol,
-                                                         c->d_rfslab, c->d_coef, d_syn, d_jac, nullptr, d_mout,
-                                                         d_status);
-    else
-      k_synth_rf<false, false><<<ncol, threads, sms, s>>>(c->d_params, c->d_rf, c->d_lam, c->d_gain, ncol,
-                                                          c->d_rfslab, c->d_coef, d_syn, d_jac, nullptr, d_mout,
-                                                          d_status);
-  }
-  FZ_CK(cudaGetLastError());
-  return 0;
 }
 
 void lm_free_pool(LMSlots& L) {
@@ -1476,8 +1506,9 @@ void lm_free_pool(LMSlots& L) {
   cudaFree(L.mbest);
   cudaFree(L.syn);
   cudaFree(L.synb);
-  cudaFree(L.jac);
   cudaFree(L.jacb);
+  cudaFree(L.need_rf);
+  cudaFree(L.rf_list);
   cudaFree(L.obs);
   cudaFree(L.diff);
   cudaFree(L.H);
@@ -1505,8 +1536,9 @@ int lm_alloc_pool(LMSlots& L, int S, int np, int nf, int nm) {
   FZ_CK(cudaMalloc(&L.mbest, (size_t)S * nm * sizeof(float)));
   FZ_CK(cudaMalloc(&L.syn, (size_t)S * nf * sizeof(double)));
   FZ_CK(cudaMalloc(&L.synb, (size_t)S * nf * sizeof(double)));
-  FZ_CK(cudaMalloc(&L.jac, (size_t)S * np * nf * sizeof(float)));
   FZ_CK(cudaMalloc(&L.jacb, (size_t)S * np * nf * sizeof(float)));
+  FZ_CK(cudaMalloc(&L.need_rf, (size_t)S * sizeof(int)));
+  FZ_CK(cudaMalloc(&L.rf_list, (size_t)S * sizeof(int)));
   FZ_CK(cudaMalloc(&L.obs, (size_t)S * nf * sizeof(double)));
   FZ_CK(cudaMalloc(&L.diff, (size_t)S * nf * sizeof(double)));
   FZ_CK(cudaMalloc(&L.H, (size_t)S * np * np * sizeof(double)));
@@ -1974,7 +2006,18 @@ int fz_invert_device(fz_ctx* c, int npix, const double* d_obs, const float* d_in
   int S = (opts && opts->slots > 0) ? opts->slots : c->tune.lm_slots;
   if (S > npix) S = npix;
   if ((rc = lm_alloc(c, S))) return rc;
-  cudaStream_t s = (cudaStream_t)stream;
+  // The iterations run on the context's own stream (capturable, unlike a
+  // caller's legacy default stream), after the work already enqueued on the
+  // caller's stream; the call returns with everything complete.
+  cudaStream_t s = c->stream;
+  {
+    cudaEvent_t ev = nullptr;
+    FZ_CK(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+    const cudaError_t e1 = cudaEventRecord(ev, (cudaStream_t)stream);
+    const cudaError_t e2 = e1 == cudaSuccess ? cudaStreamWaitEvent(s, ev, 0) : e1;
+    cudaEventDestroy(ev);
+    FZ_CK(e2);
+  }
   if (!c->d_q) FZ_CK(cudaMalloc(&c->d_q, sizeof(LMQueue)));
   if (!c->h_done) FZ_CK(cudaMallocHost(&c->h_done, sizeof(int)));
   static const float kW1[4] = {1.f, 1.f, 1.f, 1.f};
@@ -2001,17 +2044,22 @@ int fz_invert_device(fz_ctx* c, int npix, const double* d_obs, const float* d_in
   const long long cap = (long long)C.maxit * ((npix + S - 1) / S + 1) + 8;
   if (!c->h_q) FZ_CK(cudaMallocHost(&c->h_q, sizeof(LMQueue)));
   if ((rc = ensure_rf_scratch(c, S))) return rc;
-  // one LM iteration over the n slots of pool L: forward + node Jacobian,
-  // accept/refill, normal equations, solve, update, and the queue state to
-  // the host
+  // one LM iteration over the n slots of pool L: synthesis of the current
+  // models, accept/refill, the response functions of the accepted models of
+  // pixels that go on (into the best Jacobian), normal equations, solve,
+  // update, and the queue state to the host
   auto iteration = [&](int n) -> int {
-    int r = launch_forward_rf(c, n, L.mcur, hydrostatic, L.syn, L.jac, L.mcur, L.status, s);
+    int r = launch_forward(c, n, L.mcur, hydrostatic, L.syn, L.mcur, L.status, s);
     if (r) return r;
     {
       ProfScope ps(c, 6, s, n);
       k_lm_accept<<<n, 256, 0, s>>>(C, L, c->d_q, d_w, d_obs, d_init, d_target_chi2, d_model_out, d_chi2, d_iters,
                                     d_syn_out, d_status);
     }
+    k_lm_rflist<<<1, 1024, 0, s>>>(n, L.need_rf, L.rf_list, c->d_q);
+    FZ_CK(cudaGetLastError());
+    r = launch_rf_stage(c, n, hydrostatic, L.syn, L.jacb, L.mcur, L.status, s, L.rf_list, &c->d_q->rf_count);
+    if (r) return r;
     {
       ProfScope ps(c, 7, s, n);
       k_lm_normal<<<(n + 3) / 4, 128, 0, s>>>(C, L, d_w);
@@ -2067,6 +2115,11 @@ int fz_invert_device(fz_ctx* c, int npix, const double* d_obs, const float* d_in
     }
     FZ_CK(cudaStreamSynchronize(s));
     hq = *c->h_q;
+    if (c->prof) {   // columns of the RF pass: known once the iteration ran
+      c->prof_items[10] += hq.rf_count;
+      c->prof_items[3] += hq.rf_count;
+      c->prof_items[4] += hq.rf_count;
+    }
     if (hq.done >= npix) return 0;
     // the queue is drained: move the occupied slots to the front of the
     // other pool once a quarter of the pool has emptied, and iterate on them only

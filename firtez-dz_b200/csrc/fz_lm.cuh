@@ -51,8 +51,9 @@ struct LMSlots {
   float* mbest;
   double* syn;       // (S, nfreq) forward output of mcur
   double* synb;      // best synthesis
-  float* jac;        // (S, np, nfreq) forward output
-  float* jacb;       // best Jacobian
+  float* jacb;       // best Jacobian (S, np, nfreq), written by the RF pass of accepted models
+  int* need_rf;      // 1 if the slot's model was accepted and the pixel goes on: its Jacobian is needed
+  int* rf_list;      // slots needing the RF pass, compacted (k_lm_rflist)
   double* obs;       // (S, nfreq)
   double* diff;      // weighted residual (S, nfreq)
   double* H;         // (S, np, np)
@@ -65,7 +66,7 @@ struct LMQueue {
   int next;          // next pixel to load
   int done;          // finished pixels
   int active;        // occupied slots (k_lm_scan)
-  int pad;
+  int rf_count;      // slots in the RF pass of this iteration (k_lm_rflist)
 };
 
 // PARAM_NORMS (src/get_dmodel.f90:31), LOWLIM/UPPLIM (:1885-1901)
@@ -118,6 +119,12 @@ __global__ void k_lm_fill(LMConf C, LMSlots Sl, LMQueue* q, const double* __rest
 }
 
 // One CTA per slot: chi2, accept/revert, lambda, residual, stop rule, refill.
+// The synthesis of the slot's model comes from the plain forward pass; the
+// response functions are computed afterwards only where they are used: for
+// an accepted model of a pixel that goes on (need_rf).  A rejected trial
+// keeps the best model's Jacobian and a finished pixel needs none, as in
+// the reference, which discards the response functions of rejected models
+// (EQVDSYN keeps the best, src/get_dmodel.f90:995-1005).
 __global__ void __launch_bounds__(256) k_lm_accept(LMConf C, LMSlots Sl, LMQueue* q, const double* __restrict__ w,
                                                    const double* __restrict__ obs_all,
                                                    const float* __restrict__ init_all,
@@ -127,7 +134,10 @@ __global__ void __launch_bounds__(256) k_lm_accept(LMConf C, LMSlots Sl, LMQueue
   __shared__ double red[8];
   __shared__ int acc, fin, np_next;
   const int s = blockIdx.x;
-  if (threadIdx.x == 0) Sl.skip[s] = 0;
+  if (threadIdx.x == 0) {
+    Sl.skip[s] = 0;
+    Sl.need_rf[s] = 0;
+  }
   const int p = Sl.pix[s];
   if (p < 0) return;
   const int nf = C.nfreq, nm = 13 * C.nz;
@@ -184,9 +194,7 @@ __global__ void __launch_bounds__(256) k_lm_accept(LMConf C, LMSlots Sl, LMQueue
     for (int i = threadIdx.x; i < nm; i += blockDim.x) mb[i] = mc[i];
     double* sb = Sl.synb + (size_t)s * nf;
     for (int i = threadIdx.x; i < nf; i += blockDim.x) sb[i] = syn[i];
-    const float4* jc = reinterpret_cast<const float4*>(Sl.jac + (size_t)s * C.np * nf);
-    float4* jb = reinterpret_cast<float4*>(Sl.jacb + (size_t)s * C.np * nf);
-    for (int i = threadIdx.x; i < C.np * nf / 4; i += blockDim.x) jb[i] = jc[i];
+    if (threadIdx.x == 0 && !fin) Sl.need_rf[s] = 1;
   } else {
     const float* mb = Sl.mbest + (size_t)s * nm;
     float* mc = Sl.mcur + (size_t)s * nm;
@@ -507,6 +515,29 @@ __global__ void __launch_bounds__(1024) k_lm_scan(int S, const int* __restrict__
   int d = part[threadIdx.x] - n;
   for (int i = b; i < e; ++i) dest[i] = pix[i] >= 0 ? d++ : -1;
   if (threadIdx.x == blockDim.x - 1) q->active = part[threadIdx.x];
+}
+
+// One block of 1024 threads: the slots of the RF pass (need_rf) compacted
+// into rf_list, and their count.
+__global__ void __launch_bounds__(1024) k_lm_rflist(int S, const int* __restrict__ need, int* __restrict__ list,
+                                                    LMQueue* q) {
+  __shared__ int part[1024];
+  const int per = (S + blockDim.x - 1) / blockDim.x;
+  const int b = threadIdx.x * per, e = min(S, b + per);
+  int n = 0;
+  for (int i = b; i < e; ++i) n += need[i] != 0;
+  part[threadIdx.x] = n;
+  __syncthreads();
+  for (int o = 1; o < (int)blockDim.x; o <<= 1) {   // inclusive Hillis-Steele scan
+    const int v = threadIdx.x >= o ? part[threadIdx.x - o] : 0;
+    __syncthreads();
+    part[threadIdx.x] += v;
+    __syncthreads();
+  }
+  int d = part[threadIdx.x] - n;
+  for (int i = b; i < e; ++i)
+    if (need[i]) list[d++] = i;
+  if (threadIdx.x == blockDim.x - 1) q->rf_count = part[threadIdx.x];
 }
 
 // One CTA per source slot: copy an occupied slot to its compacted position
