@@ -62,10 +62,16 @@ class LMOpts(ctypes.Structure):
     """fz_lm_opts: stop rules and weights of the batched inversion."""
     _fields_ = [("maxsteps", ctypes.c_int), ("maxit", ctypes.c_int), ("dchi2", ctypes.c_double),
                 ("svdtol", ctypes.c_double), ("isigma", ctypes.c_double), ("wstk", ctypes.c_float * 4),
-                ("slots", ctypes.c_int), ("pad", ctypes.c_int)]
+                ("slots", ctypes.c_int), ("pad", ctypes.c_int), ("fallback", ctypes.c_double),
+                ("fallback_model", ctypes.c_void_p)]
 
-    def __init__(self, maxsteps=5, maxit=40, dchi2=0.0, svdtol=1e-4, isigma=4e-3, wstk=(1, 1, 1, 1), slots=0):
-        super().__init__(maxsteps, maxit, dchi2, svdtol, isigma, (ctypes.c_float * 4)(*wstk), slots, 0)
+    def __init__(self, maxsteps=5, maxit=40, dchi2=0.0, svdtol=1e-4, isigma=4e-3, wstk=(1, 1, 1, 1), slots=0,
+                 fallback=0.0, fallback_model=0):
+        """fallback_model: device pointer of one MODEL(NZ,13) float32 (e.g. a
+        torch tensor's data_ptr()) that pixels ending above fallback x their
+        chi2 goal restart from."""
+        super().__init__(maxsteps, maxit, dchi2, svdtol, isigma, (ctypes.c_float * 4)(*wstk), slots, 0,
+                         float(fallback), fallback_model or None)
 
 
 class Tune(ctypes.Structure):
@@ -338,12 +344,13 @@ class Synthesis:
         d = t.as_dict()
         return {k: d[k] for k in ("chain_warps", "chemder_blocks_per_sm", "opac_rf_threads", "lm_slots")}
 
-    def invert(self, obs, init, hydrostatic=True, opts=None, want_syn=False, target=None):
+    def invert(self, obs, init, hydrostatic=True, opts=None, want_syn=False, target=None, out=None):
         """Batched LM inversion of host-resident pixels with the node layout of
         rf_nodes().  obs: (npix, 4, numw) float64 GAIN-normalised Stokes;
         init: (npix, 13, nz) float32 initial models; target: optional
-        per-pixel chi2 goal (npix,).  Returns (best models, chi2, iterations,
-        status[, best synthesis])."""
+        per-pixel chi2 goal (npix,); out: optional preallocated (models,
+        chi2, iterations, status) host arrays (e.g. in pinned memory).
+        Returns (best models, chi2, iterations, status[, best synthesis])."""
         o = np.ascontiguousarray(obs, dtype=np.float64)
         m = np.ascontiguousarray(init, dtype=np.float32)
         npix = o.shape[0]
@@ -355,10 +362,17 @@ class Synthesis:
             if tg.shape != (npix,):
                 raise ValueError("target must be (npix,)")
         opts = opts or LMOpts()
-        mo = np.empty_like(m)
-        chi = np.zeros(npix)
-        it = np.zeros(npix, dtype=np.int32)
-        st = np.zeros(npix, dtype=np.int32)
+        if out is not None:
+            mo, chi, it, st = out
+            if (mo.shape != m.shape or mo.dtype != np.float32 or chi.shape != (npix,) or chi.dtype != np.float64
+                    or it.shape != (npix,) or it.dtype != np.int32 or st.shape != (npix,) or st.dtype != np.int32
+                    or not all(a.flags.c_contiguous for a in (mo, chi, it, st))):
+                raise ValueError("out must be contiguous (model float32, chi2 float64, iters int32, status int32)")
+        else:
+            mo = np.empty_like(m)
+            chi = np.zeros(npix)
+            it = np.zeros(npix, dtype=np.int32)
+            st = np.zeros(npix, dtype=np.int32)
         syn = np.zeros_like(o) if want_syn else None
         _check(lib().fz_invert(self._h, npix, _p(o), _p(m), None if tg is None else _p(tg), int(bool(hydrostatic)),
                                ctypes.byref(opts), _p(mo),

@@ -1240,6 +1240,15 @@ struct fz_ctx {
   double* d_syn = nullptr;
   int* d_status = nullptr;
   size_t io_cols = 0;
+  // staging of the host-buffer inversion (grow on demand, kept across calls)
+  struct {
+    double *obs = nullptr, *chi = nullptr, *syn = nullptr, *tgt = nullptr;
+    float *init = nullptr, *out = nullptr;
+    int *it = nullptr, *st = nullptr;
+    float* fb = nullptr;   // the fallback model (13, nz)
+    size_t cap = 0;
+    bool has_syn = false;
+  } inv;
   cudaStream_t stream = nullptr;
   int nsm = 148;
   // per-kernel profiling (pending event pairs are resolved on read)
@@ -1500,6 +1509,7 @@ int launch_forward_rf(fz_ctx* c, int ncol, const float* d_model, int hydrostatic
 void lm_free_pool(LMSlots& L) {
   cudaFree(L.pix);
   cudaFree(L.skip);
+  cudaFree(L.restarted);
   cudaFree(L.iter);
   cudaFree(L.st);
   cudaFree(L.mcur);
@@ -1530,6 +1540,7 @@ int lm_alloc_pool(LMSlots& L, int S, int np, int nf, int nm) {
   L.S = S;
   FZ_CK(cudaMalloc(&L.pix, S * sizeof(int)));
   FZ_CK(cudaMalloc(&L.skip, S * sizeof(int)));
+  FZ_CK(cudaMalloc(&L.restarted, S * sizeof(int)));
   FZ_CK(cudaMalloc(&L.iter, S * sizeof(int)));
   FZ_CK(cudaMalloc(&L.st, 5 * (size_t)S * sizeof(double)));
   FZ_CK(cudaMalloc(&L.mcur, (size_t)S * nm * sizeof(float)));
@@ -1594,6 +1605,8 @@ int lm_conf(fz_ctx* c, int npix, const fz_lm_opts* o, LMConf& C) {
   C.dchi2 = o ? o->dchi2 : 0.0;
   C.svdtol = o && o->svdtol > 0 ? o->svdtol : 1.0e-4;
   C.inu = (double)C.nfreq;
+  C.fallback = o && o->fallback_model ? o->fallback : 0.0;
+  C.fb_model = o ? o->fallback_model : nullptr;
   const double norms[8] = {6000.0, 1.0e5, 1.0e-5, 1.0e3, 1.0e3, 1.0e3, 1.0e6, 6.0e2};
   // nodes in reference parameter order (the slot order of the Jacobian)
   for (int p = 0; p < NSLOT; ++p) {
@@ -1856,6 +1869,9 @@ int fz_destroy(fz_ctx* c) {
   cudaFree(c->d_pf);
   cudaFree(c->d_pfd);
   cudaFree(c->d_oscr);
+  for (void* p : {(void*)c->inv.obs, (void*)c->inv.chi, (void*)c->inv.syn, (void*)c->inv.tgt, (void*)c->inv.init,
+                  (void*)c->inv.out, (void*)c->inv.it, (void*)c->inv.st, (void*)c->inv.fb})
+    cudaFree(p);
   cudaFree(c->d_lam);
   cudaFree(c->d_gain);
   cudaFree(c->d_slab);
@@ -2134,52 +2150,71 @@ int fz_invert_device(fz_ctx* c, int npix, const double* d_obs, const float* d_in
   return FZ_ERR_STATE;
 }
 
+static void inv_free(fz_ctx* c) {
+  cudaFree(c->inv.obs);
+  cudaFree(c->inv.chi);
+  cudaFree(c->inv.syn);
+  cudaFree(c->inv.tgt);
+  cudaFree(c->inv.init);
+  cudaFree(c->inv.out);
+  cudaFree(c->inv.it);
+  cudaFree(c->inv.st);
+  cudaFree(c->inv.fb);
+  c->inv = {};
+}
+
 int fz_invert(fz_ctx* c, int npix, const double* obs, const float* init, const double* target_chi2, int hydrostatic,
               const fz_lm_opts* opts, float* model_out, double* chi2, int* iters, double* syn_out, int* status) {
   if (!c || npix <= 0 || !obs || !init || !model_out || !chi2 || !iters) return FZ_ERR_ARG;
   FZ_CK(cudaSetDevice(c->device));
   const size_t nf = 4 * (size_t)c->numw, nm = 13 * (size_t)c->nz;
-  double *d_obs = nullptr, *d_chi = nullptr, *d_syn = nullptr, *d_tgt = nullptr;
-  float *d_init = nullptr, *d_out = nullptr;
-  int *d_it = nullptr, *d_st = nullptr;
-  int rc = 0;
   cudaStream_t s = c->stream;
-  do {
-    if ((rc = cuda_fail(cudaMalloc(&d_obs, npix * nf * sizeof(double))))) break;
-    if ((rc = cuda_fail(cudaMalloc(&d_init, npix * nm * sizeof(float))))) break;
-    if ((rc = cuda_fail(cudaMalloc(&d_out, npix * nm * sizeof(float))))) break;
-    if ((rc = cuda_fail(cudaMalloc(&d_chi, npix * sizeof(double))))) break;
-    if ((rc = cuda_fail(cudaMalloc(&d_it, npix * sizeof(int))))) break;
-    if ((rc = cuda_fail(cudaMalloc(&d_st, npix * sizeof(int))))) break;
-    if (syn_out && (rc = cuda_fail(cudaMalloc(&d_syn, npix * nf * sizeof(double))))) break;
-    if ((rc = cuda_fail(cudaMemcpyAsync(d_obs, obs, npix * nf * sizeof(double), cudaMemcpyHostToDevice, s)))) break;
-    if ((rc = cuda_fail(cudaMemcpyAsync(d_init, init, npix * nm * sizeof(float), cudaMemcpyHostToDevice, s)))) break;
-    if (target_chi2) {
-      if ((rc = cuda_fail(cudaMalloc(&d_tgt, npix * sizeof(double))))) break;
-      if ((rc = cuda_fail(cudaMemcpyAsync(d_tgt, target_chi2, npix * sizeof(double), cudaMemcpyHostToDevice, s))))
-        break;
+  // device staging kept in the context between calls; it grows when a call
+  // brings more pixels (or asks for the synthesis for the first time)
+  if ((size_t)npix > c->inv.cap || (syn_out && !c->inv.has_syn)) {
+    FZ_CK(cudaStreamSynchronize(s));
+    const size_t n = std::max((size_t)npix, c->inv.cap);
+    const bool ws = syn_out || c->inv.has_syn;
+    inv_free(c);
+    int rc = 0;
+    if (!rc) rc = cuda_fail(cudaMalloc(&c->inv.obs, n * nf * sizeof(double)));
+    if (!rc) rc = cuda_fail(cudaMalloc(&c->inv.init, n * nm * sizeof(float)));
+    if (!rc) rc = cuda_fail(cudaMalloc(&c->inv.out, n * nm * sizeof(float)));
+    if (!rc) rc = cuda_fail(cudaMalloc(&c->inv.chi, n * sizeof(double)));
+    if (!rc) rc = cuda_fail(cudaMalloc(&c->inv.tgt, n * sizeof(double)));
+    if (!rc) rc = cuda_fail(cudaMalloc(&c->inv.it, n * sizeof(int)));
+    if (!rc) rc = cuda_fail(cudaMalloc(&c->inv.st, n * sizeof(int)));
+    if (!rc && ws) rc = cuda_fail(cudaMalloc(&c->inv.syn, n * nf * sizeof(double)));
+    if (rc) {
+      inv_free(c);
+      return rc;
     }
-    if ((rc = fz_invert_device(c, npix, d_obs, d_init, d_tgt, hydrostatic, opts, d_out, d_chi, d_it, d_syn, d_st, s)))
-      break;
-    if ((rc = cuda_fail(cudaMemcpyAsync(model_out, d_out, npix * nm * sizeof(float), cudaMemcpyDeviceToHost, s)))) break;
-    if ((rc = cuda_fail(cudaMemcpyAsync(chi2, d_chi, npix * sizeof(double), cudaMemcpyDeviceToHost, s)))) break;
-    if ((rc = cuda_fail(cudaMemcpyAsync(iters, d_it, npix * sizeof(int), cudaMemcpyDeviceToHost, s)))) break;
-    if (status && (rc = cuda_fail(cudaMemcpyAsync(status, d_st, npix * sizeof(int), cudaMemcpyDeviceToHost, s))))
-      break;
-    if (syn_out &&
-        (rc = cuda_fail(cudaMemcpyAsync(syn_out, d_syn, npix * nf * sizeof(double), cudaMemcpyDeviceToHost, s))))
-      break;
-    rc = cuda_fail(cudaStreamSynchronize(s));
-  } while (false);
-  cudaFree(d_obs);
-  cudaFree(d_init);
-  cudaFree(d_out);
-  cudaFree(d_chi);
-  cudaFree(d_it);
-  cudaFree(d_st);
-  cudaFree(d_syn);
-  cudaFree(d_tgt);
-  return rc;
+    c->inv.cap = n;
+    c->inv.has_syn = ws;
+  }
+  FZ_CK(cudaMemcpyAsync(c->inv.obs, obs, npix * nf * sizeof(double), cudaMemcpyHostToDevice, s));
+  FZ_CK(cudaMemcpyAsync(c->inv.init, init, npix * nm * sizeof(float), cudaMemcpyHostToDevice, s));
+  if (target_chi2)
+    FZ_CK(cudaMemcpyAsync(c->inv.tgt, target_chi2, npix * sizeof(double), cudaMemcpyHostToDevice, s));
+  // the fallback model comes from host memory here
+  fz_lm_opts o{};
+  if (opts) o = *opts;
+  if (opts && opts->fallback_model) {
+    if (!c->inv.fb) FZ_CK(cudaMalloc(&c->inv.fb, nm * sizeof(float)));
+    FZ_CK(cudaMemcpyAsync(c->inv.fb, opts->fallback_model, nm * sizeof(float), cudaMemcpyHostToDevice, s));
+    o.fallback_model = c->inv.fb;
+  }
+  int rc = fz_invert_device(c, npix, c->inv.obs, c->inv.init, target_chi2 ? c->inv.tgt : nullptr, hydrostatic,
+                            opts ? &o : nullptr,
+                            c->inv.out, c->inv.chi, c->inv.it, syn_out ? c->inv.syn : nullptr, c->inv.st, s);
+  if (rc) return rc;
+  FZ_CK(cudaMemcpyAsync(model_out, c->inv.out, npix * nm * sizeof(float), cudaMemcpyDeviceToHost, s));
+  FZ_CK(cudaMemcpyAsync(chi2, c->inv.chi, npix * sizeof(double), cudaMemcpyDeviceToHost, s));
+  FZ_CK(cudaMemcpyAsync(iters, c->inv.it, npix * sizeof(int), cudaMemcpyDeviceToHost, s));
+  if (status) FZ_CK(cudaMemcpyAsync(status, c->inv.st, npix * sizeof(int), cudaMemcpyDeviceToHost, s));
+  if (syn_out) FZ_CK(cudaMemcpyAsync(syn_out, c->inv.syn, npix * nf * sizeof(double), cudaMemcpyDeviceToHost, s));
+  FZ_CK(cudaStreamSynchronize(s));
+  return 0;
 }
 
 int fz_lm_perturbation(fz_ctx* c, int npix, int np, int nfreq, const float* jac, const double* diff,

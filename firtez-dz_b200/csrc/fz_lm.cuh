@@ -34,6 +34,8 @@ struct LMConf {
   int np, nfreq, nz, npix;
   int maxsteps, maxit;
   double dchi2, svdtol, inu;
+  double fallback;             // restart factor on the chi2 goal (0 = off)
+  const float* fb_model;       // MODEL(NZ,13) a restarted pixel starts from
   int nodes_ref[8];            // node count per reference parameter
   int row_of[LM_MAXNP];        // model row of each node's parameter
   int par_of[LM_MAXNP];        // reference parameter (1-based) of each node
@@ -45,6 +47,7 @@ struct LMSlots {
   int S;
   int* pix;          // pixel index, LM_PAD if empty
   int* skip;         // LM_SKIP if the slot was refilled in this iteration
+  int* restarted;    // 0, or 1 + the first attempt's iterations once the pixel restarted from the fallback model
   int* iter;
   double* st;        // 5 per slot: chicur, chibest, lambda, steps, precyc
   float* mcur;       // (S, 13, nz)
@@ -96,6 +99,7 @@ __device__ void lm_load_slot(const LMConf& C, const LMSlots& Sl, int s, int p, c
     if (threadIdx.x == 0) {
       Sl.pix[s] = p;
       Sl.iter[s] = 0;
+      Sl.restarted[s] = 0;
       double* st = Sl.st + 5 * (size_t)s;
       st[0] = 1.0e29;
       st[1] = 1.0e29;
@@ -201,6 +205,23 @@ __global__ void __launch_bounds__(256) k_lm_accept(LMConf C, LMSlots Sl, LMQueue
     for (int i = threadIdx.x; i < nm; i += blockDim.x) mc[i] = mb[i];
   }
   __syncthreads();
+  if (fin && C.fallback > 0.0 && C.fb_model && target && !Sl.restarted[s] && st[1] > C.fallback * target[p]) {
+    // the search ended above fallback x its goal: start once more from the
+    // fallback model (INITIALIZE_CYCLE's state), the goal kept
+    float* mc = Sl.mcur + (size_t)s * nm;
+    for (int i = threadIdx.x; i < nm; i += blockDim.x) mc[i] = C.fb_model[i];
+    if (threadIdx.x == 0) {
+      st[0] = 1.0e29;
+      st[1] = 1.0e29;
+      st[2] = 10.0;
+      st[3] = 0.0;
+      st[4] = 0.0;
+      Sl.restarted[s] = 1 + Sl.iter[s];
+      Sl.iter[s] = 0;
+      Sl.skip[s] = LM_SKIP;
+    }
+    return;
+  }
   if (fin) {
     // the pixel's result is its best model (END_CYCLE, src/invert3d.f90:306-312)
     const float* mb = Sl.mbest + (size_t)s * nm;
@@ -209,7 +230,7 @@ __global__ void __launch_bounds__(256) k_lm_accept(LMConf C, LMSlots Sl, LMQueue
       for (int i = threadIdx.x; i < nf; i += blockDim.x) out_syn[(size_t)p * nf + i] = Sl.synb[(size_t)s * nf + i];
     if (threadIdx.x == 0) {
       out_chi[p] = st[1];
-      out_iter[p] = Sl.iter[s];
+      out_iter[p] = Sl.iter[s] + (Sl.restarted[s] > 0 ? Sl.restarted[s] - 1 : 0);
       if (out_status) out_status[p] = st[1] < 1.0e29 ? 0 : FZ_NAN;
       atomicAdd(&q->done, 1);
       np_next = atomicAdd(&q->next, 1);
@@ -550,6 +571,7 @@ __global__ void __launch_bounds__(256) k_lm_compact(LMConf C, LMSlots A, LMSlots
     B.pix[d] = A.pix[s];
     B.iter[d] = A.iter[s];
     B.skip[d] = A.skip[s];
+    B.restarted[d] = A.restarted[s];
   }
   if (threadIdx.x < 5) B.st[5 * (size_t)d + threadIdx.x] = A.st[5 * (size_t)s + threadIdx.x];
   for (int i = threadIdx.x; i < nm; i += blockDim.x) {

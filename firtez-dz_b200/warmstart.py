@@ -152,12 +152,19 @@ class WarmStart:
         return np.concatenate(cols, axis=1)
 
     def expand(self, nodes_v, base):
-        """EXPAND_VECTOR of predicted nodes (n, nout) into copies of base."""
+        """Copies of base moved to the predicted node values (n, nout): each
+        free row becomes base + EXPAND_VECTOR(nodes - CONTRACT_VECTOR(base)),
+        the way the inversion itself perturbs a model.  Expanding the node
+        values directly would replace the row by a piecewise-linear curve
+        through node averages, which misses a steep stratification (T) by up
+        to a third of a node step at the ends even for exact nodes."""
         m = np.array(base, dtype=np.float32, copy=True)
+        cb = self.targets(m)
         j = 0
         for p, row in self.params:
             nj = self.nodes[p]
-            m[:, row] = (nodes_v[:, j:j + nj] @ self.coefs[p].T).astype(np.float32)
+            d = nodes_v[:, j:j + nj] - cb[:, j:j + nj]
+            m[:, row] = (m[:, row].astype(np.float64) + d @ self.coefs[p].T).astype(np.float32)
             j += nj
         return m
 
@@ -220,27 +227,37 @@ class WarmStart:
         if not hasattr(self, "_dev"):
             self._dev = (torch.from_numpy(self.tsd.astype(np.float32)).cuda(),
                          torch.from_numpy(self.tmu.astype(np.float32)).cuda(),
-                         {p: torch.from_numpy(self.coefs[p].T.astype(np.float32)).cuda() for p, _ in self.params})
-        tsd, tmu, ct = self._dev
+                         {p: torch.from_numpy(self.coefs[p].T.astype(np.float32)).cuda() for p, _ in self.params},
+                         {p: torch.from_numpy((self.coefs[p] / self.coefs[p].sum(axis=0)).astype(np.float32)).cuda()
+                          for p, _ in self.params})
+        tsd, tmu, ct, cavg = self._dev
         nodes_v = y * tsd + tmu
         m = base.clone()
         j = 0
         for p, row in self.params:
             nj = self.nodes[p]
-            m[:, row] = nodes_v[:, j:j + nj] @ ct[p]
+            # base + EXPAND(nodes - CONTRACT(base)), as expand()
+            m[:, row] = m[:, row] + (nodes_v[:, j:j + nj] - m[:, row] @ cavg[p]) @ ct[p]
             j += nj
         return m
 
-    def initial_models(self, obs, base=None):
+    def initial_models(self, obs, base=None, out=None):
         """Warm-start models for host observations obs (npix, 4, numw): the
         network and the node expansion run on the device; returns host
-        models (npix, 13, nz) float32 (base: host models whose other rows
-        are kept, default_models() if None)."""
+        models (npix, 13, nz) float32, in out if given (e.g. pinned memory)
+        (base: host models whose other rows are kept, default_models() if
+        None)."""
         import torch
         n = obs.shape[0]
-        x = torch.from_numpy(np.ascontiguousarray(obs, dtype=np.float32).reshape(n, -1)).cuda()
+        x = torch.from_numpy(np.ascontiguousarray(obs).reshape(n, -1)).cuda().float()
         if base is None:
             b = torch.from_numpy(default_models(1, self.nz)).cuda().expand(n, -1, -1)
         else:
             b = torch.from_numpy(np.ascontiguousarray(base, dtype=np.float32)).cuda()
-        return self.initial_models_device(x, b).cpu().numpy()
+        m = self.initial_models_device(x, b)
+        if out is None:
+            return m.cpu().numpy()
+        if out.shape != (n, 13, self.nz) or out.dtype != np.float32 or not out.flags.c_contiguous:
+            raise ValueError("out must be a contiguous float32 (npix, 13, nz) array")
+        torch.from_numpy(out).copy_(m)
+        return out

@@ -191,12 +191,20 @@ int fz_tune_set(fz_ctx* ctx, const fz_tune* t);
  * dchi2, an accepted step whose relative chi2 gain is below it ends the
  * pixel (0 = off); svdtol, the relative SVD cut (RSVDTOL, 1e-4); isigma, the
  * noise (NOISE, 4e-3); wstk, the Stokes weights (1,1,1,1); slots, the number
- * of pixels in flight (0 = 8192). */
+ * of pixels in flight (0 = the tuned count, 8192 untuned).  fallback and
+ * fallback_model (no counterpart in the reference): with a per-pixel chi2
+ * goal, a pixel whose search ends above fallback x its goal starts once more
+ * from fallback_model (device, one MODEL(NZ,13) for every pixel, e.g. the
+ * default guess) in the same slot pool, keeping the goal; its iterations
+ * add up.  0 / NULL: off.  fallback_model is a device pointer for
+ * fz_invert_device and a host pointer for fz_invert. */
 typedef struct {
   int maxsteps, maxit;
   double dchi2, svdtol, isigma;
   float wstk[4];
   int slots, pad;
+  double fallback;
+  const float* fallback_model;
 } fz_lm_opts;
 
 /* Batched pixel-wise Levenberg-Marquardt inversion of npix pixels with the

@@ -74,3 +74,52 @@ def test_batched_inversion_matches_oracle_outcome(fz, orc):
     syn, _, _ = orc.forward(lines, reg, g, best, hydrostatic=True)
     chk = np.sum((obs.reshape(npix, -1) - syn.reshape(npix, -1)) ** 2 * w, axis=1) / syn0.shape[1]
     assert np.allclose(chk, chi, rtol=1e-3), (chk, chi)
+
+
+def test_fallback_restart_reaches_the_plain_chi2(fz, orc):
+    """fz_lm_opts.fallback: a pixel whose search ends above fallback x its
+    chi2 goal restarts once from the fallback model in the same pool.  With
+    the default guess as the fallback model and the default-guess chi2 as the
+    goal, a restarted pixel retraces that run, so no pixel ends above
+    1.1x its goal; the iterations of both attempts add up."""
+    import torch
+    from firtez_dz_b200 import warmstart as ws
+    nz, npix = 48, 64
+    lines, reg, g, ctx = _ctx(fz, orc, nz)
+    true = fz.atmos.make_columns(npix, nz, seed=33)
+    obs, true_he, _ = ctx.forward(true, hydrostatic=True)
+    obs = obs + np.random.default_rng(4).normal(0.0, 1e-3, obs.shape)
+    ctx.rf_nodes(lmcase.NODES)
+    base = ws.default_models(npix, nz)
+    opts = fz.LMOpts(maxsteps=5, maxit=30, isigma=1e-3, dchi2=1e-3, slots=24)
+    _, chi_pl, it_pl, st_pl = ctx.invert(obs, base, hydrostatic=True, opts=opts)
+    bad = lmcase.initial_guess(true_he, seed=2)
+    bad[:, 0] += 600.0                               # a poor start: many pixels stop above the goal
+    _, chi_raw, it_raw, _ = ctx.invert(obs, bad, hydrostatic=True, opts=opts, target=chi_pl)
+    fb = torch.from_numpy(np.ascontiguousarray(base[0])).cuda()
+    fopts = fz.LMOpts(maxsteps=5, maxit=30, isigma=1e-3, dchi2=1e-3, slots=24, fallback=1.1,
+                      fallback_model=fb.data_ptr())
+    d_obs = torch.from_numpy(np.ascontiguousarray(obs)).cuda()
+    d_bad = torch.from_numpy(bad).cuda()
+    out = torch.empty_like(d_bad)
+    chi = torch.empty(npix, dtype=torch.float64, device="cuda")
+    it = torch.empty(npix, dtype=torch.int32, device="cuda")
+    st = torch.empty(npix, dtype=torch.int32, device="cuda")
+    tgt = torch.from_numpy(chi_pl).cuda()
+    ctx.invert_device(npix, d_obs.data_ptr(), d_bad.data_ptr(), out.data_ptr(), chi.data_ptr(), it.data_ptr(),
+                      st.data_ptr(), opts=fopts, target_ptr=tgt.data_ptr())
+    torch.cuda.synchronize()
+    chi_fb, it_fb = chi.cpu().numpy(), it.cpu().numpy()
+    assert np.all(st.cpu().numpy() == 0) and np.all(st_pl == 0)
+    restarted = chi_raw > 1.1 * chi_pl
+    assert restarted.any()
+    assert np.all(chi_fb <= 1.1 * chi_pl)
+    np.testing.assert_array_equal(chi_fb[~restarted], chi_raw[~restarted])
+    assert np.all(it_fb[restarted] > it_raw[restarted])
+    # the host-buffer call takes the fallback model from host memory
+    hfb = np.ascontiguousarray(base[0])
+    hopts = fz.LMOpts(maxsteps=5, maxit=30, isigma=1e-3, dchi2=1e-3, slots=24, fallback=1.1,
+                      fallback_model=hfb.ctypes.data)
+    _, chi_h, it_h, _ = ctx.invert(obs, bad, hydrostatic=True, opts=hopts, target=chi_pl)
+    np.testing.assert_array_equal(chi_h, chi_fb)
+    np.testing.assert_array_equal(it_h, it_fb)
