@@ -78,7 +78,8 @@ class Tune(ctypes.Structure):
     """fz_tune: launch shapes chosen by the autotuner (and their timings)."""
     _fields_ = [("chain_warps", ctypes.c_int), ("chemder_blocks_per_sm", ctypes.c_int),
                 ("opac_rf_threads", ctypes.c_int), ("lm_slots", ctypes.c_int), ("chain_ms", ctypes.c_float),
-                ("chemder_ms", ctypes.c_float), ("opac_rf_ms", ctypes.c_float), ("lm_pixels_per_s", ctypes.c_float)]
+                ("chemder_ms", ctypes.c_float), ("opac_rf_ms", ctypes.c_float), ("lm_pixels_per_s", ctypes.c_float),
+                ("chain_lanes", ctypes.c_int), ("pad", ctypes.c_int)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
@@ -342,7 +343,7 @@ class Synthesis:
                 setattr(t, k, int(v))
             _check(lib().fz_tune_set(self._h, ctypes.byref(t)))
         d = t.as_dict()
-        return {k: d[k] for k in ("chain_warps", "chemder_blocks_per_sm", "opac_rf_threads", "lm_slots")}
+        return {k: d[k] for k in ("chain_warps", "chain_lanes", "chemder_blocks_per_sm", "opac_rf_threads", "lm_slots")}
 
     def invert(self, obs, init, hydrostatic=True, opts=None, want_syn=False, target=None, out=None):
         """Batched LM inversion of host-resident pixels with the node layout of

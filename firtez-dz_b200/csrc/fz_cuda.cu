@@ -85,29 +85,34 @@ __device__ __forceinline__ void copy_to_shared(T* dst, const T* src) {
 // (RK4_INTEGRATION_LOG, src/hydrostatic_tools.f90:150-222, RK4_LOG :350-396).
 // Writes per height (nH, ne) as FORWARD1D uses them, and rho, Pe, mu (and
 // Pg) into the output model.
-template <bool HE>
+//
+// L lanes per column: 32 (a warp) or 16 (two columns per warp: each lane
+// holds six elements, and every per-column scalar of the chain costs half
+// the warp instructions).
+template <bool HE, int L>
 __global__ void __launch_bounds__(128) k_chain(const Consts* __restrict__ Kg, const PFTable* __restrict__ tb, int ncol,
                                                int nz, const float* model, float* mout, double2* __restrict__ chem,
                                                int* __restrict__ status) {
+  constexpr int NS = WarpSahaT<L>::NS;
   __shared__ Consts K;
   copy_to_shared(&K, Kg);
   __syncthreads();
-  const int lane = threadIdx.x & 31;
-  const int col = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  const int lane = threadIdx.x & (L - 1);
+  const int col = (int)((blockIdx.x * (size_t)blockDim.x + threadIdx.x) / L);
   if (col >= ncol) return;
   const float* m = model + (size_t)col * 13 * nz;
   float* mo = mout + (size_t)col * 13 * nz;
   double2* ch = chem + (size_t)col * nz;
   if (mo != m)
-    for (int i = lane; i < 13 * nz; i += 32) mo[i] = m[i];
-  __syncwarp();
-  double ab[3];
+    for (int i = lane; i < 13 * nz; i += L) mo[i] = m[i];
+  __syncwarp(group_mask<L>());
+  double ab[NS];
 #pragma unroll
-  for (int j = 0; j < 3; ++j) ab[j] = K.lane_elem[32 * j + lane] >= 0 ? K.ab10[K.lane_elem[32 * j + lane]] : 0.0;
+  for (int j = 0; j < NS; ++j) ab[j] = K.lane_elem[L * j + lane] >= 0 ? K.ab10[K.lane_elem[L * j + lane]] : 0.0;
   int st = 0;
   if (!HE) {
     double nelec = 0.0;
-    WarpSaha w;
+    WarpSahaT<L> w;
     for (int k = 0; k < nz; ++k) {
       saha_prepare(w, (double)mget(m, nz, 0, k), K, tb, lane);
       const RhoOut r = get_rho_warp(w, ab, (double)mget(m, nz, 1, k), nelec, K, lane);
@@ -127,7 +132,7 @@ __global__ void __launch_bounds__(128) k_chain(const Consts* __restrict__ Kg, co
     // One Saha buffer serves the whole integration: within a step the RK4
     // stages need T(k+1) (stage 1), the linear midpoint (stages 2, 3) and
     // T(k) (stage 4 and the final GET_RHO), and T(k) is the next step's T(k+1).
-    WarpSaha w;
+    WarpSahaT<L> w;
     saha_prepare(w, (double)mget(m, nz, 0, top), K, tb, lane);
     {
       const RhoOut r = get_rho_warp(w, ab, exp(u0), nelec, K, lane);
@@ -1222,7 +1227,8 @@ struct fz_ctx {
   PFTable* d_pf = nullptr;
   PFDTable* d_pfd = nullptr;
   struct {
-    int chain_warps = 4;       // k_chain warps (columns) per block
+    int chain_warps = 4;       // k_chain warps per block
+    int chain_lanes = 0;       // k_chain lanes per column: 32, 16, or 0 = by column count
     int chemder_bpsm = 32;     // k_chemder resident-block cap per SM (0 = one block per 4 cells)
     int opacrf_threads = 256;  // k_opac_rf block size
     int lm_slots = 8192;       // pixels in flight when fz_lm_opts.slots == 0
@@ -1258,6 +1264,7 @@ struct fz_ctx {
     cudaEvent_t a, b;
   };
   std::vector<Pending> pending;
+  std::vector<cudaEvent_t> ev_pool;   // resolved events, reused by later scopes
   double prof_ms[NKERN] = {};
   int prof_n[NKERN] = {};
   long long prof_items[NKERN] = {};
@@ -1318,9 +1325,19 @@ struct ProfScope {
   ProfScope(fz_ctx* c_, int k, cudaStream_t s_, long long items = 0) : c(c_), kernel(k), s(s_) {
     if (!c->prof) return;
     c->prof_items[k] += items;
-    cudaEventCreate(&a);
-    cudaEventCreate(&b);
+    a = take();
+    b = take();
     cudaEventRecord(a, s);
+  }
+  cudaEvent_t take() {
+    if (c->ev_pool.empty()) {
+      cudaEvent_t e = nullptr;
+      cudaEventCreate(&e);
+      return e;
+    }
+    cudaEvent_t e = c->ev_pool.back();
+    c->ev_pool.pop_back();
+    return e;
   }
   ~ProfScope() {
     if (!c->prof) return;
@@ -1329,19 +1346,40 @@ struct ProfScope {
   }
 };
 
+// k_chain with wpb warps per block and lanes (32 or 16) lanes per column;
+// lanes = 0 picks 16 when the batch fills 8 warps per SM with two columns a
+// warp (throughput: half the warp instructions per column) and 32 below
+// (latency: every column's chain gets a warp of its own).
+void launch_k_chain(fz_ctx* c, int ncol, const float* d_model, float* d_mout, int* d_status, int hydrostatic, int wpb,
+                    int lanes, cudaStream_t s) {
+  if (lanes != 16 && lanes != 32) lanes = ncol >= 16 * c->nsm ? 16 : 32;
+  const size_t threads = (size_t)ncol * lanes;
+  const dim3 gc((unsigned)((threads + wpb * 32 - 1) / (wpb * 32)));
+  if (lanes == 16) {
+    if (hydrostatic)
+      k_chain<true, 16><<<gc, wpb * 32, 0, s>>>(c->d_consts, c->d_pf, ncol, c->nz, d_model, d_mout, c->d_chem,
+                                                d_status);
+    else
+      k_chain<false, 16><<<gc, wpb * 32, 0, s>>>(c->d_consts, c->d_pf, ncol, c->nz, d_model, d_mout, c->d_chem,
+                                                 d_status);
+  } else {
+    if (hydrostatic)
+      k_chain<true, 32><<<gc, wpb * 32, 0, s>>>(c->d_consts, c->d_pf, ncol, c->nz, d_model, d_mout, c->d_chem,
+                                                d_status);
+    else
+      k_chain<false, 32><<<gc, wpb * 32, 0, s>>>(c->d_consts, c->d_pf, ncol, c->nz, d_model, d_mout, c->d_chem,
+                                                 d_status);
+  }
+}
+
 int launch_forward(fz_ctx* c, int ncol, const float* d_model, int hydrostatic, double* d_syn, float* d_mout,
                    int* d_status, cudaStream_t s) {
   int rc = ensure_scratch(c, ncol);
   if (rc) return rc;
   if (d_status) FZ_CK(cudaMemsetAsync(d_status, 0, ncol * sizeof(int), s));
-  const int wpb = c->tune.chain_warps;
-  const dim3 gc((ncol + wpb - 1) / wpb);
   {
     ProfScope ps(c, 0, s, ncol);
-    if (hydrostatic)
-      k_chain<true><<<gc, wpb * 32, 0, s>>>(c->d_consts, c->d_pf, ncol, c->nz, d_model, d_mout, c->d_chem, d_status);
-    else
-      k_chain<false><<<gc, wpb * 32, 0, s>>>(c->d_consts, c->d_pf, ncol, c->nz, d_model, d_mout, c->d_chem, d_status);
+    launch_k_chain(c, ncol, d_model, d_mout, d_status, hydrostatic, c->tune.chain_warps, c->tune.chain_lanes, s);
   }
   FZ_CK(cudaGetLastError());
   {
@@ -1387,12 +1425,8 @@ int ensure_rf_scratch(fz_ctx* c, int ncol) {
 // The chemistry and opacity-derivative launches of the RF path with an
 // explicit launch shape (the autotuner's candidates; c->tune otherwise).
 void launch_chain(fz_ctx* c, int ncol, const float* d_model, float* d_mout, int* d_status, int hydrostatic, int wpb,
-                  cudaStream_t s) {
-  const dim3 gc((ncol + wpb - 1) / wpb);
-  if (hydrostatic)
-    k_chain<true><<<gc, wpb * 32, 0, s>>>(c->d_consts, c->d_pf, ncol, c->nz, d_model, d_mout, c->d_chem, d_status);
-  else
-    k_chain<false><<<gc, wpb * 32, 0, s>>>(c->d_consts, c->d_pf, ncol, c->nz, d_model, d_mout, c->d_chem, d_status);
+                  cudaStream_t s, int lanes = -1) {
+  launch_k_chain(c, ncol, d_model, d_mout, d_status, hydrostatic, wpb, lanes >= 0 ? lanes : c->tune.chain_lanes, s);
 }
 
 // list / nlist (device): only the columns list[0 .. *nlist) of the first ncol
@@ -1869,6 +1903,11 @@ int fz_destroy(fz_ctx* c) {
   cudaFree(c->d_pf);
   cudaFree(c->d_pfd);
   cudaFree(c->d_oscr);
+  for (cudaEvent_t e : c->ev_pool) cudaEventDestroy(e);
+  for (auto& p : c->pending) {
+    cudaEventDestroy(p.a);
+    cudaEventDestroy(p.b);
+  }
   for (void* p : {(void*)c->inv.obs, (void*)c->inv.chi, (void*)c->inv.syn, (void*)c->inv.tgt, (void*)c->inv.init,
                   (void*)c->inv.out, (void*)c->inv.it, (void*)c->inv.st, (void*)c->inv.fb})
     cudaFree(p);
@@ -1912,8 +1951,8 @@ int fz_profile_read(fz_ctx* c, double* ms, int* launches, long long* items, int 
       c->prof_ms[p.kernel] += t;
       c->prof_n[p.kernel] += 1;
     }
-    cudaEventDestroy(p.a);
-    cudaEventDestroy(p.b);
+    c->ev_pool.push_back(p.a);
+    c->ev_pool.push_back(p.b);
   }
   c->pending.clear();
   for (int i = 0; i < n && i < NKERN; ++i) {
@@ -2367,15 +2406,19 @@ int fz_autotune_forward(fz_ctx* c, int ncol, const float* d_model, int hydrostat
     return 0;
   };
   float best = 0.0f, ms = 0.0f, tchain = 0.0f, tchem = 0.0f, topac = 0.0f;
-  int bw = c->tune.chain_warps;
+  int bw = c->tune.chain_warps, bl = c->tune.chain_lanes;
+  // lanes per column stay automatic (by batch size: the inversion's batches
+  // shrink from the full pool to a few columns, so one fixed value measured
+  // on this batch would not fit them)
   static const int kWarps[] = {1, 2, 4};
+  static const int kLanes[] = {0};
   for (int i = 0; i < 3; ++i) {
-    const int w = kWarps[i];
-    if ((rc = timed([&] { launch_chain(c, ncol, d_model, d_mout, nullptr, hydrostatic, w, s); }, ms))) return rc;
-    if (i == 0 || ms < best) best = ms, bw = w;
+    const int w = kWarps[i % 3], l = kLanes[i / 3];
+    if ((rc = timed([&] { launch_chain(c, ncol, d_model, d_mout, nullptr, hydrostatic, w, s, l); }, ms))) return rc;
+    if (i == 0 || ms < best) best = ms, bw = w, bl = l;
   }
   tchain = best;
-  launch_chain(c, ncol, d_model, d_mout, nullptr, hydrostatic, bw, s);
+  launch_chain(c, ncol, d_model, d_mout, nullptr, hydrostatic, bw, s, bl);
   int bb = c->tune.chemder_bpsm;
   static const int kBpsm[] = {8, 16, 32, 64, 0};
   for (int i = 0; i < 5; ++i) {
@@ -2393,10 +2436,12 @@ int fz_autotune_forward(fz_ctx* c, int ncol, const float* d_model, int hydrostat
   }
   topac = best;
   c->tune.chain_warps = bw;
+  c->tune.chain_lanes = bl;
   c->tune.chemder_bpsm = bb;
   c->tune.opacrf_threads = bt;
   if (out) {
     out->chain_warps = bw;
+    out->chain_lanes = bl;
     out->chemder_blocks_per_sm = bb;
     out->opac_rf_threads = bt;
     out->lm_slots = c->tune.lm_slots;
@@ -2465,6 +2510,7 @@ int fz_autotune_lm(fz_ctx* c, int npix, const double* d_obs, const float* d_init
 int fz_tune_get(fz_ctx* c, fz_tune* t) {
   if (!c || !t) return FZ_ERR_ARG;
   t->chain_warps = c->tune.chain_warps;
+  t->chain_lanes = c->tune.chain_lanes;
   t->chemder_blocks_per_sm = c->tune.chemder_bpsm;
   t->opac_rf_threads = c->tune.opacrf_threads;
   t->lm_slots = c->tune.lm_slots;
@@ -2473,10 +2519,12 @@ int fz_tune_get(fz_ctx* c, fz_tune* t) {
 
 int fz_tune_set(fz_ctx* c, const fz_tune* t) {
   if (!c || !t) return FZ_ERR_ARG;
-  if (t->chain_warps < 1 || t->chain_warps > 4 || t->chemder_blocks_per_sm < 0 || t->lm_slots < 1 ||
+  if (t->chain_warps < 1 || t->chain_warps > 4 || (t->chain_lanes != 0 && t->chain_lanes != 32 && t->chain_lanes != 16) ||
+      t->chemder_blocks_per_sm < 0 || t->lm_slots < 1 ||
       (t->opac_rf_threads != 64 && t->opac_rf_threads != 128 && t->opac_rf_threads != 256))
     return FZ_ERR_ARG;
   c->tune.chain_warps = t->chain_warps;
+  c->tune.chain_lanes = t->chain_lanes;
   c->tune.chemder_bpsm = t->chemder_blocks_per_sm;
   c->tune.opacrf_threads = t->opac_rf_threads;
   c->tune.lm_slots = t->lm_slots;
@@ -2544,9 +2592,10 @@ int fz_forward_device_static(fz_ctx* c, int ncol, const float* d_model, int hydr
   const int wpb = 4;
   const dim3 gc((ncol + wpb - 1) / wpb);
   if (hydrostatic)
-    k_chain<true><<<gc, wpb * 32, 0, s>>>(c->d_consts, c->d_pf, ncol, c->nz, d_model, d_model_out, chem, d_status);
+    k_chain<true, 32><<<gc, wpb * 32, 0, s>>>(c->d_consts, c->d_pf, ncol, c->nz, d_model, d_model_out, chem, d_status);
   else
-    k_chain<false><<<gc, wpb * 32, 0, s>>>(c->d_consts, c->d_pf, ncol, c->nz, d_model, d_model_out, chem, d_status);
+    k_chain<false, 32><<<gc, wpb * 32, 0, s>>>(c->d_consts, c->d_pf, ncol, c->nz, d_model, d_model_out, chem,
+                                               d_status);
   FZ_CK(cudaGetLastError());
   const size_t total = (size_t)ncol * c->nz;
   const int blocks = (int)std::min<size_t>((total + 255) / 256, (size_t)c->nsm * 16);

@@ -123,12 +123,18 @@ __device__ __forceinline__ double rcp_d(double y) {
 }
 
 // --------------------------------------------------------- warp chemistry
-// Per-lane Saha factors of elements lane, lane+32, lane+64 at temperature T
-// (SHORT_PRE_ION_CALC_TEMPRHO, src/chemical_equilibrium.f90:1601-1652).
-struct WarpSaha {
+// One column's chemistry on a group of L lanes (L = 32: a warp; L = 16: a
+// half-warp, two columns per warp), lanes over the elements: the element of
+// lane l in slot j is lane_elem[L*j + l], NS = 96 / L slots per lane.  The
+// exponential-form elements come first in lane_elem, so only the first
+// 23 / L + 1 slots evaluate an exponential.
+template <int L>
+struct WarpSahaT {
+  static constexpr int NS = 96 / L;
   double T;
-  double a1[3], a2[3];
+  double a1[NS], a2[NS];
 };
+using WarpSaha = WarpSahaT<32>;
 
 __device__ __forceinline__ double clamp650(double e) {
   if (e > 0.0) e = fmin(e, 650.0);
@@ -136,19 +142,23 @@ __device__ __forceinline__ double clamp650(double e) {
   return e;
 }
 
-__device__ __forceinline__ void saha_prepare(WarpSaha& w, double T, const Consts& K, const PFTable* __restrict__ tb,
-                                         int lane) {
-  // SHORT_PRE_ION_CALC_TEMPRHO, src/chemical_equilibrium.f90:1601-1652
+// Per-lane Saha factors of the lane's elements at temperature T
+// (SHORT_PRE_ION_CALC_TEMPRHO, src/chemical_equilibrium.f90:1601-1652).
+template <int L>
+__device__ __forceinline__ void saha_prepare(WarpSahaT<L>& w, double T, const Consts& K,
+                                             const PFTable* __restrict__ tb, int lane) {
+  constexpr int NS = WarpSahaT<L>::NS;
+  constexpr int NEXP = 23 / L + 1;   // slots holding the 23 exponential-form elements
   w.T = T;
   const double lamelec = K.csaha1 * pow(T, -3.0 / 2.0);
   const double var[3] = {T, 1.0e-3 * T, log(5040.0 / T)};
   const double it = rcp_d(T);
 #pragma unroll
-  for (int j = 0; j < 3; ++j) {
-    const int el = K.lane_elem[32 * j + lane];
+  for (int j = 0; j < NS; ++j) {
+    const int el = K.lane_elem[L * j + lane];
     const int e = el < 0 ? 0 : el;
     double u0, u1, u2;
-    if (j == 0) {
+    if (j < NEXP) {
       u0 = pf_stage<true>(tb, e, 0, T, var);
       u1 = pf_stage<true>(tb, e, 1, T, var);
       u2 = pf_stage<true>(tb, e, 2, T, var);
@@ -170,21 +180,39 @@ __device__ __forceinline__ double warp_sum(double v) {
   return v;   // xor butterfly: bit-identical in every lane
 }
 
+// Sum over the L lanes of a group (xor butterfly within the group; mask:
+// the group's lanes).
+template <int L>
+__device__ __forceinline__ double group_sum(double v, unsigned mask) {
+#pragma unroll
+  for (int o = L / 2; o > 0; o >>= 1) v += __shfl_xor_sync(mask, v, o);
+  return v;
+}
+
+// The lanes of this thread's group of L.
+template <int L>
+__device__ __forceinline__ unsigned group_mask() {
+  return L == 32 ? 0xffffffffu : (((1u << L) - 1u) << (threadIdx.x & 31 & ~(L - 1)));
+}
+
 struct RhoOut {
   double nhyd, pelec, dens, molecw;
   int status;
 };
 
-// GET_RHO, src/chemical_equilibrium.f90:165-278.  All lanes of the warp call
-// it with the same arguments; nelec (the warm-start chain) is updated in
+// GET_RHO, src/chemical_equilibrium.f90:165-278.  All lanes of the group
+// call it with the same arguments; nelec (the warm-start chain) is updated in
 // every lane identically.  The electron sum of SHORT_ION_CALC_TEMPRHO
 // (:1659-1701), NELEC_EST = N_H+ - N_H- + sum_{Z>1} (N_II + N_III), is
 // evaluated per element as ab*(1+y)/(1+y+xy) (hydrogen: ab*(1-xy)/(1+y+xy))
 // with x = ne*alpha_I, y = ne*alpha_II: algebraically the reference's three
 // quotients, one division instead of five.  ab[j] = 10**(ABUND-12) of the
 // lane's elements (0 past element 92).
-__device__ __forceinline__ RhoOut get_rho_warp(const WarpSaha& w, const double ab[3], double PG, double& nelec,
-                                            const Consts& K, int lane) {
+template <int L>
+__device__ __forceinline__ RhoOut get_rho_warp(const WarpSahaT<L>& w, const double ab[WarpSahaT<L>::NS], double PG,
+                                               double& nelec, const Consts& K, int lane) {
+  constexpr int NS = WarpSahaT<L>::NS;
+  const unsigned mask = group_mask<L>();
   RhoOut r;
   const double T = w.T;
   double nhyd = 0.0;
@@ -202,13 +230,13 @@ __device__ __forceinline__ RhoOut get_rho_warp(const WarpSaha& w, const double a
     const double ne = nnew;
     double s = 0.0;
 #pragma unroll
-    for (int j = 0; j < 3; ++j) {
+    for (int j = 0; j < NS; ++j) {
       const double x = ne * w.a1[j], y = ne * w.a2[j];
       const double xy = x * y;
-      const double num = (K.lane_elem[32 * j + lane] == 0) ? (1.0 - xy) : (1.0 + y);   // hydrogen: N_H+ - N_H-
+      const double num = (K.lane_elem[L * j + lane] == 0) ? (1.0 - xy) : (1.0 + y);   // hydrogen: N_H+ - N_H-
       s = fma(ab[j] * num, rcp_d(1.0 + y + xy), s);
     }
-    s = warp_sum(s);
+    s = group_sum<L>(s, mask);
     const double est = nhyd * s;
     nnew = (fmax(est, 0.0) + nold) * 0.5;
     iter = iter + 1;

@@ -165,8 +165,12 @@ int fz_forward_rf_full_device(fz_ctx* ctx, int ncol, const float* d_model, int h
 
 /* Launch-shape autotuner (no counterpart in the reference).  The shapes
  * live in the context and apply to every later call on it:
- *   chain_warps            columns (warps) per block of the chemistry chain
- *                          kernel, 1..4
+ *   chain_warps            warps per block of the chemistry chain kernel,
+ *                          1..4
+ *   chain_lanes            lanes per column of the chemistry chain kernel:
+ *                          32 (one column per warp), 16 (two), or 0 (16
+ *                          for batches of at least 16 columns per SM, else
+ *                          32; the default)
  *   chemder_blocks_per_sm  grid cap of the chemistry-derivative kernel per
  *                          SM (0 = one block per 4 heights)
  *   opac_rf_threads        block size of the opacity-derivative kernel
@@ -180,6 +184,7 @@ int fz_forward_rf_full_device(fz_ctx* ctx, int ncol, const float* d_model, int h
 typedef struct {
   int chain_warps, chemder_blocks_per_sm, opac_rf_threads, lm_slots;
   float chain_ms, chemder_ms, opac_rf_ms, lm_pixels_per_s;
+  int chain_lanes, pad;
 } fz_tune;
 int fz_autotune_forward(fz_ctx* ctx, int ncol, const float* d_model, int hydrostatic, fz_tune* out);
 int fz_tune_get(fz_ctx* ctx, fz_tune* out);

@@ -40,13 +40,17 @@ def test_gain_matches_oracle(fz, orc, workload):
     assert np.all(g_gpu[:, 3] == -g_gpu[:, 0])
 
 
+@pytest.mark.parametrize("lanes", [32, 16])
 @pytest.mark.parametrize("hydrostatic", [False, True])
-def test_synthesis_matches_oracle(fz, orc, workload, hydrostatic):
+def test_synthesis_matches_oracle(fz, orc, workload, hydrostatic, lanes):
+    """lanes: lanes per column of the chemistry chain kernel (a launch shape
+    the autotuner may pick)."""
     lines, reg = workload
     nz, ncol = 96, 64
     m = fz.atmos.make_columns(ncol, nz, seed=11)
     g, _ = orc.gain(lines, reg)
     ctx = fz.Synthesis(lines, reg, nz=nz, gain=g)
+    ctx.tune(chain_lanes=lanes)
     syn, mo, st = ctx.forward(m, hydrostatic=hydrostatic)
     ref, mref, sref = orc.forward(lines, reg, g, m, hydrostatic=hydrostatic)
     assert np.all(st == 0) and np.all(sref == 0)
