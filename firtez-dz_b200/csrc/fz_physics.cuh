@@ -53,13 +53,16 @@ __device__ __forceinline__ bool pf_cond(int cond, double th, double T, double u)
          (cond == 4 && T >= th) || (cond == 5 && u != th);
 }
 
+// Horner with fused multiply-adds (the FP64 chemistry kernels evaluate the
+// pieces millions of times; the unfused form of horner_exact is kept for the
+// per-line opacities, which follow the reference's rounding step by step).
 __device__ __forceinline__ double horner6(const double* c, double x) {
   double r = c[5];
-  r = __dadd_rn(c[4], __dmul_rn(x, r));
-  r = __dadd_rn(c[3], __dmul_rn(x, r));
-  r = __dadd_rn(c[2], __dmul_rn(x, r));
-  r = __dadd_rn(c[1], __dmul_rn(x, r));
-  r = __dadd_rn(c[0], __dmul_rn(x, r));
+  r = fma(x, r, c[4]);
+  r = fma(x, r, c[3]);
+  r = fma(x, r, c[2]);
+  r = fma(x, r, c[1]);
+  r = fma(x, r, c[0]);
   return r;
 }
 
@@ -150,9 +153,9 @@ __device__ __forceinline__ void saha_prepare(WarpSahaT<L>& w, double T, const Co
   constexpr int NS = WarpSahaT<L>::NS;
   constexpr int NEXP = 23 / L + 1;   // slots holding the 23 exponential-form elements
   w.T = T;
-  const double lamelec = K.csaha1 * pow(T, -3.0 / 2.0);
-  const double var[3] = {T, 1.0e-3 * T, log(5040.0 / T)};
   const double it = rcp_d(T);
+  const double lamelec = K.csaha1 * (it * sqrt(it));   // T^(-3/2)
+  const double var[3] = {T, 1.0e-3 * T, log(5040.0 / T)};
 #pragma unroll
   for (int j = 0; j < NS; ++j) {
     const int el = K.lane_elem[L * j + lane];

@@ -73,8 +73,8 @@ __device__ __forceinline__ double sel3(const double v[3], int i) { return i == 0
 // lanes on different elements: every value piece is evaluated once (the
 // derivative pieces' conditions and factors refer to them), the active value
 // and derivative pieces are selected by predication, and only the active
-// derivative piece is evaluated.  Same pieces, same Horner order and the same
-// rounded -1/T as partition_udu, so the results agree bit for bit.
+// derivative piece is evaluated.  Same pieces, Horner order and rounded -1/T
+// as partition_udu; the Horner steps are fused (last-bit differences).
 __device__ __forceinline__ void pf_stage_udu(const PFTable* __restrict__ tb, const PFDTable* __restrict__ td, int e,
                                              int s, double T, double it, const double var[3], double& U,
                                              double& dU) {
@@ -151,7 +151,7 @@ __device__ __forceinline__ ChemDer chem_der_warp(double T, double P, double NE, 
   const double ideno = 1.0 / K.deno_sa;
   const double nh = (P - NE * KBOL * T) * (it / KBOL) * ideno;
   const double var[3] = {T, 1.0e-3 * T, log(5040.0 / T)};
-  const double lamelec = K.csaha1 * pow(T, -3.0 / 2.0);
+  const double lamelec = K.csaha1 * (it * sqrt(it));   // T^(-3/2)
   const double dlam = -1.5 * it;
   const double it2 = it * it;
   const double ine = 1.0 / NE;
