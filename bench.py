@@ -149,7 +149,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--field", type=int, default=512, help="field side (pixels)")
-    ap.add_argument("--tile", type=int, default=65536, help="pixels per step")
+    ap.add_argument("--tile", type=int, default=131072, help="pixels per step")
     ap.add_argument("--slots", type=int, default=8192)
     ap.add_argument("--nz", type=int, default=128)
     ap.add_argument("--train-pairs", type=int, default=2097152)
