@@ -1,0 +1,70 @@
+"""The bench's multi-GPU plumbing on CPU: two gloo ranks.
+
+bench.py --gpus N runs one process per GPU, each inverting a field of its
+own (weak scaling); the ranks share only a barrier and the maximum over ranks
+of each measured time.  Here two processes on the gloo backend check that
+the maximum reaches both ranks, that the barrier and the teardown work, that
+the ranks' fields are seeded differently, and that the reference arm's
+non-zero ranks exit at once without output.
+"""
+import importlib.util
+import json
+import os
+import socket
+import subprocess
+import sys
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def _bench():
+    spec = importlib.util.spec_from_file_location("fz_bench", os.path.join(ROOT, "bench.py"))
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def _free_port():
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        return s.getsockname()[1]
+
+
+def _rank_main(rank, world, port, outdir):
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port), RANK=str(rank), WORLD_SIZE=str(world))
+    bench = _bench()
+    r = bench.Ranks(world, backend="gloo", device="cpu", timeout_s=60)
+    r.barrier()
+    got = r.maxms(10.0 + 5.0 * rank)
+    r.barrier()
+    r.close()
+    with open(os.path.join(outdir, "rank%d.json" % rank), "w") as f:
+        json.dump({"max": got, "seed": bench.field_seed(rank, 0)}, f)
+
+
+def test_two_gloo_ranks_share_the_max_time(tmp_path):
+    import torch.multiprocessing as mp
+    world = 2
+    mp.spawn(_rank_main, args=(world, _free_port(), str(tmp_path)), nprocs=world, join=True)
+    res = [json.load(open(os.path.join(tmp_path, "rank%d.json" % r))) for r in range(world)]
+    assert all(x["max"] == 15.0 for x in res)
+    assert len({x["seed"] for x in res}) == world
+
+
+def test_single_rank_needs_no_process_group():
+    bench = _bench()
+    r = bench.Ranks(1)
+    r.barrier()
+    assert r.maxms(3.5) == 3.5
+    r.close()
+
+
+@pytest.mark.timeout(300)
+def test_reference_arm_other_ranks_exit_without_work():
+    env = dict(os.environ, RANK="1", WORLD_SIZE="2", LOCAL_RANK="1", MASTER_ADDR="127.0.0.1")
+    p = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference", "--gpus", "2",
+                        "--steps", "1", "--warmup", "0"], env=env, capture_output=True, text=True, timeout=280)
+    assert p.returncode == 0, p.stderr[-2000:]
+    assert p.stdout.strip() == ""
