@@ -1757,12 +1757,14 @@ int fz_create(fz_ctx** out, const fz_line* lines, int nlines, const fz_region* r
         return n < 0 ? FZ_ERR_ARG : FZ_ERR_LIMIT;
       }
       P.lu_c0[nlu] = ncomp;
-      P.lu_nc[nlu] = n;
       int at = ncomp;
-      for (int t = -1; t <= 1; ++t) {   // group by type (ZEEMAN_COMP order kept within a type)
+      // group by type (ZEEMAN_COMP order kept within a type); components of
+      // zero strength (the M = 0 -> 0 pi component of a Delta J = 0 line) add
+      // exactly nothing to any sum and are left out
+      for (int t = -1; t <= 1; ++t) {
         P.lu_nt[nlu][t + 1] = 0;
         for (int i = 0; i < n; ++i)
-          if (ty[i] == t) {
+          if (ty[i] == t && stg[i] != 0.0) {
             P.comp_shift[at] = (float)sh[i];
             P.comp_str[at] = (float)stg[i];
             P.comp_type[at] = t;
@@ -1770,7 +1772,8 @@ int fz_create(fz_ctx** out, const fz_line* lines, int nlines, const fz_region* r
             ++P.lu_nt[nlu][t + 1];
           }
       }
-      ncomp += n;
+      P.lu_nc[nlu] = at - ncomp;
+      ncomp = at;
       ++nlu;
     }
     for (int j = 0; j < R.numwave; ++j) {
