@@ -63,15 +63,21 @@ class LMOpts(ctypes.Structure):
     _fields_ = [("maxsteps", ctypes.c_int), ("maxit", ctypes.c_int), ("dchi2", ctypes.c_double),
                 ("svdtol", ctypes.c_double), ("isigma", ctypes.c_double), ("wstk", ctypes.c_float * 4),
                 ("slots", ctypes.c_int), ("pad", ctypes.c_int), ("fallback", ctypes.c_double),
-                ("fallback_model", ctypes.c_void_p)]
+                ("fallback_model", ctypes.c_void_p), ("reg_type", ctypes.c_int * 8), ("reg_alpha", ctypes.c_double * 8)]
 
     def __init__(self, maxsteps=5, maxit=40, dchi2=0.0, svdtol=1e-4, isigma=4e-3, wstk=(1, 1, 1, 1), slots=0,
-                 fallback=0.0, fallback_model=0):
+                 fallback=0.0, fallback_model=0, reg=None):
         """fallback_model: device pointer of one MODEL(NZ,13) float32 (e.g. a
         torch tensor's data_ptr()) that pixels ending above fallback x their
-        chi2 goal restart from."""
+        chi2 goal restart from (a host pointer for invert()).  reg: optional
+        {reference parameter: (type, alpha)} vertical regularisation
+        (VERTICAL REGULARIZATION: type 0 or 1, PEN_ALP)."""
+        typ, alp = [0] * 8, [0.0] * 8
+        for p, (t, a) in (reg or {}).items():
+            typ[int(p) - 1], alp[int(p) - 1] = int(t), float(a)
         super().__init__(maxsteps, maxit, dchi2, svdtol, isigma, (ctypes.c_float * 4)(*wstk), slots, 0,
-                         float(fallback), fallback_model or None)
+                         float(fallback), fallback_model or None, (ctypes.c_int * 8)(*typ),
+                         (ctypes.c_double * 8)(*alp))
 
 
 class Tune(ctypes.Structure):
@@ -127,7 +133,8 @@ def lib():
         L.fz_forward_rf_full_device.argtypes = [P, ctypes.c_int, P, ctypes.c_int, P, P, P, P, P]
         L.fz_invert.argtypes = [P, ctypes.c_int, P, P, P, ctypes.c_int, P, P, P, P, P, P]
         L.fz_invert_device.argtypes = [P, ctypes.c_int, P, P, P, ctypes.c_int, P, P, P, P, P, P, P]
-        L.fz_lm_perturbation.argtypes = [P, ctypes.c_int, ctypes.c_int, ctypes.c_int, P, P, P, ctypes.c_double, P]
+        L.fz_lm_perturbation.argtypes = [P, ctypes.c_int, ctypes.c_int, ctypes.c_int, P, P, P, P, P, ctypes.c_double,
+                                         P]
         _lib = L
     return _lib
 
@@ -393,15 +400,20 @@ class Synthesis:
                                       ctypes.c_void_p(status_ptr) if status_ptr else None,
                                       ctypes.c_void_p(stream) if stream else None))
 
-    def lm_perturbation(self, jac, diff, lam, svdtol=1e-4):
+    def lm_perturbation(self, jac, diff, lam, svdtol=1e-4, reg_pen=None, reg_hss=None):
         """Batched GET_PERTURBATION: jac (npix, np, nfreq) normalised Jacobian,
-        diff (npix, nfreq), lam (npix,).  Returns delta (npix, np)."""
+        diff (npix, nfreq), lam (npix,); optional reg_pen (npix, np) and
+        reg_hss (npix, np, np).  Returns delta (npix, np)."""
         j = np.ascontiguousarray(jac, dtype=np.float32)
         d = np.ascontiguousarray(diff, dtype=np.float64)
         lm = np.ascontiguousarray(lam, dtype=np.float64)
         npix, npar, nf = j.shape
+        rp = None if reg_pen is None else np.ascontiguousarray(reg_pen, dtype=np.float64).reshape(npix, npar)
+        rh = None if reg_hss is None else np.ascontiguousarray(reg_hss, dtype=np.float64).reshape(npix, npar, npar)
         out = np.zeros((npix, npar))
-        _check(lib().fz_lm_perturbation(self._h, npix, npar, nf, _p(j), _p(d), _p(lm), float(svdtol), _p(out)))
+        _check(lib().fz_lm_perturbation(self._h, npix, npar, nf, _p(j), _p(d), _p(lm),
+                                        None if rp is None else _p(rp), None if rh is None else _p(rh),
+                                        float(svdtol), _p(out)))
         return out
 
     def forward_rf_device(self, model_ptr, ncol, syn_ptr, jac_ptr, model_out_ptr, status_ptr=0, stream=0,

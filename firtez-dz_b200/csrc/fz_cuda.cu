@@ -1553,6 +1553,7 @@ void lm_free_pool(LMSlots& L) {
   cudaFree(L.jacb);
   cudaFree(L.need_rf);
   cudaFree(L.rf_list);
+  cudaFree(L.pen);
   cudaFree(L.obs);
   cudaFree(L.diff);
   cudaFree(L.H);
@@ -1583,6 +1584,7 @@ int lm_alloc_pool(LMSlots& L, int S, int np, int nf, int nm) {
   FZ_CK(cudaMalloc(&L.synb, (size_t)S * nf * sizeof(double)));
   FZ_CK(cudaMalloc(&L.jacb, (size_t)S * np * nf * sizeof(float)));
   FZ_CK(cudaMalloc(&L.need_rf, (size_t)S * sizeof(int)));
+  FZ_CK(cudaMalloc(&L.pen, (size_t)S * np * sizeof(double)));
   FZ_CK(cudaMalloc(&L.rf_list, (size_t)S * sizeof(int)));
   FZ_CK(cudaMalloc(&L.obs, (size_t)S * nf * sizeof(double)));
   FZ_CK(cudaMalloc(&L.diff, (size_t)S * nf * sizeof(double)));
@@ -1641,6 +1643,13 @@ int lm_conf(fz_ctx* c, int npix, const fz_lm_opts* o, LMConf& C) {
   C.inu = (double)C.nfreq;
   C.fallback = o && o->fallback_model ? o->fallback : 0.0;
   C.fb_model = o ? o->fallback_model : nullptr;
+  // GET_IT_PENALTIES operators (src/get_dmodel.f90:1103-1146): per free
+  // parameter L = sqrt(PEN_ALP / IFREEP) D, D = diag(1/NJ) (type 0) or first
+  // differences to the previous node (type 1); PEN_HSS = L^T L block diagonal
+  if (o)
+    for (int p = 0; p < 8; ++p)
+      if (o->reg_alpha[p] < 0.0 || (o->reg_alpha[p] > 0.0 && o->reg_type[p] != 0 && o->reg_type[p] != 1))
+        return FZ_ERR_ARG;
   const double norms[8] = {6000.0, 1.0e5, 1.0e-5, 1.0e3, 1.0e3, 1.0e3, 1.0e6, 6.0e2};
   // nodes in reference parameter order (the slot order of the Jacobian)
   for (int p = 0; p < NSLOT; ++p) {
@@ -1651,6 +1660,30 @@ int lm_conf(fz_ctx* c, int npix, const fz_lm_opts* o, LMConf& C) {
       C.row_of[n] = kRow[rp];
       C.par_of[n] = rp;
       C.norm[n] = norms[rp - 1];
+    }
+  }
+  if (o) {
+    for (int p = 0; p < NSLOT; ++p) {
+      const int rp = kRef[p], nj = c->rf.nj[p], j0 = c->rf.n0[p];
+      const double alp = o->reg_alpha[rp - 1];
+      if (nj <= 0 || alp <= 0.0) continue;
+      C.reg = 1;
+      const double a2 = alp / (double)C.np;   // ALP^2
+      for (int k = 0; k < nj; ++k)
+        for (int l = 0; l < nj; ++l) {
+          double v = 0.0;   // (D^T D)(k, l)
+          if (o->reg_type[rp - 1] == 0) {
+            v = k == l ? 1.0 / ((double)nj * nj) : 0.0;
+          } else {
+            // D rows r >= 1: e_r - e_{r-1}
+            for (int r = 1; r < nj; ++r) {
+              const double dk = (k == r ? 1.0 : 0.0) - (k == r - 1 ? 1.0 : 0.0);
+              const double dl = (l == r ? 1.0 : 0.0) - (l == r - 1 ? 1.0 : 0.0);
+              v += dk * dl;
+            }
+          }
+          C.reg_hss[(j0 + k) * C.np + (j0 + l)] = a2 * v;
+        }
     }
   }
   return 0;
@@ -2091,6 +2124,7 @@ int fz_invert_device(fz_ctx* c, int npix, const double* d_obs, const float* d_in
   FZ_CK(cudaMemsetAsync(c->d_q, 0, sizeof(LMQueue), s));
   if (d_status) FZ_CK(cudaMemsetAsync(d_status, 0, npix * sizeof(int), s));
   LMSlots L = c->lm, L2 = c->lm2;   // L is the pool in use; it shrinks to the occupied slots in the tail
+  if (!C.reg) L.pen = L2.pen = nullptr;
   {
     ProfScope ps(c, 5, s, S);
     k_lm_fill<<<S, 128, 0, s>>>(C, L, c->d_q, d_obs, d_init);
@@ -2112,7 +2146,7 @@ int fz_invert_device(fz_ctx* c, int npix, const double* d_obs, const float* d_in
     {
       ProfScope ps(c, 6, s, n);
       k_lm_accept<<<n, 256, 0, s>>>(C, L, c->d_q, d_w, d_obs, d_init, d_target_chi2, d_model_out, d_chi2, d_iters,
-                                    d_syn_out, d_status);
+                                    d_syn_out, d_status, c->d_coef64);
     }
     k_lm_rflist<<<1, 1024, 0, s>>>(n, L.need_rf, L.rf_list, c->d_q);
     FZ_CK(cudaGetLastError());
@@ -2260,7 +2294,8 @@ int fz_invert(fz_ctx* c, int npix, const double* obs, const float* init, const d
 }
 
 int fz_lm_perturbation(fz_ctx* c, int npix, int np, int nfreq, const float* jac, const double* diff,
-                       const double* lambda, double svdtol, double* delta) {
+                       const double* lambda, const double* reg_pen, const double* reg_hss, double svdtol,
+                       double* delta) {
   if (!c || npix <= 0 || np <= 0 || np > LM_MAXNP || nfreq <= 0 || (nfreq & 3) || !jac || !diff || !lambda || !delta)
     return FZ_ERR_ARG;
   FZ_CK(cudaSetDevice(c->device));
@@ -2289,6 +2324,14 @@ int fz_lm_perturbation(fz_ctx* c, int npix, int np, int nfreq, const float* jac,
     if ((rc = cuda_fail(cudaMalloc(&L.g, (size_t)npix * np * sizeof(double))))) break;
     if ((rc = cuda_fail(cudaMalloc(&L.delta, (size_t)npix * np * sizeof(double))))) break;
     if ((rc = cuda_fail(cudaMalloc(&d_w, nfreq * sizeof(double))))) break;
+    if (reg_pen) {
+      if ((rc = cuda_fail(cudaMalloc(&L.pen, (size_t)npix * np * sizeof(double))))) break;
+      cudaMemcpy(L.pen, reg_pen, (size_t)npix * np * sizeof(double), cudaMemcpyHostToDevice);
+    }
+    if (reg_hss) {
+      if ((rc = cuda_fail(cudaMalloc(&L.hss, (size_t)npix * np * np * sizeof(double))))) break;
+      cudaMemcpy(L.hss, reg_hss, (size_t)npix * np * np * sizeof(double), cudaMemcpyHostToDevice);
+    }
     cudaMemcpy(L.pix, zeros.data(), npix * sizeof(int), cudaMemcpyHostToDevice);
     cudaMemcpy(L.skip, zeros.data(), npix * sizeof(int), cudaMemcpyHostToDevice);
     cudaMemcpy(L.st, st.data(), st.size() * sizeof(double), cudaMemcpyHostToDevice);
@@ -2309,6 +2352,8 @@ int fz_lm_perturbation(fz_ctx* c, int npix, int np, int nfreq, const float* jac,
   cudaFree(L.H);
   cudaFree(L.g);
   cudaFree(L.delta);
+  cudaFree(L.pen);
+  cudaFree(L.hss);
   cudaFree(d_w);
   return rc;
 }

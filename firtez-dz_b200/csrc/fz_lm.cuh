@@ -36,6 +36,8 @@ struct LMConf {
   double dchi2, svdtol, inu;
   double fallback;             // restart factor on the chi2 goal (0 = off)
   const float* fb_model;       // MODEL(NZ,13) a restarted pixel starts from
+  int reg;                     // vertical regularisation on (GET_IT_PENALTIES)
+  double reg_hss[LM_MAXNP * LM_MAXNP];   // PEN_HSS = L^T L (model independent)
   int nodes_ref[8];            // node count per reference parameter
   int row_of[LM_MAXNP];        // model row of each node's parameter
   int par_of[LM_MAXNP];        // reference parameter (1-based) of each node
@@ -56,6 +58,8 @@ struct LMSlots {
   double* synb;      // best synthesis
   float* jacb;       // best Jacobian (S, np, nfreq), written by the RF pass of accepted models
   int* need_rf;      // 1 if the slot's model was accepted and the pixel goes on: its Jacobian is needed
+  double* pen;       // PEN_RES of the best model (S, np), subtracted from J^T r; may be null
+  double* hss;       // per-slot PEN_HSS (S, np, np) added to J^T J; null: C.reg_hss when C.reg
   int* rf_list;      // slots needing the RF pass, compacted (k_lm_rflist)
   double* obs;       // (S, nfreq)
   double* diff;      // weighted residual (S, nfreq)
@@ -76,6 +80,28 @@ struct LMQueue {
 __constant__ double c_lm_norm[8] = {6000.0, 1.0e5, 1.0e-5, 1.0e3, 1.0e3, 1.0e3, 1.0e6, 6.0e2};
 __constant__ double c_lm_low[8] = {2500.0, 1.0e-2, 1.0e-10, -5.0e4, -5.0e4, -5.0e4, -1.0e7, 1.0e-8};
 __constant__ double c_lm_upp[8] = {1.8e4, 1.0e12, 1.0e10, 5.0e4, 5.0e4, 5.0e4, 1.0e7, 1.0e12};
+
+// Node values of the free parameters of model m (13, nz): CONTRACT_VECTOR
+// (src/get_dmodel.f90:861-880) over the hat table coef (nz, np), divided by
+// PARAM_NORM -- the x of GET_IT_PENALTIES (:1041-1197).  Thread j < np.
+__device__ __forceinline__ double lm_node_value(const LMConf& C, const float* __restrict__ m,
+                                                const double* __restrict__ coef, int j) {
+  const float* row = m + (size_t)C.row_of[j] * C.nz;
+  double a = 0.0, cs = 0.0;
+  for (int k = 0; k < C.nz; ++k) {
+    const double c = coef[(size_t)k * C.np + j];
+    a += (double)row[k] * c;
+    cs += c;
+  }
+  return a / cs / C.norm[j];
+}
+
+// PEN_RES_j = (PEN_HSS x)_j of model m for thread j < np (x in shared xs)
+__device__ __forceinline__ double lm_pen_res(const LMConf& C, const double* xs, int j) {
+  double r = 0.0;
+  for (int i = 0; i < C.np; ++i) r += C.reg_hss[j * C.np + i] * xs[i];
+  return r;
+}
 
 __device__ __forceinline__ double block_sum_d(double v, double* red) {
   for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
@@ -134,8 +160,10 @@ __global__ void __launch_bounds__(256) k_lm_accept(LMConf C, LMSlots Sl, LMQueue
                                                    const float* __restrict__ init_all,
                                                    const double* __restrict__ target, float* __restrict__ out_model,
                                                    double* __restrict__ out_chi, int* __restrict__ out_iter,
-                                                   double* __restrict__ out_syn, int* __restrict__ out_status) {
+                                                   double* __restrict__ out_syn, int* __restrict__ out_status,
+                                                   const double* __restrict__ coef) {
   __shared__ double red[8];
+  __shared__ double xs[LM_MAXNP], pr[LM_MAXNP];
   __shared__ int acc, fin, np_next;
   const int s = blockIdx.x;
   if (threadIdx.x == 0) {
@@ -152,7 +180,19 @@ __global__ void __launch_bounds__(256) k_lm_accept(LMConf C, LMSlots Sl, LMQueue
     const double d = obs[i] - syn[i];
     e += d * d * w[i];
   }
-  const double chi = block_sum_d(e, red) / C.inu;
+  double chi = block_sum_d(e, red) / C.inu;
+  if (C.reg) {
+    // NEW_CALCULATE_CHI2 with regularisation (src/get_dmodel.f90:966-983):
+    // + sum(PEN_RES^2) of the current model, PEN_FACTOR = 1
+    const float* mc = Sl.mcur + (size_t)s * nm;
+    if (threadIdx.x < C.np) xs[threadIdx.x] = lm_node_value(C, mc, coef, threadIdx.x);
+    __syncthreads();
+    if (threadIdx.x < C.np) pr[threadIdx.x] = lm_pen_res(C, xs, threadIdx.x);
+    __syncthreads();
+    double pp = 0.0;
+    for (int j = 0; j < C.np; ++j) pp += pr[j] * pr[j];
+    chi += pp;
+  }
   double* st = Sl.st + 5 * (size_t)s;
   if (threadIdx.x == 0) {
     const double chibest = st[1];
@@ -205,6 +245,19 @@ __global__ void __launch_bounds__(256) k_lm_accept(LMConf C, LMSlots Sl, LMQueue
     for (int i = threadIdx.x; i < nm; i += blockDim.x) mc[i] = mb[i];
   }
   __syncthreads();
+  if (C.reg && Sl.pen && !fin) {
+    // GET_IT_PENALTIES of the best model for the normal equations: after an
+    // accepted step the current one, after a rejection the restored one
+    // (:1010-1015)
+    if (!acc) {
+      const float* mb = Sl.mbest + (size_t)s * nm;
+      if (threadIdx.x < C.np) xs[threadIdx.x] = lm_node_value(C, mb, coef, threadIdx.x);
+      __syncthreads();
+      if (threadIdx.x < C.np) pr[threadIdx.x] = lm_pen_res(C, xs, threadIdx.x);
+      __syncthreads();
+    }
+    if (threadIdx.x < C.np) Sl.pen[(size_t)s * C.np + threadIdx.x] = pr[threadIdx.x];
+  }
   if (fin && C.fallback > 0.0 && C.fb_model && target && !Sl.restarted[s] && st[1] > C.fallback * target[p]) {
     // the search ended above fallback x its goal: start once more from the
     // fallback model (INITIALIZE_CYCLE's state), the goal kept
@@ -324,8 +377,10 @@ __global__ void __launch_bounds__(128) k_lm_normal(LMConf C, LMSlots Sl, const d
   for (int i = 0; i < 4; ++i) {
     const int row = grp + (i >= 2 ? 8 : 0);
     const int colA = 2 * t + (i & 1), colB = 8 + 2 * t + (i & 1);
-    if (row < np && colA < np) H[row * np + colA] = (double)c0[i];
-    if (row < np && colB < np) H[row * np + colB] = (double)c1[i];
+    // GET_PERTURBATION adds REG_HSS to J^T J (src/lm.f90:173-174)
+    const double* rh = Sl.hss ? Sl.hss + (size_t)s * np * np : (C.reg ? C.reg_hss : nullptr);
+    if (row < np && colA < np) H[row * np + colA] = (double)c0[i] + (rh ? rh[row * np + colA] : 0.0);
+    if (row < np && colB < np) H[row * np + colB] = (double)c1[i] + (rh ? rh[row * np + colB] : 0.0);
   }
   // g = Jn^T r (FP64)
   const double* df = Sl.diff + (size_t)s * nf;
@@ -334,7 +389,9 @@ __global__ void __launch_bounds__(128) k_lm_normal(LMConf C, LMSlots Sl, const d
     double acc = 0.0;
     for (int k = lane; k < nf; k += 32) acc += (double)rc[k] * sqrt(w[k]) * df[k];
     for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
-    if (lane == 0) Sl.g[(size_t)s * np + c] = acc * C.norm[c] / sqrt(C.inu);
+    // ... and subtracts REG_PEN from J^T r (:169-170)
+    if (lane == 0)
+      Sl.g[(size_t)s * np + c] = acc * C.norm[c] / sqrt(C.inu) - (Sl.pen ? Sl.pen[(size_t)s * np + c] : 0.0);
   }
 }
 

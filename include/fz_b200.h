@@ -202,7 +202,12 @@ int fz_tune_set(fz_ctx* ctx, const fz_tune* t);
  * from fallback_model (device, one MODEL(NZ,13) for every pixel, e.g. the
  * default guess) in the same slot pool, keeping the goal; its iterations
  * add up.  0 / NULL: off.  fallback_model is a device pointer for
- * fz_invert_device and a host pointer for fz_invert. */
+ * fz_invert_device and a host pointer for fz_invert.  reg_type, reg_alpha:
+ * the vertical regularisation of VERTICAL REGULARIZATION
+ * (GET_IT_PENALTIES, src/get_dmodel.f90:1041-1197), per reference parameter
+ * 1..8: type 0 (node values to zero, D = diag(1/NJ)) or 1 (differences to
+ * the previous node) and PEN_ALP (0: off); chi2 gains sum(PEN_RES^2) of the
+ * current model, the normal equations PEN_HSS and -PEN_RES of the best. */
 typedef struct {
   int maxsteps, maxit;
   double dchi2, svdtol, isigma;
@@ -210,6 +215,8 @@ typedef struct {
   int slots, pad;
   double fallback;
   const float* fallback_model;
+  int reg_type[8];
+  double reg_alpha[8];
 } fz_lm_opts;
 
 /* Batched pixel-wise Levenberg-Marquardt inversion of npix pixels with the
@@ -240,9 +247,12 @@ int fz_autotune_lm(fz_ctx* ctx, int npix, const double* d_obs, const float* d_in
  * accumulation), g = J^T diff, (H + lambda diag H)^+ g by an FP64 Jacobi SVD
  * with singular values below svdtol * max dropped.  jac is the normalised
  * JACOB as REAL*4, (nfreq, np, npix); diff (nfreq, npix); lambda (npix);
- * delta (np, npix).  np <= 16, nfreq a multiple of 4. */
+ * reg_pen (np, npix) and reg_hss (np, np, npix), may be NULL: REG_PEN is
+ * subtracted from J^T diff and REG_HSS added to J^T J as the reference
+ * does (:169-174); delta (np, npix).  np <= 16, nfreq a multiple of 4. */
 int fz_lm_perturbation(fz_ctx* ctx, int npix, int np, int nfreq, const float* jac, const double* diff,
-                       const double* lambda, double svdtol, double* delta);
+                       const double* lambda, const double* reg_pen, const double* reg_hss, double svdtol,
+                       double* delta);
 
 /* Warm-start network (no counterpart in the reference): an MLP of nlayers
  * fully connected layers dims[0] -> dims[1] -> ... -> dims[nlayers] with GELU

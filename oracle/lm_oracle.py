@@ -97,11 +97,16 @@ def pinv_dgesvd(m, svdtol=RSVDTOL):
     return vt.T @ (np.diag(si) @ u.T)
 
 
-def get_perturbation(jac_n, diff, lam, svdtol=RSVDTOL):
+def get_perturbation(jac_n, diff, lam, svdtol=RSVDTOL, reg_pen=None, reg_hss=None):
     """GET_PERTURBATION (src/lm.f90:137-204) with SOLVER_METHOD = 1: jac_n is
-    the normalised JACOB (NFREQ, NP), diff the weighted residual."""
+    the normalised JACOB (NFREQ, NP), diff the weighted residual; REG_PEN is
+    subtracted from J^T diff and REG_HSS added to J^T J (:170-174)."""
     hss = jac_n.T @ jac_n
     term2 = jac_n.T @ diff
+    if reg_pen is not None:
+        term2 = term2 - reg_pen
+    if reg_hss is not None:
+        hss = hss + reg_hss
     term1 = hss.copy()
     term1[np.diag_indices_from(term1)] += np.diag(hss) * lam
     delta = pinv_dgesvd(term1, svdtol) @ term2
@@ -163,6 +168,38 @@ def rearange(model, delta, nodes):
         j0 += nj
 
 
+def it_penalties(model, nodes, pen_typ, pen_alp):
+    """GET_IT_PENALTIES (src/get_dmodel.f90:1041-1197) on model (13, NZ): per
+    free parameter p the node values x = CONTRACT_VECTOR(row) / PARAM_NORM, the
+    operator L = ALP D with ALP = sqrt(PEN_ALP / IFREEP) and D = diag(1/NJ)
+    (type 0) or first differences to the previous node (type 1, first row
+    zero); returns (PEN_RES = L^T L x, PEN_HSS = L^T L), block diagonal over
+    the parameters in node order.  pen_typ, pen_alp: per reference parameter
+    1..8."""
+    nz = model.shape[1]
+    npar = sum(n for n in nodes.values() if n > 0)
+    res = np.zeros(npar)
+    hss = np.zeros((npar, npar))
+    j0 = 0
+    for p in range(1, 9):
+        nj = nodes.get(p, 0)
+        if nj <= 0:
+            continue
+        x = contract(model[ATMPOS[p]], int_coefs(nz, nj)) / PARAM_NORMS[p - 1]
+        lop = np.zeros((nj, nj))
+        if pen_typ[p - 1] == 0:
+            lop[np.diag_indices(nj)] = 1.0 / nj
+        elif pen_typ[p - 1] == 1:
+            for k in range(1, nj):
+                lop[k, k] = 1.0
+                lop[k, k - 1] = -1.0
+        lop *= np.sqrt(float(pen_alp[p - 1]) / float(npar))
+        res[j0:j0 + nj] = lop.T @ (lop @ x)
+        hss[j0:j0 + nj, j0:j0 + nj] = lop.T @ lop
+        j0 += nj
+    return res, hss
+
+
 def normalize_jacob(jac, w, inu, nodes):
     """NORMALIZE_JACOB: JACOB (NFREQ, NP) REAL*8 of the REAL*4 EQVDSYN."""
     j = jac.astype(np.float64) * (np.sqrt(w) / np.sqrt(inu))[:, None]
@@ -187,11 +224,15 @@ class PixelState:
         self.best_jac = None
 
 
-def lm_accept(st, obs, syn, jac, w, ok=True):
+def lm_accept(st, obs, syn, jac, w, ok=True, reg=None):
     """NEW_CALCULATE_CHI2 + UPDATE_LAMBDA for one pixel; returns (chi, accepted,
-    previous best chi)."""
+    previous best chi).  reg = (nodes, pen_typ, pen_alp): the penalty of the
+    current model, sum(PEN_RES^2), is added to chi2 (:966-983)."""
     inu = float(obs.size)
     chi = float(np.sum((obs - syn) ** 2 * w) / inu) if ok else 1.0e300
+    if reg is not None and ok:
+        pen, _ = it_penalties(st.cur, *reg)
+        chi += float(np.sum(pen * pen))
     prev = st.chibest
     st.chicur = chi
     acc = chi < st.chibest
@@ -205,13 +246,17 @@ def lm_accept(st, obs, syn, jac, w, ok=True):
     return chi, acc, prev
 
 
-def lm_perturb(st, obs, w, nodes):
-    """The rest of GET_PERT_1D: normalised Jacobian, GET_PERTURBATION and
-    REARANGE_DA_MODEL; st.cur becomes the next trial model."""
+def lm_perturb(st, obs, w, nodes, reg=None):
+    """The rest of GET_PERT_1D: normalised Jacobian, GET_PERTURBATION (with the
+    penalties of the best model, reg as in lm_accept) and REARANGE_DA_MODEL;
+    st.cur becomes the next trial model."""
     inu = float(obs.size)
     diff = (obs - st.best_syn) * np.sqrt(w) / np.sqrt(inu)
     jn = normalize_jacob(st.best_jac, w, inu, nodes)
-    delta = get_perturbation(jn, diff, st.lam)
+    pen = hss = None
+    if reg is not None:
+        pen, hss = it_penalties(st.best, *reg)
+    delta = get_perturbation(jn, diff, st.lam, reg_pen=pen, reg_hss=hss)
     rearange(st.cur, delta, nodes)
     return delta
 
@@ -223,12 +268,16 @@ def lm_step(st, obs, syn, jac, w, nodes):
     return lm_perturb(st, obs, w, nodes)
 
 
-def invert(forward_rf, obs, init, nodes, w, maxsteps=5, maxit=40, dchi2=0.0):
+def invert(forward_rf, obs, init, nodes, w, maxsteps=5, maxit=40, dchi2=0.0, reg=None):
     """Pixel-wise inversion with the stop rules of the batched GPU inversion
     (steps > maxsteps, maxit iterations, or an accepted step gaining less than
     dchi2 relative).  forward_rf(models (n,13,nz)) -> (syn (n,nfreq),
-    jac (n,nfreq,np), models_out, status); obs (npix, nfreq).
-    Returns (best models, chi2, iterations)."""
+    jac (n,nfreq,np), models_out, status); obs (npix, nfreq); reg =
+    (pen_typ, pen_alp) per reference parameter adds the vertical
+    regularisation of GET_IT_PENALTIES.  Returns (best models, chi2,
+    iterations)."""
+    if reg is not None:
+        reg = (nodes,) + tuple(reg)
     npix = obs.shape[0]
     states = [PixelState(init[i]) for i in range(npix)]
     iters = np.zeros(npix, dtype=np.int32)
@@ -240,12 +289,12 @@ def invert(forward_rf, obs, init, nodes, w, maxsteps=5, maxit=40, dchi2=0.0):
         for a, i in enumerate(active):
             st = states[i]
             st.cur = mo[a].copy()
-            _, acc, prev = lm_accept(st, obs[i], syn[a], jac[a], w, ok=status[a] == 0)
+            _, acc, prev = lm_accept(st, obs[i], syn[a], jac[a], w, ok=status[a] == 0, reg=reg)
             iters[i] += 1
             small = acc and prev < 1.0e29 and (prev - st.chibest) < dchi2 * prev
             if st.steps > maxsteps or iters[i] >= maxit or small:
                 continue
-            lm_perturb(st, obs[i], w, nodes)
+            lm_perturb(st, obs[i], w, nodes, reg=reg)
             still.append(i)
         active = still
     best = np.stack([st.best for st in states])

@@ -123,3 +123,58 @@ def test_fallback_restart_reaches_the_plain_chi2(fz, orc):
     _, chi_h, it_h, _ = ctx.invert(obs, bad, hydrostatic=True, opts=hopts, target=chi_pl)
     np.testing.assert_array_equal(chi_h, chi_fb)
     np.testing.assert_array_equal(it_h, it_fb)
+
+
+def test_lm_perturbation_with_regularisation_matches_oracle(fz, orc):
+    """GET_PERTURBATION with REG_PEN subtracted from J^T diff and REG_HSS added
+    to J^T J (per-pixel arrays), against the FP64 oracle."""
+    _, _, _, ctx = _ctx(fz, orc, 32)
+    rng = np.random.default_rng(9)
+    npix, npar, nf = 12, 13, 896
+    jac = np.zeros((npix, npar, nf), dtype=np.float32)
+    for i in range(npix):
+        u, _ = np.linalg.qr(rng.standard_normal((nf, npar)))
+        v, _ = np.linalg.qr(rng.standard_normal((npar, npar)))
+        s = np.logspace(0, -1.0, npar) * 50.0
+        jac[i] = ((u * s) @ v.T).T.astype(np.float32)
+    diff = rng.standard_normal((npix, nf))
+    lam = 10.0 ** rng.uniform(-2, 1, npix)
+    pen = rng.standard_normal((npix, npar))
+    a = rng.standard_normal((npix, npar, npar)) * 3.0
+    hss = np.einsum("nij,nkj->nik", a, a)           # symmetric positive semi-definite
+    d = ctx.lm_perturbation(jac, diff, lam, reg_pen=pen, reg_hss=hss)
+    for i in range(npix):
+        ref = lmo.get_perturbation(jac[i].T.astype(np.float64), diff[i], lam[i], reg_pen=pen[i], reg_hss=hss[i])
+        assert np.linalg.norm(d[i] - ref) <= 1e-3 * np.linalg.norm(ref), i
+
+
+def test_regularised_inversion_matches_oracle_outcome(fz, orc):
+    """VERTICAL REGULARIZATION (GET_IT_PENALTIES): first differences of the T
+    nodes and node values of B_z toward zero.  The batched inversion and the
+    oracle's reach chi2 (data term + sum PEN_RES^2) within a factor 2 of each
+    other, and the reported chi2 is that of the returned model, penalty
+    included."""
+    nz, npix = 48, 8
+    lines, reg, g, ctx = _ctx(fz, orc, nz)
+    true = fz.atmos.make_columns(npix, nz, seed=15)
+    obs, true_he, _ = orc.forward(lines, reg, g, true, hydrostatic=True)
+    init = lmcase.initial_guess(true_he, seed=4)
+    w = lmo.weights(ctx.numw, isigma=1e-3)
+    f = lmcase.oracle_forward_rf(orc, lines, reg, g, he=True)
+    typ = [1, 0, 0, 0, 0, 0, 0, 0]
+    alp = [300.0, 0.0, 0.0, 0.0, 0.0, 30.0, 0.0, 0.0]
+    _, ochi, _ = lmo.invert(f, obs.reshape(npix, -1), init, lmcase.NODES, w, maxsteps=5, maxit=25,
+                            reg=(typ, alp))
+    ctx.rf_nodes(lmcase.NODES)
+    opts = fz.LMOpts(maxsteps=5, maxit=25, isigma=1e-3, slots=5, reg={1: (1, 300.0), 6: (0, 30.0)})
+    best, chi, it, st = ctx.invert(obs, init, hydrostatic=True, opts=opts)
+    assert np.all(st == 0) and np.all(np.isfinite(best))
+    ratio = np.median(chi / ochi)
+    assert 0.5 <= ratio <= 2.0, (chi, ochi)
+    syn, _, _ = orc.forward(lines, reg, g, best, hydrostatic=True)
+    data = np.sum((obs.reshape(npix, -1) - syn.reshape(npix, -1)) ** 2 * w, axis=1) / syn.reshape(npix, -1).shape[1]
+    pen = np.array([np.sum(lmo.it_penalties(best[i], lmcase.NODES, typ, alp)[0] ** 2) for i in range(npix)])
+    assert np.all(pen > 0)
+    assert np.allclose(data + pen, chi, rtol=1e-3), (data + pen, chi)
+    with pytest.raises(fz.FzError):
+        ctx.invert(obs, init, hydrostatic=True, opts=fz.LMOpts(reg={1: (2, 1.0)}))

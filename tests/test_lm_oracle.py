@@ -69,3 +69,37 @@ def test_oracle_inversion_recovers_the_atmosphere(fz, orc):
     assert np.all(chi < 0.2 * chi0), (chi0, chi)
     assert np.all(it < 25)
     assert np.all(np.isfinite(best))
+
+
+def test_it_penalties_operators():
+    """GET_IT_PENALTIES: type 0 is diag(1/NJ), type 1 first differences to the
+    previous node, both scaled by sqrt(PEN_ALP / IFREEP); PEN_RES = PEN_HSS x
+    with x the node averages over PARAM_NORM; parameters with zero alpha add
+    nothing."""
+    nz = 40
+    nodes = {1: 4, 4: 2, 6: 3}
+    rng = np.random.default_rng(2)
+    model = np.zeros((13, nz), dtype=np.float32)
+    model[0] = 6000.0 + 200.0 * rng.standard_normal(nz)
+    model[5] = 300.0 * rng.standard_normal(nz)
+    model[7] = 500.0 + 100.0 * rng.standard_normal(nz)
+    typ = [1, 0, 0, 0, 0, 1, 0, 0]
+    alp = [2.0, 0.0, 0.0, 0.5, 0.0, 3.0, 0.0, 0.0]
+    res, hss = lmo.it_penalties(model, nodes, typ, alp)
+    npar = 9
+    assert res.shape == (npar,) and hss.shape == (npar, npar)
+    x = np.concatenate([lmo.contract(model[lmo.ATMPOS[p]], lmo.int_coefs(nz, n)) / lmo.PARAM_NORMS[p - 1]
+                        for p, n in sorted(nodes.items())])
+    np.testing.assert_allclose(res, hss @ x, rtol=1e-12, atol=1e-15)
+    d = np.zeros((4, 4))
+    for k in range(1, 4):
+        d[k, k], d[k, k - 1] = 1.0, -1.0
+    np.testing.assert_allclose(hss[:4, :4], 2.0 / npar * d.T @ d, rtol=1e-12)
+    np.testing.assert_allclose(hss[4:6, 4:6], 0.5 / npar * np.eye(2) / 4.0, rtol=1e-12)
+    d3 = np.zeros((3, 3))
+    for k in range(1, 3):
+        d3[k, k], d3[k, k - 1] = 1.0, -1.0
+    np.testing.assert_allclose(hss[6:, 6:], 3.0 / npar * d3.T @ d3, rtol=1e-12)
+    assert np.all(hss[:4, 4:] == 0) and np.all(hss[4:6, 6:] == 0)
+    res0, hss0 = lmo.it_penalties(model, nodes, typ, [0.0] * 8)
+    assert np.all(res0 == 0) and np.all(hss0 == 0)
