@@ -126,6 +126,10 @@ def lib():
         L.fz_forward_rf.argtypes = [P, ctypes.c_int, P, ctypes.c_int, P, P, P, P]
         L.fz_forward_rf_device.argtypes = [P, ctypes.c_int, P, ctypes.c_int, P, P, P, P, P]
         L.fz_forward_rf_full.argtypes = [P, ctypes.c_int, P, ctypes.c_int, P, P, P, P]
+        L.fz_smooth.argtypes = [P, ctypes.c_int, ctypes.c_int, P, P]
+        L.fz_smooth_device.argtypes = [P, ctypes.c_int, ctypes.c_int, P, P, P]
+        L.fz_invert_cycles_device.argtypes = [P, ctypes.c_int, ctypes.c_int, P, P, ctypes.c_int, P, ctypes.c_int, P,
+                                              P, P, P, P]
         L.fz_autotune_forward.argtypes = [P, ctypes.c_int, P, ctypes.c_int, P]
         L.fz_autotune_lm.argtypes = [P, ctypes.c_int, P, P, P, ctypes.c_int, P, P, ctypes.c_int, P]
         L.fz_tune_get.argtypes = [P, P]
@@ -351,6 +355,61 @@ class Synthesis:
             _check(lib().fz_tune_set(self._h, ctypes.byref(t)))
         d = t.as_dict()
         return {k: d[k] for k in ("chain_warps", "chain_lanes", "chemder_blocks_per_sm", "opac_rf_threads", "lm_slots")}
+
+    def smooth(self, models, nx, ny, params=None):
+        """SMOOTHING_B of host models (ny*nx, 13, nz), pixel iy + ny*ix,
+        in a new array; params: iterable of reference parameters (1..8), None
+        = the free parameters of rf_nodes()."""
+        m = np.array(models, dtype=np.float32, order="C", copy=True)
+        if m.shape != (nx * ny, 13, self.nz):
+            raise ValueError("models must be (nx*ny, 13, nz)")
+        f = None
+        if params is not None:
+            f = np.zeros(8, dtype=np.int32)
+            for p in params:
+                f[int(p) - 1] = 1
+        _check(lib().fz_smooth(self._h, int(nx), int(ny), _p(m), None if f is None else _p(f)))
+        return m
+
+    def smooth_device(self, models_ptr, nx, ny, params=None, stream=0):
+        """SMOOTHING_B in place on device models (see smooth())."""
+        f = None
+        if params is not None:
+            f = np.zeros(8, dtype=np.int32)
+            for p in params:
+                f[int(p) - 1] = 1
+        _check(lib().fz_smooth_device(self._h, int(nx), int(ny), ctypes.c_void_p(models_ptr),
+                                      None if f is None else _p(f), ctypes.c_void_p(stream) if stream else None))
+
+    def invert_cycles(self, obs, init, nx, ny, cycles, hydrostatic=True, opts=None):
+        """INVERT3D's cycles on host arrays: obs (ny*nx, 4, numw), init
+        (ny*nx, 13, nz) (pixel iy + ny*ix), cycles = list of node layouts
+        ({reference parameter: NJ}).  Returns (final models, chi2, iterations,
+        status) of the last cycle; the context keeps its node layout."""
+        import torch
+        npix = nx * ny
+        o = np.ascontiguousarray(obs, dtype=np.float64)
+        m = np.ascontiguousarray(init, dtype=np.float32)
+        if o.shape != (npix, 4, self.numw) or m.shape != (npix, 13, self.nz):
+            raise ValueError("obs must be (nx*ny, 4, numw) and init (nx*ny, 13, nz)")
+        nodes = np.zeros((len(cycles), 8), dtype=np.int32)
+        for c, lay in enumerate(cycles):
+            for p, n in lay.items():
+                nodes[c, int(p) - 1] = int(n)
+        d_o = torch.from_numpy(o).cuda()
+        d_m = torch.from_numpy(m.copy()).cuda()
+        chi = torch.zeros(npix, dtype=torch.float64, device="cuda")
+        it = torch.zeros(npix, dtype=torch.int32, device="cuda")
+        st = torch.zeros(npix, dtype=torch.int32, device="cuda")
+        torch.cuda.synchronize()
+        opts = opts or LMOpts()
+        _check(lib().fz_invert_cycles_device(self._h, int(nx), int(ny), ctypes.c_void_p(d_o.data_ptr()),
+                                             ctypes.c_void_p(d_m.data_ptr()), len(cycles), _p(nodes),
+                                             int(bool(hydrostatic)), ctypes.byref(opts),
+                                             ctypes.c_void_p(chi.data_ptr()), ctypes.c_void_p(it.data_ptr()),
+                                             ctypes.c_void_p(st.data_ptr()), None))
+        self.np = int(nodes[-1].sum())
+        return d_m.cpu().numpy(), chi.cpu().numpy(), it.cpu().numpy(), st.cpu().numpy()
 
     def invert(self, obs, init, hydrostatic=True, opts=None, want_syn=False, target=None, out=None):
         """Batched LM inversion of host-resident pixels with the node layout of

@@ -1234,6 +1234,8 @@ struct fz_ctx {
     int lm_slots = 8192;       // pixels in flight when fz_lm_opts.slots == 0
   } tune;
   float* d_oscr = nullptr;   // operators of the full-height RF path (ncol, nz, 16, numw)
+  double* d_smooth = nullptr;   // SMOOTHING_B buffers
+  size_t smooth_len = 0;
   size_t oscr_len = 0;
   LamP* d_lam = nullptr;
   float* d_gain = nullptr;
@@ -1719,9 +1721,144 @@ bool int_coefs(int nz, int nj, std::vector<double>& coef) {
   return true;
 }
 
+// ------------------------------------------------------------ SMOOTHING_B
+// The 1-2-1 smoothing of the free parameters' cubes at the start of every
+// cycle (SMOOTHING_B, src/model_spatial_extension.f90:351-491, called from
+// INITIALIZE_CYCLE, src/invert3d.f90:228-325): in FP64, along x (pixels
+// iy + NY ix), then y, then z, each pass on the previous pass's whole array
+// (array assignment), the first and last index of a direction kept, a
+// direction of 4 or fewer points left alone; the result rounded to REAL*4.
+// Buffers: (nrow, npix, nz) doubles.
+__global__ void k_smooth_load(int npix, int nz, int nrow, const int* __restrict__ rows, const float* __restrict__ m,
+                              double* __restrict__ a) {
+  const size_t total = (size_t)nrow * npix * nz;
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (size_t)gridDim.x * blockDim.x) {
+    const int k = (int)(i % nz);
+    const size_t pr = i / nz;
+    const int pix = (int)(pr % npix), r = (int)(pr / npix);
+    a[i] = (double)m[((size_t)pix * 13 + rows[r]) * nz + k];
+  }
+}
+
+// dir 0: x (stride NY pixels), 1: y (stride 1 pixel), 2: z; the last pass
+// writes REAL*4 into the model rows
+__global__ void k_smooth_pass(int nx, int ny, int nz, int nrow, int dir, const int* __restrict__ rows,
+                              const double* __restrict__ a, double* __restrict__ b, float* __restrict__ m) {
+  const int npix = nx * ny;
+  const size_t total = (size_t)nrow * npix * nz;
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (size_t)gridDim.x * blockDim.x) {
+    const int k = (int)(i % nz);
+    const size_t pr = i / nz;
+    const int pix = (int)(pr % npix), r = (int)(pr / npix);
+    const int iy = pix % ny, ix = pix / ny;
+    double v = a[i];
+    if (dir == 0 && nx > 4 && ix > 0 && ix < nx - 1)
+      v = __dadd_rn(__dadd_rn(a[i + (size_t)ny * nz], a[i - (size_t)ny * nz]), __dmul_rn(v, 2.0)) / 4.0;
+    else if (dir == 1 && ny > 4 && iy > 0 && iy < ny - 1)
+      v = __dadd_rn(__dadd_rn(a[i + nz], a[i - nz]), __dmul_rn(v, 2.0)) / 4.0;
+    else if (dir == 2 && nz > 4 && k > 0 && k < nz - 1)
+      v = __dadd_rn(__dadd_rn(a[i + 1], a[i - 1]), __dmul_rn(v, 2.0)) / 4.0;
+    if (m)
+      m[((size_t)pix * 13 + rows[r]) * nz + k] = (float)v;
+    else
+      b[i] = v;
+  }
+}
+
 }  // namespace
 
 extern "C" {
+
+int fz_smooth_device(fz_ctx* c, int nx, int ny, float* d_models, const int* params, void* stream) {
+  if (!c || nx <= 0 || ny <= 0 || !d_models) return FZ_ERR_ARG;
+  // model row of reference parameter 1..8 (P0 smooths Pg, as the reference)
+  static const int kRow[9] = {0, 0, 1, 2, 5, 6, 7, 10, 1};
+  static const int kRef[NSLOT] = {1, 2, 4, 5, 6, 7};
+  int rows[8], nrow = 0;
+  for (int p = 1; p <= 8; ++p) {
+    bool on;
+    if (params) {
+      on = params[p - 1] != 0;
+    } else {
+      on = false;
+      for (int q = 0; q < NSLOT; ++q) on = on || (kRef[q] == p && c->rf.np > 0 && c->rf.nj[q] > 0);
+    }
+    if (on) rows[nrow++] = kRow[p];
+  }
+  if (nrow == 0) return 0;
+  FZ_CK(cudaSetDevice(c->device));
+  cudaStream_t s = (cudaStream_t)stream;
+  const size_t npix = (size_t)nx * ny, n = (size_t)nrow * npix * c->nz;
+  if (n > c->smooth_len) {
+    FZ_CK(cudaStreamSynchronize(s));
+    cudaFree(c->d_smooth);
+    c->d_smooth = nullptr;
+    c->smooth_len = 0;
+    FZ_CK(cudaMalloc(&c->d_smooth, 2 * n * sizeof(double) + 8 * sizeof(int)));
+    c->smooth_len = n;
+  }
+  double* a = c->d_smooth;
+  double* b = a + n;
+  int* d_rows = reinterpret_cast<int*>(b + n);
+  FZ_CK(cudaMemcpyAsync(d_rows, rows, nrow * sizeof(int), cudaMemcpyHostToDevice, s));
+  const int blocks = (int)std::min<size_t>((n + 255) / 256, (size_t)c->nsm * 32);
+  k_smooth_load<<<blocks, 256, 0, s>>>((int)npix, c->nz, nrow, d_rows, d_models, a);
+  k_smooth_pass<<<blocks, 256, 0, s>>>(nx, ny, c->nz, nrow, 0, d_rows, a, b, nullptr);
+  k_smooth_pass<<<blocks, 256, 0, s>>>(nx, ny, c->nz, nrow, 1, d_rows, b, a, nullptr);
+  k_smooth_pass<<<blocks, 256, 0, s>>>(nx, ny, c->nz, nrow, 2, d_rows, a, nullptr, d_models);
+  FZ_CK(cudaGetLastError());
+  return 0;
+}
+
+int fz_invert_cycles_device(fz_ctx* c, int nx, int ny, const double* d_obs, float* d_models, int ncycles,
+                            const int* nodes, int hydrostatic, const fz_lm_opts* opts, double* d_chi2, int* d_iters,
+                            int* d_status, void* stream) {
+  if (!c || nx <= 0 || ny <= 0 || !d_obs || !d_models || ncycles <= 0 || !nodes || !d_chi2 || !d_iters)
+    return FZ_ERR_ARG;
+  FZ_CK(cudaSetDevice(c->device));
+  const int npix = nx * ny;
+  const size_t nm = 13 * (size_t)c->nz;
+  cudaStream_t s = (cudaStream_t)stream;
+  float* d_best = nullptr;
+  double* d_syn = nullptr;
+  int rc = 0;
+  do {
+    if ((rc = cuda_fail(cudaMalloc(&d_best, (size_t)npix * nm * sizeof(float))))) break;
+    if ((rc = cuda_fail(cudaMalloc(&d_syn, (size_t)npix * 4 * c->numw * sizeof(double))))) break;
+    for (int cy = 0; cy < ncycles && !rc; ++cy) {
+      // INITIALIZE_CYCLE: the cycle's node layout, SMOOTHING_B of the models
+      if ((rc = cuda_fail(cudaStreamSynchronize(s)))) break;
+      if ((rc = fz_rf_nodes(c, nodes + 8 * cy)) < 0) break;   // >= 0: the layout's NP
+      rc = 0;
+      if ((rc = fz_smooth_device(c, nx, ny, d_models, nullptr, s))) break;
+      // the cycle's iterations, each pixel from a fresh LM state
+      if ((rc = fz_invert_device(c, npix, d_obs, d_models, nullptr, hydrostatic, opts, d_best, d_chi2, d_iters,
+                                 nullptr, d_status, s)))
+        break;
+      // END_CYCLE: the best models through a plain synthesis (the derived
+      // rows: Pg in hydrostatic mode, rho, Pe, mu, log tau5)
+      if ((rc = launch_forward(c, npix, d_best, hydrostatic, d_syn, d_models, nullptr, s))) break;
+    }
+    if (!rc) rc = cuda_fail(cudaStreamSynchronize(s));
+  } while (false);
+  cudaFree(d_best);
+  cudaFree(d_syn);
+  return rc;
+}
+
+int fz_smooth(fz_ctx* c, int nx, int ny, float* models, const int* params) {
+  if (!c || nx <= 0 || ny <= 0 || !models) return FZ_ERR_ARG;
+  FZ_CK(cudaSetDevice(c->device));
+  const size_t bytes = (size_t)nx * ny * 13 * c->nz * sizeof(float);
+  float* d = nullptr;
+  FZ_CK(cudaMalloc(&d, bytes));
+  int rc = cuda_fail(cudaMemcpyAsync(d, models, bytes, cudaMemcpyHostToDevice, c->stream));
+  if (!rc) rc = fz_smooth_device(c, nx, ny, d, params, c->stream);
+  if (!rc) rc = cuda_fail(cudaMemcpyAsync(models, d, bytes, cudaMemcpyDeviceToHost, c->stream));
+  if (!rc) rc = cuda_fail(cudaStreamSynchronize(c->stream));
+  cudaFree(d);
+  return rc;
+}
 
 int fz_version(void) { return 100; }
 
@@ -1939,6 +2076,7 @@ int fz_destroy(fz_ctx* c) {
   cudaFree(c->d_pf);
   cudaFree(c->d_pfd);
   cudaFree(c->d_oscr);
+  cudaFree(c->d_smooth);
   for (cudaEvent_t e : c->ev_pool) cudaEventDestroy(e);
   for (auto& p : c->pending) {
     cudaEventDestroy(p.a);

@@ -190,6 +190,18 @@ int fz_autotune_forward(fz_ctx* ctx, int ncol, const float* d_model, int hydrost
 int fz_tune_get(fz_ctx* ctx, fz_tune* out);
 int fz_tune_set(fz_ctx* ctx, const fz_tune* t);
 
+/* SMOOTHING_B (src/model_spatial_extension.f90:351-491), which
+ * INITIALIZE_CYCLE applies to the models of the free parameters at the start
+ * of every cycle, the first included (src/invert3d.f90:228-325): a 1-2-1
+ * average in FP64 along x, then y, then height, the end points of each
+ * direction kept and directions of 4 or fewer points left alone, rounded to
+ * REAL*4.  models: MODEL(NZ,13,NY*NX) with pixel iy + NY*ix (the order of
+ * the reference's (NZ,NY,NX) cubes), smoothed in place.  params[8] flags the
+ * reference parameters to smooth (1..8 = T, Pg, rho, Bx, By, Bz, v_z, P0; P0
+ * smooths Pg); NULL: the free parameters of fz_rf_nodes. */
+int fz_smooth(fz_ctx* ctx, int nx, int ny, float* models, const int* params);
+int fz_smooth_device(fz_ctx* ctx, int nx, int ny, float* d_models, const int* params, void* stream);
+
 /* Options of the batched inversion (the reference's control-file values in
  * brackets): maxsteps, the per-pixel limit on the STEPS counter of
  * UPDATE_LAMBDA (MAXITER, 5); maxit, a hard cap on iterations per pixel;
@@ -241,6 +253,19 @@ int fz_invert_device(fz_ctx* ctx, int npix, const double* d_obs, const float* d_
 
 int fz_autotune_lm(fz_ctx* ctx, int npix, const double* d_obs, const float* d_init, const double* d_target_chi2,
                    int hydrostatic, const fz_lm_opts* opts, const int* candidates, int ncand, fz_tune* out);
+
+/* INVERT3D's cycle loop (src/invert3d.f90:57-178, :228-408) on device
+ * buffers for an NX x NY field (pixel iy + NY*ix): for each cycle the node
+ * layout nodes[8*cycle .. 8*cycle+7] (fz_rf_nodes), SMOOTHING_B of the
+ * current models (fz_smooth_device), the batched inversion from them with a
+ * fresh LM state per pixel (fz_invert_device), then END_CYCLE's plain
+ * synthesis of the best models, which become the next cycle's models.
+ * d_models (MODEL(NZ,13,NX*NY)) holds the initial models on entry and the
+ * final ones on return; d_chi2, d_iters, d_status are those of the last
+ * cycle.  The context keeps the last cycle's node layout. */
+int fz_invert_cycles_device(fz_ctx* ctx, int nx, int ny, const double* d_obs, float* d_models, int ncycles,
+                            const int* nodes, int hydrostatic, const fz_lm_opts* opts, double* d_chi2, int* d_iters,
+                            int* d_status, void* stream);
 
 /* Batched GET_PERTURBATION (src/lm.f90:137-204, SOLVER_METHOD = 1) on host
  * buffers: for each pixel H = J^T J (tensor cores, split-bf16 x3, FP32

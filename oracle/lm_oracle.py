@@ -300,3 +300,27 @@ def invert(forward_rf, obs, init, nodes, w, maxsteps=5, maxit=40, dchi2=0.0, reg
     best = np.stack([st.best for st in states])
     chi = np.array([st.chibest for st in states])
     return best, chi, iters
+
+
+def smoothing_b(models, nx, ny, params):
+    """SMOOTHING_B (src/model_spatial_extension.f90:351-491): models
+    (NY*NX, 13, NZ) REAL*4 with pixel iy + NY*ix; for every reference
+    parameter in params (1..8; 8 = P0 smooths Pg) the cube is taken to REAL*8,
+    averaged 1-2-1 along x, then y, then z (array assignments: each pass
+    reads the previous pass's whole array; first and last points of a
+    direction kept; a direction of 4 or fewer points skipped) and rounded
+    back to REAL*4.  The kernel built with FFTW in the routine never touches
+    the model."""
+    m = np.array(models, dtype=np.float32, copy=True)
+    nz = m.shape[2]
+    for p in params:
+        row = ATMPOS[p] if p != 8 else 1
+        a = m[:, row, :].astype(np.float64).reshape(nx, ny, nz)
+        if nx > 4:
+            a[1:-1] = (a[2:] + a[:-2] + a[1:-1] * 2.0) / 4.0
+        if ny > 4:
+            a[:, 1:-1] = (a[:, 2:] + a[:, :-2] + a[:, 1:-1] * 2.0) / 4.0
+        if nz > 4:
+            a[:, :, 1:-1] = (a[:, :, 2:] + a[:, :, :-2] + a[:, :, 1:-1] * 2.0) / 4.0
+        m[:, row, :] = a.reshape(nx * ny, nz).astype(np.float32)
+    return m

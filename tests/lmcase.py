@@ -15,9 +15,11 @@ def initial_guess(true, seed=0):
     return m.astype(np.float32)
 
 
-def oracle_forward_rf(orc, lines, reg, g, he):
+def oracle_forward_rf(orc, lines, reg, g, he, nodes=None):
+    nodes = nodes or NODES
+
     def f(models):
-        syn, jac, mo, st = orc.forward_rf(lines, reg, g, models, NODES, hydrostatic=he)
+        syn, jac, mo, st = orc.forward_rf(lines, reg, g, models, nodes, hydrostatic=he)
         n = syn.shape[0]
         return syn.reshape(n, -1), np.transpose(jac, (0, 2, 1)), mo, st
     return f

@@ -178,3 +178,53 @@ def test_regularised_inversion_matches_oracle_outcome(fz, orc):
     assert np.allclose(data + pen, chi, rtol=1e-3), (data + pen, chi)
     with pytest.raises(fz.FzError):
         ctx.invert(obs, init, hydrostatic=True, opts=fz.LMOpts(reg={1: (2, 1.0)}))
+
+
+@pytest.mark.parametrize("nx,ny,nz", [(7, 6, 9), (3, 8, 4), (5, 5, 16)])
+def test_smoothing_b_matches_oracle(fz, orc, nx, ny, nz):
+    """SMOOTHING_B (the 1-2-1 smoothing of INITIALIZE_CYCLE) on the device
+    against the oracle, bit for bit (FP64 passes, one REAL*4 rounding),
+    including directions of 4 or fewer points that are left alone."""
+    lines, reg, g, ctx = _ctx(fz, orc, nz)
+    rng = np.random.default_rng(nx * 100 + ny)
+    m = rng.standard_normal((nx * ny, 13, nz)).astype(np.float32) * 300.0 + 5000.0
+    params = (1, 4, 6, 7)
+    out = ctx.smooth(m, nx, ny, params=params)
+    ref = lmo.smoothing_b(m, nx, ny, params)
+    np.testing.assert_array_equal(out, ref)
+    untouched = [r for r in range(13) if r not in (0, 5, 7, 10)]
+    np.testing.assert_array_equal(out[:, untouched], m[:, untouched])
+    # default: the free parameters of the node layout
+    ctx.rf_nodes({1: 2, 4: 1, 5: 1, 6: 1, 7: 1})
+    np.testing.assert_array_equal(ctx.smooth(m, nx, ny), lmo.smoothing_b(m, nx, ny, (1, 4, 5, 6, 7)))
+
+
+def test_inversion_cycles_match_oracle(fz, orc):
+    """INVERT3D's cycles on a 6 x 5 field: cycle 1 with T 2, B_z 1, v_z 1 nodes,
+    cycle 2 with the full layout; each cycle starts with SMOOTHING_B of the
+    current models and ends with the plain synthesis of the best ones.  The
+    oracle runs the same sequence (smoothing, pixel-wise LM, forward); the
+    final chi2 of the two agree within a factor 2 in the median, and the
+    second cycle's models are the smoothed first cycle's result carried on."""
+    nx, ny, nz = 6, 5, 40
+    npix = nx * ny
+    lines, reg, g, ctx = _ctx(fz, orc, nz)
+    true = fz.atmos.make_columns(npix, nz, seed=21)
+    obs, true_he, _ = orc.forward(lines, reg, g, true, hydrostatic=True)
+    init = lmcase.initial_guess(true_he, seed=6)
+    cycles = [{1: 2, 6: 1, 7: 1}, lmcase.NODES]
+    w = lmo.weights(ctx.numw, isigma=1e-3)
+    m = init.copy()
+    for nodes in cycles:
+        free = tuple(sorted(nodes))
+        m = lmo.smoothing_b(m, nx, ny, free)
+        f = lmcase.oracle_forward_rf(orc, lines, reg, g, he=True, nodes=nodes)
+        best, ochi, _ = lmo.invert(f, obs.reshape(npix, -1), m, nodes, w, maxsteps=5, maxit=15)
+        _, m, _ = orc.forward(lines, reg, g, best, hydrostatic=True)
+    opts = fz.LMOpts(maxsteps=5, maxit=15, isigma=1e-3, slots=16)
+    mod, chi, it, st = ctx.invert_cycles(obs, init, nx, ny, cycles, hydrostatic=True, opts=opts)
+    assert np.all(st == 0) and np.all(np.isfinite(mod))
+    assert np.all(it >= 1) and np.all(it <= 15)
+    ratio = np.median(chi / ochi)
+    assert 0.5 <= ratio <= 2.0, (chi, ochi)
+    assert ctx.np == 13
