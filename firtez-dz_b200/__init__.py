@@ -130,6 +130,8 @@ def lib():
         L.fz_smooth_device.argtypes = [P, ctypes.c_int, ctypes.c_int, P, P, P]
         L.fz_invert_cycles_device.argtypes = [P, ctypes.c_int, ctypes.c_int, P, P, ctypes.c_int, P, ctypes.c_int, P,
                                               P, P, P, P]
+        L.fz_errors.argtypes = [P, ctypes.c_int, P, P, ctypes.c_int, P, P, P, P]
+        L.fz_errors_device.argtypes = [P, ctypes.c_int, P, P, ctypes.c_int, P, P, P, P, P]
         L.fz_autotune_forward.argtypes = [P, ctypes.c_int, P, ctypes.c_int, P]
         L.fz_autotune_lm.argtypes = [P, ctypes.c_int, P, P, P, ctypes.c_int, P, P, ctypes.c_int, P]
         L.fz_tune_get.argtypes = [P, P]
@@ -380,6 +382,34 @@ class Synthesis:
                 f[int(p) - 1] = 1
         _check(lib().fz_smooth_device(self._h, int(nx), int(ny), ctypes.c_void_p(models_ptr),
                                       None if f is None else _p(f), ctypes.c_void_p(stream) if stream else None))
+
+    def errors(self, obs, models, hydrostatic=True, opts=None):
+        """The errors mode for host models (npix, 13, nz) against obs (npix,
+        4, numw) with the node layout of rf_nodes(): returns (err (npix, 13,
+        nz) float32, chi2 (npix,), status (npix,)); err rows of parameters
+        without nodes are zero.  opts: isigma, wstk, reg."""
+        o = np.ascontiguousarray(obs, dtype=np.float64)
+        m = np.ascontiguousarray(models, dtype=np.float32)
+        npix = o.shape[0]
+        if o.shape[1:] != (4, self.numw) or m.shape != (npix, 13, self.nz):
+            raise ValueError("obs must be (npix, 4, numw) and models (npix, 13, nz)")
+        err = np.zeros_like(m)
+        chi = np.zeros(npix)
+        st = np.zeros(npix, dtype=np.int32)
+        opts = opts or LMOpts()
+        _check(lib().fz_errors(self._h, npix, _p(o), _p(m), int(bool(hydrostatic)), ctypes.byref(opts), _p(err),
+                               _p(chi), _p(st)))
+        return err, chi, st
+
+    def errors_device(self, npix, obs_ptr, models_ptr, err_ptr, chi2_ptr, status_ptr=0, hydrostatic=True,
+                      opts=None, stream=0):
+        """The errors mode on device pointers (see errors())."""
+        opts = opts or LMOpts()
+        _check(lib().fz_errors_device(self._h, int(npix), ctypes.c_void_p(obs_ptr), ctypes.c_void_p(models_ptr),
+                                      int(bool(hydrostatic)), ctypes.byref(opts), ctypes.c_void_p(err_ptr),
+                                      ctypes.c_void_p(chi2_ptr),
+                                      ctypes.c_void_p(status_ptr) if status_ptr else None,
+                                      ctypes.c_void_p(stream) if stream else None))
 
     def invert_cycles(self, obs, init, nx, ny, cycles, hydrostatic=True, opts=None):
         """INVERT3D's cycles on host arrays: obs (ny*nx, 4, numw), init

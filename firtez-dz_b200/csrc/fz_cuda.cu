@@ -1846,6 +1846,86 @@ int fz_invert_cycles_device(fz_ctx* c, int nx, int ny, const double* d_obs, floa
   return rc;
 }
 
+int fz_errors_device(fz_ctx* c, int npix, const double* d_obs, const float* d_models, int hydrostatic,
+                     const fz_lm_opts* opts, float* d_err, double* d_chi2, int* d_status, void* stream) {
+  if (!c || npix <= 0 || !d_obs || !d_models || !d_err || !d_chi2) return FZ_ERR_ARG;
+  FZ_CK(cudaSetDevice(c->device));
+  LMConf C;
+  int rc = lm_conf(c, npix, opts, C);
+  if (rc) return rc;
+  cudaStream_t s = (cudaStream_t)stream;
+  static const float kW1[4] = {1.f, 1.f, 1.f, 1.f};
+  const std::vector<double> w =
+      lm_weights(c->numw, opts ? opts->wstk : kW1, (opts && opts->isigma > 0) ? opts->isigma : 4.0e-3);
+  const int nf = C.nfreq, nm = 13 * c->nz;
+  // the node Jacobians pass through HBM in chunks of at most 16384 pixels
+  // (0.76 GB of REAL*4 EQVDSYN at NP = 13, NFREQ = 896)
+  const int chunk = std::min(npix, 16384);
+  double *d_w = nullptr, *d_syn = nullptr;
+  float *d_jac = nullptr, *d_mout = nullptr;
+  int* d_st = nullptr;
+  do {
+    if ((rc = cuda_fail(cudaMalloc(&d_w, w.size() * sizeof(double))))) break;
+    if ((rc = cuda_fail(cudaMalloc(&d_syn, (size_t)chunk * nf * sizeof(double))))) break;
+    if ((rc = cuda_fail(cudaMalloc(&d_jac, (size_t)chunk * C.np * nf * sizeof(float))))) break;
+    if ((rc = cuda_fail(cudaMalloc(&d_mout, (size_t)chunk * nm * sizeof(float))))) break;
+    if (!d_status && (rc = cuda_fail(cudaMalloc(&d_st, (size_t)chunk * sizeof(int))))) break;
+    if ((rc = cuda_fail(cudaMemcpyAsync(d_w, w.data(), w.size() * sizeof(double), cudaMemcpyHostToDevice, s))))
+      break;
+    const size_t smem = (size_t)c->nz * (sizeof(double) + sizeof(float));
+    for (int p0 = 0; p0 < npix && !rc; p0 += chunk) {
+      const int n = std::min(chunk, npix - p0);
+      int* st = d_status ? d_status + p0 : d_st;
+      if ((rc = launch_forward_rf(c, n, d_models + (size_t)p0 * nm, hydrostatic, d_syn, d_jac, d_mout, st, s)))
+        break;
+      k_lm_errors<<<n, 256, smem, s>>>(C, n, d_obs + (size_t)p0 * nf, d_syn, d_jac, d_mout, d_w, c->d_coef64,
+                                       d_err + (size_t)p0 * nm, d_chi2 + p0);
+      rc = cuda_fail(cudaGetLastError());
+    }
+    if (!rc) rc = cuda_fail(cudaStreamSynchronize(s));
+  } while (false);
+  cudaFree(d_w);
+  cudaFree(d_syn);
+  cudaFree(d_jac);
+  cudaFree(d_mout);
+  cudaFree(d_st);
+  return rc;
+}
+
+int fz_errors(fz_ctx* c, int npix, const double* obs, const float* models, int hydrostatic, const fz_lm_opts* opts,
+              float* err, double* chi2, int* status) {
+  if (!c || npix <= 0 || !obs || !models || !err || !chi2) return FZ_ERR_ARG;
+  FZ_CK(cudaSetDevice(c->device));
+  const size_t nf = 4 * (size_t)c->numw, nm = 13 * (size_t)c->nz;
+  cudaStream_t s = c->stream;
+  double *d_obs = nullptr, *d_chi = nullptr;
+  float *d_m = nullptr, *d_err = nullptr;
+  int* d_st = nullptr;
+  int rc = 0;
+  do {
+    if ((rc = cuda_fail(cudaMalloc(&d_obs, npix * nf * sizeof(double))))) break;
+    if ((rc = cuda_fail(cudaMalloc(&d_m, npix * nm * sizeof(float))))) break;
+    if ((rc = cuda_fail(cudaMalloc(&d_err, npix * nm * sizeof(float))))) break;
+    if ((rc = cuda_fail(cudaMalloc(&d_chi, npix * sizeof(double))))) break;
+    if ((rc = cuda_fail(cudaMalloc(&d_st, npix * sizeof(int))))) break;
+    if ((rc = cuda_fail(cudaMemcpyAsync(d_obs, obs, npix * nf * sizeof(double), cudaMemcpyHostToDevice, s)))) break;
+    if ((rc = cuda_fail(cudaMemcpyAsync(d_m, models, npix * nm * sizeof(float), cudaMemcpyHostToDevice, s)))) break;
+    if ((rc = fz_errors_device(c, npix, d_obs, d_m, hydrostatic, opts, d_err, d_chi, d_st, s))) break;
+    if ((rc = cuda_fail(cudaMemcpyAsync(err, d_err, npix * nm * sizeof(float), cudaMemcpyDeviceToHost, s)))) break;
+    if ((rc = cuda_fail(cudaMemcpyAsync(chi2, d_chi, npix * sizeof(double), cudaMemcpyDeviceToHost, s)))) break;
+    if (status &&
+        (rc = cuda_fail(cudaMemcpyAsync(status, d_st, npix * sizeof(int), cudaMemcpyDeviceToHost, s))))
+      break;
+    rc = cuda_fail(cudaStreamSynchronize(s));
+  } while (false);
+  cudaFree(d_obs);
+  cudaFree(d_m);
+  cudaFree(d_err);
+  cudaFree(d_chi);
+  cudaFree(d_st);
+  return rc;
+}
+
 int fz_smooth(fz_ctx* c, int nx, int ny, float* models, const int* params) {
   if (!c || nx <= 0 || ny <= 0 || !models) return FZ_ERR_ARG;
   FZ_CK(cudaSetDevice(c->device));

@@ -573,6 +573,120 @@ __global__ void __launch_bounds__(128) k_lm_update(LMConf C, LMSlots Sl, const d
   }
 }
 
+// One CTA per pixel: the errors mode (GET_ERROR_1D, src/get_dmodel.f90:1248-
+// 1287, with NEW_SOLVE_ERRORS :1291-1323).  chi2 of the model's synthesis
+// (NEW_CALCULATE_CHI2 :960-983, penalties included under regularisation),
+// the diagonal of H = Jn^T Jn of the normalised Jacobian (NORMALIZE_JACOB,
+// FP64 over the REAL*4 EQVDSYN), per node sigma_i = sqrt((chi2/INU)/H_ii)
+// (1e32 where H_ii <= 1e-32), then REARANGE_DA_MODEL in its errors form on a
+// zeroed model (:1877-1883: limits 0 and 1e20; the clip of SORT_DELTA at
+// PARAM_NORM * MPERT since the zero model's node averages are 0; the T taper
+// reads log tau5 = 0 and so leaves the profile alone).  err: MODEL(NZ,13),
+// rows of fixed parameters zero, as ESPLIT_MODEL3D receives it (:291-334).
+// Dynamic shared memory: nz doubles + nz floats.
+__global__ void __launch_bounds__(256) k_lm_errors(LMConf C, int n, const double* __restrict__ obs,
+                                                   const double* __restrict__ syn, const float* __restrict__ jac,
+                                                   const float* __restrict__ model, const double* __restrict__ w,
+                                                   const double* __restrict__ coef, float* __restrict__ err,
+                                                   double* __restrict__ chi_out) {
+  extern __shared__ double sm_err[];
+  __shared__ double red[8];
+  __shared__ double xs[LM_MAXNP], pr[LM_MAXNP], hd[LM_MAXNP], itd[LM_MAXNP], csum[LM_MAXNP];
+  __shared__ double nume;
+  const int p = blockIdx.x;
+  if (p >= n) return;
+  const int nf = C.nfreq, np = C.np, nz = C.nz, nm = 13 * nz;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
+  const double* o = obs + (size_t)p * nf;
+  const double* sy = syn + (size_t)p * nf;
+  double e = 0.0;
+  for (int i = threadIdx.x; i < nf; i += blockDim.x) {
+    const double d = o[i] - sy[i];
+    e += d * d * w[i];
+  }
+  double chi = block_sum_d(e, red) / C.inu;
+  if (C.reg) {
+    const float* m = model + (size_t)p * nm;
+    if (threadIdx.x < np) xs[threadIdx.x] = lm_node_value(C, m, coef, threadIdx.x);
+    __syncthreads();
+    if (threadIdx.x < np) pr[threadIdx.x] = lm_pen_res(C, xs, threadIdx.x);
+    __syncthreads();
+    double pp = 0.0;
+    for (int j = 0; j < np; ++j) pp += pr[j] * pr[j];
+    chi += pp;
+  }
+  // H_ii: one warp per node, FP64 sums over the frequencies
+  const float* J = jac + (size_t)p * np * nf;
+  const double rin = 1.0 / sqrt(C.inu);
+  for (int j = warp; j < np; j += nwarp) {
+    double h = 0.0;
+    for (int f = lane; f < nf; f += 32) {
+      const double t = (double)J[(size_t)j * nf + f] * (sqrt(w[f]) * rin) * C.norm[j];
+      h += t * t;
+    }
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) h += __shfl_xor_sync(0xffffffffu, h, off);
+    if (lane == 0) hd[j] = h;
+  }
+  if (threadIdx.x == 0) {
+    chi_out[p] = chi;
+    nume = chi / C.inu;
+  }
+  __syncthreads();
+  double* nzp = sm_err;                                  // nz
+  float* pert = reinterpret_cast<float*>(nzp + nz);      // nz
+  float* out = err + (size_t)p * nm;
+  for (int i = threadIdx.x; i < nm; i += blockDim.x) out[i] = 0.0f;
+  __syncthreads();
+  const double MPERT = 0.15;
+  int j0 = 0;
+  for (int rp = 1; rp <= 8; ++rp) {
+    const int nj = C.nodes_ref[rp - 1];
+    if (nj <= 0) continue;
+    const int row = C.row_of[j0];
+    const double absl = c_lm_norm[rp - 1] * MPERT;
+    if (threadIdx.x < nj) {
+      const int j = j0 + threadIdx.x;
+      const double sig = hd[j] > 1.0e-32 ? sqrt(nume / hd[j]) : 1.0e32;
+      double cs = 0.0;
+      for (int k = 0; k < nz; ++k) cs += coef[k * np + j];
+      double t = sig * c_lm_norm[rp - 1];
+      if (fabs(t) > absl) t = t / fabs(t) * absl;
+      itd[threadIdx.x] = t;
+      csum[threadIdx.x] = cs;
+    }
+    __syncthreads();
+    // NZPERT = EXPAND(0 + ITDELTA) - 0
+    for (int k = threadIdx.x; k < nz; k += blockDim.x) {
+      double v = 0.0;
+      for (int j = 0; j < nj; ++j) v += itd[j] * coef[k * np + j0 + j];
+      nzp[k] = v;
+    }
+    __syncthreads();
+    // ITDELTA = CONTRACT(REAL(NZPERT))
+    if (threadIdx.x < nj) {
+      const int j = j0 + threadIdx.x;
+      double a = 0.0;
+      for (int k = 0; k < nz; ++k) a += (double)(float)nzp[k] * coef[k * np + j];
+      itd[threadIdx.x] = a / csum[threadIdx.x];
+    }
+    __syncthreads();
+    // NZPERT = EXPAND(ITDELTA), limits [0, 1e20] on 0 + NZPERT
+    for (int k = threadIdx.x; k < nz; k += blockDim.x) {
+      double v = 0.0;
+      for (int j = 0; j < nj; ++j) v += itd[j] * coef[k * np + j0 + j];
+      const float op = (float)v;
+      if (op < 0.0f) v = 0.0;
+      if (op > 1.0e20f) v = 1.0e20;
+      pert[k] = (float)v;
+    }
+    __syncthreads();
+    for (int k = threadIdx.x; k < nz; k += blockDim.x) out[row * nz + k] = pert[k];
+    __syncthreads();
+    j0 += nj;
+  }
+}
+
 // One block of 1024 threads: destination of every occupied slot when the
 // pool is compacted (exclusive scan of the occupancy flags), and their count.
 __global__ void __launch_bounds__(1024) k_lm_scan(int S, const int* __restrict__ pix, int* __restrict__ dest,

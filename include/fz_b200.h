@@ -267,6 +267,22 @@ int fz_invert_cycles_device(fz_ctx* ctx, int nx, int ny, const double* d_obs, fl
                             const int* nodes, int hydrostatic, const fz_lm_opts* opts, double* d_chi2, int* d_iters,
                             int* d_status, void* stream);
 
+/* The errors mode (GET_ERRORS3DS / GET_ERROR_1D / NEW_SOLVE_ERRORS,
+ * src/get_dmodel.f90:1248-1323, :1581-1703), replacing the per-pixel worker
+ * loop: for the models (usually the inversion's best), with the node layout
+ * of fz_rf_nodes, the synthesis and node Jacobian, chi2 (as
+ * NEW_CALCULATE_CHI2; the penalties of opts->reg_* included), per node
+ * sigma_i = sqrt((chi2 / NFREQ) / H_ii) with H = Jn^T Jn the normalised
+ * Jacobian's Gram diagonal, mapped to heights by REARANGE_DA_MODEL's errors
+ * branch (limits [0, 1e20], node values clipped at 0.15 PARAM_NORM).
+ * err: MODEL(NZ,13,npix), the rows of parameters without nodes zero (the
+ * E*3D cubes of ESPLIT_MODEL3D); chi2 (npix); status may be NULL.  opts
+ * supplies isigma, wstk and reg_*; the LM fields are unused. */
+int fz_errors_device(fz_ctx* ctx, int npix, const double* d_obs, const float* d_models, int hydrostatic,
+                     const fz_lm_opts* opts, float* d_err, double* d_chi2, int* d_status, void* stream);
+int fz_errors(fz_ctx* ctx, int npix, const double* obs, const float* models, int hydrostatic, const fz_lm_opts* opts,
+              float* err, double* chi2, int* status);
+
 /* Batched GET_PERTURBATION (src/lm.f90:137-204, SOLVER_METHOD = 1) on host
  * buffers: for each pixel H = J^T J (tensor cores, split-bf16 x3, FP32
  * accumulation), g = J^T diff, (H + lambda diag H)^+ g by an FP64 Jacobi SVD

@@ -324,3 +324,40 @@ def smoothing_b(models, nx, ny, params):
             a[:, :, 1:-1] = (a[:, :, 2:] + a[:, :, :-2] + a[:, :, 1:-1] * 2.0) / 4.0
         m[:, row, :] = a.reshape(nx * ny, nz).astype(np.float32)
     return m
+
+
+def errors_1d(obs, syn, jac, model, w, nodes, reg=None):
+    """GET_ERROR_1D (src/get_dmodel.f90:1248-1287) for one pixel: obs, syn
+    RSYN1D (NFREQ,); jac EQVDSYN (NFREQ, NP) REAL*4 of model (13, NZ); reg =
+    (pen_typ, pen_alp) adds the current model's penalties to chi2 as
+    NEW_CALCULATE_CHI2 does (:966-983).  NEW_SOLVE_ERRORS (:1291-1323):
+    NUME = chi2 / INU, H = HESSIAN of the normalised Jacobian, sigma_i =
+    sqrt(NUME / H_ii) where H_ii > 1e-32, else 1e32 (its GET_INVERSE_COV
+    result is unused).  LIMIT_PERTURBATION with ERRORS on MODEL = 0:
+    REARANGE_DA_MODEL's errors limits LOWLIM = 0, UPPLIM = 1e20 (:1877-1883).
+    Returns (err (13, NZ) REAL*4, chi2)."""
+    inu = float(obs.size)
+    chi = float(np.sum((obs - syn) ** 2 * w) / inu)
+    if reg is not None:
+        pen, _ = it_penalties(model, nodes, *reg)
+        chi += float(np.sum(pen * pen))
+    jn = normalize_jacob(jac, w, inu, nodes)
+    hd = np.einsum("fi,fi->i", jn, jn)
+    nume = chi / inu
+    sig = np.where(hd > 1.0e-32, np.sqrt(nume / np.where(hd > 0, hd, 1.0)), 1.0e32)
+    nz = model.shape[1]
+    err = np.zeros((13, nz), dtype=np.float32)
+    j0 = 0
+    for p in range(1, 9):
+        nj = nodes.get(p, 0)
+        if nj <= 0:
+            continue
+        row = ATMPOS[p]
+        coefs = int_coefs(nz, nj)
+        pert, _ = sort_delta(sig[j0:j0 + nj], PARAM_NORMS[p - 1], err[row], 0.0, 1.0e20, coefs,
+                             PARAM_NORMS[p - 1] * MPERT)
+        # the T taper reads log tau5 of the zeroed model: 0 lies inside
+        # (-11.5, 0.5], so the profile is kept
+        err[row] = (pert + err[row]).astype(np.float32)
+        j0 += nj
+    return err, chi

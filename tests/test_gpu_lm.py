@@ -228,3 +228,43 @@ def test_inversion_cycles_match_oracle(fz, orc):
     ratio = np.median(chi / ochi)
     assert 0.5 <= ratio <= 2.0, (chi, ochi)
     assert ctx.np == 13
+
+
+@pytest.mark.parametrize("case", ["noisy_true", "offset_guess", "regularised"])
+def test_errors_match_oracle(fz, orc, case):
+    """The errors mode (GET_ERROR_1D) against the oracle on the oracle's own
+    synthesis and node Jacobian of the same models: chi2 within 1e-4
+    relative (the two syntheses agree to ~1e-5 of I; with noise-sized
+    residuals chi2 moves by a few 1e-6), the height errors within 2e-4
+    relative (the FP32 response functions of the two sides differ by ~1e-5;
+    sigma goes as (chi2 / H_ii)^1/2).
+    noisy_true: the true models against observations with 1e-3 Ic noise
+    (chi2 ~ 1, unclipped sigmas); offset_guess: a 200 K offset guess (sigmas
+    clipped at 0.15 PARAM_NORM); regularised: first-difference penalties on
+    T and v_z add to chi2."""
+    nz, npix = 40, 24
+    lines, reg, g, ctx = _ctx(fz, orc, nz)
+    true = fz.atmos.make_columns(npix, nz, seed=33)
+    obs, true_he, _ = orc.forward(lines, reg, g, true, hydrostatic=True)
+    rng = np.random.default_rng(4)
+    obs = obs + rng.normal(0.0, 1.0e-3, obs.shape)
+    models = true_he if case != "offset_guess" else lmcase.initial_guess(true_he, seed=2)
+    ctx.rf_nodes(lmcase.NODES)
+    opts = fz.LMOpts(isigma=1e-3)
+    regp = None
+    if case == "regularised":
+        opts = fz.LMOpts(isigma=1e-3, reg={1: (1, 0.5), 7: (1, 0.2)})
+        regp = ([1, 0, 0, 0, 0, 0, 1, 0], [0.5, 0, 0, 0, 0, 0, 0.2, 0])
+    err, chi, st = ctx.errors(obs, models, hydrostatic=True, opts=opts)
+    assert np.all(st == 0)
+    syn, jac, mo, ost = orc.forward_rf(lines, reg, g, models, lmcase.NODES, hydrostatic=True)
+    assert np.all(ost == 0)
+    w = lmo.weights(ctx.numw, isigma=1e-3)
+    for i in range(npix):
+        e_ref, c_ref = lmo.errors_1d(obs[i].reshape(-1), syn[i].reshape(-1), jac[i].T, mo[i], w, lmcase.NODES,
+                                     reg=regp)
+        np.testing.assert_allclose(chi[i], c_ref, rtol=1e-4)
+        np.testing.assert_allclose(err[i], e_ref, rtol=2e-4, atol=0)
+    free = [0, 5, 6, 7, 10]
+    fixed = [r for r in range(13) if r not in free]
+    assert np.all(err[:, fixed] == 0) and np.all(err[:, free] > 0)

@@ -103,3 +103,24 @@ def test_it_penalties_operators():
     assert np.all(hss[:4, 4:] == 0) and np.all(hss[4:6, 6:] == 0)
     res0, hss0 = lmo.it_penalties(model, nodes, typ, [0.0] * 8)
     assert np.all(res0 == 0) and np.all(hss0 == 0)
+
+
+def test_errors_1d_analytic():
+    """GET_ERROR_1D with one T node and a Jacobian of known normalised
+    Gram diagonal: sigma = sqrt((chi2/INU) / H_11), the height profile is
+    that constant times PARAM_NORM (one node expands to a flat profile),
+    clipped at 0.15 PARAM_NORM; every other row is zero."""
+    nf, nz = 8, 6
+    w = np.full(nf, 4.0)
+    obs = np.zeros(nf)
+    syn = np.full(nf, 0.5)                     # chi2 = sum(0.25 * 4) / 8 = 1
+    for scale, expect in ((1.0e-3, None), (1.0e-6, 0.15 * 6000.0)):
+        jac = np.full((nf, 1), scale, dtype=np.float32)
+        model = np.zeros((13, nz), dtype=np.float32)
+        err, chi = lmo.errors_1d(obs, syn, jac, model, w, {1: 1})
+        assert chi == pytest.approx(1.0)
+        jn = np.float64(np.float32(scale)) * np.sqrt(4.0) / np.sqrt(nf) * 6000.0
+        sigma = np.sqrt((1.0 / nf) / (nf * jn * jn)) * 6000.0
+        want = min(sigma, 0.15 * 6000.0) if expect is None else expect
+        np.testing.assert_allclose(err[0], want, rtol=1e-6)
+        assert np.all(err[1:] == 0)
