@@ -400,7 +400,43 @@ def main():
     errors["default_guess"] = height_errors(base[:1].expand(tru_c.shape[0], -1, -1), tru_c)
     errors["heights_compared_per_pixel"] = float(((tru_c[:, 11] >= -3.0) & (tru_c[:, 11] <= 0.0)).sum()
                                                  / tru_c.shape[0])
-    del outs
+
+    # ------------------------------------------------------------ errors mode
+    # GET_ERROR_1D for the headline arm's inverted models of one tile: the
+    # node Jacobian of each model, chi2 and sigma = sqrt(chi2/NFREQ / H_ii)
+    # mapped to heights (fz_errors_device)
+    k0 = common[0]
+    e_m = torch.empty((a.tile, 13, a.nz), dtype=torch.float32, device="cuda")
+    e_c = torch.empty(a.tile, dtype=torch.float64, device="cuda")
+    e_s = torch.empty(a.tile, dtype=torch.int32, device="cuda")
+
+    def err_call():
+        ctx.errors_device(a.tile, obs[k0 * a.tile:(k0 + 1) * a.tile].data_ptr(), outs[("nn", k0)].data_ptr(),
+                          e_m.data_ptr(), e_c.data_ptr(), e_s.data_ptr(), hydrostatic=True, opts=opts,
+                          stream=stream)
+
+    # the warm-up call in an NVTX range: a profiler can pick its launches,
+    # whose k_synth_rf lists every column of the chunk
+    torch.cuda.nvtx.range_push("errors_mode")
+    err_call()
+    torch.cuda.synchronize()
+    torch.cuda.nvtx.range_pop()
+    ee0, ee1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ee0.record()
+    for _ in range(2):
+        err_call()
+    ee1.record()
+    torch.cuda.synchronize()
+    ms_err = maxms(ee0.elapsed_time(ee1) / 2)
+    tru0 = true_models[k0 * a.tile:(k0 + 1) * a.tile]
+    msk0 = (tru0[:, 11] >= -3.0) & (tru0[:, 11] <= 0.0)
+    errors_mode = {"value": world * a.tile / (ms_err * 1e-3), "unit": "pixels/s", "ms_per_call": ms_err,
+                   "workload": "%d inverted pixels (headline arm), NP = 13, %d heights, NFREQ %d: synthesis, "
+                               "node Jacobian, chi2, sigma per node, height errors" % (a.tile, a.nz, nf),
+                   "median_sigma_T_K": float(torch.median(e_m[:, 0][msk0])),
+                   "median_sigma_vz_km_s": float(torch.median(e_m[:, 10][msk0])) * 1e-5,
+                   "status_errors": int(e_s.max().item())}
+    del outs, e_m, e_c, e_s
 
     # ------------------------------------------------------------- end to end
     # host buffers in pinned memory: observations and goals in, models,
@@ -564,6 +600,7 @@ def main():
                                            "log tau5 is in [-3, 0], over the compared pixels"),
            "synthesis": synthesis,
            "rf_full": rf_full,
+           "errors_mode": errors_mode,
            "roofline": {"bound": "hbm", "kernel": kname, "achieved": achieved, "peak": hbm, "unit": "GB/s",
                         "frac": achieved / hbm, "traffic": traffic,
                         "peak_source": how + " (MEASURED_PEAKS.json hbm_gbs)" if how == "measured" else how,
