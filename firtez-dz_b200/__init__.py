@@ -131,6 +131,19 @@ def lib():
         L.fz_invert_cycles_device.argtypes = [P, ctypes.c_int, ctypes.c_int, P, P, ctypes.c_int, P, ctypes.c_int, P,
                                               P, P, P, P]
         L.fz_errors.argtypes = [P, ctypes.c_int, P, P, ctypes.c_int, P, P, P, P]
+        I, S = ctypes.c_int, ctypes.c_char_p
+        L.fz_v3_header.argtypes = [S, P, P, P, P]
+        L.fz_v3_read_model.argtypes = [S, I, I, I, P]
+        L.fz_v3_write_model.argtypes = [S, I, I, I, P]
+        L.fz_v3_read_profiles.argtypes = [S, I, I, I, P, P, P]
+        L.fz_v3_write_profiles.argtypes = [S, I, I, I, P, P, P]
+        L.fz_v3_write_rfs.argtypes = [S, I, I, I, I, P, P, P, P, P]
+        L.fz_v3_read_rfs.argtypes = [S, I, I, I, I, P, P, P, P, P]
+        L.fz_model_from_v3_device.argtypes = [I, I, I, P, P, P]
+        L.fz_model_to_v3_device.argtypes = [I, I, I, P, P, P, P, P]
+        L.fz_obs_from_v3_device.argtypes = [I, I, P, P, P]
+        L.fz_syn_to_v3_device.argtypes = [I, I, P, P, P]
+        L.fz_rf_to_v3_device.argtypes = [I, I, I, P, P, P]
         L.fz_errors_device.argtypes = [P, ctypes.c_int, P, P, ctypes.c_int, P, P, P, P, P]
         L.fz_autotune_forward.argtypes = [P, ctypes.c_int, P, ctypes.c_int, P]
         L.fz_autotune_lm.argtypes = [P, ctypes.c_int, P, P, P, ctypes.c_int, P, P, ctypes.c_int, P]

@@ -1765,6 +1765,111 @@ __global__ void k_smooth_pass(int nx, int ny, int nz, int nrow, int dir, const i
   }
 }
 
+// ------------------------------------------------------------ v3 layouts
+// Cube of the v3 model file feeding each MODEL row (-1: vx, vy, zero; the
+// file has no cube for them): JOIN_MODEL2 (src/forward.f90:363-405) over the
+// cubes of READ_MODEL_3D (src/misc.f90:459-491).
+__constant__ int c_v3_cube_of_row[13] = {0, 1, 2, 7, 8, 3, 4, 5, -1, -1, 6, 9, 12};
+// MODEL row written into each of the first ten cubes (WRITE_MODEL3D_V3)
+__constant__ int c_v3_row_of_cube[10] = {0, 1, 2, 5, 6, 7, 10, 3, 4, 11};
+
+// One thread per model value, heights fastest on both sides (every cube and
+// every model row is a contiguous run of nz values per pixel).
+__global__ void k_model_from_v3(int npix, int nz, const float* __restrict__ cubes, float* __restrict__ model) {
+  const size_t total = (size_t)npix * 13 * nz, cube = (size_t)npix * nz;
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (size_t)gridDim.x * blockDim.x) {
+    const int k = (int)(i % nz);
+    const size_t pr = i / nz;
+    const int row = (int)(pr % 13);
+    const size_t p = pr / 13;
+    const int c = c_v3_cube_of_row[row];
+    float v = 0.0f;
+    if (c == 12)
+      v = cubes[12 * cube + k];   // ZZ: the first pixel's z column
+    else if (c >= 0)
+      v = cubes[(size_t)c * cube + p * nz + k];
+    model[i] = v;
+  }
+}
+
+__global__ void k_model_to_v3(int ny, int npix, int nz, const float* __restrict__ model, const double* __restrict__ x,
+                              const double* __restrict__ y, float* __restrict__ cubes) {
+  const size_t cube = (size_t)npix * nz, total = 13 * cube;
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (size_t)gridDim.x * blockDim.x) {
+    const int c = (int)(i / cube);
+    const size_t r = i % cube;
+    const size_t p = r / nz;
+    const int k = (int)(r % nz);
+    float v;
+    if (c < 10)
+      v = model[(p * 13 + c_v3_row_of_cube[c]) * nz + k];
+    else if (c == 10)
+      v = (float)x[p / ny];
+    else if (c == 11)
+      v = (float)y[p % ny];
+    else
+      v = model[(p * 13 + 12) * nz + k];
+    cubes[i] = v;
+  }
+}
+
+// STOKES(4,NW,npix) REAL*4 <-> OBS3D/RSYN1D(4*NW,npix) REAL*8 (Stokes-major
+// blocks): one thread per (pixel, wavelength), its four Stokes values.
+__global__ void k_obs_from_v3(int npix, int nw, const float* __restrict__ st, double* __restrict__ obs) {
+  const size_t total = (size_t)npix * nw;
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (size_t)gridDim.x * blockDim.x) {
+    const size_t p = i / nw;
+    const int w = (int)(i % nw);
+    const float* s = st + 4 * i;
+    double* o = obs + p * 4 * nw + w;
+#pragma unroll
+    for (int q = 0; q < 4; ++q) o[(size_t)q * nw] = (double)s[q];
+  }
+}
+
+__global__ void k_syn_to_v3(int npix, int nw, const double* __restrict__ syn, float* __restrict__ st) {
+  const size_t total = (size_t)npix * nw;
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (size_t)gridDim.x * blockDim.x) {
+    const size_t p = i / nw;
+    const int w = (int)(i % nw);
+    const double* s = syn + p * 4 * nw + w;
+    float* o = st + 4 * i;
+#pragma unroll
+    for (int q = 0; q < 4; ++q) o[q] = (float)s[(size_t)q * nw];
+  }
+}
+
+// The RF payload of WRITE_RFS3D_V3 from fz_forward_rf_full's output: one
+// CTA per (pixel, height) stages the six parameters' NFREQ responses
+// (coalesced rows) in shared memory and writes them back parameter-fastest,
+// (parameter, Stokes, wavelength) per height (coalesced).  Dynamic shared
+// memory: 6 * 4 * nw floats.
+__global__ void __launch_bounds__(256) k_rf_to_v3(int nz, int nw, const float* __restrict__ rf,
+                                                  float* __restrict__ out) {
+  extern __shared__ float sm_rf[];
+  const int nf = 4 * nw;
+  const size_t p = blockIdx.x / nz;
+  const int k = (int)(blockIdx.x % nz);
+  for (int q = 0; q < 6; ++q) {
+    const float* src = rf + ((p * 6 + q) * nz + k) * nf;
+    for (int f = threadIdx.x; f < nf; f += blockDim.x) sm_rf[q * nf + f] = src[f];
+  }
+  __syncthreads();
+  float* dst = out + (p * nz + k) * (size_t)nf * 6;
+  for (int i = threadIdx.x; i < nf * 6; i += blockDim.x) {
+    const int q = i % 6, r = i / 6;   // r = w * 4 + s
+    const int w = r >> 2, s = r & 3;
+    dst[i] = sm_rf[q * nf + s * nw + w];
+  }
+}
+
+int grid_for(size_t n, int threads) {
+  int dev = 0, nsm = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+  return (int)std::max<size_t>(1, std::min<size_t>((n + threads - 1) / threads, (size_t)nsm * 16));
+}
+
 }  // namespace
 
 extern "C" {
@@ -1844,6 +1949,55 @@ int fz_invert_cycles_device(fz_ctx* c, int nx, int ny, const double* d_obs, floa
   cudaFree(d_best);
   cudaFree(d_syn);
   return rc;
+}
+
+int fz_model_from_v3_device(int nx, int ny, int nz, const float* d_cubes, float* d_model, void* stream) {
+  if (nx <= 0 || ny <= 0 || nz <= 0 || !d_cubes || !d_model) return FZ_ERR_ARG;
+  const int npix = nx * ny;
+  k_model_from_v3<<<grid_for((size_t)npix * 13 * nz, 256), 256, 0, (cudaStream_t)stream>>>(npix, nz, d_cubes,
+                                                                                              d_model);
+  return cuda_fail(cudaGetLastError());
+}
+
+int fz_model_to_v3_device(int nx, int ny, int nz, const float* d_model, const double* x, const double* y,
+                          float* d_cubes, void* stream) {
+  if (nx <= 0 || ny <= 0 || nz <= 0 || !d_model || !x || !y || !d_cubes) return FZ_ERR_ARG;
+  cudaStream_t s = (cudaStream_t)stream;
+  double* d_xy = nullptr;
+  FZ_CK(cudaMalloc(&d_xy, (size_t)(nx + ny) * sizeof(double)));
+  int rc = cuda_fail(cudaMemcpyAsync(d_xy, x, nx * sizeof(double), cudaMemcpyHostToDevice, s));
+  if (!rc) rc = cuda_fail(cudaMemcpyAsync(d_xy + nx, y, ny * sizeof(double), cudaMemcpyHostToDevice, s));
+  if (!rc) {
+    const int npix = nx * ny;
+    k_model_to_v3<<<grid_for((size_t)npix * 13 * nz, 256), 256, 0, s>>>(ny, npix, nz, d_model, d_xy, d_xy + nx,
+                                                                         d_cubes);
+    rc = cuda_fail(cudaGetLastError());
+  }
+  if (!rc) rc = cuda_fail(cudaStreamSynchronize(s));   // before the vectors are freed
+  cudaFree(d_xy);
+  return rc;
+}
+
+int fz_obs_from_v3_device(int npix, int nw, const float* d_stokes, double* d_obs, void* stream) {
+  if (npix <= 0 || nw <= 0 || !d_stokes || !d_obs) return FZ_ERR_ARG;
+  k_obs_from_v3<<<grid_for((size_t)npix * nw, 256), 256, 0, (cudaStream_t)stream>>>(npix, nw, d_stokes, d_obs);
+  return cuda_fail(cudaGetLastError());
+}
+
+int fz_syn_to_v3_device(int npix, int nw, const double* d_syn, float* d_stokes, void* stream) {
+  if (npix <= 0 || nw <= 0 || !d_syn || !d_stokes) return FZ_ERR_ARG;
+  k_syn_to_v3<<<grid_for((size_t)npix * nw, 256), 256, 0, (cudaStream_t)stream>>>(npix, nw, d_syn, d_stokes);
+  return cuda_fail(cudaGetLastError());
+}
+
+int fz_rf_to_v3_device(int npix, int nz, int nw, const float* d_rf, float* d_out, void* stream) {
+  if (npix <= 0 || nz <= 0 || nw <= 0 || !d_rf || !d_out) return FZ_ERR_ARG;
+  const size_t smem = (size_t)24 * nw * sizeof(float);
+  if (smem > 227 * 1024) return FZ_ERR_LIMIT;
+  if ((size_t)npix * nz > 0x7fffffffULL) return FZ_ERR_LIMIT;
+  if (smem > 48 * 1024) FZ_CK(cudaFuncSetAttribute(k_rf_to_v3, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  k_rf_to_v3<<<(unsigned)((size_t)npix * nz), 256, smem, (cudaStream_t)stream>>>(nz, nw, d_rf, d_out);
+  return cuda_fail(cudaGetLastError());
 }
 
 int fz_errors_device(fz_ctx* c, int npix, const double* d_obs, const float* d_models, int hydrostatic,

@@ -331,6 +331,64 @@ int fz_profile_read(fz_ctx* ctx, double* ms, int* launches, long long* items, in
  * FP32-pipe roofline of the synthesis kernel. */
 int fz_measure_fp32_peak(int device, double* tflops);
 
+/* ---------------------------------------------------------------- v3 files
+ * The model, profile and response-function files of src/misc.f90, as the
+ * Fortran host reads and writes them (READ_MODEL / READ_MODEL_3D :78-553,
+ * WRITE_MODEL3D_V3 :801-929, READ_PROFILE_3D :1338-1642,
+ * WRITE_PROFILES3D_V3 :1147-1249, WRITE_RFS3D_V3 :1862-1999): Fortran
+ * unformatted sequential records, REAL*4 payloads, a header record
+ * (3000+v, 3000-v, ID, NRECS, NDIMS, dims...), data records of at most
+ * 268,435,446 values.  Host functions (no GPU); the payload is moved as it
+ * lies in the file:
+ *   model cubes   (NZ,NY,NX) x 13 in file order: T, Pg, rho, Bx, By, Bz, vz,
+ *                 Pe, mu, log tau5, x, y, z
+ *   profiles      STOKES(4,NW,NY,NX)
+ *   RFs           DSTOKES(P,4,NW,NZ,NY,NX), P over the LOGV-flagged of
+ *                 T, Pg, rho, Bx, By, Bz, vz, P0
+ * The layout changes to MODEL(NZ,13,npix), OBS3D(NFREQ,npix) and the RF
+ * output of fz_forward_rf_full are the fz_*_v3_device kernels below.
+ * Errors: FZ_ERR_ARG (open/write failure, bad argument), FZ_ERR_PARSE (not
+ * such a file, or truncated), FZ_ERR_LIMIT (dimensions differ from the
+ * caller's). */
+int fz_v3_header(const char* path, int* id, int* version, int* ndims, int dims[8]);
+int fz_v3_read_model(const char* path, int nx, int ny, int nz, float* cubes);
+int fz_v3_write_model(const char* path, int nx, int ny, int nz, const float* cubes);
+int fz_v3_read_profiles(const char* path, int nx, int ny, int nw, float* ind /* NULL ok */, float* wave /* NULL ok */,
+                        float* stokes);
+int fz_v3_write_profiles(const char* path, int nx, int ny, int nw, const double* ind, const double* wave,
+                         const float* stokes);
+/* logv[8]: 1 for each of T, Pg, rho, Bx, By, Bz, vz, P0 present in data */
+int fz_v3_write_rfs(const char* path, int nx, int ny, int nz, int nw, const double* z, const int* logv,
+                    const double* ind, const double* wave, const float* data);
+/* Returns the number of parameters present (>= 0); with data NULL only the
+ * small records are read (call again with a buffer of that many
+ * parameters). */
+int fz_v3_read_rfs(const char* path, int nx, int ny, int nz, int nw, float* z, int* logv, float* ind, float* wave,
+                   float* data);
+
+/* Layout changes on the device (stream-ordered, no allocation except the
+ * x/y vectors of fz_model_to_v3_device):
+ *   fz_model_from_v3_device  cubes -> MODEL(NZ,13,NY*NX): T, Pg, rho, Pe, mu,
+ *       Bx, By, Bz, vx = vy = 0, vz, log tau5, and z = the first pixel's z
+ *       column for every pixel (JOIN_MODEL2, src/forward.f90:363-405, with
+ *       ZZ from READ_MODEL_3D's Z(:) = TMP(:,1,1))
+ *   fz_model_to_v3_device    MODEL -> cubes, x and y cubes REAL(X(ix)),
+ *       REAL(Y(iy)) from host vectors, z cube from each pixel's z row
+ *       (WRITE_MODEL3D_V3)
+ *   fz_obs_from_v3_device    STOKES(4,NW,NY,NX) REAL*4 -> OBS3D(4*NW,npix)
+ *       REAL*8, Stokes-major blocks (ALLOCATE_AND_READ, src/pre_post_duties.f90:421-431)
+ *   fz_syn_to_v3_device      RSYN1D(4*NW,npix) REAL*8 -> STOKES REAL*4
+ *       (WRITE_STOKES_PROFILES, src/pre_post_duties.f90:235-245)
+ *   fz_rf_to_v3_device       fz_forward_rf_full's (4*NW,NZ,6,npix) -> the
+ *       DSTOKES payload with LOGV = T, Pg, Bx, By, Bz, vz
+ *       (WRITE_RESPONSE_FUNCTIONS, src/pre_post_duties.f90:316-356) */
+int fz_model_from_v3_device(int nx, int ny, int nz, const float* d_cubes, float* d_model, void* stream);
+int fz_model_to_v3_device(int nx, int ny, int nz, const float* d_model, const double* x, const double* y,
+                          float* d_cubes, void* stream);
+int fz_obs_from_v3_device(int npix, int nw, const float* d_stokes, double* d_obs, void* stream);
+int fz_syn_to_v3_device(int npix, int nw, const double* d_syn, float* d_stokes, void* stream);
+int fz_rf_to_v3_device(int npix, int nz, int nw, const float* d_rf, float* d_out, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
