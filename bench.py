@@ -534,6 +534,80 @@ def main():
                                   "parameter's largest response; Stokes I 1e-5 relative, Q/U/V 1e-6 I_c"}
     del rfo, sor, mor
     torch.cuda.empty_cache()
+
+    # --------------------------------------------------------------- v3 files
+    # the reference's file formats around the path: the GPU layout changes of
+    # one tile (profile file payload -> OBS3D, synthesis -> profile payload,
+    # model-file cubes <-> MODEL) and of 1,024 columns of full-height RFs ->
+    # the RF file payload, timed with CUDA events (5 calls after one warm-up;
+    # bytes = what each kernel must read + write), and the host record I/O of
+    # a 16,384-pixel slice on a RAM-backed directory (wall clock)
+    from firtez_dz_b200 import v3io
+    nyv = 256
+    nxv = a.tile // nyv
+    tst = torch.zeros((nxv, nyv, numw, 4), dtype=torch.float32, device="cuda")
+    tob = torch.empty((a.tile, 4, numw), dtype=torch.float64, device="cuda")
+    tcu = torch.zeros((13, nxv, nyv, a.nz), dtype=torch.float32, device="cuda")
+    tmo = torch.empty((a.tile, 13, a.nz), dtype=torch.float32, device="cuda")
+    ncr = 1024
+    trf = torch.zeros((ncr, 6, a.nz, nf), dtype=torch.float32, device="cuda")
+    tro = torch.empty((ncr, 1, a.nz, numw, 4, 6), dtype=torch.float32, device="cuda")
+    xs, ys = np.arange(nxv) * 16.0, np.arange(nyv) * 16.0
+    layout = {
+        "obs_from_profile_file": (lambda: v3io.obs_from_stokes_device(tst, out=tob, stream=stream),
+                                  a.tile * numw * 4 * (4 + 8)),
+        "syn_to_profile_file": (lambda: v3io.stokes_from_syn_device(tob, nxv, nyv, out=tst, stream=stream),
+                                a.tile * numw * 4 * (8 + 4)),
+        "model_from_model_file": (lambda: v3io.model_from_cubes_device(tcu, out=tmo, stream=stream),
+                                  a.tile * 13 * a.nz * 4 * 2),
+        "model_to_model_file": (lambda: v3io.cubes_from_model_device(tmo, nxv, nyv, xs, ys, out=tcu, stream=stream),
+                                a.tile * 13 * a.nz * 4 * 2),
+        "rf_full_to_rf_file": (lambda: v3io.rf_file_layout_device(trf, ncr, 1, out=tro, stream=stream),
+                               ncr * 6 * a.nz * nf * 4 * 2),
+    }
+    hbm_pk, hbm_how = peaks()
+    v3_kernels = {}
+    for name, (fn, nbytes) in layout.items():
+        fn()
+        torch.cuda.synchronize()
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ev0.record()
+        for _ in range(5):
+            fn()
+        ev1.record()
+        torch.cuda.synchronize()
+        ms_k = maxms(ev0.elapsed_time(ev1) / 5)
+        v3_kernels[name] = {"ms": ms_k, "bytes": nbytes, "gbs": nbytes / (ms_k * 1e-3) / 1e9,
+                            "frac_hbm": nbytes / (ms_k * 1e-3) / 1e9 / hbm_pk}
+    v3_kernels["model_to_model_file"]["note"] = ("includes the copy of the x, y vectors to the device and the "
+                                                 "call's stream synchronisation")
+    del tst, tob, tcu, tmo, trf, tro
+    torch.cuda.empty_cache()
+    import tempfile
+    nsl = 16384
+    base_dir = "/dev/shm" if os.path.isdir("/dev/shm") else None
+    rng_v3 = np.random.default_rng(7)
+    h_st = rng_v3.standard_normal((nsl // nyv, nyv, numw, 4)).astype(np.float32)
+    h_cu = rng_v3.standard_normal((13, nsl // nyv, nyv, a.nz)).astype(np.float32)
+    host_io = {}
+    with tempfile.TemporaryDirectory(dir=base_dir) as td:
+        for kind, wr, rd, nbytes in (
+                ("profile", lambda f: v3io.write_profile(f, np.ones(numw), np.arange(numw, dtype=np.float64), h_st),
+                 v3io.read_profile, h_st.nbytes),
+                ("model", lambda f: v3io.write_model(f, h_cu), v3io.read_model, h_cu.nbytes)):
+            fn_ = os.path.join(td, kind + ".bin")
+            t0 = time.perf_counter()
+            wr(fn_)
+            t1 = time.perf_counter()
+            rd(fn_)
+            t2 = time.perf_counter()
+            host_io[kind] = {"bytes": nbytes, "write_mb_s": nbytes / (t1 - t0) / 1e6,
+                             "read_mb_s": nbytes / (t2 - t1) / 1e6}
+    v3_files = {"layout_kernels": v3_kernels, "peak_gbs": hbm_pk, "peak_source": hbm_how,
+                "workload": "one %d-pixel tile (%d x %d), NZ %d, NUMW %d; RFs: %d columns" % (a.tile, nxv, nyv,
+                                                                                              a.nz, numw, ncr),
+                "host_record_io": dict(host_io, slice_pixels=nsl, directory=base_dir or "tempfile default")}
+
     if rank != 0:
         ranks.close()
         return
@@ -601,6 +675,7 @@ def main():
            "synthesis": synthesis,
            "rf_full": rf_full,
            "errors_mode": errors_mode,
+           "v3_files": v3_files,
            "roofline": {"bound": "hbm", "kernel": kname, "achieved": achieved, "peak": hbm, "unit": "GB/s",
                         "frac": achieved / hbm, "traffic": traffic,
                         "peak_source": how + " (MEASURED_PEAKS.json hbm_gbs)" if how == "measured" else how,

@@ -1773,43 +1773,59 @@ __constant__ int c_v3_cube_of_row[13] = {0, 1, 2, 7, 8, 3, 4, 5, -1, -1, 6, 9, 1
 // MODEL row written into each of the first ten cubes (WRITE_MODEL3D_V3)
 __constant__ int c_v3_row_of_cube[10] = {0, 1, 2, 5, 6, 7, 10, 3, 4, 11};
 
-// One thread per model value, heights fastest on both sides (every cube and
-// every model row is a contiguous run of nz values per pixel).
-__global__ void k_model_from_v3(int npix, int nz, const float* __restrict__ cubes, float* __restrict__ model) {
-  const size_t total = (size_t)npix * 13 * nz, cube = (size_t)npix * nz;
-  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (size_t)gridDim.x * blockDim.x) {
-    const int k = (int)(i % nz);
-    const size_t pr = i / nz;
-    const int row = (int)(pr % 13);
-    const size_t p = pr / 13;
-    const int c = c_v3_cube_of_row[row];
-    float v = 0.0f;
-    if (c == 12)
-      v = cubes[12 * cube + k];   // ZZ: the first pixel's z column
-    else if (c >= 0)
-      v = cubes[(size_t)c * cube + p * nz + k];
-    model[i] = v;
+// One warp per (pixel, model row) or (cube, pixel): both sides hold the
+// row as a contiguous run of nz values, moved as float4 when nz is a
+// multiple of 4 and both bases are 16-byte aligned (vec), else as floats.
+__device__ __forceinline__ void warp_copy(const float* __restrict__ src, float* __restrict__ dst, int nz, bool vec,
+                                          int lane) {
+  if (vec) {
+    const float4* s4 = reinterpret_cast<const float4*>(src);
+    float4* d4 = reinterpret_cast<float4*>(dst);
+    for (int i = lane; i < (nz >> 2); i += 32) d4[i] = s4[i];
+  } else {
+    for (int i = lane; i < nz; i += 32) dst[i] = src[i];
   }
 }
 
-__global__ void k_model_to_v3(int ny, int npix, int nz, const float* __restrict__ model, const double* __restrict__ x,
-                              const double* __restrict__ y, float* __restrict__ cubes) {
-  const size_t cube = (size_t)npix * nz, total = 13 * cube;
-  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (size_t)gridDim.x * blockDim.x) {
-    const int c = (int)(i / cube);
-    const size_t r = i % cube;
-    const size_t p = r / nz;
-    const int k = (int)(r % nz);
-    float v;
-    if (c < 10)
-      v = model[(p * 13 + c_v3_row_of_cube[c]) * nz + k];
-    else if (c == 10)
-      v = (float)x[p / ny];
+__device__ __forceinline__ void warp_fill(float v, float* __restrict__ dst, int nz, bool vec, int lane) {
+  if (vec) {
+    float4* d4 = reinterpret_cast<float4*>(dst);
+    for (int i = lane; i < (nz >> 2); i += 32) d4[i] = make_float4(v, v, v, v);
+  } else {
+    for (int i = lane; i < nz; i += 32) dst[i] = v;
+  }
+}
+
+__global__ void k_model_from_v3(int npix, int nz, bool vec, const float* __restrict__ cubes,
+                                float* __restrict__ model) {
+  const int lane = threadIdx.x & 31, wpb = blockDim.x >> 5;
+  const size_t cube = (size_t)npix * nz, pairs = (size_t)npix * 13;
+  for (size_t pr = (size_t)blockIdx.x * wpb + (threadIdx.x >> 5); pr < pairs; pr += (size_t)gridDim.x * wpb) {
+    const int row = (int)(pr % 13);
+    const size_t p = pr / 13;
+    const int c = c_v3_cube_of_row[row];
+    float* dst = model + pr * nz;
+    if (c < 0)
+      warp_fill(0.0f, dst, nz, vec, lane);
+    else   // the z row: ZZ, the first pixel's z column
+      warp_copy(c == 12 ? cubes + 12 * cube : cubes + (size_t)c * cube + p * nz, dst, nz, vec, lane);
+  }
+}
+
+__global__ void k_model_to_v3(int ny, int npix, int nz, bool vec, const float* __restrict__ model,
+                              const double* __restrict__ x, const double* __restrict__ y, float* __restrict__ cubes) {
+  const int lane = threadIdx.x & 31, wpb = blockDim.x >> 5;
+  const size_t pairs = (size_t)npix * 13;
+  for (size_t cp = (size_t)blockIdx.x * wpb + (threadIdx.x >> 5); cp < pairs; cp += (size_t)gridDim.x * wpb) {
+    const int c = (int)(cp / npix);
+    const size_t p = cp % npix;
+    float* dst = cubes + cp * nz;
+    if (c == 10)
+      warp_fill((float)x[p / ny], dst, nz, vec, lane);
     else if (c == 11)
-      v = (float)y[p % ny];
+      warp_fill((float)y[p % ny], dst, nz, vec, lane);
     else
-      v = model[(p * 13 + 12) * nz + k];
-    cubes[i] = v;
+      warp_copy(model + (p * 13 + (c < 10 ? c_v3_row_of_cube[c] : 12)) * nz, dst, nz, vec, lane);
   }
 }
 
@@ -1840,26 +1856,26 @@ __global__ void k_syn_to_v3(int npix, int nw, const double* __restrict__ syn, fl
 }
 
 // The RF payload of WRITE_RFS3D_V3 from fz_forward_rf_full's output: one
-// CTA per (pixel, height) stages the six parameters' NFREQ responses
-// (coalesced rows) in shared memory and writes them back parameter-fastest,
-// (parameter, Stokes, wavelength) per height (coalesced).  Dynamic shared
-// memory: 6 * 4 * nw floats.
-__global__ void __launch_bounds__(256) k_rf_to_v3(int nz, int nw, const float* __restrict__ rf,
-                                                  float* __restrict__ out) {
-  extern __shared__ float sm_rf[];
+// thread per (pixel, height, wavelength, Stokes) gathers the six parameters'
+// responses (for a warp: four Stokes rows, 8 consecutive wavelengths each)
+// and stores them as one run of six floats (a warp: 768 contiguous bytes).
+__global__ void k_rf_to_v3(int npix, int nz, int nw, const float* __restrict__ rf, float* __restrict__ out) {
   const int nf = 4 * nw;
-  const size_t p = blockIdx.x / nz;
-  const int k = (int)(blockIdx.x % nz);
-  for (int q = 0; q < 6; ++q) {
-    const float* src = rf + ((p * 6 + q) * nz + k) * nf;
-    for (int f = threadIdx.x; f < nf; f += blockDim.x) sm_rf[q * nf + f] = src[f];
-  }
-  __syncthreads();
-  float* dst = out + (p * nz + k) * (size_t)nf * 6;
-  for (int i = threadIdx.x; i < nf * 6; i += blockDim.x) {
-    const int q = i % 6, r = i / 6;   // r = w * 4 + s
+  const size_t total = (size_t)npix * nz * nf;
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (size_t)gridDim.x * blockDim.x) {
+    const int r = (int)(i % nf);   // w * 4 + s
+    const size_t pk = i / nf;      // p * nz + k
+    const size_t p = pk / nz;
+    const int k = (int)(pk % nz);
     const int w = r >> 2, s = r & 3;
-    dst[i] = sm_rf[q * nf + s * nw + w];
+    const float* src = rf + (p * 6 * nz + k) * nf + s * nw + w;
+    float v[6];
+#pragma unroll
+    for (int q = 0; q < 6; ++q) v[q] = src[(size_t)q * nz * nf];
+    float2* d = reinterpret_cast<float2*>(out + i * 6);
+    d[0] = make_float2(v[0], v[1]);
+    d[1] = make_float2(v[2], v[3]);
+    d[2] = make_float2(v[4], v[5]);
   }
 }
 
@@ -1954,7 +1970,8 @@ int fz_invert_cycles_device(fz_ctx* c, int nx, int ny, const double* d_obs, floa
 int fz_model_from_v3_device(int nx, int ny, int nz, const float* d_cubes, float* d_model, void* stream) {
   if (nx <= 0 || ny <= 0 || nz <= 0 || !d_cubes || !d_model) return FZ_ERR_ARG;
   const int npix = nx * ny;
-  k_model_from_v3<<<grid_for((size_t)npix * 13 * nz, 256), 256, 0, (cudaStream_t)stream>>>(npix, nz, d_cubes,
+  const bool vec = (nz & 3) == 0 && ((uintptr_t)d_cubes & 15) == 0 && ((uintptr_t)d_model & 15) == 0;
+  k_model_from_v3<<<grid_for((size_t)npix * 13 * 32, 256), 256, 0, (cudaStream_t)stream>>>(npix, nz, vec, d_cubes,
                                                                                               d_model);
   return cuda_fail(cudaGetLastError());
 }
@@ -1969,8 +1986,9 @@ int fz_model_to_v3_device(int nx, int ny, int nz, const float* d_model, const do
   if (!rc) rc = cuda_fail(cudaMemcpyAsync(d_xy + nx, y, ny * sizeof(double), cudaMemcpyHostToDevice, s));
   if (!rc) {
     const int npix = nx * ny;
-    k_model_to_v3<<<grid_for((size_t)npix * 13 * nz, 256), 256, 0, s>>>(ny, npix, nz, d_model, d_xy, d_xy + nx,
-                                                                         d_cubes);
+    const bool vec = (nz & 3) == 0 && ((uintptr_t)d_model & 15) == 0 && ((uintptr_t)d_cubes & 15) == 0;
+    k_model_to_v3<<<grid_for((size_t)npix * 13 * 32, 256), 256, 0, s>>>(ny, npix, nz, vec, d_model, d_xy,
+                                                                         d_xy + nx, d_cubes);
     rc = cuda_fail(cudaGetLastError());
   }
   if (!rc) rc = cuda_fail(cudaStreamSynchronize(s));   // before the vectors are freed
@@ -1992,11 +2010,8 @@ int fz_syn_to_v3_device(int npix, int nw, const double* d_syn, float* d_stokes, 
 
 int fz_rf_to_v3_device(int npix, int nz, int nw, const float* d_rf, float* d_out, void* stream) {
   if (npix <= 0 || nz <= 0 || nw <= 0 || !d_rf || !d_out) return FZ_ERR_ARG;
-  const size_t smem = (size_t)24 * nw * sizeof(float);
-  if (smem > 227 * 1024) return FZ_ERR_LIMIT;
-  if ((size_t)npix * nz > 0x7fffffffULL) return FZ_ERR_LIMIT;
-  if (smem > 48 * 1024) FZ_CK(cudaFuncSetAttribute(k_rf_to_v3, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  k_rf_to_v3<<<(unsigned)((size_t)npix * nz), 256, smem, (cudaStream_t)stream>>>(nz, nw, d_rf, d_out);
+  if (((uintptr_t)d_out & 7) != 0) return FZ_ERR_ARG;   // float2 stores
+  k_rf_to_v3<<<grid_for((size_t)npix * nz * 4 * nw, 256), 256, 0, (cudaStream_t)stream>>>(npix, nz, nw, d_rf, d_out);
   return cuda_fail(cudaGetLastError());
 }
 
