@@ -34,7 +34,7 @@ TEM, PG, RHO, PEL, MW, BX, BY, BZ, VX, VY, VZ, TAU5, ZZ = range(13)
 
 FZ_OK, FZ_CHEM_NOCONV, FZ_NAN = 0, 1, 2
 KERNELS = ("k_chain", "k_opac", "k_synth", "k_opac_rf", "k_synth_rf", "k_lm_fill", "k_lm_accept", "k_lm_normal",
-           "k_lm_solve", "k_lm_update", "k_chemder", "k_rf_prop")
+           "k_lm_solve", "k_lm_update", "k_chemder", "k_rf_prop", "k_lsf")
 
 # free-parameter indices of the reference (atm_param.f90 order, 1-based) that
 # carry response functions
@@ -140,6 +140,11 @@ def lib():
         L.fz_v3_write_rfs.argtypes = [S, I, I, I, I, P, P, P, P, P]
         L.fz_v3_read_rfs.argtypes = [S, I, I, I, I, P, P, P, P, P]
         L.fz_model_from_v3_device.argtypes = [I, I, I, P, P, P]
+        L.fz_v3_read_lsf.argtypes = [S, I, P]
+        L.fz_v3_write_lsf.argtypes = [S, I, P]
+        L.fz_lsf_gaussian.argtypes = [P, I, ctypes.c_double, ctypes.c_double]
+        L.fz_lsf_kernel.argtypes = [P, I, P, I]
+        L.fz_lsf_clear.argtypes = [P]
         L.fz_model_to_v3_device.argtypes = [I, I, I, P, P, P, P, P]
         L.fz_obs_from_v3_device.argtypes = [I, I, P, P, P]
         L.fz_syn_to_v3_device.argtypes = [I, I, P, P, P]
@@ -395,6 +400,20 @@ class Synthesis:
                 f[int(p) - 1] = 1
         _check(lib().fz_smooth_device(self._h, int(nx), int(ny), ctypes.c_void_p(models_ptr),
                                       None if f is None else _p(f), ctypes.c_void_p(stream) if stream else None))
+
+    def lsf_gaussian(self, region, sigma, w0=0.0):
+        """The reference's Gaussian line spread function (sigma, centre w0 in
+        mA) for spectral region `region` (0-based); returns True if valid."""
+        return bool(_check(lib().fz_lsf_gaussian(self._h, int(region), float(sigma), float(w0))))
+
+    def lsf_kernel(self, region, yk):
+        """A line spread function as an LSF file holds it (NUMWAVE values of
+        the region, index 0 = centre); returns True if valid."""
+        k = np.ascontiguousarray(yk, dtype=np.float64)
+        return bool(_check(lib().fz_lsf_kernel(self._h, int(region), _p(k), k.size)))
+
+    def lsf_clear(self):
+        _check(lib().fz_lsf_clear(self._h))
 
     def errors(self, obs, models, hydrostatic=True, opts=None):
         """The errors mode for host models (npix, 13, nz) against obs (npix,

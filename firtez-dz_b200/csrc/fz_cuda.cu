@@ -1213,7 +1213,62 @@ LineP host_line(const fz_line& L, double wdif, const Consts& K) {
 
 }  // namespace
 
-constexpr int NKERN = 12;   // k_chain, k_opac, k_synth, k_opac_rf, k_synth_rf, k_lm_fill, k_lm_accept, k_lm_normal, k_lm_solve, k_lm_update, k_chemder, k_rf_prop
+// ----------------------------------------------------------- LSF convolution
+// CALCULATE_EQUIVALENT_SYN1D / CALCULATE_EQUIVALENT_DSYN with MLSF
+// (src/forward.f90:793-853, :615-657, :736-772): every Stokes row of NUMW
+// values is convolved, region by region, with the region's line spread
+// function -- a circular convolution over the region's NUMWAVE points (the
+// reference's real FFT pair without padding, the kernel divided by its
+// length against FFTW's unnormalised inverse): out(i) = sum_j s(j)
+// YK((i - j) mod n), in FP64 on the DBLE of the row, the result REAL*4.
+// Regions without a valid LSF are left as they are.
+struct LsfConf {
+  int nreg;
+  int off[MAXREG + 1];
+  int valid[MAXREG];
+};
+
+// One warp per (row, region); rows of numw values, rows_per_col rows per
+// column; with list, column c of the launch is column list[c] (c < *nlist).
+// Dynamic shared memory: numw doubles per warp.
+template <typename T>
+__global__ void __launch_bounds__(256) k_lsf(LsfConf L, long long nrows, int rows_per_col, int numw,
+                                             const int* __restrict__ list, const int* __restrict__ nlist,
+                                             const double* __restrict__ ker, T* __restrict__ data) {
+  extern __shared__ double sm_lsf[];
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5, wpb = blockDim.x >> 5;
+  double* sv = sm_lsf + (size_t)wib * numw;
+  const long long nwork = nrows * L.nreg;
+  const long long nl = list ? (long long)*nlist : 0;
+  for (long long wk = (long long)blockIdx.x * wpb + wib; wk < nwork; wk += (long long)gridDim.x * wpb) {
+    const int reg = (int)(wk % L.nreg);
+    const long long r = wk / L.nreg;
+    if (!L.valid[reg]) continue;
+    long long col = r / rows_per_col;
+    const int sub = (int)(r % rows_per_col);
+    if (list) {
+      if (col >= nl) continue;
+      col = list[col];
+    }
+    T* row = data + ((size_t)col * rows_per_col + sub) * numw;
+    const int o = L.off[reg], n = L.off[reg + 1] - o;
+    for (int j = lane; j < n; j += 32) sv[j] = (double)row[o + j];
+    __syncwarp();
+    const double* kr = ker + o;
+    for (int i = lane; i < n; i += 32) {
+      double acc = 0.0;
+      int ki = i;   // (i - j) mod n
+      for (int j = 0; j < n; ++j) {
+        acc = fma(sv[j], kr[ki], acc);
+        ki = ki == 0 ? n - 1 : ki - 1;
+      }
+      row[o + i] = (T)(float)acc;
+    }
+    __syncwarp();
+  }
+}
+
+constexpr int NKERN = 13;   // k_chain, k_opac, k_synth, k_opac_rf, k_synth_rf, k_lm_fill, k_lm_accept, k_lm_normal, k_lm_solve, k_lm_update, k_chemder, k_rf_prop, k_lsf
 
 struct fz_ctx {
   int device = 0;
@@ -1235,6 +1290,14 @@ struct fz_ctx {
   } tune;
   float* d_oscr = nullptr;   // operators of the full-height RF path (ncol, nz, 16, numw)
   double* d_smooth = nullptr;   // SMOOTHING_B buffers
+  // LSF convolution per spectral region (LSF_INIT, src/pre_post_duties.f90:742-900):
+  // kernels YK (sum 1, index 0 = centre) at the regions' offsets in d_lsf
+  struct {
+    bool on = false;
+    int valid[MAXREG] = {};
+    std::vector<double> yk;
+  } lsf;
+  double* d_lsf = nullptr;
   size_t smooth_len = 0;
   size_t oscr_len = 0;
   LamP* d_lam = nullptr;
@@ -1302,6 +1365,11 @@ int cuda_fail(cudaError_t e) {
 #define FZ_CK(x)                              \
   do {                                        \
     int _rc = cuda_fail(x);                   \
+    if (_rc) return _rc;                      \
+  } while (0)
+#define FZ_CK_RC(x)                           \
+  do {                                        \
+    int _rc = (x);                            \
     if (_rc) return _rc;                      \
   } while (0)
 
@@ -1374,6 +1442,29 @@ void launch_k_chain(fz_ctx* c, int ncol, const float* d_model, float* d_mout, in
   }
 }
 
+// The LSF pass over nrows rows of numw values (no-op without a valid LSF).
+template <typename T>
+int launch_lsf(fz_ctx* c, T* d_data, long long nrows, int rows_per_col, cudaStream_t s, const int* list = nullptr,
+               const int* nlist = nullptr) {
+  if (!c->lsf.on || nrows <= 0) return 0;
+  LsfConf L{};
+  L.nreg = c->nreg;
+  for (int r = 0; r < c->nreg; ++r) {
+    L.off[r + 1] = L.off[r] + c->regs[r].numwave;
+    L.valid[r] = c->lsf.valid[r];
+  }
+  const size_t smem = (size_t)8 * c->numw * sizeof(double);
+  if (smem > 227 * 1024) return FZ_ERR_LIMIT;
+  if (smem > 48 * 1024) FZ_CK(cudaFuncSetAttribute(k_lsf<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  const long long work = nrows * c->nreg;
+  const int blocks = (int)std::min<long long>((work + 7) / 8, (long long)c->nsm * 16);
+  {
+    ProfScope ps(c, 12, s, list ? 0 : (nrows / rows_per_col));
+    k_lsf<T><<<blocks, 256, smem, s>>>(L, nrows, rows_per_col, c->numw, list, nlist, c->d_lsf, d_data);
+  }
+  return cuda_fail(cudaGetLastError());
+}
+
 int launch_forward(fz_ctx* c, int ncol, const float* d_model, int hydrostatic, double* d_syn, float* d_mout,
                    int* d_status, cudaStream_t s) {
   int rc = ensure_scratch(c, ncol);
@@ -1398,7 +1489,7 @@ int launch_forward(fz_ctx* c, int ncol, const float* d_model, int hydrostatic, d
     k_synth<<<ncol, threads, sms, s>>>(c->d_params, c->d_lam, c->d_gain, ncol, c->d_slab, d_syn, d_mout, d_status);
   }
   FZ_CK(cudaGetLastError());
-  return 0;
+  return launch_lsf<double>(c, d_syn, (long long)ncol * 4, 4, s);
 }
 
 size_t rf_smem(const fz_ctx* c) {
@@ -1479,6 +1570,10 @@ int launch_rf_stage(fz_ctx* c, int ncol, int hydrostatic, double* d_syn, float* 
                                                           d_status, list, nlist);
   }
   FZ_CK(cudaGetLastError());
+  if (c->lsf.on) {
+    FZ_CK_RC(launch_lsf<double>(c, d_syn, (long long)ncol * 4, 4, s, list, nlist));
+    FZ_CK_RC(launch_lsf<float>(c, d_jac, (long long)ncol * 4 * c->rf.np, 4 * c->rf.np, s, list, nlist));
+  }
   return 0;
 }
 
@@ -1538,6 +1633,10 @@ int launch_forward_rf(fz_ctx* c, int ncol, const float* d_model, int hydrostatic
       k_rf_prop<<<ncol, threads, c->nz * sizeof(int), s>>>(c->nz, c->numw, c->d_gain, c->d_oscr, d_jac);
     }
     FZ_CK(cudaGetLastError());
+    if (c->lsf.on) {
+      FZ_CK_RC(launch_lsf<double>(c, d_syn, (long long)ncol * 4, 4, s));
+      FZ_CK_RC(launch_lsf<float>(c, d_jac, (long long)ncol * 24 * c->nz, 24 * c->nz, s));
+    }
     return 0;
   }
 }
@@ -2095,6 +2194,73 @@ int fz_errors(fz_ctx* c, int npix, const double* obs, const float* models, int h
   return rc;
 }
 
+// LSF_INIT's check and upload of one region's kernel (src/pre_post_duties.f90:
+// 814-842): valid when |sum(YK) - 1| < 0.01, then YK / sum(YK) once more;
+// an invalid region stays unconvolved.  Returns 1 (valid) or 0.
+static int lsf_install(fz_ctx* c, int region, std::vector<double>& yk) {
+  double sum = 0.0;
+  for (double v : yk) sum += v;
+  const int valid = std::fabs(sum - 1.0) < 0.01 ? 1 : 0;
+  int o = 0;
+  for (int r = 0; r < region; ++r) o += c->regs[r].numwave;
+  if (c->lsf.yk.size() != (size_t)c->numw) c->lsf.yk.assign(c->numw, 0.0);
+  if (valid)
+    for (size_t j = 0; j < yk.size(); ++j) c->lsf.yk[o + j] = yk[j] / sum;
+  c->lsf.valid[region] = valid;
+  FZ_CK(cudaSetDevice(c->device));
+  FZ_CK(cudaStreamSynchronize(c->stream));
+  if (!c->d_lsf) FZ_CK(cudaMalloc(&c->d_lsf, (size_t)c->numw * sizeof(double)));
+  FZ_CK(cudaMemcpy(c->d_lsf, c->lsf.yk.data(), (size_t)c->numw * sizeof(double), cudaMemcpyHostToDevice));
+  c->lsf.on = false;
+  for (int r = 0; r < c->nreg; ++r) c->lsf.on = c->lsf.on || c->lsf.valid[r];
+  return valid;
+}
+
+int fz_lsf_gaussian(fz_ctx* c, int region, double sigma, double w0) {
+  if (!c || region < 0 || region >= c->nreg || !(sigma > 0.0)) return FZ_ERR_ARG;
+  const fz_region& R = c->regs[region];
+  const int n = R.numwave;
+  if (n < 2) return FZ_ERR_ARG;
+  // LSF_INIT's Gaussian (:795-812): pixel positions centred on the region,
+  // in mA of WAVE(WI+1) - WAVE(WI), half a step off for even sizes, then
+  // normalised and circularly shifted by n/2 (centre to index 0)
+  const double dw = (R.wave_ini + R.dlambda * 1.0) - (R.wave_ini + R.dlambda * 0.0);
+  std::vector<double> xk(n), yk(n);
+  double m = 0.0;
+  for (int j = 0; j < n; ++j) {
+    xk[j] = (double)(j + 1);
+    m += xk[j];
+  }
+  m /= (double)n;
+  for (int j = 0; j < n; ++j) xk[j] = (xk[j] - m) * dw;
+  const double woff = (n % 2 == 0) ? (xk[1] - xk[0]) / 2.0 : 0.0;
+  double sum = 0.0;
+  for (int j = 0; j < n; ++j) {
+    const double d = xk[j] - w0 - woff;
+    yk[j] = std::exp(-(d * d / (2.0 * sigma * sigma)));
+    sum += yk[j];
+  }
+  std::vector<double> sh(n);
+  for (int j = 0; j < n; ++j) sh[j] = yk[(j + n / 2) % n] / sum;
+  return lsf_install(c, region, sh);
+}
+
+int fz_lsf_kernel(fz_ctx* c, int region, const double* yk, int n) {
+  if (!c || region < 0 || region >= c->nreg || !yk) return FZ_ERR_ARG;
+  if (n != c->regs[region].numwave) return FZ_ERR_LIMIT;   // READ_LSF_FILE's size check
+  std::vector<double> v(yk, yk + n);
+  return lsf_install(c, region, v);
+}
+
+int fz_lsf_clear(fz_ctx* c) {
+  if (!c) return FZ_ERR_ARG;
+  FZ_CK(cudaSetDevice(c->device));
+  FZ_CK(cudaStreamSynchronize(c->stream));
+  c->lsf.on = false;
+  for (int r = 0; r < MAXREG; ++r) c->lsf.valid[r] = 0;
+  return 0;
+}
+
 int fz_smooth(fz_ctx* c, int nx, int ny, float* models, const int* params) {
   if (!c || nx <= 0 || ny <= 0 || !models) return FZ_ERR_ARG;
   FZ_CK(cudaSetDevice(c->device));
@@ -2326,6 +2492,7 @@ int fz_destroy(fz_ctx* c) {
   cudaFree(c->d_pfd);
   cudaFree(c->d_oscr);
   cudaFree(c->d_smooth);
+  cudaFree(c->d_lsf);
   for (cudaEvent_t e : c->ev_pool) cudaEventDestroy(e);
   for (auto& p : c->pending) {
     cudaEventDestroy(p.a);
@@ -3040,7 +3207,7 @@ int fz_forward_device_static(fz_ctx* c, int ncol, const float* d_model, int hydr
   const size_t sms = (size_t)c->nz * c->sw * sizeof(float);
   k_synth<<<ncol, threads, sms, s>>>(c->d_params, c->d_lam, c->d_gain, ncol, slab, d_syn, d_model_out, d_status);
   FZ_CK(cudaGetLastError());
-  return 0;
+  return launch_lsf<double>(c, d_syn, (long long)ncol * 4, 4, s);   // allocates nothing
 }
 
 int fz_forward(fz_ctx* c, int ncol, const float* model, int hydrostatic, double* syn, float* model_out,

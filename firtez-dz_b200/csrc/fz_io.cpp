@@ -234,4 +234,36 @@ int fz_v3_read_rfs(const char* path, int nx, int ny, int nz, int nw, float* z, i
   return get_data(F.f, data, n) ? np : FZ_ERR_PARSE;
 }
 
+int fz_v3_read_lsf(const char* path, int n, double* yk) {
+  if (n <= 0 || !yk) return FZ_ERR_ARG;
+  File F;
+  if (int rc = check_open(F, path, "rb")) return rc;
+  float h[16];
+  int nh = 0;
+  if (int rc = read_header(F.f, h, nh)) return rc;
+  // READ_LSF_FILE (misc.f90:2422-2555): ID 3330904, one dimension NIW
+  if (nh != 6 || std::fabs(h[2] - 3330904.f) > 0.5f || (int)h[4] != 1) return FZ_ERR_PARSE;
+  if ((int)h[5] != n) return FZ_ERR_LIMIT;
+  std::vector<float> v(n);
+  for (int64_t o = 0; o < n; o += kMaxRec)
+    if (!get_rec(F.f, v.data() + o, std::min<int64_t>(kMaxRec, n - o))) return FZ_ERR_PARSE;
+  for (int i = 0; i < n; ++i) yk[i] = (double)v[i];
+  return 0;
+}
+
+int fz_v3_write_lsf(const char* path, int n, const double* yk) {
+  if (n <= 0 || !yk) return FZ_ERR_ARG;
+  File F;
+  if (int rc = check_open(F, path, "wb")) return rc;
+  // the reference's Python write_lsf: header 3003, 2997, 3330904, NRECS+1,
+  // 1, NW (its record count is sized for 4 NW values: one record up to
+  // 67,108,861 wavelengths)
+  const int64_t nrec = (4 * (int64_t)n + kMaxRec - 1) / kMaxRec;
+  const float h[6] = {3003.f, 2997.f, 3330904.f, (float)(nrec + 1), 1.f, (float)n};
+  std::vector<float> v(n);
+  for (int i = 0; i < n; ++i) v[i] = (float)yk[i];
+  if (!put_rec(F.f, h, 6) || !put_data(F.f, v.data(), n)) return FZ_ERR_ARG;
+  return std::fclose(std::exchange(F.f, nullptr)) == 0 ? 0 : FZ_ERR_ARG;
+}
+
 }  // extern "C"

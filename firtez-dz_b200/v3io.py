@@ -106,6 +106,18 @@ def write_rf(path, z, logv, ind, wave, data):
     _check(lib().fz_v3_write_rfs(_path(path), nx, ny, nz, nw, _p(zz), _p(lv), _p(i), _p(w), _p(d)))
 
 
+def read_lsf(path, n):
+    """The n-point line spread function of an LSF file (READ_LSF_FILE)."""
+    yk = np.empty(n, dtype=np.float64)
+    _check(lib().fz_v3_read_lsf(_path(path), int(n), _p(yk)))
+    return yk
+
+
+def write_lsf(path, yk):
+    k = np.ascontiguousarray(yk, dtype=np.float64)
+    _check(lib().fz_v3_write_lsf(_path(path), k.size, _p(k)))
+
+
 # ---------------------------------------------------------------- device
 def _ptr(t):
     return ctypes.c_void_p(t.data_ptr())

@@ -267,6 +267,23 @@ int fz_invert_cycles_device(fz_ctx* ctx, int nx, int ny, const double* d_obs, fl
                             const int* nodes, int hydrostatic, const fz_lm_opts* opts, double* d_chi2, int* d_iters,
                             int* d_status, void* stream);
 
+/* Line spread function of a spectral region (LSF_INIT, src/pre_post_duties.f90:
+ * 742-900; applied by CALCULATE_EQUIVALENT_SYN1D / _DSYN, src/forward.f90:
+ * 615-657, :793-853): every synthesis row and every node-Jacobian (and full
+ * response-function) row of the region is circularly convolved with the
+ * region's kernel YK, in FP64, the result rounded to REAL*4.
+ *   fz_lsf_gaussian: the reference's Gaussian of sigma and centre w0 [mA]
+ *     over the region's NUMWAVE points (step WAVE(WI+1) - WAVE(WI)).
+ *   fz_lsf_kernel:   a kernel as READ_LSF_FILE gives it (n = NUMWAVE of the
+ *     region, index 0 = the centre, as the reference convolves it).
+ * A kernel is valid when its sum is within 0.01 of 1 (then renormalised);
+ * both return 1 (valid, the region is convolved from now on) or 0 (the
+ * region is left unconvolved, as the reference does).  fz_lsf_clear turns
+ * the LSF off.  Applies to every later synthesis, RF and inversion call. */
+int fz_lsf_gaussian(fz_ctx* ctx, int region, double sigma, double w0);
+int fz_lsf_kernel(fz_ctx* ctx, int region, const double* yk, int n);
+int fz_lsf_clear(fz_ctx* ctx);
+
 /* The errors mode (GET_ERRORS3DS / GET_ERROR_1D / NEW_SOLVE_ERRORS,
  * src/get_dmodel.f90:1248-1323, :1581-1703), replacing the per-pixel worker
  * loop: for the models (usually the inversion's best), with the node layout
@@ -365,6 +382,12 @@ int fz_v3_write_rfs(const char* path, int nx, int ny, int nz, int nw, const doub
  * parameters). */
 int fz_v3_read_rfs(const char* path, int nx, int ny, int nz, int nw, float* z, int* logv, float* ind, float* wave,
                    float* data);
+
+/* Line spread function files (READ_LSF_FILE, misc.f90:2422-2555; the
+ * reference's Python write_lsf): header 3003, 2997, 3330904, NRECS+1, 1, NW,
+ * then NW REAL*4 values. */
+int fz_v3_read_lsf(const char* path, int n, double* yk);
+int fz_v3_write_lsf(const char* path, int n, const double* yk);
 
 /* Layout changes on the device (stream-ordered, no allocation except the
  * x/y vectors of fz_model_to_v3_device):

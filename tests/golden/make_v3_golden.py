@@ -11,6 +11,7 @@ writers use it for the record size).  Writes, next to this script:
                            3 x 2 x 4 model
   v3_profile_pywriter.bin  stk_profile3D.write (write_profile3D_v3) of seeded
                            3 x 2 profiles of 5 wavelengths
+  v3_lsf_pywriter.bin      write_lsf of a seeded 7-point line spread function
   v3_golden.npz            the seeded inputs, and what the reference's
                            read_rf returns for a 2 x 3 x 4 x 5 RF file laid
                            out by the oracle's WRITE_RFS3D_V3 restatement
@@ -72,6 +73,11 @@ p = fzpy.stk_profile3D(nw, pnx, pny)
 p.set_profiles(stokes.astype(np.float64), ind, wave)
 p.write(os.path.join(here, "v3_profile_pywriter.bin"))
 
+# ---- line spread function file
+lsf = rng.random(7)
+lsf = lsf / lsf.sum()
+fzpy.write_lsf(os.path.join(here, "v3_lsf_pywriter.bin"), lsf)
+
 # ---- RFs: the oracle's file layout read back by the reference's reader
 rnx, rny, rnz, rnw = 2, 3, 4, 5
 logv = [1, 1, 0, 1, 1, 1, 1, 0]
@@ -87,6 +93,6 @@ with tempfile.TemporaryDirectory() as td:
               for n in ("tem", "pg", "rho", "bx", "by", "bz", "vz", "p0")}
 
 np.savez(os.path.join(here, "v3_golden.npz"), model_cubes=cubes, prof_stokes=stokes, prof_ind=ind, prof_wave=wave,
-         rf_data=rfdata, rf_z=rz, rf_ind=rind, rf_wave=rwave, rf_logv=np.array(logv, dtype=np.int32),
+         lsf=lsf, rf_data=rfdata, rf_z=rz, rf_ind=rind, rf_wave=rwave, rf_logv=np.array(logv, dtype=np.int32),
          **{"rf_ref_" + k: v for k, v in rf_ref.items()})
-print("wrote v3_model_pywriter.bin, v3_profile_pywriter.bin, v3_golden.npz")
+print("wrote v3_model_pywriter.bin, v3_profile_pywriter.bin, v3_lsf_pywriter.bin, v3_golden.npz")

@@ -126,3 +126,14 @@ def test_malformed_files_refused(fz, v3, gold, tmp_path):
     # a missing file
     with pytest.raises(fz.FzError):
         v3.read_header(tmp_path / "none.bin")
+
+
+def test_lsf_file_matches_reference_writer(v3, gold, tmp_path):
+    """The LSF file (READ_LSF_FILE's format) byte for byte as the reference's
+    Python write_lsf writes it, and read back."""
+    out = tmp_path / "lsf.bin"
+    v3.write_lsf(out, gold["lsf"])
+    assert _bytes(out) == _bytes(os.path.join(GOLD, "v3_lsf_pywriter.bin"))
+    np.testing.assert_array_equal(v3.read_lsf(out, gold["lsf"].size), np.float32(gold["lsf"]).astype(np.float64))
+    with pytest.raises(Exception):
+        v3.read_lsf(out, gold["lsf"].size + 1)
