@@ -499,6 +499,32 @@ def main():
     synthesis = {"value": world * ns * numw / (ms_syn * 1e-3), "unit": "columns*lambda/s",
                  "workload": "%d columns x %d heights x %d lambda, hydrostatic" % (ns, a.nz, numw),
                  "ms_per_call": ms_syn, "kernel_ms": {k: v[0] / max(v[1], 1) for k, v in sprof.items() if v[1]}}
+    # ------------------------------------ synthesis with a line spread function
+    # the same columns with the reference's Gaussian LSF (sigma 30 mA) in both
+    # regions: k_lsf convolves each Stokes row region by region in FP64
+    # (2 n^2 FLOP per region row, n = NUMWAVE)
+    for r in range(len(ctx.regions)):
+        ctx.lsf_gaussian(r, 30.0, 0.0)
+    ctx.forward_device(m.data_ptr(), ns, so.data_ptr(), mo.data_ptr(), 0, stream=stream, hydrostatic=True)
+    torch.cuda.synchronize()
+    ctx.profile(True)
+    ctx.profile_read()
+    e0.record()
+    for _ in range(5):
+        ctx.forward_device(m.data_ptr(), ns, so.data_ptr(), mo.data_ptr(), 0, stream=stream, hydrostatic=True)
+    e1.record()
+    torch.cuda.synchronize()
+    ctx.profile(False)
+    lprof = ctx.profile_read()
+    ctx.lsf_clear()
+    ms_lsf = maxms(e0.elapsed_time(e1) / 5)
+    k_lsf_ms = lprof["k_lsf"][0] / max(lprof["k_lsf"][1], 1)
+    lsf_flop = ns * 4 * sum(2.0 * int(n) ** 2 for n in ctx.regions["numwave"])
+    synthesis_lsf = {"value": world * ns * numw / (ms_lsf * 1e-3), "unit": "columns*lambda/s",
+                     "workload": synthesis["workload"] + ", Gaussian LSF sigma 30 mA in every region",
+                     "ms_per_call": ms_lsf, "k_lsf_ms": k_lsf_ms,
+                     "k_lsf_fp64_gflops": lsf_flop / (k_lsf_ms * 1e-3) / 1e9,
+                     "k_lsf_gbs": ns * nf * 8 * 2 / (k_lsf_ms * 1e-3) / 1e9}
     # ------------------------------- response functions at every height (C2)
     # 256x256 columns (the synthesis sub-metric's) through fz_forward_rf_full
     # in batches of rf_chunk columns; each batch's output (rf_chunk x 6 x NZ x
@@ -674,6 +700,7 @@ def main():
                                            "log tau5 is in [-3, 0], over the compared pixels"),
            "synthesis": synthesis,
            "rf_full": rf_full,
+           "synthesis_lsf": synthesis_lsf,
            "errors_mode": errors_mode,
            "v3_files": v3_files,
            "roofline": {"bound": "hbm", "kernel": kname, "achieved": achieved, "peak": hbm, "unit": "GB/s",

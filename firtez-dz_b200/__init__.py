@@ -62,20 +62,22 @@ class LMOpts(ctypes.Structure):
     """fz_lm_opts: stop rules and weights of the batched inversion."""
     _fields_ = [("maxsteps", ctypes.c_int), ("maxit", ctypes.c_int), ("dchi2", ctypes.c_double),
                 ("svdtol", ctypes.c_double), ("isigma", ctypes.c_double), ("wstk", ctypes.c_float * 4),
-                ("slots", ctypes.c_int), ("pad", ctypes.c_int), ("fallback", ctypes.c_double),
+                ("slots", ctypes.c_int), ("assist", ctypes.c_int), ("fallback", ctypes.c_double),
                 ("fallback_model", ctypes.c_void_p), ("reg_type", ctypes.c_int * 8), ("reg_alpha", ctypes.c_double * 8)]
 
     def __init__(self, maxsteps=5, maxit=40, dchi2=0.0, svdtol=1e-4, isigma=4e-3, wstk=(1, 1, 1, 1), slots=0,
-                 fallback=0.0, fallback_model=0, reg=None):
+                 fallback=0.0, fallback_model=0, reg=None, assist=()):
         """fallback_model: device pointer of one MODEL(NZ,13) float32 (e.g. a
         torch tensor's data_ptr()) that pixels ending above fallback x their
         chi2 goal restart from (a host pointer for invert()).  reg: optional
         {reference parameter: (type, alpha)} vertical regularisation
-        (VERTICAL REGULARIZATION: type 0 or 1, PEN_ALP)."""
+        (VERTICAL REGULARIZATION: type 0 or 1, PEN_ALP).  assist: SET_TAU's
+        assists for invert_cycles (temp, pgas, bvec, vlos, progressive)."""
         typ, alp = [0] * 8, [0.0] * 8
         for p, (t, a) in (reg or {}).items():
             typ[int(p) - 1], alp[int(p) - 1] = int(t), float(a)
-        super().__init__(maxsteps, maxit, dchi2, svdtol, isigma, (ctypes.c_float * 4)(*wstk), slots, 0,
+        super().__init__(maxsteps, maxit, dchi2, svdtol, isigma, (ctypes.c_float * 4)(*wstk), slots,
+                         assist_bits(assist),
                          float(fallback), fallback_model or None, (ctypes.c_int * 8)(*typ),
                          (ctypes.c_double * 8)(*alp))
 
@@ -145,6 +147,8 @@ def lib():
         L.fz_lsf_gaussian.argtypes = [P, I, ctypes.c_double, ctypes.c_double]
         L.fz_lsf_kernel.argtypes = [P, I, P, I]
         L.fz_lsf_clear.argtypes = [P]
+        L.fz_set_tau.argtypes = [P, I, I, P, P, I]
+        L.fz_set_tau_device.argtypes = [P, I, I, P, P, I, P]
         L.fz_model_to_v3_device.argtypes = [I, I, I, P, P, P, P, P]
         L.fz_obs_from_v3_device.argtypes = [I, I, P, P, P]
         L.fz_syn_to_v3_device.argtypes = [I, I, P, P, P]
@@ -161,6 +165,17 @@ def lib():
                                          P]
         _lib = L
     return _lib
+
+
+ASSIST = {"temp": 1, "pgas": 2, "bvec": 4, "vlos": 8, "progressive": 16}
+
+
+def assist_bits(names):
+    """FZ_ASSIST_* bits of assist names (temp, pgas, bvec, vlos, progressive)."""
+    b = 0
+    for n in names or ():
+        b |= ASSIST[n.lower()]
+    return b
 
 
 def _check(rc):
@@ -400,6 +415,17 @@ class Synthesis:
                 f[int(p) - 1] = 1
         _check(lib().fz_smooth_device(self._h, int(nx), int(ny), ctypes.c_void_p(models_ptr),
                                       None if f is None else _p(f), ctypes.c_void_p(stream) if stream else None))
+
+    def set_tau(self, obs, models, nx, ny, assist=("temp", "bvec", "vlos")):
+        """SET_TAU's assists on host arrays: obs (nx*ny, 4, numw), models
+        (nx*ny, 13, nz) (pixel iy + ny*ix); assist: names among temp, pgas,
+        bvec, vlos.  Returns the assisted models."""
+        o = np.ascontiguousarray(obs, dtype=np.float64)
+        m = np.array(models, dtype=np.float32, order="C", copy=True)
+        if o.shape != (nx * ny, 4, self.numw) or m.shape != (nx * ny, 13, self.nz):
+            raise ValueError("obs must be (nx*ny, 4, numw) and models (nx*ny, 13, nz)")
+        _check(lib().fz_set_tau(self._h, int(nx), int(ny), _p(o), _p(m), assist_bits(assist)))
+        return m
 
     def lsf_gaussian(self, region, sigma, w0=0.0):
         """The reference's Gaussian line spread function (sigma, centre w0 in

@@ -1864,6 +1864,136 @@ __global__ void k_smooth_pass(int nx, int ny, int nz, int nrow, int dir, const i
   }
 }
 
+// ------------------------------------------------------------- SET_TAU
+// The assists of SET_TAU (src/invert3d.f90:492-727): field-wide template
+// vectors from the summed Stokes I of the first spectral region, per-pixel
+// projections, field maxima, then per-pixel rewrites of B, v_z, T and Pg.
+// Pixels iy + NY ix; obs (npix, 4, numw) REAL*8 (OBS3D).
+
+// Partial sums of Stokes I over y for every x (SUM(SUM(OBS3D(..),DIM=2),DIM=2)
+// takes the y sum first): one thread per (x, wavelength of region 1).
+__global__ void k_tau_ysum(int nx, int ny, int numw, int n1, const double* __restrict__ obs,
+                           double* __restrict__ part) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nx * n1) return;
+  const int ix = i / n1, j = i % n1;
+  double t = 0.0;
+  for (int iy = 0; iy < ny; ++iy) t += obs[((size_t)ix * ny + iy) * 4 * numw + j];
+  part[i] = t;
+}
+
+// then over x, in order: one thread per wavelength
+__global__ void k_tau_xsum(int nx, int n1, const double* __restrict__ part, double* __restrict__ tot) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= n1) return;
+  double t = 0.0;
+  for (int ix = 0; ix < nx; ++ix) t += part[(size_t)ix * n1 + j];
+  tot[j] = t;
+}
+
+// One warp per pixel: the projections of region 1 (vec = the three template
+// vectors, 3 x n1): proj[p] = {V.v2, Q.v3, U.v3, I.v2, I.v1, mean I}.
+__global__ void k_tau_proj(int npix, int numw, int n1, const double* __restrict__ obs, const double* __restrict__ vec,
+                           double* __restrict__ proj) {
+  const int lane = threadIdx.x & 31;
+  const size_t p = ((size_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  if (p >= (size_t)npix) return;
+  const double* o = obs + p * 4 * numw;
+  double a[6] = {0, 0, 0, 0, 0, 0};
+  for (int j = lane; j < n1; j += 32) {
+    const double I = o[j], Q = o[numw + j], U = o[2 * numw + j], V = o[3 * numw + j];
+    a[0] += V * vec[n1 + j];
+    a[1] += Q * vec[2 * n1 + j];
+    a[2] += U * vec[2 * n1 + j];
+    a[3] += I * vec[n1 + j];
+    a[4] += I * vec[j];
+    a[5] += I;
+  }
+#pragma unroll
+  for (int q = 0; q < 6; ++q)
+    for (int off = 16; off > 0; off >>= 1) a[q] += __shfl_xor_sync(0xffffffffu, a[q], off);
+  if (lane == 0) {
+    for (int q = 0; q < 5; ++q) proj[p * 6 + q] = a[q];
+    proj[p * 6 + 5] = a[5] / (double)n1;   // SUM(DBLE(I)) / DBLE(n)
+  }
+}
+
+// Field maxima |V.v2|, sqrt((Q.v3)^2 + (U.v3)^2), |I.v2 - I.v1 KOL| as
+// order-independent atomic maxima of non-negative doubles (bit patterns
+// order like the values); mx zeroed by the caller.
+__global__ void k_tau_max(int npix, double kol, const double* __restrict__ proj, unsigned long long* __restrict__ mx) {
+  double m0 = 0.0, m1 = 0.0, m2 = 0.0;
+  for (size_t p = (size_t)blockIdx.x * blockDim.x + threadIdx.x; p < (size_t)npix; p += (size_t)gridDim.x * blockDim.x) {
+    const double* q = proj + p * 6;
+    m0 = fmax(m0, fabs(q[0]));
+    m1 = fmax(m1, sqrt(q[1] * q[1] + q[2] * q[2]));
+    m2 = fmax(m2, fabs(q[3] - q[4] * kol));
+  }
+  for (int off = 16; off > 0; off >>= 1) {
+    m0 = fmax(m0, __shfl_xor_sync(0xffffffffu, m0, off));
+    m1 = fmax(m1, __shfl_xor_sync(0xffffffffu, m1, off));
+    m2 = fmax(m2, __shfl_xor_sync(0xffffffffu, m2, off));
+  }
+  if ((threadIdx.x & 31) == 0) {
+    atomicMax(mx + 0, (unsigned long long)__double_as_longlong(m0));
+    atomicMax(mx + 1, (unsigned long long)__double_as_longlong(m1));
+    atomicMax(mx + 2, (unsigned long long)__double_as_longlong(m2));
+  }
+}
+
+struct TauConf {
+  int assist;     // 1 T, 2 Pg, 4 B, 8 v_z
+  int nz, itz;    // ITZ - 1 = CEILING(NZ/3) - 1
+  double kol, lk_hc;
+};
+
+// One warp per pixel: the assists in the reference's order B, v_z, T, Pg,
+// with its REAL*4 / REAL*8 mixing (invert3d.f90:563-570, :621-625,
+// :640-652, :666-671).
+__global__ void k_tau_apply(TauConf C, int npix, const double* __restrict__ proj,
+                            const unsigned long long* __restrict__ mx, float* __restrict__ models) {
+  const int lane = threadIdx.x & 31;
+  const size_t p = ((size_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  if (p >= (size_t)npix) return;
+  const int nz = C.nz;
+  float* m = models + p * 13 * nz;
+  const double* q = proj + p * 6;
+  if (C.assist & 4) {
+    const double t3 = q[0] / __longlong_as_double((long long)mx[0]);
+    const double t4 = sqrt(q[1] * q[1] + q[2] * q[2]) / __longlong_as_double((long long)mx[1]);
+    const double atn2 = atan2(q[2], q[1]) / 2.0;
+    const float bx = (float)((double)(-(float)sin(atn2) * 1000.0f) * t4);
+    const float by = (float)((double)((float)cos(atn2) * 1000.0f) * t4);
+    const float bz = (float)t3 * (-1000.0f);
+    for (int k = lane; k < nz; k += 32) {
+      m[5 * nz + k] = bx;
+      m[6 * nz + k] = by;
+      m[7 * nz + k] = bz;
+    }
+  }
+  if (C.assist & 8) {
+    const double d = (q[3] - q[4] * C.kol) / __longlong_as_double((long long)mx[2]);
+    const float vz = (float)d * (-2.0e5f);
+    for (int k = lane; k < nz; k += 32) m[10 * nz + k] = vz;
+  }
+  __syncwarp();
+  if (C.assist & 1) {
+    const double imean = q[5];
+    const double tb = 1.0 / (C.lk_hc * log(1.0 + 1.0 / imean * (exp(1.0 / 6.39e3 / C.lk_hc) - 1.0)));
+    const double sh = tb - (double)m[C.itz];
+    __syncwarp();
+    for (int k = lane; k < nz; k += 32) m[k] = (float)((double)m[k] + sh);
+  }
+  __syncwarp();
+  if (C.assist & 2) {
+    const float p0 = m[nz + C.itz];
+    __syncwarp();
+    for (int k = lane; k < nz; k += 32) m[nz + k] = m[nz + k] * 1.333e5f / p0;
+  }
+  if (C.assist & 3)
+    for (int k = lane; k < nz; k += 32) m[11 * nz + k] = k == C.itz ? 0.0f : 1.0f;
+}
+
 // ------------------------------------------------------------ v3 layouts
 // Cube of the v3 model file feeding each MODEL row (-1: vx, vy, zero; the
 // file has no cube for them): JOIN_MODEL2 (src/forward.f90:363-405) over the
@@ -2050,6 +2180,11 @@ int fz_invert_cycles_device(fz_ctx* c, int nx, int ny, const double* d_obs, floa
       if ((rc = cuda_fail(cudaStreamSynchronize(s)))) break;
       if ((rc = fz_rf_nodes(c, nodes + 8 * cy)) < 0) break;   // >= 0: the layout's NP
       rc = 0;
+      // SET_TAU's assists when neither Pg nor P0 is free, every cycle or,
+      // with PROGRESSIVE, the first only (invert3d.f90:505-520)
+      const int assist = opts ? (opts->assist & 15) : 0;
+      if (assist && nodes[8 * cy + 1] == 0 && nodes[8 * cy + 7] == 0 && (cy == 0 || !(opts->assist & 16)))
+        if ((rc = fz_set_tau_device(c, nx, ny, d_obs, d_models, assist, s))) break;
       if ((rc = fz_smooth_device(c, nx, ny, d_models, nullptr, s))) break;
       // the cycle's iterations, each pixel from a fresh LM state
       if ((rc = fz_invert_device(c, npix, d_obs, d_models, nullptr, hydrostatic, opts, d_best, d_chi2, d_iters,
@@ -2259,6 +2394,103 @@ int fz_lsf_clear(fz_ctx* c) {
   c->lsf.on = false;
   for (int r = 0; r < MAXREG; ++r) c->lsf.valid[r] = 0;
   return 0;
+}
+
+int fz_set_tau_device(fz_ctx* c, int nx, int ny, const double* d_obs, float* d_models, int assist, void* stream) {
+  if (!c || nx <= 0 || ny <= 0 || !d_obs || !d_models || (assist & ~15)) return FZ_ERR_ARG;
+  if (assist == 0) return 0;
+  const int npix = nx * ny, numw = c->numw, n1 = c->regs[0].numwave, nz = c->nz;
+  if (n1 < 3) return FZ_ERR_ARG;
+  FZ_CK(cudaSetDevice(c->device));
+  cudaStream_t s = (cudaStream_t)stream;
+  double *d_part = nullptr, *d_vec = nullptr, *d_proj = nullptr, *d_syn = nullptr;
+  unsigned long long* d_mx = nullptr;
+  int rc = 0;
+  do {
+    if ((rc = cuda_fail(cudaMalloc(&d_part, ((size_t)nx + 1) * n1 * sizeof(double))))) break;
+    if ((rc = cuda_fail(cudaMalloc(&d_vec, (size_t)3 * n1 * sizeof(double))))) break;
+    if ((rc = cuda_fail(cudaMalloc(&d_proj, (size_t)npix * 6 * sizeof(double))))) break;
+    if ((rc = cuda_fail(cudaMalloc(&d_mx, 3 * sizeof(unsigned long long))))) break;
+    double* d_tot = d_part + (size_t)nx * n1;
+    k_tau_ysum<<<(nx * n1 + 255) / 256, 256, 0, s>>>(nx, ny, numw, n1, d_obs, d_part);
+    k_tau_xsum<<<(n1 + 127) / 128, 128, 0, s>>>(nx, n1, d_part, d_tot);
+    if ((rc = cuda_fail(cudaGetLastError()))) break;
+    std::vector<double> v(3 * (size_t)n1);
+    if ((rc = cuda_fail(cudaMemcpyAsync(v.data(), d_tot, n1 * sizeof(double), cudaMemcpyDeviceToHost, s)))) break;
+    if ((rc = cuda_fail(cudaStreamSynchronize(s)))) break;
+    // VECTORS(:,1..3): the normalised field sum and its two centred
+    // derivatives, end points copied, each over SUM(ABS(.)) (:522-534)
+    auto norm1 = [&](double* a) {
+      double t = 0.0;
+      for (int j = 0; j < n1; ++j) t += std::fabs(a[j]);
+      for (int j = 0; j < n1; ++j) a[j] = a[j] / t;
+    };
+    auto deriv = [&](const double* a, double* b) {
+      for (int j = 1; j < n1 - 1; ++j) b[j] = (a[j + 1] - a[j - 1]) / 2.0;
+      b[0] = b[1];
+      b[n1 - 1] = b[n1 - 2];
+    };
+    double *v1 = v.data(), *v2 = v1 + n1, *v3 = v2 + n1;
+    norm1(v1);
+    deriv(v1, v2);
+    norm1(v2);
+    deriv(v2, v3);
+    norm1(v3);
+    double kol = 0.0;   // KOL = VECTORS(:,2) . VECTORS(:,1) (:613)
+    for (int j = 0; j < n1; ++j) kol += v2[j] * v1[j];
+    if ((rc = cuda_fail(cudaMemcpyAsync(d_vec, v.data(), v.size() * sizeof(double), cudaMemcpyHostToDevice, s))))
+      break;
+    const int wblocks = (int)(((size_t)npix * 32 + 255) / 256);
+    k_tau_proj<<<wblocks, 256, 0, s>>>(npix, numw, n1, d_obs, d_vec, d_proj);
+    if ((rc = cuda_fail(cudaMemsetAsync(d_mx, 0, 3 * sizeof(unsigned long long), s)))) break;
+    k_tau_max<<<grid_for(npix, 256), 256, 0, s>>>(npix, kol, d_proj, d_mx);
+    TauConf C{};
+    C.assist = assist;
+    C.nz = nz;
+    C.itz = (int)std::ceil((float)nz / 3.0f) - 1;   // CEILING(REAL(NZ)/3.)
+    C.kol = kol;
+    const double l0 = c->lines[c->regs[0].line[0]].l0;   // LINE_L0(IND_LINE(1)) [A]
+    C.lk_hc = (l0 * 1.0e-8 * KBOL) / (HPLA * LIGHT);
+    k_tau_apply<<<wblocks, 256, 0, s>>>(C, npix, d_proj, d_mx, d_models);
+    if ((rc = cuda_fail(cudaGetLastError()))) break;
+    if (assist & 3) {
+      // FORWARD3D with HYDRO_TOP off (:675-678): rho, Pe, mu and log tau5 of
+      // the new T and Pg
+      if ((rc = cuda_fail(cudaMalloc(&d_syn, (size_t)npix * 4 * numw * sizeof(double))))) break;
+      if ((rc = launch_forward(c, npix, d_models, 0, d_syn, d_models, nullptr, s))) break;
+    }
+    rc = cuda_fail(cudaStreamSynchronize(s));
+  } while (false);
+  cudaFree(d_part);
+  cudaFree(d_vec);
+  cudaFree(d_proj);
+  cudaFree(d_mx);
+  cudaFree(d_syn);
+  return rc;
+}
+
+int fz_set_tau(fz_ctx* c, int nx, int ny, const double* obs, float* models, int assist) {
+  if (!c || nx <= 0 || ny <= 0 || !obs || !models) return FZ_ERR_ARG;
+  FZ_CK(cudaSetDevice(c->device));
+  const size_t npix = (size_t)nx * ny, nf = 4 * (size_t)c->numw, nm = 13 * (size_t)c->nz;
+  double* d_obs = nullptr;
+  float* d_m = nullptr;
+  int rc = 0;
+  do {
+    if ((rc = cuda_fail(cudaMalloc(&d_obs, npix * nf * sizeof(double))))) break;
+    if ((rc = cuda_fail(cudaMalloc(&d_m, npix * nm * sizeof(float))))) break;
+    if ((rc = cuda_fail(cudaMemcpyAsync(d_obs, obs, npix * nf * sizeof(double), cudaMemcpyHostToDevice, c->stream))))
+      break;
+    if ((rc = cuda_fail(cudaMemcpyAsync(d_m, models, npix * nm * sizeof(float), cudaMemcpyHostToDevice, c->stream))))
+      break;
+    if ((rc = fz_set_tau_device(c, nx, ny, d_obs, d_m, assist, c->stream))) break;
+    if ((rc = cuda_fail(cudaMemcpyAsync(models, d_m, npix * nm * sizeof(float), cudaMemcpyDeviceToHost, c->stream))))
+      break;
+    rc = cuda_fail(cudaStreamSynchronize(c->stream));
+  } while (false);
+  cudaFree(d_obs);
+  cudaFree(d_m);
+  return rc;
 }
 
 int fz_smooth(fz_ctx* c, int nx, int ny, float* models, const int* params) {

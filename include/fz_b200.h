@@ -219,12 +219,19 @@ int fz_smooth_device(fz_ctx* ctx, int nx, int ny, float* d_models, const int* pa
  * (GET_IT_PENALTIES, src/get_dmodel.f90:1041-1197), per reference parameter
  * 1..8: type 0 (node values to zero, D = diag(1/NJ)) or 1 (differences to
  * the previous node) and PEN_ALP (0: off); chi2 gains sum(PEN_RES^2) of the
- * current model, the normal equations PEN_HSS and -PEN_RES of the best. */
+ * current model, the normal equations PEN_HSS and -PEN_RES of the best.
+ * assist: SET_TAU's initial-guess assists for fz_invert_cycles_device
+ * (FZ_ASSIST_* bits; the control file's ASSIST line and PROGRESSIVE). */
+#define FZ_ASSIST_TEMP 1
+#define FZ_ASSIST_PGAS 2
+#define FZ_ASSIST_BVEC 4
+#define FZ_ASSIST_VLOS 8
+#define FZ_ASSIST_PROGRESSIVE 16
 typedef struct {
   int maxsteps, maxit;
   double dchi2, svdtol, isigma;
   float wstk[4];
-  int slots, pad;
+  int slots, assist;
   double fallback;
   const float* fallback_model;
   int reg_type[8];
@@ -283,6 +290,24 @@ int fz_invert_cycles_device(fz_ctx* ctx, int nx, int ny, const double* d_obs, fl
 int fz_lsf_gaussian(fz_ctx* ctx, int region, double sigma, double w0);
 int fz_lsf_kernel(fz_ctx* ctx, int region, const double* yk, int n);
 int fz_lsf_clear(fz_ctx* ctx);
+
+/* SET_TAU's assists (src/invert3d.f90:492-727) on an NX x NY field (pixel
+ * iy + NY*ix) before a cycle: from the observations' Stokes I of the first
+ * spectral region summed over the field, three template vectors (the
+ * normalised sum and its two centred derivatives); per pixel, with field
+ * maxima as the scale:
+ *   FZ_ASSIST_BVEC  Bx, By from the Q, U projections on the second
+ *                   derivative (azimuth atan2(U,Q)/2, 1000 G at the field
+ *                   maximum), Bz from the V projection on the first (-1000 G)
+ *   FZ_ASSIST_VLOS  v_z from the I projection on the first derivative less
+ *                   its component along the sum (-2 km/s at the maximum)
+ *   FZ_ASSIST_TEMP  T shifted so that T at height CEILING(NZ/3) is the
+ *                   brightness temperature of the mean I (6390 K at I = 1)
+ *   FZ_ASSIST_PGAS  Pg scaled to 1.333e5 at that height
+ * with TEMP or PGAS, a plain synthesis with Pg given then updates rho, Pe,
+ * mu and log tau5.  Constant-in-height B and v_z, as the reference. */
+int fz_set_tau_device(fz_ctx* ctx, int nx, int ny, const double* d_obs, float* d_models, int assist, void* stream);
+int fz_set_tau(fz_ctx* ctx, int nx, int ny, const double* obs, float* models, int assist);
 
 /* The errors mode (GET_ERRORS3DS / GET_ERROR_1D / NEW_SOLVE_ERRORS,
  * src/get_dmodel.f90:1248-1323, :1581-1703), replacing the per-pixel worker
