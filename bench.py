@@ -296,7 +296,12 @@ def main():
             "chi": torch.empty(a.tile, dtype=torch.float64, device="cuda"),
             "it": torch.empty(a.tile, dtype=torch.int32, device="cuda"),
             "st": torch.empty(a.tile, dtype=torch.int32, device="cuda")}
-    results = {"nn": {}, "plain": {}, "free": {}, "raw": {}}
+    results = {"nn": {}, "plain": {}, "free": {}, "raw": {}, "tau": {}}
+    # the reference's own non-learned guess: SET_TAU's T, B and v_z assists
+    # on the default model over the tile as a 512 x 256 field
+    tau_init = torch.empty_like(base)
+    tau_ny = 256
+    tau_nx = a.tile // tau_ny
     targets = {}
     # the headline arm's fallback: a pixel whose NN-warm search ends above
     # 1.1x its plain chi2 restarts once from the default guess in the same pool
@@ -311,7 +316,14 @@ def main():
     def step(i, arm):
         k = i % ntiles
         o = obs[k * a.tile:(k + 1) * a.tile]
-        init = base if arm == "plain" else warm.initial_models_device(obs32[k * a.tile:(k + 1) * a.tile], base)
+        if arm == "plain":
+            init = base
+        elif arm == "tau":
+            init = tau_init
+            init.copy_(base)
+            ctx.set_tau_device(tau_nx, tau_ny, o.data_ptr(), init.data_ptr(), ("temp", "bvec", "vlos"), stream=stream)
+        else:
+            init = warm.initial_models_device(obs32[k * a.tile:(k + 1) * a.tile], base)
         tgt = targets[k].data_ptr() if arm in ("nn", "raw") else 0
         ctx.invert_device(a.tile, o.data_ptr(), init.data_ptr(), outs[(arm, k)].data_ptr(), bufs["chi"].data_ptr(),
                           bufs["it"].data_ptr(), bufs["st"].data_ptr(), hydrostatic=True,
@@ -368,10 +380,15 @@ def main():
     # NN-warm LM with the plain stop rules only (its own chi2)
     ms_fr, _, _ = timed("free", a.steps, 0, "free")
     free_value = world * a.tile / (ms_fr * 1e-3)
-    common = sorted(set(results["plain"]) & set(results["nn"]) & set(results["free"]) & set(results["raw"]))
+    # plain LM from SET_TAU's assisted guess (the plain stop rules)
+    ms_tau, _, _ = timed("tau", a.steps, 0, "tau")
+    tau_value = world * a.tile / (ms_tau * 1e-3)
+    common = sorted(set(results["plain"]) & set(results["nn"]) & set(results["free"]) & set(results["raw"])
+                    & set(results["tau"]))
     cat = lambda arm, j: np.concatenate([results[arm][k][j] for k in common])  # noqa: E731
     chi_nn, chi_pl, chi_fr, chi_rw = cat("nn", 0), cat("plain", 0), cat("free", 0), cat("raw", 0)
     it_nn, it_pl, it_fr, it_rw = cat("nn", 1), cat("plain", 1), cat("free", 1), cat("raw", 1)
+    chi_tau, it_tau = cat("tau", 0), cat("tau", 1)
     status_bad = max(results[arm][k][2] for arm in results for k in results[arm])
 
     # ------------------------------------------------------ parameter errors
@@ -394,7 +411,8 @@ def main():
         return torch.cat([src(k) for k in common])
 
     tru_c = tiles(lambda k: true_models[k * a.tile:(k + 1) * a.tile])
-    errors = {arm: height_errors(tiles(lambda k: outs[(arm, k)]), tru_c) for arm in ("plain", "nn", "free", "raw")}
+    errors = {arm: height_errors(tiles(lambda k: outs[(arm, k)]), tru_c)
+              for arm in ("plain", "nn", "free", "raw", "tau")}
     errors["nn_prior"] = height_errors(
         tiles(lambda k: warm.initial_models_device(obs32[k * a.tile:(k + 1) * a.tile], base)), tru_c)
     errors["default_guess"] = height_errors(base[:1].expand(tru_c.shape[0], -1, -1), tru_c)
@@ -695,6 +713,12 @@ def main():
                             "median_chi2": float(np.median(chi_fr)), "mean_iterations": float(it_fr.mean()),
                             "speedup_vs_plain": free_value / plain_value,
                             "frac_pixels_chi2_above_1.1x_plain": float(np.mean(chi_fr > 1.1 * chi_pl))},
+           "set_tau_plain": {"value": tau_value, "definition": "LM with the plain stop rules from the default "
+                                                             "model after SET_TAU's T, B and v_z assists over the "
+                                                             "tile (the reference's non-learned initial guess)",
+                             "median_chi2": float(np.median(chi_tau)), "mean_iterations": float(it_tau.mean()),
+                             "speedup_vs_plain": tau_value / plain_value,
+                             "frac_pixels_chi2_above_1.1x_plain": float(np.mean(chi_tau > 1.1 * chi_pl))},
            "parameter_errors": dict(errors, definition="errors of T, Bz, v_z and |B_perp| of the inverted "
                                            "atmospheres against the true ones at the heights where the true "
                                            "log tau5 is in [-3, 0], over the compared pixels"),

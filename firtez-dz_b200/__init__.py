@@ -147,8 +147,8 @@ def lib():
         L.fz_lsf_gaussian.argtypes = [P, I, ctypes.c_double, ctypes.c_double]
         L.fz_lsf_kernel.argtypes = [P, I, P, I]
         L.fz_lsf_clear.argtypes = [P]
-        L.fz_set_tau.argtypes = [P, I, I, P, P, I]
-        L.fz_set_tau_device.argtypes = [P, I, I, P, P, I, P]
+        L.fz_set_tau.argtypes = [P, I, I, P, P, I, I]
+        L.fz_set_tau_device.argtypes = [P, I, I, P, P, I, I, P]
         L.fz_model_to_v3_device.argtypes = [I, I, I, P, P, P, P, P]
         L.fz_obs_from_v3_device.argtypes = [I, I, P, P, P]
         L.fz_syn_to_v3_device.argtypes = [I, I, P, P, P]
@@ -176,6 +176,14 @@ def assist_bits(names):
     for n in names or ():
         b |= ASSIST[n.lower()]
     return b
+
+
+def he_mode(hydrostatic):
+    """FZ_HE_* of a hydrostatic argument: False/0 Pg given, True/1 from the
+    top (HYDRO_TOP), "ltau"/2 from the height of least |log tau5|."""
+    if isinstance(hydrostatic, str):
+        return {"none": 0, "top": 1, "ltau": 2}[hydrostatic]
+    return 2 if hydrostatic == 2 else int(bool(hydrostatic))
 
 
 def _check(rc):
@@ -266,7 +274,7 @@ class Synthesis:
         syn = np.zeros((ncol, 4, self.numw))
         mo = np.empty_like(m)
         st = np.zeros(ncol, dtype=np.int32)
-        _check(lib().fz_forward(self._h, ncol, _p(m), int(bool(hydrostatic)), _p(syn), _p(mo), _p(st)))
+        _check(lib().fz_forward(self._h, ncol, _p(m), he_mode(hydrostatic), _p(syn), _p(mo), _p(st)))
         return syn, mo, st
 
     def forward_device_static(self, model_ptr, ncol, syn_ptr, model_out_ptr, status_ptr=0, stream=0,
@@ -274,7 +282,7 @@ class Synthesis:
         """forward_device without any device allocation: the per-call scratch is
         a 64 MiB static device array (batches larger than it are rejected).
         For callers that must not allocate device memory during a call."""
-        _check(lib().fz_forward_device_static(self._h, int(ncol), ctypes.c_void_p(model_ptr), int(bool(hydrostatic)),
+        _check(lib().fz_forward_device_static(self._h, int(ncol), ctypes.c_void_p(model_ptr), he_mode(hydrostatic),
                                               ctypes.c_void_p(syn_ptr), ctypes.c_void_p(model_out_ptr),
                                               ctypes.c_void_p(status_ptr) if status_ptr else None,
                                               ctypes.c_void_p(stream) if stream else None))
@@ -325,7 +333,7 @@ class Synthesis:
         jac = np.zeros((ncol, self.np, 4 * self.numw), dtype=np.float32)
         mo = np.empty_like(m)
         st = np.zeros(ncol, dtype=np.int32)
-        _check(lib().fz_forward_rf(self._h, ncol, _p(m), int(bool(hydrostatic)), _p(syn), _p(jac), _p(mo), _p(st)))
+        _check(lib().fz_forward_rf(self._h, ncol, _p(m), he_mode(hydrostatic), _p(syn), _p(jac), _p(mo), _p(st)))
         return syn, jac, mo, st
 
     def forward_rf_full(self, model, hydrostatic=False):
@@ -345,7 +353,7 @@ class Synthesis:
         rf = np.zeros((ncol, 6, self.nz, 4 * self.numw), dtype=np.float32)
         mo = np.empty_like(m)
         st = np.zeros(ncol, dtype=np.int32)
-        _check(lib().fz_forward_rf_full(self._h, ncol, _p(m), int(bool(hydrostatic)), _p(syn), _p(rf), _p(mo),
+        _check(lib().fz_forward_rf_full(self._h, ncol, _p(m), he_mode(hydrostatic), _p(syn), _p(rf), _p(mo),
                                         _p(st)))
         return syn, rf, mo, st
 
@@ -416,7 +424,7 @@ class Synthesis:
         _check(lib().fz_smooth_device(self._h, int(nx), int(ny), ctypes.c_void_p(models_ptr),
                                       None if f is None else _p(f), ctypes.c_void_p(stream) if stream else None))
 
-    def set_tau(self, obs, models, nx, ny, assist=("temp", "bvec", "vlos")):
+    def set_tau(self, obs, models, nx, ny, assist=("temp", "bvec", "vlos"), hydrostatic=True):
         """SET_TAU's assists on host arrays: obs (nx*ny, 4, numw), models
         (nx*ny, 13, nz) (pixel iy + ny*ix); assist: names among temp, pgas,
         bvec, vlos.  Returns the assisted models."""
@@ -424,8 +432,14 @@ class Synthesis:
         m = np.array(models, dtype=np.float32, order="C", copy=True)
         if o.shape != (nx * ny, 4, self.numw) or m.shape != (nx * ny, 13, self.nz):
             raise ValueError("obs must be (nx*ny, 4, numw) and models (nx*ny, 13, nz)")
-        _check(lib().fz_set_tau(self._h, int(nx), int(ny), _p(o), _p(m), assist_bits(assist)))
+        _check(lib().fz_set_tau(self._h, int(nx), int(ny), _p(o), _p(m), assist_bits(assist), int(bool(hydrostatic))))
         return m
+
+    def set_tau_device(self, nx, ny, obs_ptr, models_ptr, assist=("temp", "bvec", "vlos"), hydrostatic=True, stream=0):
+        """SET_TAU's assists in place on device models (see set_tau())."""
+        _check(lib().fz_set_tau_device(self._h, int(nx), int(ny), ctypes.c_void_p(obs_ptr),
+                                       ctypes.c_void_p(models_ptr), assist_bits(assist), int(bool(hydrostatic)),
+                                       ctypes.c_void_p(stream) if stream else None))
 
     def lsf_gaussian(self, region, sigma, w0=0.0):
         """The reference's Gaussian line spread function (sigma, centre w0 in
@@ -574,7 +588,7 @@ class Synthesis:
 
     def forward_device(self, model_ptr, ncol, syn_ptr, model_out_ptr, status_ptr=0, stream=0, hydrostatic=False):
         """Enqueue a synthesis on device pointers (e.g. torch ``data_ptr()``)."""
-        _check(lib().fz_forward_device(self._h, int(ncol), ctypes.c_void_p(model_ptr), int(bool(hydrostatic)),
+        _check(lib().fz_forward_device(self._h, int(ncol), ctypes.c_void_p(model_ptr), he_mode(hydrostatic),
                                        ctypes.c_void_p(syn_ptr), ctypes.c_void_p(model_out_ptr),
                                        ctypes.c_void_p(status_ptr) if status_ptr else None,
                                        ctypes.c_void_p(stream) if stream else None))

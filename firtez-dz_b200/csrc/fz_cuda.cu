@@ -185,6 +185,102 @@ __global__ void __launch_bounds__(128) k_chain(const Consts* __restrict__ Kg, co
   if (lane == 0 && status) status[col] = st;
 }
 
+// HE anchored at the height of least |log tau5| of the input model
+// (RK4_INTEGRATION_LOG_LTAUM05 -> _MED, src/hydrostatic_tools.f90:226-346;
+// FORWARD1D with HYDROSTATIC and HYDRO_TOP off, src/forward.f90:890-905):
+// Pg kept there, RK4_LOG steps up to the top, then from the anchor down to
+// the bottom with NELEC restarted from the anchor's Pe.  One warp per
+// column (the synthesis-only entry points and SET_TAU use it; the
+// inversion integrates from the top, k_chain).
+__global__ void __launch_bounds__(128) k_chain_med(const Consts* __restrict__ Kg, const PFTable* __restrict__ tb,
+                                                   int ncol, int nz, const float* model, float* mout,
+                                                   double2* __restrict__ chem, int* __restrict__ status) {
+  constexpr int L = 32;
+  constexpr int NS = WarpSahaT<L>::NS;
+  __shared__ Consts K;
+  copy_to_shared(&K, Kg);
+  __syncthreads();
+  const int lane = threadIdx.x & (L - 1);
+  const int col = (int)((blockIdx.x * (size_t)blockDim.x + threadIdx.x) / L);
+  if (col >= ncol) return;
+  const float* m = model + (size_t)col * 13 * nz;
+  float* mo = mout + (size_t)col * 13 * nz;
+  double2* ch = chem + (size_t)col * nz;
+  // the anchor from the input model, before mo (which may alias m) changes
+  int iz = 0;
+  for (int k = 1; k < nz; ++k)
+    if (fabsf(mget(m, nz, 11, k)) < fabsf(mget(m, nz, 11, iz))) iz = k;
+  __syncwarp();
+  if (mo != m)
+    for (int i = lane; i < 13 * nz; i += L) mo[i] = m[i];
+  __syncwarp();
+  double ab[NS];
+#pragma unroll
+  for (int j = 0; j < NS; ++j) ab[j] = K.lane_elem[L * j + lane] >= 0 ? K.ab10[K.lane_elem[L * j + lane]] : 0.0;
+  int st = 0;
+  const double tz = (double)mget(mo, nz, 0, iz);
+  double nelec = (double)mget(mo, nz, 3, iz) / KBOL / tz;
+  const double ua = log((double)mget(mo, nz, 1, iz));
+  WarpSahaT<L> w;
+  saha_prepare(w, tz, K, tb, lane);
+  double nelec_down;
+  {
+    const RhoOut r = get_rho_warp(w, ab, exp(ua), nelec, K, lane);
+    st |= r.status;
+    nelec_down = r.pelec / KBOL / tz;
+    __syncwarp();
+    if (lane == 0) {
+      const float pel = (float)r.pelec;
+      mo[1 * nz + iz] = (float)exp(ua);
+      mo[2 * nz + iz] = (float)r.dens;
+      mo[3 * nz + iz] = pel;
+      mo[4 * nz + iz] = (float)r.molecw;
+      ch[iz] = make_double2(r.nhyd, (double)pel / KBOL / tz);
+    }
+  }
+  // the Saha buffer holds T(kf) when a step from kf to kt starts
+  auto step = [&](int kf, int kt, double& t0, double& u0) {
+    const double dz = ((double)mget(m, nz, 12, kt) - (double)mget(m, nz, 12, kf)) * 1000.0 * 100.0;
+    const double tm0 = (double)mget(m, nz, 0, kf), tm1 = (double)mget(m, nz, 0, kt);
+    const double it1 = t0 + dz / 2.0;
+    const double tmid = tm0 / dz * (t0 + dz - it1) + tm1 / dz * (it1 - t0);
+    double kk[4] = {0.0, 0.0, 0.0, 0.0};
+    double u1 = 0.0;
+#pragma unroll 1
+    for (int stg = 0; stg < 5; ++stg) {
+      if (stg == 1 || stg == 3) saha_prepare(w, stg == 1 ? tmid : tm1, K, tb, lane);
+      const double tem = stg == 0 ? tm0 : (stg < 3 ? tmid : tm1);
+      const double y = stg == 0 ? u0 : (stg == 1 ? u0 + kk[0] / 2.0 : (stg == 2 ? u0 + kk[1] / 2.0 : (stg == 3 ? u0 + kk[2] : u1)));
+      const RhoOut q = get_rho_warp(w, ab, exp(y), nelec, K, lane);
+      st |= q.status;
+      if (stg < 4) {
+        const double d = (-q.molecw * MAMU * GRAV / (KBOL * tem)) * dz;
+        kk[stg] = d;
+        if (stg == 3) u1 = u0 + 1.0 / 6.0 * (kk[0] + 2.0 * kk[1] + 2.0 * kk[2] + kk[3]);
+      } else if (lane == 0) {
+        const float pel = (float)q.pelec;
+        mo[1 * nz + kt] = (float)exp(u1);
+        mo[2 * nz + kt] = (float)q.dens;
+        mo[3 * nz + kt] = pel;
+        mo[4 * nz + kt] = (float)q.molecw;
+        ch[kt] = make_double2(q.nhyd, (double)pel / KBOL / tm1);
+      }
+    }
+    u0 = u1;
+    t0 = t0 + dz;
+  };
+  double t0 = (double)mget(m, nz, 12, iz) * 1000.0 * 100.0, u0 = ua;
+  for (int k = iz + 1; k < nz; ++k) step(k - 1, k, t0, u0);
+  if (iz > 0) {
+    t0 = (double)mget(m, nz, 12, iz) * 1000.0 * 100.0;
+    u0 = ua;
+    nelec = nelec_down;
+    saha_prepare(w, tz, K, tb, lane);
+    for (int k = iz - 1; k >= 0; --k) step(k + 1, k, t0, u0);
+  }
+  if (lane == 0 && status) status[col] = st;
+}
+
 // ------------------------------------------------------------------ k_opac
 // One thread per (column, height): every per-height quantity of the slab.
 // KC5 and the boundary flag (src/forward.f90:926-931), KC of each region at
@@ -1422,6 +1518,11 @@ struct ProfScope {
 // (latency: every column's chain gets a warp of its own).
 void launch_k_chain(fz_ctx* c, int ncol, const float* d_model, float* d_mout, int* d_status, int hydrostatic, int wpb,
                     int lanes, cudaStream_t s) {
+  if (hydrostatic == 2) {   // HE anchored at log tau5 ~ 0 (HYDRO_TOP off)
+    const dim3 g((unsigned)(((size_t)ncol * 32 + 127) / 128));
+    k_chain_med<<<g, 128, 0, s>>>(c->d_consts, c->d_pf, ncol, c->nz, d_model, d_mout, c->d_chem, d_status);
+    return;
+  }
   if (lanes != 16 && lanes != 32) lanes = ncol >= 16 * c->nsm ? 16 : 32;
   const size_t threads = (size_t)ncol * lanes;
   const dim3 gc((unsigned)((threads + wpb * 32 - 1) / (wpb * 32)));
@@ -1582,6 +1683,7 @@ int launch_rf_stage(fz_ctx* c, int ncol, int hydrostatic, double* d_syn, float* 
 // (NFREQ, 6 NZ) per column.
 int launch_forward_rf(fz_ctx* c, int ncol, const float* d_model, int hydrostatic, double* d_syn, float* d_jac,
                       float* d_mout, int* d_status, cudaStream_t s, bool full = false) {
+  if (hydrostatic < 0 || hydrostatic > 1) return FZ_ERR_ARG;   // RFs: HE from the top only
   if (!full && (c->rf.np <= 0 || !c->d_coef)) return FZ_ERR_STATE;
   int rc = ensure_rf_scratch(c, ncol);
   if (rc) return rc;
@@ -2165,6 +2267,7 @@ int fz_invert_cycles_device(fz_ctx* c, int nx, int ny, const double* d_obs, floa
                             int* d_status, void* stream) {
   if (!c || nx <= 0 || ny <= 0 || !d_obs || !d_models || ncycles <= 0 || !nodes || !d_chi2 || !d_iters)
     return FZ_ERR_ARG;
+  if (hydrostatic < 0 || hydrostatic > 1) return FZ_ERR_ARG;
   FZ_CK(cudaSetDevice(c->device));
   const int npix = nx * ny;
   const size_t nm = 13 * (size_t)c->nz;
@@ -2184,7 +2287,7 @@ int fz_invert_cycles_device(fz_ctx* c, int nx, int ny, const double* d_obs, floa
       // with PROGRESSIVE, the first only (invert3d.f90:505-520)
       const int assist = opts ? (opts->assist & 15) : 0;
       if (assist && nodes[8 * cy + 1] == 0 && nodes[8 * cy + 7] == 0 && (cy == 0 || !(opts->assist & 16)))
-        if ((rc = fz_set_tau_device(c, nx, ny, d_obs, d_models, assist, s))) break;
+        if ((rc = fz_set_tau_device(c, nx, ny, d_obs, d_models, assist, hydrostatic, s))) break;
       if ((rc = fz_smooth_device(c, nx, ny, d_models, nullptr, s))) break;
       // the cycle's iterations, each pixel from a fresh LM state
       if ((rc = fz_invert_device(c, npix, d_obs, d_models, nullptr, hydrostatic, opts, d_best, d_chi2, d_iters,
@@ -2252,6 +2355,7 @@ int fz_rf_to_v3_device(int npix, int nz, int nw, const float* d_rf, float* d_out
 int fz_errors_device(fz_ctx* c, int npix, const double* d_obs, const float* d_models, int hydrostatic,
                      const fz_lm_opts* opts, float* d_err, double* d_chi2, int* d_status, void* stream) {
   if (!c || npix <= 0 || !d_obs || !d_models || !d_err || !d_chi2) return FZ_ERR_ARG;
+  if (hydrostatic < 0 || hydrostatic > 1) return FZ_ERR_ARG;
   FZ_CK(cudaSetDevice(c->device));
   LMConf C;
   int rc = lm_conf(c, npix, opts, C);
@@ -2396,7 +2500,8 @@ int fz_lsf_clear(fz_ctx* c) {
   return 0;
 }
 
-int fz_set_tau_device(fz_ctx* c, int nx, int ny, const double* d_obs, float* d_models, int assist, void* stream) {
+int fz_set_tau_device(fz_ctx* c, int nx, int ny, const double* d_obs, float* d_models, int assist, int hydrostatic,
+                      void* stream) {
   if (!c || nx <= 0 || ny <= 0 || !d_obs || !d_models || (assist & ~15)) return FZ_ERR_ARG;
   if (assist == 0) return 0;
   const int npix = nx * ny, numw = c->numw, n1 = c->regs[0].numwave, nz = c->nz;
@@ -2454,10 +2559,11 @@ int fz_set_tau_device(fz_ctx* c, int nx, int ny, const double* d_obs, float* d_m
     k_tau_apply<<<wblocks, 256, 0, s>>>(C, npix, d_proj, d_mx, d_models);
     if ((rc = cuda_fail(cudaGetLastError()))) break;
     if (assist & 3) {
-      // FORWARD3D with HYDRO_TOP off (:675-678): rho, Pe, mu and log tau5 of
-      // the new T and Pg
+      // FORWARD3D with HYDRO_TOP off (:675-678): in a hydrostatic run Pg is
+      // integrated from the anchor log tau5 = 0 (at ITZ, as just set), then
+      // rho, Pe, mu and log tau5 of the new T and Pg
       if ((rc = cuda_fail(cudaMalloc(&d_syn, (size_t)npix * 4 * numw * sizeof(double))))) break;
-      if ((rc = launch_forward(c, npix, d_models, 0, d_syn, d_models, nullptr, s))) break;
+      if ((rc = launch_forward(c, npix, d_models, hydrostatic ? 2 : 0, d_syn, d_models, nullptr, s))) break;
     }
     rc = cuda_fail(cudaStreamSynchronize(s));
   } while (false);
@@ -2469,7 +2575,7 @@ int fz_set_tau_device(fz_ctx* c, int nx, int ny, const double* d_obs, float* d_m
   return rc;
 }
 
-int fz_set_tau(fz_ctx* c, int nx, int ny, const double* obs, float* models, int assist) {
+int fz_set_tau(fz_ctx* c, int nx, int ny, const double* obs, float* models, int assist, int hydrostatic) {
   if (!c || nx <= 0 || ny <= 0 || !obs || !models) return FZ_ERR_ARG;
   FZ_CK(cudaSetDevice(c->device));
   const size_t npix = (size_t)nx * ny, nf = 4 * (size_t)c->numw, nm = 13 * (size_t)c->nz;
@@ -2483,7 +2589,7 @@ int fz_set_tau(fz_ctx* c, int nx, int ny, const double* obs, float* models, int 
       break;
     if ((rc = cuda_fail(cudaMemcpyAsync(d_m, models, npix * nm * sizeof(float), cudaMemcpyHostToDevice, c->stream))))
       break;
-    if ((rc = fz_set_tau_device(c, nx, ny, d_obs, d_m, assist, c->stream))) break;
+    if ((rc = fz_set_tau_device(c, nx, ny, d_obs, d_m, assist, hydrostatic, c->stream))) break;
     if ((rc = cuda_fail(cudaMemcpyAsync(models, d_m, npix * nm * sizeof(float), cudaMemcpyDeviceToHost, c->stream))))
       break;
     rc = cuda_fail(cudaStreamSynchronize(c->stream));
@@ -2797,6 +2903,7 @@ int fz_get_gain(fz_ctx* c, float* gain) {
 int fz_forward_device(fz_ctx* c, int ncol, const float* d_model, int hydrostatic, double* d_syn,
                       float* d_model_out, int* d_status, void* stream) {
   if (!c || ncol <= 0 || !d_model || !d_syn || !d_model_out) return FZ_ERR_ARG;
+  if (hydrostatic < 0 || hydrostatic > 2) return FZ_ERR_ARG;
   FZ_CK(cudaSetDevice(c->device));
   return launch_forward(c, ncol, d_model, hydrostatic, d_syn, d_model_out, d_status, (cudaStream_t)stream);
 }
@@ -2876,6 +2983,7 @@ int fz_invert_device(fz_ctx* c, int npix, const double* d_obs, const float* d_in
                      int hydrostatic, const fz_lm_opts* opts, float* d_model_out, double* d_chi2, int* d_iters,
                      double* d_syn_out, int* d_status, void* stream) {
   if (!c || npix <= 0 || !d_obs || !d_init || !d_model_out || !d_chi2 || !d_iters) return FZ_ERR_ARG;
+  if (hydrostatic < 0 || hydrostatic > 1) return FZ_ERR_ARG;
   FZ_CK(cudaSetDevice(c->device));
   LMConf C;
   int rc = lm_conf(c, npix, opts, C);
@@ -3404,6 +3512,7 @@ extern "C" {
 int fz_forward_device_static(fz_ctx* c, int ncol, const float* d_model, int hydrostatic, double* d_syn,
                              float* d_model_out, int* d_status, void* stream) {
   if (!c || ncol <= 0 || !d_model || !d_syn || !d_model_out) return FZ_ERR_ARG;
+  if (hydrostatic < 0 || hydrostatic > 2) return FZ_ERR_ARG;
   const size_t chem_bytes = ((size_t)ncol * c->nz * sizeof(double2) + 255) & ~(size_t)255;
   const size_t slab_bytes = (size_t)ncol * c->nz * c->sw * sizeof(float);
   if (chem_bytes + slab_bytes > FZ_NOALLOC_SCRATCH_BYTES) {
@@ -3425,7 +3534,9 @@ int fz_forward_device_static(fz_ctx* c, int ncol, const float* d_model, int hydr
   if (d_status) FZ_CK(cudaMemsetAsync(d_status, 0, ncol * sizeof(int), s));
   const int wpb = 4;
   const dim3 gc((ncol + wpb - 1) / wpb);
-  if (hydrostatic)
+  if (hydrostatic == 2)
+    k_chain_med<<<gc, wpb * 32, 0, s>>>(c->d_consts, c->d_pf, ncol, c->nz, d_model, d_model_out, chem, d_status);
+  else if (hydrostatic)
     k_chain<true, 32><<<gc, wpb * 32, 0, s>>>(c->d_consts, c->d_pf, ncol, c->nz, d_model, d_model_out, chem, d_status);
   else
     k_chain<false, 32><<<gc, wpb * 32, 0, s>>>(c->d_consts, c->d_pf, ncol, c->nz, d_model, d_model_out, chem,
@@ -3445,6 +3556,7 @@ int fz_forward_device_static(fz_ctx* c, int ncol, const float* d_model, int hydr
 int fz_forward(fz_ctx* c, int ncol, const float* model, int hydrostatic, double* syn, float* model_out,
                int* status) {
   if (!c || ncol <= 0 || !model || !syn) return FZ_ERR_ARG;
+  if (hydrostatic < 0 || hydrostatic > 2) return FZ_ERR_ARG;
   FZ_CK(cudaSetDevice(c->device));
   if ((size_t)ncol > c->io_cols) {
     cudaFree(c->d_model);

@@ -90,6 +90,16 @@ int fz_numw(const fz_ctx* ctx);
 /* Copy GAIN1D(4,NUMW) to host memory. */
 int fz_get_gain(fz_ctx* ctx, float* gain);
 
+/* hydrostatic, for the synthesis entry points (fz_forward*, not the response
+ * functions or the inversion, which take 0 or 1): 0 = Pg given (GET_NHNEMU_G),
+ * 1 = hydrostatic equilibrium integrated from the top (HYDRO_TOP,
+ * RK4_INTEGRATION_LOG), 2 = integrated from the height of least |log tau5| of
+ * the input model, Pg kept there (HYDRO_TOP off, RK4_INTEGRATION_LOG_LTAUM05,
+ * src/hydrostatic_tools.f90:226-346). */
+#define FZ_HE_NONE 0
+#define FZ_HE_TOP 1
+#define FZ_HE_LTAU 2
+
 /* Forward synthesis of ncol columns, host buffers: the batched equivalent of
  * the worker side of FORWARD3D + FORWARD1D (src/forward.f90:106-291,
  * :857-1029) without response functions.  model is read; model_out (may be
@@ -304,10 +314,13 @@ int fz_lsf_clear(fz_ctx* ctx);
  *   FZ_ASSIST_TEMP  T shifted so that T at height CEILING(NZ/3) is the
  *                   brightness temperature of the mean I (6390 K at I = 1)
  *   FZ_ASSIST_PGAS  Pg scaled to 1.333e5 at that height
- * with TEMP or PGAS, a plain synthesis with Pg given then updates rho, Pe,
- * mu and log tau5.  Constant-in-height B and v_z, as the reference. */
-int fz_set_tau_device(fz_ctx* ctx, int nx, int ny, const double* d_obs, float* d_models, int assist, void* stream);
-int fz_set_tau(fz_ctx* ctx, int nx, int ny, const double* obs, float* models, int assist);
+ * with TEMP or PGAS, a plain synthesis then updates rho, Pe, mu and log tau5:
+ * hydrostatic != 0 integrates Pg from the anchor log tau5 = 0 the assists
+ * set (hydrostatic mode 2 of fz_forward), else Pg is kept.  Constant-in-
+ * height B and v_z, as the reference. */
+int fz_set_tau_device(fz_ctx* ctx, int nx, int ny, const double* d_obs, float* d_models, int assist, int hydrostatic,
+                      void* stream);
+int fz_set_tau(fz_ctx* ctx, int nx, int ny, const double* obs, float* models, int assist, int hydrostatic);
 
 /* The errors mode (GET_ERRORS3DS / GET_ERROR_1D / NEW_SOLVE_ERRORS,
  * src/get_dmodel.f90:1248-1323, :1581-1703), replacing the per-pixel worker

@@ -836,6 +836,70 @@ int rk4_integration_log(Col& c, std::vector<double>& vnhyd) {
   return st;
 }
 
+// RK4_INTEGRATION_LOG_LTAUM05 -> RK4_INTEGRATION_LOG_MED
+// (src/hydrostatic_tools.f90:226-346): HE anchored at IZ = MINLOC(ABS(TAU5))
+// (the first least |log tau5|, from the input model), Pg(IZ) kept, RK4 up
+// to the top, then from IZ down to the bottom with NELEC restarted from the
+// anchor's Pe.
+int rk4_integration_log_med(Col& c, std::vector<double>& vnhyd) {
+  const int nz = c.nz;
+  int iz = 0;
+  for (int k = 1; k < nz; ++k)
+    if (std::fabs(c.TAU(k)) < std::fabs(c.TAU(iz))) iz = k;
+  int st = ORC_OK;
+  std::vector<double> pg8(nz, 0), rho8(nz, 0), pel8(nz, 0), mw8(nz, 0), t8(nz);
+  for (int k = 0; k < nz; ++k) t8[k] = (double)c.T(k);
+  pg8[iz] = std::log((double)c.PG(iz));
+  pel8[iz] = c.PEL(iz);
+  double nelec = pel8[iz] / KBOL / t8[iz];
+  Rho r = get_rho(t8[iz], std::exp(pg8[iz]), nelec);
+  if (r.status) st = r.status;
+  rho8[iz] = r.dens;
+  pel8[iz] = r.pelec;
+  mw8[iz] = r.molecw;
+  vnhyd[iz] = r.nhyd;
+  auto dpdz = [&](double y, double tem) {
+    Rho q = get_rho(tem, std::exp(y), nelec);
+    if (q.status) st = q.status;
+    return -q.molecw * MAMU * GRAV / (KBOL * tem);
+  };
+  // one RK4_LOG step from height kf to the adjacent kt, then GET_RHO at kt
+  auto step = [&](int kf, int kt, double& t0, double& u0) {
+    const double dz = (c.Z(kt) - c.Z(kf)) * 1000.0 * 100.0;
+    const double t1 = t0 + dz;
+    const double tm0 = t8[kf], tm1 = t8[kt];
+    const double k1 = dpdz(u0, tm0) * dz;
+    const double it1 = t0 + dz / 2.0;
+    const double tmid = tm0 / dz * (t0 + dz - it1) + tm1 / dz * (it1 - t0);
+    const double k2 = dpdz(u0 + k1 / 2.0, tmid) * dz;
+    const double k3 = dpdz(u0 + k2 / 2.0, tmid) * dz;
+    const double k4 = dpdz(u0 + k3, tm1) * dz;
+    const double u1 = u0 + 1.0 / 6.0 * (k1 + 2.0 * k2 + 2.0 * k3 + k4);
+    Rho q = get_rho(t8[kt], std::exp(u1), nelec);
+    if (q.status) st = q.status;
+    rho8[kt] = q.dens;
+    pel8[kt] = q.pelec;
+    mw8[kt] = q.molecw;
+    pg8[kt] = u1;
+    vnhyd[kt] = q.nhyd;
+    u0 = u1;
+    t0 = t1;
+  };
+  double t0 = c.Z(iz) * 1000.0 * 100.0, u0 = pg8[iz];
+  for (int k = iz + 1; k < nz; ++k) step(k - 1, k, t0, u0);
+  t0 = c.Z(iz) * 1000.0 * 100.0;
+  u0 = pg8[iz];
+  nelec = pel8[iz] / KBOL / t8[iz];
+  for (int k = iz - 1; k >= 0; --k) step(k + 1, k, t0, u0);
+  for (int k = 0; k < nz; ++k) {
+    c.PG(k) = (float)std::exp(pg8[k]);
+    c.RHO(k) = (float)rho8[k];
+    c.PEL(k) = (float)pel8[k];
+    c.MW(k) = (float)mw8[k];
+  }
+  return st;
+}
+
 // FORWARD1D without response functions, src/forward.f90:857-1029
 int forward1d(const Setup& s, const float* gain, Col& c, int hydrostatic, double* stokes) {
   const int nz = c.nz, numw = s.numw;
@@ -843,7 +907,8 @@ int forward1d(const Setup& s, const float* gain, Col& c, int hydrostatic, double
   int st = ORC_OK;
   std::vector<double> vnhyd(nz, 0.0), vnelec(nz, 0.0), kc5(nz, 0.0);
   if (hydrostatic) {
-    st = rk4_integration_log(c, vnhyd);
+    // 1: HYDRO_TOP (from the top); 2: anchored at log tau5 ~ 0 (HYDRO_TOP off)
+    st = hydrostatic == 2 ? rk4_integration_log_med(c, vnhyd) : rk4_integration_log(c, vnhyd);
     for (int k = 0; k < nz; ++k) vnelec[k] = (double)c.PEL(k) / KBOL / (double)c.T(k);
   }
   std::vector<double> syn(4 * numw, 0.0);

@@ -128,7 +128,7 @@ def forward(lines, regions, gain_, model, hydrostatic=False, nthreads=0):
     stokes = np.zeros((ncol, 4, numw))
     status = np.zeros(ncol, dtype=np.int32)
     lib().orc_forward(_p(lines), len(lines), _p(regions), len(regions), _p(g), nz, ncol, _p(m),
-                      int(bool(hydrostatic)), _p(stokes), _p(status), int(nthreads))
+                      int(hydrostatic), _p(stokes), _p(status), int(nthreads))
     return stokes, m, status
 
 

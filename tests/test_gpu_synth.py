@@ -87,3 +87,34 @@ def test_reference_fixture_with_blend(fz, orc):
     print("fixture: max rel err I %.3e, max abs err QUV %.3e" % (ei, eq))
     assert np.all(syn[0, 1:] == 0.0)          # B = 0 column
     assert ei < TOL_I and eq < TOL_QUV
+
+
+def test_hydrostatic_from_log_tau5_anchor(fz, orc):
+    """Hydrostatic equilibrium anchored at the height of least |log tau5| of
+    the input model (HYDRO_TOP off, RK4_INTEGRATION_LOG_LTAUM05): the
+    synthesis and the integrated Pg, rho, Pe, mu against the oracle's
+    restatement with the same tolerances as the top-anchored mode; Pg at the
+    anchor is kept; the anchor at the bottom and at the top columns work."""
+    lines = fz.lines_parse(fz.atmos.line_database_text())
+    reg = fz.regions_from_lines_section(fz.atmos.lines_section(2), lines)
+    g, _ = orc.gain(lines, reg)
+    nz = 64
+    ctx = fz.Synthesis(lines, reg, nz=nz, gain=g)
+    m0 = fz.atmos.make_columns(10, nz, seed=17)
+    _, m, st = orc.forward(lines, reg, g, m0, hydrostatic=True)   # a log tau5 row to anchor on
+    assert np.all(st == 0)
+    m[8, 11, :] = np.linspace(-1.0, 5.0, nz, dtype=np.float32)     # anchor at the bottom
+    m[9, 11, :] = np.linspace(-5.0, -1.0, nz, dtype=np.float32)    # anchor at the top
+    m[:, 1, :] *= np.float32(1.3)                                   # Pg off equilibrium elsewhere
+    syn, mo, st = ctx.forward(m, hydrostatic="ltau")
+    osyn, omo, ost = orc.forward(lines, reg, g, m, hydrostatic=2)
+    assert np.all(st == 0) and np.all(ost == 0)
+    assert np.max(np.abs(syn[:, 0] - osyn[:, 0]) / np.abs(osyn[:, 0])) < 1e-5
+    assert np.max(np.abs(syn[:, 1:] - osyn[:, 1:])) < 1e-6
+    for p in (1, 2, 3, 4):
+        assert np.max(np.abs(mo[:, p] / omo[:, p] - 1)) < 2e-6, p
+    iz = np.argmin(np.abs(m[:, 11, :]), axis=1)
+    np.testing.assert_allclose(mo[np.arange(10), 1, iz], m[np.arange(10), 1, iz], rtol=1.2e-7)
+    with pytest.raises(fz.FzError):
+        ctx.rf_nodes({1: 2})
+        ctx.forward_rf(m, hydrostatic=2)
