@@ -147,6 +147,10 @@ def lib():
         L.fz_lsf_gaussian.argtypes = [P, I, ctypes.c_double, ctypes.c_double]
         L.fz_lsf_kernel.argtypes = [P, I, P, I]
         L.fz_lsf_clear.argtypes = [P]
+        L.fz_hydrostatic.argtypes = [P, I, P, I, P, P]
+        L.fz_hydrostatic_device.argtypes = [P, I, P, I, P, P, P]
+        L.fz_log_tau5.argtypes = [P, I, P, I, P, P]
+        L.fz_log_tau5_device.argtypes = [P, I, P, I, P, P, P]
         L.fz_set_tau.argtypes = [P, I, I, P, P, I, I]
         L.fz_set_tau_device.argtypes = [P, I, I, P, P, I, I, P]
         L.fz_model_to_v3_device.argtypes = [I, I, I, P, P, P, P, P]
@@ -440,6 +444,25 @@ class Synthesis:
         _check(lib().fz_set_tau_device(self._h, int(nx), int(ny), ctypes.c_void_p(obs_ptr),
                                        ctypes.c_void_p(models_ptr), assist_bits(assist), int(bool(hydrostatic)),
                                        ctypes.c_void_p(stream) if stream else None))
+
+    def hydrostatic(self, model, mode=True):
+        """MODE h: hydrostatic equilibrium only (mode True/"top" or "ltau").
+        Returns (model_out, status)."""
+        return self._model_only(model, mode, lib().fz_hydrostatic)
+
+    def log_tau5(self, model, hydrostatic=False):
+        """MODE t: log tau5 (and the chemistry rows) without the synthesis.
+        Returns (model_out, status)."""
+        return self._model_only(model, hydrostatic, lib().fz_log_tau5)
+
+    def _model_only(self, model, he, fn):
+        m = np.ascontiguousarray(model, dtype=np.float32)
+        if m.ndim != 3 or m.shape[1:] != (13, self.nz):
+            raise ValueError("model must be (ncol, 13, %d)" % self.nz)
+        mo = np.empty_like(m)
+        st = np.zeros(m.shape[0], dtype=np.int32)
+        _check(fn(self._h, m.shape[0], _p(m), he_mode(he), _p(mo), _p(st)))
+        return mo, st
 
     def lsf_gaussian(self, region, sigma, w0=0.0):
         """The reference's Gaussian line spread function (sigma, centre w0 in

@@ -1922,6 +1922,26 @@ bool int_coefs(int nz, int nj, std::vector<double>& coef) {
   return true;
 }
 
+// ------------------------------------------------------------- log tau5
+// The GETTAU mode (MODE t, src/invert3d.f90:159-178 with MSYNTHESIS off):
+// log tau5 of every column from the opacity slab k_opac leaves, the
+// integration of src/forward.f90:1000-1006 (REAL*4 accumulation from the
+// top, as k_synth does), without the Stokes synthesis.
+__global__ void k_tau5(int ncol, int nz, int sw, const float* __restrict__ slab, float* __restrict__ mout) {
+  const int col = blockIdx.x * blockDim.x + threadIdx.x;
+  if (col >= ncol) return;
+  const float* sm = slab + (size_t)col * nz * sw;
+  float* mo = mout + (size_t)col * 13 * nz;
+  float tau = 1e-9f;
+  mo[11 * nz + nz - 1] = log10f(tau);
+  for (int k = nz - 2; k >= 0; --k) {
+    const float a = (sm[k * sw + 2] * sm[k * sw + 3] + sm[(k + 1) * sw + 2] * sm[(k + 1) * sw + 3]) / 2.0f;
+    const double b = ((double)mo[12 * nz + k + 1] - (double)mo[12 * nz + k]) * 1000.0 * 100.0;
+    tau = (float)((double)tau + (double)a * b);
+    mo[11 * nz + k] = log10f(tau);
+  }
+}
+
 // ------------------------------------------------------------ SMOOTHING_B
 // The 1-2-1 smoothing of the free parameters' cubes at the start of every
 // cycle (SMOOTHING_B, src/model_spatial_extension.f90:351-491, called from
@@ -2597,6 +2617,68 @@ int fz_set_tau(fz_ctx* c, int nx, int ny, const double* obs, float* models, int 
   cudaFree(d_obs);
   cudaFree(d_m);
   return rc;
+}
+
+int fz_hydrostatic_device(fz_ctx* c, int ncol, const float* d_model, int hydrostatic, float* d_model_out,
+                          int* d_status, void* stream) {
+  if (!c || ncol <= 0 || !d_model || !d_model_out || hydrostatic < 1 || hydrostatic > 2) return FZ_ERR_ARG;
+  FZ_CK(cudaSetDevice(c->device));
+  if (int rc = ensure_scratch(c, ncol)) return rc;
+  cudaStream_t s = (cudaStream_t)stream;
+  if (d_status) FZ_CK(cudaMemsetAsync(d_status, 0, ncol * sizeof(int), s));
+  launch_k_chain(c, ncol, d_model, d_model_out, d_status, hydrostatic, c->tune.chain_warps, c->tune.chain_lanes, s);
+  return cuda_fail(cudaGetLastError());
+}
+
+int fz_log_tau5_device(fz_ctx* c, int ncol, const float* d_model, int hydrostatic, float* d_model_out, int* d_status,
+                       void* stream) {
+  if (!c || ncol <= 0 || !d_model || !d_model_out || hydrostatic < 0 || hydrostatic > 2) return FZ_ERR_ARG;
+  FZ_CK(cudaSetDevice(c->device));
+  if (int rc = ensure_scratch(c, ncol)) return rc;
+  cudaStream_t s = (cudaStream_t)stream;
+  if (d_status) FZ_CK(cudaMemsetAsync(d_status, 0, ncol * sizeof(int), s));
+  launch_k_chain(c, ncol, d_model, d_model_out, d_status, hydrostatic, c->tune.chain_warps, c->tune.chain_lanes, s);
+  FZ_CK(cudaGetLastError());
+  const size_t total = (size_t)ncol * c->nz;
+  const int blocks = (int)std::min<size_t>((total + 255) / 256, (size_t)c->nsm * 16);
+  k_opac<<<blocks, 256, 0, s>>>(c->d_params, c->d_consts, ncol, d_model_out, c->d_chem, c->d_slab);
+  k_tau5<<<(ncol + 127) / 128, 128, 0, s>>>(ncol, c->nz, c->sw, c->d_slab, d_model_out);
+  return cuda_fail(cudaGetLastError());
+}
+
+// the two on host buffers (staging allocated per call)
+static int model_only_host(fz_ctx* c, int ncol, const float* model, int hydrostatic, float* model_out, int* status,
+                           bool tau) {
+  if (!c || ncol <= 0 || !model || !model_out) return FZ_ERR_ARG;
+  FZ_CK(cudaSetDevice(c->device));
+  const size_t nm = (size_t)ncol * 13 * c->nz;
+  float* d_m = nullptr;
+  int* d_st = nullptr;
+  int rc = 0;
+  do {
+    if ((rc = cuda_fail(cudaMalloc(&d_m, nm * sizeof(float))))) break;
+    if ((rc = cuda_fail(cudaMalloc(&d_st, ncol * sizeof(int))))) break;
+    if ((rc = cuda_fail(cudaMemcpyAsync(d_m, model, nm * sizeof(float), cudaMemcpyHostToDevice, c->stream)))) break;
+    rc = tau ? fz_log_tau5_device(c, ncol, d_m, hydrostatic, d_m, d_st, c->stream)
+             : fz_hydrostatic_device(c, ncol, d_m, hydrostatic, d_m, d_st, c->stream);
+    if (rc) break;
+    if ((rc = cuda_fail(cudaMemcpyAsync(model_out, d_m, nm * sizeof(float), cudaMemcpyDeviceToHost, c->stream)))) break;
+    if (status &&
+        (rc = cuda_fail(cudaMemcpyAsync(status, d_st, ncol * sizeof(int), cudaMemcpyDeviceToHost, c->stream))))
+      break;
+    rc = cuda_fail(cudaStreamSynchronize(c->stream));
+  } while (false);
+  cudaFree(d_m);
+  cudaFree(d_st);
+  return rc;
+}
+
+int fz_hydrostatic(fz_ctx* c, int ncol, const float* model, int hydrostatic, float* model_out, int* status) {
+  return model_only_host(c, ncol, model, hydrostatic, model_out, status, false);
+}
+
+int fz_log_tau5(fz_ctx* c, int ncol, const float* model, int hydrostatic, float* model_out, int* status) {
+  return model_only_host(c, ncol, model, hydrostatic, model_out, status, true);
 }
 
 int fz_smooth(fz_ctx* c, int nx, int ny, float* models, const int* params) {

@@ -135,6 +135,21 @@ int fz_forward_device(fz_ctx* ctx, int ncol, const float* d_model, int hydrostat
 int fz_forward_device_static(fz_ctx* ctx, int ncol, const float* d_model, int hydrostatic, double* d_syn,
                              float* d_model_out, int* d_status, void* stream);
 
+/* The model-only modes of FIRTEZ-dz (MODE h / t, src/invert3d.f90:159-178):
+ *   fz_hydrostatic: hydrostatic equilibrium only (MGETHEQ; FORWARD1D stops
+ *     after the HE integration, src/forward.f90:890-909): Pg, rho, Pe, mu of
+ *     model_out; hydrostatic = FZ_HE_TOP or FZ_HE_LTAU.
+ *   fz_log_tau5: the GETTAU mode (MGETTAU): chemistry (HE as hydrostatic
+ *     says), the continuum opacity at 5000 A and log tau5 from the top
+ *     (src/forward.f90:1000-1006), without the Stokes synthesis.
+ * model_out may equal model; status as fz_forward. */
+int fz_hydrostatic(fz_ctx* ctx, int ncol, const float* model, int hydrostatic, float* model_out, int* status);
+int fz_hydrostatic_device(fz_ctx* ctx, int ncol, const float* d_model, int hydrostatic, float* d_model_out,
+                          int* d_status, void* stream);
+int fz_log_tau5(fz_ctx* ctx, int ncol, const float* model, int hydrostatic, float* model_out, int* status);
+int fz_log_tau5_device(fz_ctx* ctx, int ncol, const float* d_model, int hydrostatic, float* d_model_out,
+                       int* d_status, void* stream);
+
 /* Response functions.  fz_rf_nodes selects the free parameters and their
  * node counts, nodes[p-1] for the reference parameter p of atm_param.f90
  * (1 T, 2 Pg, 4 Bx, 5 By, 6 Bz, 7 v_z; 3 rho and 8 P0 must be 0); the hat

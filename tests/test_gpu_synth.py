@@ -118,3 +118,24 @@ def test_hydrostatic_from_log_tau5_anchor(fz, orc):
     with pytest.raises(fz.FzError):
         ctx.rf_nodes({1: 2})
         ctx.forward_rf(m, hydrostatic=2)
+
+
+@pytest.mark.parametrize("he", [False, True, "ltau"])
+def test_model_only_modes(fz, orc, he):
+    """MODE t (log tau5 without the synthesis) and MODE h (HE only) give the
+    same model rows, bit for bit, as the full synthesis computes them."""
+    lines = fz.lines_parse(fz.atmos.line_database_text())
+    reg = fz.regions_from_lines_section(fz.atmos.lines_section(2), lines)
+    g, _ = orc.gain(lines, reg)
+    nz = 48
+    ctx = fz.Synthesis(lines, reg, nz=nz, gain=g)
+    _, m, _ = orc.forward(lines, reg, g, fz.atmos.make_columns(20, nz, seed=3), hydrostatic=True)
+    _, mo, st = ctx.forward(m, hydrostatic=he)
+    assert np.all(st == 0)
+    mt, st2 = ctx.log_tau5(m, hydrostatic=he)
+    assert np.all(st2 == 0)
+    np.testing.assert_array_equal(mt, mo)
+    if he:
+        mh, _ = ctx.hydrostatic(m, mode=he)
+        np.testing.assert_array_equal(mh[:, :5], mo[:, :5])
+        np.testing.assert_array_equal(mh[:, 5:11], m[:, 5:11])
