@@ -18,8 +18,9 @@ inversion call), inputs resident in HBM.  The plain arm (LM from the default
 guess) runs first and is the judge: its per-pixel chi2 is the goal of the
 headline arm.  ``value`` = converged pixels per second of NN-warm LM (network
 inference + batched LM) where a pixel is converged once its chi2 reaches its
-plain-LM chi2 (or by the plain stop rules), a pixel stopping above 1.1x its
-plain chi2 restarting once from the default guess in the same pool --
+plain-LM chi2 (or by the plain stop rules), a pixel whose search stagnates
+while above 1.1x its plain chi2 restarting once from the default guess in the
+same pool --
 "converged pixels/s at plain-LM chi2".  Beside it: the same arm without the
 restart and NN-warm LM with the plain stop rules only.  ``e2e``: the headline
 arm through the host-buffer calls from pinned host memory.  Multi-GPU: each
@@ -303,11 +304,12 @@ def main():
     tau_ny = 256
     tau_nx = a.tile // tau_ny
     targets = {}
-    # the headline arm's fallback: a pixel whose NN-warm search ends above
-    # 1.1x its plain chi2 restarts once from the default guess in the same pool
+    # the headline arm's fallback: a pixel whose NN-warm search stagnates (one
+    # rejected or too-small step) while above 1.1x its plain chi2 restarts
+    # once from the default guess in the same pool
     fb_model = base[0].contiguous()
     opts_nn = fz.LMOpts(maxsteps=5, maxit=40, dchi2=1e-3, isigma=1e-3, slots=opts.slots, fallback=1.1,
-                        fallback_model=fb_model.data_ptr())
+                        fallback_model=fb_model.data_ptr(), fallback_steps=1)
     # one output model buffer per (arm, tile), allocated before any timing:
     # the inverted models are compared with the true atmospheres afterwards
     outs = {(arm, k): torch.empty((a.tile, 13, a.nz), dtype=torch.float32, device="cuda")
@@ -370,8 +372,8 @@ def main():
     ms_pl, clocks_pl, _ = timed("plain", a.steps, a.warmup, "plain")
     plain_value = world * a.tile / (ms_pl * 1e-3)
     # headline: NN-warm LM, each pixel converged once it reaches its plain-LM
-    # chi2; a pixel that stops above 1.1x it restarts once from the default
-    # guess in the same pool (plain LM stays the fallback and the judge)
+    # chi2; a pixel that stagnates above 1.1x it restarts once from the
+    # default guess in the same pool (plain LM stays the fallback and the judge)
     ms_nn, clocks, prof = timed("nn", a.steps, a.warmup, "nn", profile=True)
     value = world * a.tile / (ms_nn * 1e-3)
     # the same without the fallback
@@ -473,7 +475,7 @@ def main():
     h_fb = pin((13, a.nz), torch.float32)
     h_fb[:] = fb_model.cpu().numpy()
     opts_e2e = fz.LMOpts(maxsteps=5, maxit=40, dchi2=1e-3, isigma=1e-3, slots=opts.slots, fallback=1.1,
-                         fallback_model=h_fb.ctypes.data)   # a host pointer for the host-buffer call
+                         fallback_model=h_fb.ctypes.data, fallback_steps=1)   # a host pointer for the host-buffer call
 
     def e2e_step():
         warm.initial_models(h_obs, out=h_init)
@@ -696,14 +698,14 @@ def main():
                      "median_chi2": float(np.median(chi_pl)), "mean_iterations": float(it_pl.mean()),
                      "clocks": clocks_pl},
            "nn_warm": {"value": value, "definition": "NN-warm LM; a pixel is converged when its chi2 reaches its "
-                                                     "plain-LM chi2 or by the plain stop rules; a pixel that "
-                                                     "stops above 1.1x its plain chi2 restarts once from the "
-                                                     "default guess in the same slot pool",
+                                                     "plain-LM chi2 or by the plain stop rules; a pixel whose "
+                                                     "search stagnates once (a rejected or too-small step, "
+                                                     "STEPS >= 1) while above 1.1x its plain chi2 restarts once "
+                                                     "from the default guess in the same slot pool",
                        "median_chi2": float(np.median(chi_nn)), "mean_iterations": float(it_nn.mean()),
                        "speedup_vs_plain": value / plain_value,
                        "frac_pixels_at_or_below_plain_chi2": float(np.mean(chi_nn <= chi_pl)),
                        "frac_pixels_chi2_above_1.1x_plain": float(np.mean(chi_nn > 1.1 * chi_pl)),
-                       "frac_pixels_restarted": float(np.mean(chi_rw > 1.1 * chi_pl)),
                        "pixels_compared": int(chi_nn.size), "status_errors": status_bad, "mlp": mlp_info},
            "nn_warm_no_fallback": {"value": raw_value, "definition": "the headline arm without the restart",
                                    "median_chi2": float(np.median(chi_rw)), "mean_iterations": float(it_rw.mean()),

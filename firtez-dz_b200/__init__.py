@@ -63,23 +63,26 @@ class LMOpts(ctypes.Structure):
     _fields_ = [("maxsteps", ctypes.c_int), ("maxit", ctypes.c_int), ("dchi2", ctypes.c_double),
                 ("svdtol", ctypes.c_double), ("isigma", ctypes.c_double), ("wstk", ctypes.c_float * 4),
                 ("slots", ctypes.c_int), ("assist", ctypes.c_int), ("fallback", ctypes.c_double),
-                ("fallback_model", ctypes.c_void_p), ("reg_type", ctypes.c_int * 8), ("reg_alpha", ctypes.c_double * 8)]
+                ("fallback_model", ctypes.c_void_p), ("reg_type", ctypes.c_int * 8), ("reg_alpha", ctypes.c_double * 8),
+                ("fallback_steps", ctypes.c_int), ("pad2", ctypes.c_int)]
 
     def __init__(self, maxsteps=5, maxit=40, dchi2=0.0, svdtol=1e-4, isigma=4e-3, wstk=(1, 1, 1, 1), slots=0,
-                 fallback=0.0, fallback_model=0, reg=None, assist=()):
+                 fallback=0.0, fallback_model=0, reg=None, assist=(), fallback_steps=0):
         """fallback_model: device pointer of one MODEL(NZ,13) float32 (e.g. a
         torch tensor's data_ptr()) that pixels ending above fallback x their
         chi2 goal restart from (a host pointer for invert()).  reg: optional
         {reference parameter: (type, alpha)} vertical regularisation
         (VERTICAL REGULARIZATION: type 0 or 1, PEN_ALP).  assist: SET_TAU's
-        assists for invert_cycles (temp, pgas, bvec, vlos, progressive)."""
+        assists for invert_cycles (temp, pgas, bvec, vlos, progressive).
+        fallback_steps: restart once STEPS reaches it while above fallback x
+        the goal (0: when the search ends)."""
         typ, alp = [0] * 8, [0.0] * 8
         for p, (t, a) in (reg or {}).items():
             typ[int(p) - 1], alp[int(p) - 1] = int(t), float(a)
         super().__init__(maxsteps, maxit, dchi2, svdtol, isigma, (ctypes.c_float * 4)(*wstk), slots,
                          assist_bits(assist),
                          float(fallback), fallback_model or None, (ctypes.c_int * 8)(*typ),
-                         (ctypes.c_double * 8)(*alp))
+                         (ctypes.c_double * 8)(*alp), int(fallback_steps), 0)
 
 
 class Tune(ctypes.Structure):

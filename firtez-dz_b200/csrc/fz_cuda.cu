@@ -1846,6 +1846,7 @@ int lm_conf(fz_ctx* c, int npix, const fz_lm_opts* o, LMConf& C) {
   C.inu = (double)C.nfreq;
   C.fallback = o && o->fallback_model ? o->fallback : 0.0;
   C.fb_model = o ? o->fallback_model : nullptr;
+  C.fb_steps = o && o->fallback_steps > 0 ? o->fallback_steps : (1 << 30);
   // GET_IT_PENALTIES operators (src/get_dmodel.f90:1103-1146): per free
   // parameter L = sqrt(PEN_ALP / IFREEP) D, D = diag(1/NJ) (type 0) or first
   // differences to the previous node (type 1); PEN_HSS = L^T L block diagonal

@@ -36,6 +36,7 @@ struct LMConf {
   double dchi2, svdtol, inu;
   double fallback;             // restart factor on the chi2 goal (0 = off)
   const float* fb_model;       // MODEL(NZ,13) a restarted pixel starts from
+  int fb_steps;                // restart once STEPS reaches this while above fallback x goal
   int reg;                     // vertical regularisation on (GET_IT_PENALTIES)
   double reg_hss[LM_MAXNP * LM_MAXNP];   // PEN_HSS = L^T L (model independent)
   int nodes_ref[8];            // node count per reference parameter
@@ -164,7 +165,7 @@ __global__ void __launch_bounds__(256) k_lm_accept(LMConf C, LMSlots Sl, LMQueue
                                                    const double* __restrict__ coef) {
   __shared__ double red[8];
   __shared__ double xs[LM_MAXNP], pr[LM_MAXNP];
-  __shared__ int acc, fin, np_next;
+  __shared__ int acc, fin, early, np_next;
   const int s = blockIdx.x;
   if (threadIdx.x == 0) {
     Sl.skip[s] = 0;
@@ -225,6 +226,10 @@ __global__ void __launch_bounds__(256) k_lm_accept(LMConf C, LMSlots Sl, LMQueue
     // optional per-pixel goal: stop once the best chi2 reaches it
     const bool goal = target != nullptr && chipre <= target[p];
     fin = steps > (double)C.maxsteps || it >= C.maxit || small || goal;
+    // an early restart: the search has stagnated fb_steps times and is still
+    // above fallback x its goal
+    early = !fin && C.fallback > 0.0 && C.fb_model && target && !Sl.restarted[s] && steps >= (double)C.fb_steps &&
+            chipre > C.fallback * target[p];
     st[0] = chi;
     st[1] = chipre;
     st[2] = lam;
@@ -238,7 +243,7 @@ __global__ void __launch_bounds__(256) k_lm_accept(LMConf C, LMSlots Sl, LMQueue
     for (int i = threadIdx.x; i < nm; i += blockDim.x) mb[i] = mc[i];
     double* sb = Sl.synb + (size_t)s * nf;
     for (int i = threadIdx.x; i < nf; i += blockDim.x) sb[i] = syn[i];
-    if (threadIdx.x == 0 && !fin) Sl.need_rf[s] = 1;
+    if (threadIdx.x == 0 && !fin && !early) Sl.need_rf[s] = 1;
   } else {
     const float* mb = Sl.mbest + (size_t)s * nm;
     float* mc = Sl.mcur + (size_t)s * nm;
@@ -258,7 +263,8 @@ __global__ void __launch_bounds__(256) k_lm_accept(LMConf C, LMSlots Sl, LMQueue
     }
     if (threadIdx.x < C.np) Sl.pen[(size_t)s * C.np + threadIdx.x] = pr[threadIdx.x];
   }
-  if (fin && C.fallback > 0.0 && C.fb_model && target && !Sl.restarted[s] && st[1] > C.fallback * target[p]) {
+  if ((fin || early) && C.fallback > 0.0 && C.fb_model && target && !Sl.restarted[s] &&
+      st[1] > C.fallback * target[p]) {
     // the search ended above fallback x its goal: start once more from the
     // fallback model (INITIALIZE_CYCLE's state), the goal kept
     float* mc = Sl.mcur + (size_t)s * nm;

@@ -245,6 +245,10 @@ int fz_smooth_device(fz_ctx* ctx, int nx, int ny, float* d_models, const int* pa
  * 1..8: type 0 (node values to zero, D = diag(1/NJ)) or 1 (differences to
  * the previous node) and PEN_ALP (0: off); chi2 gains sum(PEN_RES^2) of the
  * current model, the normal equations PEN_HSS and -PEN_RES of the best.
+ * fallback_steps: with fallback on, a pixel restarts as soon as its
+ * stagnation counter (the STEPS of UPDATE_LAMBDA) reaches fallback_steps
+ * while its best chi2 is still above fallback x its goal, instead of when
+ * its search ends (0: when it ends).
  * assist: SET_TAU's initial-guess assists for fz_invert_cycles_device
  * (FZ_ASSIST_* bits; the control file's ASSIST line and PROGRESSIVE). */
 #define FZ_ASSIST_TEMP 1
@@ -261,6 +265,7 @@ typedef struct {
   const float* fallback_model;
   int reg_type[8];
   double reg_alpha[8];
+  int fallback_steps, pad2;
 } fz_lm_opts;
 
 /* Batched pixel-wise Levenberg-Marquardt inversion of npix pixels with the

@@ -180,6 +180,39 @@ def test_regularised_inversion_matches_oracle_outcome(fz, orc):
         ctx.invert(obs, init, hydrostatic=True, opts=fz.LMOpts(reg={1: (2, 1.0)}))
 
 
+
+def test_early_fallback_restart(fz, orc):
+    """fz_lm_opts.fallback_steps = 1: a pixel restarts as soon as its search
+    stagnates once (STEPS >= 1) while above fallback x its goal.  As with the
+    restart at the end of the search, no pixel ends above 1.1x its goal (the
+    restart retraces the goal's own run); pixels that reach the goal before
+    stagnating are untouched; the restarted pixels spend fewer iterations
+    than with the restart at the end of the search."""
+    import torch
+    from firtez_dz_b200 import warmstart as ws
+    nz, npix = 48, 64
+    lines, reg, g, ctx = _ctx(fz, orc, nz)
+    true = fz.atmos.make_columns(npix, nz, seed=33)
+    obs, true_he, _ = ctx.forward(true, hydrostatic=True)
+    obs = obs + np.random.default_rng(4).normal(0.0, 1e-3, obs.shape)
+    ctx.rf_nodes(lmcase.NODES)
+    base = ws.default_models(npix, nz)
+    opts = fz.LMOpts(maxsteps=5, maxit=30, isigma=1e-3, dchi2=1e-3, slots=24)
+    _, chi_pl, _, _ = ctx.invert(obs, base, hydrostatic=True, opts=opts)
+    bad = lmcase.initial_guess(true_he, seed=2)
+    bad[:, 0] += 600.0
+    fb = np.ascontiguousarray(base[0])
+    res = {}
+    for fbs in (0, 1):
+        fopts = fz.LMOpts(maxsteps=5, maxit=30, isigma=1e-3, dchi2=1e-3, slots=24, fallback=1.1,
+                          fallback_model=fb.ctypes.data, fallback_steps=fbs)
+        _, chi, it, st = ctx.invert(obs, bad, hydrostatic=True, opts=fopts, target=chi_pl)
+        assert np.all(st == 0)
+        assert np.all(chi <= 1.1 * chi_pl)
+        res[fbs] = (chi, it)
+    assert res[1][1].sum() < res[0][1].sum()
+
+
 @pytest.mark.parametrize("nx,ny,nz", [(7, 6, 9), (3, 8, 4), (5, 5, 16)])
 def test_smoothing_b_matches_oracle(fz, orc, nx, ny, nz):
     """SMOOTHING_B (the 1-2-1 smoothing of INITIALIZE_CYCLE) on the device
