@@ -133,6 +133,7 @@ def lib():
         L.fz_forward_rf_full.argtypes = [P, ctypes.c_int, P, ctypes.c_int, P, P, P, P]
         L.fz_smooth.argtypes = [P, ctypes.c_int, ctypes.c_int, P, P]
         L.fz_smooth_device.argtypes = [P, ctypes.c_int, ctypes.c_int, P, P, P]
+        L.fz_smooth_shard_device.argtypes = [P, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, P, P, P]
         L.fz_invert_cycles_device.argtypes = [P, ctypes.c_int, ctypes.c_int, P, P, ctypes.c_int, P, ctypes.c_int, P,
                                               P, P, P, P]
         L.fz_errors.argtypes = [P, ctypes.c_int, P, P, ctypes.c_int, P, P, P, P]
@@ -508,6 +509,18 @@ class Synthesis:
                                       ctypes.c_void_p(chi2_ptr),
                                       ctypes.c_void_p(status_ptr) if status_ptr else None,
                                       ctypes.c_void_p(stream) if stream else None))
+
+    def smooth_shard_device(self, models_ptr, nx, ny, x0, nx_field, params=None, stream=0):
+        """SMOOTHING_B of a shard (columns x0 .. x0+nx-1 of an nx_field-column
+        field, halo columns included) in place on device models."""
+        f = None
+        if params is not None:
+            f = np.zeros(8, dtype=np.int32)
+            for p in params:
+                f[int(p) - 1] = 1
+        _check(lib().fz_smooth_shard_device(self._h, int(nx), int(ny), int(x0), int(nx_field),
+                                            ctypes.c_void_p(models_ptr), None if f is None else _p(f),
+                                            ctypes.c_void_p(stream) if stream else None))
 
     def invert_cycles(self, obs, init, nx, ny, cycles, hydrostatic=True, opts=None):
         """INVERT3D's cycles on host arrays: obs (ny*nx, 4, numw), init

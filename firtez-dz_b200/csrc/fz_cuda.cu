@@ -1963,9 +1963,12 @@ __global__ void k_smooth_load(int npix, int nz, int nrow, const int* __restrict_
 }
 
 // dir 0: x (stride NY pixels), 1: y (stride 1 pixel), 2: z; the last pass
-// writes REAL*4 into the model rows
+// writes REAL*4 into the model rows.  A shard of the field holds columns
+// x0g .. of an nxg-column field (the edge and 4-point rules are the
+// field's), its array extended by the neighbours' halo columns.
 __global__ void k_smooth_pass(int nx, int ny, int nz, int nrow, int dir, const int* __restrict__ rows,
-                              const double* __restrict__ a, double* __restrict__ b, float* __restrict__ m) {
+                              const double* __restrict__ a, double* __restrict__ b, float* __restrict__ m,
+                              int x0g, int nxg) {
   const int npix = nx * ny;
   const size_t total = (size_t)nrow * npix * nz;
   for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (size_t)gridDim.x * blockDim.x) {
@@ -1974,7 +1977,8 @@ __global__ void k_smooth_pass(int nx, int ny, int nz, int nrow, int dir, const i
     const int pix = (int)(pr % npix), r = (int)(pr / npix);
     const int iy = pix % ny, ix = pix / ny;
     double v = a[i];
-    if (dir == 0 && nx > 4 && ix > 0 && ix < nx - 1)
+    const int gx = ix + x0g;   // the field's column
+    if (dir == 0 && nxg > 4 && gx > 0 && gx < nxg - 1 && ix > 0 && ix < nx - 1)
       v = __dadd_rn(__dadd_rn(a[i + (size_t)ny * nz], a[i - (size_t)ny * nz]), __dmul_rn(v, 2.0)) / 4.0;
     else if (dir == 1 && ny > 4 && iy > 0 && iy < ny - 1)
       v = __dadd_rn(__dadd_rn(a[i + nz], a[i - nz]), __dmul_rn(v, 2.0)) / 4.0;
@@ -2242,8 +2246,9 @@ int grid_for(size_t n, int threads) {
 
 extern "C" {
 
-int fz_smooth_device(fz_ctx* c, int nx, int ny, float* d_models, const int* params, void* stream) {
-  if (!c || nx <= 0 || ny <= 0 || !d_models) return FZ_ERR_ARG;
+int fz_smooth_shard_device(fz_ctx* c, int nx, int ny, int x0, int nx_field, float* d_models, const int* params,
+                           void* stream) {
+  if (!c || nx <= 0 || ny <= 0 || !d_models || x0 < 0 || nx_field < x0 + nx) return FZ_ERR_ARG;
   // model row of reference parameter 1..8 (P0 smooths Pg, as the reference)
   static const int kRow[9] = {0, 0, 1, 2, 5, 6, 7, 10, 1};
   static const int kRef[NSLOT] = {1, 2, 4, 5, 6, 7};
@@ -2276,11 +2281,15 @@ int fz_smooth_device(fz_ctx* c, int nx, int ny, float* d_models, const int* para
   FZ_CK(cudaMemcpyAsync(d_rows, rows, nrow * sizeof(int), cudaMemcpyHostToDevice, s));
   const int blocks = (int)std::min<size_t>((n + 255) / 256, (size_t)c->nsm * 32);
   k_smooth_load<<<blocks, 256, 0, s>>>((int)npix, c->nz, nrow, d_rows, d_models, a);
-  k_smooth_pass<<<blocks, 256, 0, s>>>(nx, ny, c->nz, nrow, 0, d_rows, a, b, nullptr);
-  k_smooth_pass<<<blocks, 256, 0, s>>>(nx, ny, c->nz, nrow, 1, d_rows, b, a, nullptr);
-  k_smooth_pass<<<blocks, 256, 0, s>>>(nx, ny, c->nz, nrow, 2, d_rows, a, nullptr, d_models);
+  k_smooth_pass<<<blocks, 256, 0, s>>>(nx, ny, c->nz, nrow, 0, d_rows, a, b, nullptr, x0, nx_field);
+  k_smooth_pass<<<blocks, 256, 0, s>>>(nx, ny, c->nz, nrow, 1, d_rows, b, a, nullptr, x0, nx_field);
+  k_smooth_pass<<<blocks, 256, 0, s>>>(nx, ny, c->nz, nrow, 2, d_rows, a, nullptr, d_models, x0, nx_field);
   FZ_CK(cudaGetLastError());
   return 0;
+}
+
+int fz_smooth_device(fz_ctx* c, int nx, int ny, float* d_models, const int* params, void* stream) {
+  return fz_smooth_shard_device(c, nx, ny, 0, nx, d_models, params, stream);
 }
 
 int fz_invert_cycles_device(fz_ctx* c, int nx, int ny, const double* d_obs, float* d_models, int ncycles,

@@ -291,6 +291,17 @@ int fz_invert_device(fz_ctx* ctx, int npix, const double* d_obs, const float* d_
 int fz_autotune_lm(fz_ctx* ctx, int npix, const double* d_obs, const float* d_init, const double* d_target_chi2,
                    int hydrostatic, const fz_lm_opts* opts, const int* candidates, int ncand, fz_tune* out);
 
+/* SMOOTHING_B of one shard of a field split over ranks by x: the shard's
+ * nx columns are field columns x0 .. x0+nx-1 of an nx_field-column field
+ * (pixel iy + NY*ix within the array).  The array may carry the neighbours'
+ * halo columns at its ends (then x0 and nx count them): the x pass reads
+ * them, the field's own first and last columns are kept and its 4-point
+ * rule applies, so the interior columns come out as in the whole field's
+ * SMOOTHING_B.  fz_smooth_device is the whole-field case (x0 = 0,
+ * nx_field = nx). */
+int fz_smooth_shard_device(fz_ctx* ctx, int nx, int ny, int x0, int nx_field, float* d_models, const int* params,
+                           void* stream);
+
 /* INVERT3D's cycle loop (src/invert3d.f90:57-178, :228-408) on device
  * buffers for an NX x NY field (pixel iy + NY*ix): for each cycle the node
  * layout nodes[8*cycle .. 8*cycle+7] (fz_rf_nodes), SMOOTHING_B of the

@@ -361,3 +361,29 @@ def errors_1d(obs, syn, jac, model, w, nodes, reg=None):
         err[row] = (pert + err[row]).astype(np.float32)
         j0 += nj
     return err, chi
+
+
+def smoothing_b_shard(models, nx, ny, x0, nx_field, params):
+    """SMOOTHING_B of a shard: models (nx*ny, 13, NZ) hold field columns
+    x0 .. x0+nx-1 (halo columns included) of an nx_field-column field; the x
+    pass applies to the field's interior columns that have both neighbours
+    in the array, the field's own 4-point rule decides; y and z as
+    smoothing_b.  The interior columns match smoothing_b of the whole field."""
+    m = np.array(models, dtype=np.float32, copy=True)
+    nz = m.shape[2]
+    for p in params:
+        row = ATMPOS[p] if p != 8 else 1
+        a = m[:, row, :].astype(np.float64).reshape(nx, ny, nz)
+        if nx_field > 4:
+            b = a.copy()
+            for ix in range(1, nx - 1):
+                gx = ix + x0
+                if 0 < gx < nx_field - 1:
+                    b[ix] = (a[ix + 1] + a[ix - 1] + a[ix] * 2.0) / 4.0
+            a = b
+        if ny > 4:
+            a[:, 1:-1] = (a[:, 2:] + a[:, :-2] + a[:, 1:-1] * 2.0) / 4.0
+        if nz > 4:
+            a[:, :, 1:-1] = (a[:, :, 2:] + a[:, :, :-2] + a[:, :, 1:-1] * 2.0) / 4.0
+        m[:, row, :] = a.reshape(nx * ny, nz).astype(np.float32)
+    return m
