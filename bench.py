@@ -15,7 +15,7 @@ default).
 
 One step = the inversion of one tile of 131072 pixels of the field (one
 inversion call), inputs resident in HBM.  The plain arm (LM from the default
-guess) runs first and is the judge: its per-pixel chi2 is the goal of the
+guess) runs first and is the yardstick: its per-pixel chi2 is the goal of the
 headline arm.  ``value`` = converged pixels per second of NN-warm LM (network
 inference + batched LM) where a pixel is converged once its chi2 reaches its
 plain-LM chi2 (or by the plain stop rules), a pixel whose search stagnates
@@ -112,7 +112,10 @@ class ClockSampler:
     def __init__(self, index, tag):
         self.index = index
         self.proc = None
-        self.path = os.path.join(ROOT, "gpurun_out", "clocks_%s_rank%d.csv" % (tag, index))
+        # the raw samples go to $FZ_CLOCKS_DIR (default: the system's temporary directory)
+        import tempfile
+        self.path = os.path.join(os.environ.get("FZ_CLOCKS_DIR", tempfile.gettempdir()),
+                                 "clocks_%s_rank%d.csv" % (tag, index))
 
     def start(self):
         try:
@@ -367,13 +370,13 @@ def main():
             prof = ctx.profile_read(items=True)
         return maxms(e0.elapsed_time(e1) / steps), clocks, prof
 
-    # plain LM from the default guess: the judge, and the chi2 goal of the
+    # plain LM from the default guess: the yardstick, and the chi2 goal of the
     # headline arm (same tiles: the warm-up tiles first, then the timed ones)
     ms_pl, clocks_pl, _ = timed("plain", a.steps, a.warmup, "plain")
     plain_value = world * a.tile / (ms_pl * 1e-3)
     # headline: NN-warm LM, each pixel converged once it reaches its plain-LM
     # chi2; a pixel that stagnates above 1.1x it restarts once from the
-    # default guess in the same pool (plain LM stays the fallback and the judge)
+    # default guess in the same pool (plain LM stays the fallback and the yardstick)
     ms_nn, clocks, prof = timed("nn", a.steps, a.warmup, "nn", profile=True)
     value = world * a.tile / (ms_nn * 1e-3)
     # the same without the fallback

@@ -1,7 +1,8 @@
 """GPU response functions against the FP64 oracle.
 
-The GPU evaluates the response functions in FP32 (the north-star precision
-split) and accumulates the node Jacobian forward along z; the oracle restates
+The GPU evaluates the response functions in FP32 (the library's precision
+split: FP64 only for the chemistry, the pressure integration and the LM
+solve) and accumulates the node Jacobian forward along z; the oracle restates
 the reference's FP64 chain (local RFs, OLD_DSYN_PROPAGATION,
 CALCULATE_EQUIVALENT_DSYN).  Each Jacobian column (one node of one parameter,
 all Stokes parameters and wavelengths) is compared relative to its own
