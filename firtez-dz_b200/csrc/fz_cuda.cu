@@ -1599,9 +1599,25 @@ size_t rf_smem(const fz_ctx* c) {
          sizeof(float);
 }
 
+// The response-function kernels run one thread per wavelength in blocks of
+// at most 256 (two blocks per SM): NUMW <= 256, and their shared memory
+// within the 227 KB an SM block may have.
+int rf_check(const fz_ctx* c) {
+  if (((c->numw + 31) & ~31) > 256) return FZ_ERR_LIMIT;
+  if (rf_smem(c) > 227 * 1024) return FZ_ERR_LIMIT;
+  return 0;
+}
+
 int ensure_rf_scratch(fz_ctx* c, int ncol) {
   int rc = ensure_scratch(c, ncol);
   if (rc) return rc;
+  // the node kernels' shared memory above the default 48 KB (set here, before
+  // any stream capture of the inversion's iteration)
+  const size_t sms = rf_smem(c);
+  if (sms > 48 * 1024) {
+    FZ_CK(cudaFuncSetAttribute(k_synth_rf<true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sms));
+    FZ_CK(cudaFuncSetAttribute(k_synth_rf<false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sms));
+  }
   const int swr = rf_w(c->nreg, c->nlu);
   if ((size_t)ncol > c->rf_cols) {
     cudaFree(c->d_rfslab);
@@ -1685,6 +1701,7 @@ int launch_forward_rf(fz_ctx* c, int ncol, const float* d_model, int hydrostatic
                       float* d_mout, int* d_status, cudaStream_t s, bool full = false) {
   if (hydrostatic < 0 || hydrostatic > 1) return FZ_ERR_ARG;   // RFs: HE from the top only
   if (!full && (c->rf.np <= 0 || !c->d_coef)) return FZ_ERR_STATE;
+  if (int rc = rf_check(c)) return rc;
   int rc = ensure_rf_scratch(c, ncol);
   if (rc) return rc;
   const int swr = rf_w(c->nreg, c->nlu);
@@ -3076,6 +3093,7 @@ int fz_invert_device(fz_ctx* c, int npix, const double* d_obs, const float* d_in
                      double* d_syn_out, int* d_status, void* stream) {
   if (!c || npix <= 0 || !d_obs || !d_init || !d_model_out || !d_chi2 || !d_iters) return FZ_ERR_ARG;
   if (hydrostatic < 0 || hydrostatic > 1) return FZ_ERR_ARG;
+  if (int rc = rf_check(c)) return rc;
   FZ_CK(cudaSetDevice(c->device));
   LMConf C;
   int rc = lm_conf(c, npix, opts, C);

@@ -139,3 +139,28 @@ def test_model_only_modes(fz, orc, he):
         mh, _ = ctx.hydrostatic(m, mode=he)
         np.testing.assert_array_equal(mh[:, :5], mo[:, :5])
         np.testing.assert_array_equal(mh[:, 5:11], m[:, 5:11])
+
+
+def test_many_wavelengths_synthesis_and_rf_limit(fz, orc):
+    """Four spectral regions of 96 wavelengths (NUMW 384, the two-band
+    configuration): the synthesis runs and matches the oracle; the
+    response-function and inversion entry points, which run one thread per
+    wavelength in blocks of at most 256, refuse with FZ_ERR_LIMIT instead of
+    failing at launch."""
+    lines = fz.lines_parse(fz.atmos.line_database_text())
+    reg = fz.regions_from_lines_section(fz.atmos.lines_section(4), lines)
+    g, _ = orc.gain(lines, reg)
+    nz = 40
+    ctx = fz.Synthesis(lines, reg, nz=nz, gain=g)
+    assert ctx.numw == 384
+    m = fz.atmos.make_columns(6, nz, seed=2)
+    syn, mo, st = ctx.forward(m, hydrostatic=True)
+    osyn, omo, ost = orc.forward(lines, reg, g, m, hydrostatic=True)
+    assert np.all(st == 0) and np.all(ost == 0)
+    assert np.max(np.abs(syn[:, 0] - osyn[:, 0]) / np.abs(osyn[:, 0])) < 1e-5
+    assert np.max(np.abs(syn[:, 1:] - osyn[:, 1:])) < 1e-6
+    ctx.rf_nodes({1: 2, 6: 1})
+    with pytest.raises(fz.FzError, match="limit|LIMIT|Limit"):
+        ctx.forward_rf(m, hydrostatic=True)
+    with pytest.raises(fz.FzError, match="limit|LIMIT|Limit"):
+        ctx.invert(syn, m, hydrostatic=True, opts=fz.LMOpts(maxit=2))
