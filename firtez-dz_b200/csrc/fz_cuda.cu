@@ -682,8 +682,10 @@ __device__ __forceinline__ void lmap(const Geo& g, const float h[3], const float
 // jac in the (NFREQ, 6 NZ) layout and the layer's operator to oscr
 // ((nz, 16, NUMW) per column, zero where the boundary condition is taken);
 // k_rf_prop then applies the products of the operators above each layer.
-template <bool HE, bool FULL>
-__global__ void __launch_bounds__(256, 2) k_synth_rf(const DevParams* __restrict__ Pg, const RFConf* __restrict__ Rg,
+// MAXT: the block-size bound, 256 (two blocks per SM) up to 256
+// wavelengths, 512 (one) up to 512; both hold 128 registers a thread.
+template <bool HE, bool FULL, int MAXT>
+__global__ void __launch_bounds__(MAXT, (MAXT <= 256 ? 2 : 1)) k_synth_rf(const DevParams* __restrict__ Pg, const RFConf* __restrict__ Rg,
                                                   const LamP* __restrict__ lam, const float* __restrict__ gain,
                                                   int ncol, const float* __restrict__ slab,
                                                   const float* __restrict__ coefg, double* __restrict__ syn,
@@ -998,6 +1000,21 @@ __global__ void __launch_bounds__(256, 2) k_synth_rf(const DevParams* __restrict
   if (status && __any_sync(__activemask(), bad) && (l & 31) == 0) atomicOr(&status[col], FZ_NAN);
 }
 
+// k_synth_rf with the block-size bound its thread count needs
+template <bool HE, bool FULL, typename... A>
+void launch_synth_rf(int blocks, int threads, size_t sms, cudaStream_t s, A... a) {
+  if (threads <= 256)
+    k_synth_rf<HE, FULL, 256><<<blocks, threads, sms, s>>>(a...);
+  else
+    k_synth_rf<HE, FULL, 512><<<blocks, threads, sms, s>>>(a...);
+}
+
+template <bool HE, bool FULL>
+cudaError_t set_synth_rf_attr(cudaFuncAttribute attr, int v) {
+  cudaError_t e = cudaFuncSetAttribute(k_synth_rf<HE, FULL, 256>, attr, v);
+  return e == cudaSuccess ? cudaFuncSetAttribute(k_synth_rf<HE, FULL, 512>, attr, v) : e;
+}
+
 // Response functions at emergence from the local ones (FULL mode of
 // k_synth_rf): RF(K) = O_NZ ... O_{K+1} RF_loc(K), OLD_DSYN_PROPAGATION
 // (src/forward.f90:511-548), times GAIN as CALCULATE_EQUIVALENT_DSYN with
@@ -1005,7 +1022,7 @@ __global__ void __launch_bounds__(256, 2) k_synth_rf(const DevParams* __restrict
 // down from the top with the 4x4 product of the operators above in
 // registers; in place on rf.  A (parameter, height) column with an infinite
 // entry is zeroed, the SUM(ABS(.)) > HUGE test of :672-679.
-__global__ void __launch_bounds__(256) k_rf_prop(int nz, int nw, const float* __restrict__ gain,
+__global__ void __launch_bounds__(512) k_rf_prop(int nz, int nw, const float* __restrict__ gain,
                                                  const float* __restrict__ oscr, float* __restrict__ rf) {
   extern __shared__ int flg[];
   const int col = blockIdx.x, l = threadIdx.x;
@@ -1600,10 +1617,10 @@ size_t rf_smem(const fz_ctx* c) {
 }
 
 // The response-function kernels run one thread per wavelength in blocks of
-// at most 256 (two blocks per SM): NUMW <= 256, and their shared memory
-// within the 227 KB an SM block may have.
+// at most 512: NUMW <= 512, and their shared memory within the 227 KB a
+// block may have.
 int rf_check(const fz_ctx* c) {
-  if (((c->numw + 31) & ~31) > 256) return FZ_ERR_LIMIT;
+  if (((c->numw + 31) & ~31) > 512) return FZ_ERR_LIMIT;
   if (rf_smem(c) > 227 * 1024) return FZ_ERR_LIMIT;
   return 0;
 }
@@ -1615,8 +1632,8 @@ int ensure_rf_scratch(fz_ctx* c, int ncol) {
   // any stream capture of the inversion's iteration)
   const size_t sms = rf_smem(c);
   if (sms > 48 * 1024) {
-    FZ_CK(cudaFuncSetAttribute(k_synth_rf<true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sms));
-    FZ_CK(cudaFuncSetAttribute(k_synth_rf<false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sms));
+    FZ_CK((set_synth_rf_attr<true, false>(cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sms)));
+    FZ_CK((set_synth_rf_attr<false, false>(cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sms)));
   }
   const int swr = rf_w(c->nreg, c->nlu);
   if ((size_t)ncol > c->rf_cols) {
@@ -1678,11 +1695,11 @@ int launch_rf_stage(fz_ctx* c, int ncol, int hydrostatic, double* d_syn, float* 
   {
     ProfScope ps(c, 4, s, list ? 0 : ncol);
     if (hydrostatic)
-      k_synth_rf<true, false><<<ncol, threads, sms, s>>>(c->d_params, c->d_rf, c->d_lam, c->d_gain, ncol,
+      launch_synth_rf<true, false>(ncol, threads, sms, s, c->d_params, c->d_rf, c->d_lam, c->d_gain, ncol,
                                                          c->d_rfslab, c->d_coef, d_syn, d_jac, nullptr, d_mout,
                                                          d_status, list, nlist);
     else
-      k_synth_rf<false, false><<<ncol, threads, sms, s>>>(c->d_params, c->d_rf, c->d_lam, c->d_gain, ncol,
+      launch_synth_rf<false, false>(ncol, threads, sms, s, c->d_params, c->d_rf, c->d_lam, c->d_gain, ncol,
                                                           c->d_rfslab, c->d_coef, d_syn, d_jac, nullptr, d_mout,
                                                           d_status, list, nlist);
   }
@@ -1733,16 +1750,16 @@ int launch_forward_rf(fz_ctx* c, int ncol, const float* d_model, int hydrostatic
       c->oscr_len = need;
     }
     const size_t sms = (size_t)c->nz * swr * sizeof(float);
-    FZ_CK(cudaFuncSetAttribute(k_synth_rf<true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sms));
-    FZ_CK(cudaFuncSetAttribute(k_synth_rf<false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sms));
+    FZ_CK((set_synth_rf_attr<true, true>(cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sms)));
+    FZ_CK((set_synth_rf_attr<false, true>(cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sms)));
     {
       ProfScope ps(c, 4, s, ncol);
       if (hydrostatic)
-        k_synth_rf<true, true><<<ncol, threads, sms, s>>>(c->d_params, c->d_rf, c->d_lam, c->d_gain, ncol,
+        launch_synth_rf<true, true>(ncol, threads, sms, s, c->d_params, c->d_rf, c->d_lam, c->d_gain, ncol,
                                                           c->d_rfslab, nullptr, d_syn, d_jac, c->d_oscr, d_mout,
                                                           d_status, nullptr, nullptr);
       else
-        k_synth_rf<false, true><<<ncol, threads, sms, s>>>(c->d_params, c->d_rf, c->d_lam, c->d_gain, ncol,
+        launch_synth_rf<false, true>(ncol, threads, sms, s, c->d_params, c->d_rf, c->d_lam, c->d_gain, ncol,
                                                            c->d_rfslab, nullptr, d_syn, d_jac, c->d_oscr, d_mout,
                                                            d_status, nullptr, nullptr);
     }
@@ -3072,12 +3089,12 @@ int fz_rf_nodes(fz_ctx* c, const int* nodes) {
     c->rf.np = 0;
     return FZ_ERR_LIMIT;
   }
-  FZ_CK(cudaFuncSetAttribute(k_synth_rf<true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sms));
-  FZ_CK(cudaFuncSetAttribute(k_synth_rf<false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sms));
+  FZ_CK((set_synth_rf_attr<true, false>(cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sms)));
+  FZ_CK((set_synth_rf_attr<false, false>(cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sms)));
   // all of the SM's unified L1/shared storage as shared memory: two CTAs of
   // ~90 KB each can then be resident
-  FZ_CK(cudaFuncSetAttribute(k_synth_rf<true, false>, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
-  FZ_CK(cudaFuncSetAttribute(k_synth_rf<false, false>, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
+  FZ_CK((set_synth_rf_attr<true, false>(cudaFuncAttributePreferredSharedMemoryCarveout, 100)));
+  FZ_CK((set_synth_rf_attr<false, false>(cudaFuncAttributePreferredSharedMemoryCarveout, 100)));
   return np;
 }
 

@@ -141,12 +141,13 @@ def test_model_only_modes(fz, orc, he):
         np.testing.assert_array_equal(mh[:, 5:11], m[:, 5:11])
 
 
-def test_many_wavelengths_synthesis_and_rf_limit(fz, orc):
+def test_many_wavelengths(fz, orc):
     """Four spectral regions of 96 wavelengths (NUMW 384, the two-band
-    configuration): the synthesis runs and matches the oracle; the
-    response-function and inversion entry points, which run one thread per
-    wavelength in blocks of at most 256, refuse with FZ_ERR_LIMIT instead of
-    failing at launch."""
+    configuration): the synthesis and the node Jacobian (blocks of 512
+    threads, one per wavelength) match the oracle with the tolerances of the
+    two-line case, and an inversion runs; NUMW 544 (beyond 512) is refused by
+    the response-function and inversion entry points with FZ_ERR_LIMIT while
+    the synthesis still runs."""
     lines = fz.lines_parse(fz.atmos.line_database_text())
     reg = fz.regions_from_lines_section(fz.atmos.lines_section(4), lines)
     g, _ = orc.gain(lines, reg)
@@ -159,8 +160,21 @@ def test_many_wavelengths_synthesis_and_rf_limit(fz, orc):
     assert np.all(st == 0) and np.all(ost == 0)
     assert np.max(np.abs(syn[:, 0] - osyn[:, 0]) / np.abs(osyn[:, 0])) < 1e-5
     assert np.max(np.abs(syn[:, 1:] - osyn[:, 1:])) < 1e-6
-    ctx.rf_nodes({1: 2, 6: 1})
-    with pytest.raises(fz.FzError, match="limit|LIMIT|Limit"):
-        ctx.forward_rf(m, hydrostatic=True)
-    with pytest.raises(fz.FzError, match="limit|LIMIT|Limit"):
-        ctx.invert(syn, m, hydrostatic=True, opts=fz.LMOpts(maxit=2))
+    nodes = {1: 3, 4: 1, 5: 1, 6: 2, 7: 2}
+    ctx.rf_nodes(nodes)
+    rsyn, jac, _, st = ctx.forward_rf(m, hydrostatic=True)
+    orsyn, ojac, _, ost = orc.forward_rf(lines, reg, g, m, nodes, hydrostatic=True)
+    assert np.all(st == 0) and np.all(ost == 0)
+    assert np.max(np.abs(rsyn[:, 0] - orsyn[:, 0]) / np.abs(orsyn[:, 0])) < 1e-5
+    scale = np.abs(ojac).max(axis=2)
+    rel = np.abs(jac.astype(np.float64) - ojac).max(axis=2) / np.where(scale > 0, scale, 1.0)
+    assert rel.max() <= 2e-3, rel.max()
+    best, chi, it, st = ctx.invert(syn, m, hydrostatic=True, opts=fz.LMOpts(maxit=3, isigma=1e-3, slots=4))
+    assert np.all(st == 0) and np.all(np.isfinite(chi))
+    reg5 = fz.regions_from_lines_section(fz.atmos.lines_section(4, nw=136), lines)
+    ctx5 = fz.Synthesis(lines, reg5, nz=nz, gain=orc.gain(lines, reg5)[0])
+    assert ctx5.numw == 544
+    ctx5.forward(m, hydrostatic=True)
+    ctx5.rf_nodes({1: 2, 6: 1})
+    with pytest.raises(fz.FzError, match="limit"):
+        ctx5.forward_rf(m, hydrostatic=True)
