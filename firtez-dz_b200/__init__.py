@@ -64,10 +64,11 @@ class LMOpts(ctypes.Structure):
                 ("svdtol", ctypes.c_double), ("isigma", ctypes.c_double), ("wstk", ctypes.c_float * 4),
                 ("slots", ctypes.c_int), ("assist", ctypes.c_int), ("fallback", ctypes.c_double),
                 ("fallback_model", ctypes.c_void_p), ("reg_type", ctypes.c_int * 8), ("reg_alpha", ctypes.c_double * 8),
-                ("fallback_steps", ctypes.c_int), ("pad2", ctypes.c_int)]
+                ("fallback_steps", ctypes.c_int), ("solver", ctypes.c_int), ("node_expansion", ctypes.c_int),
+                ("pad2", ctypes.c_int)]
 
     def __init__(self, maxsteps=5, maxit=40, dchi2=0.0, svdtol=1e-4, isigma=4e-3, wstk=(1, 1, 1, 1), slots=0,
-                 fallback=0.0, fallback_model=0, reg=None, assist=(), fallback_steps=0):
+                 fallback=0.0, fallback_model=0, reg=None, assist=(), fallback_steps=0, solver=1, node_expansion=1):
         """fallback_model: device pointer of one MODEL(NZ,13) float32 (e.g. a
         torch tensor's data_ptr()) that pixels ending above fallback x their
         chi2 goal restart from (a host pointer for invert()).  reg: optional
@@ -75,14 +76,16 @@ class LMOpts(ctypes.Structure):
         (VERTICAL REGULARIZATION: type 0 or 1, PEN_ALP).  assist: SET_TAU's
         assists for invert_cycles (temp, pgas, bvec, vlos, progressive).
         fallback_steps: restart once STEPS reaches it while above fallback x
-        the goal (0: when the search ends)."""
+        the goal (0: when the search ends).  solver: 1 SVD, 2 conjugate
+        gradients (LINEAR_SOLVER); node_expansion: 1 SIR-like, 2 STiC-like
+        (PERTURBATION_TYPE)."""
         typ, alp = [0] * 8, [0.0] * 8
         for p, (t, a) in (reg or {}).items():
             typ[int(p) - 1], alp[int(p) - 1] = int(t), float(a)
         super().__init__(maxsteps, maxit, dchi2, svdtol, isigma, (ctypes.c_float * 4)(*wstk), slots,
                          assist_bits(assist),
                          float(fallback), fallback_model or None, (ctypes.c_int * 8)(*typ),
-                         (ctypes.c_double * 8)(*alp), int(fallback_steps), 0)
+                         (ctypes.c_double * 8)(*alp), int(fallback_steps), int(solver), int(node_expansion), 0)
 
 
 class Tune(ctypes.Structure):
@@ -169,8 +172,8 @@ def lib():
         L.fz_forward_rf_full_device.argtypes = [P, ctypes.c_int, P, ctypes.c_int, P, P, P, P, P]
         L.fz_invert.argtypes = [P, ctypes.c_int, P, P, P, ctypes.c_int, P, P, P, P, P, P]
         L.fz_invert_device.argtypes = [P, ctypes.c_int, P, P, P, ctypes.c_int, P, P, P, P, P, P, P]
-        L.fz_lm_perturbation.argtypes = [P, ctypes.c_int, ctypes.c_int, ctypes.c_int, P, P, P, P, P, ctypes.c_double,
-                                         P]
+        L.fz_lm_perturbation.argtypes = [P, ctypes.c_int, ctypes.c_int, ctypes.c_int, P, P, P, P, P, ctypes.c_int,
+                                         ctypes.c_double, P]
         _lib = L
     return _lib
 
@@ -600,10 +603,11 @@ class Synthesis:
                                       ctypes.c_void_p(status_ptr) if status_ptr else None,
                                       ctypes.c_void_p(stream) if stream else None))
 
-    def lm_perturbation(self, jac, diff, lam, svdtol=1e-4, reg_pen=None, reg_hss=None):
+    def lm_perturbation(self, jac, diff, lam, svdtol=1e-4, reg_pen=None, reg_hss=None, dtype=1):
         """Batched GET_PERTURBATION: jac (npix, np, nfreq) normalised Jacobian,
         diff (npix, nfreq), lam (npix,); optional reg_pen (npix, np) and
-        reg_hss (npix, np, np).  Returns delta (npix, np)."""
+        reg_hss (npix, np, np); dtype 1 SVD, 2 conjugate gradients.  Returns
+        delta (npix, np)."""
         j = np.ascontiguousarray(jac, dtype=np.float32)
         d = np.ascontiguousarray(diff, dtype=np.float64)
         lm = np.ascontiguousarray(lam, dtype=np.float64)
@@ -613,7 +617,7 @@ class Synthesis:
         out = np.zeros((npix, npar))
         _check(lib().fz_lm_perturbation(self._h, npix, npar, nf, _p(j), _p(d), _p(lm),
                                         None if rp is None else _p(rp), None if rh is None else _p(rh),
-                                        float(svdtol), _p(out)))
+                                        int(dtype), float(svdtol), _p(out)))
         return out
 
     def forward_rf_device(self, model_ptr, ncol, syn_ptr, jac_ptr, model_out_ptr, status_ptr=0, stream=0,

@@ -1881,6 +1881,9 @@ int lm_conf(fz_ctx* c, int npix, const fz_lm_opts* o, LMConf& C) {
   C.fallback = o && o->fallback_model ? o->fallback : 0.0;
   C.fb_model = o ? o->fallback_model : nullptr;
   C.fb_steps = o && o->fallback_steps > 0 ? o->fallback_steps : (1 << 30);
+  C.solver = o && o->solver == 2 ? 2 : 1;
+  C.node_exp = o && o->node_expansion == 2 ? 2 : 1;
+  if (o && (o->solver < 0 || o->solver > 2 || o->node_expansion < 0 || o->node_expansion > 2)) return FZ_ERR_ARG;
   // GET_IT_PENALTIES operators (src/get_dmodel.f90:1103-1146): per free
   // parameter L = sqrt(PEN_ALP / IFREEP) D, D = diag(1/NJ) (type 0) or first
   // differences to the previous node (type 1); PEN_HSS = L^T L block diagonal
@@ -3315,10 +3318,11 @@ int fz_invert(fz_ctx* c, int npix, const double* obs, const float* init, const d
 }
 
 int fz_lm_perturbation(fz_ctx* c, int npix, int np, int nfreq, const float* jac, const double* diff,
-                       const double* lambda, const double* reg_pen, const double* reg_hss, double svdtol,
+                       const double* lambda, const double* reg_pen, const double* reg_hss, int dtype, double svdtol,
                        double* delta) {
   if (!c || npix <= 0 || np <= 0 || np > LM_MAXNP || nfreq <= 0 || (nfreq & 3) || !jac || !diff || !lambda || !delta)
     return FZ_ERR_ARG;
+  if (dtype < 0 || dtype > 2) return FZ_ERR_ARG;   // GET_PERTURBATION's DTYPE (0 taken as 1)
   FZ_CK(cudaSetDevice(c->device));
   LMConf C;
   std::memset(&C, 0, sizeof(C));
@@ -3326,6 +3330,7 @@ int fz_lm_perturbation(fz_ctx* c, int npix, int np, int nfreq, const float* jac,
   C.nfreq = nfreq;
   C.inu = 1.0;
   C.svdtol = svdtol > 0 ? svdtol : 1.0e-4;
+  C.solver = dtype == 2 ? 2 : 1;
   for (int j = 0; j < np; ++j) C.norm[j] = 1.0;
   LMSlots L{};
   L.S = npix;

@@ -37,6 +37,8 @@ struct LMConf {
   double fallback;             // restart factor on the chi2 goal (0 = off)
   const float* fb_model;       // MODEL(NZ,13) a restarted pixel starts from
   int fb_steps;                // restart once STEPS reaches this while above fallback x goal
+  int solver;                  // SOLVER_METHOD: 1 SVD (GET_INVERSE), 2 CG (NEW_CALCULATE_DELTA_UBICGSTAB)
+  int node_exp;                // NODE_EXPANSION: 1 SIR/NICOLE-like, 2 STiC-like
   int reg;                     // vertical regularisation on (GET_IT_PENALTIES)
   double reg_hss[LM_MAXNP * LM_MAXNP];   // PEN_HSS = L^T L (model independent)
   int nodes_ref[8];            // node count per reference parameter
@@ -425,6 +427,59 @@ __global__ void __launch_bounds__(128) k_lm_solve(LMConf C, LMSlots Sl) {
       V[lane][j] = (lane == j) ? 1.0 : 0.0;
     }
   __syncwarp();
+  if (C.solver == 2) {
+    // NEW_CALCULATE_DELTA_UBICGSTAB (src/lm.f90:375-453): conjugate gradients
+    // on TERM1 delta = TERM2 from delta = 0, stopped when the mean squared
+    // relative residual sum(((A x - b)/(|b| + 1e-5))^2)/NP drops below 1e-3
+    // (or grows by more than 1e30), at most 100000 iterations; unconverged:
+    // x / 10.  A non-finite residual ends the loop at once (its delta would
+    // come out non-finite and be zeroed all the same).
+    const double b = lane < np ? Sl.g[(size_t)s * np + lane] : 0.0;
+    auto dot = [&](double u, double v) {
+      double t = lane < np ? u * v : 0.0;
+      for (int o = 16; o > 0; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
+      return t;
+    };
+    auto matvec = [&](double v) {
+      double t = 0.0;
+      for (int j = 0; j < np; ++j) {
+        const double vj = __shfl_sync(0xffffffffu, v, j);
+        if (lane < np) t += A[lane][j] * vj;
+      }
+      return t;
+    };
+    double x = 0.0, pv = b, rv = b;
+    double rho = dot(rv, rv);
+    double qv = matvec(pv);
+    double alpha = rho / dot(pv, qv);
+    x += alpha * pv;
+    rv -= alpha * qv;
+    double pcond = 1.0e29, dcond = -1.0e29;
+    bool failed = true;
+    for (int it = 1; it <= 100000; ++it) {
+      const double rho0 = rho;
+      rho = dot(rv, rv);
+      const double beta = rho / rho0;
+      pv = rv + beta * pv;
+      qv = matvec(pv);
+      alpha = rho / dot(pv, qv);
+      x += alpha * pv;
+      rv -= alpha * qv;
+      const double ck = matvec(x);
+      const double e = (ck - b) / (fabs(b) + 1.0e-5);
+      const double cond = dot(e, e) / (double)np;
+      if (cond < 1.0e-3 || dcond > 1.0e30) {
+        failed = false;
+        break;
+      }
+      if (cond != cond) break;
+      dcond = cond - pcond;
+      pcond = cond;
+    }
+    const double d = failed ? x / 10.0 : x;
+    if (lane < np) Sl.delta[(size_t)s * np + lane] = (d == d) ? d : 0.0;
+    return;
+  }
   for (int sweep = 0; sweep < 40; ++sweep) {
     int rot = 0;
     for (int p = 0; p < np - 1; ++p)
@@ -535,15 +590,29 @@ __global__ void __launch_bounds__(128) k_lm_update(LMConf C, LMSlots Sl, const d
       csum[threadIdx.x] = cs;
     }
     __syncthreads();
+    if (C.node_exp == 2) {
+      // NODE_EXPANSION = 2 (STiC-like, :1792-1804): the new profile is the
+      // expansion of the clipped node values, limited to [INF, SUP]; the
+      // perturbation is its difference to the current profile
+      for (int k = threadIdx.x; k < nz; k += blockDim.x) {
+        double v = 0.0;
+        for (int j = 0; j < nj; ++j) v += (avg[j] + itd[j]) * coef[k * np + j0 + j];
+        float op = (float)v;
+        if ((double)op < inf) op = (float)inf;
+        if ((double)op > sup) op = (float)sup;
+        pert[k] = op - ip[k];
+      }
+      __syncthreads();
+    }
     // NZPERT = EXPAND(avg + itd) - IPAR
-    for (int k = threadIdx.x; k < nz; k += blockDim.x) {
+    for (int k = threadIdx.x; C.node_exp != 2 && k < nz; k += blockDim.x) {
       double v = 0.0;
       for (int j = 0; j < nj; ++j) v += (avg[j] + itd[j]) * coef[k * np + j0 + j];
       nzp[k] = v - (double)ip[k];
     }
     __syncthreads();
     // ITDELTA = CONTRACT(REAL(NZPERT))
-    if (threadIdx.x < nj) {
+    if (C.node_exp != 2 && threadIdx.x < nj) {
       const int j = j0 + threadIdx.x;
       double a = 0.0;
       for (int k = 0; k < nz; ++k) a += (double)(float)nzp[k] * coef[k * np + j];
@@ -551,7 +620,7 @@ __global__ void __launch_bounds__(128) k_lm_update(LMConf C, LMSlots Sl, const d
     }
     __syncthreads();
     // NZPERT = EXPAND(ITDELTA), limits
-    for (int k = threadIdx.x; k < nz; k += blockDim.x) {
+    for (int k = threadIdx.x; C.node_exp != 2 && k < nz; k += blockDim.x) {
       double v = 0.0;
       for (int j = 0; j < nj; ++j) v += itd[j] * coef[k * np + j0 + j];
       const float op = ip[k] + (float)v;

@@ -249,6 +249,12 @@ int fz_smooth_device(fz_ctx* ctx, int nx, int ny, float* d_models, const int* pa
  * stagnation counter (the STEPS of UPDATE_LAMBDA) reaches fallback_steps
  * while its best chi2 is still above fallback x its goal, instead of when
  * its search ends (0: when it ends).
+ * solver: SOLVER_METHOD (MISC SETUP LINEAR_SOLVER), 1 (or 0) = the SVD
+ * pseudo-inverse of GET_INVERSE, 2 = the conjugate-gradient iteration of
+ * NEW_CALCULATE_DELTA_UBICGSTAB (src/lm.f90:375-453).  node_expansion:
+ * NODE_EXPANSION (PERTURBATION_TYPE), 1 (or 0) = SIR/NICOLE-like node
+ * perturbations, 2 = STiC-like (the expanded node values are the new
+ * profile; src/get_dmodel.f90:1792-1804).
  * assist: SET_TAU's initial-guess assists for fz_invert_cycles_device
  * (FZ_ASSIST_* bits; the control file's ASSIST line and PROGRESSIVE). */
 #define FZ_ASSIST_TEMP 1
@@ -265,7 +271,7 @@ typedef struct {
   const float* fallback_model;
   int reg_type[8];
   double reg_alpha[8];
-  int fallback_steps, pad2;
+  int fallback_steps, solver, node_expansion, pad2;
 } fz_lm_opts;
 
 /* Batched pixel-wise Levenberg-Marquardt inversion of npix pixels with the
@@ -378,7 +384,7 @@ int fz_errors(fz_ctx* ctx, int npix, const double* obs, const float* models, int
  * subtracted from J^T diff and REG_HSS added to J^T J as the reference
  * does (:169-174); delta (np, npix).  np <= 16, nfreq a multiple of 4. */
 int fz_lm_perturbation(fz_ctx* ctx, int npix, int np, int nfreq, const float* jac, const double* diff,
-                       const double* lambda, const double* reg_pen, const double* reg_hss, double svdtol,
+                       const double* lambda, const double* reg_pen, const double* reg_hss, int dtype, double svdtol,
                        double* delta);
 
 /* Warm-start network (no counterpart in the reference): an MLP of nlayers

@@ -15,9 +15,9 @@ Followed routines (src/get_dmodel.f90 unless noted):
   INITIALIZE_CYCLE src/invert3d.f90:228-300 (initial state), IFREE_VAR_SPACE
   :411-442 (MPERT = 0.15, RSVDTOL = 1e-4).
 
-Vertical regularisation (GET_IT_PENALTIES) is off, as in the configurations
-the library targets; SOLVER_METHOD = 1 (SVD) and NODE_EXPANSION = 1 (SIR-like,
-the reference default, src/input_file.f90:452-453).
+Vertical regularisation (GET_IT_PENALTIES), SOLVER_METHOD 1 (SVD) or 2
+(conjugate gradients) and NODE_EXPANSION 1 (SIR-like, the reference default,
+src/input_file.f90:452-453) or 2 (STiC-like) are options.
 """
 import numpy as np
 from scipy.linalg import lapack
@@ -97,10 +97,47 @@ def pinv_dgesvd(m, svdtol=RSVDTOL):
     return vt.T @ (np.diag(si) @ u.T)
 
 
-def get_perturbation(jac_n, diff, lam, svdtol=RSVDTOL, reg_pen=None, reg_hss=None):
-    """GET_PERTURBATION (src/lm.f90:137-204) with SOLVER_METHOD = 1: jac_n is
-    the normalised JACOB (NFREQ, NP), diff the weighted residual; REG_PEN is
-    subtracted from J^T diff and REG_HSS added to J^T J (:170-174)."""
+def cg_delta(a, b):
+    """NEW_CALCULATE_DELTA_UBICGSTAB (src/lm.f90:375-453): conjugate
+    gradients from x = 0 until mean(((A x - b)/(|b| + 1e-5))^2) < 1e-3 (or
+    the measure grows by more than 1e30), at most 100000 iterations; x / 10
+    when it does not converge (a non-finite measure gives up at once: its
+    result is non-finite either way)."""
+    npar = b.size
+    x = np.zeros(npar)
+    p = b.copy()
+    r = b - a @ x
+    rho = float(r @ r)
+    q = a @ p
+    alpha = rho / float(p @ q)
+    x = x + alpha * p
+    r = r - alpha * q
+    pc, dc = 1.0e29, -1.0e29
+    with np.errstate(all="ignore"):
+        for _ in range(100000):
+            rho0 = rho
+            rho = float(r @ r)
+            beta = rho / rho0
+            p = r + beta * p
+            q = a @ p
+            alpha = rho / float(p @ q)
+            x = x + alpha * p
+            r = r - alpha * q
+            cond = float(np.sum(((a @ x - b) / (np.abs(b) + 1.0e-5)) ** 2)) / npar
+            if cond < 1.0e-3 or dc > 1.0e30:
+                return x
+            if cond != cond:
+                break
+            dc = cond - pc
+            pc = cond
+    return x / 10.0
+
+
+def get_perturbation(jac_n, diff, lam, svdtol=RSVDTOL, reg_pen=None, reg_hss=None, dtype=1):
+    """GET_PERTURBATION (src/lm.f90:137-204), DTYPE 1 (SVD) or 2 (conjugate
+    gradients): jac_n is the normalised JACOB (NFREQ, NP), diff the weighted
+    residual; REG_PEN is subtracted from J^T diff and REG_HSS added to J^T J
+    (:170-174)."""
     hss = jac_n.T @ jac_n
     term2 = jac_n.T @ diff
     if reg_pen is not None:
@@ -109,7 +146,7 @@ def get_perturbation(jac_n, diff, lam, svdtol=RSVDTOL, reg_pen=None, reg_hss=Non
         hss = hss + reg_hss
     term1 = hss.copy()
     term1[np.diag_indices_from(term1)] += np.diag(hss) * lam
-    delta = pinv_dgesvd(term1, svdtol) @ term2
+    delta = cg_delta(term1, term2) if dtype == 2 else pinv_dgesvd(term1, svdtol) @ term2
     return np.where(np.isnan(delta), 0.0, delta)
 
 
@@ -124,15 +161,21 @@ def expand(ivec, coefs):
     return coefs @ ivec
 
 
-def sort_delta(delta, factor, ipar, inf, sup, coefs, absolute):
-    """SORT_DELTA_TO_ATMOSPHERE with NODE_EXPANSION = 1: returns the REAL*4
-    height perturbation of one parameter (and the clipped node deltas)."""
+def sort_delta(delta, factor, ipar, inf, sup, coefs, absolute, node_expansion=1):
+    """SORT_DELTA_TO_ATMOSPHERE with NODE_EXPANSION = 1 (SIR-like) or 2
+    (STiC-like, :1792-1804): returns the REAL*4 height perturbation of one
+    parameter (and the clipped node deltas)."""
     itd = delta * factor
     avg = contract(ipar, coefs)
     pert = np.maximum(absolute, np.abs(MPERT * avg)) if absolute > 0 else np.abs(MPERT * avg)
     pert = np.where(avg == 0, absolute, pert)
     itd = np.where(np.abs(itd) > pert, itd / np.abs(np.where(itd == 0, 1.0, itd)) * pert, itd)
     nzpert = expand(avg + itd, coefs)
+    if node_expansion == 2:
+        opar = nzpert.astype(np.float32)
+        opar = np.where(opar.astype(np.float64) < inf, np.float32(inf), opar)
+        opar = np.where(opar.astype(np.float64) > sup, np.float32(sup), opar)
+        return (opar - ipar.astype(np.float32)).astype(np.float32), itd
     nzpert = nzpert - ipar.astype(np.float64)
     itd = contract(nzpert.astype(np.float32), coefs)
     nzpert = expand(itd, coefs)
@@ -142,7 +185,7 @@ def sort_delta(delta, factor, ipar, inf, sup, coefs, absolute):
     return nzpert.astype(np.float32), itd
 
 
-def rearange(model, delta, nodes):
+def rearange(model, delta, nodes, node_expansion=1):
     """REARANGE_DA_MODEL (non-errors limits): applies the node perturbation
     delta to model (13, NZ) REAL*4 in place.  nodes: {param: NJ}."""
     nz = model.shape[1]
@@ -155,7 +198,7 @@ def rearange(model, delta, nodes):
         coefs = int_coefs(nz, nj)
         bumod = model[row].copy()
         pert, _ = sort_delta(delta[j0:j0 + nj], PARAM_NORMS[p - 1], model[row], LOWLIM[p - 1], UPPLIM[p - 1],
-                             coefs, PARAM_NORMS[p - 1] * MPERT)
+                             coefs, PARAM_NORMS[p - 1] * MPERT, node_expansion)
         if p == 1:
             tll, tul = np.float32(-11.5), np.float32(0.5)
             tau = model[TAU_ROW]
@@ -246,7 +289,7 @@ def lm_accept(st, obs, syn, jac, w, ok=True, reg=None):
     return chi, acc, prev
 
 
-def lm_perturb(st, obs, w, nodes, reg=None):
+def lm_perturb(st, obs, w, nodes, reg=None, solver=1, node_expansion=1):
     """The rest of GET_PERT_1D: normalised Jacobian, GET_PERTURBATION (with the
     penalties of the best model, reg as in lm_accept) and REARANGE_DA_MODEL;
     st.cur becomes the next trial model."""
@@ -256,8 +299,8 @@ def lm_perturb(st, obs, w, nodes, reg=None):
     pen = hss = None
     if reg is not None:
         pen, hss = it_penalties(st.best, *reg)
-    delta = get_perturbation(jn, diff, st.lam, reg_pen=pen, reg_hss=hss)
-    rearange(st.cur, delta, nodes)
+    delta = get_perturbation(jn, diff, st.lam, reg_pen=pen, reg_hss=hss, dtype=solver)
+    rearange(st.cur, delta, nodes, node_expansion)
     return delta
 
 
@@ -268,7 +311,8 @@ def lm_step(st, obs, syn, jac, w, nodes):
     return lm_perturb(st, obs, w, nodes)
 
 
-def invert(forward_rf, obs, init, nodes, w, maxsteps=5, maxit=40, dchi2=0.0, reg=None):
+def invert(forward_rf, obs, init, nodes, w, maxsteps=5, maxit=40, dchi2=0.0, reg=None, solver=1,
+           node_expansion=1):
     """Pixel-wise inversion with the stop rules of the batched GPU inversion
     (steps > maxsteps, maxit iterations, or an accepted step gaining less than
     dchi2 relative).  forward_rf(models (n,13,nz)) -> (syn (n,nfreq),
@@ -294,7 +338,7 @@ def invert(forward_rf, obs, init, nodes, w, maxsteps=5, maxit=40, dchi2=0.0, reg
             small = acc and prev < 1.0e29 and (prev - st.chibest) < dchi2 * prev
             if st.steps > maxsteps or iters[i] >= maxit or small:
                 continue
-            lm_perturb(st, obs[i], w, nodes, reg=reg)
+            lm_perturb(st, obs[i], w, nodes, reg=reg, solver=solver, node_expansion=node_expansion)
             still.append(i)
         active = still
     best = np.stack([st.best for st in states])

@@ -124,3 +124,25 @@ def test_errors_1d_analytic():
         want = min(sigma, 0.15 * 6000.0) if expect is None else expect
         np.testing.assert_allclose(err[0], want, rtol=1e-6)
         assert np.all(err[1:] == 0)
+
+
+def test_cg_delta_and_node_expansion_two():
+    """The oracle's NEW_CALCULATE_DELTA_UBICGSTAB meets its own stopping test
+    and tends to the exact solution on an SPD system; SORT_DELTA with
+    NODE_EXPANSION = 2 makes the new profile the expansion of the node values
+    plus the clipped node deltas (limits aside)."""
+    rng = np.random.default_rng(3)
+    m = rng.standard_normal((13, 13))
+    a = m @ m.T + 13 * np.eye(13)
+    b = rng.standard_normal(13)
+    x = lmo.cg_delta(a, b)
+    assert np.sum(((a @ x - b) / (np.abs(b) + 1e-5)) ** 2) / 13 < 1e-3
+    np.testing.assert_allclose(x, np.linalg.solve(a, b), rtol=0.1, atol=1e-3)
+    nz, nj = 40, 5
+    coefs = lmo.int_coefs(nz, nj)
+    ipar = np.linspace(9000.0, 4500.0, nz).astype(np.float32)
+    delta = np.array([0.01, -0.02, 0.0, 0.015, -0.01])
+    pert2, itd = lmo.sort_delta(delta, 6000.0, ipar, 2500.0, 1.8e4, coefs, 900.0, node_expansion=2)
+    avg = lmo.contract(ipar, coefs)
+    want = (lmo.expand(avg + itd, coefs).astype(np.float32) - ipar).astype(np.float32)
+    np.testing.assert_array_equal(pert2, want)
