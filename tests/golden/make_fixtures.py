@@ -6,6 +6,8 @@ TEST INFRASTRUCTURE.  Reads the reference tree (default /root/reference):
 
   default/test_atmos.bin, default/rf_test_atmos.bin  -- v3 model files (1x1x256)
   default/lines_database.dat                         -- line database
+  tests/*/control_file.dat                           -- the test cases' control
+      files (copied to control/<case>.dat)
   src/atom_database.f90:89-97                         -- the commented-out
       "Abundances Vigeesh" set; the fixtures' rho, Pe, mu were computed with it.
 """
@@ -20,6 +22,11 @@ ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
 here = os.path.dirname(os.path.abspath(__file__))
 for f in ("test_atmos.bin", "rf_test_atmos.bin", "lines_database.dat"):
     shutil.copyfile(os.path.join(ref, "default", f), os.path.join(here, f))
+os.makedirs(os.path.join(here, "control"), exist_ok=True)
+for case in sorted(os.listdir(os.path.join(ref, "tests"))):
+    cf = os.path.join(ref, "tests", case, "control_file.dat")
+    if os.path.isfile(cf):
+        shutil.copyfile(cf, os.path.join(here, "control", case + ".dat"))
 src = open(os.path.join(ref, "src", "atom_database.f90")).read().splitlines()
 i0 = next(i for i, l in enumerate(src) if "Abundances Vigeesh" in l)
 txt = ""
