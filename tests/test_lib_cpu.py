@@ -63,3 +63,36 @@ def test_regions_from_lines_section(fz):
     reg = fz.regions_from_lines_section("4,5 500 -700.0 5.0", lines)
     assert reg["nblend"][0] == 2 and reg["numwave"][0] == 500
     assert abs(reg["wdif"][0, 1] - 1e3 * (6302.493652 - 6301.500977)) < 1e-6
+
+
+def _c_layout(tmp_path, struct, fields):
+    """sizeof and offsetof of a C struct of include/fz_b200.h (gcc)."""
+    import subprocess
+    src = tmp_path / ("probe_%s.c" % struct)
+    lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "fz_b200.h"', "int main(void) {",
+             '  printf("%%zu\\n", sizeof(%s));' % struct]
+    lines += ['  printf("%%zu\\n", offsetof(%s, %s));' % (struct, f) for f in fields]
+    lines += ["  return 0;", "}"]
+    src.write_text("\n".join(lines) + "\n")
+    exe = tmp_path / ("probe_%s" % struct)
+    subprocess.check_call(["gcc", "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe)])
+    out = [int(x) for x in subprocess.check_output([str(exe)]).split()]
+    return out[0], dict(zip(fields, out[1:]))
+
+
+def test_struct_layouts_match_the_header(fz, tmp_path):
+    """The ctypes / numpy mirrors of fz_lm_opts, fz_tune, fz_line and
+    fz_region have the C header's sizes and field offsets."""
+    import ctypes
+    for struct, cls in (("fz_lm_opts", fz.LMOpts), ("fz_tune", fz.Tune)):
+        names = [f[0] for f in cls._fields_]
+        size, offs = _c_layout(tmp_path, struct, names)
+        assert ctypes.sizeof(cls) == size, struct
+        for n in names:
+            assert getattr(cls, n).offset == offs[n], (struct, n)
+    for struct, dt in (("fz_line", fz.LINE_DTYPE), ("fz_region", fz.REGION_DTYPE)):
+        names = list(dt.names)
+        size, offs = _c_layout(tmp_path, struct, names)
+        assert dt.itemsize == size, struct
+        for n in names:
+            assert dt.fields[n][1] == offs[n], (struct, n)
