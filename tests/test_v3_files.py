@@ -137,3 +137,29 @@ def test_lsf_file_matches_reference_writer(v3, gold, tmp_path):
     np.testing.assert_array_equal(v3.read_lsf(out, gold["lsf"].size), np.float32(gold["lsf"]).astype(np.float64))
     with pytest.raises(Exception):
         v3.read_lsf(out, gold["lsf"].size + 1)
+
+
+def test_multi_record_model_file(v3, tmp_path):
+    """A model above NMAXREC = 268,435,446 values (13 x 4096 x 5042, 1.07 GB)
+    goes into two data records, as WRITE_MODEL3D_V3 splits it: the header's
+    record count, both records' markers and sizes, and the read-back."""
+    import struct
+    nx, ny, nz = 64, 64, 5042
+    n = 13 * nx * ny * nz
+    assert n > vo.NMAXREC
+    cubes = np.zeros((13, nx, ny, nz), dtype=np.float32)
+    cubes.reshape(-1)[::9973] = np.arange(cubes.size // 9973 + 1, dtype=np.float32)[: cubes.reshape(-1)[::9973].size]
+    out = tmp_path / "big.bin"
+    v3.write_model(out, cubes)
+    with open(out, "rb") as f:
+        assert struct.unpack("<i", f.read(4))[0] == 36
+        head = np.frombuffer(f.read(36), "<f4")
+        assert head[3] == 3 and struct.unpack("<i", f.read(4))[0] == 36     # header + 2 data records
+        for size in (vo.NMAXREC, n - vo.NMAXREC):
+            b0 = struct.unpack("<i", f.read(4))[0]
+            f.seek(b0, 1)
+            assert b0 == 4 * size and struct.unpack("<i", f.read(4))[0] == b0
+        assert f.read(1) == b""
+    back = v3.read_model(out)
+    out.unlink()
+    assert np.array_equal(back, cubes)
