@@ -96,3 +96,23 @@ def test_struct_layouts_match_the_header(fz, tmp_path):
         assert dt.itemsize == size, struct
         for n in names:
             assert dt.fields[n][1] == offs[n], (struct, n)
+
+
+def test_fortran_interfaces_match_the_header():
+    """Every ISO_C_BINDING interface INTEGRATION.md gives the Fortran host
+    binds a function the header declares, with the same number of
+    arguments."""
+    hdr = "".join(open(os.path.join(ROOT, "include", f)).read()
+                  for f in os.listdir(os.path.join(ROOT, "include")) if f.endswith(".h"))
+    hdr = re.sub(r"/\*.*?\*/", "", hdr, flags=re.S)
+    protos = {}
+    for m in re.finditer(r"\b(fz_\w+)\s*\(([^)]*)\)\s*;", hdr):
+        args = m.group(2).strip()
+        protos[m.group(1)] = 0 if args in ("", "void") else args.count(",") + 1
+    doc = open(os.path.join(ROOT, "INTEGRATION.md")).read().replace("&\n", " ")
+    found = re.findall(r"FUNCTION\s+FZ_\w+\(([^)]*)\)\s*BIND\(C,\s*NAME='(fz_\w+)'\)", doc)
+    assert len(found) >= 10
+    for args, name in found:
+        assert name in protos, name
+        n = 0 if not args.strip() else args.count(",") + 1
+        assert n == protos[name], (name, n, protos[name])
