@@ -159,19 +159,54 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
-def cpu_lm_sample(fz, lines, reg, he, nz, npix, seed, nthreads=0):
-    """The oracle's pixel-wise LM (plain initial guess) on npix pixels of the
-    workload; returns (pixels/s, seconds, median chi2)."""
-    sys.path.insert(0, os.path.join(ROOT, "tests"))
-    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+def _oracle_side():
+    """The modules the CPU arms use: the oracle's ctypes wrapper (tests/orc.py),
+    its LM (oracle/lm_oracle.py) and the workload generator atmos.py loaded as
+    a plain module -- never the package or libfzb200.so."""
+    for d in (os.path.join(ROOT, "tests"), os.path.join(ROOT, "oracle")):
+        if d not in sys.path:
+            sys.path.insert(0, d)
     import orc
     import lm_oracle as lmo
-    from firtez_dz_b200 import warmstart as ws
+    name = "fz_workload_atmos"
+    if name not in sys.modules:
+        spec = importlib.util.spec_from_file_location(name, os.path.join(PKG_DIR, "atmos.py"))
+        mod = importlib.util.module_from_spec(spec)
+        spec.loader.exec_module(mod)
+        sys.modules[name] = mod
+    return orc, lmo, sys.modules[name]
+
+
+def cpu_workload():
+    """Line table and regions of the workload parsed by the oracle."""
+    orc, _, atm = _oracle_side()
+    lines = orc.parse_lines(atm.line_database_text())
+    return lines, orc.regions(atm.lines_section(2), lines)
+
+
+def default_guess(atm, npix, nz, b=100.0):
+    """The plain initial guess: the mean temperature stratification, its
+    hydrostatic pressure, a field of (b, b, b) G and v_z = 0."""
+    z = atm.z_grid(nz)
+    T = atm.mean_temperature(z)[None, :]
+    m = np.zeros((npix, 13, nz), dtype=np.float32)
+    m[:, 0] = T
+    m[:, 1] = atm.hydrostatic_pg(T, z)
+    m[:, 5:8] = b
+    m[:, 12] = z[None, :]
+    return m
+
+
+def cpu_lm_sample(lines, reg, he, nz, npix, seed, nthreads=0):
+    """The oracle's pixel-wise LM (plain initial guess) on npix pixels of the
+    workload, OpenMP over the pixels of each forward pass; returns (pixels/s,
+    seconds, median chi2)."""
+    orc, lmo, atm = _oracle_side()
     gain, _ = orc.gain(lines, reg)
-    true = fz.atmos.make_columns(npix, nz, seed=seed)
+    true = atm.make_columns(npix, nz, seed=seed)
     obs, _, _ = orc.forward(lines, reg, gain, true, hydrostatic=he, nthreads=nthreads)
     obs = obs.reshape(npix, -1) + np.random.default_rng(seed).normal(0.0, 1e-3, (npix, obs.shape[1] * obs.shape[2]))
-    init = ws.default_models(npix, nz)
+    init = default_guess(atm, npix, nz)
     w = lmo.weights(obs.shape[1] // 4, isigma=1e-3)
 
     def fwd(models):
@@ -182,6 +217,53 @@ def cpu_lm_sample(fz, lines, reg, he, nz, npix, seed, nthreads=0):
     _, chi, _ = lmo.invert(fwd, obs, init, NODES, w, maxsteps=5, maxit=40, dchi2=1e-3)
     el = time.perf_counter() - t0
     return npix / el, el, float(np.median(chi))
+
+
+def cpu_synth_sample(lines, reg, he, nz, ncol, seed, nthreads=0):
+    """The oracle's FP64 synthesis of ncol seeded columns, OpenMP over
+    columns; returns (columns*lambda/s, seconds)."""
+    orc, _, atm = _oracle_side()
+    gain, _ = orc.gain(lines, reg)
+    m = atm.make_columns(ncol, nz, seed=seed)
+    numw = int(reg["numwave"].sum())
+    t0 = time.perf_counter()
+    orc.forward(lines, reg, gain, m, hydrostatic=he, nthreads=nthreads)
+    el = time.perf_counter() - t0
+    return ncol * numw / el, el
+
+
+def reference_arm(a, config, he):
+    """``--impl reference``: the CPU restatement of the reference (the Fortran
+    reference cannot be built here: no gfortran/MPI/LAPACK) timed on all host
+    cores -- plain LM from the default guess, each step a bounded sample of
+    4 x cores pixels of the workload; beside it the FP64 synthesis of 256
+    columns of the synthesis sub-metric's shape.  Rank 0 only."""
+    lines, reg = cpu_workload()
+    cores = os.cpu_count()
+    npx = a.cpu_pixels if a.cpu_pixels > 0 else 4 * cores
+    numw = int(reg["numwave"].sum())
+    tot_t, chis = 0.0, []
+    for i in range(a.warmup):
+        cpu_lm_sample(lines, reg, he, a.nz, 2, seed=900 + i)
+    for i in range(a.steps):
+        _, el, c = cpu_lm_sample(lines, reg, he, a.nz, npx, seed=1000 + i)
+        tot_t += el
+        chis.append(c)
+    value = float(a.steps * npx / tot_t)
+    sv, sel = cpu_synth_sample(lines, reg, he, a.nz, 256, seed=2)
+    sample = ("%d pixels per step (4 x %d cores), LM from the default guess to the plain stop rules, FP64 C++ "
+              "restatement of the reference's forward/RF routines (OpenMP over pixels) + numpy/LAPACK LM; the "
+              "Fortran reference needs gfortran/MPI/LAPACK, absent on this image" % (npx, cores))
+    out = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": a.gpus,
+           "steps": a.steps, "warmup": a.warmup, "ms_per_step": 1e3 * tot_t / a.steps,
+           "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+           "data": "synthetic", "config": config, "median_chi2": float(np.median(chis)),
+           "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample},
+           "synthesis": {"value": sv, "unit": "columns*lambda/s", "seconds": sel,
+                         "workload": "256 columns x %d heights x %d lambda, hydrostatic, FP64 oracle on %d cores"
+                                     % (a.nz, numw, cores)},
+           "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(out))
 
 
 def main():
@@ -196,7 +278,7 @@ def main():
     ap.add_argument("--nz", type=int, default=128)
     ap.add_argument("--train-pairs", type=int, default=2097152)
     ap.add_argument("--epochs", type=int, default=6)
-    ap.add_argument("--cpu-pixels", type=int, default=24)
+    ap.add_argument("--cpu-pixels", type=int, default=0, help="CPU LM pixels per sample (0: 4 x cores)")
     ap.add_argument("--synth-cols", type=int, default=256 * 256)
     ap.add_argument("--rf-chunk", type=int, default=4096, help="columns per full-height RF call")
     ap.add_argument("--no-tune", action="store_true", help="keep the default launch shapes")
@@ -205,10 +287,7 @@ def main():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     he = True
-    fz = load_package()
-    lines = fz.lines_parse(fz.atmos.line_database_text())
-    reg = fz.regions_from_lines_section(fz.atmos.lines_section(2), lines)
-    numw = int(reg["numwave"].sum())
+    numw = 2 * 112
     nf = 4 * numw
     config = {"workload": "batched LM inversion, %dx%d pixels x %d heights, Fe I 6301.5+6302.5 x 112 lambda, "
                           "nodes T5 Bx2 By2 Bz2 vz2 (NP=13), noise 1e-3 Ic, NN-warm start "
@@ -219,28 +298,15 @@ def main():
               "parallelism": "pixel tiles sharded per GPU" if world > 1 else "single GPU"}
 
     if a.impl == "reference":
-        if rank != 0:
-            return
-        tot_t, chis = 0.0, []
-        for i in range(a.warmup):
-            cpu_lm_sample(fz, lines, reg, he, a.nz, 2, seed=900 + i)
-        for i in range(a.steps):
-            _, el, c = cpu_lm_sample(fz, lines, reg, he, a.nz, a.cpu_pixels, seed=1000 + i)
-            tot_t += el
-            chis.append(c)
-        value = float(a.steps * a.cpu_pixels / tot_t)
-        out = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": a.gpus,
-               "steps": a.steps, "warmup": a.warmup, "ms_per_step": 1e3 * tot_t / a.steps,
-               "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-               "data": "synthetic", "config": config, "median_chi2": float(np.median(chis)),
-               "cpu_baseline": {"value": value, "unit": UNIT, "cores": os.cpu_count(), "kind": "port",
-                                "sample": "%d pixels per step, LM from the default guess, FP64 C++/numpy "
-                                          "restatement of the reference (OpenMP over columns; the Fortran "
-                                          "reference needs gfortran/MPI/LAPACK, absent on this image)"
-                                          % a.cpu_pixels},
-               "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
-        print(json.dumps(out))
+        # before anything of the product is imported or loaded
+        if rank == 0:
+            reference_arm(a, config, he)
         return
+
+    fz = load_package()
+    lines = fz.lines_parse(fz.atmos.line_database_text())
+    reg = fz.regions_from_lines_section(fz.atmos.lines_section(2), lines)
+    assert int(reg["numwave"].sum()) == numw
 
     import torch
     from firtez_dz_b200 import warmstart as ws
@@ -757,11 +823,19 @@ def main():
                                               % per_launch["k_synth_rf"][2],
                                 "peak_source": "measured FMA-chain kernel (fz_measure_fp32_peak)"}
     if world == 1:
-        v, el, c = cpu_lm_sample(fz, lines, reg, he, a.nz, a.cpu_pixels, seed=1000)
+        # the oracle on the host cores, with its own line parse (the same rows)
+        olines, oreg = cpu_workload()
+        npx = a.cpu_pixels if a.cpu_pixels > 0 else 4 * os.cpu_count()
+        v, el, c = cpu_lm_sample(olines, oreg, he, a.nz, npx, seed=1000)
+        sv, sel = cpu_synth_sample(olines, oreg, he, a.nz, 256, seed=2)
         out["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": os.cpu_count(), "kind": "port",
-                               "sample": "%d pixels, LM from the default guess, in %.1f s (FP64 C++/numpy "
-                                         "restatement of the reference, OpenMP over columns); median chi2 %.3g"
-                                         % (a.cpu_pixels, el, c)}
+                               "sample": "%d pixels (4 x cores), LM from the default guess, in %.1f s (FP64 C++ "
+                                         "restatement of the reference's forward/RF routines, OpenMP over pixels, "
+                                         "+ numpy/LAPACK LM); median chi2 %.3g" % (npx, el, c),
+                               "synthesis": {"value": sv, "unit": "columns*lambda/s", "seconds": sel,
+                                             "workload": "256 columns x %d heights x %d lambda, hydrostatic, "
+                                                         "FP64" % (a.nz, numw),
+                                             "gpu_over_cpu": synthesis["value"] / sv}}
     print(json.dumps(out))
     sys.stdout.flush()
     ranks.close()

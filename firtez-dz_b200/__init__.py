@@ -65,10 +65,12 @@ class LMOpts(ctypes.Structure):
                 ("slots", ctypes.c_int), ("assist", ctypes.c_int), ("fallback", ctypes.c_double),
                 ("fallback_model", ctypes.c_void_p), ("reg_type", ctypes.c_int * 8), ("reg_alpha", ctypes.c_double * 8),
                 ("fallback_steps", ctypes.c_int), ("solver", ctypes.c_int), ("node_expansion", ctypes.c_int),
-                ("pad2", ctypes.c_int)]
+                ("global_stop", ctypes.c_int), ("cycles_left", ctypes.c_int), ("pad3", ctypes.c_int),
+                ("state_out", ctypes.c_void_p)]
 
     def __init__(self, maxsteps=5, maxit=40, dchi2=0.0, svdtol=1e-4, isigma=4e-3, wstk=(1, 1, 1, 1), slots=0,
-                 fallback=0.0, fallback_model=0, reg=None, assist=(), fallback_steps=0, solver=1, node_expansion=1):
+                 fallback=0.0, fallback_model=0, reg=None, assist=(), fallback_steps=0, solver=1, node_expansion=1,
+                 global_stop=False, cycles_left=0, state_out=0):
         """fallback_model: device pointer of one MODEL(NZ,13) float32 (e.g. a
         torch tensor's data_ptr()) that pixels ending above fallback x their
         chi2 goal restart from (a host pointer for invert()).  reg: optional
@@ -78,14 +80,19 @@ class LMOpts(ctypes.Structure):
         fallback_steps: restart once STEPS reaches it while above fallback x
         the goal (0: when the search ends).  solver: 1 SVD, 2 conjugate
         gradients (LINEAR_SOLVER); node_expansion: 1 SIR-like, 2 STiC-like
-        (PERTURBATION_TYPE)."""
+        (PERTURBATION_TYPE).  global_stop: MAKE_DECISION's field-wide stop on
+        the mean STEPS (threshold max(1, maxsteps - cycles_left)); state_out:
+        pointer of a (npix, 5) float64 array receiving each pixel's final
+        STEPS, chi2 of its last model, best chi2, PRECYC and lambda (device
+        pointer for the device calls, host pointer for invert())."""
         typ, alp = [0] * 8, [0.0] * 8
         for p, (t, a) in (reg or {}).items():
             typ[int(p) - 1], alp[int(p) - 1] = int(t), float(a)
         super().__init__(maxsteps, maxit, dchi2, svdtol, isigma, (ctypes.c_float * 4)(*wstk), slots,
                          assist_bits(assist),
                          float(fallback), fallback_model or None, (ctypes.c_int * 8)(*typ),
-                         (ctypes.c_double * 8)(*alp), int(fallback_steps), int(solver), int(node_expansion), 0)
+                         (ctypes.c_double * 8)(*alp), int(fallback_steps), int(solver), int(node_expansion),
+                         int(bool(global_stop)), int(cycles_left), 0, state_out or None)
 
 
 class Tune(ctypes.Structure):
@@ -174,6 +181,10 @@ def lib():
         L.fz_invert_device.argtypes = [P, ctypes.c_int, P, P, P, ctypes.c_int, P, P, P, P, P, P, P]
         L.fz_lm_perturbation.argtypes = [P, ctypes.c_int, ctypes.c_int, ctypes.c_int, P, P, P, P, P, ctypes.c_int,
                                          ctypes.c_double, P]
+        L.fz_lm_perturbation_f32.argtypes = L.fz_lm_perturbation.argtypes
+        L.fz_lm_update_lambda.argtypes = [ctypes.c_int, P, P, P, P, P]
+        L.fz_lm_rearange.argtypes = [P, ctypes.c_int, P, P, ctypes.c_int]
+        L.fz_lm_rearange_device.argtypes = [P, ctypes.c_int, P, P, ctypes.c_int, P]
         _lib = L
     return _lib
 
@@ -604,21 +615,34 @@ class Synthesis:
                                       ctypes.c_void_p(stream) if stream else None))
 
     def lm_perturbation(self, jac, diff, lam, svdtol=1e-4, reg_pen=None, reg_hss=None, dtype=1):
-        """Batched GET_PERTURBATION: jac (npix, np, nfreq) normalised Jacobian,
-        diff (npix, nfreq), lam (npix,); optional reg_pen (npix, np) and
-        reg_hss (npix, np, np); dtype 1 SVD, 2 conjugate gradients.  Returns
-        delta (npix, np)."""
-        j = np.ascontiguousarray(jac, dtype=np.float32)
+        """Batched GET_PERTURBATION: jac (npix, np, nfreq) normalised Jacobian
+        -- float64 (IJACOBIAN, fz_lm_perturbation) or float32
+        (fz_lm_perturbation_f32) --, diff (npix, nfreq), lam (npix,); optional
+        reg_pen (npix, np) and reg_hss (npix, np, np); dtype 1 SVD, 2
+        conjugate gradients.  Returns delta (npix, np)."""
+        j = np.asarray(jac)
+        j = np.ascontiguousarray(j, dtype=np.float32 if j.dtype == np.float32 else np.float64)
         d = np.ascontiguousarray(diff, dtype=np.float64)
         lm = np.ascontiguousarray(lam, dtype=np.float64)
         npix, npar, nf = j.shape
         rp = None if reg_pen is None else np.ascontiguousarray(reg_pen, dtype=np.float64).reshape(npix, npar)
         rh = None if reg_hss is None else np.ascontiguousarray(reg_hss, dtype=np.float64).reshape(npix, npar, npar)
         out = np.zeros((npix, npar))
-        _check(lib().fz_lm_perturbation(self._h, npix, npar, nf, _p(j), _p(d), _p(lm),
-                                        None if rp is None else _p(rp), None if rh is None else _p(rh),
-                                        int(dtype), float(svdtol), _p(out)))
+        fn = lib().fz_lm_perturbation_f32 if j.dtype == np.float32 else lib().fz_lm_perturbation
+        _check(fn(self._h, npix, npar, nf, _p(j), _p(d), _p(lm), None if rp is None else _p(rp),
+                  None if rh is None else _p(rh), int(dtype), float(svdtol), _p(out)))
         return out
+
+    def lm_rearange(self, models, delta, node_expansion=1):
+        """Batched REARANGE_DA_MODEL: the normalised node perturbation delta
+        (npix, np) applied to models (npix, 13, nz) with the node layout of
+        rf_nodes(); returns the new models."""
+        m = np.array(models, dtype=np.float32, order="C", copy=True)
+        d = np.ascontiguousarray(delta, dtype=np.float64)
+        if m.ndim != 3 or m.shape[1:] != (13, self.nz) or d.shape[0] != m.shape[0]:
+            raise ValueError("models must be (npix, 13, nz) and delta (npix, np)")
+        _check(lib().fz_lm_rearange(self._h, m.shape[0], _p(m), _p(d), int(node_expansion)))
+        return m
 
     def forward_rf_device(self, model_ptr, ncol, syn_ptr, jac_ptr, model_out_ptr, status_ptr=0, stream=0,
                           hydrostatic=False):
@@ -635,6 +659,15 @@ class Synthesis:
                                        ctypes.c_void_p(syn_ptr), ctypes.c_void_p(model_out_ptr),
                                        ctypes.c_void_p(status_ptr) if status_ptr else None,
                                        ctypes.c_void_p(stream) if stream else None))
+
+
+def lm_update_lambda(chicur, chipre, lam, steps, precyc):
+    """Batched UPDATE_LAMBDA on the GPU; returns the updated (chipre, lambda,
+    steps, precyc) arrays."""
+    cc = np.ascontiguousarray(chicur, dtype=np.float64)
+    out = [np.array(a, dtype=np.float64, copy=True).reshape(cc.shape) for a in (chipre, lam, steps, precyc)]
+    _check(lib().fz_lm_update_lambda(cc.size, _p(cc), *[_p(a) for a in out]))
+    return tuple(out)
 
 
 def measure_fp32_peak(device=0):

@@ -1430,7 +1430,8 @@ struct fz_ctx {
     float *init = nullptr, *out = nullptr;
     int *it = nullptr, *st = nullptr;
     float* fb = nullptr;   // the fallback model (13, nz)
-    size_t cap = 0;
+    double* state = nullptr;   // the final LM states (5, npix), when asked for
+    size_t cap = 0, state_cap = 0;
     bool has_syn = false;
   } inv;
   cudaStream_t stream = nullptr;
@@ -1532,12 +1533,14 @@ struct ProfScope {
 // k_chain with wpb warps per block and lanes (32 or 16) lanes per column;
 // lanes = 0 picks 16 when the batch fills 8 warps per SM with two columns a
 // warp (throughput: half the warp instructions per column) and 32 below
-// (latency: every column's chain gets a warp of its own).
+// (latency: every column's chain gets a warp of its own).  chem: the (nH, ne)
+// scratch of the batch, the context's own buffer when null.
 void launch_k_chain(fz_ctx* c, int ncol, const float* d_model, float* d_mout, int* d_status, int hydrostatic, int wpb,
-                    int lanes, cudaStream_t s) {
+                    int lanes, cudaStream_t s, double2* chem = nullptr) {
+  if (!chem) chem = c->d_chem;
   if (hydrostatic == 2) {   // HE anchored at log tau5 ~ 0 (HYDRO_TOP off)
     const dim3 g((unsigned)(((size_t)ncol * 32 + 127) / 128));
-    k_chain_med<<<g, 128, 0, s>>>(c->d_consts, c->d_pf, ncol, c->nz, d_model, d_mout, c->d_chem, d_status);
+    k_chain_med<<<g, 128, 0, s>>>(c->d_consts, c->d_pf, ncol, c->nz, d_model, d_mout, chem, d_status);
     return;
   }
   if (lanes != 16 && lanes != 32) lanes = ncol >= 16 * c->nsm ? 16 : 32;
@@ -1545,17 +1548,17 @@ void launch_k_chain(fz_ctx* c, int ncol, const float* d_model, float* d_mout, in
   const dim3 gc((unsigned)((threads + wpb * 32 - 1) / (wpb * 32)));
   if (lanes == 16) {
     if (hydrostatic)
-      k_chain<true, 16><<<gc, wpb * 32, 0, s>>>(c->d_consts, c->d_pf, ncol, c->nz, d_model, d_mout, c->d_chem,
+      k_chain<true, 16><<<gc, wpb * 32, 0, s>>>(c->d_consts, c->d_pf, ncol, c->nz, d_model, d_mout, chem,
                                                 d_status);
     else
-      k_chain<false, 16><<<gc, wpb * 32, 0, s>>>(c->d_consts, c->d_pf, ncol, c->nz, d_model, d_mout, c->d_chem,
+      k_chain<false, 16><<<gc, wpb * 32, 0, s>>>(c->d_consts, c->d_pf, ncol, c->nz, d_model, d_mout, chem,
                                                  d_status);
   } else {
     if (hydrostatic)
-      k_chain<true, 32><<<gc, wpb * 32, 0, s>>>(c->d_consts, c->d_pf, ncol, c->nz, d_model, d_mout, c->d_chem,
+      k_chain<true, 32><<<gc, wpb * 32, 0, s>>>(c->d_consts, c->d_pf, ncol, c->nz, d_model, d_mout, chem,
                                                 d_status);
     else
-      k_chain<false, 32><<<gc, wpb * 32, 0, s>>>(c->d_consts, c->d_pf, ncol, c->nz, d_model, d_mout, c->d_chem,
+      k_chain<false, 32><<<gc, wpb * 32, 0, s>>>(c->d_consts, c->d_pf, ncol, c->nz, d_model, d_mout, chem,
                                                  d_status);
   }
 }
@@ -1883,6 +1886,9 @@ int lm_conf(fz_ctx* c, int npix, const fz_lm_opts* o, LMConf& C) {
   C.fb_steps = o && o->fallback_steps > 0 ? o->fallback_steps : (1 << 30);
   C.solver = o && o->solver == 2 ? 2 : 1;
   C.node_exp = o && o->node_expansion == 2 ? 2 : 1;
+  C.global_stop = o && o->global_stop ? 1 : 0;
+  C.state_out = o ? o->state_out : nullptr;
+  if (o && o->cycles_left < 0) return FZ_ERR_ARG;
   if (o && (o->solver < 0 || o->solver > 2 || o->node_expansion < 0 || o->node_expansion > 2)) return FZ_ERR_ARG;
   // GET_IT_PENALTIES operators (src/get_dmodel.f90:1103-1146): per free
   // parameter L = sqrt(PEN_ALP / IFREEP) D, D = diag(1/NJ) (type 0) or first
@@ -1965,6 +1971,13 @@ bool int_coefs(int nz, int nj, std::vector<double>& coef) {
 // log tau5 of every column from the opacity slab k_opac leaves, the
 // integration of src/forward.f90:1000-1006 (REAL*4 accumulation from the
 // top, as k_synth does), without the Stokes synthesis.
+// Grid-stride FP64 -> FP32 rounding (a REAL*8 Jacobian into the FP32
+// operand of the split-bf16 normal equations).
+__global__ void k_f64_to_f32(size_t n, const double* __restrict__ a, float* __restrict__ b) {
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+    b[i] = (float)a[i];
+}
+
 __global__ void k_tau5(int ncol, int nz, int sw, const float* __restrict__ slab, float* __restrict__ mout) {
   const int col = blockIdx.x * blockDim.x + threadIdx.x;
   if (col >= ncol) return;
@@ -2356,9 +2369,13 @@ int fz_invert_cycles_device(fz_ctx* c, int nx, int ny, const double* d_obs, floa
       if (assist && nodes[8 * cy + 1] == 0 && nodes[8 * cy + 7] == 0 && (cy == 0 || !(opts->assist & 16)))
         if ((rc = fz_set_tau_device(c, nx, ny, d_obs, d_models, assist, hydrostatic, s))) break;
       if ((rc = fz_smooth_device(c, nx, ny, d_models, nullptr, s))) break;
-      // the cycle's iterations, each pixel from a fresh LM state
-      if ((rc = fz_invert_device(c, npix, d_obs, d_models, nullptr, hydrostatic, opts, d_best, d_chi2, d_iters,
-                                 nullptr, d_status, s)))
+      // the cycle's iterations, each pixel from a fresh LM state; the field
+      // rule's threshold depends on the cycles still to come
+      fz_lm_opts oc{};
+      if (opts) oc = *opts;
+      oc.cycles_left = ncycles - 1 - cy;
+      if ((rc = fz_invert_device(c, npix, d_obs, d_models, nullptr, hydrostatic, opts ? &oc : nullptr, d_best, d_chi2,
+                                 d_iters, nullptr, d_status, s)))
         break;
       // END_CYCLE: the best models through a plain synthesis (the derived
       // rows: Pg in hydrostatic mode, rho, Pe, mu, log tau5)
@@ -3119,6 +3136,7 @@ int fz_invert_device(fz_ctx* c, int npix, const double* d_obs, const float* d_in
   int rc = lm_conf(c, npix, opts, C);
   if (rc) return rc;
   int S = (opts && opts->slots > 0) ? opts->slots : c->tune.lm_slots;
+  if (C.global_stop) S = npix;   // the field rule needs every pixel in flight
   if (S > npix) S = npix;
   if ((rc = lm_alloc(c, S))) return rc;
   // The iterations run on the context's own stream (capturable, unlike a
@@ -3237,6 +3255,17 @@ int fz_invert_device(fz_ctx* c, int npix, const double* d_obs, const float* d_in
       c->prof_items[4] += hq.rf_count;
     }
     if (hq.done >= npix) return 0;
+    if (C.global_stop) {
+      // MAKE_DECISION: the field stops once the mean STEPS over its pixels
+      // reaches max(1, MAXSTEPS - (MAXITER - CURIC))
+      const int thr = std::max(1, C.maxsteps - opts->cycles_left);
+      if ((double)(long long)hq.steps_sum >= (double)thr * (double)npix) {
+        k_lm_finish_all<<<n, 256, 0, s>>>(C, L, c->d_q, d_model_out, d_chi2, d_iters, d_syn_out, d_status);
+        FZ_CK(cudaGetLastError());
+        FZ_CK(cudaStreamSynchronize(s));
+        return 0;
+      }
+    }
     // the queue is drained: move the occupied slots to the front of the
     // other pool once a quarter of the pool has emptied, and iterate on them only
     if (hq.next >= npix && hq.active > 0 && hq.active <= (3 * n) / 4) {
@@ -3260,6 +3289,7 @@ static void inv_free(fz_ctx* c) {
   cudaFree(c->inv.it);
   cudaFree(c->inv.st);
   cudaFree(c->inv.fb);
+  cudaFree(c->inv.state);
   c->inv = {};
 }
 
@@ -3304,6 +3334,16 @@ int fz_invert(fz_ctx* c, int npix, const double* obs, const float* init, const d
     FZ_CK(cudaMemcpyAsync(c->inv.fb, opts->fallback_model, nm * sizeof(float), cudaMemcpyHostToDevice, s));
     o.fallback_model = c->inv.fb;
   }
+  if (opts && opts->state_out) {
+    if ((size_t)npix > c->inv.state_cap) {
+      cudaFree(c->inv.state);
+      c->inv.state = nullptr;
+      c->inv.state_cap = 0;
+      FZ_CK(cudaMalloc(&c->inv.state, (size_t)npix * 5 * sizeof(double)));
+      c->inv.state_cap = npix;
+    }
+    o.state_out = c->inv.state;
+  }
   int rc = fz_invert_device(c, npix, c->inv.obs, c->inv.init, target_chi2 ? c->inv.tgt : nullptr, hydrostatic,
                             opts ? &o : nullptr,
                             c->inv.out, c->inv.chi, c->inv.it, syn_out ? c->inv.syn : nullptr, c->inv.st, s);
@@ -3313,14 +3353,20 @@ int fz_invert(fz_ctx* c, int npix, const double* obs, const float* init, const d
   FZ_CK(cudaMemcpyAsync(iters, c->inv.it, npix * sizeof(int), cudaMemcpyDeviceToHost, s));
   if (status) FZ_CK(cudaMemcpyAsync(status, c->inv.st, npix * sizeof(int), cudaMemcpyDeviceToHost, s));
   if (syn_out) FZ_CK(cudaMemcpyAsync(syn_out, c->inv.syn, npix * nf * sizeof(double), cudaMemcpyDeviceToHost, s));
+  if (opts && opts->state_out)
+    FZ_CK(cudaMemcpyAsync(opts->state_out, c->inv.state, (size_t)npix * 5 * sizeof(double), cudaMemcpyDeviceToHost,
+                          s));
   FZ_CK(cudaStreamSynchronize(s));
   return 0;
 }
 
-int fz_lm_perturbation(fz_ctx* c, int npix, int np, int nfreq, const float* jac, const double* diff,
-                       const double* lambda, const double* reg_pen, const double* reg_hss, int dtype, double svdtol,
-                       double* delta) {
-  if (!c || npix <= 0 || np <= 0 || np > LM_MAXNP || nfreq <= 0 || (nfreq & 3) || !jac || !diff || !lambda || !delta)
+// Batched GET_PERTURBATION on host buffers; the Jacobian comes as REAL*8
+// (jac64) or REAL*4 (jac32), exactly one of them given.  A REAL*8 Jacobian is
+// rounded to FP32 on the device before the split-bf16 normal equations.
+static int lm_perturbation_host(fz_ctx* c, int npix, int np, int nfreq, const double* jac64, const float* jac32,
+                                const double* diff, const double* lambda, const double* reg_pen,
+                                const double* reg_hss, int dtype, double svdtol, double* delta) {
+  if (!c || npix <= 0 || np <= 0 || np > LM_MAXNP || nfreq <= 0 || (nfreq & 3) || (!jac64 == !jac32) || !diff || !lambda || !delta)
     return FZ_ERR_ARG;
   if (dtype < 0 || dtype > 2) return FZ_ERR_ARG;   // GET_PERTURBATION's DTYPE (0 taken as 1)
   FZ_CK(cudaSetDevice(c->device));
@@ -3361,7 +3407,22 @@ int fz_lm_perturbation(fz_ctx* c, int npix, int np, int nfreq, const float* jac,
     cudaMemcpy(L.pix, zeros.data(), npix * sizeof(int), cudaMemcpyHostToDevice);
     cudaMemcpy(L.skip, zeros.data(), npix * sizeof(int), cudaMemcpyHostToDevice);
     cudaMemcpy(L.st, st.data(), st.size() * sizeof(double), cudaMemcpyHostToDevice);
-    cudaMemcpy(L.jacb, jac, (size_t)npix * np * nfreq * sizeof(float), cudaMemcpyHostToDevice);
+    if (jac32) {
+      cudaMemcpy(L.jacb, jac32, (size_t)npix * np * nfreq * sizeof(float), cudaMemcpyHostToDevice);
+    } else {
+      // the REAL*8 IJACOBIAN in a buffer of its own, rounded into L.jacb
+      double* d_j64 = nullptr;
+      const size_t nj = (size_t)npix * np * nfreq;
+      if ((rc = cuda_fail(cudaMalloc(&d_j64, nj * sizeof(double))))) break;
+      rc = cuda_fail(cudaMemcpy(d_j64, jac64, nj * sizeof(double), cudaMemcpyHostToDevice));
+      if (!rc) {
+        k_f64_to_f32<<<(int)std::min<size_t>((nj + 255) / 256, (size_t)c->nsm * 16), 256, 0, c->stream>>>(
+            nj, d_j64, L.jacb);
+        rc = cuda_fail(cudaStreamSynchronize(c->stream));
+      }
+      cudaFree(d_j64);
+      if (rc) break;
+    }
     cudaMemcpy(L.diff, diff, (size_t)npix * nfreq * sizeof(double), cudaMemcpyHostToDevice);
     cudaMemcpy(d_w, ones.data(), nfreq * sizeof(double), cudaMemcpyHostToDevice);
     k_lm_normal<<<(npix + 3) / 4, 128, 0, c->stream>>>(C, L, d_w);
@@ -3381,6 +3442,80 @@ int fz_lm_perturbation(fz_ctx* c, int npix, int np, int nfreq, const float* jac,
   cudaFree(L.pen);
   cudaFree(L.hss);
   cudaFree(d_w);
+  return rc;
+}
+
+int fz_lm_perturbation(fz_ctx* c, int npix, int np, int nfreq, const double* jac, const double* diff,
+                       const double* lambda, const double* reg_pen, const double* reg_hss, int dtype, double svdtol,
+                       double* delta) {
+  if (!jac) return FZ_ERR_ARG;
+  return lm_perturbation_host(c, npix, np, nfreq, jac, nullptr, diff, lambda, reg_pen, reg_hss, dtype, svdtol, delta);
+}
+
+int fz_lm_perturbation_f32(fz_ctx* c, int npix, int np, int nfreq, const float* jac, const double* diff,
+                           const double* lambda, const double* reg_pen, const double* reg_hss, int dtype,
+                           double svdtol, double* delta) {
+  if (!jac) return FZ_ERR_ARG;
+  return lm_perturbation_host(c, npix, np, nfreq, nullptr, jac, diff, lambda, reg_pen, reg_hss, dtype, svdtol, delta);
+}
+
+int fz_lm_update_lambda_device(int n, const double* d_chicur, double* d_chipre, double* d_lambda, double* d_steps,
+                               double* d_precyc, void* stream) {
+  if (n <= 0 || !d_chicur || !d_chipre || !d_lambda || !d_steps || !d_precyc) return FZ_ERR_ARG;
+  k_lm_lambda<<<(n + 255) / 256, 256, 0, (cudaStream_t)stream>>>(n, d_chicur, d_chipre, d_lambda, d_steps, d_precyc);
+  return cuda_fail(cudaGetLastError());
+}
+
+int fz_lm_update_lambda(int n, const double* chicur, double* chipre, double* lambda, double* steps, double* precyc) {
+  if (n <= 0 || !chicur || !chipre || !lambda || !steps || !precyc) return FZ_ERR_ARG;
+  double* d = nullptr;
+  const size_t b = (size_t)n * sizeof(double);
+  FZ_CK(cudaMalloc(&d, 5 * b));
+  int rc = 0;
+  const double* src[5] = {chicur, chipre, lambda, steps, precyc};
+  for (int k = 0; k < 5 && !rc; ++k) rc = cuda_fail(cudaMemcpy(d + (size_t)k * n, src[k], b, cudaMemcpyHostToDevice));
+  if (!rc) rc = fz_lm_update_lambda_device(n, d, d + n, d + 2 * (size_t)n, d + 3 * (size_t)n, d + 4 * (size_t)n, nullptr);
+  double* dst[4] = {chipre, lambda, steps, precyc};
+  for (int k = 0; k < 4 && !rc; ++k)
+    rc = cuda_fail(cudaMemcpy(dst[k], d + (size_t)(k + 1) * n, b, cudaMemcpyDeviceToHost));
+  cudaFree(d);
+  return rc;
+}
+
+int fz_lm_rearange_device(fz_ctx* c, int npix, float* d_models, const double* d_delta, int node_expansion,
+                          void* stream) {
+  if (!c || npix <= 0 || !d_models || !d_delta || node_expansion < 0 || node_expansion > 2) return FZ_ERR_ARG;
+  FZ_CK(cudaSetDevice(c->device));
+  fz_lm_opts o{};
+  o.node_expansion = node_expansion;
+  LMConf C;
+  int rc = lm_conf(c, npix, &o, C);
+  if (rc) return rc;
+  LMSlots L{};
+  L.S = npix;
+  L.mcur = d_models;
+  L.delta = const_cast<double*>(d_delta);
+  const size_t usm = (size_t)(C.nz + 3 * C.np) * sizeof(double) + (size_t)C.nz * sizeof(float);
+  k_lm_update<<<npix, 128, usm, (cudaStream_t)stream>>>(C, L, c->d_coef64);
+  return cuda_fail(cudaGetLastError());
+}
+
+int fz_lm_rearange(fz_ctx* c, int npix, float* models, const double* delta, int node_expansion) {
+  if (!c || npix <= 0 || !models || !delta) return FZ_ERR_ARG;
+  FZ_CK(cudaSetDevice(c->device));
+  if (c->rf.np <= 0) return FZ_ERR_STATE;
+  const size_t mb = (size_t)npix * 13 * c->nz * sizeof(float), db = (size_t)npix * c->rf.np * sizeof(double);
+  float* dm = nullptr;
+  double* dd = nullptr;
+  int rc = cuda_fail(cudaMalloc(&dm, mb));
+  if (!rc) rc = cuda_fail(cudaMalloc(&dd, db));
+  if (!rc) rc = cuda_fail(cudaMemcpy(dm, models, mb, cudaMemcpyHostToDevice));
+  if (!rc) rc = cuda_fail(cudaMemcpy(dd, delta, db, cudaMemcpyHostToDevice));
+  if (!rc) rc = fz_lm_rearange_device(c, npix, dm, dd, node_expansion, c->stream);
+  if (!rc) rc = cuda_fail(cudaStreamSynchronize(c->stream));
+  if (!rc) rc = cuda_fail(cudaMemcpy(models, dm, mb, cudaMemcpyDeviceToHost));
+  cudaFree(dm);
+  cudaFree(dd);
   return rc;
 }
 
@@ -3664,15 +3799,10 @@ int fz_forward_device_static(fz_ctx* c, int ncol, const float* d_model, int hydr
   // Every scratch word a kernel reads is written earlier in the same call
   // (k_chain fills chem, k_opac fills the slab rows), so nothing is cleared.
   if (d_status) FZ_CK(cudaMemsetAsync(d_status, 0, ncol * sizeof(int), s));
-  const int wpb = 4;
-  const dim3 gc((ncol + wpb - 1) / wpb);
-  if (hydrostatic == 2)
-    k_chain_med<<<gc, wpb * 32, 0, s>>>(c->d_consts, c->d_pf, ncol, c->nz, d_model, d_model_out, chem, d_status);
-  else if (hydrostatic)
-    k_chain<true, 32><<<gc, wpb * 32, 0, s>>>(c->d_consts, c->d_pf, ncol, c->nz, d_model, d_model_out, chem, d_status);
-  else
-    k_chain<false, 32><<<gc, wpb * 32, 0, s>>>(c->d_consts, c->d_pf, ncol, c->nz, d_model, d_model_out, chem,
-                                               d_status);
+  // the chemistry chain with the context's launch shape (tuned or default),
+  // so that both entry points run the same schedule and agree bit for bit
+  launch_k_chain(c, ncol, d_model, d_model_out, d_status, hydrostatic, c->tune.chain_warps, c->tune.chain_lanes, s,
+                 chem);
   FZ_CK(cudaGetLastError());
   const size_t total = (size_t)ncol * c->nz;
   const int blocks = (int)std::min<size_t>((total + 255) / 256, (size_t)c->nsm * 16);

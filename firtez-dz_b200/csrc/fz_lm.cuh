@@ -41,6 +41,8 @@ struct LMConf {
   int node_exp;                // NODE_EXPANSION: 1 SIR/NICOLE-like, 2 STiC-like
   int reg;                     // vertical regularisation on (GET_IT_PENALTIES)
   double reg_hss[LM_MAXNP * LM_MAXNP];   // PEN_HSS = L^T L (model independent)
+  int global_stop;             // MAKE_DECISION's field rule on the mean STEPS (steps summed in the queue)
+  double* state_out;           // (npix, 5) final STEPS, chi2 cur, chi2 best, PRECYC, lambda; may be null
   int nodes_ref[8];            // node count per reference parameter
   int row_of[LM_MAXNP];        // model row of each node's parameter
   int par_of[LM_MAXNP];        // reference parameter (1-based) of each node
@@ -77,7 +79,57 @@ struct LMQueue {
   int done;          // finished pixels
   int active;        // occupied slots (k_lm_scan)
   int rf_count;      // slots in the RF pass of this iteration (k_lm_rflist)
+  unsigned long long steps_sum;   // sum over the call's pixels of STEPS (global stop rule; two's complement)
 };
+
+// UPDATE_LAMBDA (src/get_dmodel.f90:917-956) with FACTOR = 0.01: an
+// improvement moves the best chi2 to chicur and divides lambda by sqrt(10),
+// lowering STEPS by one when it gains more than 1 % (else raising it); no
+// improvement multiplies lambda by 3 right after a cycle start (PRECYC ~ 1,
+// which it clears) or else by 10, and raises STEPS; lambda >= 1e-2.
+__device__ __forceinline__ void lm_update_lambda(double chicur, double& chipre, double& lam, double& steps,
+                                                 double& precyc) {
+  const double gain = chipre - chicur;
+  if (gain > 0) {
+    steps = (gain > 0.01 * chipre) ? fmax(0.0, steps - 1.0) : steps + 1.0;
+    chipre = chicur;
+    lam = lam / sqrt(10.0);
+  } else {
+    if (fabs(precyc - 1.0) < 1.0e-2) {
+      precyc = 0.0;
+      lam = lam * 3.0;
+    } else {
+      lam = lam * 10.0;
+    }
+    steps = steps + 1.0;
+  }
+  lam = fmax(1.0e-2, lam);
+}
+
+// Batched UPDATE_LAMBDA on arrays (one thread per pixel).
+__global__ void k_lm_lambda(int n, const double* __restrict__ chicur, double* __restrict__ chipre,
+                            double* __restrict__ lam, double* __restrict__ steps, double* __restrict__ precyc) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double cp = chipre[i], l = lam[i], st = steps[i], pc = precyc[i];
+  lm_update_lambda(chicur[i], cp, l, st, pc);
+  chipre[i] = cp;
+  lam[i] = l;
+  steps[i] = st;
+  precyc[i] = pc;
+}
+
+// Final LM state of pixel p: INV_SLA(1:4) and INV_SLA(9) (STEPS, chi2 of the
+// last model, best chi2, PRECYC, lambda; src/invert3d.f90:275-286).
+__device__ __forceinline__ void lm_state_out(const LMConf& C, const double* st, int p) {
+  if (!C.state_out) return;
+  double* o = C.state_out + 5 * (size_t)p;
+  o[0] = st[3];
+  o[1] = st[0];
+  o[2] = st[1];
+  o[3] = st[4];
+  o[4] = st[2];
+}
 
 // PARAM_NORMS (src/get_dmodel.f90:31), LOWLIM/UPPLIM (:1885-1901)
 __constant__ double c_lm_norm[8] = {6000.0, 1.0e5, 1.0e-5, 1.0e3, 1.0e3, 1.0e3, 1.0e6, 6.0e2};
@@ -201,24 +253,11 @@ __global__ void __launch_bounds__(256) k_lm_accept(LMConf C, LMSlots Sl, LMQueue
     const double chibest = st[1];
     const int ok = Sl.status[s] == 0 && chi == chi;
     acc = ok && chi < chibest;
-    // UPDATE_LAMBDA (src/get_dmodel.f90:917-956), FACTOR = 0.01
     double lam = st[2], steps = st[3], precyc = st[4], chipre = chibest;
     const double cc = ok ? chi : 1.0e300;
-    const double gain = chipre - cc;
-    if (gain > 0) {
-      steps = (gain > 0.01 * chipre) ? fmax(0.0, steps - 1.0) : steps + 1.0;
-      chipre = cc;
-      lam = lam / sqrt(10.0);
-    } else {
-      if (fabs(precyc - 1.0) < 1.0e-2) {
-        precyc = 0.0;
-        lam = lam * 3.0;
-      } else {
-        lam = lam * 10.0;
-      }
-      steps = steps + 1.0;
-    }
-    lam = fmax(1.0e-2, lam);
+    lm_update_lambda(cc, chipre, lam, steps, precyc);
+    if (C.global_stop)
+      atomicAdd(&q->steps_sum, (unsigned long long)((long long)steps - (long long)st[3]));
     const int it = Sl.iter[s] + 1;
     Sl.iter[s] = it;
     // stop rule: steps > MAXSTEPS (GET_DMODEL3DS, src/get_dmodel.f90:1476),
@@ -272,6 +311,7 @@ __global__ void __launch_bounds__(256) k_lm_accept(LMConf C, LMSlots Sl, LMQueue
     float* mc = Sl.mcur + (size_t)s * nm;
     for (int i = threadIdx.x; i < nm; i += blockDim.x) mc[i] = C.fb_model[i];
     if (threadIdx.x == 0) {
+      if (C.global_stop) atomicAdd(&q->steps_sum, (unsigned long long)(-(long long)st[3]));
       st[0] = 1.0e29;
       st[1] = 1.0e29;
       st[2] = 10.0;
@@ -293,6 +333,7 @@ __global__ void __launch_bounds__(256) k_lm_accept(LMConf C, LMSlots Sl, LMQueue
       out_chi[p] = st[1];
       out_iter[p] = Sl.iter[s] + (Sl.restarted[s] > 0 ? Sl.restarted[s] - 1 : 0);
       if (out_status) out_status[p] = st[1] < 1.0e29 ? 0 : FZ_NAN;
+      lm_state_out(C, st, p);
       atomicAdd(&q->done, 1);
       np_next = atomicAdd(&q->next, 1);
       Sl.skip[s] = LM_SKIP;
@@ -553,7 +594,7 @@ __global__ void __launch_bounds__(128) k_lm_solve(LMConf C, LMSlots Sl) {
 __global__ void __launch_bounds__(128) k_lm_update(LMConf C, LMSlots Sl, const double* __restrict__ coef) {
   extern __shared__ double sm_upd[];
   const int s = blockIdx.x;
-  if (Sl.pix[s] < 0 || Sl.skip[s]) return;
+  if (Sl.pix && (Sl.pix[s] < 0 || Sl.skip[s])) return;   // no occupancy arrays: every row is a pixel
   const int nz = C.nz, np = C.np;
   double* nzp = sm_upd;             // nz
   double* avg = nzp + nz;           // np
@@ -759,6 +800,31 @@ __global__ void __launch_bounds__(256) k_lm_errors(LMConf C, int n, const double
     for (int k = threadIdx.x; k < nz; k += blockDim.x) out[row * nz + k] = pert[k];
     __syncthreads();
     j0 += nj;
+  }
+}
+
+// One CTA per slot: the field-wide stop of MAKE_DECISION (src/invert3d.f90:
+// 843-846) ends every pixel still in flight; each writes its best model out
+// as a finished pixel does (END_CYCLE).
+__global__ void __launch_bounds__(256) k_lm_finish_all(LMConf C, LMSlots Sl, LMQueue* q, float* __restrict__ out_model,
+                                                       double* __restrict__ out_chi, int* __restrict__ out_iter,
+                                                       double* __restrict__ out_syn, int* __restrict__ out_status) {
+  const int s = blockIdx.x;
+  const int p = Sl.pix[s];
+  if (p < 0) return;
+  const int nf = C.nfreq, nm = 13 * C.nz;
+  const double* st = Sl.st + 5 * (size_t)s;
+  const float* mb = Sl.mbest + (size_t)s * nm;
+  for (int i = threadIdx.x; i < nm; i += blockDim.x) out_model[(size_t)p * nm + i] = mb[i];
+  if (out_syn)
+    for (int i = threadIdx.x; i < nf; i += blockDim.x) out_syn[(size_t)p * nf + i] = Sl.synb[(size_t)s * nf + i];
+  if (threadIdx.x == 0) {
+    out_chi[p] = st[1];
+    out_iter[p] = Sl.iter[s] + (Sl.restarted[s] > 0 ? Sl.restarted[s] - 1 : 0);
+    if (out_status) out_status[p] = st[1] < 1.0e29 ? 0 : FZ_NAN;
+    lm_state_out(C, st, p);
+    atomicAdd(&q->done, 1);
+    Sl.pix[s] = LM_PAD;
   }
 }
 

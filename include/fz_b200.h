@@ -256,7 +256,17 @@ int fz_smooth_device(fz_ctx* ctx, int nx, int ny, float* d_models, const int* pa
  * perturbations, 2 = STiC-like (the expanded node values are the new
  * profile; src/get_dmodel.f90:1792-1804).
  * assist: SET_TAU's initial-guess assists for fz_invert_cycles_device
- * (FZ_ASSIST_* bits; the control file's ASSIST line and PROGRESSIVE). */
+ * (FZ_ASSIST_* bits; the control file's ASSIST line and PROGRESSIVE).
+ * global_stop: MAKE_DECISION's field-wide rule (src/invert3d.f90:843-846):
+ * every pixel of the call stops once the mean of STEPS over its npix pixels
+ * reaches max(1, maxsteps - cycles_left), cycles_left being MAXITER - CURIC
+ * (0 in the last or only cycle; fz_invert_cycles_device sets it per cycle).
+ * The rule is defined for a field iterating in lockstep, so with it on all
+ * pixels are in flight at once (slots = npix).  state_out: (5, npix) REAL*8,
+ * the final INV_SLA(1:4) and INV_SLA(9) of each pixel -- STEPS, chi2 of its
+ * last model, best chi2, PRECYC, lambda (src/invert3d.f90:275-286) --; a
+ * device pointer for fz_invert_device, a host pointer for fz_invert; NULL:
+ * not written. */
 #define FZ_ASSIST_TEMP 1
 #define FZ_ASSIST_PGAS 2
 #define FZ_ASSIST_BVEC 4
@@ -271,7 +281,9 @@ typedef struct {
   const float* fallback_model;
   int reg_type[8];
   double reg_alpha[8];
-  int fallback_steps, solver, node_expansion, pad2;
+  int fallback_steps, solver, node_expansion, global_stop;
+  int cycles_left, pad3;
+  double* state_out;
 } fz_lm_opts;
 
 /* Batched pixel-wise Levenberg-Marquardt inversion of npix pixels with the
@@ -375,17 +387,54 @@ int fz_errors_device(fz_ctx* ctx, int npix, const double* d_obs, const float* d_
 int fz_errors(fz_ctx* ctx, int npix, const double* obs, const float* models, int hydrostatic, const fz_lm_opts* opts,
               float* err, double* chi2, int* status);
 
-/* Batched GET_PERTURBATION (src/lm.f90:137-204, SOLVER_METHOD = 1) on host
- * buffers: for each pixel H = J^T J (tensor cores, split-bf16 x3, FP32
- * accumulation), g = J^T diff, (H + lambda diag H)^+ g by an FP64 Jacobi SVD
- * with singular values below svdtol * max dropped.  jac is the normalised
- * JACOB as REAL*4, (nfreq, np, npix); diff (nfreq, npix); lambda (npix);
+/* Batched GET_PERTURBATION (src/lm.f90:137-204) on host buffers, the call
+ * at src/get_dmodel.f90:799-803: for each pixel H = J^T J (tensor cores,
+ * split-bf16 x3 of the FP32-rounded Jacobian, FP32 accumulation), g = J^T
+ * diff, then with dtype 1 (0 taken as 1) (H + lambda diag H)^+ g by an FP64
+ * Jacobi SVD with singular values below svdtol * max dropped (GET_INVERSE,
+ * :61-133; svdtol <= 0: RSVDTOL 1e-4), with dtype 2 the conjugate-gradient
+ * solve (NEW_CALCULATE_DELTA_UBICGSTAB, :375-453).  jac is IJACOBIAN(NF,NP)
+ * REAL*8 per pixel, (nfreq, np, npix); diff (nfreq, npix); lambda (npix);
  * reg_pen (np, npix) and reg_hss (np, np, npix), may be NULL: REG_PEN is
- * subtracted from J^T diff and REG_HSS added to J^T J as the reference
- * does (:169-174); delta (np, npix).  np <= 16, nfreq a multiple of 4. */
-int fz_lm_perturbation(fz_ctx* ctx, int npix, int np, int nfreq, const float* jac, const double* diff,
+ * subtracted from J^T diff and REG_HSS added to J^T J as the reference does
+ * (:169-174); delta (np, npix), NaN entries zeroed (NEW_SOLVE_PERTURBATION).
+ * np <= 16, nfreq a multiple of 4. */
+int fz_lm_perturbation(fz_ctx* ctx, int npix, int np, int nfreq, const double* jac, const double* diff,
                        const double* lambda, const double* reg_pen, const double* reg_hss, int dtype, double svdtol,
                        double* delta);
+/* The same with the Jacobian as REAL*4 (nfreq, np, npix), e.g. the
+ * normalised EQVDSYN the library itself produces (no counterpart routine:
+ * the reference widens EQVDSYN to REAL*8 before GET_PERTURBATION). */
+int fz_lm_perturbation_f32(fz_ctx* ctx, int npix, int np, int nfreq, const float* jac, const double* diff,
+                           const double* lambda, const double* reg_pen, const double* reg_hss, int dtype,
+                           double svdtol, double* delta);
+
+/* Batched UPDATE_LAMBDA (src/get_dmodel.f90:917-956, FACTOR = 0.01) of n
+ * pixels, the per-iteration lambda rule of GET_PERT_1D: chicur is the chi2
+ * of the model just synthesised (1e300 for a failed synthesis); chipre
+ * (best chi2), lambda, steps (STEPS) and precyc (PRECYC) are updated in
+ * place -- an improvement sets chipre = chicur and divides lambda by
+ * sqrt(10), lowering steps by one when it gains more than 1 % of chipre and
+ * raising it otherwise; no improvement multiplies lambda by 3 when precyc is
+ * 1 (which it clears) or else by 10, and raises steps; lambda >= 1e-2.  The
+ * batched inversion applies the same rule in its accept step.  Host arrays,
+ * or device arrays with the _device variant (enqueued on stream). */
+int fz_lm_update_lambda(int n, const double* chicur, double* chipre, double* lambda, double* steps, double* precyc);
+int fz_lm_update_lambda_device(int n, const double* d_chicur, double* d_chipre, double* d_lambda, double* d_steps,
+                               double* d_precyc, void* stream);
+
+/* Batched LIMIT_PERTURBATION -> REARANGE_DA_MODEL (src/get_dmodel.f90:
+ * 884-907, :1843-2016) with SORT_DELTA_TO_ATMOSPHERE (:1715-1836): the node
+ * perturbation delta (np, npix), normalised by PARAM_NORMS, applied to
+ * MODEL(NZ,13,npix) in place with the node layout of fz_rf_nodes -- node
+ * deltas clipped at 0.15 max(|node average|, PARAM_NORM), node_expansion 1
+ * (or 0; SIR-like: CONTRACT(EXPAND(avg + delta) - profile) expanded again)
+ * or 2 (STiC-like: the expanded clipped node values are the new profile),
+ * LOWLIM/UPPLIM, and the log tau5 taper of T (:1975-1989).  The batched
+ * inversion applies the same update to every trial model. */
+int fz_lm_rearange(fz_ctx* ctx, int npix, float* models, const double* delta, int node_expansion);
+int fz_lm_rearange_device(fz_ctx* ctx, int npix, float* d_models, const double* d_delta, int node_expansion,
+                          void* stream);
 
 /* Warm-start network (no counterpart in the reference): an MLP of nlayers
  * fully connected layers dims[0] -> dims[1] -> ... -> dims[nlayers] with GELU

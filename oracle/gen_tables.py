@@ -2,7 +2,7 @@
 """Generate the physical data tables shared by the CUDA library and the oracle.
 
 TEST INFRASTRUCTURE / BUILD RECIPE.  This script reads the FIRTEZ-dz Fortran
-sources (default location ``/root/reference/src``) and writes
+sources (the reference's ``src`` directory, ``--ref``, required) and writes
 
   * ``firtez-dz_b200/csrc/fz_tables.h``   -- data tables in this project's own
     layout (per-element atomic constants, partition-function pieces, ABO
@@ -40,8 +40,6 @@ import re
 import sys
 
 import numpy as np
-
-REF_DEFAULT = "/root/reference/src"
 
 # ----------------------------------------------------------------------------
 # Fortran-typed scalar
@@ -577,7 +575,7 @@ def eval_pieces(vp, dp, T):
 # ----------------------------------------------------------------------------
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", default=REF_DEFAULT)
+    ap.add_argument("--ref", required=True, help="the reference's src directory")
     ap.add_argument("--out-header", default=None)
     ap.add_argument("--out-golden", default=None)
     a = ap.parse_args()

@@ -312,14 +312,18 @@ def lm_step(st, obs, syn, jac, w, nodes):
 
 
 def invert(forward_rf, obs, init, nodes, w, maxsteps=5, maxit=40, dchi2=0.0, reg=None, solver=1,
-           node_expansion=1):
+           node_expansion=1, record=None):
     """Pixel-wise inversion with the stop rules of the batched GPU inversion
     (steps > maxsteps, maxit iterations, or an accepted step gaining less than
     dchi2 relative).  forward_rf(models (n,13,nz)) -> (syn (n,nfreq),
     jac (n,nfreq,np), models_out, status); obs (npix, nfreq); reg =
     (pen_typ, pen_alp) per reference parameter adds the vertical
-    regularisation of GET_IT_PENALTIES.  Returns (best models, chi2,
-    iterations)."""
+    regularisation of GET_IT_PENALTIES.  record: a list that receives, per
+    iteration k (record[k-1], a dict by pixel), each pixel's state right after
+    that iteration's accept step -- (STEPS, chi2 of the model just
+    synthesised, best chi2, PRECYC, lambda, best model, accepted) -- which is
+    the final state of the same inversion stopped at maxit = k.  Returns (best
+    models, chi2, iterations)."""
     if reg is not None:
         reg = (nodes,) + tuple(reg)
     npix = obs.shape[0]
@@ -335,6 +339,10 @@ def invert(forward_rf, obs, init, nodes, w, maxsteps=5, maxit=40, dchi2=0.0, reg
             st.cur = mo[a].copy()
             _, acc, prev = lm_accept(st, obs[i], syn[a], jac[a], w, ok=status[a] == 0, reg=reg)
             iters[i] += 1
+            if record is not None:
+                while len(record) < iters[i]:
+                    record.append({})
+                record[iters[i] - 1][i] = (st.steps, st.chicur, st.chibest, st.precyc, st.lam, st.best.copy(), acc)
             small = acc and prev < 1.0e29 and (prev - st.chibest) < dchi2 * prev
             if st.steps > maxsteps or iters[i] >= maxit or small:
                 continue

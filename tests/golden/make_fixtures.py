@@ -2,7 +2,7 @@
 """Copy the reference's data fixtures into tests/golden/ and extract the
 alternative abundance set they were generated with.
 
-TEST INFRASTRUCTURE.  Reads the reference tree (default /root/reference):
+TEST INFRASTRUCTURE.  Reads the reference tree given as the one argument:
 
   default/test_atmos.bin, default/rf_test_atmos.bin  -- v3 model files (1x1x256)
   default/lines_database.dat                         -- line database
@@ -18,7 +18,9 @@ import sys
 
 import numpy as np
 
-ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+if len(sys.argv) != 2:
+    sys.exit("usage: make_fixtures.py <path of the reference tree>")
+ref = sys.argv[1]
 here = os.path.dirname(os.path.abspath(__file__))
 for f in ("test_atmos.bin", "rf_test_atmos.bin", "lines_database.dat"):
     shutil.copyfile(os.path.join(ref, "default", f), os.path.join(here, f))

@@ -2,7 +2,7 @@
 """Golden v3 files written and read by the reference's own Python module.
 
 TEST INFRASTRUCTURE.  Imports python/firtez_dz.py from the reference tree
-(default /root/reference) with two shims that touch nothing of its file
+(its path the one argument) with two shims that touch nothing of its file
 code: a do-nothing matplotlib (the module sets up plotting at import; the
 package is not installed here) and np.int = int (removed in numpy 2; the
 writers use it for the record size).  Writes, next to this script:
@@ -28,7 +28,9 @@ import types
 import numpy as np
 
 here = os.path.dirname(os.path.abspath(__file__))
-ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+if len(sys.argv) != 2:
+    sys.exit("usage: make_v3_golden.py <path of the reference tree>")
+ref = sys.argv[1]
 sys.path.insert(0, os.path.join(os.path.dirname(os.path.dirname(here)), "oracle"))
 import v3_oracle  # noqa: E402
 

@@ -91,6 +91,26 @@ def parse_lines(text):
     return out[:n].copy()
 
 
+def regions(section, lines):
+    """REGION_DTYPE rows of a LINES: section (src/input_file.f90:290-366):
+    ``ids numwave wave_ini dlambda`` per row, ids comma-separated database
+    numbers of the main line and its blends; BLENDSDIFF = 1e3 (lambda_blend -
+    lambda_main) mA (:346-354)."""
+    pos = {int(n): i for i, n in enumerate(lines["num"])}
+    rows = [r.split() for r in section.strip().splitlines() if r.strip() and not r.strip().startswith("#")]
+    out = np.zeros(len(rows), dtype=REGION_DTYPE)
+    for k, f in enumerate(rows):
+        ids = [int(x) for x in f[0].split(",") if x]
+        if not ids or len(ids) > MAXBLEND or any(i not in pos for i in ids):
+            raise ValueError("LINES row %r" % " ".join(f))
+        out["nblend"][k] = len(ids)
+        for b, i in enumerate(ids):
+            out["line"][k, b] = pos[i]
+            out["wdif"][k, b] = 1.0e3 * (lines["l0"][pos[i]] - lines["l0"][pos[ids[0]]]) if b else 0.0
+        out["numwave"][k], out["wave_ini"][k], out["dlambda"][k] = int(f[1]), float(f[2]), float(f[3])
+    return out
+
+
 def zeeman(line):
     ln = np.ascontiguousarray(np.array(line, dtype=LINE_DTYPE).reshape(1))
     sh, st, ty = np.zeros(64), np.zeros(64), np.zeros(64, dtype=np.int32)

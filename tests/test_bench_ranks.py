@@ -68,3 +68,23 @@ def test_reference_arm_other_ranks_exit_without_work():
                         "--steps", "1", "--warmup", "0"], env=env, capture_output=True, text=True, timeout=280)
     assert p.returncode == 0, p.stderr[-2000:]
     assert p.stdout.strip() == ""
+
+
+@pytest.mark.timeout(300)
+def test_reference_arm_loads_nothing_of_the_product():
+    """The reference arm times the oracle alone: after a (small) run of it the
+    process has mapped oracle/liborc.so and never the product's
+    libfzb200.so, and the package module was never imported."""
+    code = ("import sys, json, types; sys.path.insert(0, %r); import importlib.util as u; "
+            "s = u.spec_from_file_location('fz_bench', %r); b = u.module_from_spec(s); s.loader.exec_module(b); "
+            "a = types.SimpleNamespace(cpu_pixels=2, warmup=0, steps=1, nz=32, gpus=1); "
+            "b.reference_arm(a, {}, True); maps = open('/proc/self/maps').read(); "
+            "print(json.dumps({'orc': 'liborc.so' in maps, 'fz': 'libfzb200' in maps, "
+            "'pkg': 'firtez_dz_b200' in sys.modules}))") % (ROOT, os.path.join(ROOT, "bench.py"))
+    p = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, timeout=280)
+    assert p.returncode == 0, p.stderr[-2000:]
+    lines = p.stdout.strip().splitlines()
+    line = json.loads(lines[0])
+    assert line["impl"] == "reference" and line["cpu_baseline"]["kind"] == "port"
+    got = json.loads(lines[-1])
+    assert got == {"orc": True, "fz": False, "pkg": False}

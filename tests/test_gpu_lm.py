@@ -32,10 +32,14 @@ def _ctx(fz, orc, nz):
 
 
 def test_lm_perturbation_matches_oracle(fz, orc):
+    """GET_PERTURBATION's own argument types: IJACOBIAN(NF,NP) REAL*8 in
+    (fz_lm_perturbation), against the oracle's FP64 + DGESVD on the same
+    REAL*8 Jacobian; and the REAL*4 variant (fz_lm_perturbation_f32) on the
+    FP32-rounded Jacobian."""
     _, _, _, ctx = _ctx(fz, orc, 32)
     rng = np.random.default_rng(5)
     npix, npar, nf = 24, 13, 896
-    jac = np.zeros((npix, npar, nf), dtype=np.float32)
+    jac = np.zeros((npix, npar, nf), dtype=np.float64)
     diff = rng.standard_normal((npix, nf))
     lam = 10.0 ** rng.uniform(-2, 1, npix)
     for i in range(npix):
@@ -44,12 +48,15 @@ def test_lm_perturbation_matches_oracle(fz, orc):
         # singular values of J: kept directions down to 3e-2 (H: 1e-3),
         # dropped ones at 3e-3 (H: 1e-5): a 10x gap around the cut in H
         s = np.concatenate([np.logspace(0, -1.5, npar - 3), np.full(3, 3e-3)]) * 50.0
-        jac[i] = ((u * s) @ v.T).T.astype(np.float32)
-    d = ctx.lm_perturbation(jac, diff, lam)
+        jac[i] = ((u * s) @ v.T).T
+    d64 = ctx.lm_perturbation(jac, diff, lam)
+    j32 = jac.astype(np.float32)
+    d32 = ctx.lm_perturbation(j32, diff, lam)
     for i in range(npix):
-        ref = lmo.get_perturbation(jac[i].T.astype(np.float64), diff[i], lam[i])
-        assert np.linalg.norm(d[i] - ref) <= 1e-3 * np.linalg.norm(ref), i
-
+        ref = lmo.get_perturbation(jac[i].T, diff[i], lam[i])
+        assert np.linalg.norm(d64[i] - ref) <= 1e-3 * np.linalg.norm(ref), i
+        ref32 = lmo.get_perturbation(j32[i].T.astype(np.float64), diff[i], lam[i])
+        assert np.linalg.norm(d32[i] - ref32) <= 1e-3 * np.linalg.norm(ref32), i
 
 
 def test_lm_perturbation_conjugate_gradients(fz, orc):

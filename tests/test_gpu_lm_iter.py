@@ -1,0 +1,145 @@
+"""The batched LM inversion pinned per iteration against the FP64 oracle.
+
+LM is deterministic: from the same initial models and observations, the
+GPU's first iterations must reproduce the oracle's pixel by pixel, not only
+its outcome.  At the benchmark's shape (NZ 128, two Fe I lines x 112
+wavelengths = NUMW 224, NFREQ 896, nodes T 5, Bx/By/Bz/v_z 2 each = NP 13)
+the inversion is run with maxit = 1, 2 and 3 -- its result is then the state
+after that many accept steps -- and compared with the oracle's inversion
+stopped at the same iteration (GET_PERT_1D, NEW_CALCULATE_CHI2,
+UPDATE_LAMBDA, NORMALIZE_JACOB, GET_PERTURBATION, REARANGE_DA_MODEL;
+src/get_dmodel.f90:725-1244, :1715-2016; src/lm.f90:30-204):
+
+* chi2 of the last model and the best chi2: 1e-4 relative (FP32 synthesis
+  against FP64);
+* the accept decision, lambda, STEPS and PRECYC: exactly;
+* the node values of the free parameters of the best model (CONTRACT_VECTOR
+  of T, Bx, By, Bz, v_z): within 1e-4 of PARAM_NORM (the tensor-core normal
+  equations and the FP32 Jacobian move delta by ~1e-4 relative).
+
+Besides, each branch of UPDATE_LAMBDA and each clip of REARANGE_DA_MODEL
+runs through the library's own batched entry points on crafted inputs and
+matches the oracle.
+"""
+import os
+import sys
+
+import numpy as np
+import pytest
+
+sys.path.insert(0, os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "oracle"))
+import lm_oracle as lmo  # noqa: E402
+import lmcase  # noqa: E402
+
+pytestmark = pytest.mark.gpu
+
+NZ, NPIX = 128, 64
+NORMS = {1: 6000.0, 4: 1.0e3, 5: 1.0e3, 6: 1.0e3, 7: 1.0e6}
+
+
+def _setup(fz, orc, nz=NZ, nlines=2):
+    lines = fz.lines_parse(fz.atmos.line_database_text())
+    reg = fz.regions_from_lines_section(fz.atmos.lines_section(nlines), lines)
+    g, _ = orc.gain(lines, reg)
+    return lines, reg, g, fz.Synthesis(lines, reg, nz=nz, gain=g)
+
+
+def _nodes(model):
+    """Node values of the free parameters (node order T, Bx, By, Bz, v_z)."""
+    out = []
+    for p, nj in lmcase.NODES.items():
+        c = lmo.int_coefs(model.shape[1], nj)
+        out.append(lmo.contract(model[lmo.ATMPOS[p]], c) / NORMS[p])
+    return np.concatenate(out)
+
+
+@pytest.mark.parametrize("he,start", [(True, "default"), (False, "perturbed")])
+def test_lm_iterations_match_oracle_at_benchmark_shape(fz, orc, he, start):
+    from firtez_dz_b200 import warmstart as ws
+    lines, reg, g, ctx = _setup(fz, orc)
+    numw = ctx.numw
+    true = fz.atmos.make_columns(NPIX, NZ, seed=4100 + int(he))
+    obs, _, _ = orc.forward(lines, reg, g, true, hydrostatic=he)
+    obs = obs.reshape(NPIX, -1) + np.random.default_rng(3).normal(0.0, 1e-3, (NPIX, 4 * numw))
+    init = ws.default_models(NPIX, NZ) if start == "default" else lmcase.initial_guess(true, seed=2)
+    w = lmo.weights(numw, isigma=1e-3)
+    rec = []
+    lmo.invert(lmcase.oracle_forward_rf(orc, lines, reg, g, he), obs, init, lmcase.NODES, w, maxsteps=5, maxit=3,
+               dchi2=0.0, record=rec)
+    ctx.rf_nodes(lmcase.NODES)
+    nacc = 0
+    for k in (1, 2, 3):
+        state = np.zeros((NPIX, 5))
+        opts = fz.LMOpts(maxsteps=5, maxit=k, dchi2=0.0, isigma=1e-3, slots=NPIX, state_out=state.ctypes.data)
+        mo, chi, it, st = ctx.invert(obs.reshape(NPIX, 4, numw), init, hydrostatic=he, opts=opts)
+        assert np.all(st == 0) and np.all(it == k), (k, st.max(), it.min(), it.max())
+        for i in range(NPIX):
+            steps, chicur, chibest, precyc, lam, best, acc = rec[k - 1][i]
+            where = (he, k, i)
+            assert abs(state[i, 2] - chibest) <= 1e-4 * chibest, where + (state[i, 2], chibest)
+            assert abs(chi[i] - chibest) <= 1e-4 * chibest, where
+            assert abs(state[i, 1] - chicur) <= 1e-4 * chicur, where + (state[i, 1], chicur)
+            gpu_acc = state[i, 1] == state[i, 2]
+            assert gpu_acc == acc, where
+            assert (state[i, 0], state[i, 3], state[i, 4]) == (steps, precyc, lam), where + (tuple(state[i]),)
+            dn = np.abs(_nodes(mo[i]) - _nodes(best))
+            assert dn.max() <= 1e-4, where + (float(dn.max()),)
+            nacc += acc
+    # the case exercises both decisions of the accept step
+    assert 0 < nacc < 3 * NPIX
+
+
+def test_update_lambda_branches_match_oracle(fz):
+    """Every branch of UPDATE_LAMBDA through fz_lm_update_lambda: gain above
+    1 % (STEPS down, floored at 0), gain below 1 % (STEPS up), no gain right
+    after a cycle start (lambda x 3, PRECYC cleared), no gain otherwise
+    (lambda x 10), the 1e-2 floor of lambda, a failed synthesis (1e300)."""
+    cases = [  # chicur, chipre, lambda, steps, precyc
+        (50.0, 100.0, 10.0, 2.0, 0.0), (50.0, 100.0, 10.0, 0.0, 0.0), (99.5, 100.0, 10.0, 1.0, 0.0),
+        (100.0, 100.0, 10.0, 1.0, 1.0), (101.0, 100.0, 10.0, 1.0, 1.005), (101.0, 100.0, 10.0, 3.0, 0.0),
+        (90.0, 100.0, 0.011, 0.0, 0.0), (1.0e300, 100.0, 1.0, 0.0, 0.0), (1.0e300, 1.0e29, 10.0, 0.0, 1.0),
+        (20.0, 1.0e29, 10.0, 0.0, 1.0), (100.0 - 1e-9, 100.0, 0.05, 4.0, 0.0), (1.0, 100.0, 1e-2, 0.0, 0.98)]
+    a = np.array(cases)
+    chipre, lam, steps, precyc = fz.lm_update_lambda(a[:, 0], a[:, 1], a[:, 2], a[:, 3], a[:, 4])
+    for i, (cc, cp, l0, s0, p0) in enumerate(cases):
+        ref = lmo.update_lambda(cc, cp, l0, s0, p0, 0.01)
+        assert (chipre[i], lam[i], steps[i], precyc[i]) == ref, (i, ref)
+
+
+@pytest.mark.parametrize("node_expansion", [1, 2])
+def test_rearange_clips_match_oracle(fz, orc, node_expansion):
+    """REARANGE_DA_MODEL through fz_lm_rearange on crafted node deltas: the
+    0.15 max(|avg|, PARAM_NORM) clip (above and below it), the LOWLIM and
+    UPPLIM limits of T, the field and v_z (a node average of 0 takes the
+    absolute limit), and the log tau5 taper of T (heights below -11.5 damped,
+    above 0.5 copied from the next height up)."""
+    nz = 40
+    _, _, _, ctx = _setup(fz, orc, nz=nz)
+    ctx.rf_nodes(lmcase.NODES)
+    rng = np.random.default_rng(11)
+    npix = 12
+    m = fz.atmos.make_columns(npix, nz, seed=9)
+    m[:, 11] = np.linspace(1.5, -13.0, nz)[None, :]            # log tau5 through both taper ranges
+    m[2, 0] = 2600.0                                            # T near LOWLIM 2500
+    m[3, 0] = 17900.0                                           # and near UPPLIM 1.8e4
+    m[4, 5:8] = 49000.0                                         # field near its limit 5e4
+    m[5, 10] = 0.0                                              # v_z node averages 0
+    delta = rng.normal(0.0, 0.05, (npix, 13))
+    delta[0] *= 40.0                                            # every node clipped
+    delta[1] *= 1e-3                                            # none clipped
+    delta[2, :5] = -0.14                                        # T pushed below LOWLIM
+    delta[3, :5] = 0.14                                         # and above UPPLIM
+    delta[4, 5:11] = 5.0                                        # field beyond 5e4 (clip, then limit)
+    delta[5, 11:] = 3.0                                         # v_z from 0: absolute clip
+    got = ctx.lm_rearange(m, delta, node_expansion=node_expansion)
+    for i in range(npix):
+        ref = m[i].copy()
+        lmo.rearange(ref, delta[i], lmcase.NODES, node_expansion)
+        for row in (0, 5, 6, 7, 10):
+            scale = np.maximum(np.abs(ref[row]), 1.0)
+            err = np.abs(got[i, row] - ref[row]) / scale
+            assert err.max() <= 1e-6, (node_expansion, i, row, float(err.max()))
+        assert np.array_equal(np.delete(got[i], (0, 5, 6, 7, 10), axis=0), np.delete(m[i], (0, 5, 6, 7, 10), axis=0))
+    # the crafted pixels reach the limits
+    assert got[2, 0].min() >= 2500.0 and np.isclose(got[2, 0].min(), 2500.0, rtol=1e-6)
+    assert got[3, 0].max() <= 1.8e4 + 1e-3

@@ -146,3 +146,28 @@ def test_cg_delta_and_node_expansion_two():
     avg = lmo.contract(ipar, coefs)
     want = (lmo.expand(avg + itd, coefs).astype(np.float32) - ipar).astype(np.float32)
     np.testing.assert_array_equal(pert2, want)
+
+
+def test_record_is_the_state_of_the_stopped_inversion(fz, orc):
+    """The per-iteration record of the oracle's inversion (what the GPU is
+    compared with, iteration by iteration) equals the final state of the
+    same inversion stopped at maxit = k."""
+    lines = fz.lines_parse(fz.atmos.line_database_text())
+    reg = fz.regions_from_lines_section(fz.atmos.lines_section(2, nw=24), lines)
+    g, _ = orc.gain(lines, reg)
+    nz, npix = 32, 4
+    true = fz.atmos.make_columns(npix, nz, seed=71)
+    obs, _, _ = orc.forward(lines, reg, g, true, hydrostatic=False)
+    obs = obs.reshape(npix, -1) + np.random.default_rng(1).normal(0.0, 1e-3, (npix, obs.shape[1] * obs.shape[2]))
+    init = lmcase.initial_guess(true, seed=1)
+    w = lmo.weights(obs.shape[1] // 4, isigma=1e-3)
+    f = lmcase.oracle_forward_rf(orc, lines, reg, g, False)
+    rec = []
+    lmo.invert(f, obs, init, lmcase.NODES, w, maxit=3, record=rec)
+    assert len(rec) == 3
+    for k in (1, 2, 3):
+        best, chi, it = lmo.invert(f, obs, init, lmcase.NODES, w, maxit=k)
+        assert np.all(it == k)
+        for i in range(npix):
+            assert rec[k - 1][i][2] == chi[i]
+            assert np.array_equal(rec[k - 1][i][5], best[i])

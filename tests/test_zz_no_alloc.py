@@ -17,6 +17,10 @@ pytestmark = pytest.mark.gpu
 
 
 def test_static_scratch_entry_point_matches_allocating_one(fz):
+    """Both entry points launch the same kernels with the same launch shapes
+    (the chemistry chain's lanes and warps come from the context in both) on
+    the same inputs, so they agree bit for bit: Pg given, hydrostatic from
+    the top, and hydrostatic from the log tau5 anchor (k_chain_med)."""
     import torch
     lines = fz.lines_parse(fz.atmos.line_database_text())
     reg = fz.regions_from_lines_section(fz.atmos.lines_section(2), lines)
@@ -24,8 +28,8 @@ def test_static_scratch_entry_point_matches_allocating_one(fz):
     ctx = fz.Synthesis(lines, reg, nz=nz)
     stream = torch.cuda.current_stream().cuda_stream
     for call, seed in enumerate((21, 22)):           # two calls in a row, different inputs
-        for he in (True, False):
-            m = torch.from_numpy(fz.atmos.make_columns(ncol, nz, seed=seed)).cuda()
+        for he in (0, 1, 2):                         # FZ_HE_NONE, FZ_HE_TOP, FZ_HE_LTAU
+            m = torch.from_numpy(fz.atmos.make_columns(ncol, nz, seed=seed + 10 * he)).cuda()
             syn_a = torch.zeros((ncol, 4, ctx.numw), dtype=torch.float64, device="cuda")
             syn_b = torch.full_like(syn_a, float("nan"))
             mo_a, mo_b = torch.empty_like(m), torch.empty_like(m)
@@ -37,12 +41,10 @@ def test_static_scratch_entry_point_matches_allocating_one(fz):
                                       stream=stream, hydrostatic=he)
             torch.cuda.synchronize()
             a, b = syn_a.cpu().numpy(), syn_b.cpu().numpy()
-            assert np.all(st_a.cpu().numpy() == 0) and np.all(st_b.cpu().numpy() == 0)
-            # same kernels on the same inputs: identical up to the tolerance of the parity tests
-            assert np.all(np.isfinite(b))
-            assert np.max(np.abs(a[:, 0] - b[:, 0]) / np.abs(a[:, 0])) < 1e-5
-            assert np.max(np.abs(a[:, 1:] - b[:, 1:])) < 1e-6
-            assert np.array_equal(mo_a.cpu().numpy(), mo_b.cpu().numpy())
+            assert np.all(st_a.cpu().numpy() == 0) and np.all(st_b.cpu().numpy() == 0), (call, he)
+            assert np.all(np.isfinite(b)), (call, he)
+            assert np.array_equal(a, b), (call, he, float(np.max(np.abs(a - b))))
+            assert np.array_equal(mo_a.cpu().numpy(), mo_b.cpu().numpy()), (call, he)
 
 
 def test_static_scratch_rejects_oversize_batches(fz):
