@@ -185,6 +185,8 @@ def lib():
         L.fz_lm_update_lambda.argtypes = [ctypes.c_int, P, P, P, P, P]
         L.fz_lm_rearange.argtypes = [P, ctypes.c_int, P, P, ctypes.c_int]
         L.fz_lm_rearange_device.argtypes = [P, ctypes.c_int, P, P, ctypes.c_int, P]
+        L.fz_rte_solve.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, P, P, P, P, P]
+        L.fz_voigt.argtypes = [ctypes.c_int, P, P, P, P]
         _lib = L
     return _lib
 
@@ -668,6 +670,30 @@ def lm_update_lambda(chicur, chipre, lam, steps, precyc):
     out = [np.array(a, dtype=np.float64, copy=True).reshape(cc.shape) for a in (chipre, lam, steps, precyc)]
     _check(lib().fz_lm_update_lambda(cc.size, _p(cc), *[_p(a) for a in out]))
     return tuple(out)
+
+
+def rte_solve(eta, src, zz, bnd=None):
+    """Formal solution on given absorption matrices (SET_BOUNDARY +
+    OLD_ANALYTICAL_SOLVER): eta (ncol, nz, 7, nw) ETAI..RHOV [cm^-1], src
+    (ncol, nz, nw), zz (nz,) km, bnd (ncol, nz) or None.  Returns SYN1D as
+    (ncol, nw, 4) float64."""
+    e = np.ascontiguousarray(eta, dtype=np.float32)
+    ncol, nz, _, nw = e.shape
+    s = np.ascontiguousarray(src, dtype=np.float32).reshape(ncol, nz, nw)
+    z = np.ascontiguousarray(zz, dtype=np.float64)
+    b = None if bnd is None else np.ascontiguousarray(bnd, dtype=np.int32).reshape(ncol, nz)
+    out = np.zeros((ncol, nw, 4))
+    _check(lib().fz_rte_solve(ncol, nz, nw, _p(e), _p(s), _p(z), None if b is None else _p(b), _p(out)))
+    return out
+
+
+def voigt(a, v):
+    """The library's FP32 H(a, v), F(a, v) on the GPU (a, v broadcast)."""
+    a, v = np.broadcast_arrays(np.asarray(a, dtype=np.float32), np.asarray(v, dtype=np.float32))
+    a, v = np.ascontiguousarray(a).ravel(), np.ascontiguousarray(v).ravel()
+    h, f = np.zeros_like(v), np.zeros_like(v)
+    _check(lib().fz_voigt(v.size, _p(a), _p(v), _p(h), _p(f)))
+    return h, f
 
 
 def measure_fp32_peak(device=0):

@@ -353,6 +353,20 @@ __global__ void __launch_bounds__(256) k_opac(const DevParams* __restrict__ Pg, 
 }
 
 // ----------------------------------------------------------------- k_synth
+// One height of OLD_ANALYTICAL_SOLVER (src/rtesolver.f90:163-187): I_k =
+// (1 - O) S e0 + O I_{k-1}, om0 = 1 - O(1,1).
+__device__ __forceinline__ void rte_step(const float O[16], float om0, float S, float& I0, float& I1, float& I2,
+                                         float& I3) {
+  const float n0 = fmaf(om0, S, fmaf(O[0], I0, fmaf(O[1], I1, fmaf(O[2], I2, O[3] * I3))));
+  const float n1 = fmaf(-O[4], S, fmaf(O[4], I0, fmaf(O[5], I1, fmaf(O[6], I2, O[7] * I3))));
+  const float n2 = fmaf(-O[8], S, fmaf(O[8], I0, fmaf(O[9], I1, fmaf(O[10], I2, O[11] * I3))));
+  const float n3 = fmaf(-O[12], S, fmaf(O[12], I0, fmaf(O[13], I1, fmaf(O[14], I2, O[15] * I3))));
+  I0 = n0;
+  I1 = n1;
+  I2 = n2;
+  I3 = n3;
+}
+
 __global__ void __launch_bounds__(MAXNUMW) k_synth(const DevParams* __restrict__ Pg, const LamP* __restrict__ lam,
                                                    const float* __restrict__ gain, int ncol,
                                                    const float* __restrict__ slab, double* __restrict__ syn,
@@ -447,15 +461,7 @@ __global__ void __launch_bounds__(MAXNUMW) k_synth(const DevParams* __restrict__
     } else {
       evol_f32(tI, tQ, tU, tV, rQ, rU, rV, O, om0);
     }
-    // I_k = (1 - O) S + O I_{k-1}, src/rtesolver.f90:163-187
-    const float n0 = fmaf(om0, S, fmaf(O[0], I0, fmaf(O[1], I1, fmaf(O[2], I2, O[3] * I3))));
-    const float n1 = fmaf(-O[4], S, fmaf(O[4], I0, fmaf(O[5], I1, fmaf(O[6], I2, O[7] * I3))));
-    const float n2 = fmaf(-O[8], S, fmaf(O[8], I0, fmaf(O[9], I1, fmaf(O[10], I2, O[11] * I3))));
-    const float n3 = fmaf(-O[12], S, fmaf(O[12], I0, fmaf(O[13], I1, fmaf(O[14], I2, O[15] * I3))));
-    I0 = n0;
-    I1 = n1;
-    I2 = n2;
-    I3 = n3;
+    rte_step(O, om0, S, I0, I1, I2, I3);
   }
   // CALCULATE_EQUIVALENT_SYN1D: x GAIN, Stokes-major
   const int nw = P.numw;
@@ -684,7 +690,10 @@ __device__ __forceinline__ void lmap(const Geo& g, const float h[3], const float
 // k_rf_prop then applies the products of the operators above each layer.
 // MAXT: the block-size bound, 256 (two blocks per SM) up to 256
 // wavelengths, 512 (one) up to 512; both hold 128 registers a thread.
-template <bool HE, bool FULL, int MAXT>
+// BLEND: regions with blended lines are present and every region runs the
+// general path below; without, only the single-line path is compiled in,
+// which keeps the general path's register demand out of the kernel.
+template <bool HE, bool FULL, int MAXT, bool BLEND>
 __global__ void __launch_bounds__(MAXT, (MAXT <= 256 ? 2 : 1)) k_synth_rf(const DevParams* __restrict__ Pg, const RFConf* __restrict__ Rg,
                                                   const LamP* __restrict__ lam, const float* __restrict__ gain,
                                                   int ncol, const float* __restrict__ slab,
@@ -770,6 +779,186 @@ __global__ void __launch_bounds__(MAXT, (MAXT <= 256 ? 2 : 1)) k_synth_rf(const 
     const Geo g{row[goff], row[goff + 1], row[goff + 2], row[goff + 3], row[goff + 4]};
     const float B = row[goff + 5];
     const float halfT = 0.5f / T;
+    if (!BLEND) {
+      // One line in every region (no blends): each parameter's optical-depth
+      // derivatives are formed from the line's per-type sums when its
+      // response is taken, in a runtime loop over the parameters -- one
+      // copy of the directional derivative and of the node update, and no
+      // 6 x 7 array held across the operator algebra.  The arithmetic is
+      // that of the general path below, expression for expression.
+      const float* qq = row + loff + 4 * lb;
+      const float kldz = qq[0], a = qq[1], idd = qq[2];
+      const float x0 = lp.wave + qq[3];
+      float hh[3] = {0, 0, 0}, ff[3] = {0, 0, 0}, av[3] = {0, 0, 0}, ca[3] = {0, 0, 0};
+      float avu[3] = {0, 0, 0}, cau[3] = {0, 0, 0}, avs[3] = {0, 0, 0}, cas[3] = {0, 0, 0};
+      {
+        int c = P.lu_c0[lb];
+#pragma unroll
+        for (int t = 0; t < 3; ++t) {
+          const int e = c + P.lu_nt[lb][t];
+          for (; c < e; ++c) {
+            const float shf = P.comp_shift[c], st = P.comp_str[c];
+            const float u = fmaf(shf, B, x0) * idd;
+            float h, f;
+            voigt_f32(a, u, h, f);
+            const float dhv = 2.0f * fmaf(a, f, -u * h);
+            const float dha = 2.0f * (fmaf(a, h, u * f) - 0.56418958354775628f);
+            hh[t] = fmaf(st, h, hh[t]);
+            ff[t] = fmaf(st, f, ff[t]);
+            const float sv = st * dhv, sa = st * dha;
+            av[t] += sv;
+            ca[t] += sa;
+            avu[t] = fmaf(sv, u, avu[t]);
+            cau[t] = fmaf(sa, u, cau[t]);
+            avs[t] = fmaf(sv, shf, avs[t]);
+            cas[t] = fmaf(sa, shf, cas[t]);
+          }
+        }
+      }
+      float tI = row[4 + r], tQ, tU, tV, rQ, rU, rV;
+      {
+        const float hs = hh[0] + hh[2], fs = ff[0] + ff[2];
+        const float hl = 0.5f * hh[1] - 0.25f * hs, fl = 0.5f * ff[1] - 0.25f * fs;
+        tI = fmaf(kldz, g.g1 * hs + g.g2 * hh[1], tI);
+        tQ = fmaf(kldz, g.g3 * hl, 0.f);
+        tU = fmaf(kldz, g.g4 * hl, 0.f);
+        tV = fmaf(kldz, g.g5 * (hh[0] - hh[2]), 0.f);
+        rQ = fmaf(kldz, g.g3 * fl, 0.f);
+        rU = fmaf(kldz, g.g4 * fl, 0.f);
+        rV = fmaf(kldz, g.g5 * (ff[0] - ff[2]), 0.f);
+      }
+      const float* dl = row + dloff + 4 * lb;
+      const float dkt = dl[0], dkp = dl[1], ddt = dl[2], ddp = dl[3];
+      float O[16], om0 = 0.0f;
+      EvolSt es;
+      const bool fin = isfinite(tI) && isfinite(tQ) && isfinite(tU) && isfinite(tV) && isfinite(rQ) &&
+                       isfinite(rU) && isfinite(rV);
+      if (!fin) {
+        bad = 1;
+#pragma unroll
+        for (int i = 0; i < 16; ++i) O[i] = (i % 5 == 0) ? 1.f : 0.f;
+      } else {
+        evol_state(tI, tQ, tU, tV, rQ, rU, rV, O, om0, es);
+      }
+      const float n0 = fmaf(om0, S, fmaf(O[0], I0, fmaf(O[1], I1, fmaf(O[2], I2, O[3] * I3))));
+      const float n1 = fmaf(-O[4], S, fmaf(O[4], I0, fmaf(O[5], I1, fmaf(O[6], I2, O[7] * I3))));
+      const float n2 = fmaf(-O[8], S, fmaf(O[8], I0, fmaf(O[9], I1, fmaf(O[10], I2, O[11] * I3))));
+      const float n3 = fmaf(-O[12], S, fmaf(O[12], I0, fmaf(O[13], I1, fmaf(O[14], I2, O[15] * I3))));
+      // the operator products with the incoming vector (T, Pg; every
+      // parameter without HE) -- with HE the B and v_z responses use the
+      // outgoing one, switched to at p = 2
+      EvolW v;
+      if (fin) {
+        const float win[4] = {I0 - S, I1, I2, I3};
+        evol_w(es, O, win, v);
+      }
+      const float dS = lp.c1 * (q / T) * ((em1 + 1.0f) / (em1 * em1));
+      float OH[4] = {0.f, 0.f, 0.f, 0.f}, ck = 0.f, pgk = 0.f;
+      bool prop = false;
+      if (HE) {
+        ck = row[heoff];
+        pgk = row[heoff + 1];
+        prop = O[0] > 1.0e-5f;
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+          OH[i] = prop ? O[4 * i] * H[0] + O[4 * i + 1] * H[1] + O[4 * i + 2] * H[2] + O[4 * i + 3] * H[3] : H[i];
+      }
+      const float* ckr = FULL ? nullptr : coef + k * np;
+#pragma unroll 1
+      for (int p = 0; p < NSLOT; ++p) {
+        float dt[7], tmp[7];
+        if (p == 0) {
+          // T at constant Pg: dKLIN, du/dT = -u/(2T), da/dT
+          float xe[3], xr[3];
+#pragma unroll
+          for (int t = 0; t < 3; ++t) {
+            xe[t] = fmaf(ca[t], ddt, -avu[t] * halfT);
+            xr[t] = fmaf(av[t], ddt, cau[t] * halfT);
+          }
+          lmap(g, xe, xr, tmp);
+          float base[7];
+          lmap(g, hh, ff, base);
+#pragma unroll
+          for (int x = 0; x < 7; ++x) dt[x] = fmaf(dkt, base[x], kldz * tmp[x]);
+          dt[0] = row[dkoff] + dt[0];
+        } else if (p == 1) {
+          // Pg at constant T: dKLIN and da/dPg
+          lmap(g, ca, av, tmp);
+          float base[7];
+          lmap(g, hh, ff, base);
+#pragma unroll
+          for (int x = 0; x < 7; ++x) dt[x] = fmaf(dkp, base[x], kldz * ddp * tmp[x]);
+          dt[0] = row[dkoff + 1] + dt[0];
+        } else if (p < 5) {
+          // B_i: geometry factors and the shift term du/dB
+          const float ncs[3] = {-cas[0], -cas[1], -cas[2]};
+          float sh7[7];
+          lmap(g, avs, ncs, sh7);
+          const float* dg = row + dgoff + 5 * (p - 2);
+          const Geo gd{dg[0], dg[1], dg[2], dg[3], dg[4]};
+          lmap(gd, hh, ff, tmp);
+          const float kb = idd * row[dboff + p - 2];
+#pragma unroll
+          for (int x = 0; x < 7; ++x) dt[x] = kldz * fmaf(kb, sh7[x], tmp[x]);
+        } else {
+          // v_z: du/dv = lu_duv / Doppler width
+          const float nca[3] = {-ca[0], -ca[1], -ca[2]};
+          lmap(g, av, nca, tmp);
+          const float kv = kldz * P.lu_duv[lb] * idd;
+#pragma unroll
+          for (int x = 0; x < 7; ++x) dt[x] = kv * tmp[x];
+        }
+        float rfp[4] = {0.f, 0.f, 0.f, 0.f};
+        if (fin) {
+          if (HE && p == 2) {
+            const float wout[4] = {n0 - S, n1, n2, n3};
+            evol_w(es, O, wout, v);
+          }
+          evol_dir(es, v, dt, rfp);
+        }
+        if (p == 0) {
+          // source-function term (1 - O) e0 dS/dT, then the HE global term
+          rfp[0] = fmaf(om0, dS, rfp[0]);
+          rfp[1] = fmaf(-O[4], dS, rfp[1]);
+          rfp[2] = fmaf(-O[8], dS, rfp[2]);
+          rfp[3] = fmaf(-O[12], dS, rfp[3]);
+          if (HE) {
+#pragma unroll
+            for (int i = 0; i < 4; ++i) rfp[i] = fmaf(ck, OH[i], rfp[i]);
+          }
+        }
+        if (HE && p == 1) {
+#pragma unroll
+          for (int i = 0; i < 4; ++i) H[i] = prop ? fmaf(rfp[i], pgk, OH[i]) : H[i];
+        }
+        if (FULL) {
+          const int nw = P.numw;
+#pragma unroll
+          for (int c = 0; c < 4; ++c) jcol[((size_t)p * nz + k) * fstride + c * nw + l] = rfp[c];
+        } else {
+          const int j0 = C.n0[p], j1 = j0 + C.nj[p];
+          for (int j = j0; j < j1; ++j) {
+            float* d = Dacc + (j * 4) * nthr + l;
+            const float d0 = d[0], d1 = d[nthr], d2 = d[2 * nthr], d3 = d[3 * nthr];
+            const float cj = ckr[j];
+            d[0] = fmaf(cj, rfp[0], fmaf(O[0], d0, fmaf(O[1], d1, fmaf(O[2], d2, O[3] * d3))));
+            d[nthr] = fmaf(cj, rfp[1], fmaf(O[4], d0, fmaf(O[5], d1, fmaf(O[6], d2, O[7] * d3))));
+            d[2 * nthr] = fmaf(cj, rfp[2], fmaf(O[8], d0, fmaf(O[9], d1, fmaf(O[10], d2, O[11] * d3))));
+            d[3 * nthr] = fmaf(cj, rfp[3], fmaf(O[12], d0, fmaf(O[13], d1, fmaf(O[14], d2, O[15] * d3))));
+          }
+        }
+      }
+      if (FULL) {
+        const int nw = P.numw;
+#pragma unroll
+        for (int i = 0; i < 16; ++i) ocol[((size_t)k * 16 + i) * nw + l] = O[i];
+      }
+      I0 = n0;
+      I1 = n1;
+      I2 = n2;
+      I3 = n3;
+      continue;
+    }
     float tI = row[4 + r], tQ = 0.f, tU = 0.f, tV = 0.f, rQ = 0.f, rU = 0.f, rV = 0.f;
     float dtau[NSLOT][7];
 #pragma unroll
@@ -1002,18 +1191,30 @@ __global__ void __launch_bounds__(MAXT, (MAXT <= 256 ? 2 : 1)) k_synth_rf(const 
 
 // k_synth_rf with the block-size bound its thread count needs
 template <bool HE, bool FULL, typename... A>
-void launch_synth_rf(int blocks, int threads, size_t sms, cudaStream_t s, A... a) {
-  if (threads <= 256)
-    k_synth_rf<HE, FULL, 256><<<blocks, threads, sms, s>>>(a...);
-  else
-    k_synth_rf<HE, FULL, 512><<<blocks, threads, sms, s>>>(a...);
+void launch_synth_rf(bool blend, int blocks, int threads, size_t sms, cudaStream_t s, A... a) {
+  if (threads <= 256) {
+    if (blend)
+      k_synth_rf<HE, FULL, 256, true><<<blocks, threads, sms, s>>>(a...);
+    else
+      k_synth_rf<HE, FULL, 256, false><<<blocks, threads, sms, s>>>(a...);
+  } else {
+    if (blend)
+      k_synth_rf<HE, FULL, 512, true><<<blocks, threads, sms, s>>>(a...);
+    else
+      k_synth_rf<HE, FULL, 512, false><<<blocks, threads, sms, s>>>(a...);
+  }
 }
 
 template <bool HE, bool FULL>
 cudaError_t set_synth_rf_attr(cudaFuncAttribute attr, int v) {
-  cudaError_t e = cudaFuncSetAttribute(k_synth_rf<HE, FULL, 256>, attr, v);
-  return e == cudaSuccess ? cudaFuncSetAttribute(k_synth_rf<HE, FULL, 512>, attr, v) : e;
+  cudaError_t e = cudaFuncSetAttribute(k_synth_rf<HE, FULL, 256, false>, attr, v);
+  if (e == cudaSuccess) e = cudaFuncSetAttribute(k_synth_rf<HE, FULL, 512, false>, attr, v);
+  if (e == cudaSuccess) e = cudaFuncSetAttribute(k_synth_rf<HE, FULL, 256, true>, attr, v);
+  return e == cudaSuccess ? cudaFuncSetAttribute(k_synth_rf<HE, FULL, 512, true>, attr, v) : e;
 }
+
+// true when some region of the context holds blended lines
+bool has_blends(const fz_ctx* c);
 
 // Response functions at emergence from the local ones (FULL mode of
 // k_synth_rf): RF(K) = O_NZ ... O_{K+1} RF_loc(K), OLD_DSYN_PROPAGATION
@@ -1501,6 +1702,12 @@ int ensure_scratch(fz_ctx* c, int ncol) {
 }
 
 // brackets one launch with events; `items` = columns (or slots) it processes
+bool has_blends(const fz_ctx* c) {
+  for (const fz_region& r : c->regs)
+    if (r.nblend > 1) return true;
+  return false;
+}
+
 struct ProfScope {
   fz_ctx* c;
   int kernel;
@@ -1698,11 +1905,11 @@ int launch_rf_stage(fz_ctx* c, int ncol, int hydrostatic, double* d_syn, float* 
   {
     ProfScope ps(c, 4, s, list ? 0 : ncol);
     if (hydrostatic)
-      launch_synth_rf<true, false>(ncol, threads, sms, s, c->d_params, c->d_rf, c->d_lam, c->d_gain, ncol,
+      launch_synth_rf<true, false>(has_blends(c), ncol, threads, sms, s, c->d_params, c->d_rf, c->d_lam, c->d_gain, ncol,
                                                          c->d_rfslab, c->d_coef, d_syn, d_jac, nullptr, d_mout,
                                                          d_status, list, nlist);
     else
-      launch_synth_rf<false, false>(ncol, threads, sms, s, c->d_params, c->d_rf, c->d_lam, c->d_gain, ncol,
+      launch_synth_rf<false, false>(has_blends(c), ncol, threads, sms, s, c->d_params, c->d_rf, c->d_lam, c->d_gain, ncol,
                                                           c->d_rfslab, c->d_coef, d_syn, d_jac, nullptr, d_mout,
                                                           d_status, list, nlist);
   }
@@ -1758,11 +1965,11 @@ int launch_forward_rf(fz_ctx* c, int ncol, const float* d_model, int hydrostatic
     {
       ProfScope ps(c, 4, s, ncol);
       if (hydrostatic)
-        launch_synth_rf<true, true>(ncol, threads, sms, s, c->d_params, c->d_rf, c->d_lam, c->d_gain, ncol,
+        launch_synth_rf<true, true>(has_blends(c), ncol, threads, sms, s, c->d_params, c->d_rf, c->d_lam, c->d_gain, ncol,
                                                           c->d_rfslab, nullptr, d_syn, d_jac, c->d_oscr, d_mout,
                                                           d_status, nullptr, nullptr);
       else
-        launch_synth_rf<false, true>(ncol, threads, sms, s, c->d_params, c->d_rf, c->d_lam, c->d_gain, ncol,
+        launch_synth_rf<false, true>(has_blends(c), ncol, threads, sms, s, c->d_params, c->d_rf, c->d_lam, c->d_gain, ncol,
                                                            c->d_rfslab, nullptr, d_syn, d_jac, c->d_oscr, d_mout,
                                                            d_status, nullptr, nullptr);
     }
@@ -1976,6 +2183,61 @@ bool int_coefs(int nz, int nj, std::vector<double>& coef) {
 __global__ void k_f64_to_f32(size_t n, const double* __restrict__ a, float* __restrict__ b) {
   for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
     b[i] = (float)a[i];
+}
+
+// The formal solution alone on given absorption matrices (SET_BOUNDARY +
+// OLD_ANALYTICAL_SOLVER): one thread per (column, wavelength), the height
+// recursion of the synthesis kernel with the layer optical depths
+// eta * dz (dz from the reference's rule: z_{k+1} - z_k, the top height's
+// backward difference).  eta (nw, 7, nz, ncol), src (nw, nz, ncol), bnd
+// (nz, ncol) or null, out (4, nw, ncol).
+__global__ void k_rte(int ncol, int nz, int nw, const float* __restrict__ eta, const float* __restrict__ src,
+                      const double* __restrict__ zz, const int* __restrict__ bnd, double* __restrict__ out) {
+  const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= (long long)ncol * nw) return;
+  const int col = (int)(idx / nw), l = (int)(idx % nw);
+  float I0 = 0.f, I1 = 0.f, I2 = 0.f, I3 = 0.f;
+  for (int k = 0; k < nz; ++k) {
+    const float S = src[((size_t)col * nz + k) * nw + l];
+    if (k == 0 || (bnd && bnd[(size_t)col * nz + k])) {
+      I0 = S;
+      I1 = I2 = I3 = 0.f;
+      continue;
+    }
+    const double dz = 1e5 * fabs(k == nz - 1 ? zz[k] - zz[k - 1] : zz[k + 1] - zz[k]);
+    const float* e = eta + ((size_t)col * nz + k) * 7 * nw + l;
+    float t[7];
+    bool fin = true;
+#pragma unroll
+    for (int i = 0; i < 7; ++i) {
+      t[i] = (float)((double)e[(size_t)i * nw] * dz);
+      fin = fin && isfinite(t[i]);
+    }
+    float O[16], om0 = 0.0f;
+    if (!fin) {
+#pragma unroll
+      for (int i = 0; i < 16; ++i) O[i] = (i % 5 == 0) ? 1.f : 0.f;
+    } else {
+      evol_f32(t[0], t[1], t[2], t[3], t[4], t[5], t[6], O, om0);
+    }
+    rte_step(O, om0, S, I0, I1, I2, I3);
+  }
+  double* o = out + ((size_t)col * nw + l) * 4;
+  o[0] = I0;
+  o[1] = I1;
+  o[2] = I2;
+  o[3] = I3;
+}
+
+// VOIGT on arrays: the FP32 Voigt/Faraday-Voigt pair of the synthesis kernels.
+__global__ void k_voigt(int n, const float* __restrict__ a, const float* __restrict__ v, float* __restrict__ h,
+                        float* __restrict__ f) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  float hh, ff;
+  voigt_f32(a[i], v[i], hh, ff);
+  h[i] = hh;
+  f[i] = ff;
 }
 
 __global__ void k_tau5(int ncol, int nz, int sw, const float* __restrict__ slab, float* __restrict__ mout) {
@@ -3516,6 +3778,58 @@ int fz_lm_rearange(fz_ctx* c, int npix, float* models, const double* delta, int 
   if (!rc) rc = cuda_fail(cudaMemcpy(models, dm, mb, cudaMemcpyDeviceToHost));
   cudaFree(dm);
   cudaFree(dd);
+  return rc;
+}
+
+int fz_rte_solve_device(int ncol, int nz, int nw, const float* d_eta, const float* d_src, const double* d_zz,
+                        const int* d_bnd, double* d_out, void* stream) {
+  if (ncol <= 0 || nz <= 1 || nw <= 0 || !d_eta || !d_src || !d_zz || !d_out) return FZ_ERR_ARG;
+  const long long n = (long long)ncol * nw;
+  k_rte<<<(unsigned)((n + 127) / 128), 128, 0, (cudaStream_t)stream>>>(ncol, nz, nw, d_eta, d_src, d_zz, d_bnd,
+                                                                          d_out);
+  return cuda_fail(cudaGetLastError());
+}
+
+int fz_rte_solve(int ncol, int nz, int nw, const float* eta, const float* src, const double* zz, const int* bnd,
+                 double* out) {
+  if (ncol <= 0 || nz <= 1 || nw <= 0 || !eta || !src || !zz || !out) return FZ_ERR_ARG;
+  const size_t ne = (size_t)ncol * nz * 7 * nw, ns = (size_t)ncol * nz * nw, no = (size_t)ncol * nw * 4;
+  float *de = nullptr, *ds = nullptr;
+  double *dz = nullptr, *dout = nullptr;
+  int* db = nullptr;
+  int rc = cuda_fail(cudaMalloc(&de, ne * sizeof(float)));
+  if (!rc) rc = cuda_fail(cudaMalloc(&ds, ns * sizeof(float)));
+  if (!rc) rc = cuda_fail(cudaMalloc(&dz, nz * sizeof(double)));
+  if (!rc) rc = cuda_fail(cudaMalloc(&dout, no * sizeof(double)));
+  if (!rc && bnd) rc = cuda_fail(cudaMalloc(&db, (size_t)ncol * nz * sizeof(int)));
+  if (!rc) rc = cuda_fail(cudaMemcpy(de, eta, ne * sizeof(float), cudaMemcpyHostToDevice));
+  if (!rc) rc = cuda_fail(cudaMemcpy(ds, src, ns * sizeof(float), cudaMemcpyHostToDevice));
+  if (!rc) rc = cuda_fail(cudaMemcpy(dz, zz, nz * sizeof(double), cudaMemcpyHostToDevice));
+  if (!rc && bnd) rc = cuda_fail(cudaMemcpy(db, bnd, (size_t)ncol * nz * sizeof(int), cudaMemcpyHostToDevice));
+  if (!rc) rc = fz_rte_solve_device(ncol, nz, nw, de, ds, dz, db, dout, nullptr);
+  if (!rc) rc = cuda_fail(cudaMemcpy(out, dout, no * sizeof(double), cudaMemcpyDeviceToHost));
+  cudaFree(de);
+  cudaFree(ds);
+  cudaFree(dz);
+  cudaFree(dout);
+  cudaFree(db);
+  return rc;
+}
+
+int fz_voigt(int n, const float* a, const float* v, float* h, float* f) {
+  if (n <= 0 || !a || !v || !h || !f) return FZ_ERR_ARG;
+  float* d = nullptr;
+  const size_t b = (size_t)n * sizeof(float);
+  FZ_CK(cudaMalloc(&d, 4 * b));
+  int rc = cuda_fail(cudaMemcpy(d, a, b, cudaMemcpyHostToDevice));
+  if (!rc) rc = cuda_fail(cudaMemcpy(d + n, v, b, cudaMemcpyHostToDevice));
+  if (!rc) {
+    k_voigt<<<(n + 255) / 256, 256>>>(n, d, d + n, d + 2 * (size_t)n, d + 3 * (size_t)n);
+    rc = cuda_fail(cudaGetLastError());
+  }
+  if (!rc) rc = cuda_fail(cudaMemcpy(h, d + 2 * (size_t)n, b, cudaMemcpyDeviceToHost));
+  if (!rc) rc = cuda_fail(cudaMemcpy(f, d + 3 * (size_t)n, b, cudaMemcpyDeviceToHost));
+  cudaFree(d);
   return rc;
 }
 

@@ -427,7 +427,7 @@ MODULE FZ_B200
       TYPE(C_PTR), VALUE         :: REG_HSS                ! PEN_HSS(NP,NP,NPIX) or C_NULL_PTR
       INTEGER(C_INT), VALUE      :: DTYPE
       REAL(C_DOUBLE), VALUE      :: SVDTOL
-      REAL(C_DOUBLE)             :: DELTA(*)
+      REAL(C_DOUBLE)             :: DELTA(*)               ! (NP,NPIX)
     END FUNCTION
     INTEGER(C_INT) FUNCTION FZ_LM_PERTURBATION_F32(CTX, NPIX, NP, NFREQ, JAC, DIFF, LAMBDA, &
         REG_PEN, REG_HSS, DTYPE, SVDTOL, DELTA) BIND(C, NAME='fz_lm_perturbation_f32')
@@ -443,13 +443,13 @@ MODULE FZ_B200
       TYPE(C_PTR), VALUE         :: REG_HSS                ! PEN_HSS(NP,NP,NPIX) or C_NULL_PTR
       INTEGER(C_INT), VALUE      :: DTYPE
       REAL(C_DOUBLE), VALUE      :: SVDTOL
-      REAL(C_DOUBLE)             :: DELTA(*)
+      REAL(C_DOUBLE)             :: DELTA(*)               ! (NP,NPIX)
     END FUNCTION
     INTEGER(C_INT) FUNCTION FZ_LM_UPDATE_LAMBDA(N, CHICUR, CHIPRE, LAMBDA, STEPS, PRECYC) &
         BIND(C, NAME='fz_lm_update_lambda')
       IMPORT
       INTEGER(C_INT), VALUE      :: N
-      REAL(C_DOUBLE)             :: CHICUR(*)
+      REAL(C_DOUBLE)             :: CHICUR(*)              ! chi2 of the new models
       REAL(C_DOUBLE)             :: CHIPRE(*)
       REAL(C_DOUBLE)             :: LAMBDA(*)
       REAL(C_DOUBLE)             :: STEPS(*)
@@ -472,7 +472,7 @@ MODULE FZ_B200
       TYPE(C_PTR), VALUE         :: CTX
       INTEGER(C_INT), VALUE      :: NPIX
       REAL(C_FLOAT)              :: MODELS(*)              ! MODEL(NZ,13,NPIX)
-      REAL(C_DOUBLE)             :: DELTA(*)
+      REAL(C_DOUBLE)             :: DELTA(*)               ! (NP,NPIX)
       INTEGER(C_INT), VALUE      :: NODE_EXPANSION
     END FUNCTION
     INTEGER(C_INT) FUNCTION FZ_LM_REARANGE_DEVICE(CTX, NPIX, D_MODELS, D_DELTA, NODE_EXPANSION, &
@@ -484,6 +484,39 @@ MODULE FZ_B200
       TYPE(C_PTR), VALUE         :: D_DELTA
       INTEGER(C_INT), VALUE      :: NODE_EXPANSION
       TYPE(C_PTR), VALUE         :: STREAM                 ! cudaStream_t or C_NULL_PTR
+    END FUNCTION
+    INTEGER(C_INT) FUNCTION FZ_RTE_SOLVE(NCOL, NZ, NW, ETA, SRC, ZZ, BND, OUT) BIND(C, &
+        NAME='fz_rte_solve')
+      IMPORT
+      INTEGER(C_INT), VALUE      :: NCOL
+      INTEGER(C_INT), VALUE      :: NZ
+      INTEGER(C_INT), VALUE      :: NW
+      REAL(C_FLOAT)              :: ETA(*)                 ! (NW,7,NZ,NCOL) ETAI..RHOV
+      REAL(C_FLOAT)              :: SRC(*)
+      REAL(C_DOUBLE)             :: ZZ(*)                  ! ZZ(NZ) km
+      TYPE(C_PTR), VALUE         :: BND                    ! (NZ,NCOL) boundary flags
+      REAL(C_DOUBLE)             :: OUT(*)
+    END FUNCTION
+    INTEGER(C_INT) FUNCTION FZ_RTE_SOLVE_DEVICE(NCOL, NZ, NW, D_ETA, D_SRC, D_ZZ, D_BND, D_OUT, &
+        STREAM) BIND(C, NAME='fz_rte_solve_device')
+      IMPORT
+      INTEGER(C_INT), VALUE      :: NCOL
+      INTEGER(C_INT), VALUE      :: NZ
+      INTEGER(C_INT), VALUE      :: NW
+      TYPE(C_PTR), VALUE         :: D_ETA
+      TYPE(C_PTR), VALUE         :: D_SRC
+      TYPE(C_PTR), VALUE         :: D_ZZ
+      TYPE(C_PTR), VALUE         :: D_BND
+      TYPE(C_PTR), VALUE         :: D_OUT
+      TYPE(C_PTR), VALUE         :: STREAM                 ! cudaStream_t or C_NULL_PTR
+    END FUNCTION
+    INTEGER(C_INT) FUNCTION FZ_VOIGT(N, A, V, H, F) BIND(C, NAME='fz_voigt')
+      IMPORT
+      INTEGER(C_INT), VALUE      :: N
+      REAL(C_FLOAT)              :: A(*)
+      REAL(C_FLOAT)              :: V(*)
+      REAL(C_FLOAT)              :: H(*)
+      REAL(C_FLOAT)              :: F(*)
     END FUNCTION
     INTEGER(C_INT) FUNCTION FZ_MLP_CREATE(MLP, NLAYERS, DIMS, SEED, DEVICE) BIND(C, &
         NAME='fz_mlp_create')

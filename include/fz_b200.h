@@ -436,6 +436,28 @@ int fz_lm_rearange(fz_ctx* ctx, int npix, float* models, const double* delta, in
 int fz_lm_rearange_device(fz_ctx* ctx, int npix, float* d_models, const double* d_delta, int node_expansion,
                           void* stream);
 
+/* The formal solution on given absorption matrices: SET_BOUNDARY +
+ * OLD_ANALYTICAL_SOLVER with EVOL_OPERATOR (src/rtesolver.f90:163-473,
+ * :1134-1147; the per-(K, lambda) calls at src/forward.f90:971-975), for a
+ * host that builds its own absorption matrix.  From the bottom up, I =
+ * (S, 0, 0, 0) at the first height and wherever bnd is set, else I_K =
+ * (1 - O_K) S_K + O_K I_{K-1} with O_K the evolution operator of the height's
+ * matrix over dz = 1e5 |z_{K+1} - z_K| cm (the top height: its backward
+ * difference).  eta: (NW, 7, NZ, ncol) REAL*4, per height the seven arrays
+ * ETAI, ETAQ, ETAU, ETAV, RHOQ, RHOU, RHOV in cm^-1; src: (NW, NZ, ncol)
+ * source function; zz: ZZ(NZ) in km; bnd: (NZ, ncol) boundary flags or NULL;
+ * out: SYN1D(4, NW, ncol) REAL*8 (without GAIN).  FP32 arithmetic, as in the
+ * synthesis kernels. */
+int fz_rte_solve(int ncol, int nz, int nw, const float* eta, const float* src, const double* zz, const int* bnd,
+                 double* out);
+int fz_rte_solve_device(int ncol, int nz, int nw, const float* d_eta, const float* d_src, const double* d_zz,
+                        const int* d_bnd, double* d_out, void* stream);
+
+/* VOIGT (src/voigt.f:17-98) on arrays, in the FP32 form the synthesis
+ * kernels evaluate: H(a, v) and the Faraday-Voigt F(a, v) (the reference's
+ * HH, FF) of n (damping, v) pairs, host buffers. */
+int fz_voigt(int n, const float* a, const float* v, float* h, float* f);
+
 /* Warm-start network (no counterpart in the reference): an MLP of nlayers
  * fully connected layers dims[0] -> dims[1] -> ... -> dims[nlayers] with GELU
  * between layers, trained and evaluated with hand-written BF16 tensor-core

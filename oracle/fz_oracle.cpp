@@ -1219,6 +1219,41 @@ void orc_voigt(int n, double a, const double* v, double* h, double* f) {
   for (int i = 0; i < n; ++i) voigt1(a, v[i], h[i], f[i]);
 }
 
+// SET_BOUNDARY + OLD_ANALYTICAL_SOLVER (src/rtesolver.f90:163-187,
+// :1134-1147) on given absorption-matrix elements and source functions:
+// from the bottom up, I = (S, 0, 0, 0) at K = 1 and wherever bnd[K] is set,
+// else I_K = (1 - O_K) S_K + O_K I_{K-1}, O_K = EVOL_OPERATOR of the
+// height's matrix over dz = 1e5 |z_{K+1} - z_K| cm (the top height's
+// backward difference).  eta: (7, nw, nz) as ETAI, ETAQ, ETAU, ETAV, RHOQ,
+// RHOU, RHOV (nw fastest); src (nw, nz); out (4, nw) SYN1D.
+void orc_rte_solve(int nz, int nw, const double* eta, const double* src, const double* zz, const int* bnd,
+                   double* out) {
+  AbsMat A;
+  A.resize(nw);
+  std::vector<double*> rows = {A.ei.data(), A.eq.data(), A.eu.data(), A.ev.data(), A.rq.data(), A.ru.data(),
+                               A.rv.data()};
+  for (int k = 0; k < nz; ++k) {
+    for (int e = 0; e < 7; ++e)
+      for (int l = 0; l < nw; ++l) rows[e][l] = eta[((size_t)k * 7 + e) * nw + l];
+    for (int l = 0; l < nw; ++l) {
+      const double S = src[(size_t)k * nw + l];
+      double* o = out + 4 * (size_t)l;
+      if (k == 0 || (bnd && bnd[k])) {
+        o[0] = S;
+        o[1] = o[2] = o[3] = 0.0;
+        continue;
+      }
+      const double dz = (k == nz - 1) ? 1e5 * std::fabs(zz[k] - zz[k - 1]) : 1e5 * std::fabs(zz[k + 1] - zz[k]);
+      double O[4][4];
+      evol_operator(A, l, dz, O);
+      const double in[4] = {o[0], o[1], o[2], o[3]};
+      for (int i = 0; i < 4; ++i)
+        o[i] = ((i == 0 ? 1.0 : 0.0) - O[i][0]) * S + O[i][0] * in[0] + O[i][1] * in[1] + O[i][2] * in[2] +
+               O[i][3] * in[3];
+    }
+  }
+}
+
 // GET_NORM, src/normalization.f90:696-754
 int orc_gain(const orc_line* lines, int nlines, const orc_region* regs, int nreg, float* gain) {
   Setup s = make_setup(lines, nlines, regs, nreg);

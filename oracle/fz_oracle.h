@@ -77,6 +77,13 @@ int orc_zeeman(const orc_line* ln, double* shift, double* strength, int* type, i
 /* Voigt/Faraday (src/voigt.f:17-98, REAL*8 build). */
 void orc_voigt(int n, double a, const double* v, double* h, double* f);
 
+/* SET_BOUNDARY + OLD_ANALYTICAL_SOLVER (src/rtesolver.f90:163-187,
+ * :1134-1147) on given absorption matrices: eta (7, nw, nz) ETAI..RHOV in
+ * cm^-1, src (nw, nz), zz (nz) km, bnd (nz) boundary flags or NULL; out
+ * (4, nw) SYN1D at the top. */
+void orc_rte_solve(int nz, int nw, const double* eta, const double* src, const double* zz, const int* bnd,
+                   double* out);
+
 /* HSRA continuum normalisation GAIN(4,NUMW) (src/normalization.f90:696-754). */
 int orc_gain(const orc_line* lines, int nlines, const orc_region* regs, int nreg,
              float* gain /* (4,NUMW) */);

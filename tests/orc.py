@@ -48,6 +48,7 @@ def lib():
         L.orc_parse_lines.argtypes = [ctypes.c_char_p, P, ctypes.c_int]
         L.orc_zeeman.argtypes = [P, P, P, P, ctypes.c_int]
         L.orc_voigt.argtypes = [ctypes.c_int, ctypes.c_double, P, P, P]
+        L.orc_rte_solve.argtypes = [ctypes.c_int, ctypes.c_int, P, P, P, P, P]
         L.orc_gain.argtypes = [P, ctypes.c_int, P, ctypes.c_int, P]
         L.orc_forward.argtypes = [P, ctypes.c_int, P, ctypes.c_int, P, ctypes.c_int, ctypes.c_int, P,
                                   ctypes.c_int, P, P, ctypes.c_int]
@@ -123,6 +124,20 @@ def voigt(a, v):
     h, f = np.zeros_like(v), np.zeros_like(v)
     lib().orc_voigt(len(v), float(a), _p(v), _p(h), _p(f))
     return h, f
+
+
+def rte_solve(eta, src, zz, bnd=None):
+    """SET_BOUNDARY + OLD_ANALYTICAL_SOLVER on given matrices: eta (nz, 7,
+    nw) ETAI..RHOV [cm^-1], src (nz, nw), zz (nz) km, bnd (nz) or None.
+    Returns SYN1D as (nw, 4)."""
+    eta = np.ascontiguousarray(eta, dtype=np.float64)
+    nz, _, nw = eta.shape
+    src = np.ascontiguousarray(src, dtype=np.float64)
+    zz = np.ascontiguousarray(zz, dtype=np.float64)
+    b = None if bnd is None else np.ascontiguousarray(bnd, dtype=np.int32)
+    out = np.zeros((nw, 4))
+    lib().orc_rte_solve(nz, nw, _p(eta), _p(src), _p(zz), None if b is None else _p(b), _p(out))
+    return out
 
 
 def gain(lines, regions):

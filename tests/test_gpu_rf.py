@@ -8,7 +8,10 @@ CALCULATE_EQUIVALENT_DSYN).  Each Jacobian column (one node of one parameter,
 all Stokes parameters and wavelengths) is compared relative to its own
 largest entry:
 
-    max |J_gpu - J_oracle| <= RF_TOL * max |J_oracle|     (RF_TOL = 2e-3)
+    max |J_gpu - J_oracle| <= RF_TOL * max |J_oracle|     (RF_TOL = 2e-4)
+
+(FP32 against FP64 measures ~3e-5; the bound leaves a 6x margin and still
+catches a wrong term in any one parameter's derivative chain)
 
 and the Stokes vector of the same call to the synthesis tolerances (1e-5
 relative in I, 1e-6 absolute in Q, U, V).
@@ -18,7 +21,7 @@ import pytest
 
 pytestmark = pytest.mark.gpu
 
-RF_TOL = 2e-3
+RF_TOL = 2e-4
 
 
 def _setup(fz, orc, nz, ncol, seed):
@@ -82,13 +85,13 @@ def test_rf_nodes_validation(fz, orc):
 
 
 @pytest.mark.parametrize("he", [True, False])
-def test_full_height_rf_matches_oracle(fz, orc, he):
+@pytest.mark.parametrize("nz,ncol", [(32, 4), (128, 2)])
+def test_full_height_rf_matches_oracle(fz, orc, he, nz, ncol):
     """fz_forward_rf_full: the WRITE RESPONSE FUNCTION output (one node per
     height for T, Pg, Bx, By, Bz, v_z) against the oracle's EQVDSYN with
-    NJ = NZ; heights compared against the strongest height of the same
-    (column, parameter)."""
-    nz = 32
-    lines, reg, g, m = _setup(fz, orc, nz=nz, ncol=4, seed=11)
+    NJ = NZ, at 32 heights and at the benchmark's 128; heights compared
+    against the strongest height of the same (column, parameter)."""
+    lines, reg, g, m = _setup(fz, orc, nz=nz, ncol=ncol, seed=11)
     if not he:
         _, m, _ = orc.forward(lines, reg, g, m, hydrostatic=True)
     ctx = fz.Synthesis(lines, reg, nz=nz, gain=g)

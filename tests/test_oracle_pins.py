@@ -103,3 +103,32 @@ def test_zeeman_patterns(orc):
     assert len(sh) == 3
     geff = abs(sh[ty == 1][0]) / (4.66685e-10 * ln["l0"] ** 2)
     assert abs(geff - 2.5) < 1e-6
+
+
+def test_generated_tables_match_a_second_parse_of_the_reference():
+    """fz_tables.h (written by oracle/gen_tables.py, compiled into both the
+    library and the oracle) against tests/golden/table_pins.npz, a second
+    parse of the same Fortran DATA by tests/golden/make_table_pins.py that
+    shares no code with the generator: the six ABO cross-section / velocity
+    exponent grids (src/damping.f90:24-840) and the HSRA T, Pg, rho, z
+    (src/normalization.f90:135-393), bit for bit."""
+    import re
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    hdr = open(os.path.join(root, "firtez-dz_b200", "csrc", "fz_tables.h")).read()
+    pins = np.load(os.path.join(root, "tests", "golden", "table_pins.npz"))
+
+    def c_array(name):
+        m = re.search(r"\b%s(\[[^=]*)=\s*\{(.*?)\};" % name, hdr, flags=re.S)
+        dims = [d for d in re.findall(r"\[(\w+)\]", m.group(1))]
+        nums = [float(x) for x in re.findall(r"[-+]?(?:\d+\.\d*|\.\d+|\d+)(?:[eE][-+]?\d+)?", m.group(2))]
+        return dims, np.array(nums)
+
+    for key in pins.files:
+        dims, vals = c_array("fz_tab_" + key)
+        ref = pins[key]
+        assert vals.size == ref.size, key
+        if key.startswith("hsra"):
+            assert np.array_equal(vals.astype(np.float32), ref), key
+        else:
+            assert [int(d) for d in dims] == list(ref.shape), key
+            assert np.array_equal(vals.reshape(ref.shape), ref), key
