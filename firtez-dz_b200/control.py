@@ -280,9 +280,11 @@ def run(path, device=0):
         d_obs = v3io.obs_from_stokes_device(torch.from_numpy(st).to(dev))
         cycles = c.schedule(nz)
         reg_ = {p: (c.pen_typ.get(p, 0), c.pen_alp.get(p, 0.0)) for p in c.pen_alp}
+        # MAKE_DECISION's field-wide stop on the mean STEPS (src/invert3d.f90:
+        # 843-846) besides the per-pixel rule; 40 iterations as a safety cap
         opts = LMOpts(maxsteps=c.maxsteps, maxit=40, isigma=c.isigma, svdtol=c.svdtol, wstk=c.wstk,
                       reg=reg_ or None, assist=tuple(c.assist) + (("progressive",) if c.progressive else ()),
-                      solver=c.solver, node_expansion=c.node_expansion)
+                      solver=c.solver, node_expansion=c.node_expansion, global_stop=True)
         mod, _, _, _ = ctx.invert_cycles(d_obs.cpu().numpy(), d_model.cpu().numpy(), nx, ny, cycles,
                                          hydrostatic=c.hydrostatic, opts=opts)
         d_m = torch.from_numpy(mod).to(dev)

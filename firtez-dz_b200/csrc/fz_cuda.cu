@@ -1224,9 +1224,12 @@ bool has_blends(const fz_ctx* c);
 // registers; in place on rf.  A (parameter, height) column with an infinite
 // entry is zeroed, the SUM(ABS(.)) > HUGE test of :672-679.
 __global__ void __launch_bounds__(512) k_rf_prop(int nz, int nw, const float* __restrict__ gain,
-                                                 const float* __restrict__ oscr, float* __restrict__ rf) {
+                                                 const float* __restrict__ oscr, float* __restrict__ rf,
+                                                 const int* __restrict__ list = nullptr,
+                                                 const int* __restrict__ nlist = nullptr) {
   extern __shared__ int flg[];
-  const int col = blockIdx.x, l = threadIdx.x;
+  if (list && (int)blockIdx.x >= *nlist) return;
+  const int col = list ? list[blockIdx.x] : (int)blockIdx.x, l = threadIdx.x;
   for (int i = l; i < nz; i += blockDim.x) flg[i] = 0;
   __syncthreads();
   const bool active = l < nw;
@@ -1282,6 +1285,7 @@ __global__ void __launch_bounds__(512) k_rf_prop(int nz, int nw, const float* __
 }  // namespace
 
 #include "fz_lm.cuh"
+#include "fz_lm_big.cuh"
 
 namespace {
 
@@ -1666,6 +1670,19 @@ struct fz_ctx {
   LMQueue* d_q = nullptr;
   int* h_done = nullptr;
   LMQueue* h_q = nullptr;   // pinned copy of the work-queue state   // pinned
+  // node layouts whose forward accumulation does not fit in shared memory:
+  // the node Jacobian is contracted from the response functions at every
+  // height (scratch (columns, 6, nz, NFREQ)), and the LM runs its large-NP
+  // kernels with the per-node tables in device memory
+  bool rf_full = false;
+  float* d_rfbig = nullptr;
+  size_t rfbig_len = 0;
+  int* d_nrow = nullptr;       // (np) model row of each node
+  double* d_nnorm = nullptr;   // (np) PARAM_NORMS of each node
+  double* d_nhss = nullptr;    // (np, np) PEN_HSS of the last configured regularisation
+  std::vector<double> nhss_host;
+  double* d_svd = nullptr;     // per-slot SVD scratch (2 np^2)
+  size_t svd_len = 0;
 };
 
 namespace {
@@ -1828,10 +1845,12 @@ size_t rf_smem(const fz_ctx* c) {
 
 // The response-function kernels run one thread per wavelength in blocks of
 // at most 512: NUMW <= 512, and their shared memory within the 227 KB a
-// block may have.
+// block may have (the slab alone when the node Jacobian is contracted from
+// the full response functions).
 int rf_check(const fz_ctx* c) {
   if (((c->numw + 31) & ~31) > 512) return FZ_ERR_LIMIT;
-  if (rf_smem(c) > 227 * 1024) return FZ_ERR_LIMIT;
+  const size_t full = (size_t)c->nz * rf_w(c->nreg, c->nlu) * sizeof(float);
+  if ((c->rf_full ? full : rf_smem(c)) > 227 * 1024) return FZ_ERR_LIMIT;
   return 0;
 }
 
@@ -1840,12 +1859,36 @@ int ensure_rf_scratch(fz_ctx* c, int ncol) {
   if (rc) return rc;
   // the node kernels' shared memory above the default 48 KB (set here, before
   // any stream capture of the inversion's iteration)
-  const size_t sms = rf_smem(c);
-  if (sms > 48 * 1024) {
-    FZ_CK((set_synth_rf_attr<true, false>(cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sms)));
-    FZ_CK((set_synth_rf_attr<false, false>(cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sms)));
-  }
   const int swr = rf_w(c->nreg, c->nlu);
+  if (c->rf_full) {
+    // the node Jacobian through the response functions at every height:
+    // their scratch and the operators of k_rf_prop for ncol columns
+    const size_t nrf = (size_t)ncol * NSLOT * c->nz * 4 * c->numw;
+    if (nrf > c->rfbig_len) {
+      cudaFree(c->d_rfbig);
+      c->d_rfbig = nullptr;
+      c->rfbig_len = 0;
+      FZ_CK(cudaMalloc(&c->d_rfbig, nrf * sizeof(float)));
+      c->rfbig_len = nrf;
+    }
+    const size_t nop = (size_t)ncol * c->nz * 16 * c->numw;
+    if (nop > c->oscr_len) {
+      cudaFree(c->d_oscr);
+      c->d_oscr = nullptr;
+      c->oscr_len = 0;
+      FZ_CK(cudaMalloc(&c->d_oscr, nop * sizeof(float)));
+      c->oscr_len = nop;
+    }
+    const size_t fsm = (size_t)c->nz * swr * sizeof(float);
+    FZ_CK((set_synth_rf_attr<true, true>(cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fsm)));
+    FZ_CK((set_synth_rf_attr<false, true>(cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fsm)));
+  } else {
+    const size_t sms = rf_smem(c);
+    if (sms > 48 * 1024) {
+      FZ_CK((set_synth_rf_attr<true, false>(cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sms)));
+      FZ_CK((set_synth_rf_attr<false, false>(cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sms)));
+    }
+  }
   if ((size_t)ncol > c->rf_cols) {
     cudaFree(c->d_rfslab);
     cudaFree(c->d_chemd);
@@ -1888,8 +1931,12 @@ void launch_opac_rf(fz_ctx* c, int ncol, const float* d_mout, int threads, cudaS
 // The response-function stage of the node path (chemistry derivatives,
 // opacity derivatives, RF synthesis + node Jacobian) on columns whose
 // chemistry k_chain has already left in the context's scratch.
+int launch_rf_stage_full(fz_ctx* c, int ncol, int hydrostatic, double* d_syn, float* d_jac, float* d_mout,
+                         int* d_status, cudaStream_t s, const int* list, const int* nlist);
+
 int launch_rf_stage(fz_ctx* c, int ncol, int hydrostatic, double* d_syn, float* d_jac, float* d_mout, int* d_status,
                     cudaStream_t s, const int* list = nullptr, const int* nlist = nullptr) {
+  if (c->rf_full) return launch_rf_stage_full(c, ncol, hydrostatic, d_syn, d_jac, d_mout, d_status, s, list, nlist);
   {
     ProfScope ps(c, 10, s, list ? 0 : ncol);
     launch_chemder(c, ncol, d_mout, c->tune.chemder_bpsm, s, list, nlist);
@@ -1913,6 +1960,55 @@ int launch_rf_stage(fz_ctx* c, int ncol, int hydrostatic, double* d_syn, float* 
                                                           c->d_rfslab, c->d_coef, d_syn, d_jac, nullptr, d_mout,
                                                           d_status, list, nlist);
   }
+  FZ_CK(cudaGetLastError());
+  if (c->lsf.on) {
+    FZ_CK_RC(launch_lsf<double>(c, d_syn, (long long)ncol * 4, 4, s, list, nlist));
+    FZ_CK_RC(launch_lsf<float>(c, d_jac, (long long)ncol * 4 * c->rf.np, 4 * c->rf.np, s, list, nlist));
+  }
+  return 0;
+}
+
+// The RF stage of node layouts too large for the forward accumulation: the
+// response functions at every height of the columns (FULL synthesis,
+// k_rf_prop with GAIN) into the context's scratch, contracted by the hat
+// table into the node Jacobian (NFREQ, NP) per column of d_jac.  Scratch and
+// kernel attributes come from ensure_rf_scratch (before any capture).
+int launch_rf_stage_full(fz_ctx* c, int ncol, int hydrostatic, double* d_syn, float* d_jac, float* d_mout,
+                         int* d_status, cudaStream_t s, const int* list, const int* nlist) {
+  if (!c->d_rfbig || c->rfbig_len < (size_t)ncol * NSLOT * c->nz * 4 * c->numw) return FZ_ERR_STATE;
+  {
+    ProfScope ps(c, 10, s, list ? 0 : ncol);
+    launch_chemder(c, ncol, d_mout, c->tune.chemder_bpsm, s, list, nlist);
+  }
+  FZ_CK(cudaGetLastError());
+  {
+    ProfScope ps(c, 3, s, list ? 0 : ncol);
+    launch_opac_rf(c, ncol, d_mout, c->tune.opacrf_threads, s, list, nlist);
+  }
+  FZ_CK(cudaGetLastError());
+  const int threads = (c->numw + 31) & ~31;
+  const size_t sms = (size_t)c->nz * rf_w(c->nreg, c->nlu) * sizeof(float);
+  {
+    ProfScope ps(c, 4, s, list ? 0 : ncol);
+    if (hydrostatic)
+      launch_synth_rf<true, true>(has_blends(c), ncol, threads, sms, s, c->d_params, c->d_rf, c->d_lam, c->d_gain,
+                                  ncol, c->d_rfslab, nullptr, d_syn, c->d_rfbig, c->d_oscr, d_mout, d_status, list,
+                                  nlist);
+    else
+      launch_synth_rf<false, true>(has_blends(c), ncol, threads, sms, s, c->d_params, c->d_rf, c->d_lam, c->d_gain,
+                                   ncol, c->d_rfslab, nullptr, d_syn, c->d_rfbig, c->d_oscr, d_mout, d_status, list,
+                                   nlist);
+  }
+  FZ_CK(cudaGetLastError());
+  {
+    ProfScope ps(c, 11, s, list ? 0 : ncol);
+    k_rf_prop<<<ncol, threads, c->nz * sizeof(int), s>>>(c->nz, c->numw, c->d_gain, c->d_oscr, c->d_rfbig, list,
+                                                         nlist);
+  }
+  FZ_CK(cudaGetLastError());
+  const int nf = 4 * c->numw;
+  k_rf_contract<<<dim3((nf + 255) / 256, c->rf.np, ncol), 256, 0, s>>>(c->nz, nf, c->rf, c->d_coef, c->d_rfbig,
+                                                                       d_jac, list, nlist);
   FZ_CK(cudaGetLastError());
   if (c->lsf.on) {
     FZ_CK_RC(launch_lsf<double>(c, d_syn, (long long)ncol * 4, 4, s, list, nlist));
@@ -2075,7 +2171,8 @@ std::vector<double> lm_weights(int numw, const float wstk[4], double isigma) {
 
 int lm_conf(fz_ctx* c, int npix, const fz_lm_opts* o, LMConf& C) {
   if (c->rf.np <= 0) return FZ_ERR_STATE;
-  if (c->rf.np > LM_MAXNP) return FZ_ERR_LIMIT;
+  if (c->rf.np > LM_MAXNP_BIG) return FZ_ERR_LIMIT;
+  const bool big = c->rf.np > LM_MAXNP;   // per-node tables in device memory
   static const int kRef[NSLOT] = {1, 2, 4, 5, 6, 7};
   static const int kRow[9] = {0, 0, 1, 2, 5, 6, 7, 10, 1};   // model row of reference parameter 1..8
   std::memset(&C, 0, sizeof(C));
@@ -2109,13 +2206,17 @@ int lm_conf(fz_ctx* c, int npix, const fz_lm_opts* o, LMConf& C) {
   for (int p = 0; p < NSLOT; ++p) {
     const int rp = kRef[p];
     C.nodes_ref[rp - 1] = c->rf.nj[p];
-    for (int j = 0; j < c->rf.nj[p]; ++j) {
+    for (int j = 0; !big && j < c->rf.nj[p]; ++j) {
       const int n = c->rf.n0[p] + j;
       C.row_of[n] = kRow[rp];
       C.par_of[n] = rp;
       C.norm[n] = norms[rp - 1];
     }
   }
+  C.d_row = c->d_nrow;
+  C.d_norm = c->d_nnorm;
+  std::vector<double> hbig;
+  if (big) hbig.assign((size_t)C.np * C.np, 0.0);
   if (o) {
     for (int p = 0; p < NSLOT; ++p) {
       const int rp = kRef[p], nj = c->rf.nj[p], j0 = c->rf.n0[p];
@@ -2136,9 +2237,26 @@ int lm_conf(fz_ctx* c, int npix, const fz_lm_opts* o, LMConf& C) {
               v += dk * dl;
             }
           }
-          C.reg_hss[(j0 + k) * C.np + (j0 + l)] = a2 * v;
+          if (big)
+            hbig[(size_t)(j0 + k) * C.np + (j0 + l)] = a2 * v;
+          else
+            C.reg_hss[(j0 + k) * C.np + (j0 + l)] = a2 * v;
         }
     }
+  }
+  if (big && C.reg) {
+    // PEN_HSS of a large layout in device memory, uploaded when it changes
+    // (after the device has finished with the previous one)
+    if (hbig != c->nhss_host) {
+      FZ_CK(cudaDeviceSynchronize());
+      cudaFree(c->d_nhss);
+      c->d_nhss = nullptr;
+      c->nhss_host.clear();
+      FZ_CK(cudaMalloc(&c->d_nhss, hbig.size() * sizeof(double)));
+      FZ_CK(cudaMemcpy(c->d_nhss, hbig.data(), hbig.size() * sizeof(double), cudaMemcpyHostToDevice));
+      c->nhss_host = hbig;
+    }
+    C.d_hss = c->d_nhss;
   }
   return 0;
 }
@@ -2700,6 +2818,7 @@ int fz_rf_to_v3_device(int npix, int nz, int nw, const float* d_rf, float* d_out
 
 int fz_errors_device(fz_ctx* c, int npix, const double* d_obs, const float* d_models, int hydrostatic,
                      const fz_lm_opts* opts, float* d_err, double* d_chi2, int* d_status, void* stream) {
+  if (c && c->rf.np > LM_MAXNP) return FZ_ERR_LIMIT;   // errors mode: node layouts of up to 16 nodes
   if (!c || npix <= 0 || !d_obs || !d_models || !d_err || !d_chi2) return FZ_ERR_ARG;
   if (hydrostatic < 0 || hydrostatic > 1) return FZ_ERR_ARG;
   FZ_CK(cudaSetDevice(c->device));
@@ -3260,6 +3379,12 @@ int fz_destroy(fz_ctx* c) {
   cudaFree(c->d_chemd);
   cudaFree(c->d_jac);
   cudaFree(c->d_coef64);
+  cudaFree(c->inv.state);
+  cudaFree(c->d_rfbig);
+  cudaFree(c->d_nrow);
+  cudaFree(c->d_nnorm);
+  cudaFree(c->d_nhss);
+  cudaFree(c->d_svd);
   lm_free(c);
   cudaFree(c->d_q);
   if (c->h_done) cudaFreeHost(c->h_done);
@@ -3331,7 +3456,7 @@ int fz_rf_nodes(fz_ctx* c, const int* nodes) {
     np += nj;
   }
   if (np <= 0) return FZ_ERR_ARG;
-  if (np > MAXNP) return FZ_ERR_LIMIT;
+  if (np > LM_MAXNP_BIG) return FZ_ERR_LIMIT;
   rf.np = np;
   std::vector<float> tab((size_t)c->nz * np, 0.0f);
   std::vector<double> cf;
@@ -3363,14 +3488,35 @@ int fz_rf_nodes(fz_ctx* c, const int* nodes) {
     FZ_CK(cudaMemcpy(c->d_coef64, t64.data(), t64.size() * sizeof(double), cudaMemcpyHostToDevice));
   }
   FZ_CK(cudaMemcpy(c->d_rf, &rf, sizeof(RFConf), cudaMemcpyHostToDevice));
+  {
+    // per-node model rows and PARAM_NORMS for the large-layout LM kernels
+    static const int kRow[9] = {0, 0, 1, 2, 5, 6, 7, 10, 1};
+    const double norms[8] = {6000.0, 1.0e5, 1.0e-5, 1.0e3, 1.0e3, 1.0e3, 1.0e6, 6.0e2};
+    std::vector<int> row(np);
+    std::vector<double> nrm(np);
+    for (int p = 0; p < NSLOT; ++p)
+      for (int j = 0; j < rf.nj[p]; ++j) {
+        row[rf.n0[p] + j] = kRow[kRef[p]];
+        nrm[rf.n0[p] + j] = norms[kRef[p] - 1];
+      }
+    cudaFree(c->d_nrow);
+    cudaFree(c->d_nnorm);
+    c->d_nrow = nullptr;
+    c->d_nnorm = nullptr;
+    FZ_CK(cudaMalloc(&c->d_nrow, np * sizeof(int)));
+    FZ_CK(cudaMalloc(&c->d_nnorm, np * sizeof(double)));
+    FZ_CK(cudaMemcpy(c->d_nrow, row.data(), np * sizeof(int), cudaMemcpyHostToDevice));
+    FZ_CK(cudaMemcpy(c->d_nnorm, nrm.data(), np * sizeof(double), cudaMemcpyHostToDevice));
+    c->nhss_host.clear();
+  }
   c->rf = rf;
   const size_t sms = rf_smem(c);
   int maxsm = 0;
   FZ_CK(cudaDeviceGetAttribute(&maxsm, cudaDevAttrMaxSharedMemoryPerBlockOptin, c->device));
-  if (sms > (size_t)maxsm) {
-    c->rf.np = 0;
-    return FZ_ERR_LIMIT;
-  }
+  // the forward accumulation keeps 4 x NP accumulators per wavelength in
+  // shared memory; larger layouts contract the full response functions
+  c->rf_full = sms > (size_t)maxsm || np > MAXNP;
+  if (c->rf_full) return np;
   FZ_CK((set_synth_rf_attr<true, false>(cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sms)));
   FZ_CK((set_synth_rf_attr<false, false>(cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sms)));
   // all of the SM's unified L1/shared storage as shared memory: two CTAs of
@@ -3400,7 +3546,33 @@ int fz_invert_device(fz_ctx* c, int npix, const double* d_obs, const float* d_in
   int S = (opts && opts->slots > 0) ? opts->slots : c->tune.lm_slots;
   if (C.global_stop) S = npix;   // the field rule needs every pixel in flight
   if (S > npix) S = npix;
+  const bool big = C.np > LM_MAXNP;
+  if (big) {
+    // large layouts: the slot count within a memory budget (Jacobian, H and
+    // SVD scratch per slot and pool, full response functions and operators)
+    const size_t nf = 4 * (size_t)c->numw, np = C.np;
+    const size_t per = 2 * (np * nf * 4 + np * np * 8) + 2 * np * np * 8 + (size_t)NSLOT * c->nz * nf * 4 +
+                       (size_t)c->nz * 16 * c->numw * 4;
+    const size_t cap = std::max<size_t>(1, ((size_t)24 << 30) / per);
+    if ((size_t)S > cap) {
+      if (C.global_stop) return FZ_ERR_LIMIT;
+      S = (int)cap;
+    }
+  }
   if ((rc = lm_alloc(c, S))) return rc;
+  if (big) {
+    if (C.solver != 2) {
+      const size_t need = (size_t)S * 2 * C.np * C.np;
+      if (need > c->svd_len) {
+        cudaFree(c->d_svd);
+        c->d_svd = nullptr;
+        c->svd_len = 0;
+        FZ_CK(cudaMalloc(&c->d_svd, need * sizeof(double)));
+        c->svd_len = need;
+      }
+    }
+    FZ_CK(cudaFuncSetAttribute(k_lm_gram_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)GT_SMEM));
+  }
   // The iterations run on the context's own stream (capturable, unlike a
   // caller's legacy default stream), after the work already enqueued on the
   // caller's stream; the call returns with everything complete.
@@ -3449,20 +3621,38 @@ int fz_invert_device(fz_ctx* c, int npix, const double* d_obs, const float* d_in
     if (r) return r;
     {
       ProfScope ps(c, 6, s, n);
-      k_lm_accept<<<n, 256, 0, s>>>(C, L, c->d_q, d_w, d_obs, d_init, d_target_chi2, d_model_out, d_chi2, d_iters,
+      k_lm_accept<<<n, 256, C.reg ? 2 * C.np * sizeof(double) : 0, s>>>(C, L, c->d_q, d_w, d_obs, d_init,
+                                                                        d_target_chi2, d_model_out, d_chi2, d_iters,
                                     d_syn_out, d_status, c->d_coef64);
     }
     k_lm_rflist<<<1, 1024, 0, s>>>(n, L.need_rf, L.rf_list, c->d_q);
     FZ_CK(cudaGetLastError());
     r = launch_rf_stage(c, n, hydrostatic, L.syn, L.jacb, L.mcur, L.status, s, L.rf_list, &c->d_q->rf_count);
     if (r) return r;
-    {
-      ProfScope ps(c, 7, s, n);
-      k_lm_normal<<<(n + 3) / 4, 128, 0, s>>>(C, L, d_w);
-    }
-    {
-      ProfScope ps(c, 8, s, n);
-      k_lm_solve<<<(n + 3) / 4, 128, 0, s>>>(C, L);
+    if (big) {
+      // tcgen05 normal equations over tile pairs, FP64 gradient, CTA solver
+      const int nb = (C.np + GT_M - 1) / GT_M;
+      {
+        ProfScope ps(c, 7, s, n);
+        k_lm_gram_tc<<<dim3(nb * (nb + 1) / 2, n), 128, GT_SMEM, s>>>(C, L, d_w, &c->d_q->tc_err);
+        k_lm_grad<<<dim3((C.np + 7) / 8, n), 256, 0, s>>>(C, L, d_w);
+      }
+      {
+        ProfScope ps(c, 8, s, n);
+        if (C.solver == 2)
+          k_lm_cg_big<<<n, 256, 6 * C.np * sizeof(double), s>>>(C, L);
+        else
+          k_lm_svd_big<<<n, 256, 2 * C.np * sizeof(double), s>>>(C, L, c->d_svd);
+      }
+    } else {
+      {
+        ProfScope ps(c, 7, s, n);
+        k_lm_normal<<<(n + 3) / 4, 128, 0, s>>>(C, L, d_w);
+      }
+      {
+        ProfScope ps(c, 8, s, n);
+        k_lm_solve<<<(n + 3) / 4, 128, 0, s>>>(C, L);
+      }
     }
     {
       ProfScope ps(c, 9, s, n);
@@ -3511,6 +3701,10 @@ int fz_invert_device(fz_ctx* c, int npix, const double* d_obs, const float* d_in
     }
     FZ_CK(cudaStreamSynchronize(s));
     hq = *c->h_q;
+    if (hq.tc_err) {
+      std::fprintf(stderr, "fz_b200: the tensor-core normal equations gave up waiting for their MMAs\n");
+      return FZ_ERR_CUDA;
+    }
     if (c->prof) {   // columns of the RF pass: known once the iteration ran
       c->prof_items[10] += hq.rf_count;
       c->prof_items[3] += hq.rf_count;
@@ -3628,7 +3822,7 @@ int fz_invert(fz_ctx* c, int npix, const double* obs, const float* init, const d
 static int lm_perturbation_host(fz_ctx* c, int npix, int np, int nfreq, const double* jac64, const float* jac32,
                                 const double* diff, const double* lambda, const double* reg_pen,
                                 const double* reg_hss, int dtype, double svdtol, double* delta) {
-  if (!c || npix <= 0 || np <= 0 || np > LM_MAXNP || nfreq <= 0 || (nfreq & 3) || (!jac64 == !jac32) || !diff || !lambda || !delta)
+  if (!c || npix <= 0 || np <= 0 || np > LM_MAXNP_BIG || nfreq <= 0 || (nfreq & 3) || (!jac64 == !jac32) || !diff || !lambda || !delta)
     return FZ_ERR_ARG;
   if (dtype < 0 || dtype > 2) return FZ_ERR_ARG;   // GET_PERTURBATION's DTYPE (0 taken as 1)
   FZ_CK(cudaSetDevice(c->device));
@@ -3639,7 +3833,11 @@ static int lm_perturbation_host(fz_ctx* c, int npix, int np, int nfreq, const do
   C.inu = 1.0;
   C.svdtol = svdtol > 0 ? svdtol : 1.0e-4;
   C.solver = dtype == 2 ? 2 : 1;
-  for (int j = 0; j < np; ++j) C.norm[j] = 1.0;
+  const bool big = np > LM_MAXNP;
+  for (int j = 0; j < np && !big; ++j) C.norm[j] = 1.0;
+  double* d_ones = nullptr;   // PARAM_NORMS of a large layout: the Jacobian comes normalised
+  int* d_err = nullptr;
+  double* d_svd = nullptr;
   LMSlots L{};
   L.S = npix;
   std::vector<int> zeros(npix, 0);
@@ -3658,6 +3856,15 @@ static int lm_perturbation_host(fz_ctx* c, int npix, int np, int nfreq, const do
     if ((rc = cuda_fail(cudaMalloc(&L.g, (size_t)npix * np * sizeof(double))))) break;
     if ((rc = cuda_fail(cudaMalloc(&L.delta, (size_t)npix * np * sizeof(double))))) break;
     if ((rc = cuda_fail(cudaMalloc(&d_w, nfreq * sizeof(double))))) break;
+    if (big) {
+      std::vector<double> ones(np, 1.0);
+      if ((rc = cuda_fail(cudaMalloc(&d_ones, np * sizeof(double))))) break;
+      if ((rc = cuda_fail(cudaMalloc(&d_err, sizeof(int))))) break;
+      if (C.solver != 2 && (rc = cuda_fail(cudaMalloc(&d_svd, (size_t)npix * 2 * np * np * sizeof(double))))) break;
+      cudaMemcpy(d_ones, ones.data(), np * sizeof(double), cudaMemcpyHostToDevice);
+      cudaMemset(d_err, 0, sizeof(int));
+      C.d_norm = d_ones;
+    }
     if (reg_pen) {
       if ((rc = cuda_fail(cudaMalloc(&L.pen, (size_t)npix * np * sizeof(double))))) break;
       cudaMemcpy(L.pen, reg_pen, (size_t)npix * np * sizeof(double), cudaMemcpyHostToDevice);
@@ -3687,11 +3894,28 @@ static int lm_perturbation_host(fz_ctx* c, int npix, int np, int nfreq, const do
     }
     cudaMemcpy(L.diff, diff, (size_t)npix * nfreq * sizeof(double), cudaMemcpyHostToDevice);
     cudaMemcpy(d_w, ones.data(), nfreq * sizeof(double), cudaMemcpyHostToDevice);
-    k_lm_normal<<<(npix + 3) / 4, 128, 0, c->stream>>>(C, L, d_w);
-    k_lm_solve<<<(npix + 3) / 4, 128, 0, c->stream>>>(C, L);
+    if (big) {
+      const int nb = (np + GT_M - 1) / GT_M;
+      if ((rc = cuda_fail(cudaFuncSetAttribute(k_lm_gram_tc, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                               (int)GT_SMEM)))) break;
+      k_lm_gram_tc<<<dim3(nb * (nb + 1) / 2, npix), 128, GT_SMEM, c->stream>>>(C, L, d_w, d_err);
+      k_lm_grad<<<dim3((np + 7) / 8, npix), 256, 0, c->stream>>>(C, L, d_w);
+      if (C.solver == 2)
+        k_lm_cg_big<<<npix, 256, 6 * np * sizeof(double), c->stream>>>(C, L);
+      else
+        k_lm_svd_big<<<npix, 256, 2 * np * sizeof(double), c->stream>>>(C, L, d_svd);
+    } else {
+      k_lm_normal<<<(npix + 3) / 4, 128, 0, c->stream>>>(C, L, d_w);
+      k_lm_solve<<<(npix + 3) / 4, 128, 0, c->stream>>>(C, L);
+    }
     if ((rc = cuda_fail(cudaGetLastError()))) break;
     if ((rc = cuda_fail(cudaStreamSynchronize(c->stream)))) break;
     rc = cuda_fail(cudaMemcpy(delta, L.delta, (size_t)npix * np * sizeof(double), cudaMemcpyDeviceToHost));
+    if (!rc && d_err) {
+      int e = 0;
+      rc = cuda_fail(cudaMemcpy(&e, d_err, sizeof(int), cudaMemcpyDeviceToHost));
+      if (!rc && e) rc = FZ_ERR_CUDA;
+    }
   } while (false);
   cudaFree(L.pix);
   cudaFree(L.skip);
@@ -3704,6 +3928,9 @@ static int lm_perturbation_host(fz_ctx* c, int npix, int np, int nfreq, const do
   cudaFree(L.pen);
   cudaFree(L.hss);
   cudaFree(d_w);
+  cudaFree(d_ones);
+  cudaFree(d_err);
+  cudaFree(d_svd);
   return rc;
 }
 

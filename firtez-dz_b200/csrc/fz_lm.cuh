@@ -26,7 +26,8 @@
 
 namespace {
 
-constexpr int LM_MAXNP = 16;    // tensor-core tile of the normal equations
+constexpr int LM_MAXNP = 16;    // the warp kernels' tile (mma.sync normal equations, warp SVD)
+constexpr int LM_MAXNP_BIG = 1024;   // larger layouts: tcgen05 normal equations, CTA solvers
 constexpr int LM_PAD = -1;      // empty slot
 constexpr int LM_SKIP = 1;      // slot refilled this iteration: no step yet
 
@@ -47,7 +48,19 @@ struct LMConf {
   int row_of[LM_MAXNP];        // model row of each node's parameter
   int par_of[LM_MAXNP];        // reference parameter (1-based) of each node
   double norm[LM_MAXNP];       // PARAM_NORMS of each node's parameter
+  // np > LM_MAXNP: the same per-node tables in device memory
+  const int* d_row;            // (np)
+  const double* d_norm;        // (np)
+  const double* d_hss;         // (np, np) PEN_HSS, when reg
 };
+
+__device__ __forceinline__ int lm_row(const LMConf& C, int j) { return C.np <= LM_MAXNP ? C.row_of[j] : C.d_row[j]; }
+__device__ __forceinline__ double lm_nrm(const LMConf& C, int j) {
+  return C.np <= LM_MAXNP ? C.norm[j] : C.d_norm[j];
+}
+__device__ __forceinline__ double lm_hss(const LMConf& C, int j, int i) {
+  return C.np <= LM_MAXNP ? C.reg_hss[j * C.np + i] : C.d_hss[(size_t)j * C.np + i];
+}
 
 // Slot pool (device pointers), one allocation per field.
 struct LMSlots {
@@ -80,6 +93,8 @@ struct LMQueue {
   int active;        // occupied slots (k_lm_scan)
   int rf_count;      // slots in the RF pass of this iteration (k_lm_rflist)
   unsigned long long steps_sum;   // sum over the call's pixels of STEPS (global stop rule; two's complement)
+  int tc_err;        // a tensor-core kernel gave up waiting (bounded mbarrier waits)
+  int pad;
 };
 
 // UPDATE_LAMBDA (src/get_dmodel.f90:917-956) with FACTOR = 0.01: an
@@ -141,20 +156,20 @@ __constant__ double c_lm_upp[8] = {1.8e4, 1.0e12, 1.0e10, 5.0e4, 5.0e4, 5.0e4, 1
 // PARAM_NORM -- the x of GET_IT_PENALTIES (:1041-1197).  Thread j < np.
 __device__ __forceinline__ double lm_node_value(const LMConf& C, const float* __restrict__ m,
                                                 const double* __restrict__ coef, int j) {
-  const float* row = m + (size_t)C.row_of[j] * C.nz;
+  const float* row = m + (size_t)lm_row(C, j) * C.nz;
   double a = 0.0, cs = 0.0;
   for (int k = 0; k < C.nz; ++k) {
     const double c = coef[(size_t)k * C.np + j];
     a += (double)row[k] * c;
     cs += c;
   }
-  return a / cs / C.norm[j];
+  return a / cs / lm_nrm(C, j);
 }
 
-// PEN_RES_j = (PEN_HSS x)_j of model m for thread j < np (x in shared xs)
+// PEN_RES_j = (PEN_HSS x)_j of model m for node j (x in shared xs)
 __device__ __forceinline__ double lm_pen_res(const LMConf& C, const double* xs, int j) {
   double r = 0.0;
-  for (int i = 0; i < C.np; ++i) r += C.reg_hss[j * C.np + i] * xs[i];
+  for (int i = 0; i < C.np; ++i) r += lm_hss(C, j, i) * xs[i];
   return r;
 }
 
@@ -218,7 +233,9 @@ __global__ void __launch_bounds__(256) k_lm_accept(LMConf C, LMSlots Sl, LMQueue
                                                    double* __restrict__ out_syn, int* __restrict__ out_status,
                                                    const double* __restrict__ coef) {
   __shared__ double red[8];
-  __shared__ double xs[LM_MAXNP], pr[LM_MAXNP];
+  extern __shared__ double sm_acc[];   // with regularisation: xs, pr (np each)
+  double* xs = sm_acc;
+  double* pr = sm_acc + C.np;
   __shared__ int acc, fin, early, np_next;
   const int s = blockIdx.x;
   if (threadIdx.x == 0) {
@@ -240,9 +257,9 @@ __global__ void __launch_bounds__(256) k_lm_accept(LMConf C, LMSlots Sl, LMQueue
     // NEW_CALCULATE_CHI2 with regularisation (src/get_dmodel.f90:966-983):
     // + sum(PEN_RES^2) of the current model, PEN_FACTOR = 1
     const float* mc = Sl.mcur + (size_t)s * nm;
-    if (threadIdx.x < C.np) xs[threadIdx.x] = lm_node_value(C, mc, coef, threadIdx.x);
+    for (int j = threadIdx.x; j < C.np; j += blockDim.x) xs[j] = lm_node_value(C, mc, coef, j);
     __syncthreads();
-    if (threadIdx.x < C.np) pr[threadIdx.x] = lm_pen_res(C, xs, threadIdx.x);
+    for (int j = threadIdx.x; j < C.np; j += blockDim.x) pr[j] = lm_pen_res(C, xs, j);
     __syncthreads();
     double pp = 0.0;
     for (int j = 0; j < C.np; ++j) pp += pr[j] * pr[j];
@@ -297,12 +314,12 @@ __global__ void __launch_bounds__(256) k_lm_accept(LMConf C, LMSlots Sl, LMQueue
     // (:1010-1015)
     if (!acc) {
       const float* mb = Sl.mbest + (size_t)s * nm;
-      if (threadIdx.x < C.np) xs[threadIdx.x] = lm_node_value(C, mb, coef, threadIdx.x);
+      for (int j = threadIdx.x; j < C.np; j += blockDim.x) xs[j] = lm_node_value(C, mb, coef, j);
       __syncthreads();
-      if (threadIdx.x < C.np) pr[threadIdx.x] = lm_pen_res(C, xs, threadIdx.x);
+      for (int j = threadIdx.x; j < C.np; j += blockDim.x) pr[j] = lm_pen_res(C, xs, j);
       __syncthreads();
     }
-    if (threadIdx.x < C.np) Sl.pen[(size_t)s * C.np + threadIdx.x] = pr[threadIdx.x];
+    for (int j = threadIdx.x; j < C.np; j += blockDim.x) Sl.pen[(size_t)s * C.np + j] = pr[j];
   }
   if ((fin || early) && C.fallback > 0.0 && C.fb_model && target && !Sl.restarted[s] &&
       st[1] > C.fallback * target[p]) {
@@ -608,13 +625,13 @@ __global__ void __launch_bounds__(128) k_lm_update(LMConf C, LMSlots Sl, const d
   for (int rp = 1; rp <= 8; ++rp) {
     const int nj = C.nodes_ref[rp - 1];
     if (nj <= 0) continue;
-    const int row = C.row_of[j0];
+    const int row = lm_row(C, j0);
     float* ip = m + row * nz;
     const double fac = c_lm_norm[rp - 1], absl = c_lm_norm[rp - 1] * MPERT;
     const double inf = c_lm_low[rp - 1], sup = c_lm_upp[rp - 1];
     // CONTRACT_VECTOR of the current profile, clip of the node deltas
-    if (threadIdx.x < nj) {
-      const int j = j0 + threadIdx.x;
+    for (int jj = threadIdx.x; jj < nj; jj += blockDim.x) {
+      const int j = j0 + jj;
       double a = 0.0, cs = 0.0;
       for (int k = 0; k < nz; ++k) {
         const double c = coef[k * np + j];
@@ -626,9 +643,9 @@ __global__ void __launch_bounds__(128) k_lm_update(LMConf C, LMSlots Sl, const d
       if (a == 0.0) pr = absl;
       double t = delta[j] * fac;
       if (fabs(t) > pr) t = t / fabs(t) * pr;
-      avg[threadIdx.x] = a;
-      itd[threadIdx.x] = t;
-      csum[threadIdx.x] = cs;
+      avg[jj] = a;
+      itd[jj] = t;
+      csum[jj] = cs;
     }
     __syncthreads();
     if (C.node_exp == 2) {
@@ -653,11 +670,11 @@ __global__ void __launch_bounds__(128) k_lm_update(LMConf C, LMSlots Sl, const d
     }
     __syncthreads();
     // ITDELTA = CONTRACT(REAL(NZPERT))
-    if (C.node_exp != 2 && threadIdx.x < nj) {
-      const int j = j0 + threadIdx.x;
+    for (int jj = threadIdx.x; C.node_exp != 2 && jj < nj; jj += blockDim.x) {
+      const int j = j0 + jj;
       double a = 0.0;
       for (int k = 0; k < nz; ++k) a += (double)(float)nzp[k] * coef[k * np + j];
-      itd[threadIdx.x] = a / csum[threadIdx.x];
+      itd[jj] = a / csum[jj];
     }
     __syncthreads();
     // NZPERT = EXPAND(ITDELTA), limits

@@ -5,9 +5,8 @@ and line database): test_syn1 (synthesis of test_atmos.bin, 500 wavelengths
 of Fe I 6301.5 blended with 6302.5, 256 heights), test_rf (with the
 response functions to T and Bz at every height), test_he (hydrostatic
 equilibrium only) and test_tau1 (log tau5).  The files written equal the
-library's direct calls on the same model; test_inv1's last cycle frees 256
-heights of T and v_z (NP = 512), beyond the inversion's 16 nodes, and is
-refused."""
+library's direct calls on the same model.  test_inv1 (NP = 512) runs in
+tests/test_gpu_lm_big.py."""
 import os
 import shutil
 import sys
@@ -73,6 +72,3 @@ def test_reference_test_cases_run(fz, tree):
     tau = vo.model_from_cubes(v3io.read_model(out[0]))
     mt, _ = ctx.log_tau5(m, hydrostatic=False)
     np.testing.assert_array_equal(tau[:, 11], mt[:, 11])
-    # test_inv1: NP = 512 in its only cycle
-    with pytest.raises(fz.FzError):
-        control.run(str(t / "test_inv1" / "control_file.dat"))
