@@ -333,8 +333,9 @@ def main():
         obs[i:i + n] = syn.reshape(n, nf) + 1e-3 * torch.randn((n, nf), dtype=torch.float64, device="cuda",
                                                                generator=gen)
         true_models[i:i + n] = mo
-    obs32 = obs.float()
     base = torch.from_numpy(ws.default_models(a.tile, a.nz)).cuda()
+    base1 = base[0].contiguous()                      # the one default model the warm start moves
+    nn_init = torch.empty_like(base)
     # --------------------------------------------------------------- network
     t0 = time.perf_counter()
     x, t = warm.make_training_set(ctx, a.train_pairs, seed=31 + rank, noise=1e-3)
@@ -394,7 +395,9 @@ def main():
             init.copy_(base)
             ctx.set_tau_device(tau_nx, tau_ny, o.data_ptr(), init.data_ptr(), ("temp", "bvec", "vlos"), stream=stream)
         else:
-            init = warm.initial_models_device(obs32[k * a.tile:(k + 1) * a.tile], base)
+            # network + node expansion in the library (fz_warm_start_device)
+            init = nn_init
+            warm.models_device(ctx, a.tile, o.data_ptr(), base1.data_ptr(), init.data_ptr(), stream=stream)
         tgt = targets[k].data_ptr() if arm in ("nn", "raw") else 0
         ctx.invert_device(a.tile, o.data_ptr(), init.data_ptr(), outs[(arm, k)].data_ptr(), bufs["chi"].data_ptr(),
                           bufs["it"].data_ptr(), bufs["st"].data_ptr(), hydrostatic=True,
@@ -481,11 +484,18 @@ def main():
     def tiles(src):
         return torch.cat([src(k) for k in common])
 
+    def prior_models(k):
+        m_ = torch.empty_like(base)
+        warm.models_device(ctx, a.tile, obs[k * a.tile:(k + 1) * a.tile].data_ptr(), base1.data_ptr(), m_.data_ptr(),
+                           stream=stream)
+        torch.cuda.synchronize()
+        return m_
+
     tru_c = tiles(lambda k: true_models[k * a.tile:(k + 1) * a.tile])
     errors = {arm: height_errors(tiles(lambda k: outs[(arm, k)]), tru_c)
               for arm in ("plain", "nn", "free", "raw", "tau")}
     errors["nn_prior"] = height_errors(
-        tiles(lambda k: warm.initial_models_device(obs32[k * a.tile:(k + 1) * a.tile], base)), tru_c)
+        tiles(lambda k: prior_models(k)), tru_c)
     errors["default_guess"] = height_errors(base[:1].expand(tru_c.shape[0], -1, -1), tru_c)
     errors["heights_compared_per_pixel"] = float(((tru_c[:, 11] >= -3.0) & (tru_c[:, 11] <= 0.0)).sum()
                                                  / tru_c.shape[0])

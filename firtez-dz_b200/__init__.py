@@ -603,6 +603,58 @@ class Synthesis:
                                _p(chi), _p(it), None if syn is None else _p(syn), _p(st)))
         return (mo, chi, it, st, syn) if want_syn else (mo, chi, it, st)
 
+    def set_tau_shard_device(self, nx, ny, obs_ptr, models_ptr, assist, reduce, hydrostatic=True, stream=0):
+        """fz_set_tau_shard_device: SET_TAU on a shard of a field split by x,
+        the field sums and maxima through reduce(kind, data, n, nx) on a
+        numpy view of the library's buffer (see parallel.FieldShard)."""
+        L = lib()
+        if not hasattr(L, "_reduce_t"):
+            L._reduce_t = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_double),
+                                           ctypes.c_int, ctypes.c_int)
+            L.fz_set_tau_shard_device.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_void_p,
+                                                  ctypes.c_void_p, ctypes.c_int, ctypes.c_int, L._reduce_t,
+                                                  ctypes.c_void_p, ctypes.c_void_p]
+
+        def cb(user, kind, data, n, nx_):
+            try:
+                view = np.ctypeslib.as_array(data, shape=(max(n * nx_, 3),))
+                return int(reduce(int(kind), view, int(n), int(nx_)))
+            except Exception:
+                return -1
+
+        fn = L._reduce_t(cb)
+        _check(L.fz_set_tau_shard_device(self._h, int(nx), int(ny), ctypes.c_void_p(obs_ptr),
+                                         ctypes.c_void_p(models_ptr), assist_bits(assist) if not isinstance(assist, int)
+                                         else int(assist), int(bool(hydrostatic)), fn, None,
+                                         ctypes.c_void_p(stream) if stream else None))
+
+    def invert_warm(self, obs, warm, base=None, hydrostatic=True, opts=None, target=None, out=None):
+        """fz_invert_warm: the learned initial guess and the batched LM from
+        host observations (npix, 4, numw) float64, which cross to the device
+        once; warm is a trained warmstart.WarmStart for this node layout,
+        base one MODEL(NZ,13) (default: warmstart.default_models).  out:
+        optional (models, chi2, iterations, status) host arrays.  Returns
+        (models, chi2, iterations, status)."""
+        from . import warmstart as ws
+        ws._bind()
+        o = np.ascontiguousarray(obs, dtype=np.float64)
+        npix = o.shape[0]
+        if o.shape[1:] != (4, self.numw):
+            raise ValueError("obs must be (npix, 4, numw)")
+        b = np.ascontiguousarray(ws.default_models(1, self.nz)[0] if base is None else base, dtype=np.float32)
+        if getattr(warm, "_hnorm", None) is None:
+            warm._hnorm = warm.norm()
+        tg = None if target is None else np.ascontiguousarray(target, dtype=np.float64)
+        if out is None:
+            out = (np.empty((npix, 13, self.nz), dtype=np.float32), np.zeros(npix), np.zeros(npix, dtype=np.int32),
+                   np.zeros(npix, dtype=np.int32))
+        mo, chi, it, st = out
+        opts = opts or LMOpts()
+        _check(lib().fz_invert_warm(self._h, warm.mlp._h, _p(warm._hnorm), _p(b), npix, _p(o),
+                                    None if tg is None else _p(tg), int(bool(hydrostatic)), ctypes.byref(opts),
+                                    _p(mo), _p(chi), _p(it), None, _p(st)))
+        return mo, chi, it, st
+
     def invert_device(self, npix, obs_ptr, init_ptr, model_out_ptr, chi2_ptr, iters_ptr, status_ptr=0, syn_ptr=0,
                       hydrostatic=True, opts=None, stream=0, target_ptr=0):
         """Batched LM inversion on device pointers (target_ptr: optional

@@ -1683,6 +1683,10 @@ struct fz_ctx {
   std::vector<double> nhss_host;
   double* d_svd = nullptr;     // per-slot SVD scratch (2 np^2)
   size_t svd_len = 0;
+  float* d_wsy = nullptr;      // warm start: network outputs (npix, np), normalisation, base model
+  size_t wsy_len = 0;
+  float* d_wsnorm = nullptr;
+  size_t wsnorm_len = 0;
 };
 
 namespace {
@@ -2301,6 +2305,44 @@ bool int_coefs(int nz, int nj, std::vector<double>& coef) {
 __global__ void k_f64_to_f32(size_t n, const double* __restrict__ a, float* __restrict__ b) {
   for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
     b[i] = (float)a[i];
+}
+
+// Warm-start models, one CTA per pixel: the network's outputs y (node order
+// of the layout, standardised) become node values v = y tsd + tmu, and each
+// free parameter's row of the base model (13, nz) is moved by
+// EXPAND(v - CONTRACT(base)) -- the way the inversion perturbs a model
+// (CONTRACT_VECTOR / EXPAND_VECTOR, src/get_dmodel.f90:839-880); the other
+// rows are the base model's.  coef: the (nz, np) hat table in FP32.
+__global__ void __launch_bounds__(128) k_ws_expand(int npix, int nz, RFConf R, const float* __restrict__ coef,
+                                                   const float* __restrict__ y, const float* __restrict__ tmu,
+                                                   const float* __restrict__ tsd, const float* __restrict__ base,
+                                                   float* __restrict__ out) {
+  extern __shared__ float wsv[];   // np node offsets v - CONTRACT(base)
+  static const int kRow[NSLOT] = {0, 1, 5, 6, 7, 10};   // model rows of T, Pg, Bx, By, Bz, v_z
+  const int pix = blockIdx.x;
+  const int np = R.np;
+  float* m = out + (size_t)pix * 13 * nz;
+  for (int i = threadIdx.x; i < 13 * nz; i += blockDim.x) m[i] = base[i];
+  for (int j = threadIdx.x; j < np; j += blockDim.x) {
+    int p = 0;
+    while (p < NSLOT - 1 && j >= R.n0[p] + R.nj[p]) ++p;
+    const float* b = base + kRow[p] * nz;
+    float a = 0.0f, cs = 0.0f;
+    for (int k = 0; k < nz; ++k) cs += coef[(size_t)k * np + j];
+    for (int k = 0; k < nz; ++k) a += b[k] * (coef[(size_t)k * np + j] / cs);
+    wsv[j] = fmaf(y[(size_t)pix * np + j], tsd[j], tmu[j]) - a;
+  }
+  __syncthreads();
+  for (int p = 0; p < NSLOT; ++p) {
+    if (R.nj[p] == 0) continue;
+    float* row = m + kRow[p] * nz;
+    const float* b = base + kRow[p] * nz;
+    for (int k = threadIdx.x; k < nz; k += blockDim.x) {
+      float d = 0.0f;
+      for (int j = R.n0[p]; j < R.n0[p] + R.nj[p]; ++j) d = fmaf(wsv[j], coef[(size_t)k * np + j], d);
+      row[k] = b[k] + d;
+    }
+  }
 }
 
 // The formal solution alone on given absorption matrices (SET_BOUNDARY +
@@ -2967,6 +3009,11 @@ int fz_lsf_clear(fz_ctx* c) {
 
 int fz_set_tau_device(fz_ctx* c, int nx, int ny, const double* d_obs, float* d_models, int assist, int hydrostatic,
                       void* stream) {
+  return fz_set_tau_shard_device(c, nx, ny, d_obs, d_models, assist, hydrostatic, nullptr, nullptr, stream);
+}
+
+int fz_set_tau_shard_device(fz_ctx* c, int nx, int ny, const double* d_obs, float* d_models, int assist,
+                            int hydrostatic, fz_field_reduce_fn reduce, void* user, void* stream) {
   if (!c || nx <= 0 || ny <= 0 || !d_obs || !d_models || (assist & ~15)) return FZ_ERR_ARG;
   if (assist == 0) return 0;
   const int npix = nx * ny, numw = c->numw, n1 = c->regs[0].numwave, nz = c->nz;
@@ -2983,11 +3030,25 @@ int fz_set_tau_device(fz_ctx* c, int nx, int ny, const double* d_obs, float* d_m
     if ((rc = cuda_fail(cudaMalloc(&d_mx, 3 * sizeof(unsigned long long))))) break;
     double* d_tot = d_part + (size_t)nx * n1;
     k_tau_ysum<<<(nx * n1 + 255) / 256, 256, 0, s>>>(nx, ny, numw, n1, d_obs, d_part);
-    k_tau_xsum<<<(n1 + 127) / 128, 128, 0, s>>>(nx, n1, d_part, d_tot);
-    if ((rc = cuda_fail(cudaGetLastError()))) break;
-    std::vector<double> v(3 * (size_t)n1);
-    if ((rc = cuda_fail(cudaMemcpyAsync(v.data(), d_tot, n1 * sizeof(double), cudaMemcpyDeviceToHost, s)))) break;
-    if ((rc = cuda_fail(cudaStreamSynchronize(s)))) break;
+    std::vector<double> v(std::max<size_t>(3 * (size_t)n1, (size_t)nx * n1));
+    if (reduce) {
+      // a shard of a field split by x: this shard's column sums to the host,
+      // the field total (every shard's columns summed in field x order) back
+      if ((rc = cuda_fail(cudaMemcpyAsync(v.data(), d_part, (size_t)nx * n1 * sizeof(double), cudaMemcpyDeviceToHost,
+                                          s))))
+        break;
+      if ((rc = cuda_fail(cudaStreamSynchronize(s)))) break;
+      if (reduce(user, 0, v.data(), n1, nx) != 0) {
+        rc = FZ_ERR_STATE;
+        break;
+      }
+    } else {
+      k_tau_xsum<<<(n1 + 127) / 128, 128, 0, s>>>(nx, n1, d_part, d_tot);
+      if ((rc = cuda_fail(cudaGetLastError()))) break;
+      if ((rc = cuda_fail(cudaMemcpyAsync(v.data(), d_tot, n1 * sizeof(double), cudaMemcpyDeviceToHost, s)))) break;
+      if ((rc = cuda_fail(cudaStreamSynchronize(s)))) break;
+    }
+    std::fill(v.begin() + n1, v.end(), 0.0);
     // VECTORS(:,1..3): the normalised field sum and its two centred
     // derivatives, end points copied, each over SUM(ABS(.)) (:522-534)
     auto norm1 = [&](double* a) {
@@ -3008,12 +3069,28 @@ int fz_set_tau_device(fz_ctx* c, int nx, int ny, const double* d_obs, float* d_m
     norm1(v3);
     double kol = 0.0;   // KOL = VECTORS(:,2) . VECTORS(:,1) (:613)
     for (int j = 0; j < n1; ++j) kol += v2[j] * v1[j];
-    if ((rc = cuda_fail(cudaMemcpyAsync(d_vec, v.data(), v.size() * sizeof(double), cudaMemcpyHostToDevice, s))))
+    if ((rc = cuda_fail(cudaMemcpyAsync(d_vec, v.data(), 3 * (size_t)n1 * sizeof(double), cudaMemcpyHostToDevice,
+                                        s))))
       break;
     const int wblocks = (int)(((size_t)npix * 32 + 255) / 256);
     k_tau_proj<<<wblocks, 256, 0, s>>>(npix, numw, n1, d_obs, d_vec, d_proj);
     if ((rc = cuda_fail(cudaMemsetAsync(d_mx, 0, 3 * sizeof(unsigned long long), s)))) break;
     k_tau_max<<<grid_for(npix, 256), 256, 0, s>>>(npix, kol, d_proj, d_mx);
+    if (reduce) {
+      // the field maxima over every shard (non-negative doubles)
+      unsigned long long hm[3];
+      if ((rc = cuda_fail(cudaMemcpyAsync(hm, d_mx, sizeof(hm), cudaMemcpyDeviceToHost, s)))) break;
+      if ((rc = cuda_fail(cudaStreamSynchronize(s)))) break;
+      double dm[3];
+      for (int i = 0; i < 3; ++i) std::memcpy(&dm[i], &hm[i], sizeof(double));
+      if (reduce(user, 1, dm, 3, 1) != 0) {
+        rc = FZ_ERR_STATE;
+        break;
+      }
+      for (int i = 0; i < 3; ++i) std::memcpy(&hm[i], &dm[i], sizeof(double));
+      if ((rc = cuda_fail(cudaMemcpyAsync(d_mx, hm, sizeof(hm), cudaMemcpyHostToDevice, s)))) break;
+      if ((rc = cuda_fail(cudaStreamSynchronize(s)))) break;
+    }
     TauConf C{};
     C.assist = assist;
     C.nz = nz;
@@ -3385,6 +3462,8 @@ int fz_destroy(fz_ctx* c) {
   cudaFree(c->d_nnorm);
   cudaFree(c->d_nhss);
   cudaFree(c->d_svd);
+  cudaFree(c->d_wsy);
+  cudaFree(c->d_wsnorm);
   lm_free(c);
   cudaFree(c->d_q);
   if (c->h_done) cudaFreeHost(c->h_done);
@@ -3932,6 +4011,111 @@ static int lm_perturbation_host(fz_ctx* c, int npix, int np, int nfreq, const do
   cudaFree(d_err);
   cudaFree(d_svd);
   return rc;
+}
+
+int fz_warm_start_device(fz_ctx* c, fz_mlp* mlp, int npix, const double* d_obs, const float* d_norm,
+                         const float* d_base, float* d_models, void* stream) {
+  if (!c || !mlp || npix <= 0 || !d_obs || !d_norm || !d_base || !d_models) return FZ_ERR_ARG;
+  if (c->rf.np <= 0) return FZ_ERR_STATE;
+  const int nf = 4 * c->numw, np = c->rf.np;
+  int nin = 0, nout = 0;
+  if (int rc = fz_mlp_io(mlp, &nin, &nout)) return rc;
+  if (nin != nf || nout != np) return FZ_ERR_ARG;
+  FZ_CK(cudaSetDevice(c->device));
+  cudaStream_t s = (cudaStream_t)stream;
+  const size_t ny = (size_t)npix * np;
+  if (ny > c->wsy_len) {
+    FZ_CK(cudaStreamSynchronize(s));
+    cudaFree(c->d_wsy);
+    c->d_wsy = nullptr;
+    c->wsy_len = 0;
+    FZ_CK(cudaMalloc(&c->d_wsy, ny * sizeof(float)));
+    c->wsy_len = ny;
+  }
+  if (int rc = fz_mlp_forward_obs_device(mlp, npix, d_obs, d_norm, d_norm + nf, c->d_wsy, stream)) return rc;
+  k_ws_expand<<<npix, 128, np * sizeof(float), s>>>(npix, c->nz, c->rf, c->d_coef, c->d_wsy, d_norm + 2 * nf,
+                                                    d_norm + 2 * nf + np, d_base, d_models);
+  return cuda_fail(cudaGetLastError());
+}
+
+int fz_invert_warm(fz_ctx* c, fz_mlp* mlp, const float* norm, const float* base, int npix, const double* obs,
+                   const double* target_chi2, int hydrostatic, const fz_lm_opts* opts, float* model_out,
+                   double* chi2, int* iters, double* syn_out, int* status) {
+  if (!c || !mlp || !norm || !base || npix <= 0 || !obs || !model_out || !chi2 || !iters) return FZ_ERR_ARG;
+  if (c->rf.np <= 0) return FZ_ERR_STATE;
+  FZ_CK(cudaSetDevice(c->device));
+  const size_t nf = 4 * (size_t)c->numw, nm = 13 * (size_t)c->nz;
+  cudaStream_t s = c->stream;
+  // the staging of fz_invert, grown on demand (a call with no pixels of its
+  // own runs it at zero size first)
+  if ((size_t)npix > c->inv.cap) {
+    FZ_CK(cudaStreamSynchronize(s));
+    const size_t n = npix;
+    inv_free(c);
+    int rc = 0;
+    if (!rc) rc = cuda_fail(cudaMalloc(&c->inv.obs, n * nf * sizeof(double)));
+    if (!rc) rc = cuda_fail(cudaMalloc(&c->inv.init, n * nm * sizeof(float)));
+    if (!rc) rc = cuda_fail(cudaMalloc(&c->inv.out, n * nm * sizeof(float)));
+    if (!rc) rc = cuda_fail(cudaMalloc(&c->inv.chi, n * sizeof(double)));
+    if (!rc) rc = cuda_fail(cudaMalloc(&c->inv.tgt, n * sizeof(double)));
+    if (!rc) rc = cuda_fail(cudaMalloc(&c->inv.it, n * sizeof(int)));
+    if (!rc) rc = cuda_fail(cudaMalloc(&c->inv.st, n * sizeof(int)));
+    if (rc) {
+      inv_free(c);
+      return rc;
+    }
+    c->inv.cap = n;
+  }
+  if (syn_out && !c->inv.syn) FZ_CK(cudaMalloc(&c->inv.syn, c->inv.cap * nf * sizeof(double)));
+  if (syn_out) c->inv.has_syn = true;
+  const size_t nnorm = 2 * nf + 2 * (size_t)c->rf.np + nm;   // normalisation, then the base model
+  if (nnorm > c->wsnorm_len) {
+    cudaFree(c->d_wsnorm);
+    c->d_wsnorm = nullptr;
+    c->wsnorm_len = 0;
+    FZ_CK(cudaMalloc(&c->d_wsnorm, nnorm * sizeof(float)));
+    c->wsnorm_len = nnorm;
+  }
+  const size_t nn = 2 * nf + 2 * (size_t)c->rf.np;
+  FZ_CK(cudaMemcpyAsync(c->d_wsnorm, norm, nn * sizeof(float), cudaMemcpyHostToDevice, s));
+  FZ_CK(cudaMemcpyAsync(c->d_wsnorm + nn, base, nm * sizeof(float), cudaMemcpyHostToDevice, s));
+  FZ_CK(cudaMemcpyAsync(c->inv.obs, obs, npix * nf * sizeof(double), cudaMemcpyHostToDevice, s));
+  if (target_chi2)
+    FZ_CK(cudaMemcpyAsync(c->inv.tgt, target_chi2, npix * sizeof(double), cudaMemcpyHostToDevice, s));
+  // the warm-start models straight into the inversion's initial models
+  if (int rc = fz_warm_start_device(c, mlp, npix, c->inv.obs, c->d_wsnorm, c->d_wsnorm + nn, c->inv.init, s))
+    return rc;
+  fz_lm_opts o{};
+  if (opts) o = *opts;
+  if (opts && opts->fallback_model) {
+    if (!c->inv.fb) FZ_CK(cudaMalloc(&c->inv.fb, nm * sizeof(float)));
+    FZ_CK(cudaMemcpyAsync(c->inv.fb, opts->fallback_model, nm * sizeof(float), cudaMemcpyHostToDevice, s));
+    o.fallback_model = c->inv.fb;
+  }
+  if (opts && opts->state_out) {
+    if ((size_t)npix > c->inv.state_cap) {
+      cudaFree(c->inv.state);
+      c->inv.state = nullptr;
+      c->inv.state_cap = 0;
+      FZ_CK(cudaMalloc(&c->inv.state, (size_t)npix * 5 * sizeof(double)));
+      c->inv.state_cap = npix;
+    }
+    o.state_out = c->inv.state;
+  }
+  int rc = fz_invert_device(c, npix, c->inv.obs, c->inv.init, target_chi2 ? c->inv.tgt : nullptr, hydrostatic,
+                            opts ? &o : nullptr, c->inv.out, c->inv.chi, c->inv.it, syn_out ? c->inv.syn : nullptr,
+                            c->inv.st, s);
+  if (rc) return rc;
+  FZ_CK(cudaMemcpyAsync(model_out, c->inv.out, npix * nm * sizeof(float), cudaMemcpyDeviceToHost, s));
+  FZ_CK(cudaMemcpyAsync(chi2, c->inv.chi, npix * sizeof(double), cudaMemcpyDeviceToHost, s));
+  FZ_CK(cudaMemcpyAsync(iters, c->inv.it, npix * sizeof(int), cudaMemcpyDeviceToHost, s));
+  if (status) FZ_CK(cudaMemcpyAsync(status, c->inv.st, npix * sizeof(int), cudaMemcpyDeviceToHost, s));
+  if (syn_out) FZ_CK(cudaMemcpyAsync(syn_out, c->inv.syn, npix * nf * sizeof(double), cudaMemcpyDeviceToHost, s));
+  if (opts && opts->state_out)
+    FZ_CK(cudaMemcpyAsync(opts->state_out, c->inv.state, (size_t)npix * 5 * sizeof(double), cudaMemcpyDeviceToHost,
+                          s));
+  FZ_CK(cudaStreamSynchronize(s));
+  return 0;
 }
 
 int fz_lm_perturbation(fz_ctx* c, int npix, int np, int nfreq, const double* jac, const double* diff,

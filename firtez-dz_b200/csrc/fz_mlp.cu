@@ -1,8 +1,8 @@
 // Warm-start network of the inversion: an MLP from the observed Stokes vector
 // to the node values of the model, trained and run with hand-written BF16
-// kernels (sm_100a): tensor-core GEMMs (mma.sync m16n8k16 bf16, FP32
-// accumulation) with fused bias / GELU / GELU' epilogues, an MSE loss kernel
-// and Adam on FP32 master weights.  It has no counterpart in the reference,
+// kernels (sm_100a): tcgen05 tensor-core GEMMs (bf16 operands, FP32
+// accumulation in tensor memory) with fused bias / GELU / GELU' epilogues,
+// an MSE loss kernel and Adam on FP32 master weights.  It has no counterpart in the reference,
 // whose initial guess is the model in the control file (or the Stokes-moment
 // assists of SET_TAU, src/invert3d.f90:492-727).
 //
@@ -18,10 +18,10 @@
 #include <vector>
 
 #include "../../include/fz_b200.h"
+#include "fz_tc.cuh"
 
 namespace {
 
-constexpr int BM = 128, BN = 128, BK = 32, SK = BK + 8;   // smem row stride (bf16) avoids bank conflicts
 constexpr int MLP_MAXL = 8;
 
 enum GemmMode { NT = 0, NN = 1, TN = 2 };
@@ -34,104 +34,148 @@ __device__ __forceinline__ float gelu_d(float z) {
   return cdf + z * pdf;
 }
 
-__device__ __forceinline__ void mma16816(float c[4], const unsigned a[4], const unsigned b[2]) {
-  asm volatile(
-      "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
-      "{%0,%1,%2,%3};\n"
-      : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
-      : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b[0]), "r"(b[1]));
-}
-
-// Element (m, k) of the logical A (M x K) and (n, k) of the logical B^T
-// (N x K) for each mode:
+// C (M x N) = A B^T with the logical operands of each mode:
 //   NT: A[m][k] = a[m*lda + k],  B[n][k] = b[n*ldb + k]   (Y = X W^T)
 //   NN: A[m][k] = a[m*lda + k],  B[n][k] = b[k*ldb + n]   (dX = dZ W)
 //   TN: A[m][k] = a[k*lda + m],  B[n][k] = b[k*ldb + n]   (dW = dZ^T X)
-template <int MODE>
-__device__ __forceinline__ __nv_bfloat16 ldA(const __nv_bfloat16* a, int lda, int m, int k, int M, int K) {
-  if (m >= M || k >= K) return __float2bfloat16(0.0f);
-  return MODE == TN ? a[(size_t)k * lda + m] : a[(size_t)m * lda + k];
-}
-template <int MODE>
-__device__ __forceinline__ __nv_bfloat16 ldB(const __nv_bfloat16* b, int ldb, int n, int k, int N, int K) {
-  if (n >= N || k >= K) return __float2bfloat16(0.0f);
-  return MODE == NT ? b[(size_t)n * ldb + k] : b[(size_t)k * ldb + n];
-}
-
-// C (M x N) = A B^T with the logical operands above; 256 threads, 128x128
-// tile, 8 warps as 2 (m) x 4 (n), each warp 64 x 32 = 4 x 4 mma tiles.
-// Epilogues:
+// and the epilogues
 //   EPI_FWD_GELU: z = C + bias[n] -> zout (fp32, pre-activation), out = bf16(gelu(z))
 //   EPI_FWD_LIN : z = C + bias[n] -> fout (fp32)
 //   EPI_BWD_GELU: out = bf16(C * gelu'(zin[m][n]))
 //   EPI_F32     : fout = C (fp32)
-template <int MODE, int EPI>
-__global__ void __launch_bounds__(256) k_gemm(int M, int N, int K, const __nv_bfloat16* __restrict__ A, int lda,
-                                              const __nv_bfloat16* __restrict__ B, int ldb,
-                                              const float* __restrict__ bias, const float* __restrict__ zin,
-                                              float* __restrict__ zout, float* __restrict__ fout,
-                                              __nv_bfloat16* __restrict__ out, int ldc) {
-  __shared__ __align__(16) __nv_bfloat16 As[BM][SK];
-  __shared__ __align__(16) __nv_bfloat16 Bs[BN][SK];
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const int wm = warp >> 2, wn = warp & 3;   // warp tile origin: (wm*64, wn*32)
-  const int m0 = blockIdx.y * BM, n0 = blockIdx.x * BN;
-  const int grp = lane >> 2, t4 = lane & 3;
-  float acc[4][4][4];
+// on the fifth-generation tensor cores (tcgen05): a 128 x 128
+// output tile per CTA of 256 threads, K in blocks of 64 staged into shared
+// memory in the canonical K-major layout (fz_tc.cuh) through three buffers,
+// one elected thread issuing tcgen05.mma (bf16 x bf16 -> FP32 in tensor
+// memory) and committing each block to the buffer's mbarrier, the epilogue
+// read back with tcgen05.ld (warps w and w + 4 share TMEM lanes 32 (w % 4)..,
+// columns 0-63 and 64-127).  Operands whose leading dimension allows it move
+// in 16-byte vectors, the others element by element.
+constexpr int TC_BK = 64, TC_NKC = TC_BK / 8, TC_STAGES = 3;
+constexpr int TC_TILE = 128 * TC_BK * 2;                      // one 128 x 64 bf16 tile
+constexpr size_t TC_SMEM = (size_t)TC_STAGES * 2 * TC_TILE;   // A and B per stage: 96 KB
+constexpr unsigned long long TC_WAIT_NS = 2000000000ull;
+
+// Rows [row0, row0 + 128) x K [k0, k0 + 64) of a logical operand X (R x K)
+// stored K-contiguous (X[r * ld + k], kcont) or row-contiguous (X[k * ld +
+// r]) into the K-major tile dst; out-of-range elements are zero.
+__device__ __forceinline__ void tc_stage(const __nv_bfloat16* __restrict__ X, int ld, bool kcont, bool vec, int row0,
+                                         int k0, int R, int K, unsigned char* dst) {
+  const unsigned short* x = reinterpret_cast<const unsigned short*>(X);
+  if (kcont) {
+    for (int i = threadIdx.x; i < 128 * (TC_BK / 8); i += blockDim.x) {
+      const int r = i / (TC_BK / 8), c = i % (TC_BK / 8);
+      const int gr = row0 + r, gk = k0 + 8 * c;
+      uint4 v = make_uint4(0u, 0u, 0u, 0u);
+      if (gr < R) {
+        const unsigned short* src = x + (size_t)gr * ld + gk;
+        if (vec && gk + 8 <= K) {
+          v = *reinterpret_cast<const uint4*>(src);
+        } else {
+          unsigned short e[8];
 #pragma unroll
-  for (int i = 0; i < 4; ++i)
-#pragma unroll
-    for (int j = 0; j < 4; ++j)
-#pragma unroll
-      for (int e = 0; e < 4; ++e) acc[i][j][e] = 0.0f;
-  for (int k0 = 0; k0 < K; k0 += BK) {
-    // stage: 128 x 32 elements of A and of B^T, 16 per thread
-    for (int i = tid; i < BM * BK; i += 256) {
-      // walk the contiguous global direction with consecutive threads
-      int r, c;
-      if (MODE == TN) { c = i / BM; r = i % BM; } else { r = i / BK; c = i % BK; }
-      As[r][c] = ldA<MODE>(A, lda, m0 + r, k0 + c, M, K);
+          for (int j = 0; j < 8; ++j) e[j] = gk + j < K ? src[j] : (unsigned short)0;
+          v = make_uint4(e[0] | ((unsigned)e[1] << 16), e[2] | ((unsigned)e[3] << 16), e[4] | ((unsigned)e[5] << 16),
+                         e[6] | ((unsigned)e[7] << 16));
+        }
+      }
+      *reinterpret_cast<uint4*>(dst + fztc::kmajor_offset(r, 8 * c, TC_NKC)) = v;
     }
-    for (int i = tid; i < BN * BK; i += 256) {
-      int r, c;
-      if (MODE == NT) { r = i / BK; c = i % BK; } else { c = i / BN; r = i % BN; }
-      Bs[r][c] = ldB<MODE>(B, ldb, n0 + r, k0 + c, N, K);
-    }
-    __syncthreads();
+  } else {
+    for (int i = threadIdx.x; i < TC_BK * 16; i += blockDim.x) {
+      const int kk = i / 16, c = i % 16;   // eight consecutive rows 8c.. at one k
+      const int gk = k0 + kk, gr = row0 + 8 * c;
+      unsigned short e[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+      if (gk < K) {
+        const unsigned short* src = x + (size_t)gk * ld + gr;
+        if (vec && gr + 8 <= R) {
+          const uint4 v = *reinterpret_cast<const uint4*>(src);
+          e[0] = v.x & 0xffff; e[1] = v.x >> 16; e[2] = v.y & 0xffff; e[3] = v.y >> 16;
+          e[4] = v.z & 0xffff; e[5] = v.z >> 16; e[6] = v.w & 0xffff; e[7] = v.w >> 16;
+        } else {
 #pragma unroll
-    for (int kk = 0; kk < BK; kk += 16) {
-      unsigned af[4][4], bf[4][2];
-#pragma unroll
-      for (int i = 0; i < 4; ++i) {
-        const int r = wm * 64 + i * 16 + grp;
-        af[i][0] = *reinterpret_cast<const unsigned*>(&As[r][kk + 2 * t4]);
-        af[i][1] = *reinterpret_cast<const unsigned*>(&As[r + 8][kk + 2 * t4]);
-        af[i][2] = *reinterpret_cast<const unsigned*>(&As[r][kk + 2 * t4 + 8]);
-        af[i][3] = *reinterpret_cast<const unsigned*>(&As[r + 8][kk + 2 * t4 + 8]);
+          for (int j = 0; j < 8; ++j) e[j] = gr + j < R ? src[j] : (unsigned short)0;
+        }
       }
 #pragma unroll
-      for (int j = 0; j < 4; ++j) {
-        const int n = wn * 32 + j * 8 + grp;
-        bf[j][0] = *reinterpret_cast<const unsigned*>(&Bs[n][kk + 2 * t4]);
-        bf[j][1] = *reinterpret_cast<const unsigned*>(&Bs[n][kk + 2 * t4 + 8]);
-      }
-#pragma unroll
-      for (int i = 0; i < 4; ++i)
-#pragma unroll
-        for (int j = 0; j < 4; ++j) mma16816(acc[i][j], af[i], bf[j]);
+      for (int j = 0; j < 8; ++j)
+        *reinterpret_cast<unsigned short*>(dst + fztc::kmajor_offset(8 * c + j, kk, TC_NKC)) = e[j];
     }
-    __syncthreads();
   }
+}
+
+template <int MODE, int EPI>
+__global__ void __launch_bounds__(256, 1) k_gemm_tc(int M, int N, int K, const __nv_bfloat16* __restrict__ A, int lda,
+                                                    const __nv_bfloat16* __restrict__ B, int ldb,
+                                                    const float* __restrict__ bias, const float* __restrict__ zin,
+                                                    float* __restrict__ zout, float* __restrict__ fout,
+                                                    __nv_bfloat16* __restrict__ out, int ldc, int* __restrict__ err) {
+  extern __shared__ __align__(1024) unsigned char tsm[];
+  __shared__ __align__(8) uint64_t mbar[TC_STAGES];
+  __shared__ uint32_t tbase;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int m0 = blockIdx.y * 128, n0 = blockIdx.x * 128;
+  // A: NT, NN K-contiguous rows of a (M x K); TN the transpose.  B: NT
+  // K-contiguous rows of b (N x K); NN, TN the transpose.
+  const bool akc = MODE != TN, bkc = MODE == NT;
+  const bool avec = (lda % 8) == 0 && (((uintptr_t)A) & 15) == 0;
+  const bool bvec = (ldb % 8) == 0 && (((uintptr_t)B) & 15) == 0;
+  if (warp == 0) {
+    fztc::tmem_alloc(&tbase, 128);
+    fztc::tmem_relinquish();
+  }
+  if (tid == 0) {
+    for (int i = 0; i < TC_STAGES; ++i) fztc::mbar_init(&mbar[i], 1);
+    fztc::fence_mbar_init();
+  }
+  fztc::fence_before_sync();
+  __syncthreads();
+  fztc::fence_after_sync();
+  const uint32_t tmem = tbase;
+  const uint32_t idesc = fztc::idesc_bf16(128, 128);
+  const int nkb = (K + TC_BK - 1) / TC_BK;
+  bool ok = true;
+  for (int kb = 0; kb < nkb && ok; ++kb) {
+    const int buf = kb % TC_STAGES;
+    unsigned char* as = tsm + (size_t)buf * 2 * TC_TILE;
+    unsigned char* bs = as + TC_TILE;
+    if (kb >= TC_STAGES) ok = fztc::mbar_wait(&mbar[buf], ((kb - TC_STAGES) / TC_STAGES) & 1, TC_WAIT_NS);
+    ok = __syncthreads_and(ok);
+    if (!ok) break;
+    tc_stage(A, lda, akc, avec, m0, kb * TC_BK, M, K, as);
+    tc_stage(B, ldb, bkc, bvec, n0, kb * TC_BK, N, K, bs);
+    fztc::fence_async_smem();
+    __syncthreads();
+    if (tid == 0) {
+      const uint32_t sa = fztc::smem_addr(as), sb = fztc::smem_addr(bs);
 #pragma unroll
-  for (int i = 0; i < 4; ++i)
+      for (int ks = 0; ks < TC_BK / 16; ++ks) {
+        const uint64_t da = fztc::desc_kmajor(sa + ks * 256, 128, TC_NKC * 128);
+        const uint64_t db = fztc::desc_kmajor(sb + ks * 256, 128, TC_NKC * 128);
+        fztc::mma_bf16(tmem, da, db, idesc, (kb > 0 || ks > 0) ? 1u : 0u);
+      }
+      fztc::commit(&mbar[buf]);
+    }
+  }
+  if (ok && nkb > 0) {
+    const int last = nkb - 1;
+    ok = fztc::mbar_wait(&mbar[last % TC_STAGES], (last / TC_STAGES) & 1, TC_WAIT_NS);
+  }
+  ok = __syncthreads_and(ok);
+  fztc::fence_after_sync();
+  if (ok) {
+    const int q = warp & 3, half = warp >> 2;
+    const int m = m0 + 32 * q + lane;
+#pragma unroll 1
+    for (int cc = 0; cc < 64; cc += 16) {
+      float v[16];
+      fztc::tmem_ld16(tmem + ((uint32_t)(32 * q) << 16) + (uint32_t)(64 * half + cc), v);
+      if (m >= M) continue;
 #pragma unroll
-    for (int j = 0; j < 4; ++j)
-#pragma unroll
-      for (int e = 0; e < 4; ++e) {
-        const int m = m0 + wm * 64 + i * 16 + grp + (e >= 2 ? 8 : 0);
-        const int n = n0 + wn * 32 + j * 8 + 2 * t4 + (e & 1);
-        if (m >= M || n >= N) continue;
-        const float c = acc[i][j][e];
+      for (int i = 0; i < 16; ++i) {
+        const int n = n0 + 64 * half + cc + i;
+        if (n >= N) continue;
+        const float c = v[i];
         const size_t o = (size_t)m * ldc + n;
         if (EPI == EPI_FWD_GELU) {
           const float z = c + bias[n];
@@ -145,6 +189,13 @@ __global__ void __launch_bounds__(256) k_gemm(int M, int N, int K, const __nv_bf
           fout[o] = c;
         }
       }
+    }
+  } else if (tid == 0) {
+    atomicExch(err, 1);
+  }
+  fztc::fence_before_sync();
+  __syncthreads();
+  if (warp == 0) fztc::tmem_dealloc(tmem, 128);
 }
 
 // MSE loss 1/(n*nout) sum (y - t)^2 and dL/dy in bf16
@@ -195,6 +246,16 @@ __global__ void k_colsum(int n, int m, const __nv_bfloat16* __restrict__ dz, flo
 __global__ void k_to_bf16(size_t n, const float* __restrict__ x, __nv_bfloat16* __restrict__ y) {
   for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
     y[i] = __float2bfloat16_rn(x[i]);
+}
+
+// Observed Stokes rows (n x d, FP64, GAIN-normalised) standardised with the
+// training set's mean and spread, (x - mu) / sd in FP32, as bf16 inputs.
+__global__ void k_obs_bf16(size_t n, int d, const double* __restrict__ x, const float* __restrict__ mu,
+                           const float* __restrict__ sd, __nv_bfloat16* __restrict__ y) {
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    const int f = (int)(i % d);
+    y[i] = __float2bfloat16_rn(((float)x[i] - mu[f]) / sd[f]);
+  }
 }
 
 // the current batch's rows (n x d) of x as bf16
@@ -265,6 +326,7 @@ struct fz_mlp {
   TrainState* tstate = nullptr;   // device
   int* order = nullptr;           // device batch order of one epoch
   int order_cap = 0;
+  int* d_err = nullptr;           // set by a tensor-core GEMM that gave up waiting for its MMAs
 };
 
 namespace {
@@ -305,10 +367,28 @@ int mlp_reserve(fz_mlp* p, int n) {
 }
 
 template <int MODE, int EPI>
-void gemm(cudaStream_t s, int M, int N, int K, const __nv_bfloat16* A, int lda, const __nv_bfloat16* B, int ldb,
-          const float* bias, const float* zin, float* zout, float* fout, __nv_bfloat16* out, int ldc) {
-  const dim3 grid((N + BN - 1) / BN, (M + BM - 1) / BM);
-  k_gemm<MODE, EPI><<<grid, 256, 0, s>>>(M, N, K, A, lda, B, ldb, bias, zin, zout, fout, out, ldc);
+void gemm(cudaStream_t s, int* err, int M, int N, int K, const __nv_bfloat16* A, int lda, const __nv_bfloat16* B,
+          int ldb, const float* bias, const float* zin, float* zout, float* fout, __nv_bfloat16* out, int ldc) {
+  const dim3 grid((N + 127) / 128, (M + 127) / 128);
+  k_gemm_tc<MODE, EPI><<<grid, 256, TC_SMEM, s>>>(M, N, K, A, lda, B, ldb, bias, zin, zout, fout, out, ldc, err);
+}
+
+// The tensor-core GEMMs' shared memory above the default 48 KB (set once,
+// before any stream capture).
+int gemm_tc_attrs() {
+  cudaError_t e = cudaFuncSetAttribute(k_gemm_tc<NT, EPI_FWD_GELU>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)TC_SMEM);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(k_gemm_tc<NT, EPI_FWD_LIN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TC_SMEM);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(k_gemm_tc<TN, EPI_F32>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TC_SMEM);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(k_gemm_tc<NN, EPI_BWD_GELU>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TC_SMEM);
+  if (e != cudaSuccess) {
+    std::fprintf(stderr, "fz_b200 mlp: CUDA error %s\n", cudaGetErrorString(e));
+    return FZ_ERR_CUDA;
+  }
+  return 0;
 }
 
 // forward of n rows already in act[0]; output in yout
@@ -316,10 +396,10 @@ void mlp_fwd(fz_mlp* p, int n) {
   for (int l = 0; l < p->nl; ++l) {
     const int in = p->dim[l], out = p->dim[l + 1];
     if (l + 1 < p->nl)
-      gemm<NT, EPI_FWD_GELU>(p->stream, n, out, in, p->act[l], in, p->Wb[l], in, p->b[l], nullptr, p->z[l], nullptr,
+      gemm<NT, EPI_FWD_GELU>(p->stream, p->d_err, n, out, in, p->act[l], in, p->Wb[l], in, p->b[l], nullptr, p->z[l], nullptr,
                              p->act[l + 1], out);
     else
-      gemm<NT, EPI_FWD_LIN>(p->stream, n, out, in, p->act[l], in, p->Wb[l], in, p->b[l], nullptr, nullptr, p->yout,
+      gemm<NT, EPI_FWD_LIN>(p->stream, p->d_err, n, out, in, p->act[l], in, p->Wb[l], in, p->b[l], nullptr, nullptr, p->yout,
                             nullptr, out);
   }
 }
@@ -329,11 +409,11 @@ void mlp_bwd(fz_mlp* p, int n) {
   for (int l = p->nl - 1; l >= 0; --l) {
     const int in = p->dim[l], out = p->dim[l + 1];
     // dW (out x in) = dZ^T (out x n) X (n x in)
-    gemm<TN, EPI_F32>(p->stream, out, in, n, p->dz[l], out, p->act[l], in, nullptr, nullptr, nullptr, p->gW[l],
+    gemm<TN, EPI_F32>(p->stream, p->d_err, out, in, n, p->dz[l], out, p->act[l], in, nullptr, nullptr, nullptr, p->gW[l],
                       nullptr, in);
     k_colsum<<<(out + 255) / 256, 256, 0, p->stream>>>(n, out, p->dz[l], p->gb[l]);
     if (l > 0)   // dZ_{l-1} = (dZ_l W_l) * gelu'(z_{l-1})
-      gemm<NN, EPI_BWD_GELU>(p->stream, n, in, out, p->dz[l], out, p->Wb[l], in, nullptr, p->z[l - 1], nullptr,
+      gemm<NN, EPI_BWD_GELU>(p->stream, p->d_err, n, in, out, p->dz[l], out, p->Wb[l], in, nullptr, p->z[l - 1], nullptr,
                              nullptr, p->dz[l - 1], in);
   }
 }
@@ -377,10 +457,26 @@ int fz_mlp_create(fz_mlp** out, int nlayers, const int* dims, unsigned long long
     cudaMemsetAsync(p->vb[l], 0, dims[l + 1] * sizeof(float), p->stream);
   }
   if ((rc = mlp_fail(cudaMalloc(&p->loss, sizeof(float))))) return fail(rc);
+  if ((rc = mlp_fail(cudaMalloc(&p->d_err, sizeof(int))))) return fail(rc);
+  if ((rc = mlp_fail(cudaMemsetAsync(p->d_err, 0, sizeof(int), p->stream)))) return fail(rc);
+  if ((rc = gemm_tc_attrs())) return fail(rc);
   if ((rc = mlp_fail(cudaStreamSynchronize(p->stream)))) return fail(rc);
   *out = p;
   return 0;
 }
+
+namespace {
+// FZ_ERR_CUDA when a tensor-core GEMM of p gave up waiting (after the stream
+// has completed); the flag is cleared.
+int mlp_tc_status(fz_mlp* p) {
+  int e = 0;
+  if (mlp_fail(cudaMemcpy(&e, p->d_err, sizeof(int), cudaMemcpyDeviceToHost))) return FZ_ERR_CUDA;
+  if (!e) return 0;
+  cudaMemset(p->d_err, 0, sizeof(int));
+  std::fprintf(stderr, "fz_b200 mlp: a tensor-core GEMM gave up waiting for its MMAs\n");
+  return FZ_ERR_CUDA;
+}
+}  // namespace
 
 int fz_mlp_destroy(fz_mlp* p) {
   if (!p) return 0;
@@ -402,6 +498,7 @@ int fz_mlp_destroy(fz_mlp* p) {
   for (int l = 0; l <= MLP_MAXL; ++l) cudaFree(p->act[l]);
   cudaFree(p->yout);
   cudaFree(p->loss);
+  cudaFree(p->d_err);
   cudaFree(p->tstate);
   cudaFree(p->order);
   if (p->stream) cudaStreamDestroy(p->stream);
@@ -472,10 +569,50 @@ int fz_mlp_forward_device(fz_mlp* p, int n, const float* d_x, float* d_y, void* 
   }
   cudaEventRecord(ev, s);
   if (stream) cudaStreamWaitEvent((cudaStream_t)stream, ev, 0);
-  const int r2 = mlp_fail(cudaGetLastError());
-  if (!stream) cudaStreamSynchronize(s);
+  int r2 = mlp_fail(cudaGetLastError());
+  if (!stream) {
+    cudaStreamSynchronize(s);
+    if (!r2) r2 = mlp_tc_status(p);
+  }
   cudaEventDestroy(ev);
   return r2;
+}
+
+// Forward of observed Stokes rows: d_obs (n x dim0, FP64) standardised by
+// d_mu, d_sd (dim0, FP32) on the way to bf16, then the network; y (n x
+// dimL, FP32).  Enqueued after the work on `stream`, which waits for it.
+int fz_mlp_forward_obs_device(fz_mlp* p, int n, const double* d_obs, const float* d_mu, const float* d_sd, float* d_y,
+                              void* stream) {
+  if (!p || n <= 0 || !d_obs || !d_mu || !d_sd || !d_y) return FZ_ERR_ARG;
+  MLP_CK(cudaSetDevice(p->device));
+  const int chunk = 16384;
+  int rc = mlp_reserve(p, std::min(n, chunk));
+  if (rc) return rc;
+  cudaStream_t s = p->stream;
+  cudaEvent_t ev;
+  MLP_CK(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+  cudaEventRecord(ev, (cudaStream_t)stream);
+  cudaStreamWaitEvent(s, ev, 0);
+  const int d0 = p->dim[0], dl = p->dim[p->nl];
+  for (int i = 0; i < n; i += chunk) {
+    const int m = std::min(chunk, n - i);
+    k_obs_bf16<<<grid1((size_t)m * d0), 256, 0, s>>>((size_t)m * d0, d0, d_obs + (size_t)i * d0, d_mu, d_sd,
+                                                      p->act[0]);
+    mlp_fwd(p, m);
+    cudaMemcpyAsync(d_y + (size_t)i * dl, p->yout, (size_t)m * dl * sizeof(float), cudaMemcpyDeviceToDevice, s);
+  }
+  cudaEventRecord(ev, s);
+  cudaStreamWaitEvent((cudaStream_t)stream, ev, 0);
+  const int r2 = mlp_fail(cudaGetLastError());
+  cudaEventDestroy(ev);
+  return r2;
+}
+
+int fz_mlp_io(const fz_mlp* p, int* nin, int* nout) {
+  if (!p) return FZ_ERR_ARG;
+  if (nin) *nin = p->dim[0];
+  if (nout) *nout = p->dim[p->nl];
+  return 0;
 }
 
 // Loss and gradients of one batch (no update); loss to *loss (host).
@@ -494,7 +631,7 @@ int fz_mlp_grad_device(fz_mlp* p, int n, const float* d_x, const float* d_t, flo
   MLP_CK(cudaGetLastError());
   if (loss) MLP_CK(cudaMemcpyAsync(loss, p->loss, sizeof(float), cudaMemcpyDeviceToHost, s));
   MLP_CK(cudaStreamSynchronize(s));
-  return 0;
+  return mlp_tc_status(p);
 }
 
 // Mini-batch Adam training over n device rows for `epochs` passes (rows
@@ -569,6 +706,7 @@ int fz_mlp_train_device(fz_mlp* p, int n, const float* d_x, const float* d_t, in
   if (exec) cudaGraphExecDestroy(exec);
   if (graph) cudaGraphDestroy(graph);
   if (!rc) rc = mlp_fail(cudaGetLastError());
+  if (!rc) rc = mlp_tc_status(p);
   if (loss) *loss = last;
   return rc;
 }

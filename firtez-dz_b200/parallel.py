@@ -1,8 +1,9 @@
 """A field split over ranks by x (one process per GPU), for the pieces of the
 inversion that couple pixels: SMOOTHING_B at the start of every cycle
 (src/model_spatial_extension.f90:351-491; its x pass reads the neighbouring
-x columns) -- the only cross-pixel step of the cycle loop; the inversion
-itself and END_CYCLE's synthesis are per pixel.
+x columns) and SET_TAU's assists (src/invert3d.f90:492-727: a field sum of
+Stokes I and three field maxima); the inversion itself and END_CYCLE's
+synthesis are per pixel.
 
 Rank r holds field columns [x0, x1) (a contiguous run of pixels iy + NY ix);
 before smoothing, every rank sends its first and last columns to its
@@ -69,6 +70,52 @@ class FieldShard:
         off = (self.x0 - x0) * self.ny
         local.copy_(ext[off:off + self.nx * self.ny])
 
+    def field_reduce(self):
+        """The two field-wide reductions of SET_TAU for this rank
+        (fz_set_tau_shard_device's reduce): fn(kind, data, n, nx) on a numpy
+        view.  kind 0 -- data[:nx*n] holds this rank's per-column sums
+        (x-major); every rank's columns are gathered in field x order and
+        summed one after another (the order of the whole field's sum), the
+        total left in data[:n]; kind 1 -- data[:3] becomes the maximum over
+        the ranks."""
+        import torch
+        import torch.distributed as dist
+        sizes = [x1 - x0 for x0, x1 in split(self.nx_field, self.world)]
+
+        def device():
+            if self.world == 1:
+                return "cpu"
+            return "cuda" if dist.get_backend(self.group) == "nccl" else "cpu"
+
+        def fn(kind, data, n, nx):
+            if kind == 0:
+                part = np.array(data[:nx * n], dtype=np.float64).reshape(nx, n)
+                if self.world == 1:
+                    rows = part
+                else:
+                    buf = torch.zeros((max(sizes), n), dtype=torch.float64, device=device())
+                    buf[:nx] = torch.from_numpy(part)
+                    got = [torch.empty_like(buf) for _ in range(self.world)]
+                    dist.all_gather(got, buf, group=self.group)
+                    rows = np.concatenate([g.cpu().numpy()[:k] for g, k in zip(got, sizes)])
+                tot = np.zeros(n)
+                for r in rows:
+                    tot = tot + r
+                data[:n] = tot
+            else:
+                t = torch.tensor(np.array(data[:3], dtype=np.float64), device=device())
+                if self.world > 1:
+                    dist.all_reduce(t, op=dist.ReduceOp.MAX, group=self.group)
+                data[:3] = t.cpu().numpy()
+            return 0
+        return fn
+
+    def set_tau(self, ctx, d_obs, d_models, assist, hydrostatic=True, stream=0):
+        """SET_TAU's assists on this rank's pixels, the field sums and maxima
+        over all ranks: equal to the whole field's fz_set_tau."""
+        ctx.set_tau_shard_device(self.nx, self.ny, d_obs.data_ptr(), d_models.data_ptr(), assist,
+                                 self.field_reduce(), hydrostatic=hydrostatic, stream=stream)
+
     def invert_cycles(self, ctx, d_obs, d_models, cycles, hydrostatic=True, opts=None, stream=0):
         """INVERT3D's cycles on this rank's pixels (d_obs (nx*ny, 4, numw)
         float64, d_models (nx*ny, 13, nz) float32, torch tensors on the GPU):
@@ -84,9 +131,15 @@ class FieldShard:
         it = torch.empty(npix, dtype=torch.int32, device=d_models.device)
         st = torch.empty(npix, dtype=torch.int32, device=d_models.device)
         smoother = device_smoother(ctx)
-        for nodes in cycles:
+        assist = (opts.assist & 15) if opts is not None else 0
+        for cy, nodes in enumerate(cycles):
             ctx.rf_nodes(nodes)
             torch.cuda.synchronize()
+            # SET_TAU's assists when neither Pg nor P0 is free, every cycle
+            # or, with PROGRESSIVE, the first (src/invert3d.f90:505-520)
+            if assist and not nodes.get(2, 0) and not nodes.get(8, 0) and (cy == 0 or not opts.assist & 16):
+                self.set_tau(ctx, d_obs, d_models, assist, hydrostatic=bool(hydrostatic), stream=stream)
+                torch.cuda.synchronize()
             self.smooth(d_models, smoother)
             torch.cuda.synchronize()
             ctx.invert_device(npix, d_obs.data_ptr(), d_models.data_ptr(), best.data_ptr(), chi.data_ptr(),

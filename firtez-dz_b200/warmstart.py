@@ -38,6 +38,9 @@ def _bind():
     L.fz_mlp_grad_device.argtypes = [P, ctypes.c_int, P, P, P]
     L.fz_mlp_train_device.argtypes = [P, ctypes.c_int, P, P, ctypes.c_int, ctypes.c_int, ctypes.c_float,
                                       ctypes.c_ulonglong, P]
+    L.fz_mlp_forward_obs_device.argtypes = [P, ctypes.c_int, P, P, P, P, P]
+    L.fz_warm_start_device.argtypes = [P, P, ctypes.c_int, P, P, P, P, P]
+    L.fz_invert_warm.argtypes = [P, P, P, P, ctypes.c_int, P, P, ctypes.c_int, P, P, P, P, P, P]
     L._mlp_bound = True
     return L
 
@@ -213,6 +216,27 @@ class WarmStart:
         torch.cuda.synchronize()
         self.mlp.forward_device(x.shape[0], x.data_ptr(), y.data_ptr())
         return y.cpu().numpy().astype(np.float64) * self.tsd + self.tmu
+
+    def norm(self):
+        """The network's standardisation as the library takes it: FP32 input
+        mean and spread (NFREQ each), node mean and spread (nout each)."""
+        if self.xmu is None:
+            raise FzError("the network has no normalisation: train it first")
+        xm = self.xmu.detach().reshape(-1).float().cpu().numpy() if hasattr(self.xmu, "detach") else self.xmu
+        xs = self.xsd.detach().reshape(-1).float().cpu().numpy() if hasattr(self.xsd, "detach") else self.xsd
+        return np.concatenate([np.ravel(xm), np.ravel(xs), np.ravel(self.tmu), np.ravel(self.tsd)]).astype(np.float32)
+
+    def models_device(self, synth, n, obs_ptr, base_ptr, out_ptr, stream=0):
+        """Warm-start models on the device through fz_warm_start_device:
+        obs_ptr (n, NFREQ) FP64 observations, base_ptr one MODEL(NZ,13)
+        float32, out_ptr (n, 13, nz) float32; the node layout of synth
+        (rf_nodes) must be the network's."""
+        import torch
+        if getattr(self, "_dnorm", None) is None:
+            self._dnorm = torch.from_numpy(self.norm()).cuda()
+        _check(_bind().fz_warm_start_device(synth._h, self.mlp._h, int(n), ctypes.c_void_p(obs_ptr),
+                                            ctypes.c_void_p(self._dnorm.data_ptr()), ctypes.c_void_p(base_ptr),
+                                            ctypes.c_void_p(out_ptr), ctypes.c_void_p(stream) if stream else None))
 
     def initial_models_device(self, x_obs, base):
         """Warm-start models on the device: x_obs (npix, 4*numw) float32 raw

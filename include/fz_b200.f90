@@ -386,6 +386,20 @@ MODULE FZ_B200
       INTEGER(C_INT), VALUE      :: ASSIST
       INTEGER(C_INT), VALUE      :: HYDROSTATIC
     END FUNCTION
+    INTEGER(C_INT) FUNCTION FZ_SET_TAU_SHARD_DEVICE(CTX, NX, NY, D_OBS, D_MODELS, ASSIST, &
+        HYDROSTATIC, REDUCE, USER, STREAM) BIND(C, NAME='fz_set_tau_shard_device')
+      IMPORT
+      TYPE(C_PTR), VALUE         :: CTX
+      INTEGER(C_INT), VALUE      :: NX
+      INTEGER(C_INT), VALUE      :: NY
+      TYPE(C_PTR), VALUE         :: D_OBS
+      TYPE(C_PTR), VALUE         :: D_MODELS
+      INTEGER(C_INT), VALUE      :: ASSIST
+      INTEGER(C_INT), VALUE      :: HYDROSTATIC
+      TYPE(C_FUNPTR), VALUE      :: REDUCE
+      TYPE(C_PTR), VALUE         :: USER
+      TYPE(C_PTR), VALUE         :: STREAM                 ! cudaStream_t or C_NULL_PTR
+    END FUNCTION
     INTEGER(C_INT) FUNCTION FZ_ERRORS_DEVICE(CTX, NPIX, D_OBS, D_MODELS, HYDROSTATIC, OPTS, &
         D_ERR, D_CHI2, D_STATUS, STREAM) BIND(C, NAME='fz_errors_device')
       IMPORT
@@ -577,6 +591,54 @@ MODULE FZ_B200
       REAL(C_FLOAT), VALUE       :: LR
       INTEGER(C_LONG_LONG), VALUE :: SEED
       REAL(C_FLOAT)              :: LOSS(*)
+    END FUNCTION
+    INTEGER(C_INT) FUNCTION FZ_MLP_FORWARD_OBS_DEVICE(MLP, N, D_OBS, D_MU, D_SD, D_Y, STREAM) &
+        BIND(C, NAME='fz_mlp_forward_obs_device')
+      IMPORT
+      TYPE(C_PTR), VALUE         :: MLP
+      INTEGER(C_INT), VALUE      :: N
+      TYPE(C_PTR), VALUE         :: D_OBS
+      TYPE(C_PTR), VALUE         :: D_MU
+      TYPE(C_PTR), VALUE         :: D_SD
+      TYPE(C_PTR), VALUE         :: D_Y
+      TYPE(C_PTR), VALUE         :: STREAM                 ! cudaStream_t or C_NULL_PTR
+    END FUNCTION
+    INTEGER(C_INT) FUNCTION FZ_MLP_IO(MLP, NIN, NOUT) BIND(C, NAME='fz_mlp_io')
+      IMPORT
+      TYPE(C_PTR), VALUE         :: MLP
+      INTEGER(C_INT)             :: NIN(*)
+      INTEGER(C_INT)             :: NOUT(*)
+    END FUNCTION
+    INTEGER(C_INT) FUNCTION FZ_WARM_START_DEVICE(CTX, MLP, NPIX, D_OBS, D_NORM, D_BASE, &
+        D_MODELS, STREAM) BIND(C, NAME='fz_warm_start_device')
+      IMPORT
+      TYPE(C_PTR), VALUE         :: CTX
+      TYPE(C_PTR), VALUE         :: MLP
+      INTEGER(C_INT), VALUE      :: NPIX
+      TYPE(C_PTR), VALUE         :: D_OBS
+      TYPE(C_PTR), VALUE         :: D_NORM
+      TYPE(C_PTR), VALUE         :: D_BASE
+      TYPE(C_PTR), VALUE         :: D_MODELS
+      TYPE(C_PTR), VALUE         :: STREAM                 ! cudaStream_t or C_NULL_PTR
+    END FUNCTION
+    INTEGER(C_INT) FUNCTION FZ_INVERT_WARM(CTX, MLP, NORM, BASE, NPIX, OBS, TARGET_CHI2, &
+        HYDROSTATIC, OPTS, MODEL_OUT, CHI2, ITERS, SYN_OUT, STATUS) BIND(C, &
+        NAME='fz_invert_warm')
+      IMPORT
+      TYPE(C_PTR), VALUE         :: CTX
+      TYPE(C_PTR), VALUE         :: MLP
+      REAL(C_FLOAT)              :: NORM(*)
+      REAL(C_FLOAT)              :: BASE(*)
+      INTEGER(C_INT), VALUE      :: NPIX
+      REAL(C_DOUBLE)             :: OBS(*)                 ! OBS3D(NFREQ,NPIX)
+      TYPE(C_PTR), VALUE         :: TARGET_CHI2            ! per-pixel chi2 goal or C_NULL_PTR
+      INTEGER(C_INT), VALUE      :: HYDROSTATIC
+      TYPE(FZ_LM_OPTS)           :: OPTS
+      REAL(C_FLOAT)              :: MODEL_OUT(*)           ! MODEL(NZ,13,NCOL), may be MODEL
+      REAL(C_DOUBLE)             :: CHI2(*)
+      INTEGER(C_INT)             :: ITERS(*)
+      TYPE(C_PTR), VALUE         :: SYN_OUT                ! RSYN1D(NFREQ,NPIX) or C_NULL_PTR
+      INTEGER(C_INT)             :: STATUS(*)              ! per column / pixel
     END FUNCTION
     INTEGER(C_INT) FUNCTION FZ_PROFILE_ENABLE(CTX, ON) BIND(C, NAME='fz_profile_enable')
       IMPORT

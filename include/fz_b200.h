@@ -155,8 +155,12 @@ int fz_log_tau5_device(fz_ctx* ctx, int ncol, const float* d_model, int hydrosta
  * (1 T, 2 Pg, 4 Bx, 5 By, 6 Bz, 7 v_z; 3 rho and 8 P0 must be 0); the hat
  * interpolation of GET_INT_COEFS (src/get_dmodel.f90:563-644) maps nodes to
  * heights, so nodes[p-1] == nz gives the response at every height.  Returns
- * NP = sum of the node counts (<= 64) or a negative error.  Replaces the node
- * set-up of UPDATE_COEFS (src/get_dmodel.f90:648-721). */
+ * NP = sum of the node counts (<= 1024) or a negative error.  Layouts whose
+ * node accumulators fit in shared memory (4 NP floats per wavelength) are
+ * accumulated along z in the RF kernel; larger ones (e.g. every height of T
+ * and v_z, the reference's last cycle) are contracted from the response
+ * functions at every height.  Replaces the node set-up of UPDATE_COEFS
+ * (src/get_dmodel.f90:648-721). */
 int fz_rf_nodes(fz_ctx* ctx, const int* nodes /* [8] */);
 
 /* Forward synthesis with response functions: as fz_forward plus the node
@@ -287,14 +291,18 @@ typedef struct {
 } fz_lm_opts;
 
 /* Batched pixel-wise Levenberg-Marquardt inversion of npix pixels with the
- * node layout of fz_rf_nodes (NP <= 16): the cycle loop of INVERT3D
+ * node layout of fz_rf_nodes: the cycle loop of INVERT3D
  * (src/invert3d.f90:57-178) with GET_DMODEL3DS/GET_PERT_1D per pixel
  * (src/get_dmodel.f90:1201-1577), each pixel iterating until its own stop
  * rule, finished pixels replaced from a device work queue.  obs is
  * OBS3D(NFREQ, npix) (Stokes-major, GAIN-normalised, as RSYN1D); init is the
  * initial model MODEL(NZ,13,npix).  Outputs: the best model, its chi2
  * (NEW_CALCULATE_CHI2 normalisation), the iterations used, optionally the
- * best synthesis (syn_out, may be NULL) and a status per pixel. */
+ * best synthesis (syn_out, may be NULL) and a status per pixel.  Layouts
+ * of up to 16 nodes solve with one warp per pixel (mma.sync normal
+ * equations, warp Jacobi SVD / CG); up to 1024 nodes with the tcgen05
+ * normal equations and a CTA per pixel for the FP64 SVD or CG, the slot
+ * count then held within a 24 GB working set. */
 int fz_invert(fz_ctx* ctx, int npix, const double* obs, const float* init, const double* target_chi2,
               int hydrostatic, const fz_lm_opts* opts, float* model_out, double* chi2, int* iters,
               double* syn_out, int* status);
@@ -371,6 +379,22 @@ int fz_set_tau_device(fz_ctx* ctx, int nx, int ny, const double* d_obs, float* d
                       void* stream);
 int fz_set_tau(fz_ctx* ctx, int nx, int ny, const double* obs, float* models, int assist, int hydrostatic);
 
+/* SET_TAU on one shard of a field split over ranks by x (contiguous runs of
+ * columns, pixel iy + NY*ix within the shard): the per-pixel work as
+ * fz_set_tau_device, its two field-wide reductions through the caller's
+ * reduce(user, kind, data, n, nx), which returns 0 on success:
+ *   kind 0: data (nx * n doubles, x-major) holds this shard's sums of Stokes
+ *           I over y per column (n = NUMWAVE of the first region); it must
+ *           leave in data[0 .. n) the field total, every shard's columns
+ *           summed in field x order (the reference's SUM order);
+ *   kind 1: data (3) holds this shard's maxima of the three projections;
+ *           it must leave the field maxima.
+ * Every shard then computes the same template vectors and scales, so the
+ * result equals the whole field's.  With reduce NULL: fz_set_tau_device. */
+typedef int (*fz_field_reduce_fn)(void* user, int kind, double* data, int n, int nx);
+int fz_set_tau_shard_device(fz_ctx* ctx, int nx, int ny, const double* d_obs, float* d_models, int assist,
+                            int hydrostatic, fz_field_reduce_fn reduce, void* user, void* stream);
+
 /* The errors mode (GET_ERRORS3DS / GET_ERROR_1D / NEW_SOLVE_ERRORS,
  * src/get_dmodel.f90:1248-1323, :1581-1703), replacing the per-pixel worker
  * loop: for the models (usually the inversion's best), with the node layout
@@ -381,7 +405,8 @@ int fz_set_tau(fz_ctx* ctx, int nx, int ny, const double* obs, float* models, in
  * branch (limits [0, 1e20], node values clipped at 0.15 PARAM_NORM).
  * err: MODEL(NZ,13,npix), the rows of parameters without nodes zero (the
  * E*3D cubes of ESPLIT_MODEL3D); chi2 (npix); status may be NULL.  opts
- * supplies isigma, wstk and reg_*; the LM fields are unused. */
+ * supplies isigma, wstk and reg_*; the LM fields are unused.  Node layouts
+ * of up to 16 nodes (FZ_ERR_LIMIT above). */
 int fz_errors_device(fz_ctx* ctx, int npix, const double* d_obs, const float* d_models, int hydrostatic,
                      const fz_lm_opts* opts, float* d_err, double* d_chi2, int* d_status, void* stream);
 int fz_errors(fz_ctx* ctx, int npix, const double* obs, const float* models, int hydrostatic, const fz_lm_opts* opts,
@@ -398,7 +423,8 @@ int fz_errors(fz_ctx* ctx, int npix, const double* obs, const float* models, int
  * reg_pen (np, npix) and reg_hss (np, np, npix), may be NULL: REG_PEN is
  * subtracted from J^T diff and REG_HSS added to J^T J as the reference does
  * (:169-174); delta (np, npix), NaN entries zeroed (NEW_SOLVE_PERTURBATION).
- * np <= 16, nfreq a multiple of 4. */
+ * np <= 1024 (above 16: tcgen05 normal equations, CTA-wide FP64 solvers),
+ * nfreq a multiple of 4. */
 int fz_lm_perturbation(fz_ctx* ctx, int npix, int np, int nfreq, const double* jac, const double* diff,
                        const double* lambda, const double* reg_pen, const double* reg_hss, int dtype, double svdtol,
                        double* delta);
@@ -460,8 +486,9 @@ int fz_voigt(int n, const float* a, const float* v, float* h, float* f);
 
 /* Warm-start network (no counterpart in the reference): an MLP of nlayers
  * fully connected layers dims[0] -> dims[1] -> ... -> dims[nlayers] with GELU
- * between layers, trained and evaluated with hand-written BF16 tensor-core
- * kernels (FP32 accumulation, FP32 master weights, Adam).  dims[0..nlayers-1]
+ * between layers, trained and evaluated with hand-written BF16 tcgen05
+ * tensor-core kernels (FP32 accumulation in tensor memory, FP32 master
+ * weights, Adam).  dims[0..nlayers-1]
  * must be multiples of 8.  Weights start from a seeded uniform
  * Glorot initialisation.  Parameters are exchanged as FP32 in layer order
  * (W0[out][in], b0, W1, b1, ...); fz_mlp_get_params with grads != 0 returns
@@ -477,6 +504,32 @@ int fz_mlp_forward_device(fz_mlp* mlp, int n, const float* d_x, float* d_y, void
 int fz_mlp_grad_device(fz_mlp* mlp, int n, const float* d_x, const float* d_t, float* loss);
 int fz_mlp_train_device(fz_mlp* mlp, int n, const float* d_x, const float* d_t, int batch, int epochs, float lr,
                         unsigned long long seed, float* loss);
+/* Forward of observed Stokes rows: d_obs (n x dims[0]) FP64, standardised
+ * with d_mu and d_sd (dims[0] each, FP32) as they are converted to the bf16
+ * inputs; d_y (n x dims[nlayers]) FP32.  Ordered after the work on stream,
+ * which waits for it.  fz_mlp_io: the input and output widths. */
+int fz_mlp_forward_obs_device(fz_mlp* mlp, int n, const double* d_obs, const float* d_mu, const float* d_sd,
+                              float* d_y, void* stream);
+int fz_mlp_io(const fz_mlp* mlp, int* nin, int* nout);
+
+/* The learned initial guess of the inversion (no counterpart in the
+ * reference, whose LM starts from the control file's model or SET_TAU's
+ * assists): the network maps each pixel's observed Stokes vector OBS3D(NFREQ)
+ * to the node values of the context's layout (fz_rf_nodes; outputs in node
+ * order, standardised), and each free parameter's row of the base model
+ * MODEL(NZ,13) moves by EXPAND(nodes - CONTRACT(base)) -- the way the
+ * inversion perturbs a model (src/get_dmodel.f90:839-880); the other rows
+ * are the base model's.  norm: FP32 x mean (NFREQ), x spread (NFREQ), node
+ * mean (NP), node spread (NP).  fz_warm_start_device: device buffers,
+ * models MODEL(NZ,13,npix), enqueued on stream.  fz_invert_warm: host
+ * buffers -- the observations cross to the device once, the warm-start
+ * models are built there and inverted by fz_invert's batched LM (other
+ * arguments as fz_invert). */
+int fz_warm_start_device(fz_ctx* ctx, fz_mlp* mlp, int npix, const double* d_obs, const float* d_norm,
+                         const float* d_base, float* d_models, void* stream);
+int fz_invert_warm(fz_ctx* ctx, fz_mlp* mlp, const float* norm, const float* base, int npix, const double* obs,
+                   const double* target_chi2, int hydrostatic, const fz_lm_opts* opts, float* model_out,
+                   double* chi2, int* iters, double* syn_out, int* status);
 
 /* Per-kernel timing: when enabled, every launch of the context is bracketed
  * by CUDA events on its stream; fz_profile_read returns the accumulated

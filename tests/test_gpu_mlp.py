@@ -94,3 +94,23 @@ def test_warm_start_beats_default_guess(fz):
     assert np.all(st_p == 0) and np.all(st_w == 0)
     assert np.median(chi_w) < np.median(chi_p), (np.median(chi_w), np.median(chi_p))
     assert it_w.mean() <= it_p.mean() + 1.0
+    # the fused path: fz_warm_start_device (standardisation inside the bf16
+    # conversion, node expansion kernel) gives the models of the host glue
+    # above to FP32 rounding, and fz_invert_warm (observations cross once)
+    # the inversion of those models
+    import torch
+    d_obs = torch.from_numpy(obs.reshape(npix, -1)).cuda()
+    d_base = torch.from_numpy(ws.default_models(1, nz)[0]).cuda()
+    d_out = torch.empty((npix, 13, nz), dtype=torch.float32, device="cuda")
+    warm.models_device(ctx, npix, d_obs.data_ptr(), d_base.data_ptr(), d_out.data_ptr())
+    torch.cuda.synchronize()
+    glue = warm.initial_models(obs)
+    fused = d_out.cpu().numpy()
+    for row in (0, 5, 6, 7, 10):
+        scale = np.maximum(np.abs(glue[:, row]).max(axis=1, keepdims=True), 1.0)
+        assert np.max(np.abs(fused[:, row] - glue[:, row]) / scale) < 1e-4, row
+    assert np.array_equal(np.delete(fused, (0, 5, 6, 7, 10), axis=1), np.delete(glue, (0, 5, 6, 7, 10), axis=1))
+    mo_f, chi_f, it_f, st_f = ctx.invert_warm(obs, warm, opts=opts)
+    mo_g, chi_g, it_g, st_g = ctx.invert(obs, fused, hydrostatic=True, opts=opts)
+    assert np.all(st_f == 0)
+    assert np.array_equal(chi_f, chi_g) and np.array_equal(it_f, it_g) and np.array_equal(mo_f, mo_g)

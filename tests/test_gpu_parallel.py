@@ -61,3 +61,74 @@ def test_field_shard_cycles_one_rank(fz, orc):
     np.testing.assert_array_equal(chi2.cpu().numpy(), chi)
     np.testing.assert_array_equal(it2.cpu().numpy(), it)
     np.testing.assert_array_equal(d_m.cpu().numpy(), mod)
+
+
+@pytest.mark.parametrize("nx,world", [(6, 2), (7, 3)])
+def test_set_tau_shards_equal_whole_field(fz, orc, nx, world):
+    """SET_TAU's assists on shards of a field (fz_set_tau_shard_device), the
+    field sum and maxima exchanged between the shards by the host threads
+    that run them (each shard its own context and stream; no kernel waits
+    for another), equal the whole field's fz_set_tau_device bit for bit."""
+    import threading
+
+    import torch
+    from firtez_dz_b200 import parallel
+    ny, nz = 5, 32
+    ctx, lines, reg, g = _ctx(fz, orc, nz)
+    numw = ctx.numw
+    true = fz.atmos.make_columns(nx * ny, nz, seed=61)
+    obs, _, _ = ctx.forward(true, hydrostatic=True)
+    obs = obs.reshape(nx * ny, -1) + np.random.default_rng(2).normal(0.0, 1e-3, (nx * ny, 4 * numw))
+    from firtez_dz_b200 import warmstart as ws
+    base = ws.default_models(nx * ny, nz)
+    assist = ("temp", "bvec", "vlos")
+    d_obs = torch.from_numpy(obs).cuda()
+    want = torch.from_numpy(base.copy()).cuda()
+    ctx.set_tau_device(nx, ny, d_obs.data_ptr(), want.data_ptr(), assist)
+    torch.cuda.synchronize()
+    # the host-side exchange of the threads: field_reduce's semantics
+    spans = parallel.split(nx, world)
+    bar = threading.Barrier(world)
+    box = {}
+
+    def reducer(r):
+        def fn(kind, data, n, nxr):
+            if kind == 0:
+                box[("p", r)] = np.array(data[:nxr * n]).reshape(nxr, n)
+                bar.wait()
+                tot = np.zeros(n)
+                for q in range(world):
+                    for row in box[("p", q)]:
+                        tot = tot + row
+                data[:n] = tot
+            else:
+                box[("m", r)] = np.array(data[:3])
+                bar.wait()
+                data[:3] = np.max([box[("m", q)] for q in range(world)], axis=0)
+            bar.wait()
+            return 0
+        return fn
+
+    ctxs = [_ctx(fz, orc, nz)[0] for _ in range(world)]
+    outs, errs = [], []
+    for r, (x0, x1) in enumerate(spans):
+        outs.append(torch.from_numpy(base[x0 * ny:x1 * ny].copy()).cuda())
+
+    def run(r):
+        try:
+            x0, x1 = spans[r]
+            ctxs[r].set_tau_shard_device(x1 - x0, ny, d_obs[x0 * ny:].data_ptr(), outs[r].data_ptr(), assist,
+                                         reducer(r))
+        except Exception as e:   # noqa: BLE001
+            errs.append(e)
+            bar.abort()
+
+    th = [threading.Thread(target=run, args=(r,)) for r in range(world)]
+    for t in th:
+        t.start()
+    for t in th:
+        t.join(timeout=120)
+    assert not errs, errs
+    torch.cuda.synchronize()
+    got = torch.cat(outs).cpu().numpy()
+    np.testing.assert_array_equal(got, want.cpu().numpy())

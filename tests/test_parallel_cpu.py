@@ -71,3 +71,44 @@ def test_field_shard_gloo_equals_whole_field(tmp_path, nx, world):
     mp.spawn(_rank, args=(world, _free_port(), nx, ny, nz, str(tmp_path)), nprocs=world, join=True)
     got = np.concatenate([np.load(os.path.join(tmp_path, "r%d.npy" % r)) for r in range(world)], 0)
     np.testing.assert_array_equal(got, lmo.smoothing_b(_field(nx, ny, nz), nx, ny, PARAMS))
+
+
+def _tau_rank(rank, world, port, nx, n, outdir):
+    """SET_TAU's field reductions (FieldShard.field_reduce) on gloo ranks:
+    the per-column sums of this rank's columns in, the field total out; the
+    rank's maxima in, the field maxima out."""
+    import torch.distributed as dist
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
+    par = _parallel()
+    sh = par.FieldShard(nx, 3, rank, world)
+    cols = np.random.default_rng(5).standard_normal((nx, n)) * 10 ** np.random.default_rng(6).uniform(-3, 3, (nx, 1))
+    fn = sh.field_reduce()
+    buf = np.zeros(max(sh.nx * n, 3))
+    buf[:sh.nx * n] = cols[sh.x0:sh.x1].ravel()
+    assert fn(0, buf, n, sh.nx) == 0
+    total = buf[:n].copy()
+    mx = np.array([rank + 0.5, 10.0 - rank, 2.0 * rank])
+    assert fn(1, mx, 3, 1) == 0
+    np.save(os.path.join(outdir, "t%d.npy" % rank), np.concatenate([total, mx]))
+    dist.barrier()
+    dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("nx,world", [(7, 2), (8, 3)])
+def test_set_tau_field_reductions_gloo(tmp_path, nx, world):
+    """Every rank gets the whole field's total bit for bit (the columns
+    summed one after another in x order, as the single-field kernel does)
+    and the maxima over the ranks."""
+    import torch.multiprocessing as mp
+    n = 11
+    mp.spawn(_tau_rank, args=(world, _free_port(), nx, n, str(tmp_path)), nprocs=world, join=True)
+    cols = np.random.default_rng(5).standard_normal((nx, n)) * 10 ** np.random.default_rng(6).uniform(-3, 3, (nx, 1))
+    want = np.zeros(n)
+    for c in cols:
+        want = want + c
+    wmax = np.max([[r + 0.5, 10.0 - r, 2.0 * r] for r in range(world)], axis=0)
+    for r in range(world):
+        got = np.load(os.path.join(tmp_path, "t%d.npy" % r))
+        np.testing.assert_array_equal(got[:n], want)
+        np.testing.assert_array_equal(got[n:], wmax)
