@@ -715,6 +715,13 @@ class Synthesis:
                                        ctypes.c_void_p(stream) if stream else None))
 
 
+def measure_fp64_peak(device=0):
+    """Measured FP64 FMA peak of the device in TFLOP/s."""
+    t = np.zeros(1)
+    _check(lib().fz_measure_fp64_peak(int(device), _p(t)))
+    return float(t[0])
+
+
 def lm_update_lambda(chicur, chipre, lam, steps, precyc):
     """Batched UPDATE_LAMBDA on the GPU; returns the updated (chipre, lambda,
     steps, precyc) arrays."""

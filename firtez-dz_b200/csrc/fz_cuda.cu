@@ -88,9 +88,11 @@ __device__ __forceinline__ void copy_to_shared(T* dst, const T* src) {
 //
 // L lanes per column: 32 (a warp) or 16 (two columns per warp: each lane
 // holds six elements, and every per-column scalar of the chain costs half
-// the warp instructions).
+// the warp instructions).  At most 128 registers a thread (four blocks, 16
+// warps per SM): the chain is bound by dependent FP64 latency, so resident
+// warps count more than the few spilled values.
 template <bool HE, int L>
-__global__ void __launch_bounds__(128) k_chain(const Consts* __restrict__ Kg, const PFTable* __restrict__ tb, int ncol,
+__global__ void __launch_bounds__(128, 4) k_chain(const Consts* __restrict__ Kg, const PFTable* __restrict__ tb, int ncol,
                                                int nz, const float* model, float* mout, double2* __restrict__ chem,
                                                int* __restrict__ status) {
   constexpr int NS = WarpSahaT<L>::NS;
@@ -1364,6 +1366,22 @@ __global__ void k_fp32_peak(float* out, int iters, float s) {
   }
   const float r = a0 + a1 + a2 + a3 + a4 + a5 + a6 + a7;
   if (r == 1234.5f) out[0] = r;   // keeps the chains live
+}
+
+// The same independent FMA chains in FP64: the FP64 pipe's peak.
+__global__ void k_fp64_peak(double* out, int iters, double s) {
+  double a0 = threadIdx.x * 1e-9, a1 = a0 + 1e-9, a2 = a0 + 2e-9, a3 = a0 + 3e-9;
+  double a4 = a0 + 4e-9, a5 = a0 + 5e-9, a6 = a0 + 6e-9, a7 = a0 + 7e-9;
+  const double m = 0.999999999;
+  for (int i = 0; i < iters; ++i) {
+#pragma unroll
+    for (int j = 0; j < 32; ++j) {
+      a0 = fma(a0, m, s); a1 = fma(a1, m, s); a2 = fma(a2, m, s); a3 = fma(a3, m, s);
+      a4 = fma(a4, m, s); a5 = fma(a5, m, s); a6 = fma(a6, m, s); a7 = fma(a7, m, s);
+    }
+  }
+  const double r = a0 + a1 + a2 + a3 + a4 + a5 + a6 + a7;
+  if (r == 1234.5) out[0] = r;
 }
 
 // ------------------------------------------------------------------ context
@@ -3420,6 +3438,38 @@ int fz_measure_fp32_peak(int device, double* tflops) {
   cudaFree(d);
   if (rc) return rc;
   const double fma = (double)blocks * threads * iters * 64 * 8;
+  *tflops = 2.0 * fma / (best * 1e-3) / 1e12;
+  return 0;
+}
+
+int fz_measure_fp64_peak(int device, double* tflops) {
+  if (!tflops) return FZ_ERR_ARG;
+  FZ_CK(cudaSetDevice(device));
+  int sms = 0;
+  FZ_CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
+  double* d = nullptr;
+  FZ_CK(cudaMalloc(&d, sizeof(double)));
+  cudaEvent_t a, b;
+  cudaEventCreate(&a);
+  cudaEventCreate(&b);
+  const int threads = 512, blocks = sms * 4, iters = 16;
+  k_fp64_peak<<<blocks, threads>>>(d, iters, 1e-9);   // warm-up
+  float best = 1e30f;
+  for (int rep = 0; rep < 5; ++rep) {
+    cudaEventRecord(a);
+    k_fp64_peak<<<blocks, threads>>>(d, iters, 1e-9);
+    cudaEventRecord(b);
+    cudaEventSynchronize(b);
+    float t = 0.f;
+    cudaEventElapsedTime(&t, a, b);
+    best = t < best ? t : best;
+  }
+  const int rc = cuda_fail(cudaGetLastError());
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  cudaFree(d);
+  if (rc) return rc;
+  const double fma = (double)blocks * threads * iters * 32 * 8;
   *tflops = 2.0 * fma / (best * 1e-3) / 1e12;
   return 0;
 }

@@ -660,6 +660,12 @@ MODULE FZ_B200
       INTEGER(C_INT), VALUE      :: DEVICE
       REAL(C_DOUBLE)             :: TFLOPS(*)
     END FUNCTION
+    INTEGER(C_INT) FUNCTION FZ_MEASURE_FP64_PEAK(DEVICE, TFLOPS) BIND(C, &
+        NAME='fz_measure_fp64_peak')
+      IMPORT
+      INTEGER(C_INT), VALUE      :: DEVICE
+      REAL(C_DOUBLE)             :: TFLOPS(*)
+    END FUNCTION
     INTEGER(C_INT) FUNCTION FZ_V3_HEADER(PATH, ID, VERSION, NDIMS, DIMS) BIND(C, &
         NAME='fz_v3_header')
       IMPORT

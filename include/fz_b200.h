@@ -546,6 +546,8 @@ int fz_profile_read(fz_ctx* ctx, double* ms, int* launches, long long* items, in
  * measured by a register-resident FMA-chain kernel; the denominator of the
  * FP32-pipe roofline of the synthesis kernel. */
 int fz_measure_fp32_peak(int device, double* tflops);
+/* The FP64 FMA peak of the device (independent FMA chains), TFLOP/s. */
+int fz_measure_fp64_peak(int device, double* tflops);
 
 /* ---------------------------------------------------------------- v3 files
  * The model, profile and response-function files of src/misc.f90, as the
