@@ -65,12 +65,12 @@ class LMOpts(ctypes.Structure):
                 ("slots", ctypes.c_int), ("assist", ctypes.c_int), ("fallback", ctypes.c_double),
                 ("fallback_model", ctypes.c_void_p), ("reg_type", ctypes.c_int * 8), ("reg_alpha", ctypes.c_double * 8),
                 ("fallback_steps", ctypes.c_int), ("solver", ctypes.c_int), ("node_expansion", ctypes.c_int),
-                ("global_stop", ctypes.c_int), ("cycles_left", ctypes.c_int), ("pad3", ctypes.c_int),
+                ("global_stop", ctypes.c_int), ("cycles_left", ctypes.c_int), ("fallback_free", ctypes.c_int),
                 ("state_out", ctypes.c_void_p)]
 
     def __init__(self, maxsteps=5, maxit=40, dchi2=0.0, svdtol=1e-4, isigma=4e-3, wstk=(1, 1, 1, 1), slots=0,
                  fallback=0.0, fallback_model=0, reg=None, assist=(), fallback_steps=0, solver=1, node_expansion=1,
-                 global_stop=False, cycles_left=0, state_out=0):
+                 global_stop=False, cycles_left=0, state_out=0, fallback_free=False):
         """fallback_model: device pointer of one MODEL(NZ,13) float32 (e.g. a
         torch tensor's data_ptr()) that pixels ending above fallback x their
         chi2 goal restart from (a host pointer for invert()).  reg: optional
@@ -78,7 +78,9 @@ class LMOpts(ctypes.Structure):
         (VERTICAL REGULARIZATION: type 0 or 1, PEN_ALP).  assist: SET_TAU's
         assists for invert_cycles (temp, pgas, bvec, vlos, progressive).
         fallback_steps: restart once STEPS reaches it while above fallback x
-        the goal (0: when the search ends).  solver: 1 SVD, 2 conjugate
+        the goal (0: when the search ends; negative: at the first
+        evaluation); fallback_free: the restarted search ignores the goal.
+        solver: 1 SVD, 2 conjugate
         gradients (LINEAR_SOLVER); node_expansion: 1 SIR-like, 2 STiC-like
         (PERTURBATION_TYPE).  global_stop: MAKE_DECISION's field-wide stop on
         the mean STEPS (threshold max(1, maxsteps - cycles_left)); state_out:
@@ -92,7 +94,7 @@ class LMOpts(ctypes.Structure):
                          assist_bits(assist),
                          float(fallback), fallback_model or None, (ctypes.c_int * 8)(*typ),
                          (ctypes.c_double * 8)(*alp), int(fallback_steps), int(solver), int(node_expansion),
-                         int(bool(global_stop)), int(cycles_left), 0, state_out or None)
+                         int(bool(global_stop)), int(cycles_left), int(bool(fallback_free)), state_out or None)
 
 
 class Tune(ctypes.Structure):

@@ -2209,7 +2209,9 @@ int lm_conf(fz_ctx* c, int npix, const fz_lm_opts* o, LMConf& C) {
   C.inu = (double)C.nfreq;
   C.fallback = o && o->fallback_model ? o->fallback : 0.0;
   C.fb_model = o ? o->fallback_model : nullptr;
-  C.fb_steps = o && o->fallback_steps > 0 ? o->fallback_steps : (1 << 30);
+  // fallback_steps > 0: at that STEPS count; < 0: at the first evaluation; 0: when the search ends
+  C.fb_steps = o && o->fallback_steps > 0 ? o->fallback_steps : (o && o->fallback_steps < 0 ? 0 : (1 << 30));
+  C.fb_free = o && o->fallback_free ? 1 : 0;
   C.solver = o && o->solver == 2 ? 2 : 1;
   C.node_exp = o && o->node_expansion == 2 ? 2 : 1;
   C.global_stop = o && o->global_stop ? 1 : 0;

@@ -38,6 +38,7 @@ struct LMConf {
   double fallback;             // restart factor on the chi2 goal (0 = off)
   const float* fb_model;       // MODEL(NZ,13) a restarted pixel starts from
   int fb_steps;                // restart once STEPS reaches this while above fallback x goal
+  int fb_free;                 // a restarted search ignores the goal
   int solver;                  // SOLVER_METHOD: 1 SVD (GET_INVERSE), 2 CG (NEW_CALCULATE_DELTA_UBICGSTAB)
   int node_exp;                // NODE_EXPANSION: 1 SIR/NICOLE-like, 2 STiC-like
   int reg;                     // vertical regularisation on (GET_IT_PENALTIES)
@@ -282,7 +283,7 @@ __global__ void __launch_bounds__(256) k_lm_accept(LMConf C, LMSlots Sl, LMQueue
     // dchi2 (relative)
     const bool small = acc && chibest < 1.0e29 && (chibest - cc) < C.dchi2 * chibest;
     // optional per-pixel goal: stop once the best chi2 reaches it
-    const bool goal = target != nullptr && chipre <= target[p];
+    const bool goal = target != nullptr && !(C.fb_free && Sl.restarted[s]) && chipre <= target[p];
     fin = steps > (double)C.maxsteps || it >= C.maxit || small || goal;
     // an early restart: the search has stagnated fb_steps times and is still
     // above fallback x its goal

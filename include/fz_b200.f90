@@ -49,7 +49,7 @@ MODULE FZ_B200
     INTEGER(C_INT) :: NODE_EXPANSION               ! 1 SIR-like, 2 STiC-like
     INTEGER(C_INT) :: GLOBAL_STOP                  ! MAKE_DECISION's field rule
     INTEGER(C_INT) :: CYCLES_LEFT                  ! MAXITER - CURIC
-    INTEGER(C_INT) :: PAD3
+    INTEGER(C_INT) :: FALLBACK_FREE                ! the restarted search ignores the goal
     TYPE(C_PTR)    :: STATE_OUT                    ! INV_SLA(1:4), INV_SLA(9) per pixel, or C_NULL_PTR
   END TYPE
   ! launch shapes of the autotuner

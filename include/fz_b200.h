@@ -252,7 +252,10 @@ int fz_smooth_device(fz_ctx* ctx, int nx, int ny, float* d_models, const int* pa
  * fallback_steps: with fallback on, a pixel restarts as soon as its
  * stagnation counter (the STEPS of UPDATE_LAMBDA) reaches fallback_steps
  * while its best chi2 is still above fallback x its goal, instead of when
- * its search ends (0: when it ends).
+ * its search ends (0: when it ends; negative: at its first evaluation, i.e.
+ * the initial model itself is judged).  fallback_free: 1 = the restarted
+ * search ignores the goal and runs to the plain stop rules, 0 = it keeps
+ * the goal.
  * solver: SOLVER_METHOD (MISC SETUP LINEAR_SOLVER), 1 (or 0) = the SVD
  * pseudo-inverse of GET_INVERSE, 2 = the conjugate-gradient iteration of
  * NEW_CALCULATE_DELTA_UBICGSTAB (src/lm.f90:375-453).  node_expansion:
@@ -286,7 +289,7 @@ typedef struct {
   int reg_type[8];
   double reg_alpha[8];
   int fallback_steps, solver, node_expansion, global_stop;
-  int cycles_left, pad3;
+  int cycles_left, fallback_free;
   double* state_out;
 } fz_lm_opts;
 

@@ -13,7 +13,7 @@ and the CTA-wide FP64 solvers.
   16-node kernels), the conjugate-gradient path within the reference's own
   stopping test and 5 % of the oracle's CG delta.
 * The node Jacobian of 72- and 96-node layouts against the oracle's,
-  within 2e-4 of each column's largest entry.
+  within 2e-4 of the largest entry of each parameter's node columns.
 * The inversion at test_inv1's shape (NZ 256, Fe I 6301.5 blended with
   6302.5 x 500 wavelengths, T and v_z at every height, CG, STiC-like
   expansion, type-1 regularisation) run for 1, 2 and 3 iterations against
@@ -91,9 +91,16 @@ def test_node_jacobian_of_large_layouts(fz, orc, nodes):
     osyn, ojac, _, ost = orc.forward_rf(lines, reg, g, m, nodes, hydrostatic=True)
     assert np.all(st == 0) and np.all(ost == 0)
     assert np.max(np.abs(syn[:, 0] - osyn[:, 0]) / np.abs(osyn[:, 0])) < 1e-5
-    scale = np.abs(ojac).max(axis=2)
-    rel = np.abs(jac.astype(np.float64) - ojac).max(axis=2) / np.where(scale > 0, scale, 1.0)
-    assert rel.max() <= 2e-4, rel.max()
+    # A node column of a layout with a node at every height is the RF of one
+    # height, which is tiny deep in the column; the error is measured against
+    # the largest entry of the parameter's node columns.
+    err = np.abs(jac.astype(np.float64) - ojac).max(axis=2)
+    j0 = 0
+    for p, nj in sorted(nodes.items()):
+        scale = np.abs(ojac[:, j0:j0 + nj]).max(axis=(1, 2))
+        rel = err[:, j0:j0 + nj].max(axis=1) / np.where(scale > 0, scale, 1.0)
+        assert rel.max() <= 2e-4, (p, rel.max())
+        j0 += nj
 
 
 def _inv1_case(fz, orc):
