@@ -6,30 +6,45 @@ Workload (one GPU): a seeded 512 x 512 field of model atmospheres, 128 heights
 from -0.5 to +1.5 Mm, Fe I 6301.5 + 6302.5 x 112 wavelengths at 21.5 mA
 (NUMW = 224, NFREQ = 896), observations = the GPU synthesis (hydrostatic) of
 the field plus Gaussian noise of 1e-3 Ic.  Free parameters on nodes: T 5,
-Bx, By, Bz, v_z 2 each (NP = 13).  Stop rule per pixel: the reference's
-STEPS > MAXSTEPS (5), an accepted step gaining less than 1e-3 in chi2
-(relative), or 40 iterations.  The warm start is the MLP 896-1024-1024-512-13
-(GELU), trained before the timed region with the library's BF16 kernels on
-pairs the GPU forward solver synthesises from seeded atmospheres (2M by
-default).
+Bx, By, Bz, v_z 2 each (NP = 13).  Plain stop rule per pixel: the
+reference's STEPS > MAXSTEPS (5), an accepted step gaining less than 1e-3 in
+chi2 (relative), or 40 iterations.  The warm start is the MLP
+896-1024-1024-512-13 (GELU), trained before the timed region with the
+library's BF16 tcgen05 kernels on pairs the GPU forward solver synthesises
+from seeded atmospheres (2M by default).
+
+Calibration, before the timed region: plain LM from the default guess on
+32,768 pixels of a separate seeded set (same generator, same noise); the
+acceptance level T is the 20th percentile of their chi2 (--accept-quantile).
 
 One step = the inversion of one tile of 131072 pixels of the field (one
-inversion call), inputs resident in HBM.  The plain arm (LM from the default
-guess) runs first and is the yardstick: its per-pixel chi2 is the goal of the
-headline arm.  ``value`` = converged pixels per second of NN-warm LM (network
-inference + batched LM) where a pixel is converged once its chi2 reaches its
-plain-LM chi2 (or by the plain stop rules), a pixel whose search stagnates
-while above 1.1x its plain chi2 restarting once from the default guess in the
-same pool --
-"converged pixels/s at plain-LM chi2".  Beside it: the same arm without the
-restart and NN-warm LM with the plain stop rules only.  ``e2e``: the headline
-arm through the host-buffer calls from pinned host memory.  Multi-GPU: each
-rank inverts tiles of its own field (weak scaling, no collective on the data
-path; a barrier and the max over ranks of each time).
+inversion call), inputs resident in HBM.  Headline arm (``value``): the
+deployable NN-warm rule -- the network's model of every pixel is evaluated
+once; a pixel whose chi2 there is at or below T is converged with it, every
+other pixel restarts at once from the default guess in the same slot pool
+and runs plain LM (fallback_steps -1, fallback_free).  ``value`` = its
+pixels/s; the plain arm (LM from the default guess, plain stop rules) is the
+yardstick, and the line gives the speed-up over it, both median chi2, the
+fraction of pixels whose chi2 ends above 1.1x their plain-LM chi2 and the
+parameter errors against the true atmospheres.  Beside it: the same rule at
+two other quantiles, NN-warm LM with the plain stop rules only, and plain LM
+from SET_TAU's assisted guess.  ``e2e``: the headline arm through
+fz_invert_warm from pinned host memory.  Multi-GPU: each rank inverts tiles of
+its own field (weak scaling, no collective on the data path; a barrier and the
+max over ranks of each time).
+
+``roofline``: the dominant kernel of the headline arm against the pipe that
+bounds it (FP32 or FP64 FLOP per column counted by ncu on 2048 columns of
+this workload, profiles/flops.json, over the peak of an FMA-chain kernel
+measured in the same run), DRAM traffic per launch from ncu and the HBM
+fraction as side figures.
 
 ``--impl reference`` times the CPU restatement of the reference (oracle/: the
 Fortran reference cannot be built on this image, no gfortran/MPI/LAPACK),
 LM from the default guess, on bounded pixel samples with all host cores.
+``--probe-kernels N`` runs one synthesis and one node-Jacobian call on N
+columns of the workload twice and exits (the launches ncu counts FLOPs on);
+``--flops-from CSV`` turns that ncu CSV into profiles/flops.json.
 """
 import argparse
 import importlib.util
@@ -232,6 +247,69 @@ def cpu_synth_sample(lines, reg, he, nz, ncol, seed, nthreads=0):
     return ncol * numw / el, el
 
 
+PROBE_SEED = 3
+CALIB_SEED = 909090
+
+
+def probe_kernels(fz, lines, reg, nz, n):
+    """One synthesis and one node-Jacobian call (fz_forward_device,
+    fz_forward_rf_device) on n seeded columns of the workload, twice: every
+    launch processes all n columns, for per-opcode counts under ncu."""
+    import torch
+    ctx = fz.Synthesis(lines, reg, nz=nz)
+    ctx.rf_nodes(NODES)
+    m = torch.from_numpy(fz.atmos.make_columns(n, nz, seed=PROBE_SEED)).cuda()
+    syn = torch.empty((n, 4, ctx.numw), dtype=torch.float64, device="cuda")
+    jac = torch.empty((n, sum(NODES.values()), 4 * ctx.numw), dtype=torch.float32, device="cuda")
+    mo = torch.empty_like(m)
+    for _ in range(2):
+        ctx.forward_device(m.data_ptr(), n, syn.data_ptr(), mo.data_ptr(), 0, hydrostatic=True)
+        ctx.forward_rf_device(m.data_ptr(), n, syn.data_ptr(), jac.data_ptr(), mo.data_ptr(), 0, hydrostatic=True)
+    torch.cuda.synchronize()
+    print(json.dumps({"probe_columns": n, "nz": nz, "numw": ctx.numw, "mean_I": float(syn[:, 0].mean())}))
+
+
+def flops_table(csv_path, ncol, nz, numw, out_path):
+    """FLOP per column of each kernel from an ncu CSV of --probe-kernels
+    (metrics smsp__sass_thread_inst_executed_op_{ffma,fadd,fmul,dfma,dadd,
+    dmul}_pred_on.sum): FP32 = 2 ffma + fadd + fmul, FP64 likewise, per
+    launch over its ncol columns; the median over a kernel's launches.  A
+    kernel is bound by the pipe with more FLOP."""
+    import csv
+    import re
+    rows = [r for r in csv.reader(open(csv_path)) if r]
+    h = next(i for i, r in enumerate(rows) if r[0] == "ID")
+    hdr = rows[h]
+    per = {}
+    for r in rows[h + 1:]:
+        rec = dict(zip(hdr, r))
+        name = re.search(r"(k_\w+)", rec["Kernel Name"]).group(1)
+        v = float(rec["Metric Value"].replace(",", ""))
+        per.setdefault((rec["ID"], name), {})[rec["Metric Name"]] = v
+    acc = {}
+    for (_, name), m in per.items():
+        g = lambda op: m.get("smsp__sass_thread_inst_executed_op_%s_pred_on.sum" % op, 0.0)  # noqa: E731
+        f32 = 2 * g("ffma") + g("fadd") + g("fmul")
+        f64 = 2 * g("dfma") + g("dadd") + g("dmul")
+        acc.setdefault(name, []).append((f32 / ncol, f64 / ncol, m.get("gpu__time_duration.sum", 0.0)))
+    kern = {}
+    for name, v in acc.items():
+        v = sorted(v)
+        f32, f64, _ = v[len(v) // 2]
+        pipe = "fp64" if f64 > f32 else "fp32"
+        kern[name] = {"pipe": pipe, "flop_per_column": f64 if pipe == "fp64" else f32,
+                      "fp32_flop_per_column": f32, "fp64_flop_per_column": f64,
+                      "flop_per_column_height_lambda": (f64 if pipe == "fp64" else f32) / (nz * numw),
+                      "launches": len(v)}
+    doc = {"_comment": "FLOP per column counted by ncu (thread-level ffma/fadd/fmul and dfma/dadd/dmul, an FMA "
+                       "counted as 2) on --probe-kernels %d: %d seeded columns, NZ %d, NUMW %d, hydrostatic, nodes "
+                       "T5 Bx2 By2 Bz2 vz2; bench.py multiplies by the columns of a launch" % (ncol, ncol, nz, numw),
+           "kernels": kern}
+    with open(out_path, "w") as f:
+        json.dump(doc, f, indent=1)
+    print(json.dumps(doc))
+
+
 def reference_arm(a, config, he):
     """``--impl reference``: the CPU restatement of the reference (the Fortran
     reference cannot be built here: no gfortran/MPI/LAPACK) timed on all host
@@ -282,6 +360,12 @@ def main():
     ap.add_argument("--synth-cols", type=int, default=256 * 256)
     ap.add_argument("--rf-chunk", type=int, default=4096, help="columns per full-height RF call")
     ap.add_argument("--no-tune", action="store_true", help="keep the default launch shapes")
+    ap.add_argument("--accept-quantile", type=float, default=0.2,
+                    help="T = this quantile of the calibration set's plain-LM chi2")
+    ap.add_argument("--calib-pixels", type=int, default=32768)
+    ap.add_argument("--sub-steps", type=int, default=4, help="timed steps of each secondary arm (at most --steps)")
+    ap.add_argument("--probe-kernels", type=int, default=0, help="run the FLOP-count launches on N columns and exit")
+    ap.add_argument("--flops-from", default="", help="ncu CSV of --probe-kernels -> profiles/flops.json, then exit")
     a = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -297,6 +381,9 @@ def main():
               "l2": "inputs larger than L2 (observations %.0f MB per GPU)" % (a.field * a.field * nf * 8 / 1e6),
               "parallelism": "pixel tiles sharded per GPU" if world > 1 else "single GPU"}
 
+    if a.flops_from:
+        flops_table(a.flops_from, a.probe_kernels or 2048, a.nz, numw, os.path.join(ROOT, "profiles", "flops.json"))
+        return
     if a.impl == "reference":
         # before anything of the product is imported or loaded
         if rank == 0:
@@ -307,6 +394,9 @@ def main():
     lines = fz.lines_parse(fz.atmos.line_database_text())
     reg = fz.regions_from_lines_section(fz.atmos.lines_section(2), lines)
     assert int(reg["numwave"].sum()) == numw
+    if a.probe_kernels:
+        probe_kernels(fz, lines, reg, a.nz, a.probe_kernels)
+        return
 
     import torch
     from firtez_dz_b200 import warmstart as ws
@@ -367,23 +457,54 @@ def main():
             "chi": torch.empty(a.tile, dtype=torch.float64, device="cuda"),
             "it": torch.empty(a.tile, dtype=torch.int32, device="cuda"),
             "st": torch.empty(a.tile, dtype=torch.int32, device="cuda")}
-    results = {"nn": {}, "plain": {}, "free": {}, "raw": {}, "tau": {}}
+    # ----------------------------------------------------------- calibration
+    # plain LM from the default guess on a separate seeded set (same
+    # generator, same noise; the same set on every rank): T = a quantile of
+    # its chi2, the level at which a warm-start model is accepted
+    t0 = time.perf_counter()
+    ncal = min(a.calib_pixels, a.tile)
+    cal_m = torch.from_numpy(fz.atmos.make_columns(ncal, a.nz, seed=CALIB_SEED)).cuda()
+    cal_syn = torch.empty((ncal, 4, numw), dtype=torch.float64, device="cuda")
+    cal_mo = torch.empty_like(cal_m)
+    ctx.forward_device(cal_m.data_ptr(), ncal, cal_syn.data_ptr(), cal_mo.data_ptr(), 0, stream=stream,
+                       hydrostatic=True)
+    cal_gen = torch.Generator(device="cuda")
+    cal_gen.manual_seed(CALIB_SEED)
+    cal_obs = cal_syn.reshape(ncal, nf) + 1e-3 * torch.randn((ncal, nf), dtype=torch.float64, device="cuda",
+                                                             generator=cal_gen)
+    ntiles = npix // a.tile
+    bufs = {"out": torch.empty((a.tile, 13, a.nz), dtype=torch.float32, device="cuda"),
+            "chi": torch.empty(a.tile, dtype=torch.float64, device="cuda"),
+            "it": torch.empty(a.tile, dtype=torch.int32, device="cuda"),
+            "st": torch.empty(a.tile, dtype=torch.int32, device="cuda")}
+    ctx.invert_device(ncal, cal_obs.data_ptr(), base.data_ptr(), bufs["out"].data_ptr(), bufs["chi"].data_ptr(),
+                      bufs["it"].data_ptr(), bufs["st"].data_ptr(), hydrostatic=True, opts=opts, stream=stream)
+    cal_chi = bufs["chi"][:ncal].clone()
+    quants = {"nn": a.accept_quantile, "nn_q10": 0.1, "nn_q30": 0.3}
+    levels = {arm: float(torch.quantile(cal_chi, q)) for arm, q in quants.items()}
+    accept = {arm: torch.full((a.tile,), t_, dtype=torch.float64, device="cuda") for arm, t_ in levels.items()}
+    calib = {"pixels": ncal, "seed": CALIB_SEED, "quantile": a.accept_quantile, "T": levels["nn"],
+             "median_chi2": float(torch.median(cal_chi)), "seconds": time.perf_counter() - t0,
+             "levels": {arm: {"quantile": quants[arm], "T": levels[arm]} for arm in quants}}
+    del cal_m, cal_syn, cal_mo, cal_obs
+
+    results = {"nn": {}, "plain": {}, "free": {}, "tau": {}, "nn_q10": {}, "nn_q30": {}}
     # the reference's own non-learned guess: SET_TAU's T, B and v_z assists
     # on the default model over the tile as a 512 x 256 field
     tau_init = torch.empty_like(base)
     tau_ny = 256
     tau_nx = a.tile // tau_ny
-    targets = {}
-    # the headline arm's fallback: a pixel whose NN-warm search stagnates (one
-    # rejected or too-small step) while above 1.1x its plain chi2 restarts
-    # once from the default guess in the same pool
-    fb_model = base[0].contiguous()
-    opts_nn = fz.LMOpts(maxsteps=5, maxit=40, dchi2=1e-3, isigma=1e-3, slots=opts.slots, fallback=1.1,
-                        fallback_model=fb_model.data_ptr(), fallback_steps=1)
+    # the deployable rule: the warm-start model is evaluated once; at or
+    # below T it is the result, above T the pixel restarts at once from the
+    # default model (fallback_steps -1) and runs plain LM without the goal
+    # (fallback_free)
+    opts_nn = fz.LMOpts(maxsteps=5, maxit=40, dchi2=1e-3, isigma=1e-3, slots=opts.slots, fallback=1.0,
+                        fallback_model=base1.data_ptr(), fallback_steps=-1, fallback_free=True)
     # one output model buffer per (arm, tile), allocated before any timing:
     # the inverted models are compared with the true atmospheres afterwards
     outs = {(arm, k): torch.empty((a.tile, 13, a.nz), dtype=torch.float32, device="cuda")
-            for arm in results for k in range(ntiles)}
+            for arm in ("plain", "nn", "free", "tau") for k in range(ntiles)}
+    outs_tmp = torch.empty((a.tile, 13, a.nz), dtype=torch.float32, device="cuda")
 
     def step(i, arm):
         k = i % ntiles
@@ -398,12 +519,12 @@ def main():
             # network + node expansion in the library (fz_warm_start_device)
             init = nn_init
             warm.models_device(ctx, a.tile, o.data_ptr(), base1.data_ptr(), init.data_ptr(), stream=stream)
-        tgt = targets[k].data_ptr() if arm in ("nn", "raw") else 0
-        ctx.invert_device(a.tile, o.data_ptr(), init.data_ptr(), outs[(arm, k)].data_ptr(), bufs["chi"].data_ptr(),
+        rule = arm in accept
+        out_m = outs.get((arm, k), outs_tmp)
+        ctx.invert_device(a.tile, o.data_ptr(), init.data_ptr(), out_m.data_ptr(), bufs["chi"].data_ptr(),
                           bufs["it"].data_ptr(), bufs["st"].data_ptr(), hydrostatic=True,
-                          opts=opts_nn if arm == "nn" else opts, stream=stream, target_ptr=tgt)
-        if arm == "plain":
-            targets[k] = bufs["chi"].clone()
+                          opts=opts_nn if rule else opts, stream=stream,
+                          target_ptr=accept[arm].data_ptr() if rule else 0)
         results[arm][k] = (bufs["chi"].cpu().numpy().copy(), bufs["it"].cpu().numpy().copy(),
                            int(bufs["st"].max().item()))
 
@@ -421,10 +542,12 @@ def main():
         barrier()
         torch.cuda.synchronize()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.nvtx.range_push("timed_" + tag)   # a profiler can select the timed launches
         e0.record()
         for i in range(a.warmup, a.warmup + steps):
             step(i, arm)
         e1.record()
+        torch.cuda.nvtx.range_pop()
         torch.cuda.synchronize()
         barrier()
         clocks = sampler.stop()
@@ -439,31 +562,42 @@ def main():
             prof = ctx.profile_read(items=True)
         return maxms(e0.elapsed_time(e1) / steps), clocks, prof
 
-    # plain LM from the default guess: the yardstick, and the chi2 goal of the
-    # headline arm (same tiles: the warm-up tiles first, then the timed ones)
+    # plain LM from the default guess: the yardstick (same tiles: the
+    # warm-up tiles first, then the timed ones)
     ms_pl, clocks_pl, _ = timed("plain", a.steps, a.warmup, "plain")
     plain_value = world * a.tile / (ms_pl * 1e-3)
-    # headline: NN-warm LM, each pixel converged once it reaches its plain-LM
-    # chi2; a pixel that stagnates above 1.1x it restarts once from the
-    # default guess in the same pool (plain LM stays the fallback and the yardstick)
+    # headline: the deployable NN-warm rule at T
     ms_nn, clocks, prof = timed("nn", a.steps, a.warmup, "nn", profile=True)
     value = world * a.tile / (ms_nn * 1e-3)
-    # the same without the fallback
-    ms_raw, _, _ = timed("raw", a.steps, 0, "raw")
-    raw_value = world * a.tile / (ms_raw * 1e-3)
-    # NN-warm LM with the plain stop rules only (its own chi2)
-    ms_fr, _, _ = timed("free", a.steps, 0, "free")
-    free_value = world * a.tile / (ms_fr * 1e-3)
-    # plain LM from SET_TAU's assisted guess (the plain stop rules)
-    ms_tau, _, _ = timed("tau", a.steps, 0, "tau")
-    tau_value = world * a.tile / (ms_tau * 1e-3)
-    common = sorted(set(results["plain"]) & set(results["nn"]) & set(results["free"]) & set(results["raw"])
-                    & set(results["tau"]))
-    cat = lambda arm, j: np.concatenate([results[arm][k][j] for k in common])  # noqa: E731
-    chi_nn, chi_pl, chi_fr, chi_rw = cat("nn", 0), cat("plain", 0), cat("free", 0), cat("raw", 0)
-    it_nn, it_pl, it_fr, it_rw = cat("nn", 1), cat("plain", 1), cat("free", 1), cat("raw", 1)
-    chi_tau, it_tau = cat("tau", 0), cat("tau", 1)
+    sub = max(1, min(a.sub_steps, a.steps))
+    ms_sub = {}
+    for arm in ("nn_q10", "nn_q30", "free", "tau"):
+        ms_sub[arm], _, _ = timed(arm, sub, 1, arm)
+
+    def versus_plain(arm):
+        """chi2 and iterations of an arm against plain LM on the same tiles."""
+        ks = sorted(set(results[arm]) & set(results["plain"]))
+        c = np.concatenate([results[arm][k][0] for k in ks])
+        it = np.concatenate([results[arm][k][1] for k in ks])
+        cp = np.concatenate([results["plain"][k][0] for k in ks])
+        return {"median_chi2": float(np.median(c)), "median_chi2_plain": float(np.median(cp)),
+                "mean_iterations": float(it.mean()),
+                "frac_pixels_at_or_below_plain_chi2": float(np.mean(c <= cp)),
+                "frac_pixels_chi2_above_1.1x_plain": float(np.mean(c > 1.1 * cp)),
+                "frac_pixels_chi2_above_2x_plain": float(np.mean(c > 2.0 * cp)),
+                "pixels_compared": int(c.size)}
+
+    def sub_arm(arm, definition):
+        v = world * a.tile / (ms_sub[arm] * 1e-3)
+        return dict(versus_plain(arm), value=v, unit=UNIT, ms_per_step=ms_sub[arm], steps=sub,
+                    speedup_vs_plain=v / plain_value, definition=definition)
+
+    common = sorted(set(results["plain"]) & set(results["nn"]) & set(results["free"]) & set(results["tau"]))
     status_bad = max(results[arm][k][2] for arm in results for k in results[arm])
+    it_pl = np.concatenate([results["plain"][k][1] for k in sorted(results["plain"])])
+    chi_pl = np.concatenate([results["plain"][k][0] for k in sorted(results["plain"])])
+    nn_cmp = versus_plain("nn")
+    nn_restart = float(np.mean(np.concatenate([results["nn"][k][1] for k in sorted(results["nn"])]) > 1))
 
     # ------------------------------------------------------ parameter errors
     # errors of the inverted atmospheres against the true ones at the heights
@@ -493,7 +627,7 @@ def main():
 
     tru_c = tiles(lambda k: true_models[k * a.tile:(k + 1) * a.tile])
     errors = {arm: height_errors(tiles(lambda k: outs[(arm, k)]), tru_c)
-              for arm in ("plain", "nn", "free", "raw", "tau")}
+              for arm in ("plain", "nn", "free", "tau")}
     errors["nn_prior"] = height_errors(
         tiles(lambda k: prior_models(k)), tru_c)
     errors["default_guess"] = height_errors(base[:1].expand(tru_c.shape[0], -1, -1), tru_c)
@@ -538,27 +672,27 @@ def main():
     del outs, e_m, e_c, e_s
 
     # ------------------------------------------------------------- end to end
-    # host buffers in pinned memory: observations and goals in, models,
-    # chi2, iterations and status out
+    # the headline arm through fz_invert_warm from pinned host memory:
+    # observations, the network's standardisation, the default model, T per
+    # pixel and the fallback model in; models, chi2, iterations and status
+    # out (the network and the LM run on the device between the copies)
     pin = lambda shape, dt: torch.empty(shape, dtype=dt, pin_memory=True).numpy()  # noqa: E731
     h_obs = pin((a.tile, 4, numw), torch.float64)
     h_obs[:] = obs[:a.tile].reshape(a.tile, 4, numw).cpu().numpy()
-    h_init = pin((a.tile, 13, a.nz), torch.float32)
     h_out = (pin((a.tile, 13, a.nz), torch.float32), pin((a.tile,), torch.float64), pin((a.tile,), torch.int32),
              pin((a.tile,), torch.int32))
-    e2e_steps = max(1, a.steps // 2)
-
+    e2e_steps = max(1, min(a.steps, a.sub_steps))
     h_target = pin((a.tile,), torch.float64)
-    h_target[:] = targets[0].cpu().numpy()
-
-    h_fb = pin((13, a.nz), torch.float32)
-    h_fb[:] = fb_model.cpu().numpy()
-    opts_e2e = fz.LMOpts(maxsteps=5, maxit=40, dchi2=1e-3, isigma=1e-3, slots=opts.slots, fallback=1.1,
-                         fallback_model=h_fb.ctypes.data, fallback_steps=1)   # a host pointer for the host-buffer call
+    h_target[:] = levels["nn"]
+    h_base = pin((13, a.nz), torch.float32)
+    h_base[:] = base1.cpu().numpy()
+    opts_e2e = fz.LMOpts(maxsteps=5, maxit=40, dchi2=1e-3, isigma=1e-3, slots=opts.slots, fallback=1.0,
+                         fallback_model=h_base.ctypes.data, fallback_steps=-1,
+                         fallback_free=True)   # a host pointer for the host-buffer call
+    warm._hnorm = warm.norm()
 
     def e2e_step():
-        warm.initial_models(h_obs, out=h_init)
-        ctx.invert(h_obs, h_init, hydrostatic=True, opts=opts_e2e, target=h_target, out=h_out)
+        ctx.invert_warm(h_obs, warm, base=h_base, hydrostatic=True, opts=opts_e2e, target=h_target, out=h_out)
 
     e2e_step()
     barrier()
@@ -568,13 +702,13 @@ def main():
         e2e_step()
     torch.cuda.synchronize()
     ms_e2e = maxms((time.perf_counter() - t0) * 1e3 / e2e_steps)
-    e2e = {"value": world * a.tile / (ms_e2e * 1e-3), "unit": UNIT,
-           "h2d_bytes_per_step": 2 * a.tile * nf * 8 + a.tile * 13 * a.nz * 4 + a.tile * 8,
-           "d2h_bytes_per_step": 2 * a.tile * 13 * a.nz * 4 + a.tile * (8 + 4 + 4),
-           "note": "the headline arm from host memory: WarmStart.initial_models (host observations in, host "
-                   "models out) then fz_invert with the plain-LM chi2 goals (host observations, models and "
-                   "goals in; models, chi2, iterations and status out); pinned host buffers; wall clock around "
-                   "the calls"}
+    nm_ = 13 * a.nz
+    e2e = {"value": world * a.tile / (ms_e2e * 1e-3), "unit": UNIT, "steps": e2e_steps,
+           "h2d_bytes_per_step": a.tile * nf * 8 + a.tile * 8 + warm._hnorm.nbytes + 2 * nm_ * 4,
+           "d2h_bytes_per_step": a.tile * nm_ * 4 + a.tile * (8 + 4 + 4),
+           "note": "the headline arm through fz_invert_warm (one C-ABI call per step): host observations, "
+                   "standardisation, default model, T per pixel and fallback model in; models, chi2, iterations "
+                   "and status out; pinned host buffers; wall clock around the calls"}
 
     # --------------------------------------------------------- synthesis rate
     ns = a.synth_cols
@@ -593,7 +727,8 @@ def main():
     e1.record()
     torch.cuda.synchronize()
     ctx.profile(False)
-    sprof = ctx.profile_read()
+    sprof_items = ctx.profile_read(items=True)
+    sprof = {k: v[:2] for k, v in sprof_items.items()}
     ms_syn = maxms(e0.elapsed_time(e1) / 5)
     synthesis = {"value": world * ns * numw / (ms_syn * 1e-3), "unit": "columns*lambda/s",
                  "workload": "%d columns x %d heights x %d lambda, hydrostatic" % (ns, a.nz, numw),
@@ -738,12 +873,40 @@ def main():
         return
 
     # -------------------------------------------------------------- roofline
+    # each kernel of the FLOP table against its pipe (FP32 or FP64 FLOP per
+    # column counted by ncu x mean columns per launch / mean launch time,
+    # over the peak of an FMA-chain kernel measured here); HBM as the side
+    # figure: algorithmic bytes per column x columns / launch time
     hbm, how = peaks()
-    per_launch = {k: (v[0] / max(v[1], 1), v[1], v[2] / max(v[1], 1)) for k, v in prof.items() if v[1]}
+    fp32 = fz.measure_fp32_peak(local)
+    fp64 = fz.measure_fp64_peak(local)
+    pipe_peak = {"fp32": fp32, "fp64": fp64}
+    flops_tab, traffic_tab = {}, {}
+    for fn_, dst in (("flops.json", flops_tab), ("traffic.json", traffic_tab)):
+        pth = os.path.join(ROOT, "profiles", fn_)
+        if os.path.exists(pth):
+            d_ = json.load(open(pth))
+            dst.update(d_.get("kernels", d_))
+
+    def launch_means(pr):
+        return {k: (v[0] / max(v[1], 1), v[1], v[2] / max(v[1], 1)) for k, v in pr.items() if v[1]}
+
+    def pipe_lines(pr):
+        out_ = {}
+        for k, (kms_, n_, cols_) in launch_means(pr).items():
+            e_ = flops_tab.get(k)
+            if not isinstance(e_, dict):
+                continue
+            ach = e_["flop_per_column"] * cols_ / (kms_ * 1e-3) / 1e12
+            out_[k] = {"pipe": e_["pipe"], "achieved_tflops": ach, "peak_tflops": pipe_peak[e_["pipe"]],
+                       "frac": ach / pipe_peak[e_["pipe"]], "mean_launch_ms": kms_, "launches": n_,
+                       "mean_columns_per_launch": cols_}
+        return out_
+
+    per_launch = launch_means(prof)
     kname = max(prof, key=lambda k: prof[k][0])
     kms, _, cols = per_launch[kname]            # mean launch time, mean columns per launch
     np_ = 13
-    flop = None
     if kname == "k_synth_rf":
         alg_col = a.nz * 6 * 4 + nf * 8 + np_ * nf * 4      # model in, RSYN1D + EQVDSYN out
     elif kname in ("k_opac_rf", "k_chemder"):
@@ -754,52 +917,54 @@ def main():
         alg_col = nf * 8 + a.nz * 4                          # RSYN1D and log tau5 out
     else:
         alg_col = a.nz * 6 * 4
-    if "k_synth_rf" in per_launch:
-        flop = per_launch["k_synth_rf"][2] * a.nz * numw * 4400.0
-    alg = alg_col * cols
-    achieved = alg / (kms * 1e-3) / 1e9
-    S = cols
-    traffic = None
-    tf = os.path.join(ROOT, "profiles", "traffic.json")
-    if os.path.exists(tf):
-        try:
-            per_col = json.load(open(tf)).get(kname)
-            traffic = per_col * S if per_col else None
-        except Exception:
-            traffic = None
-    fp32 = fz.measure_fp32_peak(local)
+    hbm_ach = alg_col * cols / (kms * 1e-3) / 1e9
+    traffic = traffic_tab.get(kname) * cols if isinstance(traffic_tab.get(kname), (int, float)) else None
+    pipes = pipe_lines(prof)
+    if kname in pipes:
+        pl_ = pipes[kname]
+        roofline = {"bound": pl_["pipe"], "kernel": kname, "achieved": pl_["achieved_tflops"],
+                    "peak": pl_["peak_tflops"], "unit": "TFLOP/s", "frac": pl_["frac"], "traffic": traffic,
+                    "peak_source": "measured in this run: FMA-chain kernel (fz_measure_%s_peak), of measured"
+                                   % pl_["pipe"],
+                    "flop_per_column": flops_tab[kname]["flop_per_column"],
+                    "flop_source": "ncu thread-level ffma/fadd/fmul (dfma/dadd/dmul) counts, an FMA as 2, on "
+                                   "2048 columns of this workload (profiles/flops.json)",
+                    "mean_launch_ms": kms, "mean_columns_per_launch": cols,
+                    "hbm_side": {"achieved_gbs": hbm_ach, "peak_gbs": hbm, "frac": hbm_ach / hbm,
+                                 "algorithmic_bytes_per_launch": alg_col * cols,
+                                 "peak_source": how + " (MEASURED_PEAKS.json hbm_gbs)" if how == "measured" else how}}
+    else:
+        roofline = {"bound": "hbm", "kernel": kname, "achieved": hbm_ach, "peak": hbm, "unit": "GB/s",
+                    "frac": hbm_ach / hbm, "traffic": traffic,
+                    "peak_source": how + " (MEASURED_PEAKS.json hbm_gbs)" if how == "measured" else how,
+                    "algorithmic_bytes_per_launch": alg_col * cols, "mean_launch_ms": kms,
+                    "mean_columns_per_launch": cols}
+    synthesis["pipe_rooflines"] = pipe_lines(sprof_items)
+    nchunk = -(-a.tile // 16384)
     out = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps, "warmup": a.warmup,
            "ms_per_step": ms_nn, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "fp32",
            "data": "synthetic (seeded atmospheres, firtez-dz_b200/atmos.py; observations = GPU synthesis + "
                    "1e-3 noise)",
            "config": dict(config, autotuned=tuned if tuned else "off (--no-tune): slots %d" % a.slots),
+           "definition": "pixels/s of the deployable NN-warm rule: the warm-start model of every pixel is "
+                         "evaluated once and kept where its chi2 <= T (T = the %.2f quantile of plain-LM chi2 on "
+                         "a separate %d-pixel calibration set inverted before the timed region); every other "
+                         "pixel restarts at once from the default guess in the same slot pool and runs plain LM "
+                         "(the reference's stop rules)" % (a.accept_quantile, ncal),
+           "calibration": calib,
            "plain": {"value": plain_value, "unit": UNIT, "ms_per_step": ms_pl,
                      "median_chi2": float(np.median(chi_pl)), "mean_iterations": float(it_pl.mean()),
                      "clocks": clocks_pl},
-           "nn_warm": {"value": value, "definition": "NN-warm LM; a pixel is converged when its chi2 reaches its "
-                                                     "plain-LM chi2 or by the plain stop rules; a pixel whose "
-                                                     "search stagnates once (a rejected or too-small step, "
-                                                     "STEPS >= 1) while above 1.1x its plain chi2 restarts once "
-                                                     "from the default guess in the same slot pool",
-                       "median_chi2": float(np.median(chi_nn)), "mean_iterations": float(it_nn.mean()),
-                       "speedup_vs_plain": value / plain_value,
-                       "frac_pixels_at_or_below_plain_chi2": float(np.mean(chi_nn <= chi_pl)),
-                       "frac_pixels_chi2_above_1.1x_plain": float(np.mean(chi_nn > 1.1 * chi_pl)),
-                       "pixels_compared": int(chi_nn.size), "status_errors": status_bad, "mlp": mlp_info},
-           "nn_warm_no_fallback": {"value": raw_value, "definition": "the headline arm without the restart",
-                                   "median_chi2": float(np.median(chi_rw)), "mean_iterations": float(it_rw.mean()),
-                                   "speedup_vs_plain": raw_value / plain_value,
-                                   "frac_pixels_chi2_above_1.1x_plain": float(np.mean(chi_rw > 1.1 * chi_pl))},
-           "nn_warm_free": {"value": free_value, "definition": "NN-warm LM with the plain stop rules only",
-                            "median_chi2": float(np.median(chi_fr)), "mean_iterations": float(it_fr.mean()),
-                            "speedup_vs_plain": free_value / plain_value,
-                            "frac_pixels_chi2_above_1.1x_plain": float(np.mean(chi_fr > 1.1 * chi_pl))},
-           "set_tau_plain": {"value": tau_value, "definition": "LM with the plain stop rules from the default "
-                                                             "model after SET_TAU's T, B and v_z assists over the "
-                                                             "tile (the reference's non-learned initial guess)",
-                             "median_chi2": float(np.median(chi_tau)), "mean_iterations": float(it_tau.mean()),
-                             "speedup_vs_plain": tau_value / plain_value,
-                             "frac_pixels_chi2_above_1.1x_plain": float(np.mean(chi_tau > 1.1 * chi_pl))},
+           "nn_warm": dict(nn_cmp, value=value, speedup_vs_plain=value / plain_value,
+                           frac_pixels_restarted=nn_restart, status_errors=status_bad, mlp=mlp_info,
+                           note="mean_iterations counts the evaluation of the warm-start model as one; a "
+                                "restarted pixel adds its plain-LM iterations"),
+           "nn_warm_q10": sub_arm("nn_q10", "the headline rule with T at the 0.10 quantile"),
+           "nn_warm_q30": sub_arm("nn_q30", "the headline rule with T at the 0.30 quantile"),
+           "nn_warm_free": sub_arm("free", "NN-warm LM with the plain stop rules only"),
+           "set_tau_plain": sub_arm("tau", "LM with the plain stop rules from the default model after "
+                                           "SET_TAU's T, B and v_z assists over the tile (the reference's "
+                                           "non-learned initial guess)"),
            "parameter_errors": dict(errors, definition="errors of T, Bz, v_z and |B_perp| of the inverted "
                                            "atmospheres against the true ones at the heights where the true "
                                            "log tau5 is in [-3, 0], over the compared pixels"),
@@ -808,30 +973,20 @@ def main():
            "synthesis_lsf": synthesis_lsf,
            "errors_mode": errors_mode,
            "v3_files": v3_files,
-           "roofline": {"bound": "hbm", "kernel": kname, "achieved": achieved, "peak": hbm, "unit": "GB/s",
-                        "frac": achieved / hbm, "traffic": traffic,
-                        "peak_source": how + " (MEASURED_PEAKS.json hbm_gbs)" if how == "measured" else how,
-                        "algorithmic_bytes_per_launch": alg, "mean_launch_ms": kms,
-                        "mean_columns_per_launch": S},
+           "roofline": roofline,
+           "pipe_rooflines": pipes,
            "kernel_ms": {k: v[0] for k, v in per_launch.items()},
            "kernel_share": {k: prof[k][0] / sum(v[0] for v in prof.values()) for k in per_launch},
            "kernel_timing": "per-kernel CUDA events of the library on its launching stream, over a repetition "
-                            "of the timed NN-warm steps (the timed pass itself runs without them)",
+                            "of the timed headline steps (the timed pass itself runs without them)",
            "kernel_launches": {k: v[1] for k, v in per_launch.items()},
            "kernel_columns_per_launch": {k: v[2] for k, v in per_launch.items()},
            "e2e": e2e,
-           # kernels counted by the context plus, per step, the network
-           # (one conversion + 4 GEMMs)
-           "gpu_launches": int(sum(v[1] for v in prof.values()) + 5 * a.steps),
+           # kernels counted by the context plus, per step, the warm start:
+           # per 16384-pixel chunk one conversion + 4 GEMMs, then the node
+           # expansion
+           "gpu_launches": int(sum(v[1] for v in prof.values()) + (5 * nchunk + 1) * a.steps),
            "clocks": clocks}
-    if flop is not None:
-        kr = per_launch["k_synth_rf"][0]
-        out["fp32_roofline"] = {"kernel": "k_synth_rf", "achieved_tflops": flop / (kr * 1e-3) / 1e12,
-                                "peak_tflops": fp32, "frac": flop / (kr * 1e-3) / 1e12 / fp32,
-                                "flop_model": "4400 FLOP per column*height*lambda (synthesis + 6 response "
-                                              "functions), mean %.0f columns per launch"
-                                              % per_launch["k_synth_rf"][2],
-                                "peak_source": "measured FMA-chain kernel (fz_measure_fp32_peak)"}
     if world == 1:
         # the oracle on the host cores, with its own line parse (the same rows)
         olines, oreg = cpu_workload()
