@@ -249,6 +249,7 @@ def cpu_synth_sample(lines, reg, he, nz, ncol, seed, nthreads=0):
 
 PROBE_SEED = 3
 CALIB_SEED = 909090
+C5_SEED = 5050
 
 
 def probe_kernels(fz, lines, reg, nz, n):
@@ -310,6 +311,116 @@ def flops_table(csv_path, ncol, nz, numw, out_path):
     print(json.dumps(doc))
 
 
+def c5_sub_metric(a, fz, rank, world, stream, maxms):
+    """The large multi-line workload: columns of a 1024 x 1024 field x 160
+    heights, Fe I 6301.5, 6302.5, 15648.5 and 15652.9 x 96 wavelengths each
+    (NUMW 384, NFREQ 1536), |B| up to 4000 G, noise 1e-3 Ic.  Its own network
+    (MLP 1536-1024-1024-512-13) trained on --c5-train-pairs pairs, its own
+    calibration (plain LM on 16,384 pixels, T at --accept-quantile), then the
+    deployable NN-warm rule against plain LM on --c5-tiles tiles of 65,536
+    pixels of the field (one warm-up step each, CUDA events, the max over
+    ranks)."""
+    import torch
+    from firtez_dz_b200 import warmstart as ws
+    nz, tile = 160, 65536
+    lines = fz.lines_parse(fz.atmos.line_database_text())
+    reg = fz.regions_from_lines_section(fz.atmos.lines_section(4), lines)
+    ctx = fz.Synthesis(lines, reg, nz=nz, device=torch.cuda.current_device())
+    numw = ctx.numw
+    nf = 4 * numw
+    npx = tile * a.c5_tiles
+    t0 = time.perf_counter()
+    obs = torch.empty((npx, nf), dtype=torch.float64, device="cuda")
+    gen = torch.Generator(device="cuda")
+    gen.manual_seed(5151 + rank)
+    for i in range(0, npx, tile):
+        m = torch.from_numpy(fz.atmos.make_columns(tile, nz, seed=C5_SEED + 1000 * rank + i // tile,
+                                                   bmax=4000.0)).cuda()
+        syn = torch.empty((tile, 4, numw), dtype=torch.float64, device="cuda")
+        mo = torch.empty_like(m)
+        ctx.forward_device(m.data_ptr(), tile, syn.data_ptr(), mo.data_ptr(), 0, stream=stream, hydrostatic=True)
+        obs[i:i + tile] = syn.reshape(tile, nf) + 1e-3 * torch.randn((tile, nf), dtype=torch.float64,
+                                                                     device="cuda", generator=gen)
+    del m, syn, mo
+    warm = ws.WarmStart(nz, NODES, numw, seed=11 + rank)
+    x, t = warm.make_training_set(ctx, a.c5_train_pairs, seed=61 + rank, noise=1e-3, bmax=4000.0)
+    loss = warm.fit(x, t, epochs=a.c5_epochs, batch=1024, lr=1e-3, seed=1)
+    del x, t
+    torch.cuda.empty_cache()
+    t_train = time.perf_counter() - t0
+    ctx.rf_nodes(NODES)
+    base = torch.from_numpy(ws.default_models(tile, nz)).cuda()
+    base1 = base[0].contiguous()
+    init = torch.empty_like(base)
+    out = torch.empty_like(base)
+    chi = torch.empty(tile, dtype=torch.float64, device="cuda")
+    it = torch.empty(tile, dtype=torch.int32, device="cuda")
+    st = torch.empty(tile, dtype=torch.int32, device="cuda")
+    slots = min(16384, tile)
+    opts = fz.LMOpts(maxsteps=5, maxit=40, dchi2=1e-3, isigma=1e-3, slots=slots)
+    # calibration on a separate seeded set
+    ncal = 16384
+    cm = torch.from_numpy(fz.atmos.make_columns(ncal, nz, seed=C5_SEED + 777, bmax=4000.0)).cuda()
+    cs = torch.empty((ncal, 4, numw), dtype=torch.float64, device="cuda")
+    cmo = torch.empty_like(cm)
+    ctx.forward_device(cm.data_ptr(), ncal, cs.data_ptr(), cmo.data_ptr(), 0, stream=stream, hydrostatic=True)
+    cg = torch.Generator(device="cuda")
+    cg.manual_seed(C5_SEED)
+    cobs = cs.reshape(ncal, nf) + 1e-3 * torch.randn((ncal, nf), dtype=torch.float64, device="cuda", generator=cg)
+    ctx.invert_device(ncal, cobs.data_ptr(), base.data_ptr(), out.data_ptr(), chi.data_ptr(), it.data_ptr(),
+                      st.data_ptr(), hydrostatic=True, opts=opts, stream=stream)
+    T = float(torch.quantile(chi[:ncal], a.accept_quantile))
+    del cm, cs, cmo, cobs
+    accept = torch.full((tile,), T, dtype=torch.float64, device="cuda")
+    opts_nn = fz.LMOpts(maxsteps=5, maxit=40, dchi2=1e-3, isigma=1e-3, slots=slots, fallback=1.0,
+                        fallback_model=base1.data_ptr(), fallback_steps=-1, fallback_free=True)
+    res = {"plain": [], "nn": []}
+
+    def run(arm, k, keep):
+        o = obs[k * tile:(k + 1) * tile]
+        if arm == "plain":
+            ini = base
+        else:
+            ini = init
+            warm.models_device(ctx, tile, o.data_ptr(), base1.data_ptr(), ini.data_ptr(), stream=stream)
+        ctx.invert_device(tile, o.data_ptr(), ini.data_ptr(), out.data_ptr(), chi.data_ptr(), it.data_ptr(),
+                          st.data_ptr(), hydrostatic=True, opts=opts_nn if arm == "nn" else opts, stream=stream,
+                          target_ptr=accept.data_ptr() if arm == "nn" else 0)
+        if keep:
+            res[arm].append((chi.cpu().numpy().copy(), it.cpu().numpy().copy(), int(st.max().item())))
+
+    ms = {}
+    for arm in ("plain", "nn"):
+        run(arm, 0, False)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for k in range(a.c5_tiles):
+            run(arm, k, True)
+        e1.record()
+        torch.cuda.synchronize()
+        ms[arm] = maxms(e0.elapsed_time(e1) / a.c5_tiles)
+    cp = np.concatenate([r[0] for r in res["plain"]])
+    cn = np.concatenate([r[0] for r in res["nn"]])
+    itp = np.concatenate([r[1] for r in res["plain"]])
+    itn = np.concatenate([r[1] for r in res["nn"]])
+    vp = world * tile / (ms["plain"] * 1e-3)
+    vn = world * tile / (ms["nn"] * 1e-3)
+    return {"value": vn, "unit": UNIT, "plain_value": vp, "speedup_vs_plain": vn / vp,
+            "median_chi2": float(np.median(cn)), "median_chi2_plain": float(np.median(cp)),
+            "mean_iterations": float(itn.mean()), "mean_iterations_plain": float(itp.mean()),
+            "frac_pixels_chi2_above_1.1x_plain": float(np.mean(cn > 1.1 * cp)),
+            "frac_pixels_restarted": float(np.mean(itn > 1)),
+            "status_errors": max(r[2] for arm in res for r in res[arm]),
+            "ms_per_step": ms["nn"], "ms_per_step_plain": ms["plain"], "T": T, "calibration_pixels": ncal,
+            "mlp": {"layers": [nf, 1024, 1024, 512, 13], "train_pairs": a.c5_train_pairs, "epochs": a.c5_epochs,
+                    "final_loss": loss, "field_and_training_s": t_train},
+            "workload": "%d tiles of %d pixels of a seeded 1024x1024 field (rank %d's rows), %d heights, Fe I "
+                        "6301.5, 6302.5, 15648.5, 15652.9 x 96 lambda (NUMW %d), |B| <= 4000 G, noise 1e-3 Ic, "
+                        "nodes T5 Bx2 By2 Bz2 vz2; the headline's rule and stop rules, %d slots"
+                        % (a.c5_tiles, tile, rank, nz, numw, slots)}
+
+
 def reference_arm(a, config, he):
     """``--impl reference``: the CPU restatement of the reference (the Fortran
     reference cannot be built here: no gfortran/MPI/LAPACK) timed on all host
@@ -364,6 +475,9 @@ def main():
                     help="T = this quantile of the calibration set's plain-LM chi2")
     ap.add_argument("--calib-pixels", type=int, default=32768)
     ap.add_argument("--sub-steps", type=int, default=4, help="timed steps of each secondary arm (at most --steps)")
+    ap.add_argument("--c5-tiles", type=int, default=2, help="65536-pixel tiles of the four-line workload (0: off)")
+    ap.add_argument("--c5-train-pairs", type=int, default=524288)
+    ap.add_argument("--c5-epochs", type=int, default=4)
     ap.add_argument("--probe-kernels", type=int, default=0, help="run the FLOP-count launches on N columns and exit")
     ap.add_argument("--flops-from", default="", help="ncu CSV of --probe-kernels -> profiles/flops.json, then exit")
     a = ap.parse_args()
@@ -868,6 +982,11 @@ def main():
                                                                                               a.nz, numw, ncr),
                 "host_record_io": dict(host_io, slice_pixels=nsl, directory=base_dir or "tempfile default")}
 
+    # ------------------------------------------------ four-line workload (C5)
+    del obs, true_models, outs_tmp
+    torch.cuda.empty_cache()
+    c5 = c5_sub_metric(a, fz, rank, world, stream, maxms) if a.c5_tiles > 0 else None
+
     if rank != 0:
         ranks.close()
         return
@@ -973,6 +1092,7 @@ def main():
            "synthesis_lsf": synthesis_lsf,
            "errors_mode": errors_mode,
            "v3_files": v3_files,
+           "four_lines_c5": c5,
            "roofline": roofline,
            "pipe_rooflines": pipes,
            "kernel_ms": {k: v[0] for k, v in per_launch.items()},

@@ -171,10 +171,11 @@ class WarmStart:
             j += nj
         return m
 
-    def make_training_set(self, synth, ncol, seed, noise=1e-3, chunk=65536):
-        """Seeded atmospheres synthesised on the GPU (hydrostatic) plus
-        Gaussian noise: returns device tensors (x (ncol, 4 numw), t (ncol, nout))
-        normalised with the set's own mean and spread."""
+    def make_training_set(self, synth, ncol, seed, noise=1e-3, chunk=65536, bmax=2500.0):
+        """Seeded atmospheres (|B| up to bmax G) synthesised on the GPU
+        (hydrostatic) plus Gaussian noise: returns device tensors (x (ncol,
+        4 numw), t (ncol, nout)) normalised with the set's own mean and
+        spread."""
         import torch
         x = torch.empty((ncol, 4 * self.numw), dtype=torch.float32, device="cuda")
         t = np.empty((ncol, self.nout))
@@ -183,7 +184,7 @@ class WarmStart:
         stream = torch.cuda.current_stream().cuda_stream
         for i in range(0, ncol, chunk):
             n = min(chunk, ncol - i)
-            m = torch.from_numpy(atmos.make_columns(n, self.nz, seed=int(seed) * 1000003 + i)).cuda()
+            m = torch.from_numpy(atmos.make_columns(n, self.nz, seed=int(seed) * 1000003 + i, bmax=bmax)).cuda()
             syn = torch.empty((n, 4, self.numw), dtype=torch.float64, device="cuda")
             mo = torch.empty_like(m)
             synth.forward_device(m.data_ptr(), n, syn.data_ptr(), mo.data_ptr(), 0, stream=stream, hydrostatic=True)

@@ -88,3 +88,27 @@ def test_reference_arm_loads_nothing_of_the_product():
     assert line["impl"] == "reference" and line["cpu_baseline"]["kind"] == "port"
     got = json.loads(lines[-1])
     assert got == {"orc": True, "fz": False, "pkg": False}
+
+
+def test_flops_table_from_an_ncu_csv(tmp_path):
+    """--flops-from: thread-level opcode counts of an ncu CSV -> FLOP per
+    column (an FMA as 2), the pipe with more FLOP, the median launch."""
+    bench = _bench()
+    hdr = ["ID", "Kernel Name", "Metric Name", "Metric Value"]
+    rows = []
+    for i, (name, ffma, dfma) in enumerate((("void k_synth_rf<1, 0, 256, 0>(int)", 1000, 4),
+                                            ("void k_chain<1, 32>(int)", 2, 500),
+                                            ("void k_chain<1, 16>(int)", 2, 700),
+                                            ("void k_chain<1, 32>(int)", 2, 600))):
+        for op, v in (("ffma", ffma), ("fadd", 10), ("fmul", 20), ("dfma", dfma), ("dadd", 0), ("dmul", 0)):
+            rows.append([str(i), name, "smsp__sass_thread_inst_executed_op_%s_pred_on.sum" % op, "{:,}".format(v)])
+        rows.append([str(i), name, "gpu__time_duration.sum", "1000"])
+    csvf = tmp_path / "f.csv"
+    csvf.write_text("==PROF== banner\n" + "\n".join(",".join('"%s"' % c for c in r) for r in [hdr] + rows) + "\n")
+    out = tmp_path / "flops.json"
+    bench.flops_table(str(csvf), 10, 2, 5, str(out))
+    k = json.load(open(out))["kernels"]
+    assert k["k_synth_rf"]["pipe"] == "fp32" and k["k_synth_rf"]["flop_per_column"] == (2000 + 30) / 10
+    assert k["k_chain"]["pipe"] == "fp64" and k["k_chain"]["launches"] == 3
+    assert k["k_chain"]["flop_per_column"] == 1200 / 10          # the median of 1000, 1200, 1400
+    assert k["k_synth_rf"]["flop_per_column_height_lambda"] == k["k_synth_rf"]["flop_per_column"] / 10
