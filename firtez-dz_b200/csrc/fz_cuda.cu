@@ -650,6 +650,29 @@ __global__ void __launch_bounds__(256) k_opac_rf(const DevParams* __restrict__ P
   }
 }
 
+// Offset (floats, 16-byte aligned) of the per-thread sums of k_synth_rf
+// behind the slab (nz x sw), the coefficient table (nz x np) and the node
+// accumulators (np x 4 x nthr); the block's dynamic shared memory is that
+// offset plus six float4 a thread.
+__host__ __device__ __forceinline__ int rf_sums_off(int nz, int sw, int np, int nthr) {
+  return (nz * sw + nz * np + np * 4 * nthr + 3) & ~3;
+}
+
+// A thread's own float4 in shared memory, stored and loaded as volatile
+// instructions: the loads are issued where they stand, so the values are not
+// kept in registers between the store and the loads.
+__device__ __forceinline__ void sts4(float4* p, float a, float b, float c, float d) {
+  asm volatile("st.shared.v4.f32 [%0], {%1, %2, %3, %4};" ::"r"(static_cast<unsigned>(__cvta_generic_to_shared(p))),
+               "f"(a), "f"(b), "f"(c), "f"(d));
+}
+__device__ __forceinline__ float4 lds4(const float4* p) {
+  float4 v;
+  asm volatile("ld.shared.v4.f32 {%0, %1, %2, %3}, [%4];"
+               : "=f"(v.x), "=f"(v.y), "=f"(v.z), "=f"(v.w)
+               : "r"(static_cast<unsigned>(__cvta_generic_to_shared(p))));
+  return v;
+}
+
 // Linear maps from the per-type (sigma_red, pi, sigma_blue) sums of one line
 // to the seven matrix elements (eta_I,Q,U,V, rho_Q,U,V), the grouping of the
 // component accumulation of src/absorption_matrix.f90:1948-2278.
@@ -717,6 +740,9 @@ __global__ void __launch_bounds__(MAXT, (MAXT <= 256 ? 2 : 1)) k_synth_rf(const 
   float* sm = reinterpret_cast<float*>(sm_rf4);
   float* coef = sm + nz * sw;
   float* Dacc = coef + nz * np;
+  // the per-wavelength sums of the single-line path, six float4 a thread
+  // (vector v of thread l at sums[v * nthr + l]), after the accumulators
+  float4* sums = reinterpret_cast<float4*>(sm + rf_sums_off(nz, sw, np, nthr));
   {
     const float4* src = reinterpret_cast<const float4*>(slab + (size_t)col * nz * sw);
     const int n4 = nz * sw / 4;
@@ -817,6 +843,15 @@ __global__ void __launch_bounds__(MAXT, (MAXT <= 256 ? 2 : 1)) k_synth_rf(const 
           }
         }
       }
+      // the sums wait in shared memory through the operator algebra and are
+      // read back per parameter: 24 registers fewer across the loop below
+      float4* su = sums + l;
+      sts4(su, hh[0], hh[1], hh[2], ff[0]);
+      sts4(su + nthr, ff[1], ff[2], av[0], av[1]);
+      sts4(su + 2 * nthr, av[2], ca[0], ca[1], ca[2]);
+      sts4(su + 3 * nthr, avu[0], avu[1], avu[2], cau[0]);
+      sts4(su + 4 * nthr, cau[1], cau[2], avs[0], avs[1]);
+      sts4(su + 5 * nthr, avs[2], cas[0], cas[1], cas[2]);
       float tI = row[4 + r], tQ, tU, tV, rQ, rU, rV;
       {
         const float hs = hh[0] + hh[2], fs = ff[0] + ff[2];
@@ -871,6 +906,10 @@ __global__ void __launch_bounds__(MAXT, (MAXT <= 256 ? 2 : 1)) k_synth_rf(const 
         float dt[7], tmp[7];
         if (p == 0) {
           // T at constant Pg: dKLIN, du/dT = -u/(2T), da/dT
+          const float4 s0 = lds4(su), s1 = lds4(su + nthr), s2 = lds4(su + 2 * nthr), s3 = lds4(su + 3 * nthr),
+                       s4 = lds4(su + 4 * nthr);
+          const float hh[3] = {s0.x, s0.y, s0.z}, ff[3] = {s0.w, s1.x, s1.y}, av[3] = {s1.z, s1.w, s2.x};
+          const float ca[3] = {s2.y, s2.z, s2.w}, avu[3] = {s3.x, s3.y, s3.z}, cau[3] = {s3.w, s4.x, s4.y};
           float xe[3], xr[3];
 #pragma unroll
           for (int t = 0; t < 3; ++t) {
@@ -885,6 +924,9 @@ __global__ void __launch_bounds__(MAXT, (MAXT <= 256 ? 2 : 1)) k_synth_rf(const 
           dt[0] = row[dkoff] + dt[0];
         } else if (p == 1) {
           // Pg at constant T: dKLIN and da/dPg
+          const float4 s0 = lds4(su), s1 = lds4(su + nthr), s2 = lds4(su + 2 * nthr);
+          const float hh[3] = {s0.x, s0.y, s0.z}, ff[3] = {s0.w, s1.x, s1.y}, av[3] = {s1.z, s1.w, s2.x};
+          const float ca[3] = {s2.y, s2.z, s2.w};
           lmap(g, ca, av, tmp);
           float base[7];
           lmap(g, hh, ff, base);
@@ -893,7 +935,9 @@ __global__ void __launch_bounds__(MAXT, (MAXT <= 256 ? 2 : 1)) k_synth_rf(const 
           dt[0] = row[dkoff + 1] + dt[0];
         } else if (p < 5) {
           // B_i: geometry factors and the shift term du/dB
-          const float ncs[3] = {-cas[0], -cas[1], -cas[2]};
+          const float4 s0 = lds4(su), s1 = lds4(su + nthr), s4 = lds4(su + 4 * nthr), s5 = lds4(su + 5 * nthr);
+          const float hh[3] = {s0.x, s0.y, s0.z}, ff[3] = {s0.w, s1.x, s1.y}, avs[3] = {s4.z, s4.w, s5.x};
+          const float ncs[3] = {-s5.y, -s5.z, -s5.w};
           float sh7[7];
           lmap(g, avs, ncs, sh7);
           const float* dg = row + dgoff + 5 * (p - 2);
@@ -904,7 +948,9 @@ __global__ void __launch_bounds__(MAXT, (MAXT <= 256 ? 2 : 1)) k_synth_rf(const 
           for (int x = 0; x < 7; ++x) dt[x] = kldz * fmaf(kb, sh7[x], tmp[x]);
         } else {
           // v_z: du/dv = lu_duv / Doppler width
-          const float nca[3] = {-ca[0], -ca[1], -ca[2]};
+          const float4 s1 = lds4(su + nthr), s2 = lds4(su + 2 * nthr);
+          const float av[3] = {s1.z, s1.w, s2.x};
+          const float nca[3] = {-s2.y, -s2.z, -s2.w};
           lmap(g, av, nca, tmp);
           const float kv = kldz * P.lu_duv[lb] * idd;
 #pragma unroll
@@ -1861,8 +1907,14 @@ int launch_forward(fz_ctx* c, int ncol, const float* d_model, int hydrostatic, d
 
 size_t rf_smem(const fz_ctx* c) {
   const int threads = (c->numw + 31) & ~31;
-  return ((size_t)c->nz * rf_w(c->nreg, c->nlu) + (size_t)c->nz * c->rf.np + (size_t)c->rf.np * 4 * threads) *
+  return ((size_t)rf_sums_off(c->nz, rf_w(c->nreg, c->nlu), c->rf.np, threads) + (size_t)24 * threads) *
          sizeof(float);
+}
+
+// the same for the FULL variant (no coefficient table or accumulators)
+size_t rf_smem_full(const fz_ctx* c) {
+  const int threads = (c->numw + 31) & ~31;
+  return ((size_t)rf_sums_off(c->nz, rf_w(c->nreg, c->nlu), 0, threads) + (size_t)24 * threads) * sizeof(float);
 }
 
 // The response-function kernels run one thread per wavelength in blocks of
@@ -1871,8 +1923,7 @@ size_t rf_smem(const fz_ctx* c) {
 // the full response functions).
 int rf_check(const fz_ctx* c) {
   if (((c->numw + 31) & ~31) > 512) return FZ_ERR_LIMIT;
-  const size_t full = (size_t)c->nz * rf_w(c->nreg, c->nlu) * sizeof(float);
-  if ((c->rf_full ? full : rf_smem(c)) > 227 * 1024) return FZ_ERR_LIMIT;
+  if ((c->rf_full ? rf_smem_full(c) : rf_smem(c)) > 227 * 1024) return FZ_ERR_LIMIT;
   return 0;
 }
 
@@ -1901,7 +1952,7 @@ int ensure_rf_scratch(fz_ctx* c, int ncol) {
       FZ_CK(cudaMalloc(&c->d_oscr, nop * sizeof(float)));
       c->oscr_len = nop;
     }
-    const size_t fsm = (size_t)c->nz * swr * sizeof(float);
+    const size_t fsm = rf_smem_full(c);
     FZ_CK((set_synth_rf_attr<true, true>(cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fsm)));
     FZ_CK((set_synth_rf_attr<false, true>(cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fsm)));
   } else {
@@ -2009,7 +2060,7 @@ int launch_rf_stage_full(fz_ctx* c, int ncol, int hydrostatic, double* d_syn, fl
   }
   FZ_CK(cudaGetLastError());
   const int threads = (c->numw + 31) & ~31;
-  const size_t sms = (size_t)c->nz * rf_w(c->nreg, c->nlu) * sizeof(float);
+  const size_t sms = rf_smem_full(c);
   {
     ProfScope ps(c, 4, s, list ? 0 : ncol);
     if (hydrostatic)
@@ -2077,7 +2128,7 @@ int launch_forward_rf(fz_ctx* c, int ncol, const float* d_model, int hydrostatic
       FZ_CK(cudaMalloc(&c->d_oscr, need * sizeof(float)));
       c->oscr_len = need;
     }
-    const size_t sms = (size_t)c->nz * swr * sizeof(float);
+    const size_t sms = rf_smem_full(c);
     FZ_CK((set_synth_rf_attr<true, true>(cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sms)));
     FZ_CK((set_synth_rf_attr<false, true>(cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sms)));
     {
