@@ -8,6 +8,7 @@
 //
 // Layouts: activations row-major [batch][features] in bf16; weights W[out][in]
 // row-major (bf16 copy for the GEMMs, FP32 master for Adam); biases FP32.
+#include <cuda.h>
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
@@ -179,7 +180,7 @@ __global__ void __launch_bounds__(256, 1) k_gemm_tc(int M, int N, int K, const _
         const size_t o = (size_t)m * ldc + n;
         if (EPI == EPI_FWD_GELU) {
           const float z = c + bias[n];
-          zout[o] = z;
+          if (zout) zout[o] = z;
           out[o] = __float2bfloat16_rn(gelu(z));
         } else if (EPI == EPI_FWD_LIN) {
           fout[o] = c + bias[n];
@@ -196,6 +197,153 @@ __global__ void __launch_bounds__(256, 1) k_gemm_tc(int M, int N, int K, const _
   fztc::fence_before_sync();
   __syncthreads();
   if (warp == 0) fztc::tmem_dealloc(tmem, 128);
+}
+
+// The forward GEMMs (mode NT, both operands K-contiguous bf16 in device
+// memory) fed by the tensor memory accelerator: a 128 x 128 output tile per
+// CTA of 256 threads, K in blocks of 64 through TM_ST shared-memory stages.
+// Warp 0's lane 0 issues the bulk tensor copies of A (128 x 64) and B
+// (128 x 64) into a stage, 128-byte swizzled, and arms the stage's "full"
+// mbarrier with their byte count; warp 1's lane 0 waits for it, issues the
+// four tcgen05.mma of the block (FP32 accumulator in 128 TMEM columns) and
+// commits them to the stage's "empty" mbarrier, which hands the stage back
+// to the copies; the last commit arrives on "done".  Then all eight warps
+// read the accumulator back (tcgen05.ld; warp w: TMEM lanes 32 (w % 4), 64
+// columns from 64 (w / 4)) and apply the epilogue, 16-byte stores where the
+// row stride allows.  Every wait is bounded (2 s): one that runs out sets
+// the error flag and the CTA frees its tensor memory.
+constexpr int TM_BM = 128, TM_BN = 128, TM_BK = 64, TM_ST = 4;
+constexpr int TM_TILE_A = TM_BM * TM_BK * 2, TM_TILE_B = TM_BN * TM_BK * 2;   // 16 KB each
+constexpr size_t TM_SMEM = (size_t)TM_ST * (TM_TILE_A + TM_TILE_B) + 1024;    // + the 1 KB alignment
+
+template <int EPI>
+__global__ void __launch_bounds__(256, 1) k_gemm_tma(const __grid_constant__ CUtensorMap ta,
+                                                     const __grid_constant__ CUtensorMap tb, int M, int N, int K,
+                                                     const float* __restrict__ bias, float* __restrict__ zout,
+                                                     float* __restrict__ fout, __nv_bfloat16* __restrict__ out,
+                                                     int ldc, int* __restrict__ err) {
+  extern __shared__ unsigned char tm_raw[];
+  __shared__ __align__(8) uint64_t full[TM_ST], empty[TM_ST], done;
+  __shared__ uint32_t tbase;
+  __shared__ int bad;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int m0 = blockIdx.y * TM_BM, n0 = blockIdx.x * TM_BN;
+  // the swizzled tiles start on a 1 KB boundary
+  const uint32_t raw = fztc::smem_addr(tm_raw);
+  const uint32_t base = (raw + 1023u) & ~1023u;
+  unsigned char* tiles = tm_raw + (base - raw);
+  if (warp == 0) {
+    fztc::tmem_alloc(&tbase, TM_BN);
+    fztc::tmem_relinquish();
+  }
+  if (tid == 0) {
+    for (int i = 0; i < TM_ST; ++i) {
+      fztc::mbar_init(&full[i], 1);
+      fztc::mbar_init(&empty[i], 1);
+    }
+    fztc::mbar_init(&done, 1);
+    bad = 0;
+    fztc::fence_mbar_init();
+  }
+  fztc::fence_before_sync();
+  __syncthreads();
+  fztc::fence_after_sync();
+  const uint32_t tmem = tbase;
+  const int nkb = (K + TM_BK - 1) / TM_BK;
+  if (warp == 0) {
+    if (lane == 0) {
+      for (int kb = 0; kb < nkb; ++kb) {
+        const int st = kb % TM_ST;
+        // the stage's previous use (block kb - TM_ST) must have been consumed
+        if (kb >= TM_ST && !fztc::mbar_wait(&empty[st], ((kb / TM_ST) - 1) & 1, TC_WAIT_NS)) {
+          atomicExch(&bad, 1);
+          break;
+        }
+        unsigned char* sa = tiles + (size_t)st * (TM_TILE_A + TM_TILE_B);
+        fztc::mbar_arrive_expect_tx(&full[st], TM_TILE_A + TM_TILE_B);
+        fztc::tma_load_2d(sa, &ta, kb * TM_BK, m0, &full[st]);
+        fztc::tma_load_2d(sa + TM_TILE_A, &tb, kb * TM_BK, n0, &full[st]);
+      }
+    }
+    __syncwarp();
+  } else if (warp == 1) {
+    if (lane == 0) {
+      const uint32_t idesc = fztc::idesc_bf16(TM_BM, TM_BN);
+      int kb = 0;
+      for (; kb < nkb; ++kb) {
+        const int st = kb % TM_ST;
+        if (!fztc::mbar_wait(&full[st], (kb / TM_ST) & 1, TC_WAIT_NS)) {
+          atomicExch(&bad, 1);
+          break;
+        }
+        fztc::fence_after_sync();
+        const uint32_t sa = base + (uint32_t)st * (TM_TILE_A + TM_TILE_B), sb = sa + TM_TILE_A;
+#pragma unroll
+        for (int ks = 0; ks < TM_BK / 16; ++ks)
+          fztc::mma_bf16(tmem, fztc::desc_sw128(sa + 32 * ks), fztc::desc_sw128(sb + 32 * ks), idesc,
+                         (kb > 0 || ks > 0) ? 1u : 0u);
+        fztc::commit(&empty[st]);
+      }
+      if (kb == nkb) fztc::commit(&done);
+    }
+    __syncwarp();
+  }
+  bool ok = fztc::mbar_wait(&done, 0, TC_WAIT_NS);
+  ok = __syncthreads_and(ok) && !*(volatile int*)&bad;
+  fztc::fence_after_sync();
+  if (ok) {
+    const int q = warp & 3, half = warp >> 2;
+    const int m = m0 + 32 * q + lane;
+    const bool vec = (ldc & 7) == 0;
+#pragma unroll 1
+    for (int cc = 0; cc < 64; cc += 16) {
+      float v[16];
+      fztc::tmem_ld16(tmem + ((uint32_t)(32 * q) << 16) + (uint32_t)(64 * half + cc), v);
+      if (m >= M) continue;
+      const int nb = n0 + 64 * half + cc;
+      const size_t o = (size_t)m * ldc + nb;
+      if (vec && nb + 16 <= N) {
+#pragma unroll
+        for (int i = 0; i < 16; ++i) v[i] += __ldg(&bias[nb + i]);
+        if (EPI == EPI_FWD_GELU) {
+          if (zout)
+#pragma unroll
+            for (int i = 0; i < 16; i += 4)
+              *reinterpret_cast<float4*>(zout + o + i) = make_float4(v[i], v[i + 1], v[i + 2], v[i + 3]);
+          uint32_t h[8];
+#pragma unroll
+          for (int i = 0; i < 8; ++i) {
+            const __nv_bfloat162 t = __floats2bfloat162_rn(gelu(v[2 * i]), gelu(v[2 * i + 1]));
+            h[i] = *reinterpret_cast<const uint32_t*>(&t);
+          }
+          *reinterpret_cast<uint4*>(out + o) = make_uint4(h[0], h[1], h[2], h[3]);
+          *reinterpret_cast<uint4*>(out + o + 8) = make_uint4(h[4], h[5], h[6], h[7]);
+        } else {
+#pragma unroll
+          for (int i = 0; i < 16; i += 4)
+            *reinterpret_cast<float4*>(fout + o + i) = make_float4(v[i], v[i + 1], v[i + 2], v[i + 3]);
+        }
+      } else {
+#pragma unroll
+        for (int i = 0; i < 16; ++i) {
+          const int n = nb + i;
+          if (n >= N) continue;
+          const float z = v[i] + bias[n];
+          if (EPI == EPI_FWD_GELU) {
+            if (zout) zout[o + i] = z;
+            out[o + i] = __float2bfloat16_rn(gelu(z));
+          } else {
+            fout[o + i] = z;
+          }
+        }
+      }
+    }
+  } else if (tid == 0) {
+    atomicExch(err, 1);
+  }
+  fztc::fence_before_sync();
+  __syncthreads();
+  if (warp == 0) fztc::tmem_dealloc(tmem, TM_BN);
 }
 
 // MSE loss 1/(n*nout) sum (y - t)^2 and dL/dy in bf16
@@ -366,9 +514,50 @@ int mlp_reserve(fz_mlp* p, int n) {
   return 0;
 }
 
+// cuTensorMapEncodeTiled through the runtime's driver entry point (no link
+// to the driver library); null when the driver does not provide it.
+using EncodeTiledFn = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                   const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                   CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+EncodeTiledFn encode_tiled() {
+  static const EncodeTiledFn fn = [] {
+    void* f = nullptr;
+    cudaDriverEntryPointQueryResult q{};
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &f, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess)
+      return EncodeTiledFn(nullptr);
+    return reinterpret_cast<EncodeTiledFn>(f);
+  }();
+  return fn;
+}
+
+// A K-contiguous bf16 operand (rows x K, row stride ld elements) as a 2-D
+// tensor map of 64 x 128 boxes with 128-byte swizzling.  False (the caller
+// then stages the operand itself) when the operand has fewer rows than a
+// box, or its base or row stride is not 16-byte aligned.
+bool tmap_kmajor(CUtensorMap* m, const __nv_bfloat16* p, int rows, int K, int ld) {
+  const EncodeTiledFn fn = encode_tiled();
+  if (!fn || rows < TM_BM || K < TM_BK || (reinterpret_cast<uintptr_t>(p) & 15) || ((size_t)ld * 2) % 16) return false;
+  const cuuint64_t dims[2] = {(cuuint64_t)K, (cuuint64_t)rows};
+  const cuuint64_t strides[1] = {(cuuint64_t)ld * 2};
+  const cuuint32_t box[2] = {(cuuint32_t)TM_BK, (cuuint32_t)TM_BM};
+  const cuuint32_t es[2] = {1, 1};
+  return fn(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<__nv_bfloat16*>(p), dims, strides, box, es,
+            CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
 template <int MODE, int EPI>
 void gemm(cudaStream_t s, int* err, int M, int N, int K, const __nv_bfloat16* A, int lda, const __nv_bfloat16* B,
           int ldb, const float* bias, const float* zin, float* zout, float* fout, __nv_bfloat16* out, int ldc) {
+  if constexpr (MODE == NT && (EPI == EPI_FWD_GELU || EPI == EPI_FWD_LIN)) {
+    CUtensorMap ma, mb;
+    if (tmap_kmajor(&ma, A, M, K, lda) && tmap_kmajor(&mb, B, N, K, ldb)) {
+      const dim3 grid((N + TM_BN - 1) / TM_BN, (M + TM_BM - 1) / TM_BM);
+      k_gemm_tma<EPI><<<grid, 256, TM_SMEM, s>>>(ma, mb, M, N, K, bias, zout, fout, out, ldc, err);
+      return;
+    }
+  }
   const dim3 grid((N + 127) / 128, (M + 127) / 128);
   k_gemm_tc<MODE, EPI><<<grid, 256, TC_SMEM, s>>>(M, N, K, A, lda, B, ldb, bias, zin, zout, fout, out, ldc, err);
 }
@@ -384,6 +573,10 @@ int gemm_tc_attrs() {
     e = cudaFuncSetAttribute(k_gemm_tc<TN, EPI_F32>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TC_SMEM);
   if (e == cudaSuccess)
     e = cudaFuncSetAttribute(k_gemm_tc<NN, EPI_BWD_GELU>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TC_SMEM);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(k_gemm_tma<EPI_FWD_GELU>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TM_SMEM);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(k_gemm_tma<EPI_FWD_LIN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TM_SMEM);
   if (e != cudaSuccess) {
     std::fprintf(stderr, "fz_b200 mlp: CUDA error %s\n", cudaGetErrorString(e));
     return FZ_ERR_CUDA;
@@ -391,13 +584,14 @@ int gemm_tc_attrs() {
   return 0;
 }
 
-// forward of n rows already in act[0]; output in yout
-void mlp_fwd(fz_mlp* p, int n) {
+// forward of n rows already in act[0]; output in yout; the pre-activations
+// are kept for a backward pass only when keep_z
+void mlp_fwd(fz_mlp* p, int n, bool keep_z = true) {
   for (int l = 0; l < p->nl; ++l) {
     const int in = p->dim[l], out = p->dim[l + 1];
     if (l + 1 < p->nl)
-      gemm<NT, EPI_FWD_GELU>(p->stream, p->d_err, n, out, in, p->act[l], in, p->Wb[l], in, p->b[l], nullptr, p->z[l], nullptr,
-                             p->act[l + 1], out);
+      gemm<NT, EPI_FWD_GELU>(p->stream, p->d_err, n, out, in, p->act[l], in, p->Wb[l], in, p->b[l], nullptr,
+                             keep_z ? p->z[l] : nullptr, nullptr, p->act[l + 1], out);
     else
       gemm<NT, EPI_FWD_LIN>(p->stream, p->d_err, n, out, in, p->act[l], in, p->Wb[l], in, p->b[l], nullptr, nullptr, p->yout,
                             nullptr, out);
@@ -564,7 +758,7 @@ int fz_mlp_forward_device(fz_mlp* p, int n, const float* d_x, float* d_y, void* 
   for (int i = 0; i < n; i += chunk) {
     const int m = std::min(chunk, n - i);
     k_to_bf16<<<grid1((size_t)m * d0), 256, 0, s>>>((size_t)m * d0, d_x + (size_t)i * d0, p->act[0]);
-    mlp_fwd(p, m);
+    mlp_fwd(p, m, false);
     cudaMemcpyAsync(d_y + (size_t)i * dl, p->yout, (size_t)m * dl * sizeof(float), cudaMemcpyDeviceToDevice, s);
   }
   cudaEventRecord(ev, s);
@@ -598,7 +792,7 @@ int fz_mlp_forward_obs_device(fz_mlp* p, int n, const double* d_obs, const float
     const int m = std::min(chunk, n - i);
     k_obs_bf16<<<grid1((size_t)m * d0), 256, 0, s>>>((size_t)m * d0, d0, d_obs + (size_t)i * d0, d_mu, d_sd,
                                                       p->act[0]);
-    mlp_fwd(p, m);
+    mlp_fwd(p, m, false);
     cudaMemcpyAsync(d_y + (size_t)i * dl, p->yout, (size_t)m * dl * sizeof(float), cudaMemcpyDeviceToDevice, s);
   }
   cudaEventRecord(ev, s);

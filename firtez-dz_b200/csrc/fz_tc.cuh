@@ -30,6 +30,16 @@ __host__ __device__ __forceinline__ uint64_t desc_kmajor(uint32_t saddr, uint32_
          ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) | ((uint64_t)1 << 46);
 }
 
+// The same for a K-major tile written by a bulk tensor copy with 128-byte
+// swizzling: rows of 64 bf16 (128 B), the 16-byte chunks of row r stored at
+// chunk index ^ (r % 8), 8-row groups 1 KB apart (SBO), LBO unused; layout
+// type SWIZZLE_128B (2) at bits 61-63.  The tile starts on a 1 KB boundary
+// and the MMA's 16-wide K step advances the start address by 32 B.
+__host__ __device__ __forceinline__ uint64_t desc_sw128(uint32_t saddr) {
+  return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)(1024u >> 4) << 32) | ((uint64_t)1 << 46) |
+         ((uint64_t)2 << 61);
+}
+
 // Instruction descriptor of kind::f16: D FP32 (bit 4), A and B bf16 (bits
 // 7-9, 10-12 = 1), both K-major, N >> 3 at bit 17, M >> 4 at bit 24.
 __host__ __device__ constexpr uint32_t idesc_bf16(int M, int N) {
@@ -80,6 +90,23 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* mbar, uint32_t parity, uint6
     if (done) return true;
     if (globaltimer() - t0 > limit_ns) return false;
   }
+}
+
+// Arrive on the mbarrier and add tx bytes to the phase's expected count.
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* mbar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(mbar)), "r"(bytes)
+               : "memory");
+}
+
+// One box of a 2-D tiled tensor map (x = innermost coordinate, in elements)
+// into shared memory, completing tx bytes on the mbarrier.  Loads only from
+// this GPU's memory; no multicast.
+__device__ __forceinline__ void tma_load_2d(void* dst, const void* tmap, int x, int y, uint64_t* mbar) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::"r"(
+          smem_addr(dst)),
+      "l"(tmap), "r"(x), "r"(y), "r"(smem_addr(mbar))
+      : "memory");
 }
 
 // Generic-proxy shared-memory writes made visible to the tensor core.

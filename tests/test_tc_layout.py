@@ -39,6 +39,7 @@ def probe(tmp_path_factory):
 int main() {
   for (int n = 16; n <= 128; n += 16) std::printf("I %d %u\n", n, fztc::idesc_bf16(128, n));
   std::printf("S %llu\n", (unsigned long long)fztc::desc_kmajor(0x1230u, 128u, 1024u));
+  std::printf("W %llu\n", (unsigned long long)fztc::desc_sw128(0x4c00u + 32u));
   for (int r = 0; r < 128; ++r)
     for (int k = 0; k < 64; k += 4) std::printf("O %d %d %u\n", r, k, fztc::kmajor_offset(r, k, 8));
   return 0;
@@ -76,6 +77,19 @@ def test_shared_memory_descriptor(probe):
     assert field(v, 46, 2) == 1                              # Blackwell descriptor version
     assert field(v, 49, 3) == 0 and field(v, 52, 1) == 0    # base offset, LBO mode
     assert field(v, 61, 3) == 0                              # SWIZZLE_NONE
+
+
+def test_swizzled_shared_memory_descriptor(probe):
+    """The descriptor of the TMA-fed GEMM's tiles: K-major, 128-byte
+    swizzle (layout type 2), 8-row groups 1 KB apart, LBO unused, the start
+    address of a 1 KB-aligned tile advanced by 32 B for the second K step."""
+    v = int([ln for ln in probe if ln.startswith("W ")][0].split()[1])
+    assert field(v, 0, 14) == (0x4c00 + 32) >> 4
+    assert field(v, 16, 14) == 0
+    assert field(v, 32, 14) == 1024 >> 4
+    assert field(v, 46, 2) == 1
+    assert field(v, 49, 3) == 0 and field(v, 52, 1) == 0
+    assert field(v, 61, 3) == 2                              # SWIZZLE_128B
 
 
 def test_operand_offsets_match_the_descriptor_addressing(probe):
