@@ -201,7 +201,8 @@ __global__ void __launch_bounds__(256, 1) k_gemm_tc(int M, int N, int K, const _
 
 // The forward GEMMs (mode NT, both operands K-contiguous bf16 in device
 // memory) fed by the tensor memory accelerator: a 128 x 128 output tile per
-// CTA of 256 threads, K in blocks of 64 through TM_ST shared-memory stages.
+// CTA of 256 threads, two CTAs per SM, K in blocks of 64 through three
+// shared-memory stages.
 // Warp 0's lane 0 issues the bulk tensor copies of A (128 x 64) and B
 // (128 x 64) into a stage, 128-byte swizzled, and arms the stage's "full"
 // mbarrier with their byte count; warp 1's lane 0 waits for it, issues the
@@ -212,12 +213,12 @@ __global__ void __launch_bounds__(256, 1) k_gemm_tc(int M, int N, int K, const _
 // columns from 64 (w / 4)) and apply the epilogue, 16-byte stores where the
 // row stride allows.  Every wait is bounded (2 s): one that runs out sets
 // the error flag and the CTA frees its tensor memory.
-constexpr int TM_BM = 128, TM_BN = 128, TM_BK = 64, TM_ST = 4;
+constexpr int TM_BM = 128, TM_BN = 128, TM_BK = 64, TM_ST = 3;
 constexpr int TM_TILE_A = TM_BM * TM_BK * 2, TM_TILE_B = TM_BN * TM_BK * 2;   // 16 KB each
 constexpr size_t TM_SMEM = (size_t)TM_ST * (TM_TILE_A + TM_TILE_B) + 1024;    // + the 1 KB alignment
 
 template <int EPI>
-__global__ void __launch_bounds__(256, 1) k_gemm_tma(const __grid_constant__ CUtensorMap ta,
+__global__ void __launch_bounds__(256, 2) k_gemm_tma(const __grid_constant__ CUtensorMap ta,
                                                      const __grid_constant__ CUtensorMap tb, int M, int N, int K,
                                                      const float* __restrict__ bias, float* __restrict__ zout,
                                                      float* __restrict__ fout, __nv_bfloat16* __restrict__ out,
@@ -577,6 +578,11 @@ int gemm_tc_attrs() {
     e = cudaFuncSetAttribute(k_gemm_tma<EPI_FWD_GELU>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TM_SMEM);
   if (e == cudaSuccess)
     e = cudaFuncSetAttribute(k_gemm_tma<EPI_FWD_LIN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TM_SMEM);
+  // two CTAs per SM (97 KB each): one CTA's epilogue overlaps the other's MMAs
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(k_gemm_tma<EPI_FWD_GELU>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(k_gemm_tma<EPI_FWD_LIN>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
   if (e != cudaSuccess) {
     std::fprintf(stderr, "fz_b200 mlp: CUDA error %s\n", cudaGetErrorString(e));
     return FZ_ERR_CUDA;
