@@ -94,14 +94,20 @@ __device__ __forceinline__ void copy_to_shared(T* dst, const T* src) {
 template <bool HE, int L>
 __global__ void __launch_bounds__(128, 4) k_chain(const Consts* __restrict__ Kg, const PFTable* __restrict__ tb, int ncol,
                                                int nz, const float* model, float* mout, double2* __restrict__ chem,
-                                               int* __restrict__ status) {
+                                               int* __restrict__ status, const int* __restrict__ list = nullptr,
+                                               const int* __restrict__ nlist = nullptr) {
   constexpr int NS = WarpSahaT<L>::NS;
+  // listed columns (list[0, *nlist) of the ncol slots): a CTA past the end
+  // of the list leaves before any work
+  const int count = list ? *nlist : ncol;
+  if ((int)((blockIdx.x * (size_t)blockDim.x) / L) >= count) return;
   __shared__ Consts K;
   copy_to_shared(&K, Kg);
   __syncthreads();
   const int lane = threadIdx.x & (L - 1);
-  const int col = (int)((blockIdx.x * (size_t)blockDim.x + threadIdx.x) / L);
-  if (col >= ncol) return;
+  const int g = (int)((blockIdx.x * (size_t)blockDim.x + threadIdx.x) / L);
+  if (g >= count) return;
+  const int col = list ? list[g] : g;
   const float* m = model + (size_t)col * 13 * nz;
   float* mo = mout + (size_t)col * 13 * nz;
   double2* ch = chem + (size_t)col * nz;
@@ -291,16 +297,21 @@ __global__ void __launch_bounds__(128) k_chain_med(const Consts* __restrict__ Kg
 // (src/absorption_matrix.f90:914-991, :1018).
 __global__ void __launch_bounds__(256) k_opac(const DevParams* __restrict__ Pg, const Consts* __restrict__ Kg,
                                               int ncol, const float* __restrict__ mout,
-                                              const double2* __restrict__ chem, float* __restrict__ slab) {
+                                              const double2* __restrict__ chem, float* __restrict__ slab,
+                                              const int* __restrict__ list = nullptr,
+                                              const int* __restrict__ nlist = nullptr) {
   __shared__ DevParams P;
   __shared__ Consts K;
+  const size_t total = (size_t)(list ? *nlist : ncol) * Pg->nz;
+  if ((size_t)blockIdx.x * blockDim.x >= total) return;
   copy_to_shared(&P, Pg);
   copy_to_shared(&K, Kg);
   __syncthreads();
   const int nz = P.nz, sw = P.sw;
-  const size_t total = (size_t)ncol * nz;
-  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (size_t)gridDim.x * blockDim.x) {
-    const int col = (int)(i / nz), k = (int)(i % nz);
+  for (size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x; t < total; t += (size_t)gridDim.x * blockDim.x) {
+    const int idx = (int)(t / nz), k = (int)(t % nz);
+    const int col = list ? list[idx] : idx;
+    const size_t i = (size_t)col * nz + k;
     const float* m = mout + (size_t)col * 13 * nz;
     const double2 c = chem[i];
     const double nhyd = c.x, nelec = c.y;
@@ -369,23 +380,12 @@ __device__ __forceinline__ void rte_step(const float O[16], float om0, float S, 
   I3 = n3;
 }
 
-__global__ void __launch_bounds__(MAXNUMW) k_synth(const DevParams* __restrict__ Pg, const LamP* __restrict__ lam,
-                                                   const float* __restrict__ gain, int ncol,
-                                                   const float* __restrict__ slab, double* __restrict__ syn,
-                                                   float* mout, int* __restrict__ status) {
-  extern __shared__ float4 sm_synth4[];
-  float* sm = reinterpret_cast<float*>(sm_synth4);
-  __shared__ DevParams P;
-  copy_to_shared(&P, Pg);
-  const int col = blockIdx.x;
-  const int nz = Pg->nz, sw = Pg->sw;
-  // stage the column's slab (nz*sw floats, 16-byte rows) in shared memory
-  {
-    const float4* src = reinterpret_cast<const float4*>(slab + (size_t)col * nz * sw);
-    const int n4 = nz * sw / 4;
-    for (int i = threadIdx.x; i < n4; i += blockDim.x) sm_synth4[i] = __ldg(src + i);
-  }
-  __syncthreads();
+// The synthesis of column col from its slab staged in shared memory (sm),
+// one thread per wavelength l.
+__device__ __forceinline__ void synth_column(const DevParams& P, const LamP* __restrict__ lam,
+                                             const float* __restrict__ gain, const float* sm, int col,
+                                             double* __restrict__ syn, float* mout, int* __restrict__ status) {
+  const int nz = P.nz, sw = P.sw;
   const int l = threadIdx.x;
   if (l >= P.numw) return;
   if (l == 0) {
@@ -474,6 +474,33 @@ __global__ void __launch_bounds__(MAXNUMW) k_synth(const DevParams* __restrict__
   o[3 * nw + l] = (double)I3 * (double)gain[4 * l + 3];
   if (!(isfinite(I0) && isfinite(I1) && isfinite(I2) && isfinite(I3))) bad = 1;
   if (status && __any_sync(__activemask(), bad) && (l & 31) == 0) atomicOr(&status[col], FZ_NAN);
+}
+
+// One CTA per column, one thread per wavelength, FP32: the Stokes synthesis
+// of the column's slab.  With a list, the CTAs walk list[0, *nlist) (the
+// occupied slots of an inversion pool) with a grid stride.
+__global__ void __launch_bounds__(MAXNUMW) k_synth(const DevParams* __restrict__ Pg, const LamP* __restrict__ lam,
+                                                   const float* __restrict__ gain, int ncol,
+                                                   const float* __restrict__ slab, double* __restrict__ syn,
+                                                   float* mout, int* __restrict__ status,
+                                                   const int* __restrict__ list = nullptr,
+                                                   const int* __restrict__ nlist = nullptr) {
+  extern __shared__ float4 sm_synth4[];
+  __shared__ DevParams P;
+  const int count = list ? *nlist : ncol;
+  if ((int)blockIdx.x >= count) return;
+  copy_to_shared(&P, Pg);
+  const int nz = Pg->nz, sw = Pg->sw;
+  for (int idx = blockIdx.x; idx < count; idx += gridDim.x) {
+    const int col = list ? list[idx] : idx;
+    __syncthreads();   // P in place; the previous column's slab no longer read
+    // stage the column's slab (nz*sw floats, 16-byte rows) in shared memory
+    const float4* src = reinterpret_cast<const float4*>(slab + (size_t)col * nz * sw);
+    const int n4 = nz * sw / 4;
+    for (int i = threadIdx.x; i < n4; i += blockDim.x) sm_synth4[i] = __ldg(src + i);
+    __syncthreads();
+    synth_column(P, lam, gain, reinterpret_cast<const float*>(sm_synth4), col, syn, mout, status);
+  }
 }
 
 // ------------------------------------------------------ response functions
@@ -1729,6 +1756,7 @@ struct fz_ctx {
   // LM slot pool (grown on demand)
   LMSlots lm{}, lm2{};   // two pools: the tail of an inversion is compacted into the other one
   int* d_dest = nullptr;
+  int* d_act = nullptr;   // the occupied slots of the pool, in order (device-driven loop)
   size_t lm_cap = 0;
   int lm_np = 0;
   LMQueue* d_q = nullptr;
@@ -1828,7 +1856,8 @@ struct ProfScope {
 // (latency: every column's chain gets a warp of its own).  chem: the (nH, ne)
 // scratch of the batch, the context's own buffer when null.
 void launch_k_chain(fz_ctx* c, int ncol, const float* d_model, float* d_mout, int* d_status, int hydrostatic, int wpb,
-                    int lanes, cudaStream_t s, double2* chem = nullptr) {
+                    int lanes, cudaStream_t s, double2* chem = nullptr, const int* list = nullptr,
+                    const int* nlist = nullptr) {
   if (!chem) chem = c->d_chem;
   if (hydrostatic == 2) {   // HE anchored at log tau5 ~ 0 (HYDRO_TOP off)
     const dim3 g((unsigned)(((size_t)ncol * 32 + 127) / 128));
@@ -1841,17 +1870,17 @@ void launch_k_chain(fz_ctx* c, int ncol, const float* d_model, float* d_mout, in
   if (lanes == 16) {
     if (hydrostatic)
       k_chain<true, 16><<<gc, wpb * 32, 0, s>>>(c->d_consts, c->d_pf, ncol, c->nz, d_model, d_mout, chem,
-                                                d_status);
+                                                d_status, list, nlist);
     else
       k_chain<false, 16><<<gc, wpb * 32, 0, s>>>(c->d_consts, c->d_pf, ncol, c->nz, d_model, d_mout, chem,
-                                                 d_status);
+                                                 d_status, list, nlist);
   } else {
     if (hydrostatic)
       k_chain<true, 32><<<gc, wpb * 32, 0, s>>>(c->d_consts, c->d_pf, ncol, c->nz, d_model, d_mout, chem,
-                                                d_status);
+                                                d_status, list, nlist);
     else
       k_chain<false, 32><<<gc, wpb * 32, 0, s>>>(c->d_consts, c->d_pf, ncol, c->nz, d_model, d_mout, chem,
-                                                 d_status);
+                                                 d_status, list, nlist);
   }
 }
 
@@ -1878,31 +1907,38 @@ int launch_lsf(fz_ctx* c, T* d_data, long long nrows, int rows_per_col, cudaStre
   return cuda_fail(cudaGetLastError());
 }
 
+// The synthesis of ncol columns, or with a list of the columns list[0,
+// *nlist) among ncol slots (an inversion pool's occupied slots; the count
+// read on the device, so that a captured graph replays for any count).
 int launch_forward(fz_ctx* c, int ncol, const float* d_model, int hydrostatic, double* d_syn, float* d_mout,
-                   int* d_status, cudaStream_t s) {
+                   int* d_status, cudaStream_t s, const int* list = nullptr, const int* nlist = nullptr) {
   int rc = ensure_scratch(c, ncol);
   if (rc) return rc;
   if (d_status) FZ_CK(cudaMemsetAsync(d_status, 0, ncol * sizeof(int), s));
   {
     ProfScope ps(c, 0, s, ncol);
-    launch_k_chain(c, ncol, d_model, d_mout, d_status, hydrostatic, c->tune.chain_warps, c->tune.chain_lanes, s);
+    launch_k_chain(c, ncol, d_model, d_mout, d_status, hydrostatic, c->tune.chain_warps, c->tune.chain_lanes, s,
+                   nullptr, list, nlist);
   }
   FZ_CK(cudaGetLastError());
   {
     ProfScope ps(c, 1, s, ncol);
     const size_t total = (size_t)ncol * c->nz;
     const int blocks = (int)std::min<size_t>((total + 255) / 256, (size_t)c->nsm * 16);
-    k_opac<<<blocks, 256, 0, s>>>(c->d_params, c->d_consts, ncol, d_mout, c->d_chem, c->d_slab);
+    k_opac<<<blocks, 256, 0, s>>>(c->d_params, c->d_consts, ncol, d_mout, c->d_chem, c->d_slab, list, nlist);
   }
   FZ_CK(cudaGetLastError());
   const int threads = (c->numw + 31) & ~31;
   const size_t sms = (size_t)c->nz * c->sw * sizeof(float);
   {
     ProfScope ps(c, 2, s, ncol);
-    k_synth<<<ncol, threads, sms, s>>>(c->d_params, c->d_lam, c->d_gain, ncol, c->d_slab, d_syn, d_mout, d_status);
+    // listed: a grid of 32 CTAs per SM walks the list
+    const int grid = list ? std::min(ncol, c->nsm * 32) : ncol;
+    k_synth<<<grid, threads, sms, s>>>(c->d_params, c->d_lam, c->d_gain, ncol, c->d_slab, d_syn, d_mout, d_status,
+                                       list, nlist);
   }
   FZ_CK(cudaGetLastError());
-  return launch_lsf<double>(c, d_syn, (long long)ncol * 4, 4, s);
+  return launch_lsf<double>(c, d_syn, (long long)ncol * 4, 4, s, list, nlist);
 }
 
 size_t rf_smem(const fz_ctx* c) {
@@ -2184,6 +2220,8 @@ void lm_free(fz_ctx* c) {
   lm_free_pool(c->lm2);
   cudaFree(c->d_dest);
   c->d_dest = nullptr;
+  cudaFree(c->d_act);
+  c->d_act = nullptr;
   c->lm_cap = 0;
 }
 
@@ -2220,6 +2258,7 @@ int lm_alloc(fz_ctx* c, int S) {
   int rc = lm_alloc_pool(c->lm, S, np, nf, nm);
   if (!rc) rc = lm_alloc_pool(c->lm2, S, np, nf, nm);
   if (!rc) rc = cuda_fail(cudaMalloc(&c->d_dest, S * sizeof(int)));
+  if (!rc) rc = cuda_fail(cudaMalloc(&c->d_act, S * sizeof(int)));
   if (rc) {
     lm_free(c);
     return rc;
@@ -3859,6 +3898,77 @@ int fz_invert_device(fz_ctx* c, int npix, const double* d_obs, const float* d_in
     }
     ~Graph() { reset(); }
   } graph;
+  // The device-driven loop (no per-kernel profiling, node layouts of the
+  // warp kernels, no LSF): one CUDA graph whose WHILE node repeats an
+  // iteration over the occupied slots of the whole pool until k_lm_ctl --
+  // the last node of the body -- finds the queue done, the iteration cap
+  // reached or the field-wide stop met.  The synthesis kernels walk the list
+  // of occupied slots the previous iteration's scan wrote (a finished pixel's
+  // slot takes the next pixel at once; once the queue is drained the list
+  // shrinks instead of the pool being compacted), the response functions
+  // the list of accepted slots; the host launches the graph once and reads
+  // the queue state once.
+  if (!c->prof && !big && !c->lsf.on) {
+    if ((rc = ensure_scratch(c, S))) return rc;
+    const int gthr = C.global_stop ? std::max(1, C.maxsteps - opts->cycles_left) : 0;
+    k_lm_scan<<<1, 1024, 0, s>>>(S, L.pix, c->d_dest, c->d_q, c->d_act);   // the filled slots
+    FZ_CK(cudaGetLastError());
+    struct Loop {
+      cudaGraph_t g = nullptr;
+      cudaGraphExec_t e = nullptr;
+      ~Loop() {
+        if (e) cudaGraphExecDestroy(e);
+        if (g) cudaGraphDestroy(g);
+      }
+    } loop;
+    FZ_CK(cudaGraphCreate(&loop.g, 0));
+    cudaGraphConditionalHandle h = 0;
+    FZ_CK(cudaGraphConditionalHandleCreate(&h, loop.g, 1, cudaGraphCondAssignDefault));
+    cudaGraphNodeParams cp{};
+    cp.type = cudaGraphNodeTypeConditional;
+    cp.conditional.handle = h;
+    cp.conditional.type = cudaGraphCondTypeWhile;
+    cp.conditional.size = 1;
+    cudaGraphNode_t node = nullptr;
+    FZ_CK(cudaGraphAddNode(&node, loop.g, nullptr, 0, &cp));
+    cudaGraph_t body = cp.conditional.phGraph_out[0];
+    FZ_CK(cudaStreamBeginCaptureToGraph(s, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+    int r = launch_forward(c, S, L.mcur, hydrostatic, L.syn, L.mcur, L.status, s, c->d_act, &c->d_q->active);
+    if (!r) {
+      k_lm_accept<<<S, 256, C.reg ? 2 * C.np * sizeof(double) : 0, s>>>(C, L, c->d_q, d_w, d_obs, d_init,
+                                                                       d_target_chi2, d_model_out, d_chi2, d_iters,
+                                                                       d_syn_out, d_status, c->d_coef64);
+      k_lm_rflist<<<1, 1024, 0, s>>>(S, L.need_rf, L.rf_list, c->d_q);
+      r = launch_rf_stage(c, S, hydrostatic, L.syn, L.jacb, L.mcur, L.status, s, L.rf_list, &c->d_q->rf_count);
+    }
+    if (!r) {
+      k_lm_normal<<<(S + 3) / 4, 128, 0, s>>>(C, L, d_w);
+      k_lm_solve<<<(S + 3) / 4, 128, 0, s>>>(C, L);
+      k_lm_update<<<S, 128, usm, s>>>(C, L, c->d_coef64);
+      k_lm_scan<<<1, 1024, 0, s>>>(S, L.pix, c->d_dest, c->d_q, c->d_act);
+      k_lm_ctl<<<1, 1, 0, s>>>(c->d_q, h, npix, cap, gthr);
+    }
+    cudaGraph_t captured = nullptr;
+    const cudaError_t ce = cudaStreamEndCapture(s, &captured);
+    if (r) return r;
+    FZ_CK(ce);
+    FZ_CK(cudaGraphInstantiate(&loop.e, loop.g, 0));
+    FZ_CK(cudaGraphLaunch(loop.e, s));
+    FZ_CK(cudaMemcpyAsync(c->h_q, c->d_q, sizeof(LMQueue), cudaMemcpyDeviceToHost, s));
+    FZ_CK(cudaStreamSynchronize(s));
+    hq = *c->h_q;
+    if (hq.tc_err) {
+      std::fprintf(stderr, "fz_b200: the tensor-core normal equations gave up waiting for their MMAs\n");
+      return FZ_ERR_CUDA;
+    }
+    if (hq.gstop) {
+      k_lm_finish_all<<<S, 256, 0, s>>>(C, L, c->d_q, d_model_out, d_chi2, d_iters, d_syn_out, d_status);
+      FZ_CK(cudaGetLastError());
+      FZ_CK(cudaStreamSynchronize(s));
+      return 0;
+    }
+    return hq.done >= npix ? 0 : FZ_ERR_STATE;
+  }
   int graph_n = -1;
   const float* graph_pool = nullptr;
   for (long long it = 0; it < cap; ++it) {

@@ -95,6 +95,8 @@ struct LMQueue {
   int rf_count;      // slots in the RF pass of this iteration (k_lm_rflist)
   unsigned long long steps_sum;   // sum over the call's pixels of STEPS (global stop rule; two's complement)
   int tc_err;        // a tensor-core kernel gave up waiting (bounded mbarrier waits)
+  int iters;         // iterations of the device-driven loop (k_lm_ctl)
+  int gstop;         // the device-driven loop ended on the field-wide stop rule
   int pad;
 };
 
@@ -849,7 +851,7 @@ __global__ void __launch_bounds__(256) k_lm_finish_all(LMConf C, LMSlots Sl, LMQ
 // One block of 1024 threads: destination of every occupied slot when the
 // pool is compacted (exclusive scan of the occupancy flags), and their count.
 __global__ void __launch_bounds__(1024) k_lm_scan(int S, const int* __restrict__ pix, int* __restrict__ dest,
-                                                  LMQueue* q) {
+                                                  LMQueue* q, int* __restrict__ list = nullptr) {
   __shared__ int part[1024];
   const int per = (S + blockDim.x - 1) / blockDim.x;
   const int b = threadIdx.x * per, e = min(S, b + per);
@@ -864,8 +866,32 @@ __global__ void __launch_bounds__(1024) k_lm_scan(int S, const int* __restrict__
     __syncthreads();
   }
   int d = part[threadIdx.x] - n;
-  for (int i = b; i < e; ++i) dest[i] = pix[i] >= 0 ? d++ : -1;
+  for (int i = b; i < e; ++i) {
+    const bool occ = pix[i] >= 0;
+    if (occ && list) list[d] = i;   // the occupied slots in order
+    dest[i] = occ ? d++ : -1;
+  }
   if (threadIdx.x == blockDim.x - 1) q->active = part[threadIdx.x];
+}
+
+// The condition of the device-driven inversion loop (a CUDA graph WHILE
+// node around one iteration): another iteration while pixels are left, no
+// tensor-core kernel gave up and fewer than cap iterations ran; with gthr >
+// 0, MAKE_DECISION's field-wide stop (mean STEPS >= gthr,
+// src/invert3d.f90:843-846) ends the loop with gstop set, and the host then
+// finishes every pixel in flight.
+__global__ void k_lm_ctl(LMQueue* q, cudaGraphConditionalHandle h, int npix, long long cap, int gthr) {
+  const int it = ++q->iters;
+  unsigned go;
+  if (q->done >= npix || q->tc_err) {
+    go = 0u;
+  } else if (gthr > 0 && (double)(long long)q->steps_sum >= (double)gthr * (double)npix) {
+    q->gstop = 1;
+    go = 0u;
+  } else {
+    go = it < cap ? 1u : 0u;
+  }
+  cudaGraphSetConditional(h, go);
 }
 
 // One block of 1024 threads: the slots of the RF pass (need_rf) compacted

@@ -136,6 +136,7 @@ struct WarpSahaT {
   static constexpr int NS = 96 / L;
   double T;
   double a1[NS], a2[NS];
+  unsigned hyd;   // bit j: the lane's slot j holds hydrogen
 };
 using WarpSaha = WarpSahaT<32>;
 
@@ -153,6 +154,7 @@ __device__ __forceinline__ void saha_prepare(WarpSahaT<L>& w, double T, const Co
   constexpr int NS = WarpSahaT<L>::NS;
   constexpr int NEXP = 23 / L + 1;   // slots holding the 23 exponential-form elements
   w.T = T;
+  w.hyd = 0u;
   const double it = rcp_d(T);
   const double lamelec = K.csaha1 * (it * sqrt(it));   // T^(-3/2)
   const double var[3] = {T, 1.0e-3 * T, log(5040.0 / T)};
@@ -172,6 +174,7 @@ __device__ __forceinline__ void saha_prepare(WarpSahaT<L>& w, double T, const Co
     }
     const double e1 = exp(clamp650(K.csaha2 * fz_tab_xi[e] * it));
     const double e2 = exp(clamp650(K.csaha2 * fz_tab_xii[e] * it));
+    if (el == 0) w.hyd |= 1u << j;
     w.a1[j] = el >= 0 ? (u0 * (0.5 * rcp_d(u1))) * lamelec * e1 : 0.0;
     w.a2[j] = el >= 0 ? (u1 * (0.5 * rcp_d(u2))) * lamelec * e2 : 0.0;
   }
@@ -236,7 +239,7 @@ __device__ __forceinline__ RhoOut get_rho_warp(const WarpSahaT<L>& w, const doub
     for (int j = 0; j < NS; ++j) {
       const double x = ne * w.a1[j], y = ne * w.a2[j];
       const double xy = x * y;
-      const double num = (K.lane_elem[L * j + lane] == 0) ? (1.0 - xy) : (1.0 + y);   // hydrogen: N_H+ - N_H-
+      const double num = ((w.hyd >> j) & 1u) ? (1.0 - xy) : (1.0 + y);   // hydrogen: N_H+ - N_H-
       s = fma(ab[j] * num, rcp_d(1.0 + y + xy), s);
     }
     s = group_sum<L>(s, mask);
