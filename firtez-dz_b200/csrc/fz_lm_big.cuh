@@ -36,23 +36,41 @@ constexpr unsigned long long GT_WAIT_NS = 2000000000ull;   // 2 s per wait on th
 
 // Stage rows [row0, row0 + 128) x K block [k0, k0 + 64) of the slot's
 // Jacobian J (np, nf) into the hi / lo bf16 tiles, normalised as
-// NORMALIZE_JACOB does (sqrt(w / INU) per frequency, PARAM_NORM per node);
-// rows >= np and frequencies >= nf are zero.
-__device__ __forceinline__ void gram_stage(const LMConf& C, const float* __restrict__ J,
-                                           const double* __restrict__ w, int row0, int k0, float rin,
-                                           unsigned char* hi, unsigned char* lo) {
+// NORMALIZE_JACOB does (wk = sqrt(w / INU) of the block's frequencies, from
+// shared memory, and PARAM_NORM per node); rows >= np and frequencies >= nf
+// are zero.
+__device__ __forceinline__ void gram_stage(const LMConf& C, const float* __restrict__ J, const float* wk, int row0,
+                                           int k0, unsigned char* hi, unsigned char* lo) {
+  // blocks of 128 threads: 16 float4 of the tile a thread, all loads issued
+  // before any is used
+  constexpr int PER = GT_M * (GT_BK / 4) / 128;
   const int np = C.np, nf = C.nfreq;
-  for (int i = threadIdx.x; i < GT_M * (GT_BK / 4); i += blockDim.x) {
-    const int r = i / (GT_BK / 4), kq = i % (GT_BK / 4);
-    const int gr = row0 + r, k = k0 + 4 * kq;
-    float v[4] = {0.f, 0.f, 0.f, 0.f};
-    if (gr < np) {
-      const float nrm = (float)lm_nrm(C, gr);
-      const float* src = J + (size_t)gr * nf;
+  float4 x[PER];
 #pragma unroll
-      for (int e = 0; e < 4; ++e)
-        if (k + e < nf) v[e] = src[k + e] * (sqrtf((float)w[k + e]) * rin) * nrm;
+  for (int u = 0; u < PER; ++u) {
+    const int i = threadIdx.x + 128 * u;
+    const int gr = row0 + (i >> 4), k = k0 + 4 * (i & 15);
+    x[u] = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (gr < np) {
+      const float* src = J + (size_t)gr * nf + k;
+      if (k + 4 <= nf) {
+        x[u] = __ldg(reinterpret_cast<const float4*>(src));
+      } else {
+        float t[4] = {0.f, 0.f, 0.f, 0.f};
+        for (int e = 0; e < 4; ++e)
+          if (k + e < nf) t[e] = src[e];
+        x[u] = make_float4(t[0], t[1], t[2], t[3]);
+      }
     }
+  }
+#pragma unroll
+  for (int u = 0; u < PER; ++u) {
+    const int i = threadIdx.x + 128 * u;
+    const int r = i >> 4, kq = i & 15;
+    const int gr = row0 + r;
+    const float nrm = gr < np ? (float)lm_nrm(C, gr) : 0.f;
+    const float v[4] = {x[u].x * wk[4 * kq] * nrm, x[u].y * wk[4 * kq + 1] * nrm, x[u].z * wk[4 * kq + 2] * nrm,
+                        x[u].w * wk[4 * kq + 3] * nrm};
     unsigned short h[4], l[4];
 #pragma unroll
     for (int e = 0; e < 4; ++e) bf16_split(v[e], h[e], l[e]);
@@ -71,6 +89,7 @@ __global__ void __launch_bounds__(128, 1) k_lm_gram_tc(LMConf C, LMSlots Sl, con
   extern __shared__ __align__(1024) unsigned char gsm[];
   __shared__ __align__(8) uint64_t mbar[2];
   __shared__ uint32_t tbase;
+  __shared__ float wk[2][GT_BK];   // sqrt(w / INU) of the K block's frequencies, per buffer
   const int s = blockIdx.y;
   if (Sl.pix[s] < 0 || Sl.skip[s]) return;
   const int np = C.np, nf = C.nfreq;
@@ -113,10 +132,14 @@ __global__ void __launch_bounds__(128, 1) k_lm_gram_tc(LMConf C, LMSlots Sl, con
     unsigned char* bl = diag ? al : ah + 3 * GT_TILE;
     // the tensor core has finished reading this buffer (block kb - 2)
     if (kb >= 2) ok = fztc::mbar_wait(&mbar[buf], ((kb - 2) >> 1) & 1, GT_WAIT_NS);
+    if (tid < GT_BK) {
+      const int k = kb * GT_BK + tid;
+      wk[buf][tid] = k < nf ? sqrtf((float)w[k]) * rin : 0.f;
+    }
     ok = __syncthreads_and(ok);
     if (!ok) break;
-    gram_stage(C, J, w, r0, kb * GT_BK, rin, ah, al);
-    if (!diag) gram_stage(C, J, w, c0, kb * GT_BK, rin, bh, bl);
+    gram_stage(C, J, wk[buf], r0, kb * GT_BK, ah, al);
+    if (!diag) gram_stage(C, J, wk[buf], c0, kb * GT_BK, bh, bl);
     fztc::fence_async_smem();
     __syncthreads();
     if (tid == 0) {

@@ -178,3 +178,38 @@ def test_many_wavelengths(fz, orc):
     ctx5.rf_nodes({1: 2, 6: 1})
     with pytest.raises(fz.FzError, match="limit"):
         ctx5.forward_rf(m, hydrostatic=True)
+
+
+def test_four_line_field_at_its_height_count(fz, orc):
+    """The four-line workload at its own shape: 160 heights, Fe I 6301.5,
+    6302.5, 15648.5 and 15652.9 x 96 wavelengths (NUMW 384, blocks of 512
+    threads), |B| up to 4000 G.  Stokes against the oracle with the
+    two-line tolerances (I 1e-5 relative, Q/U/V 1e-6 I_c) and the node
+    Jacobian of the benchmark's layout (T 5, Bx/By/Bz/v_z 2) within 2e-4 of
+    the largest entry of each parameter's node columns."""
+    lines = fz.lines_parse(fz.atmos.line_database_text())
+    reg = fz.regions_from_lines_section(fz.atmos.lines_section(4), lines)
+    g, _ = orc.gain(lines, reg)
+    nz = 160
+    ctx = fz.Synthesis(lines, reg, nz=nz, gain=g)
+    assert ctx.numw == 384
+    m = fz.atmos.make_columns(4, nz, seed=21, bmax=4000.0)
+    syn, mo, st = ctx.forward(m, hydrostatic=True)
+    osyn, omo, ost = orc.forward(lines, reg, g, m, hydrostatic=True)
+    assert np.all(st == 0) and np.all(ost == 0)
+    assert np.max(np.abs(syn[:, 0] - osyn[:, 0]) / np.abs(osyn[:, 0])) < 1e-5
+    assert np.max(np.abs(syn[:, 1:] - osyn[:, 1:])) < 1e-6
+    nodes = {1: 5, 4: 2, 5: 2, 6: 2, 7: 2}
+    ctx.rf_nodes(nodes)
+    rsyn, jac, _, st = ctx.forward_rf(m, hydrostatic=True)
+    orsyn, ojac, _, ost = orc.forward_rf(lines, reg, g, m, nodes, hydrostatic=True)
+    assert np.all(st == 0) and np.all(ost == 0)
+    assert np.max(np.abs(rsyn[:, 0] - orsyn[:, 0]) / np.abs(orsyn[:, 0])) < 1e-5
+    err = np.abs(jac.astype(np.float64) - ojac).max(axis=2)
+    j0 = 0
+    for p, nj in sorted(nodes.items()):
+        scale = np.abs(ojac[:, j0:j0 + nj]).max(axis=(1, 2))
+        assert np.all(scale > 0)
+        rel = err[:, j0:j0 + nj].max(axis=1) / scale
+        assert rel.max() <= 2e-4, (p, rel.max())
+        j0 += nj
