@@ -345,6 +345,7 @@ __device__ __forceinline__ void damp_der(const LineP& L, double nh, double T, co
 struct EvolSt {
   float tQ, tU, tV, rQ, rU, rV;
   float d, er, R, x, y, sg, it;   // eta2-rho2, eta.rho, theta/2, lambda1, lambda2, sign, 1/theta
+  float iv;                        // 1 / the larger root (x if d >= 0, else y; 0 when it is 0)
   float E, P, Qm, s2v, c2v, sh, ch;
 };
 
@@ -367,6 +368,8 @@ __device__ __forceinline__ void evol_state(float tI, float tQ, float tU, float t
     x = y > 0.0f ? fabsf(er) / y : 0.0f;
   }
   s.d = d; s.er = er; s.R = R; s.x = x; s.y = y;
+  const float root = d >= 0.0f ? x : y;
+  s.iv = root > 0.0f ? 1.0f / root : 0.0f;
   s.sg = er > 0.0f ? 1.0f : (er < 0.0f ? -1.0f : 0.0f);
   s.it = R > 0.0f ? 0.5f / R : 0.0f;
   s.E = expf(-tI);
@@ -448,17 +451,19 @@ __device__ __forceinline__ void evol_dir(const EvolSt& s, const EvolW& v, const 
   const float ede = s.tQ * deQ + s.tU * deU + s.tV * deV;
   const float rdr = s.rQ * drQ + s.rU * drU + s.rV * drV;
   const float der = s.rQ * deQ + s.rU * deU + s.rV * deV + s.tQ * drQ + s.tU * drU + s.tV * drV;
-  const float iR = s.R > 0.0f ? 1.0f / s.R : 0.0f;
+  // the layer's reciprocals come with its state: 1/R = 2 (0.5/R) exactly,
+  // 0.5/root = 0.5 (1/root) exactly; the quotients by the root are products
+  const float iR = 2.0f * s.it;
   const float dth = (s.d * (ede - rdr) + 2.0f * s.er * der) * iR;   // d theta
   float dx = 0.0f, dy = 0.0f;
   if (s.d >= 0.0f) {
     if (s.x > 0.0f) {
-      dx = (0.5f * dth + ede - rdr) * (0.5f / s.x);
-      dy = (s.sg * der - s.y * dx) / s.x;
+      dx = (0.5f * dth + ede - rdr) * (0.5f * s.iv);
+      dy = (s.sg * der - s.y * dx) * s.iv;
     }
   } else if (s.y > 0.0f) {
-    dy = (0.5f * dth - ede + rdr) * (0.5f / s.y);
-    dx = (s.sg * der - s.x * dy) / s.y;
+    dy = (0.5f * dth - ede + rdr) * (0.5f * s.iv);
+    dx = (s.sg * der - s.x * dy) * s.iv;
   }
   float Xd[4], Yd[4], M4d[4];
   xy_apply(deQ, deU, deV, drQ, drU, drV, v.w, Xd, Yd);
