@@ -392,24 +392,61 @@ __device__ __forceinline__ void voigt_f32(float a, float u, float& H, float& F) 
 // sinh at 2^53 (-> 1e15, :464-465) is reproduced; below it the operator is
 // evaluated with cancellation-free forms (cosh x -+ cos y via sinh^2(x/2),
 // sin^2(y/2); lambda_1,2 from the larger root).
-__device__ __forceinline__ void evol_f32(float tI, float tQ, float tU, float tV, float rQ, float rU, float rV,
-                                         float O[16], float& om0) {
-  const float eta2 = tQ * tQ + tU * tU + tV * tV;
-  const float rho2 = rQ * rQ + rU * rU + rV * rV;
-  const float er = tQ * rQ + tU * rU + tV * rV;
-  const float d = eta2 - rho2;
-  const float R = sqrtf(0.25f * d * d + er * er);
-  float x, y;   // lambda_1 dz, lambda_2 dz
-  if (d >= 0.0f) {
-    x = sqrtf(R + 0.5f * d);
-    y = x > 0.0f ? fabsf(er) / x : 0.0f;
+// The layer's scalars of the operator: |eta|^2, |rho|^2, eta.rho, their
+// difference d, R = theta / 2, the roots x = lambda_1 dz and y = lambda_2
+// dz, sign(eta.rho), 1/theta, e^-tI and the hyperbolic / trigonometric
+// factors (P = cosh-like, Qm = sinh^2(x/2) + sin^2(y/2), sh = sinh x,
+// s2v = sin y, c2v = cos y, ch = cosh x, amb = P - 1).
+struct EvolCore {
+  float eta2, rho2, er, d, R, x, y, sg, it, E, P, Qm, sh, s2v, c2v, ch, amb;
+  bool clamp;
+};
+
+__device__ __forceinline__ void evol_core(float tI, float tQ, float tU, float tV, float rQ, float rU, float rV,
+                                          EvolCore& c) {
+  c.eta2 = tQ * tQ + tU * tU + tV * tV;
+  c.rho2 = rQ * rQ + rU * rU + rV * rV;
+  c.er = tQ * rQ + tU * rU + tV * rV;
+  c.d = c.eta2 - c.rho2;
+  c.R = sqrtf(0.25f * c.d * c.d + c.er * c.er);
+  if (c.d >= 0.0f) {
+    c.x = sqrtf(c.R + 0.5f * c.d);
+    c.y = c.x > 0.0f ? fabsf(c.er) / c.x : 0.0f;
   } else {
-    y = sqrtf(R - 0.5f * d);
-    x = y > 0.0f ? fabsf(er) / y : 0.0f;
+    c.y = sqrtf(c.R - 0.5f * c.d);
+    c.x = c.y > 0.0f ? fabsf(c.er) / c.y : 0.0f;
   }
-  const float sg = er > 0.0f ? 1.0f : (er < 0.0f ? -1.0f : 0.0f);
-  const float theta = 2.0f * R;
-  const float it = theta > 0.0f ? 1.0f / theta : 0.0f;
+  c.sg = c.er > 0.0f ? 1.0f : (c.er < 0.0f ? -1.0f : 0.0f);
+  const float theta = 2.0f * c.R;
+  c.it = theta > 0.0f ? 1.0f / theta : 0.0f;
+  c.E = expf(-tI);
+  const float XCLAMP = 37.42994775f;   // cosh, sinh >= 2^53 in float64
+  c.amb = 0.0f;
+  c.s2v = sinf(c.y);
+  c.clamp = c.x >= XCLAMP;
+  if (c.clamp) {
+    const float c2 = cosf(c.y);
+    c.P = 0.5f * (1e15f + c2);
+    c.Qm = 0.5f * (1e15f - c2);
+    c.sh = 1e15f;
+    c.ch = 1e15f;
+    c.c2v = c2;
+  } else {
+    const float shx = sinhf(0.5f * c.x), siy = sinf(0.5f * c.y);
+    const float a = shx * shx, b = siy * siy;
+    c.amb = a - b;
+    c.P = 1.0f + c.amb;
+    c.Qm = a + b;
+    c.sh = sinhf(c.x);
+    c.ch = 1.0f + 2.0f * a;
+    c.c2v = 1.0f - 2.0f * b;
+  }
+}
+
+// O and om0 = 1 - O(1,1) from the layer's scalars.
+__device__ __forceinline__ void evol_matrix(const EvolCore& c, float tI, float tQ, float tU, float tV, float rQ,
+                                            float rU, float rV, float O[16], float& om0) {
+  const float x = c.x, y = c.y, sg = c.sg, it = c.it;
   // M2, M3, M4 (Fortran (row,col) -> O[4*(row-1)+(col-1)])
   const float m2_21 = (y * tQ - sg * x * rQ) * it, m2_31 = (y * tU - sg * x * rU) * it,
               m2_41 = (y * tV - sg * x * rV) * it;
@@ -419,36 +456,19 @@ __device__ __forceinline__ void evol_f32(float tI, float tQ, float tU, float tV,
               m3_41 = (x * tV + sg * y * rV) * it;
   const float m3_32 = (-sg * y * tV + x * rV) * it, m3_42 = (sg * y * tU - x * rU) * it,
               m3_43 = (-sg * y * tQ + x * rQ) * it;
-  const float m4_11 = (eta2 + rho2) * it;   // 2*((eta2+rho2)/2)/theta
+  const float m4_11 = (c.eta2 + c.rho2) * it;   // 2*((eta2+rho2)/2)/theta
   const float m4_21 = 2.0f * (tV * rU - tU * rV) * it, m4_31 = 2.0f * (tQ * rV - tV * rQ) * it,
               m4_41 = 2.0f * (tU * rQ - tQ * rU) * it;
   const float m4_22 = 2.0f * (tQ * tQ + rQ * rQ) * it - m4_11, m4_33 = 2.0f * (tU * tU + rU * rU) * it - m4_11,
               m4_44 = 2.0f * (tV * tV + rV * rV) * it - m4_11;
   const float m4_32 = 2.0f * (tQ * tU + rQ * rU) * it, m4_42 = 2.0f * (tV * tQ + rV * rQ) * it,
               m4_43 = 2.0f * (tU * tV + rU * rV) * it;
-  const float E = expf(-tI);
-  float P, Qm, sh, s2v;
-  const float XCLAMP = 37.42994775f;   // cosh, sinh >= 2^53 in float64
-  float amb = 0.0f;                    // sinh^2(x/2) - sin^2(y/2) = P - 1
-  s2v = sinf(y);
-  if (x >= XCLAMP) {
-    const float c2 = cosf(y);
-    P = 0.5f * (1e15f + c2);
-    Qm = 0.5f * (1e15f - c2);
-    sh = 1e15f;
-  } else {
-    const float shx = sinhf(0.5f * x), siy = sinf(0.5f * y);
-    const float a = shx * shx, b = siy * siy;
-    amb = a - b;
-    P = 1.0f + amb;
-    Qm = a + b;
-    sh = sinhf(x);
-  }
-  const float eP = E * P, eQ = E * Qm, eS = E * s2v, eH = E * sh;
+  const float E = c.E;
+  const float eP = E * c.P, eQ = E * c.Qm, eS = E * c.s2v, eH = E * c.sh;
   O[0] = eP + eQ * m4_11;
   // 1 - O(1,1) without cancellation in optically thin layers:
   // (1 - e^-tI) - e^-tI (P - 1 + Qm M4(1,1))
-  om0 = (x >= XCLAMP) ? 1.0f - O[0] : -expm1f(-tI) - E * (amb + Qm * m4_11);
+  om0 = c.clamp ? 1.0f - O[0] : -expm1f(-tI) - E * (c.amb + c.Qm * m4_11);
   O[5] = eP + eQ * m4_22;
   O[10] = eP + eQ * m4_33;
   O[15] = eP + eQ * m4_44;
@@ -466,6 +486,13 @@ __device__ __forceinline__ void evol_f32(float tI, float tQ, float tU, float tV,
   O[7] = eS * m2_42 + eH * m3_42 + eQ * m4_42;
   O[14] = -eS * m2_43 - eH * m3_43 + eQ * m4_43;
   O[11] = eS * m2_43 + eH * m3_43 + eQ * m4_43;
+}
+
+__device__ __forceinline__ void evol_f32(float tI, float tQ, float tU, float tV, float rQ, float rU, float rV,
+                                         float O[16], float& om0) {
+  EvolCore c;
+  evol_core(tI, tQ, tU, tV, rQ, rU, rV, c);
+  evol_matrix(c, tI, tQ, tU, tV, rQ, rU, rV, O, om0);
 }
 
 }  // namespace fzd

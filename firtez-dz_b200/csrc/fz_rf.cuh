@@ -349,48 +349,19 @@ struct EvolSt {
   float E, P, Qm, s2v, c2v, sh, ch;
 };
 
-// O and 1 - O(1,1) (as evol_f32) plus the state.
+// O and 1 - O(1,1) (as evol_f32) plus the state, from one evaluation of the
+// layer's scalars.
 __device__ __forceinline__ void evol_state(float tI, float tQ, float tU, float tV, float rQ, float rU, float rV,
                                            float O[16], float& om0, EvolSt& s) {
-  evol_f32(tI, tQ, tU, tV, rQ, rU, rV, O, om0);
+  EvolCore c;
+  evol_core(tI, tQ, tU, tV, rQ, rU, rV, c);
+  evol_matrix(c, tI, tQ, tU, tV, rQ, rU, rV, O, om0);
   s.tQ = tQ; s.tU = tU; s.tV = tV; s.rQ = rQ; s.rU = rU; s.rV = rV;
-  const float eta2 = tQ * tQ + tU * tU + tV * tV;
-  const float rho2 = rQ * rQ + rU * rU + rV * rV;
-  const float er = tQ * rQ + tU * rU + tV * rV;
-  const float d = eta2 - rho2;
-  const float R = sqrtf(0.25f * d * d + er * er);
-  float x, y;
-  if (d >= 0.0f) {
-    x = sqrtf(R + 0.5f * d);
-    y = x > 0.0f ? fabsf(er) / x : 0.0f;
-  } else {
-    y = sqrtf(R - 0.5f * d);
-    x = y > 0.0f ? fabsf(er) / y : 0.0f;
-  }
-  s.d = d; s.er = er; s.R = R; s.x = x; s.y = y;
-  const float root = d >= 0.0f ? x : y;
+  s.d = c.d; s.er = c.er; s.R = c.R; s.x = c.x; s.y = c.y; s.sg = c.sg;
+  s.it = c.it;   // 1/theta = 0.5/R
+  const float root = c.d >= 0.0f ? c.x : c.y;
   s.iv = root > 0.0f ? 1.0f / root : 0.0f;
-  s.sg = er > 0.0f ? 1.0f : (er < 0.0f ? -1.0f : 0.0f);
-  s.it = R > 0.0f ? 0.5f / R : 0.0f;
-  s.E = expf(-tI);
-  const float XCLAMP = 37.42994775f;
-  s.s2v = sinf(y);
-  if (x >= XCLAMP) {
-    const float c2 = cosf(y);
-    s.c2v = c2;
-    s.P = 0.5f * (1e15f + c2);
-    s.Qm = 0.5f * (1e15f - c2);
-    s.sh = 1e15f;
-    s.ch = 1e15f;
-  } else {
-    const float shx = sinhf(0.5f * x), siy = sinf(0.5f * y);
-    const float a = shx * shx, b = siy * siy;
-    s.P = 1.0f + a - b;
-    s.Qm = a + b;
-    s.sh = sinhf(x);
-    s.ch = 1.0f + 2.0f * a;
-    s.c2v = 1.0f - 2.0f * b;
-  }
+  s.E = c.E; s.P = c.P; s.Qm = c.Qm; s.s2v = c.s2v; s.c2v = c.c2v; s.sh = c.sh; s.ch = c.ch;
 }
 
 // X w = [eta.w~, eta w0 + rho x w~], Y w = [-rho.w~, -rho w0 + eta x w~]:
