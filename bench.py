@@ -669,9 +669,11 @@ def main():
         if profile:
             ctx.profile(True)
             ctx.profile_read()
+            torch.cuda.nvtx.range_push("profiled_" + tag)   # kernels launched one by one, between events
             for i in range(a.warmup, a.warmup + steps):
                 step(i, arm)
             torch.cuda.synchronize()
+            torch.cuda.nvtx.range_pop()
             ctx.profile(False)
             prof = ctx.profile_read(items=True)
         return maxms(e0.elapsed_time(e1) / steps), clocks, prof
