@@ -930,59 +930,56 @@ __global__ void __launch_bounds__(MAXT, (MAXT <= 256 ? 2 : 1)) k_synth_rf(const 
       const float* ckr = FULL ? nullptr : coef + k * np;
 #pragma unroll 1
       for (int p = 0; p < NSLOT; ++p) {
-        float dt[7], tmp[7];
-        if (p == 0) {
-          // T at constant Pg: dKLIN, du/dT = -u/(2T), da/dT
-          const float4 s0 = lds4(su), s1 = lds4(su + nthr), s2 = lds4(su + 2 * nthr), s3 = lds4(su + 3 * nthr),
-                       s4 = lds4(su + 4 * nthr);
-          const float hh[3] = {s0.x, s0.y, s0.z}, ff[3] = {s0.w, s1.x, s1.y}, av[3] = {s1.z, s1.w, s2.x};
-          const float ca[3] = {s2.y, s2.z, s2.w}, avu[3] = {s3.x, s3.y, s3.z}, cau[3] = {s3.w, s4.x, s4.y};
-          float xe[3], xr[3];
+        // every parameter's optical-depth derivatives in one form:
+        //   dt = A lmap(GA, hh, ff) + B lmap(g, U, V), dt[0] += C0
+        const float4 s0 = lds4(su), s1 = lds4(su + nthr), s2 = lds4(su + 2 * nthr);
+        const float hh[3] = {s0.x, s0.y, s0.z}, ff[3] = {s0.w, s1.x, s1.y};
+        const float av[3] = {s1.z, s1.w, s2.x}, ca[3] = {s2.y, s2.z, s2.w};
+        float U[3], V[3], A, B, C0 = 0.0f;
+        Geo GA = g;
+        if (p == 0) {   // T at constant Pg: dKLIN, du/dT = -u/(2T), da/dT
+          const float4 s3 = lds4(su + 3 * nthr), s4 = lds4(su + 4 * nthr);
+          const float avu[3] = {s3.x, s3.y, s3.z}, cau[3] = {s3.w, s4.x, s4.y};
 #pragma unroll
           for (int t = 0; t < 3; ++t) {
-            xe[t] = fmaf(ca[t], ddt, -avu[t] * halfT);
-            xr[t] = fmaf(av[t], ddt, cau[t] * halfT);
+            U[t] = fmaf(ca[t], ddt, -avu[t] * halfT);
+            V[t] = fmaf(av[t], ddt, cau[t] * halfT);
           }
-          lmap(g, xe, xr, tmp);
-          float base[7];
-          lmap(g, hh, ff, base);
+          A = dkt;
+          B = kldz;
+          C0 = row[dkoff];
+        } else if (p == 1) {   // Pg at constant T: dKLIN and da/dPg
 #pragma unroll
-          for (int x = 0; x < 7; ++x) dt[x] = fmaf(dkt, base[x], kldz * tmp[x]);
-          dt[0] = row[dkoff] + dt[0];
-        } else if (p == 1) {
-          // Pg at constant T: dKLIN and da/dPg
-          const float4 s0 = lds4(su), s1 = lds4(su + nthr), s2 = lds4(su + 2 * nthr);
-          const float hh[3] = {s0.x, s0.y, s0.z}, ff[3] = {s0.w, s1.x, s1.y}, av[3] = {s1.z, s1.w, s2.x};
-          const float ca[3] = {s2.y, s2.z, s2.w};
-          lmap(g, ca, av, tmp);
-          float base[7];
-          lmap(g, hh, ff, base);
-#pragma unroll
-          for (int x = 0; x < 7; ++x) dt[x] = fmaf(dkp, base[x], kldz * ddp * tmp[x]);
-          dt[0] = row[dkoff + 1] + dt[0];
-        } else if (p < 5) {
-          // B_i: geometry factors and the shift term du/dB
-          const float4 s0 = lds4(su), s1 = lds4(su + nthr), s4 = lds4(su + 4 * nthr), s5 = lds4(su + 5 * nthr);
-          const float hh[3] = {s0.x, s0.y, s0.z}, ff[3] = {s0.w, s1.x, s1.y}, avs[3] = {s4.z, s4.w, s5.x};
-          const float ncs[3] = {-s5.y, -s5.z, -s5.w};
-          float sh7[7];
-          lmap(g, avs, ncs, sh7);
+          for (int t = 0; t < 3; ++t) {
+            U[t] = ca[t];
+            V[t] = av[t];
+          }
+          A = dkp;
+          B = kldz * ddp;
+          C0 = row[dkoff + 1];
+        } else if (p < 5) {   // B_i: geometry factors and the shift term du/dB
+          const float4 s4 = lds4(su + 4 * nthr), s5 = lds4(su + 5 * nthr);
+          U[0] = s4.z; U[1] = s4.w; U[2] = s5.x;
+          V[0] = -s5.y; V[1] = -s5.z; V[2] = -s5.w;
           const float* dg = row + dgoff + 5 * (p - 2);
-          const Geo gd{dg[0], dg[1], dg[2], dg[3], dg[4]};
-          lmap(gd, hh, ff, tmp);
-          const float kb = idd * row[dboff + p - 2];
+          GA = Geo{dg[0], dg[1], dg[2], dg[3], dg[4]};
+          A = kldz;
+          B = kldz * (idd * row[dboff + p - 2]);
+        } else {   // v_z: du/dv = lu_duv / Doppler width
 #pragma unroll
-          for (int x = 0; x < 7; ++x) dt[x] = kldz * fmaf(kb, sh7[x], tmp[x]);
-        } else {
-          // v_z: du/dv = lu_duv / Doppler width
-          const float4 s1 = lds4(su + nthr), s2 = lds4(su + 2 * nthr);
-          const float av[3] = {s1.z, s1.w, s2.x};
-          const float nca[3] = {-s2.y, -s2.z, -s2.w};
-          lmap(g, av, nca, tmp);
-          const float kv = kldz * P.lu_duv[lb] * idd;
-#pragma unroll
-          for (int x = 0; x < 7; ++x) dt[x] = kv * tmp[x];
+          for (int t = 0; t < 3; ++t) {
+            U[t] = av[t];
+            V[t] = -ca[t];
+          }
+          A = 0.0f;
+          B = kldz * P.lu_duv[lb] * idd;
         }
+        float dt[7], ta[7], tb[7];
+        lmap(GA, hh, ff, ta);
+        lmap(g, U, V, tb);
+#pragma unroll
+        for (int x = 0; x < 7; ++x) dt[x] = A != 0.0f ? fmaf(A, ta[x], B * tb[x]) : B * tb[x];
+        dt[0] = C0 + dt[0];
         float rfp[4] = {0.f, 0.f, 0.f, 0.f};
         if (fin) {
           if (HE && p == 2) {
