@@ -281,6 +281,43 @@ def test_early_fallback_restart(fz, orc):
     assert res[1][1].sum() < res[0][1].sum()
 
 
+def test_deployable_rule_accepts_or_retraces_plain_lm(fz, orc):
+    """The benchmark's NN-warm rule (fallback 1, fallback_steps -1,
+    fallback_free) with one chi2 level T as every pixel's goal: a pixel whose
+    initial model is at or below T is the result after its one evaluation
+    (ITERS 1, chi2 = the initial model's); any other restarts at once from
+    the fallback model and, its goal dropped, ends exactly where plain LM
+    from that model ends -- chi2 and model bit for bit, one iteration more.
+    64 pixels through 24 slots, so refills and restarts share the pool."""
+    from firtez_dz_b200 import warmstart as ws
+    nz, npix = 48, 64
+    lines, reg, g, ctx = _ctx(fz, orc, nz)
+    true = fz.atmos.make_columns(npix, nz, seed=35)
+    obs, true_he, _ = ctx.forward(true, hydrostatic=True)
+    obs = obs + np.random.default_rng(6).normal(0.0, 1e-3, obs.shape)
+    ctx.rf_nodes(lmcase.NODES)
+    base = ws.default_models(npix, nz)
+    opts = fz.LMOpts(maxsteps=5, maxit=30, isigma=1e-3, dchi2=1e-3, slots=24)
+    m_pl, chi_pl, it_pl, st_pl = ctx.invert(obs, base, hydrostatic=True, opts=opts)
+    init = lmcase.initial_guess(true_he, seed=3)
+    init[::2, 0] += 600.0                            # every other start is poor
+    one = fz.LMOpts(maxsteps=5, maxit=1, isigma=1e-3, dchi2=1e-3, slots=24)
+    _, chi0, _, st0 = ctx.invert(obs, init, hydrostatic=True, opts=one)
+    T = float(np.median(chi0))
+    fb = np.ascontiguousarray(base[0])
+    rule = fz.LMOpts(maxsteps=5, maxit=30, isigma=1e-3, dchi2=1e-3, slots=24, fallback=1.0,
+                     fallback_model=fb.ctypes.data, fallback_steps=-1, fallback_free=True)
+    m, chi, it, st = ctx.invert(obs, init, hydrostatic=True, opts=rule, target=np.full(npix, T))
+    assert np.all(st == 0) and np.all(st_pl == 0) and np.all(st0 == 0)
+    acc = chi0 <= T
+    assert acc.any() and (~acc).any()
+    assert np.all(it[acc] == 1)
+    np.testing.assert_array_equal(chi[acc], chi0[acc])
+    np.testing.assert_array_equal(chi[~acc], chi_pl[~acc])
+    np.testing.assert_array_equal(it[~acc], it_pl[~acc] + 1)
+    np.testing.assert_array_equal(m[~acc], m_pl[~acc])
+
+
 @pytest.mark.parametrize("nx,ny,nz", [(7, 6, 9), (3, 8, 4), (5, 5, 16)])
 def test_smoothing_b_matches_oracle(fz, orc, nx, ny, nz):
     """SMOOTHING_B (the 1-2-1 smoothing of INITIALIZE_CYCLE) on the device
