@@ -347,7 +347,6 @@ __global__ void __launch_bounds__(256, 2) k_gemm_tma(const __grid_constant__ CUt
   if (warp == 0) fztc::tmem_dealloc(tmem, TM_BN);
 }
 
-// MSE loss 1/(n*nout) sum (y - t)^2 and dL/dy in bf16
 // Training-step state on the device, so that one captured step replays for
 // every batch: the position in the epoch's batch order and the Adam step.
 struct TrainState {
@@ -360,9 +359,11 @@ __device__ __forceinline__ size_t batch_row(const int* order, const TrainState* 
   return order ? (size_t)order[st->bi] * n : 0;
 }
 
+// MSE loss 1/(n*nout) sum lw_j (y - t)^2 (lw: per-output weights, null =
+// all 1) and dL/dy in bf16
 __global__ void k_mse(int n, int nout, const float* __restrict__ y, const float* __restrict__ t,
                       __nv_bfloat16* __restrict__ dy, float* __restrict__ loss, const int* __restrict__ order,
-                      const TrainState* __restrict__ st) {
+                      const TrainState* __restrict__ st, const float* __restrict__ lw = nullptr) {
   __shared__ float red[8];
   t += batch_row(order, st, n) * nout;
   const size_t total = (size_t)n * nout;
@@ -370,8 +371,9 @@ __global__ void k_mse(int n, int nout, const float* __restrict__ y, const float*
   const float sc = 2.0f / (float)total;
   for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (size_t)gridDim.x * blockDim.x) {
     const float d = y[i] - t[i];
-    s += d * d;
-    dy[i] = __float2bfloat16_rn(sc * d);
+    const float wd = lw ? lw[i % nout] * d : d;
+    s += wd * d;
+    dy[i] = __float2bfloat16_rn(sc * wd);
   }
   for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
   if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
@@ -476,6 +478,7 @@ struct fz_mlp {
   int* order = nullptr;           // device batch order of one epoch
   int order_cap = 0;
   int* d_err = nullptr;           // set by a tensor-core GEMM that gave up waiting for its MMAs
+  float* d_lw = nullptr;          // per-output loss weights (null: all 1)
 };
 
 namespace {
@@ -699,6 +702,7 @@ int fz_mlp_destroy(fz_mlp* p) {
   cudaFree(p->yout);
   cudaFree(p->loss);
   cudaFree(p->d_err);
+  cudaFree(p->d_lw);
   cudaFree(p->tstate);
   cudaFree(p->order);
   if (p->stream) cudaStreamDestroy(p->stream);
@@ -808,6 +812,25 @@ int fz_mlp_forward_obs_device(fz_mlp* p, int n, const double* d_obs, const float
   return r2;
 }
 
+// Per-output weights of the training loss (host, nout values), or none
+// (w null: every output weighs 1).
+int fz_mlp_set_loss_weights(fz_mlp* p, const float* w, int n) {
+  if (!p) return FZ_ERR_ARG;
+  if (w && n != p->dim[p->nl]) return FZ_ERR_ARG;
+  MLP_CK(cudaSetDevice(p->device));
+  if (p->stream) MLP_CK(cudaStreamSynchronize(p->stream));
+  if (!w) {
+    cudaFree(p->d_lw);
+    p->d_lw = nullptr;
+    return 0;
+  }
+  for (int j = 0; j < n; ++j)
+    if (!(w[j] >= 0.0f) || !std::isfinite(w[j])) return FZ_ERR_ARG;
+  if (!p->d_lw) MLP_CK(cudaMalloc(&p->d_lw, (size_t)n * sizeof(float)));
+  MLP_CK(cudaMemcpy(p->d_lw, w, (size_t)n * sizeof(float), cudaMemcpyHostToDevice));
+  return 0;
+}
+
 int fz_mlp_io(const fz_mlp* p, int* nin, int* nout) {
   if (!p) return FZ_ERR_ARG;
   if (nin) *nin = p->dim[0];
@@ -826,7 +849,8 @@ int fz_mlp_grad_device(fz_mlp* p, int n, const float* d_x, const float* d_t, flo
   k_to_bf16<<<grid1((size_t)n * d0), 256, 0, s>>>((size_t)n * d0, d_x, p->act[0]);
   mlp_fwd(p, n);
   MLP_CK(cudaMemsetAsync(p->loss, 0, sizeof(float), s));
-  k_mse<<<grid1((size_t)n * dl), 256, 0, s>>>(n, dl, p->yout, d_t, p->dz[p->nl - 1], p->loss, nullptr, nullptr);
+  k_mse<<<grid1((size_t)n * dl), 256, 0, s>>>(n, dl, p->yout, d_t, p->dz[p->nl - 1], p->loss, nullptr, nullptr,
+                                              p->d_lw);
   mlp_bwd(p, n);
   MLP_CK(cudaGetLastError());
   if (loss) MLP_CK(cudaMemcpyAsync(loss, p->loss, sizeof(float), cudaMemcpyDeviceToHost, s));
@@ -865,7 +889,7 @@ int fz_mlp_train_device(fz_mlp* p, int n, const float* d_x, const float* d_t, in
     k_batch_bf16<<<grid1((size_t)batch * d0), 256, 0, s>>>(batch, d0, d_x, p->order, p->tstate, p->act[0]);
     mlp_fwd(p, batch);
     k_mse<<<grid1((size_t)batch * dl), 256, 0, s>>>(batch, dl, p->yout, d_t, p->dz[p->nl - 1], p->loss, p->order,
-                                                   p->tstate);
+                                                   p->tstate, p->d_lw);
     mlp_bwd(p, batch);
     const float b1 = 0.9f, b2 = 0.999f;
     for (int l = 0; l < p->nl; ++l) {

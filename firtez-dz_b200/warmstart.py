@@ -39,6 +39,7 @@ def _bind():
     L.fz_mlp_train_device.argtypes = [P, ctypes.c_int, P, P, ctypes.c_int, ctypes.c_int, ctypes.c_float,
                                       ctypes.c_ulonglong, P]
     L.fz_mlp_forward_obs_device.argtypes = [P, ctypes.c_int, P, P, P, P, P]
+    L.fz_mlp_set_loss_weights.argtypes = [P, P, ctypes.c_int]
     L.fz_warm_start_device.argtypes = [P, P, ctypes.c_int, P, P, P, P, P]
     L.fz_invert_warm.argtypes = [P, P, P, P, ctypes.c_int, P, P, ctypes.c_int, P, P, P, P, P, P]
     L._mlp_bound = True
@@ -81,6 +82,14 @@ class MLP:
         if p.size != self.nparams:
             raise ValueError("expected %d parameters" % self.nparams)
         _check(_bind().fz_mlp_set_params(self._h, _p(p)))
+
+    def set_loss_weights(self, w=None):
+        """Per-output weights of the training loss (None: all 1)."""
+        if w is None:
+            _check(_bind().fz_mlp_set_loss_weights(self._h, None, 0))
+            return
+        a = np.ascontiguousarray(w, dtype=np.float32)
+        _check(_bind().fz_mlp_set_loss_weights(self._h, _p(a), int(a.size)))
 
     def forward_device(self, n, x_ptr, y_ptr, stream=0):
         _check(_bind().fz_mlp_forward_device(self._h, int(n), ctypes.c_void_p(x_ptr), ctypes.c_void_p(y_ptr),
@@ -199,8 +208,35 @@ class WarmStart:
         tt = torch.from_numpy(((t - self.tmu) / self.tsd).astype(np.float32)).cuda()
         return x, tt
 
-    def fit(self, x, t, epochs=8, batch=1024, lr=1e-3, seed=0):
-        """Adam on the device training set; returns the last epoch's mean loss."""
+    def chi2_weights(self, synth, ncol=8192, seed=97, bmax=2500.0):
+        """Loss weights under which the network's squared error approximates,
+        to first order, the chi2 its prior costs: w_j = tsd_j^2 (J^T J)_jj
+        (the node Jacobian of ncol seeded atmospheres of the training
+        generator, mean over columns; tsd_j the spread of node j in the
+        training set), normalised to mean 1.  Call after make_training_set,
+        with synth's node layout the network's."""
+        import torch
+        if self.tsd is None:
+            raise FzError("the network has no normalisation: make the training set first")
+        stream = torch.cuda.current_stream().cuda_stream
+        m = torch.from_numpy(atmos.make_columns(ncol, self.nz, seed=int(seed), bmax=bmax)).cuda()
+        syn = torch.empty((ncol, 4, self.numw), dtype=torch.float64, device="cuda")
+        jac = torch.empty((ncol, self.nout, 4 * self.numw), dtype=torch.float32, device="cuda")
+        mo = torch.empty_like(m)
+        synth.forward_rf_device(m.data_ptr(), ncol, syn.data_ptr(), jac.data_ptr(), mo.data_ptr(), 0, stream=stream,
+                                hydrostatic=True)
+        torch.cuda.synchronize()
+        jj = (jac.double() ** 2).sum(dim=2).mean(dim=0).cpu().numpy()   # (J^T J)_jj, node order
+        # the network's outputs follow PARAM_ROWS, the Jacobian's columns the
+        # reference's parameter order: the same sequence for this layout
+        w = jj * np.ravel(self.tsd) ** 2
+        return (w / w.mean()).astype(np.float32)
+
+    def fit(self, x, t, epochs=8, batch=1024, lr=1e-3, seed=0, loss_weights=None):
+        """Adam on the device training set; returns the last epoch's mean loss.
+        loss_weights: per-output weights of the squared error (e.g.
+        chi2_weights), None for the plain mean squared error."""
+        self.mlp.set_loss_weights(loss_weights)
         import torch
         torch.cuda.synchronize()
         n = (x.shape[0] // batch) * batch

@@ -609,6 +609,13 @@ MODULE FZ_B200
       INTEGER(C_INT)             :: NIN(*)
       INTEGER(C_INT)             :: NOUT(*)
     END FUNCTION
+    INTEGER(C_INT) FUNCTION FZ_MLP_SET_LOSS_WEIGHTS(MLP, W, N) BIND(C, &
+        NAME='fz_mlp_set_loss_weights')
+      IMPORT
+      TYPE(C_PTR), VALUE         :: MLP
+      REAL(C_FLOAT)              :: W(*)
+      INTEGER(C_INT), VALUE      :: N
+    END FUNCTION
     INTEGER(C_INT) FUNCTION FZ_WARM_START_DEVICE(CTX, MLP, NPIX, D_OBS, D_NORM, D_BASE, &
         D_MODELS, STREAM) BIND(C, NAME='fz_warm_start_device')
       IMPORT

@@ -514,6 +514,11 @@ int fz_mlp_train_device(fz_mlp* mlp, int n, const float* d_x, const float* d_t, 
 int fz_mlp_forward_obs_device(fz_mlp* mlp, int n, const double* d_obs, const float* d_mu, const float* d_sd,
                               float* d_y, void* stream);
 int fz_mlp_io(const fz_mlp* mlp, int* nin, int* nout);
+/* Per-output weights of the training loss, sum_j w_j (y_j - t_j)^2 / (n nout)
+ * (host array of dims[nlayers] finite values >= 0; w NULL restores equal
+ * weights).  The warm start weights each node by the chi2 its error costs
+ * to first order, so that the loss approximates the chi2 of the prior. */
+int fz_mlp_set_loss_weights(fz_mlp* mlp, const float* w, int n);
 
 /* The learned initial guess of the inversion (no counterpart in the
  * reference, whose LM starts from the control file's model or SET_TAU's

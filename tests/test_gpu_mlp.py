@@ -5,6 +5,7 @@
   also keeps the activations and dL/dz in bf16 between layers, so each
   layer's gradient is compared in relative L2 norm:
       |g_gpu - g_oracle| <= 3e-2 |g_oracle|,  outputs within 1e-2.
+* Per-output loss weights against the loss and bias gradient in numpy.
 * Training reduces the loss.
 * The gain over the method without it: LM started from the network's
   prediction reaches a lower median chi2 in fewer iterations than LM from
@@ -56,6 +57,43 @@ def test_forward_and_gradients_match_oracle(fz):
     assert abs(loss - lo) <= 1e-2 * lo
     for a, b in zip(_layers(g, DIMS), _layers(go, DIMS)):
         assert np.linalg.norm(a - b) <= 3e-2 * np.linalg.norm(b)
+
+
+def test_loss_weights(fz):
+    """fz_mlp_set_loss_weights: the loss is sum_j w_j (y_j - t_j)^2 / (n
+    nout) of the network's own outputs, and the last layer's bias gradient
+    2 w_j (y_j - t_j) / (n nout) summed over rows; equal weights give the
+    plain loss; a weight vector of the wrong length or a negative weight is
+    refused."""
+    import torch
+    from firtez_dz_b200 import warmstart as ws
+    net = ws.MLP(DIMS, seed=5)
+    rng = np.random.default_rng(6)
+    n = 256
+    x = rng.standard_normal((n, DIMS[0])).astype(np.float32)
+    t = rng.standard_normal((n, DIMS[-1])).astype(np.float32)
+    dx, dt = torch.from_numpy(x).cuda(), torch.from_numpy(t).cuda()
+    y = torch.empty((n, DIMS[-1]), dtype=torch.float32, device="cuda")
+    net.forward_device(n, dx.data_ptr(), y.data_ptr())
+    d = y.cpu().numpy().astype(np.float64) - t
+    w = rng.uniform(0.0, 3.0, DIMS[-1]).astype(np.float32)
+    net.set_loss_weights(w)
+    loss_w = net.grad_device(n, dx.data_ptr(), dt.data_ptr())
+    gb = net.get_params(grads=True)[-DIMS[-1]:]
+    ref = float(np.mean(d * d * w[None, :]))
+    assert abs(loss_w - ref) <= 1e-5 * ref
+    gref = (2.0 * d * w[None, :]).sum(axis=0) / d.size
+    assert np.linalg.norm(gb - gref) <= 2e-2 * np.linalg.norm(gref)   # dL/dy rounded to bf16
+    net.set_loss_weights(np.ones(DIMS[-1]))
+    loss_1 = net.grad_device(n, dx.data_ptr(), dt.data_ptr())
+    net.set_loss_weights(None)
+    loss_0 = net.grad_device(n, dx.data_ptr(), dt.data_ptr())
+    # the blocks' partial sums meet in atomics, in no fixed order
+    assert abs(loss_1 - loss_0) <= 1e-6 * loss_0 and abs(loss_0 - float(np.mean(d * d))) <= 1e-5 * loss_0
+    with pytest.raises(fz.FzError):
+        net.set_loss_weights(np.ones(DIMS[-1] - 1))
+    with pytest.raises(fz.FzError):
+        net.set_loss_weights(-np.ones(DIMS[-1]))
 
 
 def test_training_reduces_loss(fz):
