@@ -199,10 +199,12 @@ __global__ void __launch_bounds__(256, 1) k_gemm_tc(int M, int N, int K, const _
   if (warp == 0) fztc::tmem_dealloc(tmem, 128);
 }
 
-// The forward GEMMs (mode NT, both operands K-contiguous bf16 in device
-// memory) fed by the tensor memory accelerator: a 128 x 128 output tile per
+// The GEMMs whose bf16 operands sit in device memory with a 16-byte row
+// stride, fed by the tensor memory accelerator: a 128 x 128 output tile per
 // CTA of 256 threads, two CTAs per SM, K in blocks of 64 through three
-// shared-memory stages.
+// shared-memory stages.  An operand is K-major (AMN / BMN false: K
+// contiguous, the forward's X and W) or MN-major (true: MN contiguous, the
+// backward's dZ^T, X^T and W^T), the tensor core reading either layout.
 // Warp 0's lane 0 issues the bulk tensor copies of A (128 x 64) and B
 // (128 x 64) into a stage, 128-byte swizzled, and arms the stage's "full"
 // mbarrier with their byte count; warp 1's lane 0 waits for it, issues the
@@ -217,12 +219,13 @@ constexpr int TM_BM = 128, TM_BN = 128, TM_BK = 64, TM_ST = 3;
 constexpr int TM_TILE_A = TM_BM * TM_BK * 2, TM_TILE_B = TM_BN * TM_BK * 2;   // 16 KB each
 constexpr size_t TM_SMEM = (size_t)TM_ST * (TM_TILE_A + TM_TILE_B) + 1024;    // + the 1 KB alignment
 
-template <int EPI>
+template <int EPI, bool AMN, bool BMN>
 __global__ void __launch_bounds__(256, 2) k_gemm_tma(const __grid_constant__ CUtensorMap ta,
                                                      const __grid_constant__ CUtensorMap tb, int M, int N, int K,
-                                                     const float* __restrict__ bias, float* __restrict__ zout,
-                                                     float* __restrict__ fout, __nv_bfloat16* __restrict__ out,
-                                                     int ldc, int* __restrict__ err) {
+                                                     const float* __restrict__ bias, const float* __restrict__ zin,
+                                                     float* __restrict__ zout, float* __restrict__ fout,
+                                                     __nv_bfloat16* __restrict__ out, int ldc,
+                                                     int* __restrict__ err) {
   extern __shared__ unsigned char tm_raw[];
   __shared__ __align__(8) uint64_t full[TM_ST], empty[TM_ST], done;
   __shared__ uint32_t tbase;
@@ -261,15 +264,28 @@ __global__ void __launch_bounds__(256, 2) k_gemm_tma(const __grid_constant__ CUt
           break;
         }
         unsigned char* sa = tiles + (size_t)st * (TM_TILE_A + TM_TILE_B);
+        unsigned char* sb = sa + TM_TILE_A;
         fztc::mbar_arrive_expect_tx(&full[st], TM_TILE_A + TM_TILE_B);
-        fztc::tma_load_2d(sa, &ta, kb * TM_BK, m0, &full[st]);
-        fztc::tma_load_2d(sa + TM_TILE_A, &tb, kb * TM_BK, n0, &full[st]);
+        // K-major: one 64 (K) x 128 box; MN-major: two 64 (MN) x 64 (K)
+        // boxes, the second 64 MN elements 8 KB on
+        if (AMN) {
+          fztc::tma_load_2d(sa, &ta, m0, kb * TM_BK, &full[st]);
+          fztc::tma_load_2d(sa + TM_TILE_A / 2, &ta, m0 + 64, kb * TM_BK, &full[st]);
+        } else {
+          fztc::tma_load_2d(sa, &ta, kb * TM_BK, m0, &full[st]);
+        }
+        if (BMN) {
+          fztc::tma_load_2d(sb, &tb, n0, kb * TM_BK, &full[st]);
+          fztc::tma_load_2d(sb + TM_TILE_B / 2, &tb, n0 + 64, kb * TM_BK, &full[st]);
+        } else {
+          fztc::tma_load_2d(sb, &tb, kb * TM_BK, n0, &full[st]);
+        }
       }
     }
     __syncwarp();
   } else if (warp == 1) {
     if (lane == 0) {
-      const uint32_t idesc = fztc::idesc_bf16(TM_BM, TM_BN);
+      const uint32_t idesc = fztc::idesc_bf16_major(TM_BM, TM_BN, AMN, BMN);
       int kb = 0;
       for (; kb < nkb; ++kb) {
         const int st = kb % TM_ST;
@@ -280,9 +296,11 @@ __global__ void __launch_bounds__(256, 2) k_gemm_tma(const __grid_constant__ CUt
         fztc::fence_after_sync();
         const uint32_t sa = base + (uint32_t)st * (TM_TILE_A + TM_TILE_B), sb = sa + TM_TILE_A;
 #pragma unroll
-        for (int ks = 0; ks < TM_BK / 16; ++ks)
-          fztc::mma_bf16(tmem, fztc::desc_sw128(sa + 32 * ks), fztc::desc_sw128(sb + 32 * ks), idesc,
-                         (kb > 0 || ks > 0) ? 1u : 0u);
+        for (int ks = 0; ks < TM_BK / 16; ++ks) {
+          const uint64_t da = AMN ? fztc::desc_sw128_mn(sa + 2048 * ks, TM_TILE_A / 2) : fztc::desc_sw128(sa + 32 * ks);
+          const uint64_t db = BMN ? fztc::desc_sw128_mn(sb + 2048 * ks, TM_TILE_B / 2) : fztc::desc_sw128(sb + 32 * ks);
+          fztc::mma_bf16(tmem, da, db, idesc, (kb > 0 || ks > 0) ? 1u : 0u);
+        }
         fztc::commit(&empty[st]);
       }
       if (kb == nkb) fztc::commit(&done);
@@ -304,9 +322,20 @@ __global__ void __launch_bounds__(256, 2) k_gemm_tma(const __grid_constant__ CUt
       const int nb = n0 + 64 * half + cc;
       const size_t o = (size_t)m * ldc + nb;
       if (vec && nb + 16 <= N) {
+        if (EPI == EPI_FWD_GELU || EPI == EPI_FWD_LIN)
 #pragma unroll
-        for (int i = 0; i < 16; ++i) v[i] += __ldg(&bias[nb + i]);
-        if (EPI == EPI_FWD_GELU) {
+          for (int i = 0; i < 16; ++i) v[i] += __ldg(&bias[nb + i]);
+        if (EPI == EPI_BWD_GELU) {
+          uint32_t h[8];
+#pragma unroll
+          for (int i = 0; i < 8; ++i) {
+            const float2 z = __ldg(reinterpret_cast<const float2*>(zin + o) + i);
+            const __nv_bfloat162 t = __floats2bfloat162_rn(v[2 * i] * gelu_d(z.x), v[2 * i + 1] * gelu_d(z.y));
+            h[i] = *reinterpret_cast<const uint32_t*>(&t);
+          }
+          *reinterpret_cast<uint4*>(out + o) = make_uint4(h[0], h[1], h[2], h[3]);
+          *reinterpret_cast<uint4*>(out + o + 8) = make_uint4(h[4], h[5], h[6], h[7]);
+        } else if (EPI == EPI_FWD_GELU) {
           if (zout)
 #pragma unroll
             for (int i = 0; i < 16; i += 4)
@@ -329,12 +358,18 @@ __global__ void __launch_bounds__(256, 2) k_gemm_tma(const __grid_constant__ CUt
         for (int i = 0; i < 16; ++i) {
           const int n = nb + i;
           if (n >= N) continue;
-          const float z = v[i] + bias[n];
-          if (EPI == EPI_FWD_GELU) {
-            if (zout) zout[o + i] = z;
-            out[o + i] = __float2bfloat16_rn(gelu(z));
+          if (EPI == EPI_BWD_GELU) {
+            out[o + i] = __float2bfloat16_rn(v[i] * gelu_d(zin[o + i]));
+          } else if (EPI == EPI_F32) {
+            fout[o + i] = v[i];
           } else {
-            fout[o + i] = z;
+            const float z = v[i] + bias[n];
+            if (EPI == EPI_FWD_GELU) {
+              if (zout) zout[o + i] = z;
+              out[o + i] = __float2bfloat16_rn(gelu(z));
+            } else {
+              fout[o + i] = z;
+            }
           }
         }
       }
@@ -551,19 +586,51 @@ bool tmap_kmajor(CUtensorMap* m, const __nv_bfloat16* p, int rows, int K, int ld
             CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
+// An MN-contiguous bf16 operand (K rows of mn elements, row stride ld) as a
+// 2-D tensor map of 64 x 64 boxes (MN inner) with 128-byte swizzling.
+bool tmap_mnmajor(CUtensorMap* m, const __nv_bfloat16* p, int K, int mn, int ld) {
+  const EncodeTiledFn fn = encode_tiled();
+  if (!fn || mn < 64 || K < TM_BK || (reinterpret_cast<uintptr_t>(p) & 15) || ((size_t)ld * 2) % 16) return false;
+  const cuuint64_t dims[2] = {(cuuint64_t)mn, (cuuint64_t)K};
+  const cuuint64_t strides[1] = {(cuuint64_t)ld * 2};
+  const cuuint32_t box[2] = {64, (cuuint32_t)TM_BK};
+  const cuuint32_t es[2] = {1, 1};
+  return fn(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<__nv_bfloat16*>(p), dims, strides, box, es,
+            CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
 template <int MODE, int EPI>
 void gemm(cudaStream_t s, int* err, int M, int N, int K, const __nv_bfloat16* A, int lda, const __nv_bfloat16* B,
           int ldb, const float* bias, const float* zin, float* zout, float* fout, __nv_bfloat16* out, int ldc) {
+  const dim3 gtm((N + TM_BN - 1) / TM_BN, (M + TM_BM - 1) / TM_BM);
+  CUtensorMap ma, mb;
   if constexpr (MODE == NT && (EPI == EPI_FWD_GELU || EPI == EPI_FWD_LIN)) {
-    CUtensorMap ma, mb;
     if (tmap_kmajor(&ma, A, M, K, lda) && tmap_kmajor(&mb, B, N, K, ldb)) {
-      const dim3 grid((N + TM_BN - 1) / TM_BN, (M + TM_BM - 1) / TM_BM);
-      k_gemm_tma<EPI><<<grid, 256, TM_SMEM, s>>>(ma, mb, M, N, K, bias, zout, fout, out, ldc, err);
+      k_gemm_tma<EPI, false, false><<<gtm, 256, TM_SMEM, s>>>(ma, mb, M, N, K, bias, zin, zout, fout, out, ldc, err);
+      return;
+    }
+  } else if constexpr (MODE == NN && EPI == EPI_BWD_GELU) {
+    // A = dZ (M x K, K contiguous); B[n][k] = W[k][n]: W's rows are K
+    if (tmap_kmajor(&ma, A, M, K, lda) && tmap_mnmajor(&mb, B, K, N, ldb) && (ldc & 7) == 0) {
+      k_gemm_tma<EPI, false, true><<<gtm, 256, TM_SMEM, s>>>(ma, mb, M, N, K, bias, zin, zout, fout, out, ldc, err);
+      return;
+    }
+  } else if constexpr (MODE == TN && EPI == EPI_F32) {
+    // A[m][k] = dZ[k][m], B[n][k] = X[k][n]: both with K as the row index
+    if (tmap_mnmajor(&ma, A, K, M, lda) && tmap_mnmajor(&mb, B, K, N, ldb)) {
+      k_gemm_tma<EPI, true, true><<<gtm, 256, TM_SMEM, s>>>(ma, mb, M, N, K, bias, zin, zout, fout, out, ldc, err);
       return;
     }
   }
   const dim3 grid((N + 127) / 128, (M + 127) / 128);
   k_gemm_tc<MODE, EPI><<<grid, 256, TC_SMEM, s>>>(M, N, K, A, lda, B, ldb, bias, zin, zout, fout, out, ldc, err);
+}
+
+template <typename F>
+cudaError_t tma_attrs(F* kernel) {
+  cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TM_SMEM);
+  return e == cudaSuccess ? cudaFuncSetAttribute(kernel, cudaFuncAttributePreferredSharedMemoryCarveout, 100) : e;
 }
 
 // The tensor-core GEMMs' shared memory above the default 48 KB (set once,
@@ -577,15 +644,11 @@ int gemm_tc_attrs() {
     e = cudaFuncSetAttribute(k_gemm_tc<TN, EPI_F32>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TC_SMEM);
   if (e == cudaSuccess)
     e = cudaFuncSetAttribute(k_gemm_tc<NN, EPI_BWD_GELU>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TC_SMEM);
-  if (e == cudaSuccess)
-    e = cudaFuncSetAttribute(k_gemm_tma<EPI_FWD_GELU>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TM_SMEM);
-  if (e == cudaSuccess)
-    e = cudaFuncSetAttribute(k_gemm_tma<EPI_FWD_LIN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TM_SMEM);
   // two CTAs per SM (97 KB each): one CTA's epilogue overlaps the other's MMAs
-  if (e == cudaSuccess)
-    e = cudaFuncSetAttribute(k_gemm_tma<EPI_FWD_GELU>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
-  if (e == cudaSuccess)
-    e = cudaFuncSetAttribute(k_gemm_tma<EPI_FWD_LIN>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+  if (e == cudaSuccess) e = tma_attrs(k_gemm_tma<EPI_FWD_GELU, false, false>);
+  if (e == cudaSuccess) e = tma_attrs(k_gemm_tma<EPI_FWD_LIN, false, false>);
+  if (e == cudaSuccess) e = tma_attrs(k_gemm_tma<EPI_BWD_GELU, false, true>);
+  if (e == cudaSuccess) e = tma_attrs(k_gemm_tma<EPI_F32, true, true>);
   if (e != cudaSuccess) {
     std::fprintf(stderr, "fz_b200 mlp: CUDA error %s\n", cudaGetErrorString(e));
     return FZ_ERR_CUDA;

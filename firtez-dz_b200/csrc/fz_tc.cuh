@@ -40,10 +40,23 @@ __host__ __device__ __forceinline__ uint64_t desc_sw128(uint32_t saddr) {
          ((uint64_t)2 << 61);
 }
 
+// The same swizzle for an MN-major tile (MN contiguous): 128-byte rows of 64
+// MN elements, one row per K index; 8-row K groups 1 KB apart (SBO), the
+// next 64 MN elements lbo bytes on (LBO).  The MMA's 16-wide K step
+// advances the start address by 16 rows = 2 KB.
+__host__ __device__ __forceinline__ uint64_t desc_sw128_mn(uint32_t saddr, uint32_t lbo) {
+  return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)((lbo >> 4) & 0x3FFFu) << 16) |
+         ((uint64_t)(1024u >> 4) << 32) | ((uint64_t)1 << 46) | ((uint64_t)2 << 61);
+}
+
 // Instruction descriptor of kind::f16: D FP32 (bit 4), A and B bf16 (bits
 // 7-9, 10-12 = 1), both K-major, N >> 3 at bit 17, M >> 4 at bit 24.
 __host__ __device__ constexpr uint32_t idesc_bf16(int M, int N) {
   return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
+}
+// ... with A (bit 15) and / or B (bit 16) MN-major
+__host__ __device__ constexpr uint32_t idesc_bf16_major(int M, int N, bool a_mn, bool b_mn) {
+  return idesc_bf16(M, N) | (a_mn ? 1u << 15 : 0u) | (b_mn ? 1u << 16 : 0u);
 }
 
 // D (+)= A B^T on the tensor core, issued by one thread; acc = 0 overwrites D.

@@ -40,6 +40,9 @@ int main() {
   for (int n = 16; n <= 128; n += 16) std::printf("I %d %u\n", n, fztc::idesc_bf16(128, n));
   std::printf("S %llu\n", (unsigned long long)fztc::desc_kmajor(0x1230u, 128u, 1024u));
   std::printf("W %llu\n", (unsigned long long)fztc::desc_sw128(0x4c00u + 32u));
+  std::printf("M %llu\n", (unsigned long long)fztc::desc_sw128_mn(0x4c00u + 2048u, 8192u));
+  std::printf("J %u %u %u\n", fztc::idesc_bf16_major(128, 128, false, true), fztc::idesc_bf16_major(128, 128, true, true),
+              fztc::idesc_bf16(128, 128));
   for (int r = 0; r < 128; ++r)
     for (int k = 0; k < 64; k += 4) std::printf("O %d %d %u\n", r, k, fztc::kmajor_offset(r, k, 8));
   return 0;
@@ -90,6 +93,21 @@ def test_swizzled_shared_memory_descriptor(probe):
     assert field(v, 46, 2) == 1
     assert field(v, 49, 3) == 0 and field(v, 52, 1) == 0
     assert field(v, 61, 3) == 2                              # SWIZZLE_128B
+
+
+def test_mn_major_descriptors(probe):
+    """MN-major operands of the backward GEMMs: the 128-byte-swizzled tile of
+    two 64-element MN halves 8 KB apart (LBO) with 8-row K groups 1 KB apart
+    (SBO), the start advanced 2 KB per 16-wide K step; the instruction
+    descriptor's A- and B-major bits (15, 16) set for MN-major operands,
+    nothing else changed."""
+    v = int([ln for ln in probe if ln.startswith("M ")][0].split()[1])
+    assert field(v, 0, 14) == (0x4c00 + 2048) >> 4
+    assert field(v, 16, 14) == 8192 >> 4
+    assert field(v, 32, 14) == 1024 >> 4
+    assert field(v, 46, 2) == 1 and field(v, 61, 3) == 2
+    b_mn, ab_mn, plain = (int(x) for x in [ln for ln in probe if ln.startswith("J ")][0].split()[1:])
+    assert b_mn == plain | (1 << 16) and ab_mn == plain | (1 << 15) | (1 << 16)
 
 
 def test_operand_offsets_match_the_descriptor_addressing(probe):
