@@ -17,18 +17,18 @@ Calibration, before the timed region: plain LM from the default guess on
 32,768 pixels of a separate seeded set (same generator, same noise); the
 acceptance level T is the 20th percentile of their chi2 (--accept-quantile).
 
-One step = the inversion of one tile of 131072 pixels of the field (one
-inversion call), inputs resident in HBM.  Headline arm (``value``): the
+One step = the inversion of the whole 512 x 512 field (one inversion call
+of 262,144 pixels), inputs resident in HBM.  Headline arm (``value``): the
 deployable NN-warm rule -- the network's model of every pixel is evaluated
 once; a pixel whose chi2 there is at or below T is converged with it, every
 other pixel restarts at once from the default guess in the same slot pool
 and runs plain LM (fallback_steps -1, fallback_free).  ``value`` = its
-pixels/s; the plain arm (LM from the default guess, plain stop rules) is the
-yardstick, and the line gives the speed-up over it, both median chi2, the
+pixels/s; the plain arm (LM from the default guess, plain stop rules; at
+most --plain-steps timed steps) is the yardstick, and the line gives the speed-up over it, both median chi2, the
 fraction of pixels whose chi2 ends above 1.1x their plain-LM chi2 and the
-parameter errors against the true atmospheres.  Beside it: the same rule at
-two other quantiles, NN-warm LM with the plain stop rules only, and plain LM
-from SET_TAU's assisted guess.  ``e2e``: the headline arm through
+parameter errors against the true atmospheres.  Beside it (--sub-steps
+steps each): the same rule at two other quantiles, NN-warm LM with the plain
+stop rules only, and plain LM from SET_TAU's assisted guess.  ``e2e``: the headline arm through
 fz_invert_warm from pinned host memory.  Multi-GPU: each rank inverts tiles of
 its own field (weak scaling, no collective on the data path; a barrier and the
 max over ranks of each time).
@@ -462,7 +462,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--field", type=int, default=512, help="field side (pixels)")
-    ap.add_argument("--tile", type=int, default=131072, help="pixels per step")
+    ap.add_argument("--tile", type=int, default=0, help="pixels per step (0: the whole field)")
     ap.add_argument("--slots", type=int, default=8192)
     ap.add_argument("--nz", type=int, default=128)
     ap.add_argument("--train-pairs", type=int, default=2097152)
@@ -474,13 +474,16 @@ def main():
     ap.add_argument("--accept-quantile", type=float, default=0.2,
                     help="T = this quantile of the calibration set's plain-LM chi2")
     ap.add_argument("--calib-pixels", type=int, default=32768)
-    ap.add_argument("--sub-steps", type=int, default=4, help="timed steps of each secondary arm (at most --steps)")
+    ap.add_argument("--sub-steps", type=int, default=1, help="timed steps of each secondary arm (at most --steps)")
+    ap.add_argument("--plain-steps", type=int, default=4, help="timed steps of the plain-LM yardstick (at most --steps)")
     ap.add_argument("--c5-tiles", type=int, default=2, help="65536-pixel tiles of the four-line workload (0: off)")
     ap.add_argument("--c5-train-pairs", type=int, default=524288)
     ap.add_argument("--c5-epochs", type=int, default=4)
     ap.add_argument("--probe-kernels", type=int, default=0, help="run the FLOP-count launches on N columns and exit")
     ap.add_argument("--flops-from", default="", help="ncu CSV of --probe-kernels -> profiles/flops.json, then exit")
     a = ap.parse_args()
+    if a.tile <= 0 or a.tile > a.field * a.field:
+        a.tile = a.field * a.field   # one inversion call per step over the whole field
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -560,17 +563,13 @@ def main():
         # once per candidate; the arms below use the tuned slot count
         t0 = time.perf_counter()
         tf = ctx.autotune_forward(base.data_ptr(), min(8192, a.tile), hydrostatic=True)
-        cands = tuple(c for c in (a.tile // 4, a.tile // 2, a.tile) if c >= 256)
-        tl = ctx.autotune_lm(a.tile, obs[:a.tile].data_ptr(), base.data_ptr(), candidates=cands, opts=opts)
+        ntune = min(a.tile, 131072)   # the slot count on the field's first 131,072 pixels
+        cands = tuple(c for c in (ntune // 4, ntune // 2, ntune) if c >= 256)
+        tl = ctx.autotune_lm(ntune, obs[:ntune].data_ptr(), base.data_ptr(), candidates=cands, opts=opts)
         tuned = {"shapes": ctx.tune(), "slot_candidates": list(cands),
                  "forward_ms": {k: tf[k] for k in ("chain_ms", "chemder_ms", "opac_rf_ms")},
                  "lm_pixels_per_s_at_best": tl["lm_pixels_per_s"], "tuning_s": time.perf_counter() - t0}
         opts = fz.LMOpts(maxsteps=5, maxit=40, dchi2=1e-3, isigma=1e-3, slots=0)
-    ntiles = npix // a.tile
-    bufs = {"out": torch.empty((a.tile, 13, a.nz), dtype=torch.float32, device="cuda"),
-            "chi": torch.empty(a.tile, dtype=torch.float64, device="cuda"),
-            "it": torch.empty(a.tile, dtype=torch.int32, device="cuda"),
-            "st": torch.empty(a.tile, dtype=torch.int32, device="cuda")}
     # ----------------------------------------------------------- calibration
     # plain LM from the default guess on a separate seeded set (same
     # generator, same noise; the same set on every rank): T = a quantile of
@@ -606,7 +605,7 @@ def main():
     # the reference's own non-learned guess: SET_TAU's T, B and v_z assists
     # on the default model over the tile as a 512 x 256 field
     tau_init = torch.empty_like(base)
-    tau_ny = 256
+    tau_ny = a.field if a.tile == npix else 256
     tau_nx = a.tile // tau_ny
     # the deployable rule: the warm-start model is evaluated once; at or
     # below T it is the result, above T the pixel restarts at once from the
@@ -678,9 +677,10 @@ def main():
             prof = ctx.profile_read(items=True)
         return maxms(e0.elapsed_time(e1) / steps), clocks, prof
 
-    # plain LM from the default guess: the yardstick (same tiles: the
-    # warm-up tiles first, then the timed ones)
-    ms_pl, clocks_pl, _ = timed("plain", a.steps, a.warmup, "plain")
+    # plain LM from the default guess: the yardstick (the same field; one
+    # warm-up step, the graphs and kernels being those of the calibration)
+    steps_pl = max(1, min(a.plain_steps, a.steps))
+    ms_pl, clocks_pl, _ = timed("plain", steps_pl, 1, "plain")
     plain_value = world * a.tile / (ms_pl * 1e-3)
     # headline: the deployable NN-warm rule at T
     ms_nn, clocks, prof = timed("nn", a.steps, a.warmup, "nn", profile=True)
@@ -688,7 +688,7 @@ def main():
     sub = max(1, min(a.sub_steps, a.steps))
     ms_sub = {}
     for arm in ("nn_q10", "nn_q30", "free", "tau"):
-        ms_sub[arm], _, _ = timed(arm, sub, 1, arm)
+        ms_sub[arm], _, _ = timed(arm, sub, 0, arm)
 
     def versus_plain(arm):
         """chi2 and iterations of an arm against plain LM on the same tiles."""
@@ -797,7 +797,7 @@ def main():
     h_obs[:] = obs[:a.tile].reshape(a.tile, 4, numw).cpu().numpy()
     h_out = (pin((a.tile, 13, a.nz), torch.float32), pin((a.tile,), torch.float64), pin((a.tile,), torch.int32),
              pin((a.tile,), torch.int32))
-    e2e_steps = max(1, min(a.steps, a.sub_steps))
+    e2e_steps = max(1, min(a.steps, 2))
     h_target = pin((a.tile,), torch.float64)
     h_target[:] = levels["nn"]
     h_base = pin((13, a.nz), torch.float32)
