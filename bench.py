@@ -1105,9 +1105,9 @@ def main():
            "kernel_columns_per_launch": {k: v[2] for k, v in per_launch.items()},
            "e2e": e2e,
            # kernels counted by the context plus, per step, the warm start:
-           # per 16384-pixel chunk one conversion + 4 GEMMs, then the node
-           # expansion
-           "gpu_launches": int(sum(v[1] for v in prof.values()) + (5 * nchunk + 1) * a.steps),
+           # per 16384-pixel chunk one conversion + 4 GEMMs, then CONTRACT of
+           # the base model and the node expansion
+           "gpu_launches": int(sum(v[1] for v in prof.values()) + (5 * nchunk + 2) * a.steps),
            "clocks": clocks}
     if world == 1:
         # the oracle on the host cores, with its own line parse (the same rows)

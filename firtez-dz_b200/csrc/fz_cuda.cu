@@ -2420,16 +2420,12 @@ __global__ void k_f64_to_f32(size_t n, const double* __restrict__ a, float* __re
 // EXPAND(v - CONTRACT(base)) -- the way the inversion perturbs a model
 // (CONTRACT_VECTOR / EXPAND_VECTOR, src/get_dmodel.f90:839-880); the other
 // rows are the base model's.  coef: the (nz, np) hat table in FP32.
-__global__ void __launch_bounds__(128) k_ws_expand(int npix, int nz, RFConf R, const float* __restrict__ coef,
-                                                   const float* __restrict__ y, const float* __restrict__ tmu,
-                                                   const float* __restrict__ tsd, const float* __restrict__ base,
-                                                   float* __restrict__ out) {
-  extern __shared__ float wsv[];   // np node offsets v - CONTRACT(base)
+// CONTRACT(base) of the one base model every pixel shares: node j's hat
+// average of its parameter's row (one thread per node, once per call).
+__global__ void k_ws_contract(int nz, RFConf R, const float* __restrict__ coef, const float* __restrict__ base,
+                              float* __restrict__ cb) {
   static const int kRow[NSLOT] = {0, 1, 5, 6, 7, 10};   // model rows of T, Pg, Bx, By, Bz, v_z
-  const int pix = blockIdx.x;
   const int np = R.np;
-  float* m = out + (size_t)pix * 13 * nz;
-  for (int i = threadIdx.x; i < 13 * nz; i += blockDim.x) m[i] = base[i];
   for (int j = threadIdx.x; j < np; j += blockDim.x) {
     int p = 0;
     while (p < NSLOT - 1 && j >= R.n0[p] + R.nj[p]) ++p;
@@ -2437,8 +2433,21 @@ __global__ void __launch_bounds__(128) k_ws_expand(int npix, int nz, RFConf R, c
     float a = 0.0f, cs = 0.0f;
     for (int k = 0; k < nz; ++k) cs += coef[(size_t)k * np + j];
     for (int k = 0; k < nz; ++k) a += b[k] * (coef[(size_t)k * np + j] / cs);
-    wsv[j] = fmaf(y[(size_t)pix * np + j], tsd[j], tmu[j]) - a;
+    cb[j] = a;
   }
+}
+
+__global__ void __launch_bounds__(128) k_ws_expand(int npix, int nz, RFConf R, const float* __restrict__ coef,
+                                                   const float* __restrict__ y, const float* __restrict__ tmu,
+                                                   const float* __restrict__ tsd, const float* __restrict__ base,
+                                                   const float* __restrict__ cb, float* __restrict__ out) {
+  extern __shared__ float wsv[];   // np node offsets v - CONTRACT(base)
+  static const int kRow[NSLOT] = {0, 1, 5, 6, 7, 10};   // model rows of T, Pg, Bx, By, Bz, v_z
+  const int pix = blockIdx.x;
+  const int np = R.np;
+  float* m = out + (size_t)pix * 13 * nz;
+  for (int i = threadIdx.x; i < 13 * nz; i += blockDim.x) m[i] = base[i];
+  for (int j = threadIdx.x; j < np; j += blockDim.x) wsv[j] = fmaf(y[(size_t)pix * np + j], tsd[j], tmu[j]) - cb[j];
   __syncthreads();
   for (int p = 0; p < NSLOT; ++p) {
     if (R.nj[p] == 0) continue;
@@ -4234,17 +4243,19 @@ int fz_warm_start_device(fz_ctx* c, fz_mlp* mlp, int npix, const double* d_obs, 
   FZ_CK(cudaSetDevice(c->device));
   cudaStream_t s = (cudaStream_t)stream;
   const size_t ny = (size_t)npix * np;
-  if (ny > c->wsy_len) {
+  if (ny + np > c->wsy_len) {
     FZ_CK(cudaStreamSynchronize(s));
     cudaFree(c->d_wsy);
     c->d_wsy = nullptr;
     c->wsy_len = 0;
-    FZ_CK(cudaMalloc(&c->d_wsy, ny * sizeof(float)));
-    c->wsy_len = ny;
+    FZ_CK(cudaMalloc(&c->d_wsy, (ny + np) * sizeof(float)));
+    c->wsy_len = ny + np;
   }
   if (int rc = fz_mlp_forward_obs_device(mlp, npix, d_obs, d_norm, d_norm + nf, c->d_wsy, stream)) return rc;
+  float* cb = c->d_wsy + ny;   // CONTRACT(base), np floats behind the network's outputs
+  k_ws_contract<<<1, 32, 0, s>>>(c->nz, c->rf, c->d_coef, d_base, cb);
   k_ws_expand<<<npix, 128, np * sizeof(float), s>>>(npix, c->nz, c->rf, c->d_coef, c->d_wsy, d_norm + 2 * nf,
-                                                    d_norm + 2 * nf + np, d_base, d_models);
+                                                    d_norm + 2 * nf + np, d_base, cb, d_models);
   return cuda_fail(cudaGetLastError());
 }
 
