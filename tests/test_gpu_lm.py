@@ -318,6 +318,38 @@ def test_deployable_rule_accepts_or_retraces_plain_lm(fz, orc):
     np.testing.assert_array_equal(m[~acc], m_pl[~acc])
 
 
+def test_device_loop_equals_host_loop(fz, orc):
+    """fz_invert_device runs its iterations as one device-driven CUDA graph
+    loop (a WHILE node ended by k_lm_ctl, no compaction); with per-kernel
+    profiling on, the host-driven loop runs instead (a graph per pool state,
+    compaction of the occupied slots).  The same pixels through both: models,
+    chi2, iterations and status equal bit for bit -- plain LM and the
+    NN-warm rule's restarts, 64 pixels through 24 slots."""
+    from firtez_dz_b200 import warmstart as ws
+    nz, npix = 48, 64
+    lines, reg, g, ctx = _ctx(fz, orc, nz)
+    true = fz.atmos.make_columns(npix, nz, seed=37)
+    obs, true_he, _ = ctx.forward(true, hydrostatic=True)
+    obs = obs + np.random.default_rng(8).normal(0.0, 1e-3, obs.shape)
+    ctx.rf_nodes(lmcase.NODES)
+    base = ws.default_models(npix, nz)
+    init = lmcase.initial_guess(true_he, seed=4)
+    init[::3, 0] += 500.0
+    fb = np.ascontiguousarray(base[0])
+    cases = [(base, fz.LMOpts(maxsteps=5, maxit=30, isigma=1e-3, dchi2=1e-3, slots=24), None),
+             (init, fz.LMOpts(maxsteps=5, maxit=30, isigma=1e-3, dchi2=1e-3, slots=24, fallback=1.0,
+                              fallback_model=fb.ctypes.data, fallback_steps=-1, fallback_free=True),
+              np.full(npix, 300.0))]
+    for start, opts, target in cases:
+        dev = ctx.invert(obs, start, hydrostatic=True, opts=opts, target=target)
+        ctx.profile(True)
+        host = ctx.invert(obs, start, hydrostatic=True, opts=opts, target=target)
+        ctx.profile(False)
+        ctx.profile_read()
+        for a, b in zip(dev, host):
+            np.testing.assert_array_equal(a, b)
+
+
 @pytest.mark.parametrize("nx,ny,nz", [(7, 6, 9), (3, 8, 4), (5, 5, 16)])
 def test_smoothing_b_matches_oracle(fz, orc, nx, ny, nz):
     """SMOOTHING_B (the 1-2-1 smoothing of INITIALIZE_CYCLE) on the device
