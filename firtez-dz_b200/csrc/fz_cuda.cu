@@ -3874,7 +3874,7 @@ int fz_invert_device(fz_ctx* c, int npix, const double* d_obs, const float* d_in
     } else {
       {
         ProfScope ps(c, 7, s, n);
-        k_lm_normal<<<(n + 3) / 4, 128, 0, s>>>(C, L, d_w);
+        k_lm_normal<<<(n + 3) / 4, 128, 0, s>>>(C, L, d_w, L.rf_list, &c->d_q->rf_count);
       }
       {
         ProfScope ps(c, 8, s, n);
@@ -3948,7 +3948,7 @@ int fz_invert_device(fz_ctx* c, int npix, const double* d_obs, const float* d_in
       r = launch_rf_stage(c, S, hydrostatic, L.syn, L.jacb, L.mcur, L.status, s, L.rf_list, &c->d_q->rf_count);
     }
     if (!r) {
-      k_lm_normal<<<(S + 3) / 4, 128, 0, s>>>(C, L, d_w);
+      k_lm_normal<<<(S + 3) / 4, 128, 0, s>>>(C, L, d_w, L.rf_list, &c->d_q->rf_count);
       k_lm_solve<<<(S + 3) / 4, 128, 0, s>>>(C, L);
       k_lm_update<<<S, 128, usm, s>>>(C, L, c->d_coef64);
       k_lm_scan<<<1, 1024, 0, s>>>(S, L.pix, c->d_dest, c->d_q, c->d_act);

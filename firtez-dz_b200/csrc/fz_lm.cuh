@@ -67,7 +67,7 @@ __device__ __forceinline__ double lm_hss(const LMConf& C, int j, int i) {
 struct LMSlots {
   int S;
   int* pix;          // pixel index, LM_PAD if empty
-  int* skip;         // LM_SKIP if the slot was refilled in this iteration
+  int* skip;         // LM_SKIP if the slot was refilled or restarted in this iteration or has no accepted model yet
   int* restarted;    // 0, or 1 + the first attempt's iterations once the pixel restarted from the fallback model
   int* iter;
   double* st;        // 5 per slot: chicur, chibest, lambda, steps, precyc
@@ -192,7 +192,12 @@ __device__ void lm_load_slot(const LMConf& C, const LMSlots& Sl, int s, int p, c
                              const float* __restrict__ init_all) {
   const int nm = 13 * C.nz;
   if (p < C.npix) {
-    for (int i = threadIdx.x; i < nm; i += blockDim.x) Sl.mcur[(size_t)s * nm + i] = init_all[(size_t)p * nm + i];
+    // the best model starts as the initial one (INITIALIZE_CYCLE)
+    for (int i = threadIdx.x; i < nm; i += blockDim.x) {
+      const float v = init_all[(size_t)p * nm + i];
+      Sl.mcur[(size_t)s * nm + i] = v;
+      Sl.mbest[(size_t)s * nm + i] = v;
+    }
     for (int i = threadIdx.x; i < C.nfreq; i += blockDim.x)
       Sl.obs[(size_t)s * C.nfreq + i] = obs_all[(size_t)p * C.nfreq + i];
     if (threadIdx.x == 0) {
@@ -329,7 +334,8 @@ __global__ void __launch_bounds__(256) k_lm_accept(LMConf C, LMSlots Sl, LMQueue
     // the search ended above fallback x its goal: start once more from the
     // fallback model (INITIALIZE_CYCLE's state), the goal kept
     float* mc = Sl.mcur + (size_t)s * nm;
-    for (int i = threadIdx.x; i < nm; i += blockDim.x) mc[i] = C.fb_model[i];
+    float* mb = Sl.mbest + (size_t)s * nm;
+    for (int i = threadIdx.x; i < nm; i += blockDim.x) mc[i] = mb[i] = C.fb_model[i];
     if (threadIdx.x == 0) {
       if (C.global_stop) atomicAdd(&q->steps_sum, (unsigned long long)(-(long long)st[3]));
       st[0] = 1.0e29;
@@ -360,6 +366,14 @@ __global__ void __launch_bounds__(256) k_lm_accept(LMConf C, LMSlots Sl, LMQueue
     }
     __syncthreads();
     lm_load_slot(C, Sl, s, np_next, obs_all, init_all);
+    return;
+  }
+  if (st[1] >= 1.0e29) {
+    // no model of this attempt has been accepted yet (its first synthesis
+    // failed): there is no Jacobian to step from, so the initial model is
+    // tried again, each failure raising STEPS until the stop rule ends the
+    // pixel with its initial model and a non-zero status
+    if (threadIdx.x == 0) Sl.skip[s] = LM_SKIP;
     return;
   }
   // weighted residual of the best synthesis (:1027)
@@ -394,9 +408,20 @@ __device__ __forceinline__ void mma_bf16(float c[4], const unsigned a[4], const 
 // Per k-step of 16 frequencies a thread holds rows {grp, grp+8} x
 // frequencies {2t, 2t+1, 2t+8, 2t+9} of Jn^T: exactly its A fragment, and
 // (column grp of tile 0, column grp+8 of tile 1) its B fragments.
-__global__ void __launch_bounds__(128) k_lm_normal(LMConf C, LMSlots Sl, const double* __restrict__ w) {
+// With list, warp i serves slot list[i] for i < *nlist: the inversion passes
+// the accepted slots (rf_list).  H and g depend only on the best model's
+// Jacobian, synthesis and penalties, which change only on an accepted step;
+// a rejected trial leaves them as the last accepted step computed them, bit
+// for bit, and k_lm_solve reads them again with the new lambda.
+__global__ void __launch_bounds__(128) k_lm_normal(LMConf C, LMSlots Sl, const double* __restrict__ w,
+                                                   const int* __restrict__ list = nullptr,
+                                                   const int* __restrict__ nlist = nullptr) {
   const int lane = threadIdx.x & 31;
-  const int s = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  int s = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  if (list) {
+    if (s >= *nlist) return;
+    s = list[s];
+  }
   if (s >= Sl.S) return;
   if (Sl.pix[s] < 0 || Sl.skip[s]) return;
   const int nf = C.nfreq, np = C.np;
@@ -941,6 +966,13 @@ __global__ void __launch_bounds__(256) k_lm_compact(LMConf C, LMSlots A, LMSlots
   const float4* ja = reinterpret_cast<const float4*>(A.jacb + (size_t)s * C.np * nf);
   float4* jb = reinterpret_cast<float4*>(B.jacb + (size_t)d * C.np * nf);
   for (int i = threadIdx.x; i < C.np * nf / 4; i += blockDim.x) jb[i] = ja[i];
+  if (C.np <= LM_MAXNP) {
+    // the warp normal equations run on accepted steps only: H and g travel
+    // with the slot (the tensor-core ones are rebuilt every iteration)
+    const int np = C.np;
+    for (int i = threadIdx.x; i < np * np; i += blockDim.x) B.H[(size_t)d * np * np + i] = A.H[(size_t)s * np * np + i];
+    for (int i = threadIdx.x; i < np; i += blockDim.x) B.g[(size_t)d * np + i] = A.g[(size_t)s * np + i];
+  }
 }
 
 }  // namespace

@@ -350,6 +350,41 @@ def test_device_loop_equals_host_loop(fz, orc):
             np.testing.assert_array_equal(a, b)
 
 
+def test_failed_first_synthesis_keeps_initial_model(fz, orc):
+    """A pixel whose initial model cannot be synthesised (a non-finite
+    temperature) has no accepted model and so no Jacobian to step from: it
+    is tried again until STEPS passes maxsteps (maxsteps + 1 iterations) and
+    ends with its initial model, chi2 1e29 and a non-zero status.  The other
+    pixels of the field come out bit for bit as when inverted without it,
+    through the device-driven loop and the host-driven loop (whose
+    compaction carries each slot's normal equations along)."""
+    nz, npix = 48, 40
+    lines, reg, g, ctx = _ctx(fz, orc, nz)
+    true = fz.atmos.make_columns(npix, nz, seed=41)
+    obs, true_he, _ = ctx.forward(true, hydrostatic=True)
+    obs = obs + np.random.default_rng(9).normal(0.0, 1e-3, obs.shape)
+    ctx.rf_nodes(lmcase.NODES)
+    init = lmcase.initial_guess(true_he, seed=5)
+    bad = [3, 17, 30]
+    good = [i for i in range(npix) if i not in bad]
+    init_bad = init.copy()
+    init_bad[bad, 0, nz // 2] = np.nan
+    opts = fz.LMOpts(maxsteps=5, maxit=30, isigma=1e-3, dchi2=1e-3, slots=16)
+    ref = ctx.invert(obs[good], init[good], hydrostatic=True, opts=opts)
+    for prof in (False, True):
+        ctx.profile(prof)
+        mo, chi, it, st = ctx.invert(obs, init_bad, hydrostatic=True, opts=opts)
+        ctx.profile(False)
+        if prof:
+            ctx.profile_read()
+        for a, b in zip((mo, chi, it, st), ref):
+            np.testing.assert_array_equal(a[good], b)
+        assert np.all(st[bad] != 0)
+        assert np.all(chi[bad] == 1.0e29)
+        assert np.all(it[bad] == 6)
+        np.testing.assert_array_equal(mo[bad], init_bad[bad])
+
+
 @pytest.mark.parametrize("nx,ny,nz", [(7, 6, 9), (3, 8, 4), (5, 5, 16)])
 def test_smoothing_b_matches_oracle(fz, orc, nx, ny, nz):
     """SMOOTHING_B (the 1-2-1 smoothing of INITIALIZE_CYCLE) on the device
