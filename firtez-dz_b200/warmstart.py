@@ -208,6 +208,110 @@ class WarmStart:
         tt = torch.from_numpy(((t - self.tmu) / self.tsd).astype(np.float32)).cuda()
         return x, tt
 
+    def _basis(self, dev):
+        """Per free parameter, as FP64 tensors on dev: EXPAND (nj, nz), the
+        hat averages of CONTRACT (nz, nj) and the least-squares inverse of
+        EXPAND (nz, nj)."""
+        import torch
+        key = str(dev)
+        cache = getattr(self, "_basis_cache", {})
+        if key not in cache:
+            b = {}
+            for p, _ in self.params:
+                c = self.coefs[p]
+                b[p] = (torch.from_numpy(c.T.copy()).to(dev, torch.float64),
+                        torch.from_numpy(c / c.sum(axis=0)).to(dev, torch.float64),
+                        torch.from_numpy(np.linalg.pinv(c).T.copy()).to(dev, torch.float64))
+            cache[key] = b
+            self._basis_cache = cache
+        return cache[key]
+
+    def expand_nodes(self, nodes, base):
+        """Tensor form of expand(): nodes (n, nout) FP64, base one MODEL
+        (13, nz) float32 -> (n, 13, nz) float32 models, each free row
+        base + EXPAND(nodes - CONTRACT(base)) (on the tensors' device)."""
+        import torch
+        basis = self._basis(nodes.device)
+        m = base.expand(nodes.shape[0], -1, -1).clone()
+        j = 0
+        for p, row in self.params:
+            nj = self.nodes[p]
+            ct, cavg, _ = basis[p]
+            b = base[row].to(torch.float64)
+            m[:, row] = (b + (nodes[:, j:j + nj] - b @ cavg) @ ct).float()
+            j += nj
+        return m
+
+    def fit_nodes(self, models, base):
+        """Node values whose expansion on base (expand_nodes) reproduces the
+        free rows of models (n, 13, nz) best, in the least-squares sense:
+        CONTRACT(base) + EXPAND^+ (row - base row).  Exact (up to rounding)
+        for models that differ from base by an expansion, as the
+        inversion's models do."""
+        import torch
+        basis = self._basis(models.device)
+        out = torch.empty((models.shape[0], self.nout), dtype=torch.float64, device=models.device)
+        j = 0
+        for p, row in self.params:
+            nj = self.nodes[p]
+            _, cavg, pinv = basis[p]
+            b = base[row].to(torch.float64)
+            out[:, j:j + nj] = b @ cavg + (models[:, row].to(torch.float64) - b) @ pinv
+            j += nj
+        return out
+
+    def refine_targets(self, synth, x, t, opts, chunk=131072, stream=0):
+        """LM-refined training targets.  Each training pixel is inverted
+        (synth.invert_device with opts, hydrostatic) from the model of its
+        true node values on the default guess, and its target becomes the
+        node values whose expansion reproduces the inversion's best model
+        (fit_nodes).  The true node averages of an atmosphere are not its
+        best fit in the node space: the contraction averages away
+        stratification the lines see and the expansion puts it back smeared,
+        so their models sit well above the chi2 the inversion reaches next to
+        them.  A network trained on the refined values learns the map from
+        Stokes vectors to best-fit nodes, which is what a warm start needs.
+        x, t: the standardised device training set of make_training_set;
+        synth's node layout (rf_nodes) must be the network's.  The node
+        normalisation is recomputed.  Returns the new standardised targets
+        (device) and the inversion's statistics."""
+        import time
+        import torch
+        if self.tsd is None:
+            raise FzError("the network has no normalisation: make the training set first")
+        t0 = time.perf_counter()
+        dev = x.device
+        ntot = x.shape[0]
+        f64 = torch.float64
+        tsd = torch.from_numpy(np.ravel(self.tsd)).to(dev, f64)
+        tmu = torch.from_numpy(np.ravel(self.tmu)).to(dev, f64)
+        xsd, xmu = self.xsd.to(f64), self.xmu.to(f64)
+        base = torch.from_numpy(default_models(1, self.nz)[0]).to(dev)
+        refined = torch.empty((ntot, self.nout), dtype=f64, device=dev)
+        chis, its = [], []
+        for i in range(0, ntot, chunk):
+            n = min(chunk, ntot - i)
+            start = self.expand_nodes(t[i:i + n].to(f64) * tsd + tmu, base)
+            obs = (x[i:i + n].to(f64) * xsd + xmu).contiguous()
+            out = torch.empty_like(start)
+            chi = torch.empty(n, dtype=f64, device=dev)
+            it = torch.empty(n, dtype=torch.int32, device=dev)
+            st = torch.empty(n, dtype=torch.int32, device=dev)
+            synth.invert_device(n, obs.data_ptr(), start.data_ptr(), out.data_ptr(), chi.data_ptr(), it.data_ptr(),
+                                st.data_ptr(), hydrostatic=True, opts=opts, stream=stream)
+            torch.cuda.synchronize()
+            refined[i:i + n] = self.fit_nodes(out, base)
+            chis.append(chi)
+            its.append(it)
+        r = refined.cpu().numpy()
+        self.tmu = r.mean(axis=0, keepdims=True)
+        self.tsd = r.std(axis=0, keepdims=True) + 1e-12
+        tt = torch.from_numpy(((r - self.tmu) / self.tsd).astype(np.float32)).to(dev)
+        chi = torch.cat(chis)
+        info = {"pixels": int(ntot), "seconds": time.perf_counter() - t0,
+                "mean_iterations": float(torch.cat(its).float().mean()), "median_chi2": float(torch.median(chi))}
+        return tt, info
+
     def chi2_weights(self, synth, ncol=8192, seed=97, bmax=2500.0):
         """Loss weights under which the network's squared error approximates,
         to first order, the chi2 its prior costs: w_j = tsd_j^2 (J^T J)_jj

@@ -152,3 +152,57 @@ def test_warm_start_beats_default_guess(fz):
     mo_g, chi_g, it_g, st_g = ctx.invert(obs, fused, hydrostatic=True, opts=opts)
     assert np.all(st_f == 0)
     assert np.array_equal(chi_f, chi_g) and np.array_equal(it_f, it_g) and np.array_equal(mo_f, mo_g)
+
+
+def test_refined_targets(fz):
+    """WarmStart.refine_targets: each training pixel is inverted from the
+    model of its true node values and its target becomes the node values of
+    the inversion's best model.  Those nodes reproduce that model (their
+    expansion's chi2 is the inversion's best chi2, never above the true
+    nodes' chi2), and a network trained on them starts the held-out pixels
+    at a lower median chi2 than the same network trained on the true node
+    averages."""
+    import torch
+    from firtez_dz_b200 import warmstart as ws
+    nz, ntrain = 64, 131072
+    lines = fz.lines_parse(fz.atmos.line_database_text())
+    reg = fz.regions_from_lines_section(fz.atmos.lines_section(2), lines)
+    ctx = fz.Synthesis(lines, reg, nz=nz)
+    ctx.rf_nodes(lmcase.NODES)
+    one = fz.LMOpts(maxsteps=5, maxit=1, isigma=1e-3, dchi2=1e-3)
+    refine = fz.LMOpts(maxsteps=2, maxit=15, isigma=1e-3, dchi2=1e-3, slots=32768)
+    nets = {}
+    for kind in ("true", "refined"):
+        warm = ws.WarmStart(nz, lmcase.NODES, ctx.numw, seed=5)
+        x, t = warm.make_training_set(ctx, ntrain, seed=11, noise=1e-3)
+        if kind == "refined":
+            t_true = t[:256].double().cpu().numpy() * warm.tsd + warm.tmu
+            t, info = warm.refine_targets(ctx, x, t, refine)
+            assert info["pixels"] == ntrain and 1.0 <= info["mean_iterations"] <= 15.0
+            # the first 256 training pixels: the refined nodes' models against
+            # the true nodes' models on the same observations
+            obs = (x[:256].double() * warm.xsd.double() + warm.xmu.double()).cpu().numpy().reshape(256, 4, -1)
+            base = torch.from_numpy(ws.default_models(1, nz)[0])
+            t_ref = t[:256].double().cpu().numpy() * warm.tsd + warm.tmu
+            m_true = warm.expand_nodes(torch.from_numpy(t_true), base).numpy()
+            m_ref = warm.expand_nodes(torch.from_numpy(t_ref), base).numpy()
+            _, c_true, _, s1 = ctx.invert(obs, m_true, hydrostatic=True, opts=one)
+            _, c_ref, _, s2 = ctx.invert(obs, m_ref, hydrostatic=True, opts=one)
+            best_lm = ctx.invert(obs, m_true, hydrostatic=True, opts=refine)[1]
+            assert np.all(s1 == 0) and np.all(s2 == 0)
+            # the targets are kept standardised in float32, so the refined
+            # nodes reproduce the best model to that rounding
+            q = np.quantile(c_ref / c_true, [0.5, 0.9, 0.99, 1.0])
+            assert q[2] <= 1.0 + 1e-4, q
+            assert np.median(np.abs(c_ref / best_lm - 1.0)) < 1e-3, np.quantile(c_ref / best_lm, [0.01, 0.5, 0.99])
+        warm.fit(x, t, epochs=6, batch=1024, lr=1e-3)
+        del x
+        nets[kind] = warm
+    npix = 512
+    true = fz.atmos.make_columns(npix, nz, seed=424243)
+    obs, _, _ = ctx.forward(true, hydrostatic=True)
+    obs = obs + np.random.default_rng(19).normal(0.0, 1e-3, obs.shape)
+    med = {k: np.median(ctx.invert(obs, w.initial_models(obs), hydrostatic=True, opts=one)[1])
+           for k, w in nets.items()}
+    assert med["refined"] < med["true"], med
+
