@@ -254,6 +254,9 @@ CALIB_SEED = 909090
 C5_SEED = 5050
 
 
+SAHA_MAX_COLS = 1024   # batches up to this size run the chain on k_saha's precomputed Saha factors
+
+
 def probe_kernels(fz, lines, reg, nz, n):
     """One synthesis and one node-Jacobian call (fz_forward_device,
     fz_forward_rf_device) on n seeded columns of the workload, twice: every
@@ -308,6 +311,14 @@ def flops_table(csv_path, ncol, nz, numw, out_path):
                        "counted as 2) on --probe-kernels %d: %d seeded columns, NZ %d, NUMW %d, hydrostatic, nodes "
                        "T5 Bx2 By2 Bz2 vz2; bench.py multiplies by the columns of a launch" % (ncol, ncol, nz, numw),
            "kernels": kern}
+    if ncol <= SAHA_MAX_COLS:
+        # a small batch runs the chain on precomputed Saha factors: its two
+        # kernels join the table of the full-batch probe
+        small = {"k_saha": kern["k_saha"], "k_chain_pre": kern["k_chain"]}
+        doc = json.load(open(out_path)) if os.path.exists(out_path) else {"_comment": "", "kernels": {}}
+        doc["kernels"].update(small)
+        doc["_comment_small"] = ("k_saha and k_chain_pre (the chain of a batch of at most %d columns on precomputed "
+                                 "Saha factors) from --probe-kernels %d" % (SAHA_MAX_COLS, ncol))
     with open(out_path, "w") as f:
         json.dump(doc, f, indent=1)
     print(json.dumps(doc))

@@ -34,7 +34,8 @@ TEM, PG, RHO, PEL, MW, BX, BY, BZ, VX, VY, VZ, TAU5, ZZ = range(13)
 
 FZ_OK, FZ_CHEM_NOCONV, FZ_NAN = 0, 1, 2
 KERNELS = ("k_chain", "k_opac", "k_synth", "k_opac_rf", "k_synth_rf", "k_lm_fill", "k_lm_accept", "k_lm_normal",
-           "k_lm_solve", "k_lm_update", "k_chemder", "k_rf_prop", "k_lsf")
+           "k_lm_solve", "k_lm_update", "k_chemder", "k_rf_prop", "k_lsf", "k_saha",
+           "k_chain_pre")
 
 # free-parameter indices of the reference (atm_param.f90 order, 1-based) that
 # carry response functions

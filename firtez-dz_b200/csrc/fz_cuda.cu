@@ -79,6 +79,14 @@ __device__ __forceinline__ void copy_to_shared(T* dst, const T* src) {
 }
 
 // ----------------------------------------------------------------- k_chain
+// The temperature at the midpoint of an RK4 step of dz from height t0 (the
+// linear interpolation of RK4_LOG, src/hydrostatic_tools.f90:377), written
+// once for k_chain and k_saha so both round alike.
+__device__ __forceinline__ double chain_tmid(double t0, double dz, double tm0, double tm1) {
+  const double it1 = t0 + dz / 2.0;
+  return tm0 / dz * (t0 + dz - it1) + tm1 / dz * (it1 - t0);
+}
+
 // One warp per column walks the heights sequentially: the GET_RHO warm-start
 // chain (NELEC of one call seeds the next, src/forward.f90:914) and, in
 // hydrostatic mode, the RK4 integration of ln Pg from the top
@@ -91,23 +99,40 @@ __device__ __forceinline__ void copy_to_shared(T* dst, const T* src) {
 // the warp instructions).  At most 128 registers a thread (four blocks, 16
 // warps per SM): the chain is bound by dependent FP64 latency, so resident
 // warps count more than the few spilled values.
-template <bool HE, int L>
+//
+// PRE: the Saha factors of every temperature sample come precomputed from
+// k_saha (rows sa of the columns [c0, c0 + cn) of the list), and the chain
+// keeps only what is sequential: the GET_RHO iterations and the RK4 steps --
+// half the latency of a column's chain, the form for small batches (an
+// inversion's tail); on full batches the Saha work fills the stalls of the
+// GET_RHO iterations and the plain form is faster.  gate > 0: run only when
+// the column count is at most gate; gate < 0: only when it is above -gate (a
+// captured launch over a device-side count takes the form that suits it).
+template <bool HE, int L, bool PRE>
 __global__ void __launch_bounds__(128, 4) k_chain(const Consts* __restrict__ Kg, const PFTable* __restrict__ tb, int ncol,
                                                int nz, const float* model, float* mout, double2* __restrict__ chem,
                                                int* __restrict__ status, const int* __restrict__ list = nullptr,
-                                               const int* __restrict__ nlist = nullptr) {
+                                               const int* __restrict__ nlist = nullptr,
+                                               const double2* __restrict__ sa = nullptr, int c0 = 0, int cn = 0,
+                                               int gate = 0) {
   constexpr int NS = WarpSahaT<L>::NS;
   // listed columns (list[0, *nlist) of the ncol slots): a CTA past the end
   // of the list leaves before any work
   const int count = list ? *nlist : ncol;
-  if ((int)((blockIdx.x * (size_t)blockDim.x) / L) >= count) return;
+  if ((gate > 0 && count > gate) || (gate < 0 && count <= -gate)) return;
+  const int end = PRE ? min(count, c0 + cn) : count;
+  const int first = PRE ? c0 : 0;
+  if (first + (int)((blockIdx.x * (size_t)blockDim.x) / L) >= end) return;
   __shared__ Consts K;
   copy_to_shared(&K, Kg);
   __syncthreads();
   const int lane = threadIdx.x & (L - 1);
-  const int g = (int)((blockIdx.x * (size_t)blockDim.x + threadIdx.x) / L);
-  if (g >= count) return;
+  const int g = first + (int)((blockIdx.x * (size_t)blockDim.x + threadIdx.x) / L);
+  if (g >= end) return;
   const int col = list ? list[g] : g;
+  const int nsamp = HE ? 2 * nz - 1 : nz;
+  const double2* rows = PRE ? sa + (size_t)(g - first) * nsamp * 96 : nullptr;
+  const unsigned hyd = saha_hyd<L>(K, lane);
   const float* m = model + (size_t)col * 13 * nz;
   float* mo = mout + (size_t)col * 13 * nz;
   double2* ch = chem + (size_t)col * nz;
@@ -122,7 +147,10 @@ __global__ void __launch_bounds__(128, 4) k_chain(const Consts* __restrict__ Kg,
     double nelec = 0.0;
     WarpSahaT<L> w;
     for (int k = 0; k < nz; ++k) {
-      saha_prepare(w, (double)mget(m, nz, 0, k), K, tb, lane);
+      if (PRE)
+        saha_load(w, (double)mget(m, nz, 0, k), hyd, rows + (size_t)k * 96, lane);
+      else
+        saha_prepare(w, (double)mget(m, nz, 0, k), K, tb, lane);
       const RhoOut r = get_rho_warp(w, ab, (double)mget(m, nz, 1, k), nelec, K, lane);
       st |= r.status;
       if (lane == 0) {
@@ -141,7 +169,10 @@ __global__ void __launch_bounds__(128, 4) k_chain(const Consts* __restrict__ Kg,
     // stages need T(k+1) (stage 1), the linear midpoint (stages 2, 3) and
     // T(k) (stage 4 and the final GET_RHO), and T(k) is the next step's T(k+1).
     WarpSahaT<L> w;
-    saha_prepare(w, (double)mget(m, nz, 0, top), K, tb, lane);
+    if (PRE)
+      saha_load(w, (double)mget(m, nz, 0, top), hyd, rows, lane);
+    else
+      saha_prepare(w, (double)mget(m, nz, 0, top), K, tb, lane);
     {
       const RhoOut r = get_rho_warp(w, ab, exp(u0), nelec, K, lane);
       st |= r.status;
@@ -158,13 +189,18 @@ __global__ void __launch_bounds__(128, 4) k_chain(const Consts* __restrict__ Kg,
       const double dz = ((double)mget(m, nz, 12, k) - (double)mget(m, nz, 12, k + 1)) * 1000.0 * 100.0;
       const double t1 = t0 + dz;
       const double tm0 = (double)mget(m, nz, 0, k + 1), tm1 = (double)mget(m, nz, 0, k);
-      const double it1 = t0 + dz / 2.0;
-      const double tmid = tm0 / dz * (t0 + dz - it1) + tm1 / dz * (it1 - t0);
+      const double tmid = chain_tmid(t0, dz, tm0, tm1);
+      const double2* srow = PRE ? rows + (size_t)(2 * (nz - 2 - k) + 1) * 96 : nullptr;   // the midpoint's row, then T(k)'s
       double kk[4] = {0.0, 0.0, 0.0, 0.0};
       double u1 = 0.0;
 #pragma unroll 1
       for (int stg = 0; stg < 5; ++stg) {
-        if (stg == 1 || stg == 3) saha_prepare(w, stg == 1 ? tmid : tm1, K, tb, lane);
+        if (stg == 1 || stg == 3) {
+          if (PRE)
+            saha_load(w, stg == 1 ? tmid : tm1, hyd, stg == 1 ? srow : srow + 96, lane);
+          else
+            saha_prepare(w, stg == 1 ? tmid : tm1, K, tb, lane);
+        }
         const double tem = stg == 0 ? tm0 : (stg < 3 ? tmid : tm1);
         const double y = stg == 0 ? u0 : (stg == 1 ? u0 + kk[0] / 2.0 : (stg == 2 ? u0 + kk[1] / 2.0 : (stg == 3 ? u0 + kk[2] : u1)));
         const RhoOut q = get_rho_warp(w, ab, exp(y), nelec, K, lane);
@@ -191,6 +227,86 @@ __global__ void __launch_bounds__(128, 4) k_chain(const Consts* __restrict__ Kg,
     }
   }
   if (lane == 0 && status) status[col] = st;
+}
+
+// ------------------------------------------------------------------ k_saha
+// The Saha factors of every temperature sample of k_chain's integration, for
+// the listed columns [c0, c0 + cn): the samples are the model's T at each
+// height and, with HE, the RK4 midpoint temperature of each step --
+// functions of the model alone -- so this half of the chemistry's FP64 work
+// leaves the sequential chain and runs with every (sample, element slot) in
+// parallel, one CTA per column.  Row s of the i-th column of the chunk:
+// sa[(i * nsamp + s) * 96 + slot] = (a1, a2) of the slot's element; samples
+// (HE) 0 = T(top), 2j+1 = the midpoint of step j (height nz-2-j) and 2j+2 =
+// T(nz-2-j); without HE, s = T(s).  A warp takes one sample at a time, lane
+// l the slots l, l + 32 and l + 64 (its elements fixed for the whole
+// column, so their table lines stay in L1); gridDim.y CTAs share a column's
+// samples (small batches: latency).  gate > 0: run only when the column
+// count is at most gate.
+__host__ __device__ inline size_t saha_smem(int nz) {
+  return (size_t)(2 * nz - 1) * (sizeof(double) + sizeof(SahaT)) + (size_t)2 * nz * sizeof(double);
+}
+
+template <bool HE>
+__global__ void __launch_bounds__(256) k_saha(const Consts* __restrict__ Kg, const PFTable* __restrict__ tb,
+                                              int ncol, int nz, const float* __restrict__ model,
+                                              double2* __restrict__ sa, int c0, int cn,
+                                              const int* __restrict__ list, const int* __restrict__ nlist,
+                                              int gate) {
+  extern __shared__ double sm_saha[];
+  __shared__ Consts K;
+  const int count = list ? *nlist : ncol;
+  if (gate > 0 && count > gate) return;
+  const int g = c0 + (int)blockIdx.x;
+  if ((int)blockIdx.x >= cn || g >= count) return;
+  copy_to_shared(&K, Kg);
+  const int col = list ? list[g] : g;
+  const float* m = model + (size_t)col * 13 * nz;
+  const int nsamp = HE ? 2 * nz - 1 : nz;
+  double* ts = sm_saha;                                        // the samples' temperatures
+  SahaT* tt = reinterpret_cast<SahaT*>(sm_saha + nsamp);       // and their shared terms
+  double* dzs = sm_saha + nsamp + nsamp * (sizeof(SahaT) / sizeof(double));   // HE: dz of step j
+  double* t0s = dzs + nz;                                                     // and its start height
+  if (HE) {
+    const int top = nz - 1;
+    for (int j = threadIdx.x; j < nz - 1; j += blockDim.x) {
+      const int k = nz - 2 - j;
+      dzs[j] = ((double)mget(m, nz, 12, k) - (double)mget(m, nz, 12, k + 1)) * 1000.0 * 100.0;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {   // the integration's own running height, added in its order
+      double t0 = (double)mget(m, nz, 12, top) * 1000.0 * 100.0;
+      for (int j = 0; j < nz - 1; ++j) {
+        t0s[j] = t0;
+        t0 = t0 + dzs[j];
+      }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) ts[0] = (double)mget(m, nz, 0, top);
+    for (int j = threadIdx.x; j < nz - 1; j += blockDim.x) {
+      const int k = nz - 2 - j;
+      const double tm0 = (double)mget(m, nz, 0, k + 1), tm1 = (double)mget(m, nz, 0, k);
+      ts[2 * j + 1] = chain_tmid(t0s[j], dzs[j], tm0, tm1);
+      ts[2 * j + 2] = tm1;
+    }
+  } else {
+    for (int k = threadIdx.x; k < nz; k += blockDim.x) ts[k] = (double)mget(m, nz, 0, k);
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < nsamp; i += blockDim.x) tt[i] = saha_t(ts[i], K);
+  __syncthreads();
+  const int lane = threadIdx.x & 31;
+  const int e0 = K.lane_elem[lane], e1 = K.lane_elem[lane + 32], e2 = K.lane_elem[lane + 64];
+  double2* out = sa + (size_t)blockIdx.x * nsamp * 96;
+  const int wstride = (blockDim.x >> 5) * gridDim.y;
+  for (int smp = (threadIdx.x >> 5) + blockIdx.y * (blockDim.x >> 5); smp < nsamp; smp += wstride) {
+    const double T = ts[smp];
+    const SahaT t = tt[smp];
+    double2* o = out + (size_t)smp * 96;
+    o[lane] = saha_elem<true>(e0, T, t, K, tb);
+    o[lane + 32] = saha_elem<false>(e1, T, t, K, tb);
+    o[lane + 64] = saha_elem<false>(e2, T, t, K, tb);
+  }
 }
 
 // HE anchored at the height of least |log tau5| of the input model
@@ -1674,7 +1790,7 @@ __global__ void __launch_bounds__(256) k_lsf(LsfConf L, long long nrows, int row
   }
 }
 
-constexpr int NKERN = 13;   // k_chain, k_opac, k_synth, k_opac_rf, k_synth_rf, k_lm_fill, k_lm_accept, k_lm_normal, k_lm_solve, k_lm_update, k_chemder, k_rf_prop, k_lsf
+constexpr int NKERN = 15;   // k_chain, k_opac, k_synth, k_opac_rf, k_synth_rf, k_lm_fill, k_lm_accept, k_lm_normal, k_lm_solve, k_lm_update, k_chemder, k_rf_prop, k_lsf, k_saha, k_chain_pre
 
 struct fz_ctx {
   int device = 0;
@@ -1711,6 +1827,8 @@ struct fz_ctx {
   // scratch (grown on demand): per (column, height) nH, ne and the opacity slab
   float* d_slab = nullptr;
   double2* d_chem = nullptr;
+  double2* d_saha = nullptr;   // k_saha's rows of a chunk of columns
+  size_t saha_bytes = 0;
   size_t scratch_cols = 0;
   // staging for the host-buffer API
   float* d_model = nullptr;
@@ -1798,16 +1916,38 @@ int cuda_fail(cudaError_t e) {
     if (_rc) return _rc;                      \
   } while (0)
 
+// k_chain takes precomputed Saha factors (k_saha) for batches of at most
+// SAHA_MAX_COLS columns: the rows of that many columns.
+constexpr int SAHA_MAX_COLS = 1024;
+size_t saha_row_bytes(const fz_ctx* c) { return (size_t)(2 * c->nz - 1) * 96 * sizeof(double2); }
+int saha_chunk_cols(int ncol) { return std::min(ncol, SAHA_MAX_COLS); }
+
 int ensure_scratch(fz_ctx* c, int ncol) {
-  if ((size_t)ncol <= c->scratch_cols) return 0;
-  cudaFree(c->d_slab);
-  cudaFree(c->d_chem);
-  c->d_slab = nullptr;
-  c->d_chem = nullptr;
-  c->scratch_cols = 0;
-  FZ_CK(cudaMalloc(&c->d_slab, (size_t)ncol * c->nz * c->sw * sizeof(float)));
-  FZ_CK(cudaMalloc(&c->d_chem, (size_t)ncol * c->nz * sizeof(double2)));
-  c->scratch_cols = ncol;
+  if ((size_t)ncol > c->scratch_cols) {
+    cudaFree(c->d_slab);
+    cudaFree(c->d_chem);
+    c->d_slab = nullptr;
+    c->d_chem = nullptr;
+    c->scratch_cols = 0;
+    FZ_CK(cudaMalloc(&c->d_slab, (size_t)ncol * c->nz * c->sw * sizeof(float)));
+    FZ_CK(cudaMalloc(&c->d_chem, (size_t)ncol * c->nz * sizeof(double2)));
+    c->scratch_cols = ncol;
+  }
+  const size_t sb = (size_t)saha_chunk_cols(ncol) * saha_row_bytes(c);
+  if (sb > c->saha_bytes) {
+    cudaFree(c->d_saha);
+    c->d_saha = nullptr;
+    c->saha_bytes = 0;
+    FZ_CK(cudaMalloc(&c->d_saha, sb));
+    c->saha_bytes = sb;
+    // k_saha's shared memory (the samples' temperatures and terms) above the
+    // default 48 KB for tall columns; set here, before any stream capture
+    const size_t ssm = saha_smem(c->nz);
+    if (ssm > 48 * 1024 && ssm <= 200 * 1024) {
+      FZ_CK(cudaFuncSetAttribute(k_saha<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ssm));
+      FZ_CK(cudaFuncSetAttribute(k_saha<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ssm));
+    }
+  }
   return 0;
 }
 
@@ -1854,31 +1994,69 @@ struct ProfScope {
 // scratch of the batch, the context's own buffer when null.
 void launch_k_chain(fz_ctx* c, int ncol, const float* d_model, float* d_mout, int* d_status, int hydrostatic, int wpb,
                     int lanes, cudaStream_t s, double2* chem = nullptr, const int* list = nullptr,
-                    const int* nlist = nullptr) {
+                    const int* nlist = nullptr, bool pre = true) {
   if (!chem) chem = c->d_chem;
   if (hydrostatic == 2) {   // HE anchored at log tau5 ~ 0 (HYDRO_TOP off)
+    ProfScope ps(c, 0, s, ncol);
     const dim3 g((unsigned)(((size_t)ncol * 32 + 127) / 128));
     k_chain_med<<<g, 128, 0, s>>>(c->d_consts, c->d_pf, ncol, c->nz, d_model, d_mout, chem, d_status);
     return;
   }
   if (lanes != 16 && lanes != 32) lanes = ncol >= 16 * c->nsm ? 16 : 32;
-  const size_t threads = (size_t)ncol * lanes;
-  const dim3 gc((unsigned)((threads + wpb * 32 - 1) / (wpb * 32)));
-  if (lanes == 16) {
-    if (hydrostatic)
-      k_chain<true, 16><<<gc, wpb * 32, 0, s>>>(c->d_consts, c->d_pf, ncol, c->nz, d_model, d_mout, chem,
-                                                d_status, list, nlist);
-    else
-      k_chain<false, 16><<<gc, wpb * 32, 0, s>>>(c->d_consts, c->d_pf, ncol, c->nz, d_model, d_mout, chem,
-                                                 d_status, list, nlist);
-  } else {
-    if (hydrostatic)
-      k_chain<true, 32><<<gc, wpb * 32, 0, s>>>(c->d_consts, c->d_pf, ncol, c->nz, d_model, d_mout, chem,
-                                                d_status, list, nlist);
-    else
-      k_chain<false, 32><<<gc, wpb * 32, 0, s>>>(c->d_consts, c->d_pf, ncol, c->nz, d_model, d_mout, chem,
-                                                 d_status, list, nlist);
+  const int nsamp = hydrostatic ? 2 * c->nz - 1 : c->nz;
+  // the precomputed form when the context's rows hold the batch's first
+  // SAHA_MAX_COLS columns and k_saha's shared memory fits; a batch of known
+  // size takes one form, a listed batch (count on the device) launches both,
+  // each gated by the count
+  const int per = saha_chunk_cols(ncol);
+  const size_t ssm = saha_smem(c->nz);
+  pre = pre && c->d_saha && (size_t)per * nsamp * 96 * sizeof(double2) <= c->saha_bytes && ssm <= 200 * 1024;
+  const bool plain = !pre || list || ncol > SAHA_MAX_COLS;
+  const bool fast = pre && (list || ncol <= SAHA_MAX_COLS);
+  const int gate = list ? SAHA_MAX_COLS : 0;
+  if (plain) {
+    ProfScope ps(c, 0, s, ncol);
+    const size_t threads = (size_t)ncol * lanes;
+    const dim3 gc((unsigned)((threads + wpb * 32 - 1) / (wpb * 32)));
+    const int pg = fast ? -gate : 0;
+    if (lanes == 16) {
+      if (hydrostatic)
+        k_chain<true, 16, false><<<gc, wpb * 32, 0, s>>>(c->d_consts, c->d_pf, ncol, c->nz, d_model, d_mout, chem,
+                                                         d_status, list, nlist, nullptr, 0, 0, pg);
+      else
+        k_chain<false, 16, false><<<gc, wpb * 32, 0, s>>>(c->d_consts, c->d_pf, ncol, c->nz, d_model, d_mout, chem,
+                                                          d_status, list, nlist, nullptr, 0, 0, pg);
+    } else {
+      if (hydrostatic)
+        k_chain<true, 32, false><<<gc, wpb * 32, 0, s>>>(c->d_consts, c->d_pf, ncol, c->nz, d_model, d_mout, chem,
+                                                         d_status, list, nlist, nullptr, 0, 0, pg);
+      else
+        k_chain<false, 32, false><<<gc, wpb * 32, 0, s>>>(c->d_consts, c->d_pf, ncol, c->nz, d_model, d_mout, chem,
+                                                          d_status, list, nlist, nullptr, 0, 0, pg);
+    }
   }
+  if (!fast) return;
+  // the small-batch form: every column's Saha rows (split over a few CTAs a
+  // column, for latency), then the chains on them, always 32 lanes a column
+  const int cn = per;
+  {
+    ProfScope ps(c, 13, s, list ? 0 : cn);
+    const dim3 gs((unsigned)cn, cn <= c->nsm ? 4u : 1u);
+    if (hydrostatic)
+      k_saha<true><<<gs, 256, ssm, s>>>(c->d_consts, c->d_pf, ncol, c->nz, d_model, c->d_saha, 0, cn, list, nlist,
+                                        gate);
+    else
+      k_saha<false><<<gs, 256, ssm, s>>>(c->d_consts, c->d_pf, ncol, c->nz, d_model, c->d_saha, 0, cn, list, nlist,
+                                         gate);
+  }
+  ProfScope ps(c, 14, s, list ? 0 : cn);
+  const dim3 gc((unsigned)(((size_t)cn * 32 + wpb * 32 - 1) / (wpb * 32)));
+  if (hydrostatic)
+    k_chain<true, 32, true><<<gc, wpb * 32, 0, s>>>(c->d_consts, c->d_pf, ncol, c->nz, d_model, d_mout, chem,
+                                                    d_status, list, nlist, c->d_saha, 0, cn, gate);
+  else
+    k_chain<false, 32, true><<<gc, wpb * 32, 0, s>>>(c->d_consts, c->d_pf, ncol, c->nz, d_model, d_mout, chem,
+                                                     d_status, list, nlist, c->d_saha, 0, cn, gate);
 }
 
 // The LSF pass over nrows rows of numw values (no-op without a valid LSF).
@@ -1912,11 +2090,8 @@ int launch_forward(fz_ctx* c, int ncol, const float* d_model, int hydrostatic, d
   int rc = ensure_scratch(c, ncol);
   if (rc) return rc;
   if (d_status) FZ_CK(cudaMemsetAsync(d_status, 0, ncol * sizeof(int), s));
-  {
-    ProfScope ps(c, 0, s, ncol);
-    launch_k_chain(c, ncol, d_model, d_mout, d_status, hydrostatic, c->tune.chain_warps, c->tune.chain_lanes, s,
-                   nullptr, list, nlist);
-  }
+  launch_k_chain(c, ncol, d_model, d_mout, d_status, hydrostatic, c->tune.chain_warps, c->tune.chain_lanes, s,
+                 nullptr, list, nlist);
   FZ_CK(cudaGetLastError());
   {
     ProfScope ps(c, 1, s, ncol);
@@ -2135,10 +2310,7 @@ int launch_forward_rf(fz_ctx* c, int ncol, const float* d_model, int hydrostatic
   if (rc) return rc;
   const int swr = rf_w(c->nreg, c->nlu);
   if (d_status) FZ_CK(cudaMemsetAsync(d_status, 0, ncol * sizeof(int), s));
-  {
-    ProfScope ps(c, 0, s, ncol);
-    launch_chain(c, ncol, d_model, d_mout, d_status, hydrostatic, c->tune.chain_warps, s);
-  }
+  launch_chain(c, ncol, d_model, d_mout, d_status, hydrostatic, c->tune.chain_warps, s);
   FZ_CK(cudaGetLastError());
   if (!full) return launch_rf_stage(c, ncol, hydrostatic, d_syn, d_jac, d_mout, d_status, s);
   {
@@ -3595,6 +3767,7 @@ int fz_destroy(fz_ctx* c) {
   cudaFree(c->d_gain);
   cudaFree(c->d_slab);
   cudaFree(c->d_chem);
+  cudaFree(c->d_saha);
   cudaFree(c->d_model);
   cudaFree(c->d_syn);
   cudaFree(c->d_status);
@@ -4748,7 +4921,7 @@ int fz_forward_device_static(fz_ctx* c, int ncol, const float* d_model, int hydr
   // the chemistry chain with the context's launch shape (tuned or default),
   // so that both entry points run the same schedule and agree bit for bit
   launch_k_chain(c, ncol, d_model, d_model_out, d_status, hydrostatic, c->tune.chain_warps, c->tune.chain_lanes, s,
-                 chem);
+                 chem, nullptr, nullptr, false);
   FZ_CK(cudaGetLastError());
   const size_t total = (size_t)ncol * c->nz;
   const int blocks = (int)std::min<size_t>((total + 255) / 256, (size_t)c->nsm * 16);

@@ -130,7 +130,7 @@ __device__ __forceinline__ double rcp_d(double y) {
 // half-warp, two columns per warp), lanes over the elements: the element of
 // lane l in slot j is lane_elem[L*j + l], NS = 96 / L slots per lane.  The
 // exponential-form elements come first in lane_elem, so only the first
-// 23 / L + 1 slots evaluate an exponential.
+// 32 / L slots of a lane (the first 32 of the 96) evaluate an exponential.
 template <int L>
 struct WarpSahaT {
   static constexpr int NS = 96 / L;
@@ -146,13 +146,59 @@ __device__ __forceinline__ double clamp650(double e) {
   return e;
 }
 
+// The temperature terms the Saha factors of every element share: 1/T,
+// T^(-3/2) x CSAHA1 and the partition functions' variables (T, T/1000,
+// log(5040/T)).
+struct SahaT {
+  double it, lamelec, var[3];
+};
+
+__device__ __forceinline__ SahaT saha_t(double T, const Consts& K) {
+  SahaT t;
+  t.it = rcp_d(T);
+  t.lamelec = K.csaha1 * (t.it * sqrt(t.it));   // T^(-3/2)
+  t.var[0] = T;
+  t.var[1] = 1.0e-3 * T;
+  t.var[2] = log(5040.0 / T);
+  return t;
+}
+
+// The Saha factors (a1, a2) of element el (-1: an idle slot, (0, 0)) at
+// temperature T (SHORT_PRE_ION_CALC_TEMPRHO, src/chemical_equilibrium.f90:
+// 1601-1652).  EXPF: the element's partition-function pieces may hold an
+// exponential (every such element sits in the first 32 slots).
+template <bool EXPF>
+__device__ __forceinline__ double2 saha_elem(int el, double T, const SahaT& t, const Consts& K,
+                                             const PFTable* __restrict__ tb) {
+  const int e = el < 0 ? 0 : el;
+  const double u0 = pf_stage<EXPF>(tb, e, 0, T, t.var);
+  const double u1 = pf_stage<EXPF>(tb, e, 1, T, t.var);
+  const double u2 = pf_stage<EXPF>(tb, e, 2, T, t.var);
+  const double e1 = exp(clamp650(K.csaha2 * fz_tab_xi[e] * t.it));
+  const double e2 = exp(clamp650(K.csaha2 * fz_tab_xii[e] * t.it));
+  return make_double2(el >= 0 ? (u0 * (0.5 * rcp_d(u1))) * t.lamelec * e1 : 0.0,
+                      el >= 0 ? (u1 * (0.5 * rcp_d(u2))) * t.lamelec * e2 : 0.0);
+}
+
+// Bit j of the lane's hydrogen mask: its slot j holds hydrogen.
+template <int L>
+__device__ __forceinline__ unsigned saha_hyd(const Consts& K, int lane) {
+  unsigned h = 0u;
+#pragma unroll
+  for (int j = 0; j < WarpSahaT<L>::NS; ++j)
+    if (K.lane_elem[L * j + lane] == 0) h |= 1u << j;
+  return h;
+}
+
 // Per-lane Saha factors of the lane's elements at temperature T
-// (SHORT_PRE_ION_CALC_TEMPRHO, src/chemical_equilibrium.f90:1601-1652).
+// (SHORT_PRE_ION_CALC_TEMPRHO, src/chemical_equilibrium.f90:1601-1652): the
+// arithmetic of saha_t + saha_elem written inline (so the chain's register
+// allocation stays as it was), bit for bit the same values.
 template <int L>
 __device__ __forceinline__ void saha_prepare(WarpSahaT<L>& w, double T, const Consts& K,
                                              const PFTable* __restrict__ tb, int lane) {
   constexpr int NS = WarpSahaT<L>::NS;
-  constexpr int NEXP = 23 / L + 1;   // slots holding the 23 exponential-form elements
+  constexpr int NEXP = 32 / L;   // the lane's slots among the first 32 (the 23 exponential-form elements)
   w.T = T;
   w.hyd = 0u;
   const double it = rcp_d(T);
@@ -177,6 +223,22 @@ __device__ __forceinline__ void saha_prepare(WarpSahaT<L>& w, double T, const Co
     if (el == 0) w.hyd |= 1u << j;
     w.a1[j] = el >= 0 ? (u0 * (0.5 * rcp_d(u1))) * lamelec * e1 : 0.0;
     w.a2[j] = el >= 0 ? (u1 * (0.5 * rcp_d(u2))) * lamelec * e2 : 0.0;
+  }
+}
+
+
+// The lane's Saha factors of one temperature sample from a precomputed row
+// (96 slots of (a1, a2) in slot order, k_saha).
+template <int L>
+__device__ __forceinline__ void saha_load(WarpSahaT<L>& w, double T, unsigned hyd, const double2* __restrict__ row,
+                                          int lane) {
+  w.T = T;
+  w.hyd = hyd;
+#pragma unroll
+  for (int j = 0; j < WarpSahaT<L>::NS; ++j) {
+    const double2 a = __ldcs(row + L * j + lane);
+    w.a1[j] = a.x;
+    w.a2[j] = a.y;
   }
 }
 

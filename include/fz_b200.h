@@ -544,7 +544,9 @@ int fz_invert_warm(fz_ctx* ctx, fz_mlp* mlp, const float* norm, const float* bas
  * milliseconds, launch counts and processed columns (or LM slots; items
  * may be NULL) of the kernels (names in order:
  * "k_chain", "k_opac", "k_synth", "k_opac_rf", "k_synth_rf", "k_lm_fill",
- * "k_lm_accept", "k_lm_normal", "k_lm_solve", "k_lm_update", "k_chemder", "k_rf_prop") and resets
+ * "k_lm_accept", "k_lm_normal", "k_lm_solve", "k_lm_update", "k_chemder", "k_rf_prop", "k_lsf",
+ * "k_saha", "k_chain_pre": the chain of a batch of at most 1024 columns on
+ * k_saha's precomputed Saha factors) and resets
  * them; returns the kernel count.  Replaces the reference's
  * SYSTEM_CLOCK "Forward 3D:" timer (src/forward.f90:99-100, :295-297). */
 int fz_profile_enable(fz_ctx* ctx, int on);
