@@ -253,7 +253,7 @@ int fz_smooth_device(fz_ctx* ctx, int nx, int ny, float* d_models, const int* pa
  * stagnation counter (the STEPS of UPDATE_LAMBDA) reaches fallback_steps
  * while its best chi2 is still above fallback x its goal, instead of when
  * its search ends (0: when it ends; negative: at its first evaluation, i.e.
- * the initial model itself is judged).  fallback_free: 1 = the restarted
+ * the initial model itself decides).  fallback_free: 1 = the restarted
  * search ignores the goal and runs to the plain stop rules, 0 = it keeps
  * the goal.
  * solver: SOLVER_METHOD (MISC SETUP LINEAR_SOLVER), 1 (or 0) = the SVD
