@@ -213,3 +213,26 @@ def test_four_line_field_at_its_height_count(fz, orc):
         rel = err[:, j0:j0 + nj].max(axis=1) / scale
         assert rel.max() <= 2e-4, (p, rel.max())
         j0 += nj
+
+
+@pytest.mark.parametrize("he", [True, False])
+def test_small_batch_chain_on_precomputed_saha_factors(fz, workload, he):
+    """Batches of at most 1,024 columns run the chemistry chain on Saha
+    factors precomputed by k_saha (k_chain_pre); larger ones compute them
+    inside the chain.  Both forms (32 lanes a column at these sizes) give
+    the same columns bit for bit: 1,024 columns against the first 1,024 of
+    1,025."""
+    lines, reg = workload
+    ctx = fz.Synthesis(lines, reg, nz=64)
+    m = fz.atmos.make_columns(1025, 64, seed=77)
+    s_big, mo_big, st_big = ctx.forward(m, hydrostatic=he)
+    s_small, mo_small, st_small = ctx.forward(m[:1024], hydrostatic=he)
+    assert np.all(st_big == 0) and np.all(st_small == 0)
+    np.testing.assert_array_equal(s_small, s_big[:1024])
+    np.testing.assert_array_equal(mo_small, mo_big[:1024])
+    ctx.profile(True)
+    ctx.profile_read()
+    ctx.forward(m[:8], hydrostatic=he)
+    pr = ctx.profile_read()
+    ctx.profile(False)
+    assert pr["k_saha"][1] == 1 and pr["k_chain_pre"][1] == 1 and pr["k_chain"][1] == 0, pr
