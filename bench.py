@@ -311,9 +311,10 @@ def flops_table(csv_path, ncol, nz, numw, out_path):
                        "counted as 2) on --probe-kernels %d: %d seeded columns, NZ %d, NUMW %d, hydrostatic, nodes "
                        "T5 Bx2 By2 Bz2 vz2; bench.py multiplies by the columns of a launch" % (ncol, ncol, nz, numw),
            "kernels": kern}
-    if ncol <= SAHA_MAX_COLS:
-        # a small batch runs the chain on precomputed Saha factors: its two
-        # kernels join the table of the full-batch probe
+    if "k_saha" in kern:
+        # a small batch (at most SAHA_MAX_COLS columns) runs the chain on
+        # precomputed Saha factors: its two kernels join the table of the
+        # full-batch probe
         small = {"k_saha": kern["k_saha"], "k_chain_pre": kern["k_chain"]}
         doc = json.load(open(out_path)) if os.path.exists(out_path) else {"_comment": "", "kernels": {}}
         doc["kernels"].update(small)

@@ -1,0 +1,53 @@
+"""How far the oracle's own LM moves under rounding of its inputs, on the
+reference's test_inv1 case (T and v_z at all 256 heights, NP = 512,
+regularised): the FP64 oracle inverted twice for three iterations, once as
+is and once with its synthesis scaled by 1 + 5e-7 N(0, 1) and its node
+Jacobian by 1 + 2e-6 N(0, 1) -- the size of the FP32 rounding of the GPU
+path.  With the conjugate-gradient solver (LINEAR_SOLVER 2, stopped once
+the mean squared relative residual is below 1e-3) the chi2 after the second
+and third iterations moves by more than 1e-3, which is why the GPU-vs-oracle
+pin of that solver (tests/test_gpu_lm_big.py) holds chi2 to 2e-2 after the
+first iteration; with the SVD solver it moves by less than 1e-5."""
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(os.path.dirname(HERE), "oracle"))
+import lm_oracle as lmo  # noqa: E402
+import lmcase  # noqa: E402
+import test_gpu_lm_big as big  # noqa: E402
+
+
+def _chi2_per_iteration(orc, case, solver, nzn, eps, seed):
+    lines, reg, g, obs, init = case
+    nodes = {1: nzn, 7: nzn}
+    base = lmcase.oracle_forward_rf(orc, lines, reg, g, True, nodes)
+    rng = np.random.default_rng(seed)
+
+    def forward(models):
+        syn, jac, mo, st = base(models)
+        if eps:
+            syn = syn * (1.0 + eps * rng.standard_normal(syn.shape))
+            jac = jac * (1.0 + 4.0 * eps * rng.standard_normal(jac.shape))
+        return syn, jac, mo, st
+    rec = []
+    lmo.invert(forward, obs, init, nodes, lmo.weights(obs.shape[1] // 4, isigma=4e-3), maxsteps=5, maxit=3,
+               dchi2=0.0, reg=([1, 0, 0, 0, 0, 0, 1, 0], [0.01, 0, 0, 0, 0, 0, 0.1, 0]), solver=solver,
+               node_expansion=2, record=rec)
+    return np.array([r[0][2] for r in rec]), [r[0][6] for r in rec]
+
+
+def test_cg_chi2_moves_under_fp32_rounding_of_its_inputs(fz, orc):
+    case = big._inv1_case(fz, orc)
+    c0, a0 = _chi2_per_iteration(orc, case, 2, 256, 0.0, 0)
+    c1, a1 = _chi2_per_iteration(orc, case, 2, 256, 5e-7, 3)
+    rel = np.abs(c1 / c0 - 1.0)
+    assert a0 == a1
+    assert rel[0] < 1e-6
+    assert rel[1:].max() > 1e-3, rel
+    assert rel.max() < 2e-2, rel
+    s0, _ = _chi2_per_iteration(orc, case, 1, 32, 0.0, 0)
+    s1, _ = _chi2_per_iteration(orc, case, 1, 32, 5e-7, 3)
+    assert np.abs(s1 / s0 - 1.0).max() < 1e-5

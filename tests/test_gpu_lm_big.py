@@ -17,12 +17,16 @@ and the CTA-wide FP64 solvers.
 * The inversion at test_inv1's shape (NZ 256, Fe I 6301.5 blended with
   6302.5 x 500 wavelengths, T and v_z at every height, CG, STiC-like
   expansion, type-1 regularisation) run for 1, 2 and 3 iterations against
-  the oracle's inversion stopped at the same iteration: chi2 within 1e-3,
-  the accept decision, lambda and STEPS exactly.  The CG stops once the mean
-  squared relative residual is below 1e-3, so two FP64 runs on Hessians a
-  few 1e-6 apart may stop one iteration apart: the node values are compared
-  within 1 % of PARAM_NORM, and with the SVD solver on a 64-node layout
-  within 1e-4 of PARAM_NORM.
+  the oracle's inversion stopped at the same iteration: the accept
+  decision, lambda and STEPS exactly.  The CG stops once the mean squared
+  relative residual is below 1e-3, so two FP64 runs on Hessians a few 1e-6
+  apart may stop one iteration apart: the node values are compared within
+  1 % of PARAM_NORM, and chi2 within 1e-3 after the first iteration and
+  2e-2 after the later ones -- the oracle itself, its synthesis perturbed by
+  5e-7 and its Jacobian by 2e-6 (FP32 rounding), moves its third
+  iteration's chi2 by up to 1.2 % (tests/test_cg_sensitivity_cpu.py).  With
+  the SVD solver on a 64-node layout: chi2 within 1e-3 and node values
+  within 1e-4 of PARAM_NORM at every iteration.
 * test_inv1 itself through the control-file host.
 """
 import os
@@ -144,8 +148,9 @@ def test_large_layout_iterations_match_oracle(fz, orc, solver, nz_nodes, tol):
         mo, chi, it, st = ctx.invert(obs.reshape(1, 4, -1), init, hydrostatic=True, opts=opts)
         steps, chicur, chibest, precyc, lam, best, acc = rec[k - 1][0]
         assert st[0] == 0 and it[0] == k
-        assert abs(state[0, 2] - chibest) <= 1e-3 * chibest, (k, state[0], chibest)
-        assert abs(state[0, 1] - chicur) <= 1e-3 * chicur, (k, state[0], chicur)
+        ctol = 1e-3 if solver == 1 or k == 1 else 2e-2
+        assert abs(state[0, 2] - chibest) <= ctol * chibest, (k, state[0], chibest)
+        assert abs(state[0, 1] - chicur) <= ctol * chicur, (k, state[0], chicur)
         assert (state[0, 1] == state[0, 2]) == acc, k
         assert (state[0, 0], state[0, 3], state[0, 4]) == (steps, precyc, lam), (k, state[0])
         dn = np.abs(_nodevals(mo[0], nodes) - _nodevals(best, nodes))
