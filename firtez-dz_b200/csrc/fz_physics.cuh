@@ -415,7 +415,10 @@ __device__ __forceinline__ double get_damping(const LineP& L, double nh, double 
 // have real coefficients, so each is reduced modulo the real quadratic
 // (z^2 - 2 Re z z + |z|^2) that z solves (Knuth, TAOCP vol. 2, 4.6.4):
 // 2 FMA per degree instead of a complex multiply-add.  The quotient is
-// formed with range reduction (Smith), written without branches.
+// P conj(Q') sc / |Q'|^2 with Q' = Q sc, sc = 1 / max(|Re Q|, |Im Q|), so
+// |Q'|^2 lies in [1, 2] whatever the size of Q (an error in sc cancels);
+// its reciprocals are the approximate ones (a few ulp in all, far inside
+// the approximation's own error) and no compare or select is needed.
 __device__ __forceinline__ void voigt_f32(float a, float u, float& H, float& F) {
   const float A0 = 122.607931777104326f, A1 = 214.382388694706425f, A2 = 181.928533092181549f,
               A3 = 93.155580458138441f, A4 = 30.180142196210589f, A5 = 5.912626209773153f,
@@ -438,13 +441,11 @@ __device__ __forceinline__ void voigt_f32(float a, float u, float& H, float& F) 
   // P = p1 z + p0, Q = q1 z + q0
   const float nr = fmaf(p1, x, p0), ni = p1 * y;
   const float dr = fmaf(q1, x, q0), di = q1 * y;
-  const bool big = fabsf(dr) >= fabsf(di);
-  const float A = big ? dr : di, Bq = big ? di : dr;
-  const float X = big ? nr : ni, Y = big ? ni : nr;
-  const float rr = __fdividef(Bq, A);
-  const float den = __frcp_rn(fmaf(Bq, rr, A));
-  const float wr = fmaf(Y, rr, X) * den;
-  const float wi = (big ? 1.0f : -1.0f) * fmaf(-X, rr, Y) * den;
+  const float sc = __fdividef(1.0f, fmaxf(fabsf(dr), fabsf(di)));
+  const float dr1 = dr * sc, di1 = di * sc;
+  const float k = sc * __fdividef(1.0f, fmaf(dr1, dr1, di1 * di1));
+  const float wr = fmaf(nr, dr1, ni * di1) * k;
+  const float wi = fmaf(ni, dr1, -(nr * di1)) * k;
   H = wr;
   F = (u < 0.0f) ? -wi : wi;
 }

@@ -5,9 +5,11 @@ is and once with its synthesis scaled by 1 + 5e-7 N(0, 1) and its node
 Jacobian by 1 + 2e-6 N(0, 1) -- the size of the FP32 rounding of the GPU
 path.  With the conjugate-gradient solver (LINEAR_SOLVER 2, stopped once
 the mean squared relative residual is below 1e-3) the chi2 after the second
-and third iterations moves by more than 1e-3, which is why the GPU-vs-oracle
-pin of that solver (tests/test_gpu_lm_big.py) holds chi2 to 2e-2 after the
-first iteration; with the SVD solver it moves by less than 1e-5."""
+and third iterations moves by more than 1e-3 and the node values after the
+third by more than 1 % of PARAM_NORM, which is why the GPU-vs-oracle pin of
+that solver (tests/test_gpu_lm_big.py) holds chi2 to 2e-2 after the first
+iteration and the node values to 3 % after the third; with the SVD solver
+chi2 moves by less than 1e-5."""
 import os
 import sys
 
@@ -36,18 +38,21 @@ def _chi2_per_iteration(orc, case, solver, nzn, eps, seed):
     lmo.invert(forward, obs, init, nodes, lmo.weights(obs.shape[1] // 4, isigma=4e-3), maxsteps=5, maxit=3,
                dchi2=0.0, reg=([1, 0, 0, 0, 0, 0, 1, 0], [0.01, 0, 0, 0, 0, 0, 0.1, 0]), solver=solver,
                node_expansion=2, record=rec)
-    return np.array([r[0][2] for r in rec]), [r[0][6] for r in rec]
+    return (np.array([r[0][2] for r in rec]), [r[0][6] for r in rec],
+            [big._nodevals(r[0][5], nodes) for r in rec])
 
 
 def test_cg_chi2_moves_under_fp32_rounding_of_its_inputs(fz, orc):
     case = big._inv1_case(fz, orc)
-    c0, a0 = _chi2_per_iteration(orc, case, 2, 256, 0.0, 0)
-    c1, a1 = _chi2_per_iteration(orc, case, 2, 256, 5e-7, 3)
+    c0, a0, n0 = _chi2_per_iteration(orc, case, 2, 256, 0.0, 0)
+    c1, a1, n1 = _chi2_per_iteration(orc, case, 2, 256, 5e-7, 3)
     rel = np.abs(c1 / c0 - 1.0)
+    dn = [float(np.abs(a - b).max()) for a, b in zip(n1, n0)]
     assert a0 == a1
     assert rel[0] < 1e-6
     assert rel[1:].max() > 1e-3, rel
     assert rel.max() < 2e-2, rel
-    s0, _ = _chi2_per_iteration(orc, case, 1, 32, 0.0, 0)
-    s1, _ = _chi2_per_iteration(orc, case, 1, 32, 5e-7, 3)
+    assert dn[1] < 1e-2 < dn[2] < 3e-2, dn
+    s0, _, _ = _chi2_per_iteration(orc, case, 1, 32, 0.0, 0)
+    s1, _, _ = _chi2_per_iteration(orc, case, 1, 32, 5e-7, 3)
     assert np.abs(s1 / s0 - 1.0).max() < 1e-5

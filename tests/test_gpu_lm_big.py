@@ -20,11 +20,13 @@ and the CTA-wide FP64 solvers.
   the oracle's inversion stopped at the same iteration: the accept
   decision, lambda and STEPS exactly.  The CG stops once the mean squared
   relative residual is below 1e-3, so two FP64 runs on Hessians a few 1e-6
-  apart may stop one iteration apart: the node values are compared within
-  1 % of PARAM_NORM, and chi2 within 1e-3 after the first iteration and
-  2e-2 after the later ones -- the oracle itself, its synthesis perturbed by
-  5e-7 and its Jacobian by 2e-6 (FP32 rounding), moves its third
-  iteration's chi2 by up to 1.2 % (tests/test_cg_sensitivity_cpu.py).  With
+  apart may stop one iteration apart.  The oracle itself, its synthesis
+  perturbed by 5e-7 and its Jacobian by 2e-6 (FP32 rounding), moves its
+  chi2 by up to 0.2 % after the second iteration and 1.2 % after the
+  third, and its node values by up to 0.2 % and 2.3 % of PARAM_NORM
+  (tests/test_cg_sensitivity_cpu.py): chi2 is held within 1e-3 after the
+  first iteration and 2e-2 after the later ones, the node values within
+  1 % of PARAM_NORM after the first two and 3 % after the third.  With
   the SVD solver on a 64-node layout: chi2 within 1e-3 and node values
   within 1e-4 of PARAM_NORM at every iteration.
 * test_inv1 itself through the control-file host.
@@ -154,7 +156,8 @@ def test_large_layout_iterations_match_oracle(fz, orc, solver, nz_nodes, tol):
         assert (state[0, 1] == state[0, 2]) == acc, k
         assert (state[0, 0], state[0, 3], state[0, 4]) == (steps, precyc, lam), (k, state[0])
         dn = np.abs(_nodevals(mo[0], nodes) - _nodevals(best, nodes))
-        assert dn.max() <= tol, (k, float(dn.max()))
+        ntol = 3e-2 if solver == 2 and k == 3 else tol
+        assert dn.max() <= ntol, (k, float(dn.max()))
 
 
 def test_reference_inversion_test_case_runs(fz, tmp_path):
