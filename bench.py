@@ -311,15 +311,22 @@ def flops_table(csv_path, ncol, nz, numw, out_path):
                        "counted as 2) on --probe-kernels %d: %d seeded columns, NZ %d, NUMW %d, hydrostatic, nodes "
                        "T5 Bx2 By2 Bz2 vz2; bench.py multiplies by the columns of a launch" % (ncol, ncol, nz, numw),
            "kernels": kern}
+    old = json.load(open(out_path)) if os.path.exists(out_path) else {"_comment": "", "kernels": {}}
     if "k_saha" in kern:
         # a small batch (at most SAHA_MAX_COLS columns) runs the chain on
         # precomputed Saha factors: its two kernels join the table of the
         # full-batch probe
-        small = {"k_saha": kern["k_saha"], "k_chain_pre": kern["k_chain"]}
-        doc = json.load(open(out_path)) if os.path.exists(out_path) else {"_comment": "", "kernels": {}}
-        doc["kernels"].update(small)
+        doc = old
+        doc["kernels"].update({"k_saha": kern["k_saha"], "k_chain_pre": kern["k_chain"]})
         doc["_comment_small"] = ("k_saha and k_chain_pre (the chain of a batch of at most %d columns on precomputed "
                                  "Saha factors) from --probe-kernels %d" % (SAHA_MAX_COLS, ncol))
+    else:
+        # a full-batch table keeps the small-batch kernels of an earlier probe
+        for k in ("k_saha", "k_chain_pre"):
+            if k in old.get("kernels", {}):
+                doc["kernels"][k] = old["kernels"][k]
+        if "_comment_small" in old:
+            doc["_comment_small"] = old["_comment_small"]
     with open(out_path, "w") as f:
         json.dump(doc, f, indent=1)
     print(json.dumps(doc))
