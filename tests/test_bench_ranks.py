@@ -112,3 +112,32 @@ def test_flops_table_from_an_ncu_csv(tmp_path):
     assert k["k_chain"]["pipe"] == "fp64" and k["k_chain"]["launches"] == 3
     assert k["k_chain"]["flop_per_column"] == 1200 / 10          # the median of 1000, 1200, 1400
     assert k["k_synth_rf"]["flop_per_column_height_lambda"] == k["k_synth_rf"]["flop_per_column"] / 10
+
+
+def test_flops_table_merges_the_small_batch_kernels(tmp_path):
+    """A probe of at most 1,024 columns runs the chain on precomputed Saha
+    factors: its capture (k_saha + k_chain) adds k_saha and k_chain_pre to
+    the table of the full-batch probe, and a later full-batch table keeps
+    them."""
+    bench = _bench()
+    hdr = ["ID", "Kernel Name", "Metric Name", "Metric Value"]
+
+    def capture(path, kernels):
+        rows = []
+        for i, (name, dfma) in enumerate(kernels):
+            for op, v in (("ffma", 1), ("fadd", 0), ("fmul", 0), ("dfma", dfma), ("dadd", 0), ("dmul", 0)):
+                rows.append([str(i), name, "smsp__sass_thread_inst_executed_op_%s_pred_on.sum" % op, str(v)])
+        path.write_text("\n".join(",".join('"%s"' % c for c in r) for r in [hdr] + rows) + "\n")
+
+    out = tmp_path / "flops.json"
+    full, small = tmp_path / "full.csv", tmp_path / "small.csv"
+    capture(full, (("void k_chain<1, 16, 0>(int)", 900), ("void k_synth(int)", 0)))
+    capture(small, (("void k_saha<1>(int)", 300), ("void k_chain<1, 32, 1>(int)", 500)))
+    bench.flops_table(str(full), 10, 2, 5, str(out))
+    bench.flops_table(str(small), 10, 2, 5, str(out))
+    k = json.load(open(out))["kernels"]
+    assert k["k_chain"]["flop_per_column"] == 180 and k["k_saha"]["flop_per_column"] == 60
+    assert k["k_chain_pre"]["flop_per_column"] == 100 and "k_synth" in k
+    bench.flops_table(str(full), 10, 2, 5, str(out))
+    k = json.load(open(out))["kernels"]
+    assert k["k_chain"]["flop_per_column"] == 180 and k["k_chain_pre"]["flop_per_column"] == 100
